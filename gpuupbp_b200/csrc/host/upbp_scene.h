@@ -1,0 +1,33 @@
+// Host-side scene owned by the library (the result of the OBJ/AUX loader) and
+// the camera set-up shared by the loader and the device context.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../../include/upbp.h"
+
+struct upbp_scene {
+    std::vector<float> verts, normals;
+    std::vector<int32_t> tri_material, tri_light;
+    std::vector<upbp_material> materials;
+    std::vector<upbp_medium> media;
+    std::vector<upbp_light> lights;
+    upbp_scene_desc desc{};
+    void finalize();  // points desc at the vectors
+};
+
+namespace upbp_host {
+
+// Camera matrices and image-plane distance (gpuupbp/host/camera.hpp:33-76),
+// row-major 4x4.
+struct CameraMatrices {
+    float origin[3], direction[3];
+    float raster_to_world[16], world_to_raster[16];
+    float image_plane_dist;
+};
+CameraMatrices camera_setup(const upbp_camera_desc& c, float res_x, float res_y);
+
+void set_error(const std::string& msg);
+
+}  // namespace upbp_host

@@ -1,0 +1,205 @@
+// BVH traversal: closest hit and all-hits over triangles, and range queries
+// (point-in-radius, segment-near-point, segment/point-vs-beam) over the
+// per-iteration photon maps.  Traversal stacks live in registers/local memory,
+// bounded at kStackDepth; overflow sets kErrTraversalStack and drops the
+// remaining subtree (never an unbounded loop).
+#pragma once
+
+#include "upbp_device.cuh"
+
+namespace upbp {
+
+constexpr int kStackDepth = 64;
+
+UPBP_D float3 safe_inv(float3 d) { return make_float3(1.f / d.x, 1.f / d.y, 1.f / d.z); }
+
+// Segment [tmin, tmax] vs box [lo - pad, hi + pad].  Axes with a zero
+// direction component produce NaN/inf slabs, which fminf/fmaxf drop or
+// reject, so the test never misses a box the segment touches.
+UPBP_D bool slab(float3 lo, float3 hi, float pad, float3 o, float3 inv, float tmin, float tmax)
+{
+    const float tx0 = (lo.x - pad - o.x) * inv.x, tx1 = (hi.x + pad - o.x) * inv.x;
+    const float ty0 = (lo.y - pad - o.y) * inv.y, ty1 = (hi.y + pad - o.y) * inv.y;
+    const float tz0 = (lo.z - pad - o.z) * inv.z, tz1 = (hi.z + pad - o.z) * inv.z;
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    return tn <= tf;
+}
+
+UPBP_D bool inside(float3 lo, float3 hi, float pad, float3 x)
+{
+    return x.x >= lo.x - pad && x.x <= hi.x + pad && x.y >= lo.y - pad && x.y <= hi.y + pad && x.z >= lo.z - pad &&
+           x.z <= hi.z + pad;
+}
+
+struct NodeBoxes {
+    float3 llo, lhi, rlo, rhi;
+    int l, r;
+};
+
+UPBP_D NodeBoxes load_node(const BvhNode* nodes, int i)
+{
+    const BvhNode* n = nodes + i;
+    const float4 a = __ldg(&n->a), b = __ldg(&n->b), c = __ldg(&n->c);
+    const int4 k = __ldg(&n->link);
+    NodeBoxes r;
+    r.llo = make_float3(a.x, a.y, a.z);
+    r.lhi = make_float3(a.w, b.x, b.y);
+    r.rlo = make_float3(b.z, b.w, c.x);
+    r.rhi = make_float3(c.y, c.z, c.w);
+    r.l = k.x;
+    r.r = k.y;
+    return r;
+}
+
+// Visits every leaf whose box (dilated by pad) passes `test_box`; calls
+// leaf(sorted_index) which returns false to stop.  Returns false if the
+// traversal stack overflowed.
+template <class BoxTest, class Leaf>
+UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& leaf)
+{
+    if (bvh.count == 0) return true;
+    int stack[kStackDepth];
+    int sp = 0;
+    int node = bvh.count > 1 ? 0 : ~0;
+    bool ok = true;
+    for (;;) {
+        if (node < 0) {
+            if (!leaf(~node)) return ok;
+        } else {
+            const NodeBoxes nb = load_node(bvh.nodes, node);
+            const bool hl = test_box(nb.llo, nb.lhi, pad);
+            const bool hr = test_box(nb.rlo, nb.rhi, pad);
+            if (hl && hr) {
+                if (sp < kStackDepth) {
+                    stack[sp++] = nb.r;
+                } else {
+                    ok = false;
+                }
+                node = nb.l;
+                continue;
+            }
+            if (hl) {
+                node = nb.l;
+                continue;
+            }
+            if (hr) {
+                node = nb.r;
+                continue;
+            }
+        }
+        if (sp == 0) return ok;
+        node = stack[--sp];
+    }
+}
+
+// Moller-Trumbore, double sided; identical arithmetic to the oracle's test.
+UPBP_D bool tri_intersect(const float4* tri, int s, float3 o, float3 d, float& t, float& u, float& v)
+{
+    const float4 a = __ldg(&tri[3 * s]), b = __ldg(&tri[3 * s + 1]), c = __ldg(&tri[3 * s + 2]);
+    const float3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
+    const float3 p = cross(d, e2);
+    const float det = dot(e1, p);
+    if (det == 0.f) return false;
+    const float inv = 1.f / det;
+    const float3 sv = o - v0;
+    u = dot(sv, p) * inv;
+    if (u < 0.f || u > 1.f) return false;
+    const float3 q = cross(sv, e1);
+    v = dot(d, q) * inv;
+    if (v < 0.f || u + v > 1.f) return false;
+    t = dot(e2, q) * inv;
+    return true;
+}
+
+struct TriHit {
+    float t, u, v;
+    int prim;  // original triangle index
+};
+
+// Closest triangle hit with t in [tmin, tmax]; ordered traversal, near child first.
+UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float tmax, TriHit& hit, bool& overflow)
+{
+    if (tv.bvh.count == 0) return false;
+    const float3 inv = safe_inv(d);
+    int stack[kStackDepth];
+    int sp = 0;
+    int node = tv.bvh.count > 1 ? 0 : ~0;
+    bool found = false;
+    float best = tmax;
+    for (;;) {
+        if (node < 0) {
+            float t, u, v;
+            const int s = ~node;
+            if (tri_intersect(tv.tri, s, o, d, t, u, v) && t >= tmin && t <= best) {
+                best = t;
+                hit.t = t;
+                hit.u = u;
+                hit.v = v;
+                hit.prim = __float_as_int(__ldg(&tv.tri[3 * s]).w);
+                found = true;
+            }
+        } else {
+            const NodeBoxes nb = load_node(tv.bvh.nodes, node);
+            // entry distances for ordering
+            const float3 t0l = (nb.llo - o) * inv, t1l = (nb.lhi - o) * inv;
+            const float3 t0r = (nb.rlo - o) * inv, t1r = (nb.rhi - o) * inv;
+            const float nl = fmaxf(fmaxf(fminf(t0l.x, t1l.x), fminf(t0l.y, t1l.y)), fmaxf(fminf(t0l.z, t1l.z), tmin));
+            const float fl = fminf(fminf(fmaxf(t0l.x, t1l.x), fmaxf(t0l.y, t1l.y)), fminf(fmaxf(t0l.z, t1l.z), best));
+            const float nr = fmaxf(fmaxf(fminf(t0r.x, t1r.x), fminf(t0r.y, t1r.y)), fmaxf(fminf(t0r.z, t1r.z), tmin));
+            const float fr = fminf(fminf(fmaxf(t0r.x, t1r.x), fmaxf(t0r.y, t1r.y)), fminf(fmaxf(t0r.z, t1r.z), best));
+            const bool hl = nl <= fl * 1.00001f + 1e-7f, hr = nr <= fr * 1.00001f + 1e-7f;
+            if (hl && hr) {
+                const bool left_first = nl <= nr;
+                if (sp < kStackDepth) {
+                    stack[sp++] = left_first ? nb.r : nb.l;
+                } else {
+                    overflow = true;
+                }
+                node = left_first ? nb.l : nb.r;
+                continue;
+            }
+            if (hl) {
+                node = nb.l;
+                continue;
+            }
+            if (hr) {
+                node = nb.r;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    return found;
+}
+
+// Every triangle hit with t in [tmin, tmax]; calls f(hit) for each, f returns
+// false to stop.
+template <class F>
+UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tmax, F&& f)
+{
+    const float3 inv = safe_inv(d);
+    return bvh_walk(
+        tv.bvh, 0.f,
+        [&](float3 lo, float3 hi, float) {
+            const float3 t0 = (lo - o) * inv, t1 = (hi - o) * inv;
+            const float n = fmaxf(fmaxf(fminf(t0.x, t1.x), fminf(t0.y, t1.y)), fmaxf(fminf(t0.z, t1.z), tmin));
+            const float fa = fminf(fminf(fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y)), fminf(fmaxf(t0.z, t1.z), tmax));
+            return n <= fa * 1.00001f + 1e-7f;
+        },
+        [&](int s) {
+            float t, u, v;
+            if (tri_intersect(tv.tri, s, o, d, t, u, v) && t >= tmin && t <= tmax) {
+                TriHit h;
+                h.t = t;
+                h.u = u;
+                h.v = v;
+                h.prim = __float_as_int(__ldg(&tv.tri[3 * s]).w);
+                return f(h);
+            }
+            return true;
+        });
+}
+
+}  // namespace upbp

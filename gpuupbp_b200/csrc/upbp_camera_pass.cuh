@@ -1,0 +1,694 @@
+// Camera pass: one thread per pixel.  Emitter hits, next-event estimation,
+// BPT connections to one random light subpath, and the five photon density
+// estimators as range queries over the per-iteration photon maps.
+// Follows __raygen__trace_camera (gpuupbp/kernel/trace_camera.cu:49-390),
+// functs_camera.cuh:41-527 and the estimator bodies in gpuupbp/kernel/pde/
+// (functs_pp.cuh:44-136, functs_pb2d.cuh:57-342, functs_bb1d.cuh:57-397,
+// functs_bp2d.cuh:51-229).
+#pragma once
+
+#include "upbp_paths.cuh"
+
+namespace upbp {
+
+UPBP_D unsigned generate_camera_sample(float2& screen, unsigned pixel, PathState& s, Rng& rng)
+{
+    const DeviceParams& p = c_params;
+    const DCamera& cam = p.camera;
+    const int res_x = int(cam.res_x);
+    const unsigned x = pixel % res_x, y = pixel / res_x;
+    // The reference draws both jitter values inside one make_float2 call, whose
+    // argument order C++ leaves unspecified; the host-compiled oracle evaluates
+    // right to left, so the first draw is the y jitter.  Same below for NEE.
+    const float j1 = rng.uniform();
+    const float j0 = rng.uniform();
+    screen = make_float2(float(x) + j0, float(y) + j1);
+    const float3 wr = transform_point(cam.raster_to_world, make_float3(screen.x, screen.y, 0.f));
+    s.origin = cam.origin;
+    s.dir = normalize(wr - cam.origin);
+    const float cos_at_cam = dot(cam.direction, s.dir);
+    const float ip_dist = cam.image_plane_dist / cos_at_cam;
+    const float camera_pdf_w = (ip_dist * ip_dist) / cos_at_cam;
+    s.throughput = v3(1.f);
+    s.path_length = 1;
+    s.is_specular_path = true;
+    s.is_infinite_light = false;
+    VertexWeights& w = s.sw.w;
+    w.d_shared = p.light_subpath_count / camera_pdf_w;
+    w.d_bpt = 0.f;
+    w.d_pde = 0.f;
+    w.prev_specular = false;
+    w.prev_in_medium = false;
+    if (!init_boundary_stack(s.stack)) return kErrBoundaryStack;
+    if (cam.mat_id != -1 && cam.med_id != -1) {
+        if (!s.stack.push(Boundary{cam.mat_id, cam.med_id}, boundary_priority(cam.mat_id))) return kErrBoundaryStack;
+    }
+    return 0;
+}
+
+// Emitter hit, MIS Eq D.32/D.33 (functs_camera.cuh:107-165).
+UPBP_D float3 light_hit_radiance(const DLight& l, const PathState& s, float rs_rev)
+{
+    const DeviceParams& p = c_params;
+    if (s.is_specular_path && p.ignore_fully_spec_paths) return v3(0.f);
+    const float pick = 1.f / float(p.light_count);
+    float direct_pdf_a, emission_pdf_w;
+    const float3 rad = light_radiance(l, s.dir, direct_pdf_a, emission_pdf_w);
+    if (is_black_or_negative(rad)) return v3(0.f);
+    if (s.path_length == 1) return rad;
+    if (p.estimator_techniques && !(p.estimator_techniques & kBpt)) return s.is_specular_path ? rad : v3(0.f);
+    direct_pdf_a *= pick;
+    emission_pdf_w *= pick;
+    const VertexWeights& wc = s.sw.w;
+    const float bpt = !wc.prev_specular;
+    const float w_camera = direct_pdf_a * bpt * wc.d_shared + emission_pdf_w * rs_rev * wc.d_bpt;
+    return (1.f / (0.f + 1.f + w_camera)) * rad;
+}
+
+// Next-event estimation, MIS Eq D.36/D.37 (functs_camera.cuh:170-344).
+UPBP_D unsigned direct_illumination(float3& contrib, const PathState& s, float3 hit, const Bsdf& bsdf, Rng& rng,
+                                    VolSeg* segs)
+{
+    const DeviceParams& p = c_params;
+    const float pick = 1.f / float(p.light_count);
+    const int lid = int(rng.uniform() * float(p.light_count));
+    const float u1 = rng.uniform();
+    const float u0 = rng.uniform();
+    const DLight& l = p.lights[lid];
+    contrib = v3(0.f);
+    if (!light_is_finite(l) && p.media[p.global_medium].has_attenuation) return 0;
+    float3 dir;
+    float dist, direct_pdf_w, emission_pdf_w, cos_at_light;
+    const float3 rad = light_illuminate(l, hit, u0, u1, dir, dist, direct_pdf_w, emission_pdf_w, cos_at_light);
+    if (is_black_or_negative(rad)) return 0;
+    float fpdf, rpdf, cos_to_light, sin_theta;
+    const float3 f = bsdf_eval(bsdf, dir, cos_to_light, &fpdf, &rpdf, &sin_theta);
+    if (is_black_or_negative(f)) return 0;
+    const float cp = bsdf.cont_prob;
+    fpdf *= light_is_delta(l) ? 0.f : cp;
+    rpdf *= cp;
+    int nseg = 0;
+    bool occ;
+    const unsigned st = occluded(occ, hit, dir, dist, s.stack, bsdf.in_medium() ? kOriginInMedium : 0u, segs, nseg, rng);
+    if (st) return st;
+    if (occ) return 0;
+    float n_for = 1.f, n_rev = 1.f;
+    float3 att = v3(1.f);
+    if (nseg > 0) {
+        n_for = seg_for_pdf(segs, nseg);
+        n_rev = seg_rev_pdf(segs, nseg);
+        att = seg_attenuation(segs, nseg);
+        if (!is_positive(att)) return 0;
+    }
+    const float w_light = fpdf / (pick * direct_pdf_w);
+    const VertexWeights& wc = s.sw.w;
+    const float ft = pde_factor(bsdf.in_medium(), false, 1.f / n_rev, wc.rev_ratio, wc.for_inv, wc.for_ratio, sin_theta);
+    const float b = !wc.prev_specular;
+    const float w_camera = (emission_pdf_w * cos_to_light / (direct_pdf_w * cos_at_light)) * n_rev *
+                           (ft + b * wc.d_shared + (rpdf / wc.rev_inv) * wc.d_bpt);
+    const float mis = 1.f / (w_light + 1.f + w_camera);
+    contrib = ((cos_to_light / (pick * direct_pdf_w)) * (rad * att * f)) * mis;
+    if (is_black_or_negative(contrib)) contrib = v3(0.f);
+    return 0;
+}
+
+// BPT connection of a camera and a light vertex, Eq 4.50/4.51
+// (functs_camera.cuh:349-527).
+UPBP_D unsigned connect_vertices(float3& contrib, const LightVertex& lv, const Bsdf& cb, float3 chit, const PathState& s,
+                                 Rng& rng, VolSeg* segs)
+{
+    contrib = v3(0.f);
+    float3 dir = lv.hit - chit;
+    const float d2 = dot(dir, dir);
+    const float dist = sqrtf(d2);
+    dir /= dist;
+    float cos_c, c_fpdf, c_rpdf, sin_c;
+    const float3 cf = bsdf_eval(cb, dir, cos_c, &c_fpdf, &c_rpdf, &sin_c);
+    if (is_black_or_negative(cf)) return 0;
+    c_fpdf *= cb.cont_prob;
+    c_rpdf *= cb.cont_prob;
+    float cos_l, l_fpdf, l_rpdf, sin_l;
+    const float3 lf = bsdf_eval(lv.bsdf, -dir, cos_l, &l_fpdf, &l_rpdf, &sin_l);
+    if (is_black_or_negative(lf)) return 0;
+    l_fpdf *= lv.bsdf.cont_prob;
+    l_rpdf *= lv.bsdf.cont_prob;
+    const float g = cos_l * cos_c / d2;
+    if (g < 0.f) return 0;
+    const float c_fpdf_a = pdf_w_to_a(c_fpdf, dist, cos_l);
+    const float l_fpdf_a = pdf_w_to_a(l_fpdf, dist, cos_c);
+    unsigned sflags = 0;
+    if (cb.in_medium()) sflags |= kOriginInMedium;
+    if (lv.in_medium) sflags |= kEndInMedium;
+    int nseg = 0;
+    bool occ;
+    const unsigned st = occluded(occ, chit, dir, dist, s.stack, sflags, segs, nseg, rng);
+    if (st) return st;
+    if (occ) return 0;
+    float rs_for = 1.f, rs_rev = 1.f;
+    float3 att = v3(1.f);
+    if (nseg > 0) {
+        rs_for = seg_for_pdf(segs, nseg);
+        rs_rev = seg_rev_pdf(segs, nseg);
+        att = seg_attenuation(segs, nseg);
+        if (!is_positive(att)) return 0;
+    }
+    const VertexWeights& wl = lv.w;
+    const VertexWeights& wc = s.sw.w;
+    const float f_s = pde_factor(lv.bsdf.in_medium(), false, wl.for_inv, wl.for_ratio, 1.f / rs_for, wl.rev_ratio, sin_l);
+    const float bs = !wl.prev_specular;
+    const float w_light = c_fpdf_a * rs_for * (f_s + bs * wl.d_shared + (l_rpdf / wl.rev_inv) * wl.d_bpt);
+    const float f_t = pde_factor(cb.in_medium(), false, 1.f / rs_rev, wc.rev_ratio, wc.for_inv, wc.for_ratio, sin_c);
+    const float bt = !wc.prev_specular;
+    const float w_camera = l_fpdf_a * rs_rev * (f_t + bt * wc.d_shared + (c_rpdf / wc.rev_inv) * wc.d_bpt);
+    const float mis = 1.f / (w_light + 1.f + w_camera);
+    contrib = (g * cf * lf * att) * mis;
+    if (is_black_or_negative(contrib)) contrib = v3(0.f);
+    return 0;
+}
+
+// SURF / PP3D merge of a camera vertex with one photon, Eq 4.52/4.17/4.53
+// (functs_pp.cuh:44-136).
+UPBP_D float3 eval_point_merge(const LightVertex& lv, const PathState& s, const Bsdf& cb, bool medium)
+{
+    const DeviceParams& p = c_params;
+    const unsigned plen = lv.path_length + s.path_length;
+    if (plen > p.max_path_length || plen < p.min_path_length) return v3(0.f);
+    const float3 pdir = lv.bsdf.dir_fix();
+    float cos_c, fpdf, rpdf, sin_theta;
+    const float3 f = bsdf_eval(cb, pdir, cos_c, &fpdf, &rpdf, &sin_theta);
+    if (is_black_or_negative(f)) return v3(0.f);
+    fpdf *= cb.cont_prob;
+    rpdf *= lv.bsdf.cont_prob;
+    const VertexWeights& wl = lv.w;
+    const VertexWeights& wc = s.sw.w;
+    const float ff = p.photon_beam_type == kLongBeam ? wl.for_inv : wl.for_ratio;
+    const float rf = p.camera_beam_type == kLongBeam ? wc.for_inv : wc.for_ratio;
+    const float val = medium ? 1.f / p.mis_factor_pp3d : 1.f / p.mis_factor_surf;
+    const float bs = !wl.prev_specular;
+    const float w_light = val * (wl.d_shared * bs * p.subpath_count_bpt + fpdf * wl.d_pde / wl.rev_inv);
+    const float w_local =
+        1.f + float(medium) * val * (p.mis_factor_bb1d * sin_theta * ff * rf + p.mis_factor_bp2d * ff + p.mis_factor_pb2d * rf);
+    const float bt = !wc.prev_specular;
+    const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
+    const float mis = 1.f / (w_light + w_local + w_camera);
+    return mis * f * lv.thr;
+}
+
+UPBP_D float3 query_points(const PointMap& map, float3 x, float r, float r2, const PathState& s, const Bsdf& cb,
+                           bool medium)
+{
+    float3 acc = v3(0.f);
+    const float pad = r * 1.0001f + 1e-7f;
+    const bool ok = bvh_walk(
+        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
+        [&](int i) {
+            const float4 pp = __ldg(&map.pos[i]);
+            if (pred_point_point(x, xyz(pp), r2)) {
+                LightVertex lv;
+                load_vertex(c_params.vertices + fbits(pp.w), lv);
+                acc += eval_point_merge(lv, s, cb, medium);
+            }
+            return true;
+        });
+    if (!ok) flag_status(kErrTraversalStack);
+    return acc;
+}
+
+struct QuerySeg {
+    float3 o, d;
+    float dmin, dmax;
+    int med;
+    float for_pdf, rev_pdf;
+    unsigned flags;
+    unsigned cam_path_length;
+};
+
+// PB2D: camera query beam x photon point (functs_pb2d.cuh:57-201).
+UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVertex& lv, float isect_dist, float rad2)
+{
+    const DeviceParams& p = c_params;
+    const unsigned plen = lv.path_length + q.cam_path_length;
+    if (plen > p.max_path_length || plen < p.min_path_length) return v3(0.f);
+    const DMedium& m = p.media[q.med];
+    float3 att = attenuation(m, isect_dist - q.dmin);
+    const float pdf = component(att, m.min_pos_att_idx);
+    if (p.camera_beam_type == kShortBeam) att /= pdf;
+    float rs_for = m.min_pos_att * pdf;
+    float rs_rev = (q.flags & kOriginInMedium) ? rs_for : pdf;
+    const float ratio = 1.f / m.min_pos_att;
+    if (!is_positive(att)) return v3(0.f);
+    rs_for *= q.for_pdf;
+    rs_rev *= q.rev_pdf;
+    VertexWeights wc = cw.w;
+    if (q.cam_path_length > 1u) {
+        const float f_i = pde_factor(wc.prev_in_medium, wc.prev_specular, 1.f / rs_rev, wc.rev_ratio, wc.for_inv,
+                                     wc.for_ratio, cw.last_sin_theta);
+        wc.d_pde = cw.d_pde_a * f_i + cw.d_pde_b;
+        wc.d_bpt = cw.d_bpt_a * f_i + cw.d_bpt_b;
+    }
+    const float3 pdir = lv.bsdf.dir_fix();
+    float sin_theta;
+    const float ph = hg_pdf(-q.d, pdir, m.mean_cosine, &sin_theta);
+    const float3 f = v3(ph);
+    if (is_black_or_negative(f)) return v3(0.f);
+    const float fpdf = ph * m.cont_prob;
+    const float rpdf = ph * lv.bsdf.cont_prob;
+    wc.d_shared *= isect_dist * isect_dist;
+    wc.d_shared /= rs_for;
+    wc.d_bpt /= rs_for;
+    wc.d_pde /= rs_for;
+    wc.for_inv = 1.f / rs_for;
+    wc.rev_inv = 1.f / rs_rev;
+    wc.for_ratio = ratio;
+    wc.rev_ratio = ratio;
+    const float kernel = (1.f - rad2 / p.radius_pb2d_2) / (p.radius_pb2d_2 * kPi * .5f);
+    if (!is_positive(kernel)) return v3(0.f);
+    const float3 unweighted = lv.thr * att * m.scattering * f * kernel;
+    if (is_black_or_negative(unweighted)) return v3(0.f);
+    const VertexWeights& wl = lv.w;
+    const float ff = p.photon_beam_type == kLongBeam ? wl.for_inv : wl.for_ratio;
+    const float rf = p.camera_beam_type == kLongBeam ? wc.for_inv : wc.for_ratio;
+    const float val = 1.f / (p.mis_factor_pb2d * rf);
+    const float bs = !wl.prev_specular;
+    const float w_light = val * (wl.d_shared * bs * p.subpath_count_bpt + fpdf * wl.d_pde / wl.rev_inv);
+    const float w_local = 1.f + val * (p.mis_factor_bb1d * sin_theta * ff * rf + p.mis_factor_bp2d * ff + p.mis_factor_pp3d);
+    const float bt = !wc.prev_specular;
+    const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
+    const float mis = 1.f / (w_light + w_local + w_camera);
+    return mis * unweighted;
+}
+
+// BB1D: camera query beam x photon beam (functs_bb1d.cuh:57-248).
+UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& lb, float bb_dist, float sin_theta,
+                        float tc, float tp)
+{
+    const DeviceParams& p = c_params;
+    const unsigned plen = lb.path_length + q.cam_path_length;
+    if (plen > p.max_path_length || plen < p.min_path_length) return v3(0.f);
+    const DMedium& m = p.media[q.med];
+    float3 att_c = attenuation(m, tc - q.dmin);
+    const float pc = component(att_c, m.min_pos_att_idx);
+    if (p.camera_beam_type == kShortBeam) att_c /= pc;
+    float rsf_c = m.min_pos_att * pc;
+    float rsr_c = (q.flags & kOriginInMedium) ? rsf_c : pc;
+    const float ratio = 1.f / m.min_pos_att;
+    float3 att_p = attenuation(m, tp);
+    const float pp = component(att_p, m.min_pos_att_idx);
+    if (p.photon_beam_type == kShortBeam) att_p /= pp;
+    float rsf_p = m.min_pos_att * pp;
+    float rsr_p = (lb.flags & kOriginInMedium) ? rsf_p : pp;
+    const float3 att = att_c * att_p;
+    if (!is_positive(att)) return v3(0.f);
+    rsf_c *= q.for_pdf;
+    rsr_c *= q.rev_pdf;
+    VertexWeights wc = cw.w;
+    if (q.cam_path_length > 1u) {
+        const float f_i = pde_factor(wc.prev_in_medium, wc.prev_specular, 1.f / rsr_c, wc.rev_ratio, wc.for_inv,
+                                     wc.for_ratio, cw.last_sin_theta);
+        wc.d_pde = cw.d_pde_a * f_i + cw.d_pde_b;
+        wc.d_bpt = cw.d_bpt_a * f_i + cw.d_bpt_b;
+    }
+    rsf_p *= lb.for_pdf;
+    rsr_p *= lb.rev_pdf;
+    VertexWeights wl = lb.sw.w;
+    if (lb.path_length > 1u) {
+        const float f_i = pde_factor(wl.prev_in_medium, wl.prev_specular, wl.for_inv, wl.for_ratio, 1.f / rsr_p,
+                                     wl.rev_ratio, lb.sw.last_sin_theta);
+        wl.d_pde = lb.sw.d_pde_a * f_i + lb.sw.d_pde_b;
+        wl.d_bpt = lb.sw.d_bpt_a * f_i + lb.sw.d_bpt_b;
+    }
+    const float ph = hg_pdf(-q.d, -lb.d, m.mean_cosine, nullptr);
+    const float3 f = v3(ph);
+    if (is_black_or_negative(f)) return v3(0.f);
+    const float fpdf = ph * m.cont_prob;
+    const float rpdf = ph * m.cont_prob;
+    wc.d_shared *= tc * tc;
+    wc.d_shared /= rsf_c;
+    wc.d_bpt /= rsf_c;
+    wc.d_pde /= rsf_c;
+    wc.for_inv = 1.f / rsf_c;
+    wc.rev_inv = 1.f / rsr_c;
+    wc.for_ratio = ratio;
+    wc.rev_ratio = ratio;
+    // the reference multiplies by dist^2 except for first-segment beams of
+    // finite lights (functs_bb1d.cuh:191); kept for parity
+    if (!(lb.path_length == 1 && !lb.infinite)) wl.d_shared *= tp * tp;
+    wl.d_shared /= rsf_p;
+    wl.d_bpt /= rsf_p;
+    wl.d_pde /= rsf_p;
+    wl.for_inv = 1.f / rsf_p;
+    wl.rev_inv = 1.f / rsr_p;
+    wl.for_ratio = ratio;
+    wl.rev_ratio = ratio;
+    const float kernel = (1.f - bb_dist * bb_dist / p.radius_bb1d_2) * 3.f / (4.f * p.radius_bb1d * sin_theta);
+    if (!is_positive(kernel)) return v3(0.f);
+    const float3 unweighted = lb.thr * m.scattering * att * f * kernel;
+    if (is_black_or_negative(unweighted)) return v3(0.f);
+    const float ff = p.photon_beam_type == kLongBeam ? wl.for_inv : wl.for_ratio;
+    const float rf = p.camera_beam_type == kLongBeam ? wc.for_inv : wc.for_ratio;
+    const float val = 1.f / (p.mis_factor_bb1d * sin_theta * ff * rf);
+    const float bs = !wl.prev_specular;
+    const float w_light = val * (wl.d_shared * bs * p.subpath_count_bpt + fpdf * wl.d_pde / wl.rev_inv);
+    const float w_local = 1.f + val * (p.mis_factor_bp2d * ff + p.mis_factor_pb2d * rf + p.mis_factor_pp3d);
+    const float bt = !wc.prev_specular;
+    const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
+    const float mis = 1.f / (w_light + w_local + w_camera);
+    return mis * unweighted;
+}
+
+// BP2D: photon beam x camera point (functs_bp2d.cuh:51-198).
+UPBP_D float3 eval_bp2d(const Beam& lb, const PathState& s, const Bsdf& cb, float isect_dist, float rad2)
+{
+    const DeviceParams& p = c_params;
+    const unsigned plen = lb.path_length + s.path_length;
+    if (plen > p.max_path_length || plen < p.min_path_length) return v3(0.f);
+    const DMedium& m = p.media[lb.med];
+    float3 att = attenuation(m, isect_dist);
+    const float pdf = component(att, m.min_pos_att_idx);
+    if (p.photon_beam_type == kShortBeam) att /= pdf;
+    float rs_for = m.min_pos_att * pdf;
+    float rs_rev = (lb.flags & kOriginInMedium) ? rs_for : pdf;
+    const float ratio = 1.f / m.min_pos_att;
+    if (!is_positive(att)) return v3(0.f);
+    rs_for *= lb.for_pdf;
+    rs_rev *= lb.rev_pdf;
+    VertexWeights wl = lb.sw.w;
+    if (lb.path_length > 1u) {
+        const float f_i = pde_factor(wl.prev_in_medium, wl.prev_specular, wl.for_inv, wl.for_ratio, 1.f / rs_rev,
+                                     wl.rev_ratio, lb.sw.last_sin_theta);
+        wl.d_pde = lb.sw.d_pde_a * f_i + lb.sw.d_pde_b;
+        wl.d_bpt = lb.sw.d_bpt_a * f_i + lb.sw.d_bpt_b;
+    }
+    const float3 cdir = cb.dir_fix();
+    float sin_theta;
+    const float ph = hg_pdf(cdir, -lb.d, m.mean_cosine, &sin_theta);
+    const float3 f = v3(ph);
+    if (is_black_or_negative(f)) return v3(0.f);
+    const float fpdf = ph * cb.cont_prob;
+    const float rpdf = ph * m.cont_prob;
+    if (!(lb.path_length == 1 && lb.infinite)) wl.d_shared *= isect_dist * isect_dist;
+    wl.d_shared /= rs_for;
+    wl.d_bpt /= rs_for;
+    wl.d_pde /= rs_for;
+    wl.for_inv = 1.f / rs_for;
+    wl.rev_inv = 1.f / rs_rev;
+    wl.for_ratio = ratio;
+    wl.rev_ratio = ratio;
+    const float kernel = (1.f - rad2 / p.radius_bp2d_2) / (p.radius_bp2d_2 * kPi * .5f);
+    if (!is_positive(kernel)) return v3(0.f);
+    const float3 unweighted = lb.thr * att * m.scattering * f * kernel;
+    if (is_black_or_negative(unweighted)) return v3(0.f);
+    const VertexWeights& wc = s.sw.w;
+    const float ff = p.photon_beam_type == kLongBeam ? wl.for_inv : wl.for_ratio;
+    const float rf = p.camera_beam_type == kLongBeam ? wc.for_inv : wc.for_ratio;
+    const float val = 1.f / (p.mis_factor_bp2d * ff);
+    const float bs = !wl.prev_specular;
+    const float w_light = val * (wl.d_shared * bs * p.subpath_count_bpt + fpdf * wl.d_pde / wl.rev_inv);
+    const float w_local = 1.f + val * (p.mis_factor_bb1d * sin_theta * ff * rf + p.mis_factor_pb2d * rf + p.mis_factor_pp3d);
+    const float bt = !wc.prev_specular;
+    const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
+    const float mis = 1.f / (w_light + w_local + w_camera);
+    return mis * unweighted;
+}
+
+UPBP_D float3 query_pb2d(const QuerySeg& q, const StateWeights& cw)
+{
+    const DeviceParams& p = c_params;
+    float3 acc = v3(0.f);
+    const float3 inv = safe_inv(q.d);
+    const float pad = p.radius_pb2d * 1.0001f + 1e-7f;
+    const bool ok = bvh_walk(
+        p.med_map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, q.o, inv, q.dmin, q.dmax); },
+        [&](int i) {
+            const float4 pp = __ldg(&p.med_map.pos[i]);
+            float dist, rad2;
+            if (pred_ray_disc(q.o, q.d, q.dmin, q.dmax, xyz(pp), p.radius_pb2d_2, dist, rad2)) {
+                LightVertex lv;
+                load_vertex(p.vertices + fbits(pp.w), lv);
+                acc += eval_pb2d(q, cw, lv, dist, rad2);
+            }
+            return true;
+        });
+    if (!ok) flag_status(kErrTraversalStack);
+    return acc;
+}
+
+UPBP_D float3 query_bb1d(const QuerySeg& q, const StateWeights& cw)
+{
+    const DeviceParams& p = c_params;
+    float3 acc = v3(0.f);
+    const float3 inv = safe_inv(q.d);
+    const float pad = p.rad_beam * 1.0001f + 1e-7f;
+    const bool need_mask = p.do_bp2d != 0;
+    const bool ok = bvh_walk(
+        p.beam_map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, q.o, inv, q.dmin, q.dmax); },
+        [&](int i) {
+            const float4 s0 = __ldg(&p.beam_map.seg[2 * i]), s1 = __ldg(&p.beam_map.seg[2 * i + 1]);
+            const unsigned bits = fbits(s1.w);
+            if (need_mask && !(bits >> 31)) return true;
+            float bb, st, t1, t2;
+            if (pred_beam_beam(q.o, q.d, q.dmin, q.dmax, xyz(s0), xyz(s1), s0.w, p.radius_bb1d_2, bb, st, t1, t2)) {
+                Beam lb;
+                load_beam(p.beams + (bits & 0x7fffffffu), lb);
+                if (lb.med == q.med) acc += eval_bb1d(q, cw, lb, bb, st, t1, t2);
+            }
+            return true;
+        });
+    if (!ok) flag_status(kErrTraversalStack);
+    return acc;
+}
+
+UPBP_D float3 query_bp2d(float3 x, const PathState& s, const Bsdf& cb)
+{
+    const DeviceParams& p = c_params;
+    float3 acc = v3(0.f);
+    const float pad = p.rad_beam * 1.0001f + 1e-7f;
+    const bool ok = bvh_walk(
+        p.beam_map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
+        [&](int i) {
+            const float4 s0 = __ldg(&p.beam_map.seg[2 * i]), s1 = __ldg(&p.beam_map.seg[2 * i + 1]);
+            float dist, rad2;
+            if (pred_ray_disc(xyz(s0), xyz(s1), 0.f, s0.w, x, p.radius_bp2d_2, dist, rad2)) {
+                Beam lb;
+                load_beam(p.beams + (fbits(s1.w) & 0x7fffffffu), lb);
+                acc += eval_bp2d(lb, s, cb, dist, rad2);
+            }
+            return true;
+        });
+    if (!ok) flag_status(kErrTraversalStack);
+    return acc;
+}
+
+// Accumulates PB2D or BB1D along the query segments of one camera ray
+// (eval_*_segments, both the VolSegment and the lite-segment variants).
+template <bool kBb1d>
+UPBP_D float3 eval_query_segments(float3 ro, float3 rd, const VolSeg* segs, int nseg, const LiteSeg* lsegs, int nlseg,
+                                  bool use_lite, unsigned sflags, unsigned cam_path_length, const StateWeights& cw)
+{
+    const DeviceParams& p = c_params;
+    float3 result = v3(0.f), att = v3(1.f);
+    float fpdf = 1.f, rpdf = 1.f;
+    const int n = use_lite ? nlseg : nseg;
+    for (int i = 0; i < n; i++) {
+        const float dmin = use_lite ? lsegs[i].dmin : segs[i].dmin;
+        const float dmax = use_lite ? lsegs[i].dmax : segs[i].dmax;
+        const int med = use_lite ? lsegs[i].med : segs[i].med;
+        const DMedium& m = p.media[med];
+        float3 seg_result = v3(0.f);
+        if (m.has_scattering) {
+            QuerySeg q;
+            q.o = ro;
+            q.d = rd;
+            q.dmin = dmin;
+            q.dmax = dmax;
+            q.med = med;
+            q.for_pdf = fpdf;
+            q.rev_pdf = rpdf;
+            q.flags = kEndInMedium | (i == 0 ? sflags : 0u);
+            q.cam_path_length = cam_path_length;
+            seg_result = kBb1d ? query_bb1d(q, cw) : query_pb2d(q, cw);
+        }
+        result += att * seg_result;
+        if (use_lite) {
+            att *= attenuation(m, dmax - dmin);
+            if (!is_positive(att)) return result;
+            float sr;
+            const float sf = distance_pdf(m, dmin, dmax, i == 0 ? sflags : 0u, sr);
+            fpdf *= sf;
+            rpdf *= sr;
+        } else {
+            if (p.camera_beam_type == kShortBeam)
+                att *= segs[i].att / segs[i].pdf_for;
+            else
+                att *= segs[i].att;
+            if (!is_positive(att)) return result;
+            fpdf *= segs[i].pdf_for;
+            rpdf *= segs[i].pdf_rev;
+        }
+    }
+    return result;
+}
+
+__global__ void __launch_bounds__(128) camera_pass_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= p.screen_pixel_count) return;
+
+    VolSeg segs[kMaxVolSegments];
+    LiteSeg lsegs[kMaxVolSegments];
+    Rng rng;
+    rng.init(p.iteration + p.iteration_offset, pixel, 1u);
+    PathState s;
+    float2 screen;
+    unsigned ret = generate_camera_sample(screen, pixel, s, rng);
+    float3 color = v3(0.f);
+    bool origin_in_medium = false;
+    bool only_spec_surf = (p.estimator_techniques & (kPrevious | kCompatible)) != 0;
+
+    for (; ret == 0; s.path_length++) {
+        const float3 ro = s.origin, rd = s.dir;
+        Isect isect;
+        isect.dist = kInfinity;
+        isect.mat = isect.med = isect.light = -1;
+        isect.normal = v3(0.f);
+        isect.enter = false;
+        int nseg = 0, nlseg = 0;
+        bool hit;
+        ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
+                              segs, nseg, lsegs, nlseg, rng);
+        if (ret) break;
+        const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
+        const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
+        if (p.build_pb2d && p.n_medium > 0) {
+            const float3 c = eval_query_segments<false>(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags,
+                                                        s.path_length, s.sw);
+            color += s.throughput * p.pb2d_normalization * c;
+        }
+        if (p.build_bb1d && p.n_beams > 0) {
+            const float3 c = eval_query_segments<true>(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags,
+                                                       s.path_length, s.sw);
+            color += s.throughput * p.bb1d_normalization * c;
+        }
+        if (!hit) {
+            if (s.path_length < p.min_path_length) break;
+            if (p.background_light < 0) break;
+            if (p.media[p.global_medium].has_attenuation) break;
+        }
+        float rs_for = 1.f, rs_rev = 1.f;
+        if (nseg > 0) {
+            rs_for = seg_for_pdf(segs, nseg);
+            rs_rev = seg_rev_pdf(segs, nseg);
+            s.throughput *= seg_attenuation(segs, nseg) / rs_for;
+        }
+        if (is_black_or_negative(s.throughput)) break;
+        VertexWeights& w = s.sw.w;
+        if (s.path_length > 1u) {
+            const float f_i = pde_factor(w.prev_in_medium, w.prev_specular, 1.f / rs_rev, w.rev_ratio, w.for_inv,
+                                         w.for_ratio, s.sw.last_sin_theta);
+            w.d_bpt = s.sw.d_bpt_a * f_i + s.sw.d_bpt_b;
+            w.d_pde = s.sw.d_pde_a * f_i + s.sw.d_pde_b;
+        }
+        w.d_shared /= rs_for;
+        w.d_bpt /= rs_for;
+        w.d_pde /= rs_for;
+        if (!hit) {
+            color += s.throughput * light_hit_radiance(p.lights[p.background_light], s, rs_rev);
+            break;
+        }
+        Bsdf bsdf;
+        if (isect.on_surface())
+            bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, false, relative_ior(isect, s.stack));
+        else
+            bsdf_setup_medium(bsdf, rd, isect.med, false);
+        if (!bsdf.valid()) break;
+        float ratio = 0.f;
+        if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
+        const float3 hitpoint = ro + rd * isect.dist;
+        origin_in_medium = isect.in_medium();
+        {
+            const float d = bsdf.d_factor();
+            w.d_shared *= isect.dist * isect.dist;
+            w.d_shared /= d;
+            w.d_bpt /= d;
+            w.d_pde /= d;
+            w.for_inv = 1.f / rs_for;
+            w.rev_inv = 1.f / rs_rev;
+            w.for_ratio = ratio;
+            w.rev_ratio = ratio;
+        }
+        if (isect.light >= 0) {
+            if (s.path_length < p.min_path_length) break;
+            color += s.throughput * light_hit_radiance(p.lights[isect.light], s, rs_rev);
+            break;
+        }
+        if (s.path_length >= p.max_path_length) break;
+        if (p.do_bpt && !bsdf.delta() && s.path_length + 1 >= p.min_path_length && p.light_count > 0 &&
+            (bsdf.in_medium() || !only_spec_surf)) {
+            float3 c;
+            ret = direct_illumination(c, s, hitpoint, bsdf, rng, segs);
+            if (ret) break;
+            color += s.throughput * c;
+        }
+        if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || !only_spec_surf)) {
+            bool behind = false;
+            if (bsdf.in_medium() && s.stack.size > 0) {
+                const int mid = s.stack.top().mat;
+                if (mid >= 0 && p.materials[mid].real) behind = true;
+            }
+            const int lp = int(rng.uniform() * p.light_subpath_count);
+            const unsigned nv = p.path_vertex_count[lp];
+            const LightVertexRec* base = p.vertices + (size_t)lp * p.slots_per_path;
+            bool err = false;
+            for (unsigned k = 0; k < nv; k++) {
+                LightVertex lv;
+                load_vertex(base + k, lv);
+                const unsigned plen = lv.path_length + 1 + s.path_length;
+                if (plen > p.max_path_length) break;
+                const bool too_short = plen < p.min_path_length;
+                const bool diff_media = lv.bsdf.in_medium() && bsdf.in_medium() && lv.bsdf.id != bsdf.id &&
+                                        (lv.behind_surf || behind);
+                if (!(too_short || diff_media)) {
+                    float3 c;
+                    ret = connect_vertices(c, lv, bsdf, hitpoint, s, rng, segs);
+                    if (ret) {
+                        err = true;
+                        break;
+                    }
+                    color += s.throughput * lv.thr * c;
+                }
+            }
+            if (err) break;
+        }
+        if (p.build_surf && p.n_surface > 0 && bsdf.on_surface() && !bsdf.delta() && !only_spec_surf)
+            color += s.throughput * p.surf_normalization *
+                     query_points(p.surf_map, hitpoint, p.radius_surf, p.radius_surf_2, s, bsdf, false);
+        if (p.build_pp3d && p.n_medium > 0 && bsdf.in_medium() && !bsdf.delta())
+            color += s.throughput * p.pp3d_normalization *
+                     query_points(p.med_map, hitpoint, p.radius_pp3d, p.radius_pp3d_2, s, bsdf, true);
+        if (p.build_bp2d && p.n_beams > 0 && bsdf.in_medium())
+            color += s.throughput * p.bp2d_normalization * query_bp2d(hitpoint, s, bsdf);
+        bool cont;
+        ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
+        if (ret || !cont) break;
+        if (bsdf.on_surface()) {
+            if (!s.sw.w.prev_specular && (only_spec_surf || (p.estimator_techniques & kSpecularOnly))) break;
+        } else {
+            if (p.estimator_techniques & kSpecularOnly) break;
+            if (only_spec_surf) {
+                if (p.estimator_techniques & kCompatible)
+                    only_spec_surf = false;
+                else
+                    break;
+            }
+        }
+    }
+    if (ret) flag_status(ret);
+    if (screen.x < 0.f || screen.x >= (float)p.res_x || screen.y < 0.f || screen.y >= (float)p.res_y) return;
+    const unsigned px = (unsigned)int(screen.x) + (unsigned)int(screen.y) * p.res_x;
+    p.framebuffer[3 * px + 0] += color.x;
+    p.framebuffer[3 * px + 1] += color.y;
+    p.framebuffer[3 * px + 2] += color.z;
+}
+
+}  // namespace upbp

@@ -1,0 +1,590 @@
+// C ABI of libupbp_b200.so: context creation (scene upload, scene BVHs,
+// record buffers) and the per-iteration schedule (radius reduction, light
+// pass, photon-map builds, camera pass, accumulation).  Mirrors
+// Renderer::init (gpuupbp/renderer/renderer_init.cpp:675-929) and
+// Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host/upbp_scene.h"
+#include "upbp_build.cuh"
+#include "upbp_camera_pass.cuh"
+#include "upbp_light_pass.cuh"
+
+using namespace upbp;
+
+namespace {
+
+#define UPBP_CK(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            upbp_host::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));              \
+            return UPBP_ERR_CUDA;                                                                  \
+        }                                                                                          \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+}
+
+template <class T>
+cudaError_t dupload(T** p, const T* h, size_t n, cudaStream_t st)
+{
+    cudaError_t e = dalloc(p, n);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+__global__ void k_accumulate(const float* fb, double* acc, unsigned n)
+{
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) acc[i] += (double)fb[i];
+}
+
+struct Geometry {
+    BvhNode* nodes = nullptr;
+    float4* tri = nullptr;
+    float4* normals = nullptr;
+    int2* record = nullptr;
+    unsigned count = 0;
+};
+
+}  // namespace
+
+struct upbp_ctx {
+    upbp_config cfg{};
+    DeviceParams P{};
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    DMaterial* d_mat = nullptr;
+    DMedium* d_med = nullptr;
+    DLight* d_lights = nullptr;
+    Geometry real, imag;
+    LightVertexRec* d_vertices = nullptr;
+    unsigned* d_path_count = nullptr;
+    unsigned* d_counters = nullptr;
+    unsigned* d_idx_s = nullptr;
+    unsigned* d_idx_m = nullptr;
+    BeamRec* d_beams = nullptr;
+    float* d_fb = nullptr;
+    double* d_acc = nullptr;
+    unsigned* d_status = nullptr;
+    BvhNode *d_surf_nodes = nullptr, *d_med_nodes = nullptr, *d_beam_nodes = nullptr;
+    float4 *d_surf_pos = nullptr, *d_med_pos = nullptr, *d_beam_seg = nullptr;
+    BuildScratch sc;
+    float r0[5] = {0, 0, 0, 0, 0};  // bb1d bp2d pb2d pp3d surf
+    float bb1d_used = 0.f;
+    unsigned vertex_capacity = 0, beam_capacity = 0;
+    unsigned h_counters[4] = {0, 0, 0, 0};
+    unsigned iterations = 0;
+    bool timed = false;
+    uint64_t triangles = 0;
+};
+
+namespace {
+
+void init_medium(DMedium& m, const upbp_medium& in)
+{
+    m.absorption = make_float3(fabsf(in.absorption[0]), fabsf(in.absorption[1]), fabsf(in.absorption[2]));
+    m.emission = make_float3(fabsf(in.emission[0]), fabsf(in.emission[1]), fabsf(in.emission[2]));
+    m.scattering = make_float3(fabsf(in.scattering[0]), fabsf(in.scattering[1]), fabsf(in.scattering[2]));
+    m.attenuation = m.absorption + m.scattering;
+    m.cont_prob = in.continuation_prob;
+    m.mean_cosine = in.mean_cosine;
+    m.min_pos_att = m.attenuation.x;
+    m.min_pos_att_idx = 0;
+    if (m.attenuation.y > 0.f && (m.min_pos_att == 0.f || m.attenuation.y < m.min_pos_att)) {
+        m.min_pos_att = m.attenuation.y;
+        m.min_pos_att_idx = 1;
+    }
+    if (m.attenuation.z > 0.f && (m.min_pos_att == 0.f || m.attenuation.z < m.min_pos_att)) {
+        m.min_pos_att = m.attenuation.z;
+        m.min_pos_att_idx = 2;
+    }
+    m.has_scattering = (m.scattering.x > 0.f || m.scattering.y > 0.f || m.scattering.z > 0.f) ? 1 : 0;
+    if (m.attenuation.x > 0.f || m.attenuation.y > 0.f || m.attenuation.z > 0.f) {
+        m.has_attenuation = 1;
+        m.max_beam_length = -logf(1e-9f) / max_component(m.attenuation);
+    } else {
+        m.has_attenuation = 0;
+        m.max_beam_length = kInfinity;
+    }
+}
+
+void init_light(DLight& l, const upbp_light& in)
+{
+    std::memset(&l, 0, sizeof(l));
+    l.type = in.type;
+    l.mat_id = in.mat_id;
+    l.med_id = in.med_id;
+    const float3 I = make_float3(in.intensity[0], in.intensity[1], in.intensity[2]);
+    if (in.type == UPBP_LIGHT_AREA) {
+        const float3 p0 = make_float3(in.p0[0], in.p0[1], in.p0[2]);
+        const float3 p1 = make_float3(in.p1[0], in.p1[1], in.p1[2]);
+        const float3 p2 = make_float3(in.p2[0], in.p2[1], in.p2[2]);
+        l.p0 = p0;
+        l.e1 = p1 - p0;
+        l.e2 = p2 - p0;
+        const float3 n = cross(l.e1, l.e2);
+        l.inv_area = 2.f / length(n);
+        l.frame.set_from_z(n);
+        l.intensity = I;
+    } else if (in.type == UPBP_LIGHT_BACKGROUND) {
+        l.intensity = I * in.scale;
+    } else if (in.type == UPBP_LIGHT_DIRECTIONAL) {
+        l.frame.set_from_z(make_float3(in.position[0], in.position[1], in.position[2]));
+        l.intensity = I;
+    } else {
+        l.position = make_float3(in.position[0], in.position[1], in.position[2]);
+        l.intensity = I;
+    }
+}
+
+int upload_geometry(upbp_ctx* c, const upbp_scene_desc* s, bool real, Geometry& g)
+{
+    std::vector<float4> tri, nrm;
+    std::vector<int2> rec;
+    for (uint32_t i = 0; i < s->triangle_count; i++) {
+        const int m = s->tri_material[i];
+        if ((s->materials[m].real != 0) != real) continue;
+        const float* v = s->verts + 9 * (size_t)i;
+        const float* n = s->normals + 12 * (size_t)i;
+        tri.push_back(make_float4(v[0], v[1], v[2], 0.f));
+        tri.push_back(make_float4(v[3] - v[0], v[4] - v[1], v[5] - v[2], 0.f));
+        tri.push_back(make_float4(v[6] - v[0], v[7] - v[1], v[8] - v[2], 0.f));
+        for (int k = 0; k < 4; k++) nrm.push_back(make_float4(n[3 * k], n[3 * k + 1], n[3 * k + 2], 0.f));
+        rec.push_back(make_int2(m, s->tri_light[i]));
+    }
+    g.count = (unsigned)rec.size();
+    float4* unsorted = nullptr;
+    UPBP_CK(dupload(&unsorted, tri.data(), tri.size(), c->st));
+    UPBP_CK(dupload(&g.normals, nrm.data(), nrm.size(), c->st));
+    UPBP_CK(dupload(&g.record, rec.data(), rec.size(), c->st));
+    UPBP_CK(dalloc(&g.nodes, g.count > 1 ? g.count - 1 : 1));
+    UPBP_CK(dalloc(&g.tri, 3 * (size_t)std::max(1u, g.count)));
+    if (g.count > 0) {
+        BoxSource src{};
+        src.kind = 0;
+        src.tri = unsorted;
+        const unsigned* order = nullptr;
+        UPBP_CK(build_lbvh(src, g.count, g.nodes, c->sc, c->st, &order));
+        k_gather_tris<<<(g.count + 255) / 256, 256, 0, c->st>>>(unsorted, order, g.count, g.tri);
+        UPBP_CK(cudaGetLastError());
+    }
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    cudaFree(unsorted);
+    return UPBP_OK;
+}
+
+int alloc_scratch(BuildScratch& sc, unsigned cap)
+{
+    cap = std::max(cap, 2u);
+    sc.capacity = cap;
+    UPBP_CK(dalloc(&sc.keys, cap));
+    UPBP_CK(dalloc(&sc.keys_alt, cap));
+    UPBP_CK(dalloc(&sc.vals, cap));
+    UPBP_CK(dalloc(&sc.vals_alt, cap));
+    UPBP_CK(dalloc(&sc.parent_internal, cap));
+    UPBP_CK(dalloc(&sc.parent_leaf, cap));
+    UPBP_CK(dalloc(&sc.flags, cap));
+    UPBP_CK(dalloc(&sc.ord6, 6));
+    cub::DoubleBuffer<unsigned> kb(sc.keys, sc.keys_alt), vb(sc.vals, sc.vals_alt);
+    size_t bytes = 0;
+    UPBP_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, (int)cap, 0, 30));
+    sc.temp_bytes = bytes;
+    UPBP_CK(cudaMalloc(&sc.temp, bytes));
+    return UPBP_OK;
+}
+
+void free_scratch(BuildScratch& sc)
+{
+    cudaFree(sc.keys);
+    cudaFree(sc.keys_alt);
+    cudaFree(sc.vals);
+    cudaFree(sc.vals_alt);
+    cudaFree(sc.parent_internal);
+    cudaFree(sc.parent_leaf);
+    cudaFree(sc.flags);
+    cudaFree(sc.ord6);
+    cudaFree(sc.temp);
+    sc = BuildScratch{};
+}
+
+float relative_radius(float r, float scene_radius) { return r < 0.f ? -r * scene_radius : r; }
+
+}  // namespace
+
+extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upbp_ctx** out)
+{
+    if (!s || !cfg || !out) return UPBP_ERR_ARGS;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        upbp_host::set_error("no CUDA device");
+        return UPBP_ERR_NO_DEVICE;
+    }
+    if (s->material_count == 0 || s->medium_count == 0 || s->global_medium < 0 ||
+        (uint32_t)s->global_medium >= s->medium_count) {
+        upbp_host::set_error("scene has no materials or no valid global medium");
+        return UPBP_ERR_SCENE;
+    }
+    for (uint32_t i = 0; i < s->triangle_count; i++)
+        if (s->tri_material[i] < 0 || (uint32_t)s->tri_material[i] >= s->material_count) {
+            upbp_host::set_error("triangle material index out of range");
+            return UPBP_ERR_SCENE;
+        }
+    upbp_ctx* c = new upbp_ctx();
+    c->cfg = *cfg;
+    DeviceParams& P = c->P;
+    UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    for (auto& e : c->ev) UPBP_CK(cudaEventCreate(&e));
+
+    // scene records
+    std::vector<DMaterial> mats(s->material_count);
+    for (uint32_t i = 0; i < s->material_count; i++) {
+        const upbp_material& m = s->materials[i];
+        mats[i].diffuse = make_float3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+        mats[i].phong = make_float3(m.phong[0], m.phong[1], m.phong[2]);
+        mats[i].phong_exponent = m.phong_exponent;
+        mats[i].mirror = make_float3(m.mirror[0], m.mirror[1], m.mirror[2]);
+        mats[i].ior = m.ior;
+        mats[i].priority = m.priority;
+        mats[i].real = m.real;
+        mats[i].medium = m.medium;
+    }
+    std::vector<DMedium> meds(s->medium_count);
+    for (uint32_t i = 0; i < s->medium_count; i++) init_medium(meds[i], s->media[i]);
+    std::vector<DLight> lights(std::max(1u, s->light_count));
+    for (uint32_t i = 0; i < s->light_count; i++) init_light(lights[i], s->lights[i]);
+    UPBP_CK(dupload(&c->d_mat, mats.data(), mats.size(), c->st));
+    UPBP_CK(dupload(&c->d_med, meds.data(), meds.size(), c->st));
+    UPBP_CK(dupload(&c->d_lights, lights.data(), lights.size(), c->st));
+    P.materials = c->d_mat;
+    P.material_count = (int)s->material_count;
+    P.media = c->d_med;
+    P.medium_count = (int)s->medium_count;
+    P.global_medium = s->global_medium;
+    P.lights = c->d_lights;
+    P.light_count = (int)s->light_count;
+    P.background_light = s->background_light;
+
+    // camera and scene sphere (scene_loader.hpp:65-71)
+    const upbp_host::CameraMatrices cm = upbp_host::camera_setup(s->camera, (float)cfg->res_x, (float)cfg->res_y);
+    DCamera& cam = P.camera;
+    cam.origin = make_float3(cm.origin[0], cm.origin[1], cm.origin[2]);
+    cam.direction = make_float3(cm.direction[0], cm.direction[1], cm.direction[2]);
+    cam.res_x = (float)cfg->res_x;
+    cam.res_y = (float)cfg->res_y;
+    std::memcpy(cam.raster_to_world, cm.raster_to_world, sizeof(cam.raster_to_world));
+    std::memcpy(cam.world_to_raster, cm.world_to_raster, sizeof(cam.world_to_raster));
+    cam.image_plane_dist = cm.image_plane_dist;
+    cam.mat_id = s->camera.mat_id;
+    cam.med_id = s->camera.med_id;
+    {
+        const float3 lo = make_float3(s->bbox_min[0], s->bbox_min[1], s->bbox_min[2]);
+        const float3 hi = make_float3(s->bbox_max[0], s->bbox_max[1], s->bbox_max[2]);
+        float r2 = dot(hi - lo, hi - lo);
+        if (r2 == 0.f || r2 > kInfinity) r2 = 1.f;
+        P.scene_center = (hi + lo) * .5f;
+        P.scene_radius = std::sqrt(r2) * .5f;
+        P.inv_radius_sqr = 1.f / (P.scene_radius * P.scene_radius);
+    }
+
+    // configuration (renderer_init.cpp:681-925)
+    const uint32_t flags = cfg->algorithm_flags;
+    P.trace_light_paths = flags != 0;
+    P.trace_camera_paths = flags != 0;
+    P.do_bpt = (flags & kBpt) != 0;
+    P.do_bb1d = (flags & kBb1d) != 0;
+    P.do_bp2d = (flags & kBp2d) != 0;
+    P.do_pb2d = (flags & kPb2d) != 0;
+    P.do_pp3d = (flags & kPp3d) != 0;
+    P.do_surf = (flags & kSurf) != 0;
+    if (flags & kSpecularOnly) {
+        P.trace_light_paths = 0;
+        P.trace_camera_paths = 1;
+        P.do_bpt = P.do_bb1d = P.do_bp2d = P.do_pb2d = P.do_pp3d = P.do_surf = 0;
+    }
+    P.connect_to_camera_from_surf = (flags & (kPrevious | kCompatible)) == 0;
+    P.screen_pixel_count = cfg->res_x * cfg->res_y;
+    const unsigned L = (unsigned)cfg->path_count_per_iter;
+    P.light_subpath_count = L;
+    c->bb1d_used = cfg->bb1d_used_light_subpath_count;
+    if (c->bb1d_used < 0.f) c->bb1d_used = std::floor(-c->bb1d_used * (float)L);
+    c->r0[0] = relative_radius(cfg->bb1d_radius_initial, P.scene_radius);
+    c->r0[1] = relative_radius(cfg->bp2d_radius_initial, P.scene_radius);
+    c->r0[2] = relative_radius(cfg->pb2d_radius_initial, P.scene_radius);
+    c->r0[3] = relative_radius(cfg->pp3d_radius_initial, P.scene_radius);
+    c->r0[4] = relative_radius(cfg->surf_radius_initial, P.scene_radius);
+
+    const unsigned slots = cfg->max_path_length > 1 ? cfg->max_path_length - 1 : 1;
+    const unsigned beams_per_path = cfg->max_path_length > 2 ? cfg->max_path_length - 2 : 0;
+    unsigned beam_paths = 0;
+    if (P.do_bb1d) beam_paths = std::max(beam_paths, (unsigned)c->bb1d_used);
+    if (P.do_bp2d) beam_paths = std::max(beam_paths, L);
+    c->vertex_capacity = L * slots;
+    c->beam_capacity = beam_paths * beams_per_path;
+    P.slots_per_path = slots;
+    P.beam_capacity = c->beam_capacity;
+
+    const bool merging = cfg->max_path_length > 1;
+    P.build_bb1d = P.trace_light_paths && merging && P.do_bb1d;
+    P.build_bp2d = P.trace_light_paths && merging && P.do_bp2d;
+    P.build_pb2d = P.trace_light_paths && merging && P.do_pb2d;
+    P.build_pp3d = P.trace_light_paths && merging && P.do_pp3d;
+    P.build_surf = P.trace_light_paths && merging && P.do_surf;
+    P.iteration_offset = cfg->iteration_offset;
+    P.min_path_length = cfg->min_path_length;
+    P.max_path_length = cfg->max_path_length;
+    P.photon_beam_type = cfg->photon_beam_type;
+    P.camera_beam_type = cfg->query_beam_type;
+    P.subpath_count_bpt = float(P.do_bpt);
+    P.subpath_count_bb1d = float(P.do_bb1d) * c->bb1d_used;
+    P.subpath_count_bp2d = float(P.do_bp2d) * L;
+    P.subpath_count_pb2d = float(P.do_pb2d) * L;
+    P.subpath_count_pp3d = float(P.do_pp3d) * L;
+    P.subpath_count_surf = float(P.do_surf) * L;
+    P.ignore_fully_spec_paths = cfg->ignore_fully_spec_paths;
+    P.estimator_techniques = flags;
+    P.bb1d_used_light_subpath_count = (unsigned)c->bb1d_used;
+    P.use_shading_normal = cfg->use_shading_normal;
+    P.res_x = cfg->res_x;
+    P.res_y = cfg->res_y;
+
+    // buffers
+    unsigned n_real = 0, n_imag = 0;
+    for (uint32_t i = 0; i < s->triangle_count; i++) (s->materials[s->tri_material[i]].real ? n_real : n_imag)++;
+    c->triangles = s->triangle_count;
+    if (alloc_scratch(c->sc, std::max({n_real, n_imag, c->vertex_capacity, c->beam_capacity})) != UPBP_OK) {
+        upbp_destroy(c);
+        return UPBP_ERR_CUDA;
+    }
+    if (upload_geometry(c, s, true, c->real) != UPBP_OK || upload_geometry(c, s, false, c->imag) != UPBP_OK) {
+        upbp_destroy(c);
+        return UPBP_ERR_CUDA;
+    }
+    P.real = TriView{BvhView{c->real.nodes, c->real.count}, c->real.tri, c->real.normals, c->real.record};
+    P.imag = TriView{BvhView{c->imag.nodes, c->imag.count}, c->imag.tri, c->imag.normals, c->imag.record};
+    const size_t npx = (size_t)P.screen_pixel_count * 3;
+    UPBP_CK(dalloc(&c->d_vertices, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_path_count, std::max(1u, L)));
+    UPBP_CK(dalloc(&c->d_counters, 4));
+    UPBP_CK(dalloc(&c->d_idx_s, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_idx_m, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_beams, c->beam_capacity));
+    UPBP_CK(dalloc(&c->d_fb, npx));
+    UPBP_CK(dalloc(&c->d_acc, npx));
+    UPBP_CK(dalloc(&c->d_status, 1));
+    UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_beam_nodes, c->beam_capacity));
+    UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_med_pos, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_beam_seg, 2 * (size_t)c->beam_capacity));
+    UPBP_CK(cudaMemsetAsync(c->d_acc, 0, npx * sizeof(double), c->st));
+    UPBP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->st));
+    UPBP_CK(cudaMemsetAsync(c->d_path_count, 0, sizeof(unsigned) * std::max(1u, L), c->st));
+    P.vertices = c->d_vertices;
+    P.path_vertex_count = c->d_path_count;
+    P.counters = c->d_counters;
+    P.idx_surface = c->d_idx_s;
+    P.idx_medium = c->d_idx_m;
+    P.beams = c->d_beams;
+    P.framebuffer = c->d_fb;
+    P.status = c->d_status;
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    *out = c;
+    return UPBP_OK;
+}
+
+extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
+{
+    if (!c || iteration < 0) return UPBP_ERR_ARGS;
+    DeviceParams& P = c->P;
+    const upbp_config& cfg = c->cfg;
+    const unsigned L = P.light_subpath_count;
+    const size_t npx = (size_t)P.screen_pixel_count * 3;
+    UPBP_CK(cudaEventRecord(c->ev[0], c->st));
+    UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
+    unsigned found[4] = {0, 0, 0, 0};
+    if (P.trace_light_paths) {
+        // radius schedule and MIS factors (renderer.cpp:57-119)
+        const float eff = 1.f + (float)iteration;
+        float r_bb1d = c->r0[0] * powf(1.f + (float)iteration * c->bb1d_used / (float)L, cfg.bb1d_radius_alpha - 1.f);
+        r_bb1d = fmaxf(r_bb1d, 1e-7f);
+        float r_bp2d = fmaxf(c->r0[1] * powf(eff, (cfg.bp2d_radius_alpha - 1.f) * .5f), 1e-7f);
+        float r_pb2d = fmaxf(c->r0[2] * powf(eff, (cfg.pb2d_radius_alpha - 1.f) * .5f), 1e-7f);
+        float r_pp3d = fmaxf(c->r0[3] * powf(eff, (cfg.pp3d_radius_alpha - 1.f) * (1.f / 3.f)), 1e-7f);
+        float r_surf = fmaxf(c->r0[4] * powf(eff, (cfg.surf_radius_alpha - 1.f) * .5f), 1e-7f);
+        P.mis_factor_bb1d = .5f * r_bb1d * P.subpath_count_bb1d;
+        P.mis_factor_bp2d = (kPi * (r_bp2d * r_bp2d)) * P.subpath_count_bp2d;
+        P.mis_factor_pb2d = (kPi * (r_pb2d * r_pb2d)) * P.subpath_count_pb2d;
+        P.mis_factor_pp3d = (4.f / 3.f) * (kPi * (r_pp3d * r_pp3d * r_pp3d)) * P.subpath_count_pp3d;
+        P.mis_factor_surf = (kPi * (r_surf * r_surf)) * P.subpath_count_surf;
+        P.bb1d_normalization = 1.f / c->bb1d_used;
+        P.bp2d_normalization = 1.f / (float)L;
+        P.pb2d_normalization = 1.f / (float)L;
+        P.pp3d_normalization = 1.f / P.mis_factor_pp3d;
+        P.surf_normalization = 1.f / P.mis_factor_surf;
+        P.radius_bb1d = r_bb1d;
+        P.radius_bp2d = r_bp2d;
+        P.radius_pb2d = r_pb2d;
+        P.radius_pp3d = r_pp3d;
+        P.radius_surf = r_surf;
+        P.rad_point_med = 0.f;
+        if (P.do_pp3d) P.rad_point_med = std::max(P.rad_point_med, r_pp3d);
+        if (P.do_pb2d) P.rad_point_med = std::max(P.rad_point_med, r_pb2d);
+        P.rad_beam = 0.f;
+        if (P.do_bb1d) P.rad_beam = std::max(P.rad_beam, r_bb1d);
+        if (P.do_bp2d) P.rad_beam = std::max(P.rad_beam, r_bp2d);
+        P.radius_bb1d_2 = r_bb1d * r_bb1d;
+        P.radius_bp2d_2 = r_bp2d * r_bp2d;
+        P.radius_pb2d_2 = r_pb2d * r_pb2d;
+        P.radius_pp3d_2 = r_pp3d * r_pp3d;
+        P.radius_surf_2 = r_surf * r_surf;
+        P.iteration = (unsigned)iteration;
+        UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned), c->st));
+        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+        if (L > 0) light_pass_kernel<<<(L + 127) / 128, 128, 0, c->st>>>();
+        UPBP_CK(cudaGetLastError());
+        UPBP_CK(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        std::memcpy(found, c->h_counters, sizeof(found));
+        if (found[3] > c->beam_capacity) {
+            // the reference prints the same warning and continues (renderer.cpp:188-195)
+            std::fprintf(stderr, "error: device finds more beams than memory allocated\n");
+        }
+    } else {
+        P.iteration = (unsigned)iteration;
+    }
+    UPBP_CK(cudaEventRecord(c->ev[1], c->st));
+
+    // photon maps (renderer.cpp:206-307 builds OptiX structures here)
+    const unsigned ns = std::min(found[1], c->vertex_capacity);
+    const unsigned nm = std::min(found[2], c->vertex_capacity);
+    const unsigned nb = std::min(found[3], c->beam_capacity);
+    P.surf_map = PointMap{BvhView{c->d_surf_nodes, 0}, c->d_surf_pos};
+    P.med_map = PointMap{BvhView{c->d_med_nodes, 0}, c->d_med_pos};
+    P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg};
+    if (P.build_surf && ns > 0) {
+        BoxSource src{};
+        src.kind = 1;
+        src.slots = c->d_idx_s;
+        src.vertices = c->d_vertices;
+        const unsigned* order = nullptr;
+        UPBP_CK(build_lbvh(src, ns, c->d_surf_nodes, c->sc, c->st, &order));
+        k_gather_points<<<(ns + 255) / 256, 256, 0, c->st>>>(c->d_idx_s, c->d_vertices, order, ns, c->d_surf_pos);
+        P.surf_map.bvh.count = ns;
+    }
+    if ((P.build_pb2d || P.build_pp3d) && nm > 0) {
+        BoxSource src{};
+        src.kind = 1;
+        src.slots = c->d_idx_m;
+        src.vertices = c->d_vertices;
+        const unsigned* order = nullptr;
+        UPBP_CK(build_lbvh(src, nm, c->d_med_nodes, c->sc, c->st, &order));
+        k_gather_points<<<(nm + 255) / 256, 256, 0, c->st>>>(c->d_idx_m, c->d_vertices, order, nm, c->d_med_pos);
+        P.med_map.bvh.count = nm;
+    }
+    if ((P.build_bb1d || P.build_bp2d) && nb > 0) {
+        BoxSource src{};
+        src.kind = 2;
+        src.beams = c->d_beams;
+        const unsigned* order = nullptr;
+        UPBP_CK(build_lbvh(src, nb, c->d_beam_nodes, c->sc, c->st, &order));
+        k_gather_beams<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_beams, order, nb, P.bb1d_used_light_subpath_count,
+                                                            c->d_beam_seg);
+        P.beam_map.bvh.count = nb;
+    }
+    UPBP_CK(cudaGetLastError());
+    P.n_surface = found[1];
+    P.n_medium = found[2];
+    P.n_beams = found[3];
+    UPBP_CK(cudaEventRecord(c->ev[2], c->st));
+
+    if (P.trace_camera_paths) {
+        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+        camera_pass_kernel<<<(P.screen_pixel_count + 127) / 128, 128, 0, c->st>>>();
+        UPBP_CK(cudaGetLastError());
+    }
+    k_accumulate<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_acc, (unsigned)npx);
+    UPBP_CK(cudaGetLastError());
+    UPBP_CK(cudaEventRecord(c->ev[3], c->st));
+    c->iterations++;
+    c->timed = true;
+    return UPBP_OK;
+}
+
+extern "C" int upbp_accumulate_to_host(upbp_ctx* c, float* rgb, double scale)
+{
+    if (!c || !rgb) return UPBP_ERR_ARGS;
+    const size_t n = (size_t)c->P.screen_pixel_count * 3;
+    std::vector<double> tmp(n);
+    UPBP_CK(cudaMemcpyAsync(tmp.data(), c->d_acc, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    for (size_t i = 0; i < n; i++) rgb[i] += (float)(scale * tmp[i]);
+    return UPBP_OK;
+}
+
+extern "C" int upbp_read_iteration(upbp_ctx* c, float* rgb)
+{
+    if (!c || !rgb) return UPBP_ERR_ARGS;
+    const size_t n = (size_t)c->P.screen_pixel_count * 3;
+    UPBP_CK(cudaMemcpyAsync(rgb, c->d_fb, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    return UPBP_OK;
+}
+
+extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
+{
+    if (!c || !o) return UPBP_ERR_ARGS;
+    std::memset(o, 0, sizeof(*o));
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    unsigned status = 0;
+    UPBP_CK(cudaMemcpy(&status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    o->light_vertices = c->h_counters[0];
+    o->surface_vertices = c->h_counters[1];
+    o->medium_vertices = c->h_counters[2];
+    o->light_beams = c->h_counters[3];
+    o->light_paths = c->P.light_subpath_count;
+    o->camera_paths = c->P.screen_pixel_count;
+    o->status = status;
+    o->iterations_done = c->iterations;
+    o->triangle_count = c->triangles;
+    o->scene_radius = c->P.scene_radius;
+    if (c->timed) {
+        float a = 0.f, b = 0.f, d = 0.f;
+        UPBP_CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+        UPBP_CK(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+        UPBP_CK(cudaEventElapsedTime(&d, c->ev[2], c->ev[3]));
+        o->ms_light = a;
+        o->ms_build = b;
+        o->ms_camera = d;
+    }
+    return UPBP_OK;
+}
+
+extern "C" void upbp_destroy(upbp_ctx* c)
+{
+    if (!c) return;
+    if (c->st) cudaStreamSynchronize(c->st);
+    void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
+                    c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
+                    c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
+                    c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    free_scratch(c->sc);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}

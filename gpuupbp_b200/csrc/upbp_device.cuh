@@ -1,0 +1,182 @@
+// Device-side scene records, per-iteration parameters and the record layouts
+// of light vertices and photon beams in HBM.
+#pragma once
+
+#include "upbp_math.cuh"
+
+namespace upbp {
+
+// Estimator bits (same values as the reference's shared/shared_enums.h).
+enum : unsigned {
+    kBpt = 1u << 2, kSurf = 1u << 3, kPp3d = 1u << 4, kPb2d = 1u << 5, kBb1d = 1u << 6, kBp2d = 1u << 7,
+    kPrevious = 1u << 9, kCompatible = 1u << 10, kSpecularOnly = 1u << 12
+};
+enum : int { kShortBeam = 1, kLongBeam = 2 };
+enum : int { kLightArea = 0, kLightBackground = 1, kLightDirectional = 2, kLightPoint = 3 };
+enum : unsigned { kOriginInMedium = 1u << 0, kEndInMedium = 1u << 1 };
+
+// Status bits written to the device status word (upbp.h UPBP_STATUS_*).
+enum : unsigned {
+    kErrBoundaryStack = 1u << 0, kErrIntersectionArray = 1u << 1, kErrVolSegmentArray = 1u << 2,
+    kErrIntersectionStack = 1u << 3, kErrBeamCapacity = 1u << 4, kErrTraversalStack = 1u << 5
+};
+
+struct DMaterial {
+    float3 diffuse;
+    float3 phong;
+    float phong_exponent;
+    float3 mirror;
+    float ior;
+    int priority;
+    int real;
+    int medium;
+};
+
+struct DMedium {
+    float3 absorption, emission, scattering, attenuation;
+    float min_pos_att;      // minimum positive attenuation component
+    int min_pos_att_idx;
+    float max_beam_length;
+    int has_scattering;
+    int has_attenuation;
+    float cont_prob;
+    float mean_cosine;
+};
+
+struct DLight {
+    int type;
+    int mat_id, med_id;
+    float3 p0, e1, e2;      // area: triangle corner and edges
+    Frame frame;            // area: frame from e1 x e2; directional: from direction
+    float3 intensity;       // area/point/directional; background colour * scale
+    float inv_area;
+    float3 position;        // point light
+};
+
+struct DCamera {
+    float3 origin, direction;
+    float res_x, res_y;
+    float raster_to_world[16];   // row-major 4x4
+    float world_to_raster[16];
+    float image_plane_dist;
+    int mat_id, med_id;
+};
+
+// Two-wide BVH node: both children's boxes + child links.  A link >= 0 is an
+// internal node, a link < 0 is ~(leaf position in the sorted primitive order).
+struct BvhNode {
+    float4 a;   // left.lo.xyz, left.hi.x
+    float4 b;   // left.hi.yz, right.lo.xy
+    float4 c;   // right.lo.z, right.hi.xyz
+    int4 link;  // left, right, -, -
+};
+
+struct BvhView {
+    const BvhNode* nodes;
+    unsigned count;          // primitives
+};
+
+// Triangles in BVH leaf order: v0 (w = original index bits), e1, e2.
+struct TriView {
+    BvhView bvh;
+    const float4* tri;       // 3 float4 per triangle
+    const float4* normals;   // 4 float4 per triangle (n0, n1, n2, face), original order
+    const int2* record;      // (material, light) per triangle, original order
+};
+
+// Light vertex record: 8 x 16 B, one per stored light-subpath vertex, placed
+// at slot path * slots_per_path + k so a subpath's vertices are contiguous.
+//   q0: hitpoint.xyz, meta bits (path_length | flags << 8 | bsdf_flags << 16)
+//   q1: throughput.xyz, continuation probability
+//   q2: d_shared, d_bpt, d_pde, ray_sample_for_pdf_inv
+//   q3: ray_sample_rev_pdf_inv, for_pdfs_ratio, rev_pdfs_ratio, id bits (mat or med id | prev bits << 24)
+//   q4: frame z (shading normal or -world_dir_fix), ior or mean cosine
+//   q5: local_dir_fix.xyz (surface) / world_dir_fix (medium), cos_theta_fix_geom
+//   q6: local geometry normal.xyz, reflect coefficient
+//   q7: diffuse / phong / reflect / refract probabilities
+struct LightVertexRec {
+    float4 q[8];
+};
+
+// Photon beam record: 7 x 16 B.
+//   q0: origin.xyz, length        q1: direction.xyz, medium id bits
+//   q2: throughput at origin.xyz, ray_sample_for_pdf
+//   q3: ray_sample_rev_pdf, sampling flags bits, path index bits, path length bits
+//   q4: d_shared, d_bpt, d_pde, ray_sample_for_pdf_inv
+//   q5: ray_sample_rev_pdf_inv, for_pdfs_ratio, rev_pdfs_ratio, bits (prev_in_medium | prev_specular<<1 | infinite<<2)
+//   q6: last_sin_theta, d_bpt_a, d_bpt_b, d_pde_a ; d_pde_b goes in q7.x
+struct BeamRec {
+    float4 q[8];
+};
+
+// Point map: BVH over light-vertex positions in leaf order.
+//   pos[i] = (position.xyz, slot index bits)
+struct PointMap {
+    BvhView bvh;
+    const float4* pos;
+};
+
+// Beam map: BVH over beam segments in leaf order.
+//   seg[2i] = (origin.xyz, length), seg[2i+1] = (direction.xyz, beam index bits)
+struct BeamMap {
+    BvhView bvh;
+    const float4* seg;
+};
+
+struct DeviceParams {
+    // scene
+    const DMaterial* materials;
+    int material_count;
+    const DMedium* media;
+    int medium_count;
+    int global_medium;
+    const DLight* lights;
+    int light_count;
+    int background_light;
+    DCamera camera;
+    float3 scene_center;
+    float scene_radius, inv_radius_sqr;
+    TriView real;
+    TriView imag;
+
+    // configuration (fixed for the context)
+    unsigned min_path_length, max_path_length;
+    int photon_beam_type, camera_beam_type;
+    float subpath_count_bpt, subpath_count_bb1d, subpath_count_bp2d, subpath_count_pb2d, subpath_count_pp3d,
+        subpath_count_surf;
+    int trace_light_paths, trace_camera_paths;
+    int do_bpt, do_bb1d, do_bp2d, do_pb2d, do_pp3d, do_surf;
+    int build_bb1d, build_bp2d, build_pb2d, build_pp3d, build_surf;
+    int connect_to_camera_from_surf, ignore_fully_spec_paths, use_shading_normal;
+    unsigned estimator_techniques;
+    unsigned screen_pixel_count, light_subpath_count, bb1d_used_light_subpath_count;
+    unsigned res_x, res_y;
+    unsigned long long iteration_offset;
+
+    // per iteration
+    unsigned iteration;
+    float bb1d_normalization, bp2d_normalization, pb2d_normalization, pp3d_normalization, surf_normalization;
+    float mis_factor_bb1d, mis_factor_bp2d, mis_factor_pb2d, mis_factor_pp3d, mis_factor_surf;
+    float radius_bb1d, radius_bp2d, radius_pb2d, radius_pp3d, radius_surf;
+    float radius_bb1d_2, radius_bp2d_2, radius_pb2d_2, radius_pp3d_2, radius_surf_2;
+    float rad_point_med, rad_beam;
+
+    // light-pass records
+    LightVertexRec* vertices;
+    unsigned slots_per_path;
+    unsigned* path_vertex_count;      // stored vertices per light subpath
+    unsigned* counters;               // [0] vertices [1] surface [2] medium [3] beams
+    unsigned* idx_surface;            // vertex slots of surface vertices (append order)
+    unsigned* idx_medium;
+    BeamRec* beams;
+    unsigned beam_capacity;
+    float* framebuffer;               // W*H*3
+    unsigned* status;
+
+    // photon maps built after the light pass
+    PointMap surf_map, med_map;
+    BeamMap beam_map;
+    unsigned n_surface, n_medium, n_beams;   // host-side copies of the light-pass counters
+};
+
+}  // namespace upbp

@@ -1,0 +1,263 @@
+// Light pass: one thread per light subpath.  Emission, tracing through media,
+// photon-beam and light-vertex records, light-to-camera splats.
+// Follows __raygen__trace_light (gpuupbp/kernel/trace_light.cu:42-325) and
+// generate_light_sample / add_beams / connect_to_camera
+// (gpuupbp/kernel/functs_light.cuh:86-388).
+#pragma once
+
+#include "upbp_paths.cuh"
+
+namespace upbp {
+
+UPBP_D unsigned generate_light_sample(PathState& s, Rng& rng)
+{
+    const DeviceParams& p = c_params;
+    const float lc = (float)p.light_count;
+    const int lid = int(rng.uniform() * lc);
+    const float d0 = rng.uniform(), d1 = rng.uniform(), p0 = rng.uniform(), p1 = rng.uniform();
+    const DLight& l = p.lights[lid];
+    float emission_pdf_w, direct_pdf_a, cos_light;
+    s.throughput = light_emit(l, d0, d1, p0, p1, s.origin, s.dir, emission_pdf_w, direct_pdf_a, cos_light);
+    emission_pdf_w /= lc;
+    direct_pdf_a /= lc;
+    s.throughput /= emission_pdf_w;
+    s.path_length = 1;
+    s.is_infinite_light = !light_is_finite(l);
+    s.is_specular_path = false;
+    VertexWeights& w = s.sw.w;
+    w.d_shared = direct_pdf_a / emission_pdf_w;
+    if (!light_is_delta(l)) {
+        const float used_cos = light_is_finite(l) ? cos_light : 1.f;
+        w.d_bpt = used_cos / emission_pdf_w;
+    } else {
+        w.d_bpt = 0.f;
+    }
+    w.d_pde = w.d_bpt * p.subpath_count_bpt;
+    w.prev_specular = false;
+    w.prev_in_medium = false;
+    if (!init_boundary_stack(s.stack)) return kErrBoundaryStack;
+    if (l.mat_id != -1 && l.med_id != -1) {
+        if (!s.stack.push(Boundary{l.mat_id, l.med_id}, boundary_priority(l.mat_id))) return kErrBoundaryStack;
+    }
+    return 0;
+}
+
+// Photon beams along the traced ray (functs_light.cuh:159-247).
+UPBP_D void add_beams(float3 ro, float3 rd, float3 throughput, unsigned path_length, unsigned sflags,
+                      const VolSeg* segs, int nseg, const LiteSeg* lsegs, int nlseg, unsigned path_idx,
+                      const PathState& s)
+{
+    const DeviceParams& p = c_params;
+    float3 thr = throughput;
+    float fpdf = 1.f, rpdf = 1.f;
+    Beam b;
+    b.d = rd;
+    b.path_idx = path_idx;
+    b.sw = s.sw;
+    b.path_length = path_length;
+    b.infinite = s.is_infinite_light;
+    const bool short_beams = p.photon_beam_type == kShortBeam;
+    const int n = short_beams ? nseg : nlseg;
+    for (int i = 0; i < n; i++) {
+        const float dmin = short_beams ? segs[i].dmin : lsegs[i].dmin;
+        const float dmax = short_beams ? segs[i].dmax : lsegs[i].dmax;
+        const int med = short_beams ? segs[i].med : lsegs[i].med;
+        const DMedium& m = p.media[med];
+        if (m.has_scattering) {
+            b.med = med;
+            b.o = ro + rd * dmin;
+            b.length = fminf(dmax - dmin, m.max_beam_length);
+            b.for_pdf = fpdf;
+            b.rev_pdf = rpdf;
+            b.flags = kEndInMedium | (i == 0 ? sflags : 0u);
+            b.thr = thr;
+            const unsigned idx = atomicAdd(&p.counters[3], 1u);
+            if (idx < p.beam_capacity)
+                store_beam(p.beams + idx, b);
+            else
+                flag_status(kErrBeamCapacity);
+        }
+        if (short_beams) {
+            thr *= segs[i].att / segs[i].pdf_for;
+            fpdf *= segs[i].pdf_for;
+            rpdf *= segs[i].pdf_rev;
+        } else {
+            thr *= attenuation(m, dmax - dmin);
+            float sr;
+            const float sf = distance_pdf(m, dmin, dmax, i == 0 ? sflags : 0u, sr);
+            fpdf *= sf;
+            rpdf *= sr;
+        }
+    }
+}
+
+// Light tracing splat to the image plane (functs_light.cuh:251-388, Eq D.38).
+UPBP_D unsigned connect_to_camera(const PathState& s, float3 hit, const Bsdf& bsdf, Rng& rng, VolSeg* segs)
+{
+    const DeviceParams& p = c_params;
+    const DCamera& cam = p.camera;
+    float3 to_cam = cam.origin - hit;
+    if (dot(cam.direction, -to_cam) <= 0.f) return 0;
+    const float2 ip = world_to_raster(cam, hit);
+    if (!raster_inside(cam, ip)) return 0;
+    const float d2 = dot(to_cam, to_cam);
+    const float dist = sqrtf(d2);
+    to_cam /= dist;
+    float cos_to_cam, fpdf, rpdf, sin_theta;
+    const float3 f = bsdf_eval(bsdf, to_cam, cos_to_cam, &fpdf, &rpdf, &sin_theta);
+    if (is_black_or_negative(f)) return 0;
+    rpdf *= bsdf.cont_prob;
+    const float cos_at_cam = dot(cam.direction, -to_cam);
+    const float ip_dist = cam.image_plane_dist / cos_at_cam;
+    const float i2sa = ip_dist * ip_dist / cos_at_cam;
+    const float i2s = i2sa * fabsf(cos_to_cam) / (dist * dist);
+    const float camera_pdf_a = i2s;
+    int nseg = 0;
+    bool occ;
+    const unsigned st = occluded(occ, hit, to_cam, dist, s.stack, bsdf.in_medium() ? kOriginInMedium : 0u, segs, nseg, rng);
+    if (st) return st;
+    if (occ) return 0;
+    float rs_rev = 1.f;
+    float3 att = v3(1.f);
+    if (nseg > 0) {
+        rs_rev = seg_rev_pdf(segs, nseg);
+        att = seg_attenuation(segs, nseg);
+        if (!is_positive(att)) return 0;
+    }
+    const VertexWeights& wl = s.sw.w;
+    const float f_s = pde_factor(bsdf.in_medium(), false, wl.for_inv, wl.for_ratio, 1.f / rs_rev, wl.rev_ratio, sin_theta);
+    const float bpt_s_sub_1 = !wl.prev_specular;
+    const float w_light = (camera_pdf_a / p.light_subpath_count) * rs_rev *
+                          (f_s + bpt_s_sub_1 * wl.d_shared + (rpdf / wl.rev_inv) * wl.d_bpt);
+    const float mis = 1.f / (w_light + 1.f);
+    const float s2i = 1.f / i2s;
+    const float3 contrib = mis * s.throughput * f * att / (p.light_subpath_count * s2i);
+    if (is_black_or_negative(contrib)) return 0;
+    if (ip.x < 0.f || ip.x >= (float)p.res_x || ip.y < 0.f || ip.y >= (float)p.res_y) return 0;
+    const unsigned px = (unsigned)int(ip.x) + (unsigned)int(ip.y) * p.res_x;
+    atomicAdd(&p.framebuffer[3 * px + 0], contrib.x);
+    atomicAdd(&p.framebuffer[3 * px + 1], contrib.y);
+    atomicAdd(&p.framebuffer[3 * px + 2], contrib.z);
+    return 0;
+}
+
+__global__ void __launch_bounds__(128) light_pass_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned path_idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (path_idx >= p.light_subpath_count) return;
+
+    VolSeg segs[kMaxVolSegments];
+    LiteSeg lsegs[kMaxVolSegments];
+    Rng rng;
+    rng.init(p.iteration + p.iteration_offset, path_idx, 0u);
+    const bool store_beams = (p.do_bb1d && path_idx < p.bb1d_used_light_subpath_count) || p.do_bp2d;
+    unsigned stored = 0;
+    LightVertexRec* my_slots = p.vertices + (size_t)path_idx * p.slots_per_path;
+
+    PathState s;
+    unsigned ret = generate_light_sample(s, rng);
+    const DMedium& gm = p.media[p.global_medium];
+    if (s.is_infinite_light && gm.has_attenuation) {
+        p.path_vertex_count[path_idx] = 0;
+        return;
+    }
+    bool origin_in_medium = false;
+    for (; ret == 0; s.path_length++) {
+        const float3 ro = s.origin, rd = s.dir;
+        Isect isect;
+        isect.dist = kInfinity;
+        isect.mat = isect.med = isect.light = -1;
+        isect.normal = v3(0.f);
+        isect.enter = false;
+        int nseg = 0, nlseg = 0;
+        bool hit;
+        ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
+                              segs, nseg, lsegs, nlseg, rng);
+        if (ret) break;
+        if (store_beams)
+            add_beams(ro, rd, s.throughput, s.path_length, origin_in_medium ? kOriginInMedium : 0u, segs, nseg, lsegs,
+                      nlseg, path_idx, s);
+        if (!hit) break;
+
+        float rs_for = 1.f, rs_rev = 1.f;
+        if (nseg > 0) {
+            rs_for = seg_for_pdf(segs, nseg);
+            rs_rev = seg_rev_pdf(segs, nseg);
+            s.throughput *= seg_attenuation(segs, nseg) / rs_for;
+        }
+        if (is_black_or_negative(s.throughput)) break;
+
+        VertexWeights& w = s.sw.w;
+        if (s.path_length > 1u) {
+            const float f_i = pde_factor(w.prev_in_medium, w.prev_specular, w.for_inv, w.for_ratio, 1.f / rs_rev,
+                                         w.rev_ratio, s.sw.last_sin_theta);
+            w.d_bpt = s.sw.d_bpt_a * f_i + s.sw.d_bpt_b;
+            w.d_pde = s.sw.d_pde_a * f_i + s.sw.d_pde_b;
+        }
+        w.d_shared /= rs_for;
+        w.d_bpt /= rs_for;
+        w.d_pde /= rs_for;
+
+        Bsdf bsdf;
+        float3 frame_src;
+        if (isect.on_surface()) {
+            frame_src = isect.shading_normal;
+            bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, true, relative_ior(isect, s.stack));
+        } else {
+            frame_src = rd;
+            bsdf_setup_medium(bsdf, rd, isect.med, true);
+        }
+        if (!bsdf.valid()) break;
+        float ratio = 0.f;
+        if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
+        const float3 hitpoint = ro + rd * isect.dist;
+        origin_in_medium = isect.in_medium();
+        {
+            const float d = bsdf.d_factor();
+            if (!(s.path_length == 1 && s.is_infinite_light)) w.d_shared *= isect.dist * isect.dist;
+            w.d_shared /= d;
+            w.d_bpt /= d;
+            w.d_pde /= d;
+            w.for_inv = 1.f / rs_for;
+            w.rev_inv = 1.f / rs_rev;
+            w.for_ratio = ratio;
+            w.rev_ratio = ratio;
+        }
+        if (!bsdf.delta()) {
+            bool behind = false;
+            if (origin_in_medium && s.stack.size > 0) {
+                const int mid = s.stack.top().mat;
+                if (mid >= 0 && p.materials[mid].real) behind = true;
+            }
+            if (stored < p.slots_per_path) {
+                const unsigned slot = path_idx * p.slots_per_path + stored;
+                store_vertex(my_slots + stored, hitpoint, s.throughput, s.path_length, origin_in_medium, behind, bsdf,
+                             frame_src, w);
+                stored++;
+                atomicAdd(&p.counters[0], 1u);
+                if (origin_in_medium) {
+                    const unsigned k = atomicAdd(&p.counters[2], 1u);
+                    p.idx_medium[k] = slot;
+                } else {
+                    const unsigned k = atomicAdd(&p.counters[1], 1u);
+                    p.idx_surface[k] = slot;
+                }
+            }
+        }
+        if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || p.connect_to_camera_from_surf)) {
+            if (s.path_length + 1 >= p.min_path_length) {
+                ret = connect_to_camera(s, hitpoint, bsdf, rng, segs);
+                if (ret) break;
+            }
+        }
+        if (s.path_length + 2 > p.max_path_length) break;
+        bool cont;
+        ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
+        if (ret || !cont) break;
+    }
+    if (ret) flag_status(ret);
+    p.path_vertex_count[path_idx] = stored;
+}
+
+}  // namespace upbp

@@ -1,0 +1,87 @@
+// `upbp` executable: the reference's main (gpuupbp/gpuupbp.cpp:57-148) on the
+// C ABI: parse the command line, load the scene, run the iteration or time
+// loop with optional continuous output, average and write the image.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/upbp.h"
+
+static int save_image(const std::string& name, const std::vector<float>& rgb, uint32_t w, uint32_t h)
+{
+    if (name.size() > 4 && name.substr(name.size() - 4) == ".exr") return upbp_write_exr(name.c_str(), rgb.data(), w, h);
+    std::fprintf(stderr, "only .exr output is written by this build (%s)\n", name.c_str());
+    return UPBP_ERR_ARGS;
+}
+
+int main(int argc, const char** argv)
+{
+    upbp_config cfg;
+    const int rc = upbp_parse_command_line(argc, argv, &cfg);
+    if (rc != UPBP_OK) return rc == UPBP_HELP ? 0 : 1;
+    upbp_scene* scene = nullptr;
+    const int lrc = cfg.scene_id < 0 ? upbp_scene_load_obj(cfg.scene_path, cfg.res_x, cfg.res_y, &scene)
+                                     : upbp_scene_load_predefined(cfg.scene_id, cfg.res_x, cfg.res_y, &scene);
+    if (lrc != UPBP_OK) {
+        std::fprintf(stderr, "scene: %s\n", upbp_last_error());
+        return 1;
+    }
+    std::printf("Scene:    %s\n", cfg.scene_path);
+    if (cfg.max_time > 0)
+        std::printf("Target:   %g seconds render time\n", cfg.max_time);
+    else
+        std::printf("Target:   %d iteration(s)\n", cfg.iteration_count);
+    upbp_ctx* ctx = nullptr;
+    if (upbp_create(upbp_scene_get_desc(scene), &cfg, &ctx) != UPBP_OK) {
+        std::fprintf(stderr, "init: %s\n", upbp_last_error());
+        upbp_scene_free(scene);
+        return 1;
+    }
+    const uint32_t w = cfg.res_x, h = cfg.res_y;
+    const std::string out = cfg.output_name;
+    const std::string stem = out.substr(0, out.size() - 4), ext = out.substr(out.size() - 3);
+    auto t0 = std::chrono::steady_clock::now();
+    int iter = 0;
+    auto continuous = [&](int done) {
+        if (cfg.continuous_output > 0 && done % cfg.continuous_output == 0) {
+            std::vector<float> img((size_t)w * h * 3, 0.f);
+            upbp_accumulate_to_host(ctx, img.data(), 1.0 / done);
+            char name[2048];
+            std::snprintf(name, sizeof(name), "%s-%d.%s", stem.c_str(), done, ext.c_str());
+            save_image(name, img, w, h);
+        }
+    };
+    if (cfg.max_time > 0) {
+        for (;;) {
+            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (el >= cfg.max_time) break;
+            if (upbp_run_iteration(ctx, iter) != UPBP_OK) break;
+            iter++;
+            continuous(iter);
+        }
+    } else {
+        int percent = -1;
+        for (iter = 0; iter < cfg.iteration_count; iter++) {
+            if (upbp_run_iteration(ctx, iter) != UPBP_OK) {
+                std::fprintf(stderr, "iteration %d: %s\n", iter, upbp_last_error());
+                break;
+            }
+            const int p = (int)((float)(iter + 1) / cfg.iteration_count * 100.f);
+            if (p != percent) {
+                percent = p;
+                std::printf("%d%%\n", p);
+            }
+            continuous(iter + 1);
+        }
+    }
+    std::vector<float> img((size_t)w * h * 3, 0.f);
+    upbp_accumulate_to_host(ctx, img.data(), iter > 0 ? 1.0 / iter : 0.0);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("done in %.2f s (%i iterations)\n", secs, iter);
+    const int src = save_image(out, img, w, h);
+    upbp_destroy(ctx);
+    upbp_scene_free(scene);
+    return src == UPBP_OK ? 0 : 1;
+}

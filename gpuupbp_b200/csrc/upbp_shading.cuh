@@ -1,0 +1,600 @@
+// Scattering models, media, lights and camera mapping.  Every formula follows
+// the reference's device code so that, fed the same random numbers, a path
+// takes the same decisions:
+//   sampling warps        gpuupbp/kernel/sample.cuh:31-205
+//   HG phase function     gpuupbp/kernel/phase_function.cuh:34-137
+//   homogeneous media     gpuupbp/kernel/medium.cuh:33-171
+//   surface BSDF          gpuupbp/kernel/bsdf.cuh:61-660
+//   lights                gpuupbp/kernel/light.cuh:38-543
+//   camera                gpuupbp/kernel/camera.cuh:33-76
+#pragma once
+
+#include "upbp_device.cuh"
+
+namespace upbp {
+
+__constant__ DeviceParams c_params;
+
+// ---------------------------------------------------------------- warps
+
+UPBP_D float3 sample_cos_hemisphere(float u0, float u1, float* pdf)
+{
+    const float phi = 2.f * kPi * u0;
+    const float r = sqrtf(u1);
+    float3 d = make_float3(cosf(phi) * r, sinf(phi) * r, sqrtf(1.f - u1));
+    if (pdf) *pdf = d.z * kInvPi;
+    return d;
+}
+
+UPBP_D float3 sample_power_cos_hemisphere(float u0, float u1, float power)
+{
+    const float phi = 2.f * kPi * u0;
+    const float ct = powf(u1, 1.f / (power + 1.f));
+    const float st = sqrtf(1.f - ct * ct);
+    return make_float3(cosf(phi) * st, sinf(phi) * st, ct);
+}
+
+UPBP_D float power_cos_hemisphere_pdf(float3 n, float3 d, float power)
+{
+    const float c = fmaxf(0.f, dot(n, d));
+    return (power + 1.f) * powf(c, power) * (kInvPi * .5f);
+}
+
+UPBP_D float3 sample_uniform_sphere(float u0, float u1, float* pdf)
+{
+    const float phi = 2.f * kPi * u0;
+    const float s = 2.f * sqrtf(u1 - u1 * u1);
+    if (pdf) *pdf = kInvPi * .25f;
+    return make_float3(cosf(phi) * s, sinf(phi) * s, 1.f - 2.f * u1);
+}
+
+UPBP_D float uniform_sphere_pdf() { return kInvPi * .25f; }
+
+UPBP_D float2 sample_concentric_disc(float u0, float u1)
+{
+    float phi, r;
+    const float a = 2.f * u0 - 1.f, b = 2.f * u1 - 1.f;
+    if (a > -b) {
+        if (a > b) {
+            r = a;
+            phi = (kPi / 4.f) * (b / a);
+        } else {
+            r = b;
+            phi = (kPi / 4.f) * (2.f - (a / b));
+        }
+    } else {
+        if (a < b) {
+            r = -a;
+            phi = (kPi / 4.f) * (4.f + (b / a));
+        } else {
+            r = -b;
+            phi = b != 0.f ? (kPi / 4.f) * (6.f - (a / b)) : 0.f;
+        }
+    }
+    return make_float2(r * cosf(phi), r * sinf(phi));
+}
+
+UPBP_D float fresnel_dielectric(float cos_inc, float ior)
+{
+    if (ior < 0.f) return 1.f;
+    if (cos_inc < 0.f) cos_inc = -cos_inc;
+    const float sin_t2 = ior * ior * (1.f - cos_inc * cos_inc);
+    const float cos_t = sqrtf(fmaxf(0.f, 1.f - sin_t2));
+    const float t1 = ior * cos_t;
+    const float r_par = (cos_inc - t1) / (cos_inc + t1);
+    const float t2 = ior * cos_inc;
+    const float r_perp = (t2 - cos_t) / (t2 + cos_t);
+    return .5f * (r_par * r_par + r_perp * r_perp);
+}
+
+UPBP_D float pdf_w_to_a(float pdf_w, float dist, float cos_there) { return pdf_w * fabsf(cos_there) / (dist * dist); }
+
+// ---------------------------------------------------------------- HG phase
+
+UPBP_D float hg_pdf(float3 dir_fix, float3 dir_gen, float g, float* sin_theta)
+{
+    const float ct = -dot(dir_gen, dir_fix);
+    if (sin_theta) *sin_theta = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+    if (fabsf(g) < 1e-3f) return uniform_sphere_pdf();
+    const float g2 = g * g;
+    const float d = 1.f + g2 - (g + g) * ct;
+    return d > 0.f ? uniform_sphere_pdf() * (1.f - g2) / (d * sqrtf(d)) : 0.f;
+}
+
+// Samples around frame.z (= -dir_fix).  Returns the pdf as the phase value.
+UPBP_D float hg_sample(float3 dir_fix, float g, float u0, float u1, const Frame& frame, float3& dir_gen, float& pdf,
+                       float* sin_theta)
+{
+    if (fabsf(g) < 1e-3f) {
+        dir_gen = sample_uniform_sphere(u0, u1, &pdf);
+        if (sin_theta) {
+            const float ct = -dot(dir_gen, dir_fix);
+            *sin_theta = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+        }
+    } else {
+        const float g2 = g * g, two_g = g + g;
+        const float s = (1.f - g2) / (1.f - g + two_g * u0);
+        const float ct = (1.f + g2 - s * s) / two_g;
+        const float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+        const float phi = 2.f * kPi * u1;
+        const float d = 1.f + g2 - two_g * ct;
+        dir_gen = frame.to_world(make_float3(cosf(phi) * st, sinf(phi) * st, ct));
+        pdf = d > 0.f ? (uniform_sphere_pdf() * (1.f - g2) / (d * sqrtf(d))) : 0.f;
+        if (sin_theta) *sin_theta = st;
+    }
+    return pdf;
+}
+
+// ---------------------------------------------------------------- media
+
+UPBP_D float3 attenuation(const DMedium& m, float dist)
+{
+    return make_float3(expf(-m.attenuation.x * dist), expf(-m.attenuation.y * dist), expf(-m.attenuation.z * dist));
+}
+
+UPBP_D float3 emission(const DMedium& m, float dmin, float dmax)
+{
+    const float d = dmax - dmin;
+    return m.emission * d;
+}
+
+// Free-flight sample within [0, dist_to_boundary]; see medium.cuh:64-119.
+UPBP_D float sample_distance(const DMedium& m, float dist_to_boundary, float rnd, float& for_pdf, unsigned flags,
+                             float& rev_pdf)
+{
+    if (m.min_pos_att != 0.f && m.has_scattering) {
+        const float s = -logf(rnd) / m.min_pos_att;
+        if (s < dist_to_boundary) {
+            const float att = expf(-m.min_pos_att * s);
+            for_pdf = m.min_pos_att * att;
+            rev_pdf = (flags & kOriginInMedium) ? for_pdf : att;
+            return s;
+        }
+        const float att = expf(-m.min_pos_att * dist_to_boundary);
+        for_pdf = att;
+        rev_pdf = (flags & kOriginInMedium) ? m.min_pos_att * att : att;
+        return dist_to_boundary;
+    }
+    for_pdf = 1.f;
+    rev_pdf = 1.f;
+    return dist_to_boundary;
+}
+
+// Pdf of sampling along [dmin, dmax]; see medium.cuh:126-156.
+UPBP_D float distance_pdf(const DMedium& m, float dmin, float dmax, unsigned flags, float& rev_pdf)
+{
+    float for_pdf = 1.f;
+    rev_pdf = 1.f;
+    if (m.min_pos_att != 0.f && m.has_scattering) {
+        const float att = fmaxf(expf(-m.min_pos_att * (dmax - dmin)), 1e-35f);
+        const float minatt = fmaxf(m.min_pos_att * att, 1e-35f);
+        for_pdf = (flags & kEndInMedium) ? minatt : att;
+        rev_pdf = (flags & kOriginInMedium) ? minatt : att;
+    }
+    return for_pdf;
+}
+
+// ---------------------------------------------------------------- BSDF
+
+enum : int { kBsdfInMedium = 1, kBsdfFromLight = 2, kBsdfValid = 4, kBsdfDelta = 8 };
+enum : unsigned { kEvDiffuse = 1, kEvPhong = 2, kEvReflect = 4, kEvRefract = 8, kEvScatter = 16 };
+
+struct Bsdf {
+    Frame frame;
+    float cont_prob;
+    int flags;
+    int id;                  // material (surface) or medium index
+    // surface
+    float3 local_dir_fix;
+    float3 geom_normal;      // local
+    float cos_fix_geom;
+    float reflect_coeff;
+    float diff_prob, phong_prob, refl_prob, refr_prob;
+    float ior;
+    // medium
+    float3 world_dir_fix;
+    float mean_cosine;
+    float3 scatter_coef;
+    bool scatter_pos;
+
+    UPBP_D bool valid() const { return flags & kBsdfValid; }
+    UPBP_D bool delta() const { return flags & kBsdfDelta; }
+    UPBP_D bool in_medium() const { return flags & kBsdfInMedium; }
+    UPBP_D bool on_surface() const { return !(flags & kBsdfInMedium); }
+    UPBP_D bool from_light() const { return flags & kBsdfFromLight; }
+    UPBP_D float cos_fix() const { return local_dir_fix.z; }
+    UPBP_D float d_factor() const { return on_surface() ? fabsf(local_dir_fix.z) : 1.f; }
+    UPBP_D float3 dir_fix() const { return on_surface() ? frame.to_world(local_dir_fix) : world_dir_fix; }
+};
+
+UPBP_D void bsdf_component_probs(Bsdf& b, const DMaterial& m)
+{
+    b.reflect_coeff = fresnel_dielectric(b.local_dir_fix.z, b.ior);
+    const float ad = luminance(m.diffuse);
+    const float ap = luminance(m.phong);
+    const float ar = b.reflect_coeff * luminance(m.mirror);
+    const float at = (1.f - b.reflect_coeff) * (m.ior > 0.f ? 1.f : 0.f);
+    const float total = ad + ap + ar + at;
+    if (total < 1e-9f) {
+        b.diff_prob = b.phong_prob = b.refl_prob = b.refr_prob = 0.f;
+        b.cont_prob = 0.f;
+        return;
+    }
+    b.diff_prob = ad / total;
+    b.phong_prob = ap / total;
+    b.refl_prob = ar / total;
+    b.refr_prob = at / total;
+    const float3 tmp = m.diffuse + m.phong + b.reflect_coeff * m.mirror;
+    b.cont_prob = max_component(tmp) + (1.f - b.reflect_coeff);
+    b.cont_prob = fminf(1.f, fmaxf(0.f, b.cont_prob));
+}
+
+// Surface setup (bsdf.cuh:179-223, surface branch).
+UPBP_D void bsdf_setup_surface(Bsdf& b, float3 ray_dir, float3 normal, float3 shading_normal, int mat_id,
+                               bool from_light, float ior)
+{
+    b.flags = from_light ? kBsdfFromLight : 0;
+    const DMaterial& m = c_params.materials[mat_id];
+    b.id = mat_id;
+    b.frame.set_from_z(shading_normal);
+    b.local_dir_fix = b.frame.to_local(-ray_dir);
+    b.geom_normal = b.frame.to_local(normal);
+    b.cos_fix_geom = dot(b.local_dir_fix, b.geom_normal);
+    if (fabsf(b.local_dir_fix.z) < kEpsCosine || fabsf(b.cos_fix_geom) < kEpsCosine) {
+        b.flags = 0;
+        return;
+    }
+    b.ior = ior;
+    bsdf_component_probs(b, m);
+    if (b.diff_prob == 0.f && b.phong_prob == 0.f) b.flags |= kBsdfDelta;
+    b.flags |= kBsdfValid;
+}
+
+UPBP_D void bsdf_setup_medium(Bsdf& b, float3 ray_dir, int med_id, bool from_light)
+{
+    b.flags = (from_light ? kBsdfFromLight : 0) | kBsdfInMedium;
+    const int idx = min(med_id, c_params.medium_count - 1);
+    const DMedium& m = c_params.media[idx];
+    b.id = idx;
+    b.world_dir_fix = -ray_dir;
+    b.frame.set_from_z(-b.world_dir_fix);
+    b.cont_prob = m.cont_prob;
+    b.mean_cosine = m.mean_cosine;
+    b.scatter_coef = m.scattering;
+    b.scatter_pos = !is_black_or_negative(m.scattering);
+    b.flags |= kBsdfValid;
+}
+
+UPBP_D float3 eval_diffuse(const Bsdf& b, const DMaterial& m, float3 lg, float* fpdf, float* rpdf)
+{
+    if (b.diff_prob == 0.f) return v3(0.f);
+    if (b.local_dir_fix.z < kEpsCosine || lg.z < kEpsCosine) return v3(0.f);
+    if (fpdf) *fpdf += b.diff_prob * fmaxf(0.f, lg.z * kInvPi);
+    if (rpdf) *rpdf += b.diff_prob * fmaxf(0.f, b.local_dir_fix.z * kInvPi);
+    return m.diffuse * kInvPi;
+}
+
+UPBP_D float3 eval_phong(const Bsdf& b, const DMaterial& m, float3 lg, float* fpdf, float* rpdf)
+{
+    if (b.phong_prob == 0.f) return v3(0.f);
+    if (b.local_dir_fix.z < kEpsCosine || lg.z < kEpsCosine) return v3(0.f);
+    const float3 refl = make_float3(-b.local_dir_fix.x, -b.local_dir_fix.y, b.local_dir_fix.z);
+    const float dr = dot(refl, lg);
+    if (dr <= kEpsPhong) return v3(0.f);
+    const float pw = powf(dr, m.phong_exponent);
+    if (!is_positive(pw)) return v3(0.f);
+    if (fpdf || rpdf) {
+        const float p = b.phong_prob * power_cos_hemisphere_pdf(refl, lg, m.phong_exponent);
+        if (fpdf) *fpdf += p;
+        if (rpdf) *rpdf += p;
+    }
+    return m.phong * (m.phong_exponent + 2.f) * .5f * kInvPi * pw;
+}
+
+UPBP_D void pdf_phong(const Bsdf& b, const DMaterial& m, float3 lg, float* fpdf, float* rpdf)
+{
+    if (b.phong_prob == 0.f) return;
+    const float3 refl = make_float3(-b.local_dir_fix.x, -b.local_dir_fix.y, b.local_dir_fix.z);
+    const float dr = dot(refl, lg);
+    if (dr <= kEpsPhong) return;
+    const float p = power_cos_hemisphere_pdf(refl, lg, m.phong_exponent) * b.phong_prob;
+    if (fpdf) *fpdf += p;
+    if (rpdf) *rpdf += p;
+}
+
+// BSDF value for a generated world direction (bsdf.cuh:339-402).
+UPBP_D float3 bsdf_eval(const Bsdf& b, float3 dir_gen, float& cos_gen, float* fpdf, float* rpdf, float* sin_theta)
+{
+    if (b.on_surface()) {
+        if (fpdf) *fpdf = 0.f;
+        if (rpdf) *rpdf = 0.f;
+        if (sin_theta) *sin_theta = 0.f;
+        const float3 lg = b.frame.to_local(dir_gen);
+        const float cg = lg.z;
+        const float cgg = dot(lg, b.geom_normal);
+        cos_gen = fabsf(cg);
+        if (cos_gen < kEpsCosine || fabsf(cgg) < kEpsCosine) return v3(0.f);
+        if (cg * b.cos_fix() < 0.f || cgg * b.cos_fix_geom < 0.f) return v3(0.f);
+        const DMaterial& m = c_params.materials[b.id];
+        float3 r = eval_diffuse(b, m, lg, fpdf, rpdf);
+        r += eval_phong(b, m, lg, fpdf, rpdf);
+        return r;
+    }
+    cos_gen = 1.f;
+    if (!b.scatter_pos) {
+        if (fpdf) *fpdf = 0.f;
+        if (rpdf) *rpdf = 0.f;
+        if (sin_theta) *sin_theta = 0.f;
+        return v3(0.f);
+    }
+    const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, sin_theta);
+    if (fpdf) *fpdf = p;
+    if (rpdf) *rpdf = p;
+    return b.scatter_coef * p;
+}
+
+// Pdf of a generated direction, forward or reverse (bsdf.cuh:408-458).
+UPBP_D float bsdf_pdf(const Bsdf& b, float3 dir_gen, bool reverse)
+{
+    if (b.on_surface()) {
+        const float3 lg = b.frame.to_local(dir_gen);
+        const float cg = lg.z;
+        const float cgg = dot(lg, b.geom_normal);
+        if (fabsf(cg) < kEpsCosine || fabsf(cgg) < kEpsCosine) return 0.f;
+        if (cg * b.cos_fix() < 0.f || cgg * b.cos_fix_geom < 0.f) return 0.f;
+        float fp = 0.f, rp = 0.f;
+        const DMaterial& m = c_params.materials[b.id];
+        if (b.diff_prob != 0.f) {
+            fp += b.diff_prob * fmaxf(0.f, lg.z * kInvPi);
+            rp += b.diff_prob * fmaxf(0.f, b.local_dir_fix.z * kInvPi);
+        }
+        pdf_phong(b, m, lg, &fp, &rp);
+        return reverse ? rp : fp;
+    }
+    return hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, nullptr);
+}
+
+// Samples a direction (bsdf.cuh:571-658).
+UPBP_D float3 bsdf_sample(const Bsdf& b, float r0, float r1, float r2, float3& dir_gen, float& pdf, float& cos_gen,
+                          unsigned& event, float& sin_theta)
+{
+    if (b.on_surface()) {
+        unsigned ev;
+        if (r2 < b.diff_prob)
+            ev = kEvDiffuse;
+        else if (r2 < b.diff_prob + b.phong_prob)
+            ev = kEvPhong;
+        else if (r2 < b.diff_prob + b.phong_prob + b.refl_prob)
+            ev = kEvReflect;
+        else
+            ev = kEvRefract;
+        event = ev;
+        sin_theta = 0.f;
+        pdf = 0.f;
+        float3 result = v3(0.f);
+        float3 lg = v3(0.f);
+        const DMaterial& m = c_params.materials[b.id];
+        if (ev == kEvDiffuse) {
+            if (b.local_dir_fix.z < kEpsCosine) return v3(0.f);
+            float up;
+            lg = sample_cos_hemisphere(r0, r1, &up);
+            pdf += up * b.diff_prob;
+            result += m.diffuse * kInvPi;
+            if (is_black_or_negative(result)) return v3(0.f);
+            result += eval_phong(b, m, lg, &pdf, nullptr);
+        } else if (ev == kEvPhong) {
+            lg = sample_power_cos_hemisphere(r0, r1, m.phong_exponent);
+            const float3 refl = make_float3(-b.local_dir_fix.x, -b.local_dir_fix.y, b.local_dir_fix.z);
+            Frame f;
+            f.set_from_z(refl);
+            lg = f.to_world(lg);
+            const float dr = dot(refl, lg);
+            if (dr <= kEpsPhong) return v3(0.f);
+            pdf_phong(b, m, lg, &pdf, nullptr);
+            result += m.phong * (m.phong_exponent + 2.f) * .5f * kInvPi * powf(dr, m.phong_exponent);
+            if (is_black_or_negative(result)) return v3(0.f);
+            result += eval_diffuse(b, m, lg, &pdf, nullptr);
+        } else if (ev == kEvReflect) {
+            lg = make_float3(-b.local_dir_fix.x, -b.local_dir_fix.y, b.local_dir_fix.z);
+            pdf += b.refl_prob;
+            result += b.reflect_coeff * m.mirror / fabsf(lg.z);
+            if (is_black_or_negative(result)) return v3(0.f);
+        } else {
+            if (b.ior < 0.f) return v3(0.f);
+            float ci = b.local_dir_fix.z, ct;
+            const float eta = b.ior;
+            if (ci < 0.f) {
+                ci = -ci;
+                ct = 1.f;
+            } else {
+                ct = -1.f;
+            }
+            const float si2 = 1.f - ci * ci;
+            const float st2 = eta * eta * si2;
+            if (!(st2 < 1.f)) return v3(0.f);
+            ct *= sqrtf(fmaxf(0.f, 1.f - st2));
+            lg = make_float3(-eta * b.local_dir_fix.x, -eta * b.local_dir_fix.y, ct);
+            pdf += b.refr_prob;
+            const float rc = 1.f - b.reflect_coeff;
+            result += b.from_light() ? v3(rc / fabsf(ct)) : v3(rc * eta * eta / fabsf(ct));
+            if (is_black_or_negative(result)) return v3(0.f);
+        }
+        dir_gen = b.frame.to_world(lg);
+        lg = b.frame.to_local(dir_gen);
+        const float cg = lg.z;
+        const float cgg = dot(lg, b.geom_normal);
+        cos_gen = fabsf(cg);
+        if (cos_gen < kEpsCosine || fabsf(cgg) < kEpsCosine) return v3(0.f);
+        const bool refr = ev == kEvRefract;
+        if ((refr && cg * b.cos_fix() > 0.f) || (!refr && cg * b.cos_fix() < 0.f) ||
+            (refr && cgg * b.cos_fix_geom > 0.f) || (!refr && cgg * b.cos_fix_geom < 0.f))
+            return v3(0.f);
+        return result;
+    }
+    cos_gen = 1.f;
+    event = kEvScatter;
+    if (!b.scatter_pos) {
+        dir_gen = v3(0.f);
+        pdf = 0.f;
+        sin_theta = 0.f;
+        return v3(0.f);
+    }
+    hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
+    return b.scatter_coef * pdf;
+}
+
+// ---------------------------------------------------------------- lights
+
+UPBP_D bool light_is_finite(const DLight& l) { return l.type == kLightArea || l.type == kLightPoint; }
+UPBP_D bool light_is_delta(const DLight& l) { return l.type == kLightDirectional || l.type == kLightPoint; }
+
+// Next-event sample toward the light (light.cuh illuminate).
+UPBP_D float3 light_illuminate(const DLight& l, float3 x, float u0, float u1, float3& dir_to_light, float& dist,
+                               float& direct_pdf_w, float& emission_pdf_w, float& cos_at_light)
+{
+    switch (l.type) {
+    case kLightArea: {
+        const float su = sqrtf(u0);
+        const float bu = 1.f - su, bv = u1 * su;
+        const float3 p = l.p0 + l.e1 * bu + l.e2 * bv;
+        dir_to_light = p - x;
+        const float d2 = dot(dir_to_light, dir_to_light);
+        dist = sqrtf(d2);
+        dir_to_light = dir_to_light / dist;
+        const float cn = dot(l.frame.z, -dir_to_light);
+        if (cn < kEpsCosine) return v3(0.f);
+        direct_pdf_w = l.inv_area * d2 / cn;
+        cos_at_light = cn;
+        emission_pdf_w = l.inv_area * cn * kInvPi;
+        return l.intensity;
+    }
+    case kLightBackground: {
+        dir_to_light = sample_uniform_sphere(u0, u1, &direct_pdf_w);
+        dist = kInfinity;
+        emission_pdf_w = direct_pdf_w * kInvPi * c_params.inv_radius_sqr;
+        cos_at_light = 1.f;
+        return l.intensity;
+    }
+    case kLightDirectional: {
+        dir_to_light = -l.frame.z;
+        dist = kInfinity;
+        direct_pdf_w = 1.f;
+        cos_at_light = 1.f;
+        emission_pdf_w = kInvPi * c_params.inv_radius_sqr;
+        return l.intensity;
+    }
+    default: {
+        dir_to_light = l.position - x;
+        const float d2 = dot(dir_to_light, dir_to_light);
+        direct_pdf_w = d2;
+        dist = sqrtf(d2);
+        dir_to_light = dir_to_light / dist;
+        cos_at_light = 1.f;
+        emission_pdf_w = uniform_sphere_pdf();
+        return l.intensity;
+    }
+    }
+}
+
+// Emission sample (light.cuh emit).
+UPBP_D float3 light_emit(const DLight& l, float d0, float d1, float p0, float p1, float3& pos, float3& dir,
+                         float& emission_pdf_w, float& direct_pdf_a, float& cos_light)
+{
+    switch (l.type) {
+    case kLightArea: {
+        const float su = sqrtf(p0);
+        pos = l.p0 + l.e1 * (1.f - su) + l.e2 * (p1 * su);
+        float3 lo = sample_cos_hemisphere(d0, d1, &emission_pdf_w);
+        emission_pdf_w *= l.inv_area;
+        lo.z = fmaxf(lo.z, kEpsCosine);
+        dir = l.frame.to_world(lo);
+        direct_pdf_a = l.inv_area;
+        cos_light = lo.z;
+        return l.intensity * lo.z;
+    }
+    case kLightBackground: {
+        float fp;
+        dir = sample_uniform_sphere(d0, d1, &fp);
+        const float2 xy = sample_concentric_disc(p0, p1);
+        Frame f;
+        f.set_from_z(dir);
+        pos = c_params.scene_center + c_params.scene_radius * (-dir + f.x * xy.x + f.y * xy.y);
+        emission_pdf_w = fp * kInvPi * c_params.inv_radius_sqr;
+        direct_pdf_a = fp;
+        cos_light = 1.f;
+        return l.intensity;
+    }
+    case kLightDirectional: {
+        const float2 xy = sample_concentric_disc(p0, p1);
+        pos = c_params.scene_center + c_params.scene_radius * (-l.frame.z + l.frame.x * xy.x + l.frame.y * xy.y);
+        dir = l.frame.z;
+        emission_pdf_w = kInvPi * c_params.inv_radius_sqr;
+        direct_pdf_a = 1.f;
+        cos_light = 1.f;
+        return l.intensity;
+    }
+    default: {
+        pos = l.position;
+        dir = sample_uniform_sphere(d0, d1, &emission_pdf_w);
+        direct_pdf_a = 1.f;
+        cos_light = 1.f;
+        return l.intensity;
+    }
+    }
+}
+
+// Radiance of a light hit by a ray (light.cuh get_radiance).
+UPBP_D float3 light_radiance(const DLight& l, float3 ray_dir, float& direct_pdf_a, float& emission_pdf_w)
+{
+    if (l.type == kLightArea) {
+        const float c = fmaxf(0.f, dot(l.frame.z, -ray_dir));
+        if (c == 0.f) return v3(0.f);
+        direct_pdf_a = l.inv_area;
+        emission_pdf_w = fmaxf(0.f, dot(l.frame.z, -ray_dir)) * kInvPi * l.inv_area;
+        return l.intensity;
+    }
+    if (l.type == kLightBackground) {
+        const float fp = uniform_sphere_pdf();
+        direct_pdf_a = fp;
+        emission_pdf_w = fp * (kInvPi * c_params.inv_radius_sqr);
+        return l.intensity;
+    }
+    return v3(0.f);
+}
+
+// ---------------------------------------------------------------- camera
+
+UPBP_D float3 transform_point(const float* m, float3 v)
+{
+    float w = m[15];
+    w += m[12] * v.x;
+    w += m[13] * v.y;
+    w += m[14] * v.z;
+    const float iw = 1.f / w;
+    float x = m[3];
+    x += v.x * m[0];
+    x += v.y * m[1];
+    x += v.z * m[2];
+    float y = m[7];
+    y += v.x * m[4];
+    y += v.y * m[5];
+    y += v.z * m[6];
+    float z = m[11];
+    z += v.x * m[8];
+    z += v.y * m[9];
+    z += v.z * m[10];
+    return make_float3(x * iw, y * iw, z * iw);
+}
+
+UPBP_D float2 world_to_raster(const DCamera& c, float3 p)
+{
+    const float3 t = transform_point(c.world_to_raster, p);
+    return make_float2(t.x, t.y);
+}
+
+UPBP_D bool raster_inside(const DCamera& c, float2 r)
+{
+    return r.x >= 0.f && r.y >= 0.f && r.x < c.res_x && r.y < c.res_y;
+}
+
+}  // namespace upbp

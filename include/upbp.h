@@ -1,0 +1,200 @@
+/*
+ * upbp.h -- C ABI of the B200 UPBP renderer (libupbp_b200.so).
+ *
+ * Drop-in boundary for the reference's render path.  The reference's only
+ * plugin boundary is `struct Renderer` (gpuupbp/renderer/renderer.hpp:46-149):
+ *     int32_t init(const SceneLoader*, const Config*, Framebuffer*);  // 0 ok, -1 fail
+ *     void run_iteration(int iteration);                              // adds into Framebuffer
+ *     void cleanup();
+ * called from main (gpuupbp/gpuupbp.cpp:85-135) after parse_commandline
+ * (gpuupbp/misc/config.cpp:735-1370) and SceneLoader::load_scene
+ * (gpuupbp/misc/scene_loader.hpp:44-76).  Each entry point below names the
+ * reference interface it replaces.  Plain pointers and sizes only.
+ *
+ * Return codes: 0 ok; > 0 device status bits (UPBP_STATUS_*); < 0 host or
+ * CUDA errors (UPBP_ERR_*).  No exception crosses the ABI.
+ * Threading: one context per host thread; the caller owns host buffers, the
+ * library owns device memory.
+ */
+#ifndef UPBP_B200_H
+#define UPBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- errors */
+#define UPBP_OK 0
+#define UPBP_ERR_ARGS (-1)       /* invalid argument or command line */
+#define UPBP_ERR_IO (-2)         /* file could not be read or written */
+#define UPBP_ERR_CUDA (-3)       /* a CUDA call failed; see upbp_last_error */
+#define UPBP_ERR_NO_DEVICE (-4)  /* no CUDA device / extension not usable */
+#define UPBP_ERR_SCENE (-5)      /* scene description is inconsistent */
+#define UPBP_HELP 1              /* the command line asked for help */
+
+/* Device status bits, the reference's RETURN_WITH_ERR codes
+ * (gpuupbp/kernel/defs.cuh:36-48) turned into bits, plus capacity bits. */
+#define UPBP_STATUS_BOUNDARY_STACK (1u << 0)
+#define UPBP_STATUS_INTERSECTION_ARRAY (1u << 1)
+#define UPBP_STATUS_VOL_SEGMENT_ARRAY (1u << 2)
+#define UPBP_STATUS_INTERSECTION_STACK (1u << 3)
+#define UPBP_STATUS_BEAM_CAPACITY (1u << 4)
+#define UPBP_STATUS_TRAVERSAL_STACK (1u << 5)
+
+/* -------------------------------------------------- estimator selection */
+/* Same bit values as the reference (gpuupbp/shared/shared_enums.h:28-58). */
+#define UPBP_BPT (1u << 2)
+#define UPBP_SURF (1u << 3)
+#define UPBP_PP3D (1u << 4)
+#define UPBP_PB2D (1u << 5)
+#define UPBP_BB1D (1u << 6)
+#define UPBP_BP2D (1u << 7)
+#define UPBP_PREVIOUS (1u << 9)
+#define UPBP_COMPATIBLE (1u << 10)
+#define UPBP_SPECULAR_ONLY (1u << 12)
+#define UPBP_SHORT_BEAM 1
+#define UPBP_LONG_BEAM 2
+
+/* Mirror of the reference's Config (gpuupbp/misc/config.hpp:44-120), POD. */
+typedef struct upbp_config {
+    int scene_id;                 /* -1: OBJ file in scene_path */
+    char scene_path[1024];
+    uint32_t algorithm_flags;     /* UPBP_BPT | UPBP_SURF | ... */
+    int iteration_count;
+    float max_time;               /* seconds, < 0 if unused */
+    char output_name[1024];
+    uint32_t res_x, res_y;
+    uint32_t max_path_length, min_path_length;
+    float path_count_per_iter;    /* resolved to an absolute count by the parser */
+    int query_beam_type;          /* UPBP_SHORT_BEAM / UPBP_LONG_BEAM */
+    int photon_beam_type;
+    float bb1d_radius_initial, bb1d_radius_alpha, bb1d_used_light_subpath_count;
+    float bp2d_radius_initial, bp2d_radius_alpha;
+    float pb2d_radius_initial, pb2d_radius_alpha;
+    float pp3d_radius_initial, pp3d_radius_alpha;
+    float surf_radius_initial, surf_radius_alpha;
+    int continuous_output;
+    int ignore_fully_spec_paths;
+    int gpu_assert;
+    uint64_t iteration_offset;
+    int do_log;
+    int use_shading_normal;
+} upbp_config;
+
+/* ------------------------------------------------------ scene records */
+typedef struct upbp_material {   /* gpuupbp/shared/material.h:42-61 */
+    float diffuse[3];
+    float phong[3];
+    float phong_exponent;
+    float mirror[3];
+    float ior;
+    int priority;
+    int real;
+    int medium;                  /* -1 if none */
+} upbp_material;
+
+typedef struct upbp_medium {     /* gpuupbp/host/medium.hpp init_homogeneous_medium inputs */
+    float absorption[3];
+    float emission[3];
+    float scattering[3];
+    float continuation_prob;
+    float mean_cosine;
+} upbp_medium;
+
+#define UPBP_LIGHT_AREA 0
+#define UPBP_LIGHT_BACKGROUND 1
+#define UPBP_LIGHT_DIRECTIONAL 2
+#define UPBP_LIGHT_POINT 3
+typedef struct upbp_light {      /* gpuupbp/shared/light.h:34-81 */
+    int type;
+    int mat_id, med_id;          /* enclosing material / medium, -1 for global */
+    float p0[3], p1[3], p2[3];   /* area light triangle */
+    float intensity[3];          /* area/point/directional intensity; background colour */
+    float position[3];           /* point light position; directional light direction */
+    float scale;                 /* background scale */
+} upbp_light;
+
+typedef struct upbp_camera_desc {  /* gpuupbp/host/camera.hpp init_camera inputs */
+    float origin[3], target[3], roll[3];
+    float horizontal_fov_deg;
+    float focal_dist;
+    int mat_id, med_id;
+} upbp_camera_desc;
+
+/* Whole scene as flat host arrays (the reference's Scene + Record[],
+ * gpuupbp/shared/scene.h:98-129 and scene_loader.hpp:104-108).  Triangle i
+ * uses verts[9i..9i+8], normals[12i..12i+11] (three vertex normals then the
+ * face normal) and material/light ids; real vs imaginary follows the
+ * material's `real` flag. */
+typedef struct upbp_scene_desc {
+    uint32_t triangle_count;
+    const float* verts;
+    const float* normals;
+    const int32_t* tri_material;
+    const int32_t* tri_light;    /* -1 if the triangle is not an emitter */
+    uint32_t material_count;
+    const upbp_material* materials;
+    uint32_t medium_count;
+    const upbp_medium* media;
+    int32_t global_medium;       /* index into media */
+    uint32_t light_count;
+    const upbp_light* lights;
+    int32_t background_light;    /* index into lights, -1 if none */
+    upbp_camera_desc camera;
+    uint32_t res_x, res_y;
+    float bbox_min[3], bbox_max[3];
+} upbp_scene_desc;
+
+typedef struct upbp_scene upbp_scene;   /* host scene owned by the library */
+typedef struct upbp_ctx upbp_ctx;       /* device renderer state */
+
+typedef struct upbp_stats {
+    uint32_t light_vertices, surface_vertices, medium_vertices, light_beams;
+    uint32_t light_paths, camera_paths;
+    uint32_t status;              /* OR of UPBP_STATUS_* seen so far */
+    uint32_t iterations_done;
+    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events */
+    uint64_t triangle_count;
+    double scene_radius;
+} upbp_stats;
+
+/* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
+ * flags, defaults and errors; returns UPBP_HELP after printing help. */
+int upbp_parse_command_line(int argc, const char** argv, upbp_config* out);
+
+/* Replaces: SceneLoader::load_from_obj (gpuupbp/misc/scene_loader_obj.cpp:926-1104)
+ * with the reference's OBJ+MTL+AUX semantics. */
+int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_t res_y, upbp_scene** out);
+/* Replaces: SceneLoader::load_predefined (gpuupbp/misc/scene_loader_predef.cpp:126). */
+int upbp_scene_load_predefined(int scene_id, uint32_t res_x, uint32_t res_y, upbp_scene** out);
+const upbp_scene_desc* upbp_scene_get_desc(const upbp_scene* scene);
+void upbp_scene_free(upbp_scene* scene);
+
+/* Replaces: Renderer::init (gpuupbp/renderer/renderer_init.cpp:675-929). */
+int upbp_create(const upbp_scene_desc* scene, const upbp_config* config, upbp_ctx** out);
+/* Replaces: Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
+ * Renders iteration `iteration` and adds it to the device accumulation. */
+int upbp_run_iteration(upbp_ctx* ctx, int iteration);
+/* Replaces the D->H framebuffer copy + add_framebuffer of run_iteration
+ * (renderer.cpp:381-392): adds scale * (device accumulation) into rgb. */
+int upbp_accumulate_to_host(upbp_ctx* ctx, float* rgb, double scale);
+/* Copies the last iteration's image (W*H*3 floats, not accumulated). */
+int upbp_read_iteration(upbp_ctx* ctx, float* rgb);
+int upbp_get_stats(upbp_ctx* ctx, upbp_stats* out);
+/* Replaces: Renderer::cleanup (gpuupbp/renderer/renderer.cpp:420-508). */
+void upbp_destroy(upbp_ctx* ctx);
+
+/* Replaces: save(fb, name) -> tinyexr_wrapper::save_exr
+ * (gpuupbp/host/framebuffer.cpp:114-127, misc/tinyexr_wrapper.cpp:34-95):
+ * half-float B,G,R channels, uncompressed scanlines. */
+int upbp_write_exr(const char* path, const float* rgb, uint32_t width, uint32_t height);
+
+const char* upbp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
