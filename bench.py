@@ -1,0 +1,305 @@
+"""Benchmark of the UPBP render iteration on B200.
+
+Workload (the plain large configuration): `media_field` -- 1280x720 pixels,
+ground plane + 20 displaced icosphere media of 81 920 triangles each (about
+1.64M triangles), one emissive sphere light and one quad light, path length
+12, all five estimators plus BPT (`-a upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d`),
+one light path per pixel.  A step is one render iteration (light pass,
+photon-map builds, camera pass).
+
+Metric: paths/s = (camera + light subpaths per iteration) x iterations / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun, one rank per GPU; rank r renders iterations
+r, r+N, ... (iterations are independent given the seed), so the scaling is
+weak; value = all ranks' paths / max over ranks of the timed region.  The
+reference arm times the reference's own render loop compiled for the host
+cores (oracle/_ref/libupbp_ref_cpu.so) on a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+SCENE_DIR = os.environ.get("UPBP_SCENE_DIR", "/tmp/upbp_scenes")
+RES = (1280, 720)
+TECH = "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d"
+PATH_LENGTH = 12
+METRIC = "paths/s (camera + light subpaths per second), plain UPBP render iterations"
+
+
+def workload_args(scene_path: str, res=RES) -> list[str]:
+    return ["-s", "-1", scene_path, "-a", TECH, "-l", str(PATH_LENGTH), "-r", f"{res[0]}x{res[1]}"]
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# Algorithmic bytes of the camera-pass kernel per unit of counted work
+# (record sizes of this build's layouts): BVH node 64 B (two child boxes +
+# links), triangle 48 B (v0, e1, e2), per ray the hit's normals + record 72 B,
+# photon point 16 B, accepted photon's vertex record 128 B, beam chunk 48 B,
+# accepted beam record 128 B, BPT light-vertex record 128 B; plus 24 B of
+# framebuffer read-modify-write per pixel.
+BYTES_PER_WORK = {"nodes": 64, "tris": 48, "rays": 72, "point_cand": 16, "point_hit": 128, "beam_cand": 48,
+                  "beam_hit": 128, "vertex_loads": 128}
+
+
+def algorithmic_bytes(work: dict, pixels: int) -> float:
+    return float(sum(BYTES_PER_WORK[k] * v for k, v in work.items())) + 24.0 * pixels
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per camera-pass launch from the committed ncu summary, if any."""
+    p = os.path.join(HERE, "profiles", "camera_pass_media_field.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for ln in f:
+            if ln.startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(ln.split(":", 1)[1].strip())
+                except ValueError:
+                    return None
+    return None
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_b200(args) -> dict | None:
+    import torch
+    from gpuupbp_b200 import scenes, upbp
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    scene = scenes.write_workload("media_field", SCENE_DIR) if rank == 0 else None
+    if pg is not None:
+        pg.barrier()
+        scene = scenes.write_workload("media_field", SCENE_DIR)
+    r = upbp.Renderer(workload_args(scene))
+    paths_per_iter = r.config.res_x * r.config.res_y + int(r.config.path_count_per_iter)
+    stream = torch.cuda.ExternalStream(r.stream_handle())
+    # rank r renders iterations r, r+N, ...
+    its = iter(range(rank, 10 ** 9, world))
+    for _ in range(args.warmup):
+        r.run_iteration(next(its))
+    r.stats()  # drain the event ring
+
+    def timed(steps: int, readback: bool):
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        wall = time.perf_counter()
+        for _ in range(steps):
+            r.run_iteration(next(its))
+            if readback:
+                r.iteration_image()  # device->host of this step's result
+        t1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall
+        ms = t0.elapsed_time(t1)
+        if pg is not None:
+            t = torch.tensor([ms], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, wall
+
+    with ClockSampler(local) as clk:
+        ms, wall = timed(args.steps, False)
+    st = r.stats()
+    ms_e2e, wall_e2e = timed(args.steps, True)
+    st_e2e = r.stats()
+
+    # final reduction of the accumulated images over ranks (output time, untimed)
+    if pg is not None:
+        acc = torch.from_numpy(r.accumulated(scale=1.0)).cuda()
+        pg.all_reduce(acc)
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        r.close()
+        return None
+
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    pixels = r.config.res_x * r.config.res_y
+    cam_ms = st["ms_camera_sum"] / max(1, st["timed_iterations"])
+    b_cam = algorithmic_bytes(st["work_camera"], pixels)
+    achieved = b_cam / (cam_ms * 1e-3) / 1e9
+    traffic = profiled_traffic()
+    total_paths = paths_per_iter * args.steps * world
+    value = total_paths / (ms * 1e-3)
+    e2e = total_paths / (ms_e2e * 1e-3)
+    out = {
+        "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, OBJ/MTL/AUX)",
+        "config": {"workload": "media_field: 1280x720, 20 displaced icosphere media (1.64M tris), "
+                               "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d, path length 12, 1 light path per pixel",
+                   "triangles": int(st["triangle_count"]), "light_paths_per_iter": int(r.config.path_count_per_iter),
+                   "camera_paths_per_iter": pixels, "parallelism": f"iterations sharded over {world} rank(s)",
+                   "l2": "inputs larger than L2 (scene BVH + triangle data ~300 MB, photon records per iteration)"},
+        "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": int(st_e2e["h2d_bytes"]),
+                "d2h_bytes_per_step": int(st_e2e["d2h_bytes"]) + pixels * 12,
+                "wall_s": wall_e2e},
+        "gpu_launches": int(st["kernel_launches"]) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "camera_pass_kernel", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": b_cam, "launch_ms": cam_ms},
+        "clocks": clk.summary(),
+        "passes_ms": {"light": st["ms_light_sum"] / max(1, st["timed_iterations"]),
+                      "build": st["ms_build_sum"] / max(1, st["timed_iterations"]), "camera": cam_ms},
+        "work_camera": st["work_camera"], "status": int(st["status"]), "wall_s": wall,
+    }
+    r.close()
+    return out
+
+
+def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iters: int | None = None) -> dict:
+    """Times the reference's render loop on host cores on a bounded sample of
+    the workload: the same scene, estimators and path length at 160x90
+    pixels (1/64 of the pixels, one light path per pixel).  Iterations run
+    until `seconds` have been timed or `max_iters` iterations were timed."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import ref_cpu
+    from gpuupbp_b200 import scenes
+
+    scene = scenes.write_workload("media_field", SCENE_DIR)
+    res = (160, 90)
+    r = ref_cpu.RefRenderer(workload_args(scene, res), threads=threads)
+    for w in range(warmup):
+        r.run_iteration(w)
+    it, n, t = warmup, 0, 0.0
+    while (n == 0 or t < seconds) and (max_iters is None or n < max_iters):
+        t0 = time.perf_counter()
+        r.run_iteration(it)
+        t += time.perf_counter() - t0
+        it += 1
+        n += 1
+    st = r.stats()
+    paths = (res[0] * res[1] + st["light_paths"]) * n
+    r.close()
+    return {"value": paths / t, "unit": "paths/s", "cores": threads, "kind": "reference",
+            "sample": f"media_field scene at {res[0]}x{res[1]} (1/64 of the pixels), {n} timed iteration(s), "
+                      f"{t:.1f} s on {threads} host threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    threads = os.cpu_count() or 1
+    world, rank, _ = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # each step is one bounded iteration of the reference loop
+        s2 = run_reference_sample(seconds=1e9, threads=threads, warmup=args.warmup, max_iters=args.steps)
+        v = s2["value"]
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "paths/s", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": "media_field (reference CPU build, 160x90 sample per step)"},
+                          "cpu_baseline": s2, "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0,
+                                                      "d2h_bytes_per_step": 0}}))
+        return
+    out = run_b200(args)
+    if out is None:
+        return
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            out["cpu_baseline"] = run_reference_sample(args.cpu_seconds, threads)
+        except Exception as e:  # the oracle build is absent
+            out["cpu_baseline"] = {"value": None, "unit": "paths/s", "cores": threads, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

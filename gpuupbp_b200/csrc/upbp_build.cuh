@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "upbp_device.cuh"
 
@@ -53,13 +54,19 @@ UPBP_HD float ord2f(unsigned u)
 
 // Primitive source for a build: a box per primitive.
 struct BoxSource {
-    int kind;                 // 0: triangles (v0,e1,e2 x3 float4), 1: points via slot list, 2: beams
+    int kind;                 // 0: triangles (v0,e1,e2 x3 float4), 1: points via slot list, 2: beams, 3: beam chunks
     const float4* tri;        // kind 0: unsorted triangle float4 triples
     const unsigned* slots;    // kind 1: vertex slots
     const LightVertexRec* vertices;
     const BeamRec* beams;     // kind 2
     unsigned bb1d_paths;      // kind 2: beams of paths below this index serve BB1D
+    const uint2* chunks;      // kind 3: (beam index, chunk k | chunk count << 16)
 };
+
+// Parameter range [t0, t1) of chunk k of n along a beam of length len.  Both
+// neighbours evaluate the shared boundary with the same expression, so the
+// chunks partition [0, len) exactly.
+UPBP_HD float chunk_t(float len, unsigned k, unsigned n) { return k >= n ? len : len * (float)k / (float)n; }
 
 UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
 {
@@ -75,11 +82,23 @@ UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
     } else if (s.kind == 1) {
         const float3 p = xyz(s.vertices[s.slots[i]].q[0]);
         lo = hi = p;
-    } else {
+    } else if (s.kind == 2) {
         const float4 a = s.beams[i].q[0], b = s.beams[i].q[1];
         const float3 o = xyz(a), e = xyz(a) + xyz(b) * a.w;
         lo = make_float3(fminf(o.x, e.x), fminf(o.y, e.y), fminf(o.z, e.z));
         hi = make_float3(fmaxf(o.x, e.x), fmaxf(o.y, e.y), fmaxf(o.z, e.z));
+    } else {
+        const uint2 ch = s.chunks[i];
+        const float4 a = s.beams[ch.x].q[0], b = s.beams[ch.x].q[1];
+        const unsigned k = ch.y & 0xffffu, n = ch.y >> 16;
+        const float t0 = chunk_t(a.w, k, n), t1 = chunk_t(a.w, k + 1, n);
+        const float3 o = xyz(a) + xyz(b) * t0, e = xyz(a) + xyz(b) * t1;
+        lo = make_float3(fminf(o.x, e.x), fminf(o.y, e.y), fminf(o.z, e.z));
+        hi = make_float3(fmaxf(o.x, e.x), fmaxf(o.y, e.y), fmaxf(o.z, e.z));
+        // cover the rounding of o + d t at both ends
+        const float3 ext = (hi - lo) * 1e-6f + v3(1e-6f * (fabsf(lo.x) + fabsf(lo.y) + fabsf(lo.z) + 1e-3f));
+        lo = lo - ext;
+        hi = hi + ext;
     }
 }
 
@@ -251,6 +270,44 @@ __global__ void k_gather_beams(const BeamRec* beams, const unsigned* vals, unsig
     const unsigned bits = b | (path_idx < bb1d_paths ? 0x80000000u : 0u);
     out[2 * s] = q0;
     out[2 * s + 1] = make_float4(q1.x, q1.y, q1.z, __uint_as_float(bits));
+}
+
+// Chunk counts per beam: long beams are split so every BVH leaf box stays
+// close to the beam's own extent (an axis-aligned box of a long diagonal beam
+// would overlap most queries).
+__global__ void k_chunk_counts(const BeamRec* beams, unsigned n, float chunk_len, unsigned max_chunks, unsigned* counts)
+{
+    const unsigned b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const float len = beams[b].q[0].w;
+    unsigned c = chunk_len > 0.f ? (unsigned)ceilf(fminf(len / chunk_len, (float)max_chunks)) : 1u;
+    counts[b] = max(1u, min(c, max_chunks));
+}
+
+__global__ void k_chunk_expand(const unsigned* counts, const unsigned* offsets, unsigned n, uint2* chunks)
+{
+    const unsigned b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const unsigned c = counts[b], off = offsets[b];
+    for (unsigned k = 0; k < c; k++) chunks[off + k] = make_uint2(b, k | (c << 16));
+}
+
+// Leaf payload of the chunked beam map: (origin, length), (direction, bits),
+// (t0, t1) where bits = beam index | BB1D-eligible << 31.
+__global__ void k_gather_chunks(const uint2* chunks, const BeamRec* beams, const unsigned* vals, unsigned n,
+                                unsigned bb1d_paths, float4* out)
+{
+    const unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint2 ch = chunks[vals[s]];
+    const unsigned b = ch.x;
+    const float4 q0 = beams[b].q[0], q1 = beams[b].q[1];
+    const unsigned path_idx = __float_as_uint(beams[b].q[3].z);
+    const unsigned bits = b | (path_idx < bb1d_paths ? 0x80000000u : 0u);
+    const unsigned k = ch.y & 0xffffu, c = ch.y >> 16;
+    out[3 * s] = q0;
+    out[3 * s + 1] = make_float4(q1.x, q1.y, q1.z, __uint_as_float(bits));
+    out[3 * s + 2] = make_float4(chunk_t(q0.w, k, c), chunk_t(q0.w, k + 1, c), 0.f, 0.f);
 }
 
 // Scratch owned by a context, sized for the largest build it will run.

@@ -11,6 +11,14 @@ namespace upbp {
 
 constexpr int kStackDepth = 64;
 
+// Adds v to work counter `which`, one atomic per warp.
+UPBP_D void count_work(int which, unsigned v)
+{
+    const unsigned m = __activemask();
+    const unsigned total = __reduce_add_sync(m, v);
+    if ((threadIdx.x & 31) == __ffs(m) - 1 && total) atomicAdd(c_work_ptr() + which, (unsigned long long)total);
+}
+
 UPBP_D float3 safe_inv(float3 d) { return make_float3(1.f / d.x, 1.f / d.y, 1.f / d.z); }
 
 // Segment [tmin, tmax] vs box [lo - pad, hi + pad].  Axes with a zero
@@ -63,10 +71,15 @@ UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& l
     int sp = 0;
     int node = bvh.count > 1 ? 0 : ~0;
     bool ok = true;
+    unsigned visits = 0;
     for (;;) {
         if (node < 0) {
-            if (!leaf(~node)) return ok;
+            if (!leaf(~node)) {
+                count_work(kCtrNodes, visits);
+                return ok;
+            }
         } else {
+            visits++;
             const NodeBoxes nb = load_node(bvh.nodes, node);
             const bool hl = test_box(nb.llo, nb.lhi, pad);
             const bool hr = test_box(nb.rlo, nb.rhi, pad);
@@ -88,7 +101,10 @@ UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& l
                 continue;
             }
         }
-        if (sp == 0) return ok;
+        if (sp == 0) {
+            count_work(kCtrNodes, visits);
+            return ok;
+        }
         node = stack[--sp];
     }
 }
@@ -127,10 +143,12 @@ UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float
     int node = tv.bvh.count > 1 ? 0 : ~0;
     bool found = false;
     float best = tmax;
+    unsigned visits = 0, tests = 0;
     for (;;) {
         if (node < 0) {
             float t, u, v;
             const int s = ~node;
+            tests++;
             if (tri_intersect(tv.tri, s, o, d, t, u, v) && t >= tmin && t <= best) {
                 best = t;
                 hit.t = t;
@@ -140,6 +158,7 @@ UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float
                 found = true;
             }
         } else {
+            visits++;
             const NodeBoxes nb = load_node(tv.bvh.nodes, node);
             // entry distances for ordering
             const float3 t0l = (nb.llo - o) * inv, t1l = (nb.lhi - o) * inv;
@@ -171,6 +190,9 @@ UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float
         if (sp == 0) break;
         node = stack[--sp];
     }
+    count_work(kCtrNodes, visits);
+    count_work(kCtrTris, tests);
+    count_work(kCtrRays, 1u);
     return found;
 }
 
@@ -180,7 +202,9 @@ template <class F>
 UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tmax, F&& f)
 {
     const float3 inv = safe_inv(d);
-    return bvh_walk(
+    unsigned tests = 0;
+    count_work(kCtrRays, 1u);
+    const bool ok = bvh_walk(
         tv.bvh, 0.f,
         [&](float3 lo, float3 hi, float) {
             const float3 t0 = (lo - o) * inv, t1 = (hi - o) * inv;
@@ -190,6 +214,7 @@ UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tm
         },
         [&](int s) {
             float t, u, v;
+            tests++;
             if (tri_intersect(tv.tri, s, o, d, t, u, v) && t >= tmin && t <= tmax) {
                 TriHit h;
                 h.t = t;
@@ -200,6 +225,8 @@ UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tm
             }
             return true;
         });
+    count_work(kCtrTris, tests);
+    return ok;
 }
 
 }  // namespace upbp

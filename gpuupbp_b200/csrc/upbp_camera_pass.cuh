@@ -7,7 +7,7 @@
 // functs_bp2d.cuh:51-229).
 #pragma once
 
-#include "upbp_paths.cuh"
+#include "upbp_queries.cuh"
 
 namespace upbp {
 
@@ -198,19 +198,11 @@ UPBP_D float3 query_points(const PointMap& map, float3 x, float r, float r2, con
                            bool medium)
 {
     float3 acc = v3(0.f);
-    const float pad = r * 1.0001f + 1e-7f;
-    const bool ok = bvh_walk(
-        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
-        [&](int i) {
-            const float4 pp = __ldg(&map.pos[i]);
-            if (pred_point_point(x, xyz(pp), r2)) {
-                LightVertex lv;
-                load_vertex(c_params.vertices + fbits(pp.w), lv);
-                acc += eval_point_merge(lv, s, cb, medium);
-            }
-            return true;
-        });
-    if (!ok) flag_status(kErrTraversalStack);
+    points_in_radius(map, x, r, r2, [&](unsigned slot) {
+        LightVertex lv;
+        load_vertex(c_params.vertices + slot, lv);
+        acc += eval_point_merge(lv, s, cb, medium);
+    });
     return acc;
 }
 
@@ -415,21 +407,12 @@ UPBP_D float3 query_pb2d(const QuerySeg& q, const StateWeights& cw)
 {
     const DeviceParams& p = c_params;
     float3 acc = v3(0.f);
-    const float3 inv = safe_inv(q.d);
-    const float pad = p.radius_pb2d * 1.0001f + 1e-7f;
-    const bool ok = bvh_walk(
-        p.med_map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, q.o, inv, q.dmin, q.dmax); },
-        [&](int i) {
-            const float4 pp = __ldg(&p.med_map.pos[i]);
-            float dist, rad2;
-            if (pred_ray_disc(q.o, q.d, q.dmin, q.dmax, xyz(pp), p.radius_pb2d_2, dist, rad2)) {
-                LightVertex lv;
-                load_vertex(p.vertices + fbits(pp.w), lv);
-                acc += eval_pb2d(q, cw, lv, dist, rad2);
-            }
-            return true;
-        });
-    if (!ok) flag_status(kErrTraversalStack);
+    points_near_segment(p.med_map, q.o, q.d, q.dmin, q.dmax, p.radius_pb2d, p.radius_pb2d_2,
+                        [&](unsigned slot, float dist, float rad2) {
+                            LightVertex lv;
+                            load_vertex(p.vertices + slot, lv);
+                            acc += eval_pb2d(q, cw, lv, dist, rad2);
+                        });
     return acc;
 }
 
@@ -437,24 +420,12 @@ UPBP_D float3 query_bb1d(const QuerySeg& q, const StateWeights& cw)
 {
     const DeviceParams& p = c_params;
     float3 acc = v3(0.f);
-    const float3 inv = safe_inv(q.d);
-    const float pad = p.rad_beam * 1.0001f + 1e-7f;
-    const bool need_mask = p.do_bp2d != 0;
-    const bool ok = bvh_walk(
-        p.beam_map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, q.o, inv, q.dmin, q.dmax); },
-        [&](int i) {
-            const float4 s0 = __ldg(&p.beam_map.seg[2 * i]), s1 = __ldg(&p.beam_map.seg[2 * i + 1]);
-            const unsigned bits = fbits(s1.w);
-            if (need_mask && !(bits >> 31)) return true;
-            float bb, st, t1, t2;
-            if (pred_beam_beam(q.o, q.d, q.dmin, q.dmax, xyz(s0), xyz(s1), s0.w, p.radius_bb1d_2, bb, st, t1, t2)) {
-                Beam lb;
-                load_beam(p.beams + (bits & 0x7fffffffu), lb);
-                if (lb.med == q.med) acc += eval_bb1d(q, cw, lb, bb, st, t1, t2);
-            }
-            return true;
-        });
-    if (!ok) flag_status(kErrTraversalStack);
+    beams_near_segment(p.beam_map, q.o, q.d, q.dmin, q.dmax, p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0,
+                       [&](unsigned b, float bb, float st, float t1, float t2) {
+                           Beam lb;
+                           load_beam(p.beams + b, lb);
+                           if (lb.med == q.med) acc += eval_bb1d(q, cw, lb, bb, st, t1, t2);
+                       });
     return acc;
 }
 
@@ -462,20 +433,11 @@ UPBP_D float3 query_bp2d(float3 x, const PathState& s, const Bsdf& cb)
 {
     const DeviceParams& p = c_params;
     float3 acc = v3(0.f);
-    const float pad = p.rad_beam * 1.0001f + 1e-7f;
-    const bool ok = bvh_walk(
-        p.beam_map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
-        [&](int i) {
-            const float4 s0 = __ldg(&p.beam_map.seg[2 * i]), s1 = __ldg(&p.beam_map.seg[2 * i + 1]);
-            float dist, rad2;
-            if (pred_ray_disc(xyz(s0), xyz(s1), 0.f, s0.w, x, p.radius_bp2d_2, dist, rad2)) {
-                Beam lb;
-                load_beam(p.beams + (fbits(s1.w) & 0x7fffffffu), lb);
-                acc += eval_bp2d(lb, s, cb, dist, rad2);
-            }
-            return true;
-        });
-    if (!ok) flag_status(kErrTraversalStack);
+    beams_near_point(p.beam_map, x, p.rad_beam, p.radius_bp2d_2, [&](unsigned b, float dist, float rad2) {
+        Beam lb;
+        load_beam(p.beams + b, lb);
+        acc += eval_bp2d(lb, s, cb, dist, rad2);
+    });
     return acc;
 }
 
@@ -640,6 +602,7 @@ __global__ void __launch_bounds__(128) camera_pass_kernel()
             const unsigned nv = p.path_vertex_count[lp];
             const LightVertexRec* base = p.vertices + (size_t)lp * p.slots_per_path;
             bool err = false;
+            count_work(kCtrVertexLoads, nv);
             for (unsigned k = 0; k < nv; k++) {
                 LightVertex lv;
                 load_vertex(base + k, lv);

@@ -17,6 +17,8 @@
 
 using namespace upbp;
 
+constexpr int kEventRing = 64;
+
 namespace {
 
 #define UPBP_CK(call)                                                                              \
@@ -50,6 +52,42 @@ __global__ void k_accumulate(const float* fb, double* acc, unsigned n)
     if (i < n) acc[i] += (double)fb[i];
 }
 
+// Neighbour sets of n queries through the estimators' range-query walkers.
+// Query record: x y z dx dy dz tmin tmax (points use x y z only).
+__global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* counts, unsigned* ids, unsigned cap)
+{
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DeviceParams& p = c_params;
+    const float* r = q + 8 * (size_t)i;
+    const float3 x = make_float3(r[0], r[1], r[2]), d = make_float3(r[3], r[4], r[5]);
+    unsigned k = 0;
+    auto rec = [&](unsigned id) {
+        if (k < cap) ids[(size_t)i * cap + k] = id;
+        k++;
+    };
+    switch (kind) {
+    case 0:
+        points_in_radius(p.surf_map, x, p.radius_surf, p.radius_surf_2, [&](unsigned s) { rec(s); });
+        break;
+    case 1:
+        points_in_radius(p.med_map, x, p.radius_pp3d, p.radius_pp3d_2, [&](unsigned s) { rec(s); });
+        break;
+    case 2:
+        points_near_segment(p.med_map, x, d, r[6], r[7], p.radius_pb2d, p.radius_pb2d_2,
+                            [&](unsigned s, float, float) { rec(s); });
+        break;
+    case 3:
+        beams_near_segment(p.beam_map, x, d, r[6], r[7], p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0,
+                           [&](unsigned b, float, float, float, float) { rec(b); });
+        break;
+    default:
+        beams_near_point(p.beam_map, x, p.rad_beam, p.radius_bp2d_2, [&](unsigned b, float, float) { rec(b); });
+        break;
+    }
+    counts[i] = k;
+}
+
 struct Geometry {
     BvhNode* nodes = nullptr;
     float4* tri = nullptr;
@@ -64,7 +102,8 @@ struct upbp_ctx {
     upbp_config cfg{};
     DeviceParams P{};
     cudaStream_t st = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_ring[kEventRing][4] = {};   // per-iteration events: start, light done, maps done, camera done
+    unsigned ev_pending = 0;                   // iterations recorded since the last stats read
     DMaterial* d_mat = nullptr;
     DMedium* d_med = nullptr;
     DLight* d_lights = nullptr;
@@ -80,13 +119,20 @@ struct upbp_ctx {
     unsigned* d_status = nullptr;
     BvhNode *d_surf_nodes = nullptr, *d_med_nodes = nullptr, *d_beam_nodes = nullptr;
     float4 *d_surf_pos = nullptr, *d_med_pos = nullptr, *d_beam_seg = nullptr;
+    unsigned *d_chunk_counts = nullptr, *d_chunk_offsets = nullptr;
+    uint2* d_chunks = nullptr;
+    unsigned chunk_capacity = 0;
+    void* d_scan_temp = nullptr;
+    size_t scan_temp_bytes = 0;
+    unsigned last_chunks = 0;
+    unsigned long long* d_work = nullptr;   // 2 x kCtrCount: light pass, camera pass
+    unsigned launches = 0;
     BuildScratch sc;
     float r0[5] = {0, 0, 0, 0, 0};  // bb1d bp2d pb2d pp3d surf
     float bb1d_used = 0.f;
     unsigned vertex_capacity = 0, beam_capacity = 0;
     unsigned h_counters[4] = {0, 0, 0, 0};
     unsigned iterations = 0;
-    bool timed = false;
     uint64_t triangles = 0;
 };
 
@@ -221,6 +267,28 @@ void free_scratch(BuildScratch& sc)
 
 float relative_radius(float r, float scene_radius) { return r < 0.f ? -r * scene_radius : r; }
 
+// Grows the chunked beam-map buffers (and the build scratch) to n chunks.
+int ensure_chunks(upbp_ctx* c, unsigned n)
+{
+    if (n <= c->chunk_capacity && n <= c->sc.capacity) return UPBP_OK;
+    const unsigned cap = std::max(n + n / 4, 1024u);
+    if (cap > c->chunk_capacity) {
+        cudaFree(c->d_chunks);
+        cudaFree(c->d_beam_nodes);
+        cudaFree(c->d_beam_seg);
+        UPBP_CK(dalloc(&c->d_chunks, cap));
+        UPBP_CK(dalloc(&c->d_beam_nodes, cap));
+        UPBP_CK(dalloc(&c->d_beam_seg, 3 * (size_t)cap));
+        c->chunk_capacity = cap;
+    }
+    if (cap > c->sc.capacity) {
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        free_scratch(c->sc);
+        if (alloc_scratch(c->sc, cap) != UPBP_OK) return UPBP_ERR_CUDA;
+    }
+    return UPBP_OK;
+}
+
 }  // namespace
 
 extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upbp_ctx** out)
@@ -245,7 +313,8 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     c->cfg = *cfg;
     DeviceParams& P = c->P;
     UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
-    for (auto& e : c->ev) UPBP_CK(cudaEventCreate(&e));
+    for (auto& slot : c->ev_ring)
+        for (auto& e : slot) UPBP_CK(cudaEventCreate(&e));
 
     // scene records
     std::vector<DMaterial> mats(s->material_count);
@@ -383,12 +452,24 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     UPBP_CK(dalloc(&c->d_fb, npx));
     UPBP_CK(dalloc(&c->d_acc, npx));
     UPBP_CK(dalloc(&c->d_status, 1));
+    UPBP_CK(dalloc(&c->d_work, 2 * kCtrCount));
     UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_beam_nodes, c->beam_capacity));
     UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_med_pos, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_beam_seg, 2 * (size_t)c->beam_capacity));
+    UPBP_CK(dalloc(&c->d_chunk_counts, c->beam_capacity));
+    UPBP_CK(dalloc(&c->d_chunk_offsets, c->beam_capacity));
+    {
+        size_t bytes = 0;
+        UPBP_CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->d_chunk_counts, c->d_chunk_offsets,
+                                              (int)std::max(1u, c->beam_capacity)));
+        c->scan_temp_bytes = bytes;
+        UPBP_CK(cudaMalloc(&c->d_scan_temp, std::max<size_t>(bytes, 16)));
+    }
+    if (ensure_chunks(c, std::max(1u, c->beam_capacity) * 4) != UPBP_OK) {
+        upbp_destroy(c);
+        return UPBP_ERR_CUDA;
+    }
     UPBP_CK(cudaMemsetAsync(c->d_acc, 0, npx * sizeof(double), c->st));
     UPBP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->st));
     UPBP_CK(cudaMemsetAsync(c->d_path_count, 0, sizeof(unsigned) * std::max(1u, L), c->st));
@@ -412,8 +493,12 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     const upbp_config& cfg = c->cfg;
     const unsigned L = P.light_subpath_count;
     const size_t npx = (size_t)P.screen_pixel_count * 3;
-    UPBP_CK(cudaEventRecord(c->ev[0], c->st));
+    cudaEvent_t* ev = c->ev_ring[c->iterations % kEventRing];
+    UPBP_CK(cudaEventRecord(ev[0], c->st));
     UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
+    UPBP_CK(cudaMemsetAsync(c->d_work, 0, 2 * kCtrCount * sizeof(unsigned long long), c->st));
+    unsigned launches = 0;
+    P.work = c->d_work;
     unsigned found[4] = {0, 0, 0, 0};
     if (P.trace_light_paths) {
         // radius schedule and MIS factors (renderer.cpp:57-119)
@@ -453,7 +538,10 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         P.iteration = (unsigned)iteration;
         UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned), c->st));
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-        if (L > 0) light_pass_kernel<<<(L + 127) / 128, 128, 0, c->st>>>();
+        if (L > 0) {
+            light_pass_kernel<<<(L + 127) / 128, 128, 0, c->st>>>();
+            launches++;
+        }
         UPBP_CK(cudaGetLastError());
         UPBP_CK(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaStreamSynchronize(c->st));
@@ -465,7 +553,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     } else {
         P.iteration = (unsigned)iteration;
     }
-    UPBP_CK(cudaEventRecord(c->ev[1], c->st));
+    UPBP_CK(cudaEventRecord(ev[1], c->st));
 
     // photon maps (renderer.cpp:206-307 builds OptiX structures here)
     const unsigned ns = std::min(found[1], c->vertex_capacity);
@@ -482,6 +570,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         const unsigned* order = nullptr;
         UPBP_CK(build_lbvh(src, ns, c->d_surf_nodes, c->sc, c->st, &order));
         k_gather_points<<<(ns + 255) / 256, 256, 0, c->st>>>(c->d_idx_s, c->d_vertices, order, ns, c->d_surf_pos);
+        launches += (ns > 1 ? 4 : 2) + 1;
         P.surf_map.bvh.count = ns;
     }
     if ((P.build_pb2d || P.build_pp3d) && nm > 0) {
@@ -492,34 +581,55 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         const unsigned* order = nullptr;
         UPBP_CK(build_lbvh(src, nm, c->d_med_nodes, c->sc, c->st, &order));
         k_gather_points<<<(nm + 255) / 256, 256, 0, c->st>>>(c->d_idx_m, c->d_vertices, order, nm, c->d_med_pos);
+        launches += (nm > 1 ? 4 : 2) + 1;
         P.med_map.bvh.count = nm;
     }
     if ((P.build_bb1d || P.build_bp2d) && nb > 0) {
+        // split beams into chunks of about 6 beam radii, at most 64 per beam
+        const float chunk_len = 6.f * P.rad_beam;
+        k_chunk_counts<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_beams, nb, chunk_len, 64u, c->d_chunk_counts);
+        size_t tb = c->scan_temp_bytes;
+        UPBP_CK(cub::DeviceScan::ExclusiveSum(c->d_scan_temp, tb, c->d_chunk_counts, c->d_chunk_offsets, (int)nb, c->st));
+        unsigned tail[2] = {0, 0};
+        UPBP_CK(cudaMemcpyAsync(&tail[0], c->d_chunk_offsets + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaMemcpyAsync(&tail[1], c->d_chunk_counts + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        const unsigned nchunks = tail[0] + tail[1];
+        if (ensure_chunks(c, nchunks) != UPBP_OK) return UPBP_ERR_CUDA;
+        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg};
+        k_chunk_expand<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_chunk_counts, c->d_chunk_offsets, nb, c->d_chunks);
         BoxSource src{};
-        src.kind = 2;
+        src.kind = 3;
         src.beams = c->d_beams;
+        src.chunks = c->d_chunks;
         const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, nb, c->d_beam_nodes, c->sc, c->st, &order));
-        k_gather_beams<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_beams, order, nb, P.bb1d_used_light_subpath_count,
-                                                            c->d_beam_seg);
-        P.beam_map.bvh.count = nb;
+        UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
+        k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
+                                                                  P.bb1d_used_light_subpath_count, c->d_beam_seg);
+        P.beam_map.bvh.count = nchunks;
+        c->last_chunks = nchunks;
+        launches += 2 + (nchunks > 1 ? 4 : 2) + 1;
     }
     UPBP_CK(cudaGetLastError());
     P.n_surface = found[1];
     P.n_medium = found[2];
     P.n_beams = found[3];
-    UPBP_CK(cudaEventRecord(c->ev[2], c->st));
 
+    P.work = c->d_work + kCtrCount;
+    UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+    UPBP_CK(cudaEventRecord(ev[2], c->st));
     if (P.trace_camera_paths) {
-        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
         camera_pass_kernel<<<(P.screen_pixel_count + 127) / 128, 128, 0, c->st>>>();
+        launches++;
         UPBP_CK(cudaGetLastError());
     }
+    UPBP_CK(cudaEventRecord(ev[3], c->st));
     k_accumulate<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_acc, (unsigned)npx);
+    launches++;
+    c->launches = launches;
     UPBP_CK(cudaGetLastError());
-    UPBP_CK(cudaEventRecord(c->ev[3], c->st));
     c->iterations++;
-    c->timed = true;
+    c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
     return UPBP_OK;
 }
 
@@ -560,17 +670,102 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     o->iterations_done = c->iterations;
     o->triangle_count = c->triangles;
     o->scene_radius = c->P.scene_radius;
-    if (c->timed) {
+    unsigned long long work[2 * kCtrCount];
+    UPBP_CK(cudaMemcpy(work, c->d_work, sizeof(work), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < kCtrCount && i < 8; i++) {
+        o->work_light[i] = work[i];
+        o->work_camera[i] = work[kCtrCount + i];
+    }
+    o->beam_chunks = c->last_chunks;
+    o->radius[0] = c->P.radius_bb1d;
+    o->radius[1] = c->P.radius_bp2d;
+    o->radius[2] = c->P.radius_pb2d;
+    o->radius[3] = c->P.radius_pp3d;
+    o->radius[4] = c->P.radius_surf;
+    o->radius[5] = c->P.rad_beam;
+    o->h2d_bytes = c->P.trace_light_paths ? 2 * sizeof(DeviceParams) : sizeof(DeviceParams);
+    o->d2h_bytes = c->P.trace_light_paths ? 4 * sizeof(unsigned) + (c->last_chunks ? 2 * sizeof(unsigned) : 0) : 0;
+    o->kernel_launches = c->launches;
+    // per-pass times: the last iteration, and sums over the iterations run
+    // since the previous stats call (up to the event ring size)
+    for (unsigned k = 0; k < c->ev_pending; k++) {
+        cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
         float a = 0.f, b = 0.f, d = 0.f;
-        UPBP_CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
-        UPBP_CK(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
-        UPBP_CK(cudaEventElapsedTime(&d, c->ev[2], c->ev[3]));
-        o->ms_light = a;
-        o->ms_build = b;
-        o->ms_camera = d;
+        UPBP_CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+        UPBP_CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+        UPBP_CK(cudaEventElapsedTime(&d, ev[2], ev[3]));
+        if (k == 0) {
+            o->ms_light = a;
+            o->ms_build = b;
+            o->ms_camera = d;
+        }
+        o->ms_light_sum += a;
+        o->ms_build_sum += b;
+        o->ms_camera_sum += d;
+        o->timed_iterations++;
+    }
+    c->ev_pending = 0;
+    return UPBP_OK;
+}
+
+extern "C" int upbp_debug_photons(upbp_ctx* c, int kind, float* out, uint32_t capacity, uint32_t* count)
+{
+    if (!c || !count || kind < 0 || kind > 2) return UPBP_ERR_ARGS;
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    if (kind < 2) {
+        const PointMap& m = kind == 0 ? c->P.surf_map : c->P.med_map;
+        *count = m.bvh.count;
+        const unsigned n = std::min(m.bvh.count, capacity);
+        if (out && n) UPBP_CK(cudaMemcpy(out, m.pos, n * sizeof(float4), cudaMemcpyDeviceToHost));
+        return UPBP_OK;
+    }
+    const unsigned nb = std::min(c->h_counters[3], c->beam_capacity);
+    *count = (c->P.build_bb1d || c->P.build_bp2d) ? nb : 0;
+    const unsigned n = std::min(*count, capacity);
+    if (out && n) {
+        std::vector<BeamRec> tmp(n);
+        UPBP_CK(cudaMemcpy(tmp.data(), c->d_beams, n * sizeof(BeamRec), cudaMemcpyDeviceToHost));
+        for (unsigned i = 0; i < n; i++) {
+            const float4 q0 = tmp[i].q[0], q1 = tmp[i].q[1], q3 = tmp[i].q[3];
+            float* o = out + 8 * (size_t)i;
+            o[0] = q0.x;
+            o[1] = q0.y;
+            o[2] = q0.z;
+            o[3] = q0.w;
+            o[4] = q1.x;
+            o[5] = q1.y;
+            o[6] = q1.z;
+            std::memcpy(&o[7], &q3.z, 4);  // path index bits
+        }
     }
     return UPBP_OK;
 }
+
+extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uint32_t n, uint32_t* counts,
+                                uint32_t* ids, uint32_t ids_per_query)
+{
+    if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
+    if (n == 0) return UPBP_OK;
+    float* dq = nullptr;
+    unsigned *dc = nullptr, *di = nullptr;
+    UPBP_CK(dalloc(&dq, 8 * (size_t)n));
+    UPBP_CK(dalloc(&dc, n));
+    UPBP_CK(dalloc(&di, (size_t)n * std::max(1u, ids_per_query)));
+    UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
+    k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
+    UPBP_CK(cudaGetLastError());
+    UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    if (ids && ids_per_query)
+        UPBP_CK(cudaMemcpyAsync(ids, di, (size_t)n * ids_per_query * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    cudaFree(dq);
+    cudaFree(dc);
+    cudaFree(di);
+    return UPBP_OK;
+}
+
+extern "C" void* upbp_get_stream(upbp_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 extern "C" void upbp_destroy(upbp_ctx* c)
 {
@@ -579,12 +774,14 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
-                    c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg};
+                    c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
+                    c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work};
     for (void* b : bufs)
         if (b) cudaFree(b);
     free_scratch(c->sc);
-    for (auto& e : c->ev)
-        if (e) cudaEventDestroy(e);
+    for (auto& slot : c->ev_ring)
+        for (auto& e : slot)
+            if (e) cudaEventDestroy(e);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }

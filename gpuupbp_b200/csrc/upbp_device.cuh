@@ -21,6 +21,15 @@ enum : unsigned {
     kErrIntersectionStack = 1u << 3, kErrBeamCapacity = 1u << 4, kErrTraversalStack = 1u << 5
 };
 
+// Work counters per pass (warp-aggregated 64-bit atomics), the numerator of
+// the algorithmic-bytes roofline: BVH node visits, triangle tests, rays cast,
+// photon-point candidates / accepted merges, beam-chunk candidates / accepted
+// merges, light-vertex records read by BPT connections.
+enum : int {
+    kCtrNodes = 0, kCtrTris, kCtrRays, kCtrPointCand, kCtrPointHit, kCtrBeamCand, kCtrBeamHit, kCtrVertexLoads,
+    kCtrCount
+};
+
 struct DMaterial {
     float3 diffuse;
     float3 phong;
@@ -116,8 +125,9 @@ struct PointMap {
     const float4* pos;
 };
 
-// Beam map: BVH over beam segments in leaf order.
-//   seg[2i] = (origin.xyz, length), seg[2i+1] = (direction.xyz, beam index bits)
+// Beam map: BVH over beam chunks (sub-segments of each beam) in leaf order.
+//   seg[3i] = (origin.xyz, length), seg[3i+1] = (direction.xyz, beam index bits),
+//   seg[3i+2] = (t0, t1) of the beam chunk this leaf covers
 struct BeamMap {
     BvhView bvh;
     const float4* seg;
@@ -172,11 +182,17 @@ struct DeviceParams {
     unsigned beam_capacity;
     float* framebuffer;               // W*H*3
     unsigned* status;
+    unsigned long long* work;         // kCtrCount counters of the running pass
 
     // photon maps built after the light pass
     PointMap surf_map, med_map;
     BeamMap beam_map;
     unsigned n_surface, n_medium, n_beams;   // host-side copies of the light-pass counters
 };
+
+// Launch parameters of the running pass, uploaded before each launch.
+__constant__ DeviceParams c_params;
+
+UPBP_D unsigned long long* c_work_ptr() { return c_params.work; }
 
 }  // namespace upbp

@@ -1,0 +1,120 @@
+// Range queries over the per-iteration photon maps.  Each walker visits the
+// BVH leaves whose box, dilated by the query radius, the query touches, and
+// calls f for every photon or beam that passes the estimator's exact
+// predicate; the neighbour set is therefore defined by the predicate alone
+// (the reference's OptiX intersection programs apply the same predicates,
+// gpuupbp/kernel/pde/program_*.cu).  The estimators and the diagnostic
+// neighbour-set query both use these walkers.
+#pragma once
+
+#include "upbp_paths.cuh"
+
+namespace upbp {
+
+// Photons within radius r of x (SURF, PP3D): f(vertex slot).
+template <class F>
+UPBP_D void points_in_radius(const PointMap& map, float3 x, float r, float r2, F&& f)
+{
+    const float pad = r * 1.0001f + 1e-7f;
+    unsigned cand = 0, hits = 0;
+    const bool ok = bvh_walk(
+        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
+        [&](int i) {
+            const float4 pp = __ldg(&map.pos[i]);
+            cand++;
+            if (pred_point_point(x, xyz(pp), r2)) {
+                hits++;
+                f(fbits(pp.w));
+            }
+            return true;
+        });
+    count_work(kCtrPointCand, cand);
+    count_work(kCtrPointHit, hits);
+    if (!ok) flag_status(kErrTraversalStack);
+}
+
+// Photons whose disc of radius r the query segment (o, d, (tmin, tmax))
+// crosses (PB2D): f(vertex slot, distance along the query, squared radius).
+template <class F>
+UPBP_D void points_near_segment(const PointMap& map, float3 o, float3 d, float tmin, float tmax, float r, float r2,
+                                F&& f)
+{
+    const float3 inv = safe_inv(d);
+    const float pad = r * 1.0001f + 1e-7f;
+    unsigned cand = 0, hits = 0;
+    const bool ok = bvh_walk(
+        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
+        [&](int i) {
+            const float4 pp = __ldg(&map.pos[i]);
+            float dist, rad2;
+            cand++;
+            if (pred_ray_disc(o, d, tmin, tmax, xyz(pp), r2, dist, rad2)) {
+                hits++;
+                f(fbits(pp.w), dist, rad2);
+            }
+            return true;
+        });
+    count_work(kCtrPointCand, cand);
+    count_work(kCtrPointHit, hits);
+    if (!ok) flag_status(kErrTraversalStack);
+}
+
+// Photon beams passing within sqrt(r2) of the query segment (BB1D); with
+// need_mask only beams of the first bb1d_used_light_subpath_count light
+// paths.  f(beam index, distance, sin theta, t along query, t along beam).
+// Beams are stored as chunks; a beam is reported only through the chunk that
+// holds its closest point, so each beam appears at most once.
+template <class F>
+UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmin, float tmax, float pad_r, float r2,
+                               bool need_mask, F&& f)
+{
+    const float3 inv = safe_inv(d);
+    const float pad = pad_r * 1.0001f + 1e-7f;
+    unsigned cand = 0, hits = 0;
+    const bool ok = bvh_walk(
+        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
+        [&](int i) {
+            const float4 s1 = __ldg(&map.seg[3 * i + 1]);
+            const unsigned bits = fbits(s1.w);
+            if (need_mask && !(bits >> 31)) return true;
+            const float4 s0 = __ldg(&map.seg[3 * i]), s2 = __ldg(&map.seg[3 * i + 2]);
+            float bb, st, t1, t2;
+            cand++;
+            if (pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, bb, st, t1, t2) && t2 >= s2.x &&
+                t2 < s2.y) {
+                hits++;
+                f(bits & 0x7fffffffu, bb, st, t1, t2);
+            }
+            return true;
+        });
+    count_work(kCtrBeamCand, cand);
+    count_work(kCtrBeamHit, hits);
+    if (!ok) flag_status(kErrTraversalStack);
+}
+
+// Photon beams whose disc of radius sqrt(r2) contains x (BP2D):
+// f(beam index, distance along the beam, squared radius).
+template <class F>
+UPBP_D void beams_near_point(const BeamMap& map, float3 x, float pad_r, float r2, F&& f)
+{
+    const float pad = pad_r * 1.0001f + 1e-7f;
+    unsigned cand = 0, hits = 0;
+    const bool ok = bvh_walk(
+        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
+        [&](int i) {
+            const float4 s0 = __ldg(&map.seg[3 * i]), s1 = __ldg(&map.seg[3 * i + 1]);
+            const float4 s2 = __ldg(&map.seg[3 * i + 2]);
+            float dist, rad2;
+            cand++;
+            if (pred_ray_disc(xyz(s0), xyz(s1), 0.f, s0.w, x, r2, dist, rad2) && dist >= s2.x && dist < s2.y) {
+                hits++;
+                f(fbits(s1.w) & 0x7fffffffu, dist, rad2);
+            }
+            return true;
+        });
+    count_work(kCtrBeamCand, cand);
+    count_work(kCtrBeamHit, hits);
+    if (!ok) flag_status(kErrTraversalStack);
+}
+
+}  // namespace upbp

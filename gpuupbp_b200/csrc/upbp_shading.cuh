@@ -13,8 +13,6 @@
 
 namespace upbp {
 
-__constant__ DeviceParams c_params;
-
 // ---------------------------------------------------------------- warps
 
 UPBP_D float3 sample_cos_hemisphere(float u0, float u1, float* pdf)

@@ -152,18 +152,18 @@ class SceneBuilder:
             fo.write(f"mtllib {mtl_name}\n")
             voff, noff = 1, 1
             for mat, v, f, n in self.groups:
-                fo.write("".join("v %.7f %.7f %.7f\n" % tuple(p) for p in v))
+                np.savetxt(fo, v, fmt="v %.7f %.7f %.7f")
                 if n is not None:
-                    fo.write("".join("vn %.7f %.7f %.7f\n" % tuple(p) for p in n))
+                    np.savetxt(fo, n, fmt="vn %.7f %.7f %.7f")
                 fo.write(f"usemtl {mat}\n")
                 fv = f + voff
                 if n is not None:
                     fn = f + noff
-                    fo.write("".join("f %d//%d %d//%d %d//%d\n" % (a, na, b, nb, c, nc)
-                                     for (a, b, c), (na, nb, nc) in zip(fv, fn)))
+                    inter = np.stack([fv[:, 0], fn[:, 0], fv[:, 1], fn[:, 1], fv[:, 2], fn[:, 2]], 1)
+                    np.savetxt(fo, inter, fmt="f %d//%d %d//%d %d//%d")
                     noff += len(n)
                 else:
-                    fo.write("".join("f %d %d %d\n" % tuple(t) for t in fv))
+                    np.savetxt(fo, fv, fmt="f %d %d %d")
                 voff += len(v)
         with open(obj_path + ".aux", "w") as fa:
             c = self.camera
@@ -304,7 +304,7 @@ def dense_beams(seed: int = 5, tiny: bool = False) -> SceneBuilder:
         w = np.cross(nrm, u)
         p = nrm[None] + (qv[:, 0:1] * 2 - 1) * u[None] + (qv[:, 1:2] * 2 - 1) * w[None]
         bump = 0.03 * np.sin(7.0 * p[:, 0] + rng.uniform(0, 6)) * np.sin(5.0 * p[:, 2] + rng.uniform(0, 6))
-        p = p * (1.0 + bump[:, None] * 0.0) - nrm[None] * bump[:, None]
+        p = p - nrm[None] * bump[:, None]
         f = qf.copy()
         e = np.cross(p[f[0, 1]] - p[f[0, 0]], p[f[0, 2]] - p[f[0, 0]])
         if np.dot(e, -nrm) < 0:

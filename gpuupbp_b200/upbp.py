@@ -1,0 +1,212 @@
+"""Python mirror of the renderer interface over the C ABI (include/upbp.h).
+
+`Renderer` follows the reference's flow (gpuupbp/gpuupbp.cpp:57-148):
+parse_commandline -> SceneLoader::load_scene -> Renderer::init ->
+run_iteration per iteration -> scale and save.  All work runs in
+libupbp_b200.so on the GPU; there is no CPU path here, and the module raises
+if the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libupbp_b200.so")
+
+UPBP_OK, UPBP_HELP = 0, 1
+ERRORS = {-1: "invalid arguments", -2: "I/O error", -3: "CUDA error", -4: "no CUDA device", -5: "invalid scene"}
+STATUS_BITS = {1: "boundary stack", 2: "intersection array", 4: "volume segment array", 8: "intersection stack",
+               16: "beam capacity", 32: "traversal stack"}
+
+
+class UpbpError(RuntimeError):
+    pass
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("scene_id", ctypes.c_int), ("scene_path", ctypes.c_char * 1024), ("algorithm_flags", ctypes.c_uint32),
+        ("iteration_count", ctypes.c_int), ("max_time", ctypes.c_float), ("output_name", ctypes.c_char * 1024),
+        ("res_x", ctypes.c_uint32), ("res_y", ctypes.c_uint32), ("max_path_length", ctypes.c_uint32),
+        ("min_path_length", ctypes.c_uint32), ("path_count_per_iter", ctypes.c_float),
+        ("query_beam_type", ctypes.c_int), ("photon_beam_type", ctypes.c_int),
+        ("bb1d_radius_initial", ctypes.c_float), ("bb1d_radius_alpha", ctypes.c_float),
+        ("bb1d_used_light_subpath_count", ctypes.c_float),
+        ("bp2d_radius_initial", ctypes.c_float), ("bp2d_radius_alpha", ctypes.c_float),
+        ("pb2d_radius_initial", ctypes.c_float), ("pb2d_radius_alpha", ctypes.c_float),
+        ("pp3d_radius_initial", ctypes.c_float), ("pp3d_radius_alpha", ctypes.c_float),
+        ("surf_radius_initial", ctypes.c_float), ("surf_radius_alpha", ctypes.c_float),
+        ("continuous_output", ctypes.c_int), ("ignore_fully_spec_paths", ctypes.c_int), ("gpu_assert", ctypes.c_int),
+        ("iteration_offset", ctypes.c_uint64), ("do_log", ctypes.c_int), ("use_shading_normal", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("light_vertices", ctypes.c_uint32), ("surface_vertices", ctypes.c_uint32),
+        ("medium_vertices", ctypes.c_uint32), ("light_beams", ctypes.c_uint32),
+        ("light_paths", ctypes.c_uint32), ("camera_paths", ctypes.c_uint32), ("status", ctypes.c_uint32),
+        ("iterations_done", ctypes.c_uint32), ("ms_light", ctypes.c_double), ("ms_build", ctypes.c_double),
+        ("ms_camera", ctypes.c_double), ("triangle_count", ctypes.c_uint64), ("scene_radius", ctypes.c_double),
+        ("work_light", ctypes.c_uint64 * 8), ("work_camera", ctypes.c_uint64 * 8), ("beam_chunks", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32), ("h2d_bytes", ctypes.c_uint32), ("d2h_bytes", ctypes.c_uint32),
+        ("ms_light_sum", ctypes.c_double), ("ms_build_sum", ctypes.c_double), ("ms_camera_sum", ctypes.c_double),
+        ("timed_iterations", ctypes.c_uint32), ("radius", ctypes.c_float * 6),
+    ]
+
+
+WORK_NAMES = ["nodes", "tris", "rays", "point_cand", "point_hit", "beam_cand", "beam_hit", "vertex_loads"]
+
+
+# symbols declared in include/upbp.h
+EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_predefined", "upbp_scene_get_desc",
+           "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
+           "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
+           "upbp_debug_photons", "upbp_debug_query"]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libupbp_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise UpbpError(f"{path} is missing: run gpuupbp_b200/build.py")
+    L = ctypes.CDLL(path)
+    P, VP = ctypes.POINTER, ctypes.c_void_p
+    L.upbp_parse_command_line.argtypes = [ctypes.c_int, P(ctypes.c_char_p), P(Config)]
+    L.upbp_scene_load_obj.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, P(VP)]
+    L.upbp_scene_load_predefined.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, P(VP)]
+    L.upbp_scene_get_desc.argtypes = [VP]
+    L.upbp_scene_get_desc.restype = VP
+    L.upbp_scene_free.argtypes = [VP]
+    L.upbp_create.argtypes = [VP, P(Config), P(VP)]
+    L.upbp_run_iteration.argtypes = [VP, ctypes.c_int]
+    L.upbp_accumulate_to_host.argtypes = [VP, VP, ctypes.c_double]
+    L.upbp_read_iteration.argtypes = [VP, VP]
+    L.upbp_get_stats.argtypes = [VP, P(Stats)]
+    L.upbp_destroy.argtypes = [VP]
+    L.upbp_write_exr.argtypes = [ctypes.c_char_p, VP, ctypes.c_uint32, ctypes.c_uint32]
+    L.upbp_get_stream.argtypes = [VP]
+    L.upbp_get_stream.restype = VP
+    L.upbp_last_error.restype = ctypes.c_char_p
+    L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]
+    L.upbp_debug_query.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str):
+    if rc != UPBP_OK:
+        msg = load_library().upbp_last_error().decode(errors="replace")
+        raise UpbpError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
+
+
+def parse_command_line(args: list[str]) -> Config:
+    """The reference's parse_commandline (same flags, defaults and errors)."""
+    L = load_library()
+    argv = ["upbp"] + list(args)
+    arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
+    cfg = Config()
+    rc = L.upbp_parse_command_line(len(argv), arr, ctypes.byref(cfg))
+    if rc == UPBP_HELP:
+        raise UpbpError("help requested")
+    _check(rc, "command line")
+    return cfg
+
+
+class Renderer:
+    """Drop-in for the reference's Renderer on a scene file + command line."""
+
+    def __init__(self, args: list[str]):
+        L = load_library()
+        self.config = parse_command_line(args)
+        c = self.config
+        self._scene = ctypes.c_void_p()
+        if c.scene_id < 0:
+            rc = L.upbp_scene_load_obj(c.scene_path, c.res_x, c.res_y, ctypes.byref(self._scene))
+        else:
+            rc = L.upbp_scene_load_predefined(c.scene_id, c.res_x, c.res_y, ctypes.byref(self._scene))
+        _check(rc, "scene")
+        self._ctx = ctypes.c_void_p()
+        _check(L.upbp_create(L.upbp_scene_get_desc(self._scene), ctypes.byref(c), ctypes.byref(self._ctx)), "init")
+        self.width, self.height = c.res_x, c.res_y
+        self.iterations = 0
+
+    def run_iteration(self, iteration: int):
+        _check(load_library().upbp_run_iteration(self._ctx, iteration), f"iteration {iteration}")
+        self.iterations += 1
+
+    def iteration_image(self) -> np.ndarray:
+        """The last iteration's image, (H, W, 3) float32."""
+        out = np.empty((self.height, self.width, 3), np.float32)
+        _check(load_library().upbp_read_iteration(self._ctx, out.ctypes.data), "read")
+        return out
+
+    def accumulated(self, scale: float | None = None) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 3), np.float32)
+        s = (1.0 / max(1, self.iterations)) if scale is None else scale
+        _check(load_library().upbp_accumulate_to_host(self._ctx, out.ctypes.data, s), "accumulate")
+        return out
+
+    def render(self, iterations: int, start: int = 0) -> np.ndarray:
+        for it in range(start, start + iterations):
+            self.run_iteration(it)
+        return self.accumulated()
+
+    def stats(self) -> dict:
+        st = Stats()
+        _check(load_library().upbp_get_stats(self._ctx, ctypes.byref(st)), "stats")
+        out = {k: getattr(st, k) for k, _ in Stats._fields_}
+        out["work_light"] = dict(zip(WORK_NAMES, list(st.work_light)))
+        out["work_camera"] = dict(zip(WORK_NAMES, list(st.work_camera)))
+        out["radius"] = list(st.radius)
+        return out
+
+    def photons(self, kind: int) -> np.ndarray:
+        """Photon map contents of the last iteration (see upbp_debug_photons)."""
+        L = load_library()
+        n = ctypes.c_uint32()
+        _check(L.upbp_debug_photons(self._ctx, kind, None, 0, ctypes.byref(n)), "photons")
+        width = 4 if kind < 2 else 8
+        out = np.zeros((n.value, width), np.float32)
+        if n.value:
+            _check(L.upbp_debug_photons(self._ctx, kind, out.ctypes.data, n.value, ctypes.byref(n)), "photons")
+        return out
+
+    def query(self, kind: int, queries: np.ndarray, cap: int = 4096):
+        """Neighbour sets of the estimators' range queries (upbp_debug_query)."""
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 8)
+        counts = np.zeros(len(q), np.uint32)
+        ids = np.zeros((len(q), cap), np.uint32)
+        _check(load_library().upbp_debug_query(self._ctx, kind, q.ctypes.data, len(q), counts.ctypes.data,
+                                               ids.ctypes.data, cap), "query")
+        return [ids[i, :min(int(c), cap)].copy() for i, c in enumerate(counts)], counts
+
+    def stream_handle(self) -> int:
+        return load_library().upbp_get_stream(self._ctx) or 0
+
+    def close(self):
+        L = load_library()
+        if getattr(self, "_ctx", None):
+            L.upbp_destroy(self._ctx)
+            self._ctx = None
+        if getattr(self, "_scene", None):
+            L.upbp_scene_free(self._scene)
+            self._scene = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_exr(path: str, rgb: np.ndarray):
+    a = np.ascontiguousarray(rgb, np.float32)
+    _check(load_library().upbp_write_exr(path.encode(), a.ctypes.data, a.shape[1], a.shape[0]), "exr")

@@ -156,9 +156,26 @@ typedef struct upbp_stats {
     uint32_t light_paths, camera_paths;
     uint32_t status;              /* OR of UPBP_STATUS_* seen so far */
     uint32_t iterations_done;
-    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events */
+    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events; ms_camera is the camera-pass kernel */
     uint64_t triangle_count;
     double scene_radius;
+    /* Work counters of the last iteration, light pass then camera pass, in
+     * the order: BVH node visits, triangle tests, rays cast, photon-point
+     * candidates, accepted point merges, beam-chunk candidates, accepted beam
+     * merges, light-vertex records read by BPT connections. */
+    uint64_t work_light[8];
+    uint64_t work_camera[8];
+    uint32_t beam_chunks;         /* leaves of the last beam map */
+    uint32_t kernel_launches;     /* this library's kernel launches in the last iteration */
+    uint32_t h2d_bytes;           /* host->device bytes of the last iteration (launch parameters) */
+    uint32_t d2h_bytes;           /* device->host bytes of the last iteration (counters) */
+    /* Pass times summed over the iterations run since the previous
+     * upbp_get_stats call (at most the last 64), and their count. */
+    double ms_light_sum, ms_build_sum, ms_camera_sum;
+    uint32_t timed_iterations;
+    /* Radii of the last iteration: bb1d, bp2d, pb2d, pp3d, surf, and the beam
+     * radius used for the beam map (max of bb1d and bp2d when enabled). */
+    float radius[6];
 } upbp_stats;
 
 /* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
@@ -191,6 +208,26 @@ void upbp_destroy(upbp_ctx* ctx);
  * (gpuupbp/host/framebuffer.cpp:114-127, misc/tinyexr_wrapper.cpp:34-95):
  * half-float B,G,R channels, uncompressed scanlines. */
 int upbp_write_exr(const char* path, const float* rgb, uint32_t width, uint32_t height);
+
+/* ---- diagnostics (no counterpart in the reference; used by the parity tests)
+ * upbp_debug_photons: the last iteration's photon map contents.  kind 0/1:
+ * surface/medium photons as 4 floats (x, y, z, vertex-slot bits) in map
+ * order; kind 2: beams as 8 floats (origin xyz, length, direction xyz,
+ * light-path index bits).  *count receives the total; at most `capacity`
+ * records are written.
+ * upbp_debug_query: neighbour sets through the estimators' own range
+ * queries for the last iteration's maps and radii.  Each query is 8 floats
+ * (x y z dx dy dz tmin tmax).  kind 0 SURF and 1 PP3D (points within the
+ * radius of x), 2 PB2D (medium photons along the segment), 3 BB1D (beams
+ * near the segment), 4 BP2D (beams near x).  counts[i] = set size, ids =
+ * up to ids_per_query vertex slots (0-2) or beam indices (3-4) per query. */
+int upbp_debug_photons(upbp_ctx* ctx, int kind, float* out, uint32_t capacity, uint32_t* count);
+int upbp_debug_query(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, uint32_t* counts, uint32_t* ids,
+                     uint32_t ids_per_query);
+
+/* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
+ * caller can order its own work or time the library with events. */
+void* upbp_get_stream(upbp_ctx* ctx);
 
 const char* upbp_last_error(void);
 

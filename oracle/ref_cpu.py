@@ -49,17 +49,31 @@ def lib():
         L.upbp_ref_output_name.restype = ctypes.c_char_p
         L.upbp_ref_iteration_count.argtypes = [ctypes.c_void_p]
         L.upbp_ref_iteration_count.restype = ctypes.c_int
+        L.upbp_ref_describe.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
+        L.upbp_ref_describe.restype = ctypes.c_int
         _lib = L
     return _lib
 
 
+_current = None
+
+
 class RefRenderer:
-    """The reference renderer on host cores, driven by its own command line."""
+    """The reference renderer on host cores, driven by its own command line.
+
+    The reference keeps its launch parameters in one global, so only one
+    instance can be alive; creating a new one closes the previous one.
+    """
 
     def __init__(self, args: list[str], threads: int = 0):
+        global _current
         L = lib()
+        if _current is not None:
+            _current.close()
+        _current = self
         argv = ["gpuupbp"] + list(args)
         arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
+        self._h = None
         h = ctypes.c_void_p()
         rc = L.upbp_ref_create(len(argv), arr, threads, ctypes.byref(h))
         if rc != 0:
@@ -88,6 +102,13 @@ class RefRenderer:
                 "pixels": u[5], "width": u[6], "height": u[7],
                 "t_light": t[0], "t_build": t[1], "t_camera": t[2]}
 
+    def describe(self) -> dict:
+        """The reference's parsed Config and loaded Scene, summarised."""
+        import json
+        buf = ctypes.create_string_buffer(8192)
+        lib().upbp_ref_describe(self._h, buf, len(buf))
+        return json.loads(buf.value.decode())
+
     @staticmethod
     def exception_counts() -> list[int]:
         a = (ctypes.c_ulonglong * 8)()
@@ -95,9 +116,12 @@ class RefRenderer:
         return list(a)
 
     def close(self):
-        if self._h:
+        global _current
+        if getattr(self, "_h", None):
             lib().upbp_ref_destroy(self._h)
             self._h = None
+        if _current is self:
+            _current = None
 
     def __del__(self):
         try:

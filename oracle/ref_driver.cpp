@@ -649,6 +649,36 @@ void upbp_ref_exception_counts(unsigned long long* out8)
 
 const char* upbp_ref_output_name(RefCtx* c) { return c->setup.output_name; }
 
+// JSON summary of the parsed configuration and the loaded scene, for the
+// command-line and loader parity tests.
+int upbp_ref_describe(RefCtx* c, char* buf, int cap)
+{
+    const OracleSetup& s = c->setup;
+    const Scene& sc = s.scene;
+    const Camera& cam = sc.camera;
+    return snprintf(
+        buf, (size_t)cap,
+        "{\"algorithm_flags\": %u, \"iteration_count\": %d, \"res\": [%u, %u], \"max_path_length\": %u, "
+        "\"min_path_length\": %u, \"path_count_per_iter\": %.9g, \"query_beam_type\": %d, "
+        "\"photon_beam_type\": %d, \"radius_initial\": [%.9g, %.9g, %.9g, %.9g, %.9g], "
+        "\"radius_alpha\": [%.9g, %.9g, %.9g, %.9g, %.9g], \"bb1d_used\": %.9g, \"ignore_spec\": %d, "
+        "\"ioff\": %llu, \"shading_normal\": %d, \"output_name\": \"%s\", "
+        "\"tri_real\": %u, \"tri_imag\": %u, \"lights\": %u, \"materials\": %u, \"media\": %u, "
+        "\"global_medium\": %u, \"background\": %d, \"records\": %u, "
+        "\"camera_origin\": [%.9g, %.9g, %.9g], \"camera_dir\": [%.9g, %.9g, %.9g], "
+        "\"image_plane_dist\": %.9g, \"scene_center\": [%.9g, %.9g, %.9g], \"scene_radius\": %.9g}",
+        s.algorithm_flags, s.iteration_count, s.res_x, s.res_y, s.max_path_length, s.min_path_length,
+        s.path_count_per_iter, s.query_beam_type, s.photon_beam_type, s.surf_radius_initial, s.pp3d_radius_initial,
+        s.pb2d_radius_initial, s.bb1d_radius_initial, s.bp2d_radius_initial, s.surf_radius_alpha, s.pp3d_radius_alpha,
+        s.pb2d_radius_alpha, s.bb1d_radius_alpha, s.bp2d_radius_alpha, s.bb1d_used_light_subpath_count,
+        (int)s.ignore_fully_spec_paths, (unsigned long long)s.iteration_offset, (int)s.use_shading_normal,
+        s.output_name, sc.triangles_real.count, sc.triangles_imag.count, sc.light_count, sc.mat_count,
+        sc.med_count, sc.global_medium_idx, sc.background_light_idx == UINT32_MAX ? -1 : (int)sc.background_light_idx,
+        s.record_count, cam.origin.x, cam.origin.y, cam.origin.z, cam.direction.x, cam.direction.y,
+        cam.direction.z, cam.image_plane_dist, sc.scene_sphere.center.x, sc.scene_sphere.center.y,
+        sc.scene_sphere.center.z, sc.scene_sphere.radius);
+}
+
 int upbp_ref_iteration_count(RefCtx* c) { return c->setup.iteration_count; }
 
 void upbp_ref_destroy(RefCtx* c)

@@ -1,0 +1,38 @@
+"""Parity cases: scene workload, command line and iteration count.
+
+Each case renders per-iteration images with the reference's own render loop
+compiled for the CPU (oracle/_ref) and with the B200 library on the same
+scene files, command line and random stream.  Scenes are generated into a
+temporary directory by gpuupbp_b200.scenes (deterministic for a seed).
+"""
+
+BOX_R = ["-r_initial", "-0.02", "-r_alpha", "0.75"]
+
+CASES = {
+    # name: (workload, tiny, args (without -s), iterations)
+    "box_tiny_all": ("box_medium", True, ["-a", "upbp_all", "-l", "8", "-r", "32x32"] + BOX_R, 2),
+    "box_bpt": ("box_medium", False, ["-a", "upbp_bpt", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_surf": ("box_medium", False, ["-a", "upbp_surf", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_pp3d": ("box_medium", False, ["-a", "upbp_pp3d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_pb2d": ("box_medium", False, ["-a", "upbp_pb2d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_bb1d": ("box_medium", False, ["-a", "upbp_bb1d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_bp2d": ("box_medium", False, ["-a", "upbp_bp2d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_all_bp2d": ("box_medium", False,
+                     ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "48x48"] + BOX_R, 2),
+    "box_long_photon_short_query": ("box_medium", False,
+                                    ["-a", "upbp+pp3d+pb2d+bb1d+bp2d", "-pbt", "L", "-qbt", "S", "-l", "8",
+                                     "-r", "32x32"] + BOX_R, 1),
+    "box_compatible": ("box_medium", False, ["-a", "upbp_all", "-compatible", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_previous": ("box_medium", False, ["-a", "upbp_all", "-previous", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_pbc_ioff": ("box_medium", False,
+                     ["-a", "upbp_all", "-pbc", "300", "-ioff", "3", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "media_field_tiny": ("media_field", True,
+                         ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "12", "-r", "64x36"], 1),
+    "dense_beams_tiny": ("dense_beams", True,
+                         ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "16", "-r", "48x48",
+                          "-r_initial_bb1d", "-0.004", "-r_initial_bp2d", "-0.004"], 1),
+}
+
+
+def command_line(case: str, scene_path: str) -> list:
+    return ["-s", "-1", scene_path] + list(CASES[case][2])

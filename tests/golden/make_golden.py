@@ -1,0 +1,44 @@
+"""Regenerates tests/golden/oracle_images.npz: per-iteration images of every
+parity case rendered by the reference's own render loop compiled for the CPU
+(oracle/_ref/libupbp_ref_cpu.so, built by `make -C oracle`).
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, HERE)
+
+import ref_cpu  # noqa: E402
+from cases import CASES, command_line  # noqa: E402
+from gpuupbp_b200 import scenes  # noqa: E402
+
+
+def main():
+    out, meta = {}, {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (workload, tiny, _, iters) in CASES.items():
+            path = scenes.write_workload(workload, tmp, tiny=tiny)
+            r = ref_cpu.RefRenderer(command_line(name, path), threads=0)
+            meta[name] = []
+            for it in range(iters):
+                out[f"{name}/{it}"] = r.run_iteration(it)
+                st = r.stats()
+                meta[name].append({k: st[k] for k in ("vertices", "surface", "medium", "beams")})
+            r.close()
+            print(name, meta[name], flush=True)
+    np.savez_compressed(os.path.join(HERE, "oracle_images.npz"), **out)
+    with open(os.path.join(HERE, "oracle_counts.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
