@@ -111,13 +111,34 @@ BYTES_PER_WORK = {"nodes": 64, "tris": 48, "rays": 72, "point_cand": 16, "point_
                   "beam_hit": 128, "vertex_loads": 128}
 
 
-def algorithmic_bytes(work: dict, pixels: int) -> float:
-    return float(sum(BYTES_PER_WORK[k] * v for k, v in work.items())) + 24.0 * pixels
+def algorithmic_bytes(work: dict, extra: float = 0.0) -> float:
+    return float(sum(BYTES_PER_WORK[k] * v for k, v in work.items())) + extra
+
+
+# Bytes of the query records each camera-side kernel writes or reads.
+SEG_RECORD, POINT_RECORD = 128, 144
+
+
+def kernel_rooflines(st: dict, pixels: int) -> dict:
+    """Algorithmic bytes and time per launch of each kernel of an iteration."""
+    n = max(1, st["timed_iterations"])
+    ms = st["ms_kernel_sum"]
+    nseg, npt = st["segment_queries"], st["point_queries"]
+    extra = {"light_pass": 0.0,
+             "camera_extend": 12.0 * pixels + SEG_RECORD * nseg + POINT_RECORD * npt,
+             "pb2d_query": SEG_RECORD * nseg, "bb1d_query": SEG_RECORD * nseg,
+             "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt, "bp2d_query": POINT_RECORD * npt}
+    out = {}
+    for k, w in st["work"].items():
+        t = ms[k] / n
+        b = algorithmic_bytes(w, extra[k])
+        out[k] = {"ms": t, "bytes": b, "gbs": (b / (t * 1e-3) / 1e9) if t > 0 else 0.0}
+    return out
 
 
 def profiled_traffic() -> float | None:
     """DRAM bytes per camera-pass launch from the committed ncu summary, if any."""
-    p = os.path.join(HERE, "profiles", "camera_pass_media_field.md")
+    p = os.path.join(HERE, "profiles", "dominant_kernel_media_field.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -205,8 +226,10 @@ def run_b200(args) -> dict | None:
     hbm = hbm or 6650.0
     pixels = r.config.res_x * r.config.res_y
     cam_ms = st["ms_camera_sum"] / max(1, st["timed_iterations"])
-    b_cam = algorithmic_bytes(st["work_camera"], pixels)
-    achieved = b_cam / (cam_ms * 1e-3) / 1e9
+    kernels = kernel_rooflines(st, pixels)
+    top = max(kernels, key=lambda k: kernels[k]["ms"])
+    b_top, top_ms = kernels[top]["bytes"], kernels[top]["ms"]
+    achieved = kernels[top]["gbs"]
     traffic = profiled_traffic()
     total_paths = paths_per_iter * args.steps * world
     value = total_paths / (ms * 1e-3)
@@ -224,13 +247,15 @@ def run_b200(args) -> dict | None:
                 "d2h_bytes_per_step": int(st_e2e["d2h_bytes"]) + pixels * 12,
                 "wall_s": wall_e2e},
         "gpu_launches": int(st["kernel_launches"]) * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "camera_pass_kernel", "achieved": achieved, "peak": hbm,
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": b_cam, "launch_ms": cam_ms},
+                     "traffic": traffic, "algorithmic_bytes_per_launch": b_top, "launch_ms": top_ms},
+        "kernels": kernels,
         "clocks": clk.summary(),
         "passes_ms": {"light": st["ms_light_sum"] / max(1, st["timed_iterations"]),
                       "build": st["ms_build_sum"] / max(1, st["timed_iterations"]), "camera": cam_ms},
-        "work_camera": st["work_camera"], "status": int(st["status"]), "wall_s": wall,
+        "work": st["work"], "queries": {"segment": st["segment_queries"], "point": st["point_queries"]},
+        "status": int(st["status"]), "wall_s": wall,
     }
     r.close()
     return out

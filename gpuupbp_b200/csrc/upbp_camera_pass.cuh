@@ -168,10 +168,11 @@ UPBP_D unsigned connect_vertices(float3& contrib, const LightVertex& lv, const B
 
 // SURF / PP3D merge of a camera vertex with one photon, Eq 4.52/4.17/4.53
 // (functs_pp.cuh:44-136).
-UPBP_D float3 eval_point_merge(const LightVertex& lv, const PathState& s, const Bsdf& cb, bool medium)
+UPBP_D float3 eval_point_merge(const LightVertex& lv, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb,
+                                bool medium)
 {
     const DeviceParams& p = c_params;
-    const unsigned plen = lv.path_length + s.path_length;
+    const unsigned plen = lv.path_length + cam_len;
     if (plen > p.max_path_length || plen < p.min_path_length) return v3(0.f);
     const float3 pdir = lv.bsdf.dir_fix();
     float cos_c, fpdf, rpdf, sin_theta;
@@ -180,7 +181,6 @@ UPBP_D float3 eval_point_merge(const LightVertex& lv, const PathState& s, const 
     fpdf *= cb.cont_prob;
     rpdf *= lv.bsdf.cont_prob;
     const VertexWeights& wl = lv.w;
-    const VertexWeights& wc = s.sw.w;
     const float ff = p.photon_beam_type == kLongBeam ? wl.for_inv : wl.for_ratio;
     const float rf = p.camera_beam_type == kLongBeam ? wc.for_inv : wc.for_ratio;
     const float val = medium ? 1.f / p.mis_factor_pp3d : 1.f / p.mis_factor_surf;
@@ -194,14 +194,14 @@ UPBP_D float3 eval_point_merge(const LightVertex& lv, const PathState& s, const 
     return mis * f * lv.thr;
 }
 
-UPBP_D float3 query_points(const PointMap& map, float3 x, float r, float r2, const PathState& s, const Bsdf& cb,
-                           bool medium)
+UPBP_D float3 query_points(const PointMap& map, float3 x, float r, float r2, unsigned cam_len, const VertexWeights& wc,
+                           const Bsdf& cb, bool medium)
 {
     float3 acc = v3(0.f);
     points_in_radius(map, x, r, r2, [&](unsigned slot) {
         LightVertex lv;
         load_vertex(c_params.vertices + slot, lv);
-        acc += eval_point_merge(lv, s, cb, medium);
+        acc += eval_point_merge(lv, cam_len, wc, cb, medium);
     });
     return acc;
 }
@@ -349,10 +349,11 @@ UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& l
 }
 
 // BP2D: photon beam x camera point (functs_bp2d.cuh:51-198).
-UPBP_D float3 eval_bp2d(const Beam& lb, const PathState& s, const Bsdf& cb, float isect_dist, float rad2)
+UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb, float isect_dist,
+                        float rad2)
 {
     const DeviceParams& p = c_params;
-    const unsigned plen = lb.path_length + s.path_length;
+    const unsigned plen = lb.path_length + cam_len;
     if (plen > p.max_path_length || plen < p.min_path_length) return v3(0.f);
     const DMedium& m = p.media[lb.med];
     float3 att = attenuation(m, isect_dist);
@@ -390,7 +391,6 @@ UPBP_D float3 eval_bp2d(const Beam& lb, const PathState& s, const Bsdf& cb, floa
     if (!is_positive(kernel)) return v3(0.f);
     const float3 unweighted = lb.thr * att * m.scattering * f * kernel;
     if (is_black_or_negative(unweighted)) return v3(0.f);
-    const VertexWeights& wc = s.sw.w;
     const float ff = p.photon_beam_type == kLongBeam ? wl.for_inv : wl.for_ratio;
     const float rf = p.camera_beam_type == kLongBeam ? wc.for_inv : wc.for_ratio;
     const float val = 1.f / (p.mis_factor_bp2d * ff);
@@ -429,26 +429,28 @@ UPBP_D float3 query_bb1d(const QuerySeg& q, const StateWeights& cw)
     return acc;
 }
 
-UPBP_D float3 query_bp2d(float3 x, const PathState& s, const Bsdf& cb)
+UPBP_D float3 query_bp2d(float3 x, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb)
 {
     const DeviceParams& p = c_params;
     float3 acc = v3(0.f);
     beams_near_point(p.beam_map, x, p.rad_beam, p.radius_bp2d_2, [&](unsigned b, float dist, float rad2) {
         Beam lb;
         load_beam(p.beams + b, lb);
-        acc += eval_bp2d(lb, s, cb, dist, rad2);
+        acc += eval_bp2d(lb, cam_len, wc, cb, dist, rad2);
     });
     return acc;
 }
 
-// Accumulates PB2D or BB1D along the query segments of one camera ray
-// (eval_*_segments, both the VolSegment and the lite-segment variants).
-template <bool kBb1d>
-UPBP_D float3 eval_query_segments(float3 ro, float3 rd, const VolSeg* segs, int nseg, const LiteSeg* lsegs, int nlseg,
-                                  bool use_lite, unsigned sflags, unsigned cam_path_length, const StateWeights& cw)
+// Emits one segment-query record per scattering medium segment of a camera
+// ray, with the attenuation and sampling pdfs accumulated over the segments
+// before it (the segment loop of eval_pb2d_segments / eval_bb1d_segments,
+// functs_pb2d.cuh:226-342, functs_bb1d.cuh:273-397, both variants).
+UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int nseg, const LiteSeg* lsegs, int nlseg,
+                                 bool use_lite, unsigned sflags, unsigned cam_path_length, const StateWeights& cw,
+                                 float3 throughput, unsigned pixel)
 {
     const DeviceParams& p = c_params;
-    float3 result = v3(0.f), att = v3(1.f);
+    float3 att = v3(1.f);
     float fpdf = 1.f, rpdf = 1.f;
     const int n = use_lite ? nlseg : nseg;
     for (int i = 0; i < n; i++) {
@@ -456,24 +458,27 @@ UPBP_D float3 eval_query_segments(float3 ro, float3 rd, const VolSeg* segs, int 
         const float dmax = use_lite ? lsegs[i].dmax : segs[i].dmax;
         const int med = use_lite ? lsegs[i].med : segs[i].med;
         const DMedium& m = p.media[med];
-        float3 seg_result = v3(0.f);
         if (m.has_scattering) {
-            QuerySeg q;
-            q.o = ro;
-            q.d = rd;
-            q.dmin = dmin;
-            q.dmax = dmax;
-            q.med = med;
-            q.for_pdf = fpdf;
-            q.rev_pdf = rpdf;
-            q.flags = kEndInMedium | (i == 0 ? sflags : 0u);
-            q.cam_path_length = cam_path_length;
-            seg_result = kBb1d ? query_bb1d(q, cw) : query_pb2d(q, cw);
+            const unsigned k = atomicAdd(&p.queue_count[0], 1u);
+            if (k < p.seg_capacity) {
+                float4* q = p.seg_queue[k].q;
+                const float3 w = throughput * att;
+                const unsigned flags = kEndInMedium | (i == 0 ? sflags : 0u);
+                q[0] = make_float4(ro.x, ro.y, ro.z, dmin);
+                q[1] = make_float4(rd.x, rd.y, rd.z, dmax);
+                q[2] = make_float4(w.x, w.y, w.z, ubits((unsigned)med));
+                q[3] = make_float4(fpdf, rpdf, ubits(flags), ubits((pixel << 8) | (cam_path_length & 0xffu)));
+                const VertexWeights& vw = cw.w;
+                const unsigned bits = (vw.prev_in_medium ? 1u : 0u) | (vw.prev_specular ? 2u : 0u);
+                q[4] = make_float4(vw.d_shared, vw.d_bpt, vw.d_pde, vw.for_inv);
+                q[5] = make_float4(vw.rev_inv, vw.for_ratio, vw.rev_ratio, ubits(bits));
+                q[6] = make_float4(cw.last_sin_theta, cw.d_bpt_a, cw.d_bpt_b, cw.d_pde_a);
+                q[7] = make_float4(cw.d_pde_b, 0.f, 0.f, 0.f);
+            }
         }
-        result += att * seg_result;
         if (use_lite) {
             att *= attenuation(m, dmax - dmin);
-            if (!is_positive(att)) return result;
+            if (!is_positive(att)) return;
             float sr;
             const float sf = distance_pdf(m, dmin, dmax, i == 0 ? sflags : 0u, sr);
             fpdf *= sf;
@@ -483,15 +488,95 @@ UPBP_D float3 eval_query_segments(float3 ro, float3 rd, const VolSeg* segs, int 
                 att *= segs[i].att / segs[i].pdf_for;
             else
                 att *= segs[i].att;
-            if (!is_positive(att)) return result;
+            if (!is_positive(att)) return;
             fpdf *= segs[i].pdf_for;
             rpdf *= segs[i].pdf_rev;
         }
     }
-    return result;
 }
 
-__global__ void __launch_bounds__(128) camera_pass_kernel()
+// PB2D (kBb1d = false) or BB1D (kBb1d = true) for one segment-query record;
+// adds weight * normalization * estimate into the camera image.
+template <bool kBb1d>
+__global__ void __launch_bounds__(128) segment_query_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned n = min(*p.queue_count, p.seg_capacity);
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4* r = p.seg_queue[k].q;
+        const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]), q2 = __ldg(&r[2]), q3 = __ldg(&r[3]);
+        const float4 q4 = __ldg(&r[4]), q5 = __ldg(&r[5]), q6 = __ldg(&r[6]), q7 = __ldg(&r[7]);
+        QuerySeg q;
+        q.o = xyz(q0);
+        q.dmin = q0.w;
+        q.d = xyz(q1);
+        q.dmax = q1.w;
+        q.med = (int)fbits(q2.w);
+        q.for_pdf = q3.x;
+        q.rev_pdf = q3.y;
+        q.flags = fbits(q3.z);
+        const unsigned pk = fbits(q3.w);
+        q.cam_path_length = pk & 0xffu;
+        StateWeights cw;
+        cw.w.d_shared = q4.x;
+        cw.w.d_bpt = q4.y;
+        cw.w.d_pde = q4.z;
+        cw.w.for_inv = q4.w;
+        cw.w.rev_inv = q5.x;
+        cw.w.for_ratio = q5.y;
+        cw.w.rev_ratio = q5.z;
+        const unsigned bits = fbits(q5.w);
+        cw.w.prev_in_medium = bits & 1u;
+        cw.w.prev_specular = (bits >> 1) & 1u;
+        cw.last_sin_theta = q6.x;
+        cw.d_bpt_a = q6.y;
+        cw.d_bpt_b = q6.z;
+        cw.d_pde_a = q6.w;
+        cw.d_pde_b = q7.x;
+        const float3 est = kBb1d ? query_bb1d(q, cw) : query_pb2d(q, cw);
+        const float norm = kBb1d ? p.bb1d_normalization : p.pb2d_normalization;
+        const float3 c = xyz(q2) * norm * est;
+        if ((c.x != 0.f || c.y != 0.f || c.z != 0.f) && (pk >> 8) != 0xffffffu) {
+            const unsigned px = pk >> 8;
+            atomicAdd(&p.cam_fb[3 * px + 0], c.x);
+            atomicAdd(&p.cam_fb[3 * px + 1], c.y);
+            atomicAdd(&p.cam_fb[3 * px + 2], c.z);
+        }
+    }
+}
+
+enum : unsigned { kQuerySurf = 1u, kQueryPp3d = 2u, kQueryBp2d = 4u };
+
+// SURF, PP3D or BP2D (kKind) for one point-query record.
+template <unsigned kKind>
+__global__ void __launch_bounds__(128) point_query_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned n = min(p.queue_count[1], p.pt_capacity);
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 q8 = __ldg(&p.pt_queue[k].q8);
+        if (!(fbits(q8.y) & kKind)) continue;
+        LightVertex cv;
+        load_vertex(&p.pt_queue[k].v, cv);
+        float3 c;
+        if (kKind == kQuerySurf)
+            c = cv.thr * p.surf_normalization *
+                query_points(p.surf_map, cv.hit, p.radius_surf, p.radius_surf_2, cv.path_length, cv.w, cv.bsdf, false);
+        else if (kKind == kQueryPp3d)
+            c = cv.thr * p.pp3d_normalization *
+                query_points(p.med_map, cv.hit, p.radius_pp3d, p.radius_pp3d_2, cv.path_length, cv.w, cv.bsdf, true);
+        else
+            c = cv.thr * p.bp2d_normalization * query_bp2d(cv.hit, cv.path_length, cv.w, cv.bsdf);
+        if ((c.x != 0.f || c.y != 0.f || c.z != 0.f) && fbits(q8.x) != 0xffffffu) {
+            const unsigned px = fbits(q8.x);
+            atomicAdd(&p.cam_fb[3 * px + 0], c.x);
+            atomicAdd(&p.cam_fb[3 * px + 1], c.y);
+            atomicAdd(&p.cam_fb[3 * px + 2], c.z);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 4) camera_pass_kernel()
 {
     const DeviceParams& p = c_params;
     const unsigned pixel = blockIdx.x * blockDim.x + threadIdx.x;
@@ -505,6 +590,12 @@ __global__ void __launch_bounds__(128) camera_pass_kernel()
     float2 screen;
     unsigned ret = generate_camera_sample(screen, pixel, s, rng);
     float3 color = v3(0.f);
+    // add_color (frame_buffer.cuh:36-45) targets the pixel of the jittered
+    // sample, which float rounding can move to the next pixel or off screen
+    constexpr unsigned kNoPixel = 0xffffffu;
+    unsigned target = kNoPixel;
+    if (!(screen.x < 0.f || screen.x >= (float)p.res_x || screen.y < 0.f || screen.y >= (float)p.res_y))
+        target = (unsigned)int(screen.x) + (unsigned)int(screen.y) * p.res_x;
     bool origin_in_medium = false;
     bool only_spec_surf = (p.estimator_techniques & (kPrevious | kCompatible)) != 0;
 
@@ -520,17 +611,11 @@ __global__ void __launch_bounds__(128) camera_pass_kernel()
         ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
                               segs, nseg, lsegs, nlseg, rng);
         if (ret) break;
-        const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
-        const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
-        if (p.build_pb2d && p.n_medium > 0) {
-            const float3 c = eval_query_segments<false>(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags,
-                                                        s.path_length, s.sw);
-            color += s.throughput * p.pb2d_normalization * c;
-        }
-        if (p.build_bb1d && p.n_beams > 0) {
-            const float3 c = eval_query_segments<true>(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags,
-                                                       s.path_length, s.sw);
-            color += s.throughput * p.bb1d_normalization * c;
+        if ((p.build_pb2d && p.n_medium > 0) || (p.build_bb1d && p.n_beams > 0)) {
+            const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
+            const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
+            emit_segment_queries(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags, s.path_length, s.sw, s.throughput,
+                                 target);
         }
         if (!hit) {
             if (s.path_length < p.min_path_length) break;
@@ -623,14 +708,23 @@ __global__ void __launch_bounds__(128) camera_pass_kernel()
             }
             if (err) break;
         }
-        if (p.build_surf && p.n_surface > 0 && bsdf.on_surface() && !bsdf.delta() && !only_spec_surf)
-            color += s.throughput * p.surf_normalization *
-                     query_points(p.surf_map, hitpoint, p.radius_surf, p.radius_surf_2, s, bsdf, false);
-        if (p.build_pp3d && p.n_medium > 0 && bsdf.in_medium() && !bsdf.delta())
-            color += s.throughput * p.pp3d_normalization *
-                     query_points(p.med_map, hitpoint, p.radius_pp3d, p.radius_pp3d_2, s, bsdf, true);
-        if (p.build_bp2d && p.n_beams > 0 && bsdf.in_medium())
-            color += s.throughput * p.bp2d_normalization * query_bp2d(hitpoint, s, bsdf);
+        {
+            unsigned mask = 0;
+            if (p.build_surf && p.n_surface > 0 && bsdf.on_surface() && !bsdf.delta() && !only_spec_surf)
+                mask |= kQuerySurf;
+            if (p.build_pp3d && p.n_medium > 0 && bsdf.in_medium() && !bsdf.delta()) mask |= kQueryPp3d;
+            if (p.build_bp2d && p.n_beams > 0 && bsdf.in_medium()) mask |= kQueryBp2d;
+            if (mask) {
+                const unsigned k = atomicAdd(&p.queue_count[1], 1u);
+                if (k < p.pt_capacity) {
+                    PointQueryRec* rec = p.pt_queue + k;
+                    const float3 frame_src = bsdf.on_surface() ? isect.shading_normal : rd;
+                    store_vertex(&rec->v, hitpoint, s.throughput, s.path_length, bsdf.in_medium(), false, bsdf,
+                                 frame_src, s.sw.w);
+                    rec->q8 = make_float4(ubits(target), ubits(mask), 0.f, 0.f);
+                }
+            }
+        }
         bool cont;
         ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
         if (ret || !cont) break;
@@ -647,11 +741,21 @@ __global__ void __launch_bounds__(128) camera_pass_kernel()
         }
     }
     if (ret) flag_status(ret);
-    if (screen.x < 0.f || screen.x >= (float)p.res_x || screen.y < 0.f || screen.y >= (float)p.res_y) return;
-    const unsigned px = (unsigned)int(screen.x) + (unsigned)int(screen.y) * p.res_x;
-    p.framebuffer[3 * px + 0] += color.x;
-    p.framebuffer[3 * px + 1] += color.y;
-    p.framebuffer[3 * px + 2] += color.z;
+    if (target == kNoPixel) return;
+    atomicAdd(&p.cam_fb[3 * target + 0], color.x);
+    atomicAdd(&p.cam_fb[3 * target + 1], color.y);
+    atomicAdd(&p.cam_fb[3 * target + 2], color.z);
+}
+
+// Adds the camera image into the iteration image (which holds the light
+// tracer's splats) and the iteration image into the accumulation.
+__global__ void k_finish_iteration(float* fb, const float* cam_fb, double* acc, unsigned n)
+{
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = fb[i] + cam_fb[i];
+    fb[i] = v;
+    acc[i] += (double)v;
 }
 
 }  // namespace upbp

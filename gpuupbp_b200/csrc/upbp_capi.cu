@@ -18,6 +18,9 @@
 using namespace upbp;
 
 constexpr int kEventRing = 64;
+// events per iteration: start, light done, maps done, then one after each
+// camera-side kernel kind (extend, pb2d, bb1d, surf, pp3d, bp2d)
+constexpr int kEvPerIter = 3 + (kKernCount - 1);
 
 namespace {
 
@@ -44,12 +47,6 @@ cudaError_t dupload(T** p, const T* h, size_t n, cudaStream_t st)
     cudaError_t e = dalloc(p, n);
     if (e != cudaSuccess || n == 0) return e;
     return cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
-}
-
-__global__ void k_accumulate(const float* fb, double* acc, unsigned n)
-{
-    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) acc[i] += (double)fb[i];
 }
 
 // Neighbour sets of n queries through the estimators' range-query walkers.
@@ -102,7 +99,7 @@ struct upbp_ctx {
     upbp_config cfg{};
     DeviceParams P{};
     cudaStream_t st = nullptr;
-    cudaEvent_t ev_ring[kEventRing][4] = {};   // per-iteration events: start, light done, maps done, camera done
+    cudaEvent_t ev_ring[kEventRing][kEvPerIter] = {};
     unsigned ev_pending = 0;                   // iterations recorded since the last stats read
     DMaterial* d_mat = nullptr;
     DMedium* d_med = nullptr;
@@ -125,8 +122,14 @@ struct upbp_ctx {
     void* d_scan_temp = nullptr;
     size_t scan_temp_bytes = 0;
     unsigned last_chunks = 0;
-    unsigned long long* d_work = nullptr;   // 2 x kCtrCount: light pass, camera pass
+    unsigned long long* d_work = nullptr;   // kKernCount x kCtrCount
     unsigned launches = 0;
+    SegQueryRec* d_seg_queue = nullptr;
+    PointQueryRec* d_pt_queue = nullptr;
+    unsigned seg_capacity = 0, pt_capacity = 0;
+    unsigned* d_qcount = nullptr;
+    float* d_cam_fb = nullptr;
+    unsigned h_qcount[2] = {0, 0};
     BuildScratch sc;
     float r0[5] = {0, 0, 0, 0, 0};  // bb1d bp2d pb2d pp3d surf
     float bb1d_used = 0.f;
@@ -452,7 +455,13 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     UPBP_CK(dalloc(&c->d_fb, npx));
     UPBP_CK(dalloc(&c->d_acc, npx));
     UPBP_CK(dalloc(&c->d_status, 1));
-    UPBP_CK(dalloc(&c->d_work, 2 * kCtrCount));
+    UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
+    UPBP_CK(dalloc(&c->d_qcount, 2));
+    UPBP_CK(dalloc(&c->d_cam_fb, npx));
+    c->seg_capacity = std::max(1024u, 4 * P.screen_pixel_count);
+    c->pt_capacity = std::max(1024u, 3 * P.screen_pixel_count);
+    UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
+    UPBP_CK(dalloc(&c->d_pt_queue, c->pt_capacity));
     UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
@@ -481,6 +490,12 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     P.beams = c->d_beams;
     P.framebuffer = c->d_fb;
     P.status = c->d_status;
+    P.seg_queue = c->d_seg_queue;
+    P.seg_capacity = c->seg_capacity;
+    P.pt_queue = c->d_pt_queue;
+    P.pt_capacity = c->pt_capacity;
+    P.queue_count = c->d_qcount;
+    P.cam_fb = c->d_cam_fb;
     UPBP_CK(cudaStreamSynchronize(c->st));
     *out = c;
     return UPBP_OK;
@@ -496,9 +511,14 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     cudaEvent_t* ev = c->ev_ring[c->iterations % kEventRing];
     UPBP_CK(cudaEventRecord(ev[0], c->st));
     UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
-    UPBP_CK(cudaMemsetAsync(c->d_work, 0, 2 * kCtrCount * sizeof(unsigned long long), c->st));
+    UPBP_CK(cudaMemsetAsync(c->d_work, 0, (size_t)kKernCount * kCtrCount * sizeof(unsigned long long), c->st));
     unsigned launches = 0;
     P.work = c->d_work;
+    auto set_work = [&](int kern) -> cudaError_t {
+        unsigned long long* w = c->d_work + (size_t)kern * kCtrCount;
+        return cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st);
+    };
+    UPBP_CK(set_work(kKernLight));
     unsigned found[4] = {0, 0, 0, 0};
     if (P.trace_light_paths) {
         // radius schedule and MIS factors (renderer.cpp:57-119)
@@ -615,16 +635,81 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     P.n_medium = found[2];
     P.n_beams = found[3];
 
-    P.work = c->d_work + kCtrCount;
-    UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+    UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
     UPBP_CK(cudaEventRecord(ev[2], c->st));
     if (P.trace_camera_paths) {
-        camera_pass_kernel<<<(P.screen_pixel_count + 127) / 128, 128, 0, c->st>>>();
-        launches++;
-        UPBP_CK(cudaGetLastError());
+        // extend: tracing, emitter hits, NEE and BPT; queues the range queries
+        for (int attempt = 0; attempt < 2; attempt++) {
+            UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 2 * sizeof(unsigned), c->st));
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+            UPBP_CK(set_work(kKernCameraExtend));
+            camera_pass_kernel<<<(P.screen_pixel_count + 127) / 128, 128, 0, c->st>>>();
+            launches++;
+            UPBP_CK(cudaGetLastError());
+            UPBP_CK(cudaMemcpyAsync(c->h_qcount, c->d_qcount, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            if (c->h_qcount[0] <= c->seg_capacity && c->h_qcount[1] <= c->pt_capacity) break;
+            // a queue overflowed: grow it and render the camera pass again (the
+            // pass is a pure function of the iteration, so the rerun is exact)
+            if (c->h_qcount[0] > c->seg_capacity) {
+                cudaFree(c->d_seg_queue);
+                c->seg_capacity = c->h_qcount[0] + c->h_qcount[0] / 4;
+                UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
+            }
+            if (c->h_qcount[1] > c->pt_capacity) {
+                cudaFree(c->d_pt_queue);
+                c->pt_capacity = c->h_qcount[1] + c->h_qcount[1] / 4;
+                UPBP_CK(dalloc(&c->d_pt_queue, c->pt_capacity));
+            }
+            P.seg_queue = c->d_seg_queue;
+            P.seg_capacity = c->seg_capacity;
+            P.pt_queue = c->d_pt_queue;
+            P.pt_capacity = c->pt_capacity;
+            UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
+        }
     }
     UPBP_CK(cudaEventRecord(ev[3], c->st));
-    k_accumulate<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_acc, (unsigned)npx);
+    const unsigned nseg = std::min(c->h_qcount[0], c->seg_capacity);
+    const unsigned npt = std::min(c->h_qcount[1], c->pt_capacity);
+    auto grid_for = [](unsigned n) { return std::max(1u, std::min((n + 127) / 128, 148u * 64u)); };
+    const bool run_pb2d = P.trace_camera_paths && P.build_pb2d && P.n_medium > 0 && nseg > 0;
+    const bool run_bb1d = P.trace_camera_paths && P.build_bb1d && P.n_beams > 0 && nseg > 0;
+    const bool run_surf = P.trace_camera_paths && P.build_surf && P.n_surface > 0 && npt > 0;
+    const bool run_pp3d = P.trace_camera_paths && P.build_pp3d && P.n_medium > 0 && npt > 0;
+    const bool run_bp2d = P.trace_camera_paths && P.build_bp2d && P.n_beams > 0 && npt > 0;
+    if (run_pb2d) {
+        UPBP_CK(set_work(kKernPb2d));
+        segment_query_kernel<false><<<grid_for(nseg), 128, 0, c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaEventRecord(ev[4], c->st));
+    if (run_bb1d) {
+        UPBP_CK(set_work(kKernBb1d));
+        segment_query_kernel<true><<<grid_for(nseg), 128, 0, c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaEventRecord(ev[5], c->st));
+    if (run_surf) {
+        UPBP_CK(set_work(kKernSurf));
+        point_query_kernel<kQuerySurf><<<grid_for(npt), 128, 0, c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaEventRecord(ev[6], c->st));
+    if (run_pp3d) {
+        UPBP_CK(set_work(kKernPp3d));
+        point_query_kernel<kQueryPp3d><<<grid_for(npt), 128, 0, c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaEventRecord(ev[7], c->st));
+    if (run_bp2d) {
+        UPBP_CK(set_work(kKernBp2d));
+        point_query_kernel<kQueryBp2d><<<grid_for(npt), 128, 0, c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaGetLastError());
+    UPBP_CK(cudaEventRecord(ev[8], c->st));
+    k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
+                                                                         (unsigned)npx);
     launches++;
     c->launches = launches;
     UPBP_CK(cudaGetLastError());
@@ -670,12 +755,18 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     o->iterations_done = c->iterations;
     o->triangle_count = c->triangles;
     o->scene_radius = c->P.scene_radius;
-    unsigned long long work[2 * kCtrCount];
+    unsigned long long work[kKernCount * kCtrCount];
     UPBP_CK(cudaMemcpy(work, c->d_work, sizeof(work), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < kKernCount && k < 7; k++)
+        for (int i = 0; i < kCtrCount && i < 8; i++) o->work[k][i] = work[k * kCtrCount + i];
     for (int i = 0; i < kCtrCount && i < 8; i++) {
         o->work_light[i] = work[i];
-        o->work_camera[i] = work[kCtrCount + i];
+        unsigned long long cam = 0;
+        for (int k = 1; k < kKernCount; k++) cam += work[k * kCtrCount + i];
+        o->work_camera[i] = cam;
     }
+    o->segment_queries = c->h_qcount[0];
+    o->point_queries = c->h_qcount[1];
     o->beam_chunks = c->last_chunks;
     o->radius[0] = c->P.radius_bb1d;
     o->radius[1] = c->P.radius_bp2d;
@@ -690,18 +781,19 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     // since the previous stats call (up to the event ring size)
     for (unsigned k = 0; k < c->ev_pending; k++) {
         cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
-        float a = 0.f, b = 0.f, d = 0.f;
-        UPBP_CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-        UPBP_CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
-        UPBP_CK(cudaEventElapsedTime(&d, ev[2], ev[3]));
+        float t[kEvPerIter - 1];
+        for (int e = 0; e + 1 < kEvPerIter; e++) UPBP_CK(cudaEventElapsedTime(&t[e], ev[e], ev[e + 1]));
+        const float cam = t[2] + t[3] + t[4] + t[5] + t[6] + t[7];
         if (k == 0) {
-            o->ms_light = a;
-            o->ms_build = b;
-            o->ms_camera = d;
+            o->ms_light = t[0];
+            o->ms_build = t[1];
+            o->ms_camera = cam;
         }
-        o->ms_light_sum += a;
-        o->ms_build_sum += b;
-        o->ms_camera_sum += d;
+        o->ms_light_sum += t[0];
+        o->ms_build_sum += t[1];
+        o->ms_camera_sum += cam;
+        o->ms_kernel_sum[kKernLight] += t[0];
+        for (int kk = 1; kk < kKernCount; kk++) o->ms_kernel_sum[kk] += t[1 + kk];
         o->timed_iterations++;
     }
     c->ev_pending = 0;
@@ -775,7 +867,8 @@ extern "C" void upbp_destroy(upbp_ctx* c)
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
-                    c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work};
+                    c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
+                    c->d_qcount, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue};
     for (void* b : bufs)
         if (b) cudaFree(b);
     free_scratch(c->sc);

@@ -118,6 +118,23 @@ struct BeamRec {
     float4 q[8];
 };
 
+// Camera-pass query records (wavefront camera pass).
+// Segment query (PB2D / BB1D along one medium segment of a camera ray):
+//   q0: origin.xyz, dmin   q1: direction.xyz, dmax
+//   q2: weight.xyz (path throughput x attenuation before the segment), medium id bits
+//   q3: ray_sample_for_pdf, ray_sample_rev_pdf, sampling flags bits, pixel << 8 | camera path length
+//   q4..q7: camera StateWeights in the beam record layout (BeamRec q4..q7)
+struct SegQueryRec {
+    float4 q[8];
+};
+// Point query (SURF / PP3D / BP2D at one camera vertex): a LightVertexRec
+// of the camera vertex (throughput, weights, BSDF) plus
+//   q8: pixel bits, estimator mask bits (1 SURF, 2 PP3D, 4 BP2D), -, -
+struct PointQueryRec {
+    LightVertexRec v;
+    float4 q8;
+};
+
 // Point map: BVH over light-vertex positions in leaf order.
 //   pos[i] = (position.xyz, slot index bits)
 struct PointMap {
@@ -188,11 +205,26 @@ struct DeviceParams {
     PointMap surf_map, med_map;
     BeamMap beam_map;
     unsigned n_surface, n_medium, n_beams;   // host-side copies of the light-pass counters
+
+    // wavefront camera pass
+    SegQueryRec* seg_queue;
+    unsigned seg_capacity;
+    PointQueryRec* pt_queue;
+    unsigned pt_capacity;
+    unsigned* queue_count;            // [0] segment queries, [1] point queries
+    float* cam_fb;                    // camera-pass image, W*H*3
 };
 
 // Launch parameters of the running pass, uploaded before each launch.
 __constant__ DeviceParams c_params;
+// Work-counter set of the running kernel (one set per kernel kind).
+__constant__ unsigned long long* c_work;
 
-UPBP_D unsigned long long* c_work_ptr() { return c_params.work; }
+UPBP_D unsigned long long* c_work_ptr() { return c_work; }
+
+// Kernel kinds of an iteration, for work counters and timing.
+enum : int {
+    kKernLight = 0, kKernCameraExtend, kKernPb2d, kKernBb1d, kKernSurf, kKernPp3d, kKernBp2d, kKernCount
+};
 
 }  // namespace upbp

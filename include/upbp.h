@@ -156,7 +156,7 @@ typedef struct upbp_stats {
     uint32_t light_paths, camera_paths;
     uint32_t status;              /* OR of UPBP_STATUS_* seen so far */
     uint32_t iterations_done;
-    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events; ms_camera is the camera-pass kernel */
+    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events; camera = extend + query kernels */
     uint64_t triangle_count;
     double scene_radius;
     /* Work counters of the last iteration, light pass then camera pass, in
@@ -176,6 +176,12 @@ typedef struct upbp_stats {
     /* Radii of the last iteration: bb1d, bp2d, pb2d, pp3d, surf, and the beam
      * radius used for the beam map (max of bb1d and bp2d when enabled). */
     float radius[6];
+    /* Per kernel kind -- light pass, camera extend, PB2D, BB1D, SURF, PP3D,
+     * BP2D queries -- work counters of the last iteration and kernel times
+     * summed like the pass times above. */
+    uint64_t work[7][8];
+    double ms_kernel_sum[7];
+    uint32_t segment_queries, point_queries;   /* query records of the last camera pass */
 } upbp_stats;
 
 /* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
