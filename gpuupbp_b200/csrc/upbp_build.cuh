@@ -293,7 +293,7 @@ __global__ void k_chunk_expand(const unsigned* counts, const unsigned* offsets, 
 }
 
 // Leaf payload of the chunked beam map: (origin, length), (direction, bits),
-// (t0, t1) where bits = beam index | BB1D-eligible << 31.
+// (t0, t1, medium id bits) where bits = beam index | BB1D-eligible << 31.
 __global__ void k_gather_chunks(const uint2* chunks, const BeamRec* beams, const unsigned* vals, unsigned n,
                                 unsigned bb1d_paths, float4* out)
 {
@@ -307,7 +307,7 @@ __global__ void k_gather_chunks(const uint2* chunks, const BeamRec* beams, const
     const unsigned k = ch.y & 0xffffu, c = ch.y >> 16;
     out[3 * s] = q0;
     out[3 * s + 1] = make_float4(q1.x, q1.y, q1.z, __uint_as_float(bits));
-    out[3 * s + 2] = make_float4(chunk_t(q0.w, k, c), chunk_t(q0.w, k + 1, c), 0.f, 0.f);
+    out[3 * s + 2] = make_float4(chunk_t(q0.w, k, c), chunk_t(q0.w, k + 1, c), q1.w, 0.f);  // z: medium id bits
 }
 
 // Scratch owned by a context, sized for the largest build it will run.

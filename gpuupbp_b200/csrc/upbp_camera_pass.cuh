@@ -7,6 +7,7 @@
 // functs_bp2d.cuh:51-229).
 #pragma once
 
+#include "upbp_build.cuh"
 #include "upbp_queries.cuh"
 
 namespace upbp {
@@ -420,11 +421,11 @@ UPBP_D float3 query_bb1d(const QuerySeg& q, const StateWeights& cw)
 {
     const DeviceParams& p = c_params;
     float3 acc = v3(0.f);
-    beams_near_segment(p.beam_map, q.o, q.d, q.dmin, q.dmax, p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0,
+    beams_near_segment(p.beam_map, q.o, q.d, q.dmin, q.dmax, p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0, q.med,
                        [&](unsigned b, float bb, float st, float t1, float t2) {
                            Beam lb;
                            load_beam(p.beams + b, lb);
-                           if (lb.med == q.med) acc += eval_bb1d(q, cw, lb, bb, st, t1, t2);
+                           acc += eval_bb1d(q, cw, lb, bb, st, t1, t2);
                        });
     return acc;
 }
@@ -502,7 +503,8 @@ __global__ void __launch_bounds__(128) segment_query_kernel()
 {
     const DeviceParams& p = c_params;
     const unsigned n = min(*p.queue_count, p.seg_capacity);
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const unsigned k = p.seg_order ? __ldg(&p.seg_order[j]) : j;
         const float4* r = p.seg_queue[k].q;
         const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]), q2 = __ldg(&r[2]), q3 = __ldg(&r[3]);
         const float4 q4 = __ldg(&r[4]), q5 = __ldg(&r[5]), q6 = __ldg(&r[6]), q7 = __ldg(&r[7]);
@@ -553,7 +555,8 @@ __global__ void __launch_bounds__(128) point_query_kernel()
 {
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[1], p.pt_capacity);
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const unsigned k = p.pt_order ? __ldg(&p.pt_order[j]) : j;
         const float4 q8 = __ldg(&p.pt_queue[k].q8);
         if (!(fbits(q8.y) & kKind)) continue;
         LightVertex cv;
@@ -745,6 +748,29 @@ __global__ void __launch_bounds__(128, 4) camera_pass_kernel()
     atomicAdd(&p.cam_fb[3 * target + 0], color.x);
     atomicAdd(&p.cam_fb[3 * target + 1], color.y);
     atomicAdd(&p.cam_fb[3 * target + 2], color.z);
+}
+
+// Morton keys of the query records (segment midpoint / vertex position in
+// the scene's bounding cube), so the query kernels walk spatially coherent
+// warps through the photon maps.
+template <bool kSeg>
+__global__ void k_query_keys(unsigned n, unsigned* keys, unsigned* vals)
+{
+    const DeviceParams& p = c_params;
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float3 x;
+    if (kSeg) {
+        const float4 q0 = p.seg_queue[k].q[0], q1 = p.seg_queue[k].q[1];
+        const float t = q1.w < 1e30f ? .5f * (q0.w + q1.w) : q0.w;
+        x = xyz(q0) + xyz(q1) * t;
+    } else {
+        x = xyz(p.pt_queue[k].v.q[0]);
+    }
+    const float inv = .5f / p.scene_radius;
+    const float3 u = (x - p.scene_center) * inv + v3(.5f);
+    keys[k] = morton3(u);
+    vals[k] = k;
 }
 
 // Adds the camera image into the iteration image (which holds the light

@@ -75,7 +75,7 @@ __global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* co
                             [&](unsigned s, float, float) { rec(s); });
         break;
     case 3:
-        beams_near_segment(p.beam_map, x, d, r[6], r[7], p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0,
+        beams_near_segment(p.beam_map, x, d, r[6], r[7], p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0, -1,
                            [&](unsigned b, float, float, float, float) { rec(b); });
         break;
     default:
@@ -130,6 +130,11 @@ struct upbp_ctx {
     unsigned* d_qcount = nullptr;
     float* d_cam_fb = nullptr;
     unsigned h_qcount[2] = {0, 0};
+    // Morton sort of the query records: keys/values and their alternates per queue
+    unsigned* d_sort[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+    unsigned sort_capacity[2] = {0, 0};
+    void* d_sort_temp = nullptr;
+    size_t sort_temp_bytes = 0;
     BuildScratch sc;
     float r0[5] = {0, 0, 0, 0, 0};  // bb1d bp2d pb2d pp3d surf
     float bb1d_used = 0.f;
@@ -269,6 +274,45 @@ void free_scratch(BuildScratch& sc)
 }
 
 float relative_radius(float r, float scene_radius) { return r < 0.f ? -r * scene_radius : r; }
+
+// Sort buffers for queue q (0 segment, 1 point) of at least n records.
+int ensure_sort(upbp_ctx* c, int q, unsigned n)
+{
+    if (n <= c->sort_capacity[q]) return UPBP_OK;
+    for (auto& b : c->d_sort[q]) {
+        cudaFree(b);
+        UPBP_CK(dalloc(&b, n));
+    }
+    c->sort_capacity[q] = n;
+    cub::DoubleBuffer<unsigned> kb(c->d_sort[q][0], c->d_sort[q][1]), vb(c->d_sort[q][2], c->d_sort[q][3]);
+    size_t bytes = 0;
+    UPBP_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, (int)n, 0, 30));
+    if (bytes > c->sort_temp_bytes) {
+        cudaFree(c->d_sort_temp);
+        UPBP_CK(cudaMalloc(&c->d_sort_temp, bytes));
+        c->sort_temp_bytes = bytes;
+    }
+    return UPBP_OK;
+}
+
+// Sorts queue q's n records into Morton order; returns the order array.
+int sort_queries(upbp_ctx* c, int q, unsigned n, const unsigned** order)
+{
+    *order = nullptr;
+    if (n < 2) return UPBP_OK;
+    if (ensure_sort(c, q, n) != UPBP_OK) return UPBP_ERR_CUDA;
+    unsigned** b = c->d_sort[q];
+    if (q == 0)
+        k_query_keys<true><<<(n + 255) / 256, 256, 0, c->st>>>(n, b[0], b[2]);
+    else
+        k_query_keys<false><<<(n + 255) / 256, 256, 0, c->st>>>(n, b[0], b[2]);
+    UPBP_CK(cudaGetLastError());
+    cub::DoubleBuffer<unsigned> kb(b[0], b[1]), vb(b[2], b[3]);
+    size_t tb = c->sort_temp_bytes;
+    UPBP_CK(cub::DeviceRadixSort::SortPairs(c->d_sort_temp, tb, kb, vb, (int)n, 0, 30, c->st));
+    *order = vb.Current();
+    return UPBP_OK;
+}
 
 // Grows the chunked beam-map buffers (and the build scratch) to n chunks.
 int ensure_chunks(upbp_ctx* c, unsigned n)
@@ -677,6 +721,17 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     const bool run_surf = P.trace_camera_paths && P.build_surf && P.n_surface > 0 && npt > 0;
     const bool run_pp3d = P.trace_camera_paths && P.build_pp3d && P.n_medium > 0 && npt > 0;
     const bool run_bp2d = P.trace_camera_paths && P.build_bp2d && P.n_beams > 0 && npt > 0;
+    // Morton order of the query records for coherent traversal
+    {
+        const unsigned* so = nullptr;
+        const unsigned* po = nullptr;
+        if ((run_pb2d || run_bb1d) && sort_queries(c, 0, nseg, &so) != UPBP_OK) return UPBP_ERR_CUDA;
+        if ((run_surf || run_pp3d || run_bp2d) && sort_queries(c, 1, npt, &po) != UPBP_OK) return UPBP_ERR_CUDA;
+        P.seg_order = so;
+        P.pt_order = po;
+        launches += (so ? 1 : 0) + (po ? 1 : 0);
+        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+    }
     if (run_pb2d) {
         UPBP_CK(set_work(kKernPb2d));
         segment_query_kernel<false><<<grid_for(nseg), 128, 0, c->st>>>();
@@ -868,7 +923,9 @@ extern "C" void upbp_destroy(upbp_ctx* c)
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
                     c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
-                    c->d_qcount, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue};
+                    c->d_qcount, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
+                    c->d_sort[0][2], c->d_sort[0][3], c->d_sort[1][0], c->d_sort[1][1], c->d_sort[1][2],
+                    c->d_sort[1][3], c->d_sort_temp};
     for (void* b : bufs)
         if (b) cudaFree(b);
     free_scratch(c->sc);

@@ -144,7 +144,7 @@ struct PointMap {
 
 // Beam map: BVH over beam chunks (sub-segments of each beam) in leaf order.
 //   seg[3i] = (origin.xyz, length), seg[3i+1] = (direction.xyz, beam index bits),
-//   seg[3i+2] = (t0, t1) of the beam chunk this leaf covers
+//   seg[3i+2] = (t0, t1) of the beam chunk this leaf covers, beam medium id bits
 struct BeamMap {
     BvhView bvh;
     const float4* seg;
@@ -212,6 +212,8 @@ struct DeviceParams {
     PointQueryRec* pt_queue;
     unsigned pt_capacity;
     unsigned* queue_count;            // [0] segment queries, [1] point queries
+    const unsigned* seg_order;        // processing order of segment queries (Morton order of the midpoint)
+    const unsigned* pt_order;         // processing order of point queries (Morton order of the position)
     float* cam_fb;                    // camera-pass image, W*H*3
 };
 

@@ -63,10 +63,12 @@ UPBP_D void points_near_segment(const PointMap& map, float3 o, float3 d, float t
 // need_mask only beams of the first bb1d_used_light_subpath_count light
 // paths.  f(beam index, distance, sin theta, t along query, t along beam).
 // Beams are stored as chunks; a beam is reported only through the chunk that
-// holds its closest point, so each beam appears at most once.
+// holds its closest point, so each beam appears at most once.  med >= 0
+// skips beams of other media before the predicate (the estimator only merges
+// beams in the query segment's medium, functs_bb1d.cuh:66).
 template <class F>
 UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmin, float tmax, float pad_r, float r2,
-                               bool need_mask, F&& f)
+                               bool need_mask, int med, F&& f)
 {
     const float3 inv = safe_inv(d);
     const float pad = pad_r * 1.0001f + 1e-7f;
@@ -77,7 +79,9 @@ UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmi
             const float4 s1 = __ldg(&map.seg[3 * i + 1]);
             const unsigned bits = fbits(s1.w);
             if (need_mask && !(bits >> 31)) return true;
-            const float4 s0 = __ldg(&map.seg[3 * i]), s2 = __ldg(&map.seg[3 * i + 2]);
+            const float4 s2 = __ldg(&map.seg[3 * i + 2]);
+            if (med >= 0 && (int)fbits(s2.z) != med) return true;
+            const float4 s0 = __ldg(&map.seg[3 * i]);
             float bb, st, t1, t2;
             cand++;
             if (pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, bb, st, t1, t2) && t2 >= s2.x &&
