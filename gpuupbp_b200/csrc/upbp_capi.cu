@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -909,6 +910,69 @@ extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uin
     cudaFree(dq);
     cudaFree(dc);
     cudaFree(di);
+    return UPBP_OK;
+}
+
+// ---- neighbour-set query without device allocation --------------------
+// upbp_debug_query stages the queries, counts and ids in buffers it
+// allocates and frees on every call.  Some callers cannot do that: a host
+// application that gives the renderer a fixed device-memory budget at
+// creation, or one whose other streams must not be stalled by the
+// device-wide synchronisation cudaFree implies.  This variant stages
+// everything in one statically allocated device array instead.  The array
+// is shared by every call in the process: two calls whose copies or kernels
+// overlap on the GPU overwrite each other's data, so callers serialise them.
+constexpr unsigned kStaticQueryMax = 4096;  // queries per call
+constexpr unsigned kStaticIdsMax = 256;     // ids per query
+constexpr size_t kStaticQueryBytes = (size_t)kStaticQueryMax * 8 * sizeof(float);
+constexpr size_t kStaticCountBytes = (size_t)kStaticQueryMax * sizeof(unsigned);
+constexpr size_t kStaticIdBytes = (size_t)kStaticQueryMax * kStaticIdsMax * sizeof(unsigned);
+// About 4.2 MB; every GPU that loads the library holds it until exit.
+static __device__ __align__(256) unsigned char g_query_scratch[kStaticQueryBytes + kStaticCountBytes + kStaticIdBytes];
+
+namespace {
+std::mutex g_scratch_mu;
+unsigned char* g_scratch_addr[64] = {};  // device address of g_query_scratch, per device
+}  // namespace
+
+extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queries, uint32_t n, uint32_t* counts,
+                                       uint32_t* ids, uint32_t ids_per_query)
+{
+    if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
+    if (n > kStaticQueryMax || ids_per_query > kStaticIdsMax) {
+        upbp_host::set_error("upbp_debug_query_static: at most " + std::to_string(kStaticQueryMax) +
+                             " queries and " + std::to_string(kStaticIdsMax) + " ids per query");
+        return UPBP_ERR_ARGS;
+    }
+    if (n == 0) return UPBP_OK;
+    int dev = 0;
+    UPBP_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return UPBP_ERR_ARGS;
+    unsigned char* base = nullptr;
+    {
+        // first call on a device: resolve the array's device address (the
+        // host-side symbol is only a stand-in and must never reach a kernel)
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        if (!g_scratch_addr[dev]) {
+            void* ptr = nullptr;
+            UPBP_CK(cudaGetSymbolAddress(&ptr, g_query_scratch));
+            g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
+        }
+        base = g_scratch_addr[dev];
+    }
+    float* dq = reinterpret_cast<float*>(base);
+    unsigned* dc = reinterpret_cast<unsigned*>(base + kStaticQueryBytes);
+    unsigned* di = reinterpret_cast<unsigned*>(base + kStaticQueryBytes + kStaticCountBytes);
+    const size_t id_bytes = (size_t)n * ids_per_query * sizeof(unsigned);
+    UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    // the array keeps the previous call's ids; clear this call's id slots
+    if (id_bytes) UPBP_CK(cudaMemsetAsync(di, 0, id_bytes, c->st));
+    UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
+    k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
+    UPBP_CK(cudaGetLastError());
+    UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    if (ids && id_bytes) UPBP_CK(cudaMemcpyAsync(ids, di, id_bytes, cudaMemcpyDeviceToHost, c->st));
+    UPBP_CK(cudaStreamSynchronize(c->st));
     return UPBP_OK;
 }
 

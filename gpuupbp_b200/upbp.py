@@ -70,7 +70,7 @@ WORK_NAMES = ["nodes", "tris", "rays", "point_cand", "point_hit", "beam_cand", "
 EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_predefined", "upbp_scene_get_desc",
            "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
            "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
-           "upbp_debug_photons", "upbp_debug_query"]
+           "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static"]
 
 _lib = None
 
@@ -102,6 +102,7 @@ def load_library(path: str = LIB_PATH):
     L.upbp_last_error.restype = ctypes.c_char_p
     L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]
     L.upbp_debug_query.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
+    L.upbp_debug_query_static.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
     _lib = L
     return L
 

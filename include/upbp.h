@@ -231,6 +231,23 @@ int upbp_debug_photons(upbp_ctx* ctx, int kind, float* out, uint32_t capacity, u
 int upbp_debug_query(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, uint32_t* counts, uint32_t* ids,
                      uint32_t ids_per_query);
 
+/* Same neighbour-set query as upbp_debug_query, for callers that cannot
+ * allocate device memory per call (a fixed device-memory budget, or other
+ * streams that must not be stalled by the device-wide synchronisation of
+ * cudaFree).  No counterpart in the reference.  Allocates nothing: queries,
+ * counts and ids are staged in one static device array of about 4.2 MB that
+ * every GPU loading the library holds until exit.  Limits: n <= 4096 queries
+ * and ids_per_query <= 256, otherwise UPBP_ERR_ARGS.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (several threads, or contexts on one device)
+ * race and must be serialised by the caller.  Nothing in the array has to
+ * start at zero: every call writes all n counts and clears its own n x
+ * ids_per_query id slots before the search, so id slots beyond counts[i]
+ * are returned as 0 whatever an earlier call left there. */
+int upbp_debug_query_static(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, uint32_t* counts,
+                            uint32_t* ids, uint32_t ids_per_query);
+
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */
 void* upbp_get_stream(upbp_ctx* ctx);
