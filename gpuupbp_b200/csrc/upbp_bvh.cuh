@@ -5,6 +5,8 @@
 // remaining subtree (never an unbounded loop).
 #pragma once
 
+#include <climits>
+
 #include "upbp_device.cuh"
 
 namespace upbp {
@@ -107,6 +109,57 @@ UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& l
         }
         node = stack[--sp];
     }
+}
+
+// Resumable form of bvh_walk: walk_step() advances by exactly one internal
+// node or one leaf, so a warp can move all its lanes in lock step and give a
+// lane that finished its query a new one (the range-query search kernels).
+// Visits the same leaves in the same order as bvh_walk.
+constexpr int kWalkDone = INT_MIN;
+
+struct WalkState {
+    int node;  // next node: >= 0 internal, < 0 ~leaf, kWalkDone when finished
+    int sp;
+    int stack[kStackDepth];
+};
+
+UPBP_D void walk_begin(WalkState& s, const BvhView& bvh)
+{
+    s.sp = 0;
+    s.node = bvh.count == 0 ? kWalkDone : (bvh.count > 1 ? 0 : ~0);
+}
+
+UPBP_D void walk_pop(WalkState& s) { s.node = s.sp > 0 ? s.stack[--s.sp] : kWalkDone; }
+
+// One step of a walk with s.node != kWalkDone.  Returns the sorted index of
+// the leaf this step reached, or -1 after an internal node.
+template <class BoxTest>
+UPBP_D int walk_step(WalkState& s, const BvhView& bvh, float pad, BoxTest&& test_box, bool& overflow,
+                     unsigned& visits)
+{
+    const int node = s.node;
+    if (node < 0) {
+        walk_pop(s);
+        return ~node;
+    }
+    visits++;
+    const NodeBoxes nb = load_node(bvh.nodes, node);
+    const bool hl = test_box(nb.llo, nb.lhi, pad);
+    const bool hr = test_box(nb.rlo, nb.rhi, pad);
+    if (hl && hr) {
+        if (s.sp < kStackDepth)
+            s.stack[s.sp++] = nb.r;
+        else
+            overflow = true;
+        s.node = nb.l;
+    } else if (hl) {
+        s.node = nb.l;
+    } else if (hr) {
+        s.node = nb.r;
+    } else {
+        walk_pop(s);
+    }
+    return -1;
 }
 
 // Moller-Trumbore, double sided; identical arithmetic to the oracle's test.

@@ -496,8 +496,54 @@ UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int n
     }
 }
 
-// PB2D (kBb1d = false) or BB1D (kBb1d = true) for one segment-query record;
-// adds weight * normalization * estimate into the camera image.
+// Unpacks segment-query record k: the query, the camera-side MIS state, the
+// path weight before the segment and the packed pixel / camera path length.
+UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& weight, unsigned& pk)
+{
+    const float4* r = c_params.seg_queue[k].q;
+    const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]), q2 = __ldg(&r[2]), q3 = __ldg(&r[3]);
+    const float4 q4 = __ldg(&r[4]), q5 = __ldg(&r[5]), q6 = __ldg(&r[6]), q7 = __ldg(&r[7]);
+    q.o = xyz(q0);
+    q.dmin = q0.w;
+    q.d = xyz(q1);
+    q.dmax = q1.w;
+    q.med = (int)fbits(q2.w);
+    weight = xyz(q2);
+    q.for_pdf = q3.x;
+    q.rev_pdf = q3.y;
+    q.flags = fbits(q3.z);
+    pk = fbits(q3.w);
+    q.cam_path_length = pk & 0xffu;
+    cw.w.d_shared = q4.x;
+    cw.w.d_bpt = q4.y;
+    cw.w.d_pde = q4.z;
+    cw.w.for_inv = q4.w;
+    cw.w.rev_inv = q5.x;
+    cw.w.for_ratio = q5.y;
+    cw.w.rev_ratio = q5.z;
+    const unsigned bits = fbits(q5.w);
+    cw.w.prev_in_medium = bits & 1u;
+    cw.w.prev_specular = (bits >> 1) & 1u;
+    cw.last_sin_theta = q6.x;
+    cw.d_bpt_a = q6.y;
+    cw.d_bpt_b = q6.z;
+    cw.d_pde_a = q6.w;
+    cw.d_pde_b = q7.x;
+}
+
+// Adds c into pixel px of the camera image (pixel 0xffffff: no pixel).
+UPBP_D void splat_camera(unsigned px, float3 c)
+{
+    if ((c.x != 0.f || c.y != 0.f || c.z != 0.f) && px != 0xffffffu) {
+        float* fb = c_params.cam_fb + 3 * (size_t)px;
+        atomicAdd(fb + 0, c.x);
+        atomicAdd(fb + 1, c.y);
+        atomicAdd(fb + 2, c.z);
+    }
+}
+
+// PB2D (kBb1d = false) or BB1D (kBb1d = true) for one segment-query record
+// per thread; adds weight * normalization * estimate into the camera image.
 template <bool kBb1d>
 __global__ void __launch_bounds__(128) segment_query_kernel()
 {
@@ -505,45 +551,149 @@ __global__ void __launch_bounds__(128) segment_query_kernel()
     const unsigned n = min(*p.queue_count, p.seg_capacity);
     for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const unsigned k = p.seg_order ? __ldg(&p.seg_order[j]) : j;
-        const float4* r = p.seg_queue[k].q;
-        const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]), q2 = __ldg(&r[2]), q3 = __ldg(&r[3]);
-        const float4 q4 = __ldg(&r[4]), q5 = __ldg(&r[5]), q6 = __ldg(&r[6]), q7 = __ldg(&r[7]);
         QuerySeg q;
-        q.o = xyz(q0);
-        q.dmin = q0.w;
-        q.d = xyz(q1);
-        q.dmax = q1.w;
-        q.med = (int)fbits(q2.w);
-        q.for_pdf = q3.x;
-        q.rev_pdf = q3.y;
-        q.flags = fbits(q3.z);
-        const unsigned pk = fbits(q3.w);
-        q.cam_path_length = pk & 0xffu;
         StateWeights cw;
-        cw.w.d_shared = q4.x;
-        cw.w.d_bpt = q4.y;
-        cw.w.d_pde = q4.z;
-        cw.w.for_inv = q4.w;
-        cw.w.rev_inv = q5.x;
-        cw.w.for_ratio = q5.y;
-        cw.w.rev_ratio = q5.z;
-        const unsigned bits = fbits(q5.w);
-        cw.w.prev_in_medium = bits & 1u;
-        cw.w.prev_specular = (bits >> 1) & 1u;
-        cw.last_sin_theta = q6.x;
-        cw.d_bpt_a = q6.y;
-        cw.d_bpt_b = q6.z;
-        cw.d_pde_a = q6.w;
-        cw.d_pde_b = q7.x;
+        float3 weight;
+        unsigned pk;
+        load_seg_query(k, q, cw, weight, pk);
         const float3 est = kBb1d ? query_bb1d(q, cw) : query_pb2d(q, cw);
         const float norm = kBb1d ? p.bb1d_normalization : p.pb2d_normalization;
-        const float3 c = xyz(q2) * norm * est;
-        if ((c.x != 0.f || c.y != 0.f || c.z != 0.f) && (pk >> 8) != 0xffffffu) {
-            const unsigned px = pk >> 8;
-            atomicAdd(&p.cam_fb[3 * px + 0], c.x);
-            atomicAdd(&p.cam_fb[3 * px + 1], c.y);
-            atomicAdd(&p.cam_fb[3 * px + 2], c.z);
+        splat_camera(pk >> 8, weight * norm * est);
+    }
+}
+
+// BB1D in two kernels.  A long query segment crosses hundreds of beam chunks
+// and a short one a few, and every accepted beam costs a full MIS evaluation;
+// run inside one walk per thread, both leave most lanes of a warp idle.
+//
+// bb1d_search_kernel: persistent warps walk the beam map with one query per
+// lane, one node or leaf per step; a lane whose query is finished takes the
+// next one in Morton order from a global counter, so lanes stay busy until
+// the queue is empty.  Accepted (query, beam) pairs are gathered per warp in
+// shared memory and written out 32 at a time (one atomic per 32 hits).  When
+// the list is full the pairs past the capacity are dropped but still counted,
+// and the host grows the list and repeats the search.
+constexpr int kSearchWarps = 4;
+
+__global__ void __launch_bounds__(128) bb1d_search_kernel()
+{
+    const DeviceParams& p = c_params;
+    __shared__ uint2 s_qb[kSearchWarps][64];
+    __shared__ float4 s_geom[kSearchWarps][64];
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned n = min(p.queue_count[0], p.seg_capacity);
+    const BvhView bvh = p.beam_map.bvh;
+    const float pad = beam_map_pad(p.rad_beam);
+    const float r2 = p.radius_bb1d_2;
+    const bool need_mask = p.do_bp2d != 0;
+    WalkState s;
+    s.node = kWalkDone;
+    float3 o = v3(0.f), d = v3(0.f), inv = v3(0.f);
+    float tmin = 0.f, tmax = 0.f;
+    int med = 0;
+    unsigned qk = 0;
+    bool exhausted = false, overflow = false;
+    unsigned fill = 0;  // same value in every lane
+    unsigned visits = 0, cand = 0, hits = 0;
+    for (;;) {
+        const bool idle = s.node == kWalkDone;
+        const unsigned want = __ballot_sync(~0u, idle && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned base = 0;
+            if ((int)lane == leader) base = atomicAdd(&p.hit_count[1], (unsigned)__popc(want));
+            base = __shfl_sync(~0u, base, leader);
+            if (idle && !exhausted) {
+                const unsigned j = base + __popc(want & below);
+                if (j < n) {
+                    qk = p.seg_order ? __ldg(&p.seg_order[j]) : j;
+                    const float4* r = p.seg_queue[qk].q;
+                    const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
+                    o = xyz(q0);
+                    tmin = q0.w;
+                    d = xyz(q1);
+                    tmax = q1.w;
+                    med = (int)fbits(__ldg(&r[2]).w);
+                    inv = safe_inv(d);
+                    walk_begin(s, bvh);
+                } else {
+                    exhausted = true;
+                }
+            }
         }
+        if (__all_sync(~0u, s.node == kWalkDone)) break;
+        BeamSegHit h;
+        bool hit = false;
+        if (s.node != kWalkDone) {
+            const int leaf = walk_step(
+                s, bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
+                overflow, visits);
+            if (leaf >= 0) hit = beam_chunk_vs_segment(p.beam_map, leaf, o, d, tmin, tmax, r2, need_mask, med, cand, h);
+        }
+        const unsigned hm = __ballot_sync(~0u, hit);
+        if (hm) {
+            if (hit) {
+                const unsigned pos = fill + __popc(hm & below);
+                s_qb[warp][pos] = make_uint2(qk, h.beam);
+                s_geom[warp][pos] = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
+                hits++;
+            }
+            fill += __popc(hm);
+            if (fill >= 32) {
+                __syncwarp();
+                unsigned base = 0;
+                if (lane == 0) base = atomicAdd(&p.hit_count[0], 32u);
+                base = __shfl_sync(~0u, base, 0);
+                if (base + lane < p.hit_capacity) {
+                    p.hit_qb[base + lane] = s_qb[warp][lane];
+                    p.hit_geom[base + lane] = s_geom[warp][lane];
+                }
+                __syncwarp();
+                if (lane + 32 < fill) {
+                    s_qb[warp][lane] = s_qb[warp][lane + 32];
+                    s_geom[warp][lane] = s_geom[warp][lane + 32];
+                }
+                fill -= 32;
+                __syncwarp();
+            }
+        }
+    }
+    __syncwarp();
+    if (fill) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(&p.hit_count[0], fill);
+        base = __shfl_sync(~0u, base, 0);
+        if (lane < fill && base + lane < p.hit_capacity) {
+            p.hit_qb[base + lane] = s_qb[warp][lane];
+            p.hit_geom[base + lane] = s_geom[warp][lane];
+        }
+    }
+    count_work(kCtrNodes, visits);
+    count_work(kCtrBeamCand, cand);
+    count_work(kCtrBeamHit, hits);
+    if (overflow) flag_status(kErrTraversalStack);
+}
+
+// bb1d_eval_kernel: one accepted (query, beam) pair per thread, so every lane
+// runs the same MIS evaluation; adds weight * normalization * estimate into
+// the camera image.
+__global__ void __launch_bounds__(128) bb1d_eval_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned n = min(p.hit_count[0], p.hit_capacity);
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint2 qb = __ldg(&p.hit_qb[j]);
+        const float4 g = __ldg(&p.hit_geom[j]);
+        QuerySeg q;
+        StateWeights cw;
+        float3 weight;
+        unsigned pk;
+        load_seg_query(qb.x, q, cw, weight, pk);
+        Beam lb;
+        load_beam(p.beams + qb.y, lb);
+        const float3 est = eval_bb1d(q, cw, lb, g.x, g.y, g.z, g.w);
+        splat_camera(pk >> 8, weight * p.bb1d_normalization * est);
     }
 }
 

@@ -131,6 +131,13 @@ struct upbp_ctx {
     unsigned* d_qcount = nullptr;
     float* d_cam_fb = nullptr;
     unsigned h_qcount[2] = {0, 0};
+    // BB1D hit list (search -> evaluation)
+    uint2* d_hit_qb = nullptr;
+    float4* d_hit_geom = nullptr;
+    unsigned hit_capacity = 0;
+    unsigned* d_hit_count = nullptr;
+    unsigned h_hit_count[2] = {0, 0};
+    int search_grid = 0;
     // Morton sort of the query records: keys/values and their alternates per queue
     unsigned* d_sort[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
     unsigned sort_capacity[2] = {0, 0};
@@ -337,6 +344,23 @@ int ensure_chunks(upbp_ctx* c, unsigned n)
     return UPBP_OK;
 }
 
+// Room for n BB1D hits (24 bytes each).
+int ensure_hits(upbp_ctx* c, size_t n)
+{
+    if (n <= c->hit_capacity) return UPBP_OK;
+    const size_t cap = std::min<size_t>(std::max<size_t>(n + n / 4, 1u << 20), 0x7fffffffu);
+    UPBP_CK(cudaStreamSynchronize(c->st));
+    cudaFree(c->d_hit_qb);
+    cudaFree(c->d_hit_geom);
+    c->d_hit_qb = nullptr;
+    c->d_hit_geom = nullptr;
+    c->hit_capacity = 0;
+    UPBP_CK(dalloc(&c->d_hit_qb, cap));
+    UPBP_CK(dalloc(&c->d_hit_geom, cap));
+    c->hit_capacity = (unsigned)cap;
+    return UPBP_OK;
+}
+
 }  // namespace
 
 extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upbp_ctx** out)
@@ -502,7 +526,15 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     UPBP_CK(dalloc(&c->d_status, 1));
     UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
     UPBP_CK(dalloc(&c->d_qcount, 2));
+    UPBP_CK(dalloc(&c->d_hit_count, 2));
     UPBP_CK(dalloc(&c->d_cam_fb, npx));
+    {
+        int dev = 0, sms = 0, per_sm = 0;
+        UPBP_CK(cudaGetDevice(&dev));
+        UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb1d_search_kernel, 128, 0));
+        c->search_grid = std::max(1, sms * std::max(1, per_sm));
+    }
     c->seg_capacity = std::max(1024u, 4 * P.screen_pixel_count);
     c->pt_capacity = std::max(1024u, 3 * P.screen_pixel_count);
     UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
@@ -540,6 +572,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     P.pt_queue = c->d_pt_queue;
     P.pt_capacity = c->pt_capacity;
     P.queue_count = c->d_qcount;
+    P.hit_count = c->d_hit_count;
     P.cam_fb = c->d_cam_fb;
     UPBP_CK(cudaStreamSynchronize(c->st));
     *out = c;
@@ -740,9 +773,33 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     }
     UPBP_CK(cudaEventRecord(ev[4], c->st));
     if (run_bb1d) {
+        // search: (query, beam) pairs into the hit list; a list that was too
+        // small is grown and the search repeated (it is a pure function of
+        // the queries and the beam map)
         UPBP_CK(set_work(kKernBb1d));
-        segment_query_kernel<true><<<grid_for(nseg), 128, 0, c->st>>>();
-        launches++;
+        if (c->hit_capacity == 0 && ensure_hits(c, (size_t)nseg * 32) != UPBP_OK) return UPBP_ERR_CUDA;
+        for (int attempt = 0; attempt < 2; attempt++) {
+            UPBP_CK(cudaMemsetAsync(c->d_hit_count, 0, 2 * sizeof(unsigned), c->st));
+            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernBb1d * kCtrCount, 0,
+                                    kCtrCount * sizeof(unsigned long long), c->st));
+            P.hit_qb = c->d_hit_qb;
+            P.hit_geom = c->d_hit_geom;
+            P.hit_capacity = c->hit_capacity;
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+            bb1d_search_kernel<<<c->search_grid, 128, 0, c->st>>>();
+            launches++;
+            UPBP_CK(cudaGetLastError());
+            UPBP_CK(cudaMemcpyAsync(c->h_hit_count, c->d_hit_count, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                    c->st));
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            if (c->h_hit_count[0] <= c->hit_capacity) break;
+            if (ensure_hits(c, c->h_hit_count[0]) != UPBP_OK) return UPBP_ERR_CUDA;
+        }
+        const unsigned nh = std::min(c->h_hit_count[0], c->hit_capacity);
+        if (nh > 0) {
+            bb1d_eval_kernel<<<grid_for(nh), 128, 0, c->st>>>();
+            launches++;
+        }
     }
     UPBP_CK(cudaEventRecord(ev[5], c->st));
     if (run_surf) {
@@ -987,7 +1044,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
                     c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
-                    c->d_qcount, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
+                    c->d_qcount, c->d_hit_count, c->d_hit_qb, c->d_hit_geom, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
                     c->d_sort[0][2], c->d_sort[0][3], c->d_sort[1][0], c->d_sort[1][1], c->d_sort[1][2],
                     c->d_sort[1][3], c->d_sort_temp};
     for (void* b : bufs)

@@ -215,6 +215,13 @@ struct DeviceParams {
     const unsigned* seg_order;        // processing order of segment queries (Morton order of the midpoint)
     const unsigned* pt_order;         // processing order of point queries (Morton order of the position)
     float* cam_fb;                    // camera-pass image, W*H*3
+
+    // BB1D hit list: the search kernel appends every (segment query, beam)
+    // pair the predicate accepts; the evaluation kernel consumes the list.
+    uint2* hit_qb;                    // (segment-query record index, beam index)
+    float4* hit_geom;                 // (distance, sin theta, t along the query, t along the beam)
+    unsigned hit_capacity;
+    unsigned* hit_count;              // [0] hits found (may exceed capacity), [1] next query to hand out
 };
 
 // Launch parameters of the running pass, uploaded before each launch.

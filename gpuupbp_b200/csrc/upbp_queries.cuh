@@ -66,34 +66,61 @@ UPBP_D void points_near_segment(const PointMap& map, float3 o, float3 d, float t
 // holds its closest point, so each beam appears at most once.  med >= 0
 // skips beams of other media before the predicate (the estimator only merges
 // beams in the query segment's medium, functs_bb1d.cuh:66).
+struct BeamSegHit {
+    unsigned beam;
+    float dist, sin_theta, t1, t2;
+};
+
+// The BB1D test of one beam-map leaf against a query segment: the path mask,
+// the medium filter, the exact beam-beam predicate and the rule that only
+// the chunk holding the beam's closest point reports it.  cand counts the
+// leaves that reach the predicate.
+UPBP_D bool beam_chunk_vs_segment(const BeamMap& map, int i, float3 o, float3 d, float tmin, float tmax, float r2,
+                                  bool need_mask, int med, unsigned& cand, BeamSegHit& h)
+{
+    const float4 s1 = __ldg(&map.seg[3 * i + 1]);
+    const unsigned bits = fbits(s1.w);
+    if (need_mask && !(bits >> 31)) return false;
+    const float4 s2 = __ldg(&map.seg[3 * i + 2]);
+    if (med >= 0 && (int)fbits(s2.z) != med) return false;
+    const float4 s0 = __ldg(&map.seg[3 * i]);
+    cand++;
+    if (pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, h.dist, h.sin_theta, h.t1, h.t2) &&
+        h.t2 >= s2.x && h.t2 < s2.y) {
+        h.beam = bits & 0x7fffffffu;
+        return true;
+    }
+    return false;
+}
+
+// Box dilation of beam-map walks: the beam radius with a small margin, so
+// rounding in the box test never drops a leaf the predicate accepts.
+UPBP_D float beam_map_pad(float pad_r) { return pad_r * 1.0001f + 1e-7f; }
+
 template <class F>
 UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmin, float tmax, float pad_r, float r2,
                                bool need_mask, int med, F&& f)
 {
     const float3 inv = safe_inv(d);
-    const float pad = pad_r * 1.0001f + 1e-7f;
-    unsigned cand = 0, hits = 0;
-    const bool ok = bvh_walk(
-        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
-        [&](int i) {
-            const float4 s1 = __ldg(&map.seg[3 * i + 1]);
-            const unsigned bits = fbits(s1.w);
-            if (need_mask && !(bits >> 31)) return true;
-            const float4 s2 = __ldg(&map.seg[3 * i + 2]);
-            if (med >= 0 && (int)fbits(s2.z) != med) return true;
-            const float4 s0 = __ldg(&map.seg[3 * i]);
-            float bb, st, t1, t2;
-            cand++;
-            if (pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, bb, st, t1, t2) && t2 >= s2.x &&
-                t2 < s2.y) {
-                hits++;
-                f(bits & 0x7fffffffu, bb, st, t1, t2);
-            }
-            return true;
-        });
+    const float pad = beam_map_pad(pad_r);
+    unsigned cand = 0, hits = 0, visits = 0;
+    bool overflow = false;
+    WalkState s;
+    walk_begin(s, map.bvh);
+    while (s.node != kWalkDone) {
+        const int leaf = walk_step(
+            s, map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
+            overflow, visits);
+        BeamSegHit h;
+        if (leaf >= 0 && beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, need_mask, med, cand, h)) {
+            hits++;
+            f(h.beam, h.dist, h.sin_theta, h.t1, h.t2);
+        }
+    }
+    count_work(kCtrNodes, visits);
     count_work(kCtrBeamCand, cand);
     count_work(kCtrBeamHit, hits);
-    if (!ok) flag_status(kErrTraversalStack);
+    if (overflow) flag_status(kErrTraversalStack);
 }
 
 // Photon beams whose disc of radius sqrt(r2) contains x (BP2D):
