@@ -117,6 +117,9 @@ def algorithmic_bytes(work: dict, extra: float = 0.0) -> float:
 
 # Bytes of the query records each camera-side kernel writes or reads.
 SEG_RECORD, POINT_RECORD = 128, 144
+# BB1D hit-list entry (query, beam, distance, sin theta, t1, t2), written by
+# the search kernel and read by the evaluation kernel.
+HIT_RECORD = 24
 
 
 def kernel_rooflines(st: dict, pixels: int) -> dict:
@@ -124,9 +127,10 @@ def kernel_rooflines(st: dict, pixels: int) -> dict:
     n = max(1, st["timed_iterations"])
     ms = st["ms_kernel_sum"]
     nseg, npt = st["segment_queries"], st["point_queries"]
+    hits = st["work"]["bb1d_query"]["beam_hit"]
     extra = {"light_pass": 0.0,
              "camera_extend": 12.0 * pixels + SEG_RECORD * nseg + POINT_RECORD * npt,
-             "pb2d_query": SEG_RECORD * nseg, "bb1d_query": SEG_RECORD * nseg,
+             "pb2d_query": SEG_RECORD * nseg, "bb1d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * hits,
              "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt, "bp2d_query": POINT_RECORD * npt}
     out = {}
     for k, w in st["work"].items():
@@ -174,7 +178,7 @@ def run_b200(args) -> dict | None:
     if pg is not None:
         pg.barrier()
         scene = scenes.write_workload("media_field", SCENE_DIR)
-    r = upbp.Renderer(workload_args(scene))
+    r = upbp.Renderer(workload_args(scene, args.res))
     paths_per_iter = r.config.res_x * r.config.res_y + int(r.config.path_count_per_iter)
     stream = torch.cuda.ExternalStream(r.stream_handle())
     # rank r renders iterations r, r+N, ...
@@ -238,7 +242,7 @@ def run_b200(args) -> dict | None:
         "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, OBJ/MTL/AUX)",
-        "config": {"workload": "media_field: 1280x720, 20 displaced icosphere media (1.64M tris), "
+        "config": {"workload": f"media_field: {args.res[0]}x{args.res[1]}, 20 displaced icosphere media (1.64M tris), "
                                "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d, path length 12, 1 light path per pixel",
                    "triangles": int(st["triangle_count"]), "light_paths_per_iter": int(r.config.path_count_per_iter),
                    "camera_paths_per_iter": pixels, "parallelism": f"iterations sharded over {world} rank(s)",
@@ -298,7 +302,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--res", default=f"{RES[0]}x{RES[1]}",
+                    help="image size WxH; smaller sizes are for profiling captures, not bench lines")
     args = ap.parse_args()
+    args.res = tuple(int(v) for v in args.res.lower().split("x"))
     threads = os.cpu_count() or 1
     world, rank, _ = dist_env()
     if args.impl == "reference":
