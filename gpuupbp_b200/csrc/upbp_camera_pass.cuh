@@ -729,175 +729,241 @@ __global__ void __launch_bounds__(128) point_query_kernel()
     }
 }
 
-__global__ void __launch_bounds__(128, 4) camera_pass_kernel()
+// State of one camera subpath between bounces.
+struct CameraLane {
+    PathState s;
+    Rng rng;
+    float3 color;
+    unsigned target;  // pixel the sample lands in, kNoPixel if off screen
+    unsigned ret;     // status of a failed step (0: none)
+    bool origin_in_medium;
+    bool only_spec_surf;
+};
+
+constexpr unsigned kNoPixel = 0xffffffu;
+
+// Starts the camera subpath of `pixel`; false if it ended already.
+UPBP_D bool camera_path_begin(CameraLane& c, unsigned pixel)
 {
     const DeviceParams& p = c_params;
-    const unsigned pixel = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pixel >= p.screen_pixel_count) return;
-
-    VolSeg segs[kMaxVolSegments];
-    LiteSeg lsegs[kMaxVolSegments];
-    Rng rng;
-    rng.init(p.iteration + p.iteration_offset, pixel, 1u);
-    PathState s;
+    c.rng.init(p.iteration + p.iteration_offset, pixel, 1u);
     float2 screen;
-    unsigned ret = generate_camera_sample(screen, pixel, s, rng);
-    float3 color = v3(0.f);
+    c.ret = generate_camera_sample(screen, pixel, c.s, c.rng);
+    c.color = v3(0.f);
     // add_color (frame_buffer.cuh:36-45) targets the pixel of the jittered
     // sample, which float rounding can move to the next pixel or off screen
-    constexpr unsigned kNoPixel = 0xffffffu;
-    unsigned target = kNoPixel;
+    c.target = kNoPixel;
     if (!(screen.x < 0.f || screen.x >= (float)p.res_x || screen.y < 0.f || screen.y >= (float)p.res_y))
-        target = (unsigned)int(screen.x) + (unsigned)int(screen.y) * p.res_x;
-    bool origin_in_medium = false;
-    bool only_spec_surf = (p.estimator_techniques & (kPrevious | kCompatible)) != 0;
+        c.target = (unsigned)int(screen.x) + (unsigned)int(screen.y) * p.res_x;
+    c.origin_in_medium = false;
+    c.only_spec_surf = (p.estimator_techniques & (kPrevious | kCompatible)) != 0;
+    return c.ret == 0;
+}
 
-    for (; ret == 0; s.path_length++) {
-        const float3 ro = s.origin, rd = s.dir;
-        Isect isect;
-        isect.dist = kInfinity;
-        isect.mat = isect.med = isect.light = -1;
-        isect.normal = v3(0.f);
-        isect.enter = false;
-        int nseg = 0, nlseg = 0;
-        bool hit;
-        ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
-                              segs, nseg, lsegs, nlseg, rng);
-        if (ret) break;
-        if ((p.build_pb2d && p.n_medium > 0) || (p.build_bb1d && p.n_beams > 0)) {
-            const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
-            const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
-            emit_segment_queries(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags, s.path_length, s.sw, s.throughput,
-                                 target);
+// One bounce of a camera subpath (one iteration of the path loop of
+// __raygen__trace_camera, trace_camera.cu:79-381); false when the path ends.
+UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
+{
+    const DeviceParams& p = c_params;
+    PathState& s = c.s;
+    Rng& rng = c.rng;
+    float3& color = c.color;
+    const unsigned target = c.target;
+    bool& origin_in_medium = c.origin_in_medium;
+    bool& only_spec_surf = c.only_spec_surf;
+    unsigned& ret = c.ret;
+    const float3 ro = s.origin, rd = s.dir;
+    Isect isect;
+    isect.dist = kInfinity;
+    isect.mat = isect.med = isect.light = -1;
+    isect.normal = v3(0.f);
+    isect.enter = false;
+    int nseg = 0, nlseg = 0;
+    bool hit;
+    ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
+                          segs, nseg, lsegs, nlseg, rng);
+    if (ret) return false;
+    if ((p.build_pb2d && p.n_medium > 0) || (p.build_bb1d && p.n_beams > 0)) {
+        const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
+        const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
+        emit_segment_queries(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags, s.path_length, s.sw, s.throughput,
+                             target);
+    }
+    if (!hit) {
+        if (s.path_length < p.min_path_length) return false;
+        if (p.background_light < 0) return false;
+        if (p.media[p.global_medium].has_attenuation) return false;
+    }
+    float rs_for = 1.f, rs_rev = 1.f;
+    if (nseg > 0) {
+        rs_for = seg_for_pdf(segs, nseg);
+        rs_rev = seg_rev_pdf(segs, nseg);
+        s.throughput *= seg_attenuation(segs, nseg) / rs_for;
+    }
+    if (is_black_or_negative(s.throughput)) return false;
+    VertexWeights& w = s.sw.w;
+    if (s.path_length > 1u) {
+        const float f_i = pde_factor(w.prev_in_medium, w.prev_specular, 1.f / rs_rev, w.rev_ratio, w.for_inv,
+                                     w.for_ratio, s.sw.last_sin_theta);
+        w.d_bpt = s.sw.d_bpt_a * f_i + s.sw.d_bpt_b;
+        w.d_pde = s.sw.d_pde_a * f_i + s.sw.d_pde_b;
+    }
+    w.d_shared /= rs_for;
+    w.d_bpt /= rs_for;
+    w.d_pde /= rs_for;
+    if (!hit) {
+        color += s.throughput * light_hit_radiance(p.lights[p.background_light], s, rs_rev);
+        return false;
+    }
+    Bsdf bsdf;
+    if (isect.on_surface())
+        bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, false, relative_ior(isect, s.stack));
+    else
+        bsdf_setup_medium(bsdf, rd, isect.med, false);
+    if (!bsdf.valid()) return false;
+    float ratio = 0.f;
+    if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
+    const float3 hitpoint = ro + rd * isect.dist;
+    origin_in_medium = isect.in_medium();
+    {
+        const float d = bsdf.d_factor();
+        w.d_shared *= isect.dist * isect.dist;
+        w.d_shared /= d;
+        w.d_bpt /= d;
+        w.d_pde /= d;
+        w.for_inv = 1.f / rs_for;
+        w.rev_inv = 1.f / rs_rev;
+        w.for_ratio = ratio;
+        w.rev_ratio = ratio;
+    }
+    if (isect.light >= 0) {
+        if (s.path_length < p.min_path_length) return false;
+        color += s.throughput * light_hit_radiance(p.lights[isect.light], s, rs_rev);
+        return false;
+    }
+    if (s.path_length >= p.max_path_length) return false;
+    if (p.do_bpt && !bsdf.delta() && s.path_length + 1 >= p.min_path_length && p.light_count > 0 &&
+        (bsdf.in_medium() || !only_spec_surf)) {
+        float3 c;
+        ret = direct_illumination(c, s, hitpoint, bsdf, rng, segs);
+        if (ret) return false;
+        color += s.throughput * c;
+    }
+    if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || !only_spec_surf)) {
+        bool behind = false;
+        if (bsdf.in_medium() && s.stack.size > 0) {
+            const int mid = s.stack.top().mat;
+            if (mid >= 0 && p.materials[mid].real) behind = true;
         }
-        if (!hit) {
-            if (s.path_length < p.min_path_length) break;
-            if (p.background_light < 0) break;
-            if (p.media[p.global_medium].has_attenuation) break;
-        }
-        float rs_for = 1.f, rs_rev = 1.f;
-        if (nseg > 0) {
-            rs_for = seg_for_pdf(segs, nseg);
-            rs_rev = seg_rev_pdf(segs, nseg);
-            s.throughput *= seg_attenuation(segs, nseg) / rs_for;
-        }
-        if (is_black_or_negative(s.throughput)) break;
-        VertexWeights& w = s.sw.w;
-        if (s.path_length > 1u) {
-            const float f_i = pde_factor(w.prev_in_medium, w.prev_specular, 1.f / rs_rev, w.rev_ratio, w.for_inv,
-                                         w.for_ratio, s.sw.last_sin_theta);
-            w.d_bpt = s.sw.d_bpt_a * f_i + s.sw.d_bpt_b;
-            w.d_pde = s.sw.d_pde_a * f_i + s.sw.d_pde_b;
-        }
-        w.d_shared /= rs_for;
-        w.d_bpt /= rs_for;
-        w.d_pde /= rs_for;
-        if (!hit) {
-            color += s.throughput * light_hit_radiance(p.lights[p.background_light], s, rs_rev);
-            break;
-        }
-        Bsdf bsdf;
-        if (isect.on_surface())
-            bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, false, relative_ior(isect, s.stack));
-        else
-            bsdf_setup_medium(bsdf, rd, isect.med, false);
-        if (!bsdf.valid()) break;
-        float ratio = 0.f;
-        if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
-        const float3 hitpoint = ro + rd * isect.dist;
-        origin_in_medium = isect.in_medium();
-        {
-            const float d = bsdf.d_factor();
-            w.d_shared *= isect.dist * isect.dist;
-            w.d_shared /= d;
-            w.d_bpt /= d;
-            w.d_pde /= d;
-            w.for_inv = 1.f / rs_for;
-            w.rev_inv = 1.f / rs_rev;
-            w.for_ratio = ratio;
-            w.rev_ratio = ratio;
-        }
-        if (isect.light >= 0) {
-            if (s.path_length < p.min_path_length) break;
-            color += s.throughput * light_hit_radiance(p.lights[isect.light], s, rs_rev);
-            break;
-        }
-        if (s.path_length >= p.max_path_length) break;
-        if (p.do_bpt && !bsdf.delta() && s.path_length + 1 >= p.min_path_length && p.light_count > 0 &&
-            (bsdf.in_medium() || !only_spec_surf)) {
-            float3 c;
-            ret = direct_illumination(c, s, hitpoint, bsdf, rng, segs);
-            if (ret) break;
-            color += s.throughput * c;
-        }
-        if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || !only_spec_surf)) {
-            bool behind = false;
-            if (bsdf.in_medium() && s.stack.size > 0) {
-                const int mid = s.stack.top().mat;
-                if (mid >= 0 && p.materials[mid].real) behind = true;
-            }
-            const int lp = int(rng.uniform() * p.light_subpath_count);
-            const unsigned nv = p.path_vertex_count[lp];
-            const LightVertexRec* base = p.vertices + (size_t)lp * p.slots_per_path;
-            bool err = false;
-            count_work(kCtrVertexLoads, nv);
-            for (unsigned k = 0; k < nv; k++) {
-                LightVertex lv;
-                load_vertex(base + k, lv);
-                const unsigned plen = lv.path_length + 1 + s.path_length;
-                if (plen > p.max_path_length) break;
-                const bool too_short = plen < p.min_path_length;
-                const bool diff_media = lv.bsdf.in_medium() && bsdf.in_medium() && lv.bsdf.id != bsdf.id &&
-                                        (lv.behind_surf || behind);
-                if (!(too_short || diff_media)) {
-                    float3 c;
-                    ret = connect_vertices(c, lv, bsdf, hitpoint, s, rng, segs);
-                    if (ret) {
-                        err = true;
-                        break;
-                    }
-                    color += s.throughput * lv.thr * c;
-                }
-            }
-            if (err) break;
-        }
-        {
-            unsigned mask = 0;
-            if (p.build_surf && p.n_surface > 0 && bsdf.on_surface() && !bsdf.delta() && !only_spec_surf)
-                mask |= kQuerySurf;
-            if (p.build_pp3d && p.n_medium > 0 && bsdf.in_medium() && !bsdf.delta()) mask |= kQueryPp3d;
-            if (p.build_bp2d && p.n_beams > 0 && bsdf.in_medium()) mask |= kQueryBp2d;
-            if (mask) {
-                const unsigned k = atomicAdd(&p.queue_count[1], 1u);
-                if (k < p.pt_capacity) {
-                    PointQueryRec* rec = p.pt_queue + k;
-                    const float3 frame_src = bsdf.on_surface() ? isect.shading_normal : rd;
-                    store_vertex(&rec->v, hitpoint, s.throughput, s.path_length, bsdf.in_medium(), false, bsdf,
-                                 frame_src, s.sw.w);
-                    rec->q8 = make_float4(ubits(target), ubits(mask), 0.f, 0.f);
-                }
-            }
-        }
-        bool cont;
-        ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
-        if (ret || !cont) break;
-        if (bsdf.on_surface()) {
-            if (!s.sw.w.prev_specular && (only_spec_surf || (p.estimator_techniques & kSpecularOnly))) break;
-        } else {
-            if (p.estimator_techniques & kSpecularOnly) break;
-            if (only_spec_surf) {
-                if (p.estimator_techniques & kCompatible)
-                    only_spec_surf = false;
-                else
+        const int lp = int(rng.uniform() * p.light_subpath_count);
+        const unsigned nv = p.path_vertex_count[lp];
+        const LightVertexRec* base = p.vertices + (size_t)lp * p.slots_per_path;
+        bool err = false;
+        count_work(kCtrVertexLoads, nv);
+        for (unsigned k = 0; k < nv; k++) {
+            LightVertex lv;
+            load_vertex(base + k, lv);
+            const unsigned plen = lv.path_length + 1 + s.path_length;
+            if (plen > p.max_path_length) break;
+            const bool too_short = plen < p.min_path_length;
+            const bool diff_media = lv.bsdf.in_medium() && bsdf.in_medium() && lv.bsdf.id != bsdf.id &&
+                                    (lv.behind_surf || behind);
+            if (!(too_short || diff_media)) {
+                float3 c;
+                ret = connect_vertices(c, lv, bsdf, hitpoint, s, rng, segs);
+                if (ret) {
+                    err = true;
                     break;
+                }
+                color += s.throughput * lv.thr * c;
+            }
+        }
+        if (err) return false;
+    }
+    {
+        unsigned mask = 0;
+        if (p.build_surf && p.n_surface > 0 && bsdf.on_surface() && !bsdf.delta() && !only_spec_surf)
+            mask |= kQuerySurf;
+        if (p.build_pp3d && p.n_medium > 0 && bsdf.in_medium() && !bsdf.delta()) mask |= kQueryPp3d;
+        if (p.build_bp2d && p.n_beams > 0 && bsdf.in_medium()) mask |= kQueryBp2d;
+        if (mask) {
+            const unsigned k = atomicAdd(&p.queue_count[1], 1u);
+            if (k < p.pt_capacity) {
+                PointQueryRec* rec = p.pt_queue + k;
+                const float3 frame_src = bsdf.on_surface() ? isect.shading_normal : rd;
+                store_vertex(&rec->v, hitpoint, s.throughput, s.path_length, bsdf.in_medium(), false, bsdf,
+                             frame_src, s.sw.w);
+                rec->q8 = make_float4(ubits(target), ubits(mask), 0.f, 0.f);
             }
         }
     }
-    if (ret) flag_status(ret);
-    if (target == kNoPixel) return;
-    atomicAdd(&p.cam_fb[3 * target + 0], color.x);
-    atomicAdd(&p.cam_fb[3 * target + 1], color.y);
-    atomicAdd(&p.cam_fb[3 * target + 2], color.z);
+    bool cont;
+    ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
+    if (ret || !cont) return false;
+    if (bsdf.on_surface()) {
+        if (!s.sw.w.prev_specular && (only_spec_surf || (p.estimator_techniques & kSpecularOnly))) return false;
+    } else {
+        if (p.estimator_techniques & kSpecularOnly) return false;
+        if (only_spec_surf) {
+            if (p.estimator_techniques & kCompatible)
+                only_spec_surf = false;
+            else
+                return false;
+        }
+    }
+    s.path_length++;
+    return true;
+}
+
+// Ends a camera subpath: its status and its emitter-hit / NEE / BPT colour.
+UPBP_D void camera_path_end(const CameraLane& c)
+{
+    if (c.ret) flag_status(c.ret);
+    if (c.target == kNoPixel) return;
+    float* fb = c_params.cam_fb + 3 * (size_t)c.target;
+    atomicAdd(fb + 0, c.color.x);
+    atomicAdd(fb + 1, c.color.y);
+    atomicAdd(fb + 2, c.color.z);
+}
+
+// Camera pass (extend): persistent warps, one camera subpath per lane.  Path
+// lengths differ widely (an escaping ray ends after one bounce, a ray in a
+// dense medium scatters up to the maximum), so a lane whose path ended takes
+// the next pixel from a global counter instead of idling until the longest
+// path of its warp is done.  Each pixel's random stream depends on the pixel
+// alone, so the assignment of pixels to lanes does not change any path.
+__global__ void __launch_bounds__(128, 4) camera_pass_kernel()
+{
+    const DeviceParams& p = c_params;
+    VolSeg segs[kMaxVolSegments];
+    LiteSeg lsegs[kMaxVolSegments];
+    CameraLane c;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned n = p.screen_pixel_count;
+    bool active = false, exhausted = false;
+    for (;;) {
+        const unsigned want = __ballot_sync(~0u, !active && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned base = 0;
+            if ((int)lane == leader) base = atomicAdd(&p.queue_count[2], (unsigned)__popc(want));
+            base = __shfl_sync(~0u, base, leader);
+            if (!active && !exhausted) {
+                const unsigned j = base + __popc(want & ((1u << lane) - 1u));
+                if (j < n) {
+                    active = camera_path_begin(c, j);
+                    if (!active) camera_path_end(c);
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (__all_sync(~0u, exhausted && !active)) break;
+        if (active && !camera_path_bounce(c, segs, lsegs)) {
+            camera_path_end(c);
+            active = false;
+        }
+    }
 }
 
 // Morton keys of the query records (segment midpoint / vertex position in

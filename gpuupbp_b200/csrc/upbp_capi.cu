@@ -138,6 +138,8 @@ struct upbp_ctx {
     unsigned* d_hit_count = nullptr;
     unsigned h_hit_count[2] = {0, 0};
     int search_grid = 0;
+    int camera_grid = 0;   // resident blocks of the persistent camera pass
+    int light_grid = 0;    // resident blocks of the persistent light pass
     // Morton sort of the query records: keys/values and their alternates per queue
     unsigned* d_sort[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
     unsigned sort_capacity[2] = {0, 0};
@@ -517,7 +519,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     const size_t npx = (size_t)P.screen_pixel_count * 3;
     UPBP_CK(dalloc(&c->d_vertices, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_path_count, std::max(1u, L)));
-    UPBP_CK(dalloc(&c->d_counters, 4));
+    UPBP_CK(dalloc(&c->d_counters, 8));
     UPBP_CK(dalloc(&c->d_idx_s, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_idx_m, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_beams, c->beam_capacity));
@@ -525,7 +527,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     UPBP_CK(dalloc(&c->d_acc, npx));
     UPBP_CK(dalloc(&c->d_status, 1));
     UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
-    UPBP_CK(dalloc(&c->d_qcount, 2));
+    UPBP_CK(dalloc(&c->d_qcount, 8));
     UPBP_CK(dalloc(&c->d_hit_count, 2));
     UPBP_CK(dalloc(&c->d_cam_fb, npx));
     {
@@ -534,6 +536,10 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb1d_search_kernel, 128, 0));
         c->search_grid = std::max(1, sms * std::max(1, per_sm));
+        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, camera_pass_kernel, 128, 0));
+        c->camera_grid = std::max(1, sms * std::max(1, per_sm));
+        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light_pass_kernel, 128, 0));
+        c->light_grid = std::max(1, sms * std::max(1, per_sm));
     }
     c->seg_capacity = std::max(1024u, 4 * P.screen_pixel_count);
     c->pt_capacity = std::max(1024u, 3 * P.screen_pixel_count);
@@ -634,10 +640,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         P.radius_pp3d_2 = r_pp3d * r_pp3d;
         P.radius_surf_2 = r_surf * r_surf;
         P.iteration = (unsigned)iteration;
-        UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned), c->st));
+        // [0] vertices [1] surface [2] medium [3] beams [4] next light path to hand out
+        UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned), c->st));
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
         if (L > 0) {
-            light_pass_kernel<<<(L + 127) / 128, 128, 0, c->st>>>();
+            light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>();
             launches++;
         }
         UPBP_CK(cudaGetLastError());
@@ -718,10 +725,14 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     if (P.trace_camera_paths) {
         // extend: tracing, emitter hits, NEE and BPT; queues the range queries
         for (int attempt = 0; attempt < 2; attempt++) {
-            UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 2 * sizeof(unsigned), c->st));
+            // [0] segment queries, [1] point queries, [2] next pixel to hand out
+            UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 3 * sizeof(unsigned), c->st));
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
             UPBP_CK(set_work(kKernCameraExtend));
-            camera_pass_kernel<<<(P.screen_pixel_count + 127) / 128, 128, 0, c->st>>>();
+            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
+                                    kCtrCount * sizeof(unsigned long long), c->st));
+            camera_pass_kernel<<<std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128), 128, 0,
+                                 c->st>>>();
             launches++;
             UPBP_CK(cudaGetLastError());
             UPBP_CK(cudaMemcpyAsync(c->h_qcount, c->d_qcount, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));

@@ -192,7 +192,7 @@ struct DeviceParams {
     LightVertexRec* vertices;
     unsigned slots_per_path;
     unsigned* path_vertex_count;      // stored vertices per light subpath
-    unsigned* counters;               // [0] vertices [1] surface [2] medium [3] beams
+    unsigned* counters;               // [0] vertices [1] surface [2] medium [3] beams [4] next light path
     unsigned* idx_surface;            // vertex slots of surface vertices (append order)
     unsigned* idx_medium;
     BeamRec* beams;
@@ -211,7 +211,7 @@ struct DeviceParams {
     unsigned seg_capacity;
     PointQueryRec* pt_queue;
     unsigned pt_capacity;
-    unsigned* queue_count;            // [0] segment queries, [1] point queries
+    unsigned* queue_count;            // [0] segment queries [1] point queries [2] next camera pixel
     const unsigned* seg_order;        // processing order of segment queries (Morton order of the midpoint)
     const unsigned* pt_order;         // processing order of point queries (Morton order of the position)
     float* cam_fb;                    // camera-pass image, W*H*3

@@ -141,123 +141,185 @@ UPBP_D unsigned connect_to_camera(const PathState& s, float3 hit, const Bsdf& bs
     return 0;
 }
 
+// State of one light subpath between bounces.
+struct LightLane {
+    PathState s;
+    Rng rng;
+    LightVertexRec* my_slots;
+    unsigned path_idx, stored, ret;
+    bool store_beams, origin_in_medium;
+};
+
+// Starts light subpath path_idx; false if it ended already.
+UPBP_D bool light_path_begin(LightLane& l, unsigned path_idx)
+{
+    const DeviceParams& p = c_params;
+    l.rng.init(p.iteration + p.iteration_offset, path_idx, 0u);
+    l.path_idx = path_idx;
+    l.store_beams = (p.do_bb1d && path_idx < p.bb1d_used_light_subpath_count) || p.do_bp2d;
+    l.stored = 0;
+    l.my_slots = p.vertices + (size_t)path_idx * p.slots_per_path;
+    l.origin_in_medium = false;
+    l.ret = generate_light_sample(l.s, l.rng);
+    if (l.s.is_infinite_light && p.media[p.global_medium].has_attenuation) {
+        // the reference ends such a path before tracing it, without an error
+        l.ret = 0;
+        return false;
+    }
+    return l.ret == 0;
+}
+
+// One bounce of a light subpath (one iteration of the path loop of
+// __raygen__trace_light, trace_light.cu:84-320); false when the path ends.
+UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
+{
+    const DeviceParams& p = c_params;
+    PathState& s = l.s;
+    Rng& rng = l.rng;
+    const unsigned path_idx = l.path_idx;
+    const bool store_beams = l.store_beams;
+    unsigned& stored = l.stored;
+    LightVertexRec* my_slots = l.my_slots;
+    bool& origin_in_medium = l.origin_in_medium;
+    unsigned& ret = l.ret;
+    const float3 ro = s.origin, rd = s.dir;
+    Isect isect;
+    isect.dist = kInfinity;
+    isect.mat = isect.med = isect.light = -1;
+    isect.normal = v3(0.f);
+    isect.enter = false;
+    int nseg = 0, nlseg = 0;
+    bool hit;
+    ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
+                          segs, nseg, lsegs, nlseg, rng);
+    if (ret) return false;
+    if (store_beams)
+        add_beams(ro, rd, s.throughput, s.path_length, origin_in_medium ? kOriginInMedium : 0u, segs, nseg, lsegs,
+                  nlseg, path_idx, s);
+    if (!hit) return false;
+
+    float rs_for = 1.f, rs_rev = 1.f;
+    if (nseg > 0) {
+        rs_for = seg_for_pdf(segs, nseg);
+        rs_rev = seg_rev_pdf(segs, nseg);
+        s.throughput *= seg_attenuation(segs, nseg) / rs_for;
+    }
+    if (is_black_or_negative(s.throughput)) return false;
+
+    VertexWeights& w = s.sw.w;
+    if (s.path_length > 1u) {
+        const float f_i = pde_factor(w.prev_in_medium, w.prev_specular, w.for_inv, w.for_ratio, 1.f / rs_rev,
+                                     w.rev_ratio, s.sw.last_sin_theta);
+        w.d_bpt = s.sw.d_bpt_a * f_i + s.sw.d_bpt_b;
+        w.d_pde = s.sw.d_pde_a * f_i + s.sw.d_pde_b;
+    }
+    w.d_shared /= rs_for;
+    w.d_bpt /= rs_for;
+    w.d_pde /= rs_for;
+
+    Bsdf bsdf;
+    float3 frame_src;
+    if (isect.on_surface()) {
+        frame_src = isect.shading_normal;
+        bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, true, relative_ior(isect, s.stack));
+    } else {
+        frame_src = rd;
+        bsdf_setup_medium(bsdf, rd, isect.med, true);
+    }
+    if (!bsdf.valid()) return false;
+    float ratio = 0.f;
+    if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
+    const float3 hitpoint = ro + rd * isect.dist;
+    origin_in_medium = isect.in_medium();
+    {
+        const float d = bsdf.d_factor();
+        if (!(s.path_length == 1 && s.is_infinite_light)) w.d_shared *= isect.dist * isect.dist;
+        w.d_shared /= d;
+        w.d_bpt /= d;
+        w.d_pde /= d;
+        w.for_inv = 1.f / rs_for;
+        w.rev_inv = 1.f / rs_rev;
+        w.for_ratio = ratio;
+        w.rev_ratio = ratio;
+    }
+    if (!bsdf.delta()) {
+        bool behind = false;
+        if (origin_in_medium && s.stack.size > 0) {
+            const int mid = s.stack.top().mat;
+            if (mid >= 0 && p.materials[mid].real) behind = true;
+        }
+        if (stored < p.slots_per_path) {
+            const unsigned slot = path_idx * p.slots_per_path + stored;
+            store_vertex(my_slots + stored, hitpoint, s.throughput, s.path_length, origin_in_medium, behind, bsdf,
+                         frame_src, w);
+            stored++;
+            atomicAdd(&p.counters[0], 1u);
+            if (origin_in_medium) {
+                const unsigned k = atomicAdd(&p.counters[2], 1u);
+                p.idx_medium[k] = slot;
+            } else {
+                const unsigned k = atomicAdd(&p.counters[1], 1u);
+                p.idx_surface[k] = slot;
+            }
+        }
+    }
+    if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || p.connect_to_camera_from_surf)) {
+        if (s.path_length + 1 >= p.min_path_length) {
+            ret = connect_to_camera(s, hitpoint, bsdf, rng, segs);
+            if (ret) return false;
+        }
+    }
+    if (s.path_length + 2 > p.max_path_length) return false;
+    bool cont;
+    ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
+    if (ret || !cont) return false;
+    s.path_length++;
+    return true;
+}
+
+// Ends a light subpath: its status and its stored-vertex count.
+UPBP_D void light_path_end(const LightLane& l)
+{
+    if (l.ret) flag_status(l.ret);
+    c_params.path_vertex_count[l.path_idx] = l.stored;
+}
+
+// Light pass: persistent warps, one light subpath per lane; a lane whose
+// path ended takes the next path index from a global counter (counters[4]),
+// as the camera pass does with pixels.  Each path's random stream and
+// vertex slots depend on its index alone.
 __global__ void __launch_bounds__(128) light_pass_kernel()
 {
     const DeviceParams& p = c_params;
-    const unsigned path_idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (path_idx >= p.light_subpath_count) return;
-
     VolSeg segs[kMaxVolSegments];
     LiteSeg lsegs[kMaxVolSegments];
-    Rng rng;
-    rng.init(p.iteration + p.iteration_offset, path_idx, 0u);
-    const bool store_beams = (p.do_bb1d && path_idx < p.bb1d_used_light_subpath_count) || p.do_bp2d;
-    unsigned stored = 0;
-    LightVertexRec* my_slots = p.vertices + (size_t)path_idx * p.slots_per_path;
-
-    PathState s;
-    unsigned ret = generate_light_sample(s, rng);
-    const DMedium& gm = p.media[p.global_medium];
-    if (s.is_infinite_light && gm.has_attenuation) {
-        p.path_vertex_count[path_idx] = 0;
-        return;
-    }
-    bool origin_in_medium = false;
-    for (; ret == 0; s.path_length++) {
-        const float3 ro = s.origin, rd = s.dir;
-        Isect isect;
-        isect.dist = kInfinity;
-        isect.mat = isect.med = isect.light = -1;
-        isect.normal = v3(0.f);
-        isect.enter = false;
-        int nseg = 0, nlseg = 0;
-        bool hit;
-        ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
-                              segs, nseg, lsegs, nlseg, rng);
-        if (ret) break;
-        if (store_beams)
-            add_beams(ro, rd, s.throughput, s.path_length, origin_in_medium ? kOriginInMedium : 0u, segs, nseg, lsegs,
-                      nlseg, path_idx, s);
-        if (!hit) break;
-
-        float rs_for = 1.f, rs_rev = 1.f;
-        if (nseg > 0) {
-            rs_for = seg_for_pdf(segs, nseg);
-            rs_rev = seg_rev_pdf(segs, nseg);
-            s.throughput *= seg_attenuation(segs, nseg) / rs_for;
-        }
-        if (is_black_or_negative(s.throughput)) break;
-
-        VertexWeights& w = s.sw.w;
-        if (s.path_length > 1u) {
-            const float f_i = pde_factor(w.prev_in_medium, w.prev_specular, w.for_inv, w.for_ratio, 1.f / rs_rev,
-                                         w.rev_ratio, s.sw.last_sin_theta);
-            w.d_bpt = s.sw.d_bpt_a * f_i + s.sw.d_bpt_b;
-            w.d_pde = s.sw.d_pde_a * f_i + s.sw.d_pde_b;
-        }
-        w.d_shared /= rs_for;
-        w.d_bpt /= rs_for;
-        w.d_pde /= rs_for;
-
-        Bsdf bsdf;
-        float3 frame_src;
-        if (isect.on_surface()) {
-            frame_src = isect.shading_normal;
-            bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, true, relative_ior(isect, s.stack));
-        } else {
-            frame_src = rd;
-            bsdf_setup_medium(bsdf, rd, isect.med, true);
-        }
-        if (!bsdf.valid()) break;
-        float ratio = 0.f;
-        if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
-        const float3 hitpoint = ro + rd * isect.dist;
-        origin_in_medium = isect.in_medium();
-        {
-            const float d = bsdf.d_factor();
-            if (!(s.path_length == 1 && s.is_infinite_light)) w.d_shared *= isect.dist * isect.dist;
-            w.d_shared /= d;
-            w.d_bpt /= d;
-            w.d_pde /= d;
-            w.for_inv = 1.f / rs_for;
-            w.rev_inv = 1.f / rs_rev;
-            w.for_ratio = ratio;
-            w.rev_ratio = ratio;
-        }
-        if (!bsdf.delta()) {
-            bool behind = false;
-            if (origin_in_medium && s.stack.size > 0) {
-                const int mid = s.stack.top().mat;
-                if (mid >= 0 && p.materials[mid].real) behind = true;
-            }
-            if (stored < p.slots_per_path) {
-                const unsigned slot = path_idx * p.slots_per_path + stored;
-                store_vertex(my_slots + stored, hitpoint, s.throughput, s.path_length, origin_in_medium, behind, bsdf,
-                             frame_src, w);
-                stored++;
-                atomicAdd(&p.counters[0], 1u);
-                if (origin_in_medium) {
-                    const unsigned k = atomicAdd(&p.counters[2], 1u);
-                    p.idx_medium[k] = slot;
+    LightLane l;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned n = p.light_subpath_count;
+    bool active = false, exhausted = false;
+    for (;;) {
+        const unsigned want = __ballot_sync(~0u, !active && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned base = 0;
+            if ((int)lane == leader) base = atomicAdd(&p.counters[4], (unsigned)__popc(want));
+            base = __shfl_sync(~0u, base, leader);
+            if (!active && !exhausted) {
+                const unsigned j = base + __popc(want & ((1u << lane) - 1u));
+                if (j < n) {
+                    active = light_path_begin(l, j);
+                    if (!active) light_path_end(l);
                 } else {
-                    const unsigned k = atomicAdd(&p.counters[1], 1u);
-                    p.idx_surface[k] = slot;
+                    exhausted = true;
                 }
             }
         }
-        if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || p.connect_to_camera_from_surf)) {
-            if (s.path_length + 1 >= p.min_path_length) {
-                ret = connect_to_camera(s, hitpoint, bsdf, rng, segs);
-                if (ret) break;
-            }
+        if (__all_sync(~0u, exhausted && !active)) break;
+        if (active && !light_path_bounce(l, segs, lsegs)) {
+            light_path_end(l);
+            active = false;
         }
-        if (s.path_length + 2 > p.max_path_length) break;
-        bool cont;
-        ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
-        if (ret || !cont) break;
     }
-    if (ret) flag_status(ret);
-    p.path_vertex_count[path_idx] = stored;
 }
 
 }  // namespace upbp
