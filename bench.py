@@ -120,6 +120,11 @@ SEG_RECORD, POINT_RECORD = 128, 144
 # BB1D hit-list entry (query, beam, distance, sin theta, t1, t2), written by
 # the search kernel and read by the evaluation kernel.
 HIT_RECORD = 24
+# Deferred connections: an NEE sample reads its 80 B record and 64 B of its
+# camera vertex and writes a 16 B contribution; a BPT pair reads its 8 B
+# pair and 144 B of its camera vertex and writes 16 B (the light vertex is
+# counted by vertex_loads, the occlusion ray by the traversal counters).
+NEE_BYTES, PAIR_BYTES = 160.0, 168.0
 
 
 def kernel_rooflines(st: dict, pixels: int) -> dict:
@@ -127,11 +132,13 @@ def kernel_rooflines(st: dict, pixels: int) -> dict:
     n = max(1, st["timed_iterations"])
     ms = st["ms_kernel_sum"]
     nseg, npt = st["segment_queries"], st["point_queries"]
+    nnee, npairs = st["nee_samples"], st["bpt_pairs"]
     hits = st["work"]["bb1d_query"]["beam_hit"]
     extra = {"light_pass": 0.0,
              "camera_extend": 12.0 * pixels + SEG_RECORD * nseg + POINT_RECORD * npt,
              "pb2d_query": SEG_RECORD * nseg, "bb1d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * hits,
-             "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt, "bp2d_query": POINT_RECORD * npt}
+             "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt, "bp2d_query": POINT_RECORD * npt,
+             "nee_connect": NEE_BYTES * nnee, "bpt_connect": PAIR_BYTES * npairs}
     out = {}
     for k, w in st["work"].items():
         t = ms[k] / n

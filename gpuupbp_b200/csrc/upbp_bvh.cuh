@@ -21,6 +21,41 @@ UPBP_D void count_work(int which, unsigned v)
     if ((threadIdx.x & 31) == __ffs(m) - 1 && total) atomicAdd(c_work_ptr() + which, (unsigned long long)total);
 }
 
+// Reserves n < 256 consecutive slots of `counter` for each lane of the
+// converged group that calls it, with one atomic per group; returns the
+// lane's first slot.  The prefix over the group is summed bit by bit from
+// ballots, so any mask of active lanes works.
+UPBP_D unsigned warp_reserve(unsigned* counter, unsigned n)
+{
+    const unsigned m = __activemask();
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned below = m & ((1u << lane) - 1u);
+    unsigned prefix = 0, total = 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const unsigned bits = __ballot_sync(m, (n >> b) & 1u);
+        prefix += (unsigned)__popc(bits & below) << b;
+        total += (unsigned)__popc(bits) << b;
+    }
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if ((int)lane == leader && total) base = atomicAdd(counter, total);
+    base = __shfl_sync(m, base, leader);
+    return base + prefix;
+}
+
+// warp_reserve for one slot per lane.
+UPBP_D unsigned warp_reserve1(unsigned* counter)
+{
+    const unsigned m = __activemask();
+    const unsigned lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if ((int)lane == leader) base = atomicAdd(counter, (unsigned)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + (unsigned)__popc(m & ((1u << lane) - 1u));
+}
+
 UPBP_D float3 safe_inv(float3 d) { return make_float3(1.f / d.x, 1.f / d.y, 1.f / d.z); }
 
 // Segment [tmin, tmax] vs box [lo - pad, hi + pad].  Axes with a zero

@@ -66,9 +66,16 @@ UPBP_D float3 light_hit_radiance(const DLight& l, const PathState& s, float rs_r
     return (1.f / (0.f + 1.f + w_camera)) * rad;
 }
 
-// Next-event estimation, MIS Eq D.36/D.37 (functs_camera.cuh:170-344).
-UPBP_D unsigned direct_illumination(float3& contrib, const PathState& s, float3 hit, const Bsdf& bsdf, Rng& rng,
-                                    VolSeg* segs)
+// Next-event estimation, MIS Eq D.36/D.37 (functs_camera.cuh:170-344), in
+// two halves: nee_sample draws the light sample and evaluates the BSDF in the
+// camera pass (it consumes the path's random numbers); nee_finish traces the
+// occlusion ray and applies the MIS weight in nee_connect_kernel.
+struct NeeSample {
+    float3 dir, rad, f;
+    float dist, k, w_light, a, rpdf, sin_theta;
+};
+
+UPBP_D bool nee_sample(NeeSample& ns, float3 hit, const Bsdf& bsdf, Rng& rng)
 {
     const DeviceParams& p = c_params;
     const float pick = 1.f / float(p.light_count);
@@ -76,39 +83,52 @@ UPBP_D unsigned direct_illumination(float3& contrib, const PathState& s, float3 
     const float u1 = rng.uniform();
     const float u0 = rng.uniform();
     const DLight& l = p.lights[lid];
-    contrib = v3(0.f);
-    if (!light_is_finite(l) && p.media[p.global_medium].has_attenuation) return 0;
+    if (!light_is_finite(l) && p.media[p.global_medium].has_attenuation) return false;
     float3 dir;
     float dist, direct_pdf_w, emission_pdf_w, cos_at_light;
     const float3 rad = light_illuminate(l, hit, u0, u1, dir, dist, direct_pdf_w, emission_pdf_w, cos_at_light);
-    if (is_black_or_negative(rad)) return 0;
+    if (is_black_or_negative(rad)) return false;
     float fpdf, rpdf, cos_to_light, sin_theta;
     const float3 f = bsdf_eval(bsdf, dir, cos_to_light, &fpdf, &rpdf, &sin_theta);
-    if (is_black_or_negative(f)) return 0;
+    if (is_black_or_negative(f)) return false;
     const float cp = bsdf.cont_prob;
     fpdf *= light_is_delta(l) ? 0.f : cp;
     rpdf *= cp;
+    ns.dir = dir;
+    ns.dist = dist;
+    ns.rad = rad;
+    ns.f = f;
+    ns.w_light = fpdf / (pick * direct_pdf_w);
+    ns.a = emission_pdf_w * cos_to_light / (direct_pdf_w * cos_at_light);
+    ns.k = cos_to_light / (pick * direct_pdf_w);
+    ns.rpdf = rpdf;
+    ns.sin_theta = sin_theta;
+    return true;
+}
+
+UPBP_D unsigned nee_finish(float3& contrib, const NeeSample& ns, float3 hit, bool in_medium, const BoundaryStack& stack,
+                           const VertexWeights& wc, VolSeg* segs)
+{
+    contrib = v3(0.f);
     int nseg = 0;
     bool occ;
-    const unsigned st = occluded(occ, hit, dir, dist, s.stack, bsdf.in_medium() ? kOriginInMedium : 0u, segs, nseg, rng);
+    Rng unused;
+    unused.state = unused.inc = 0;  // occlusion rays draw no random numbers
+    const unsigned st = occluded(occ, hit, ns.dir, ns.dist, stack, in_medium ? kOriginInMedium : 0u, segs, nseg, unused);
     if (st) return st;
     if (occ) return 0;
-    float n_for = 1.f, n_rev = 1.f;
+    float n_rev = 1.f;
     float3 att = v3(1.f);
     if (nseg > 0) {
-        n_for = seg_for_pdf(segs, nseg);
         n_rev = seg_rev_pdf(segs, nseg);
         att = seg_attenuation(segs, nseg);
         if (!is_positive(att)) return 0;
     }
-    const float w_light = fpdf / (pick * direct_pdf_w);
-    const VertexWeights& wc = s.sw.w;
-    const float ft = pde_factor(bsdf.in_medium(), false, 1.f / n_rev, wc.rev_ratio, wc.for_inv, wc.for_ratio, sin_theta);
+    const float ft = pde_factor(in_medium, false, 1.f / n_rev, wc.rev_ratio, wc.for_inv, wc.for_ratio, ns.sin_theta);
     const float b = !wc.prev_specular;
-    const float w_camera = (emission_pdf_w * cos_to_light / (direct_pdf_w * cos_at_light)) * n_rev *
-                           (ft + b * wc.d_shared + (rpdf / wc.rev_inv) * wc.d_bpt);
-    const float mis = 1.f / (w_light + 1.f + w_camera);
-    contrib = ((cos_to_light / (pick * direct_pdf_w)) * (rad * att * f)) * mis;
+    const float w_camera = ns.a * n_rev * (ft + b * wc.d_shared + (ns.rpdf / wc.rev_inv) * wc.d_bpt);
+    const float mis = 1.f / (ns.w_light + 1.f + w_camera);
+    contrib = (ns.k * (ns.rad * att * ns.f)) * mis;
     if (is_black_or_negative(contrib)) contrib = v3(0.f);
     return 0;
 }
@@ -448,7 +468,7 @@ UPBP_D float3 query_bp2d(float3 x, unsigned cam_len, const VertexWeights& wc, co
 // functs_pb2d.cuh:226-342, functs_bb1d.cuh:273-397, both variants).
 UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int nseg, const LiteSeg* lsegs, int nlseg,
                                  bool use_lite, unsigned sflags, unsigned cam_path_length, const StateWeights& cw,
-                                 float3 throughput, unsigned pixel)
+                                 float3 throughput, unsigned pixel, unsigned path)
 {
     const DeviceParams& p = c_params;
     float3 att = v3(1.f);
@@ -460,7 +480,7 @@ UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int n
         const int med = use_lite ? lsegs[i].med : segs[i].med;
         const DMedium& m = p.media[med];
         if (m.has_scattering) {
-            const unsigned k = atomicAdd(&p.queue_count[0], 1u);
+            const unsigned k = warp_reserve1(&p.queue_count[0]);
             if (k < p.seg_capacity) {
                 float4* q = p.seg_queue[k].q;
                 const float3 w = throughput * att;
@@ -474,7 +494,7 @@ UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int n
                 q[4] = make_float4(vw.d_shared, vw.d_bpt, vw.d_pde, vw.for_inv);
                 q[5] = make_float4(vw.rev_inv, vw.for_ratio, vw.rev_ratio, ubits(bits));
                 q[6] = make_float4(cw.last_sin_theta, cw.d_bpt_a, cw.d_bpt_b, cw.d_pde_a);
-                q[7] = make_float4(cw.d_pde_b, 0.f, 0.f, 0.f);
+                q[7] = make_float4(cw.d_pde_b, ubits(path), ubits(event_key(cam_path_length, kEvSegment)), 0.f);
             }
         }
         if (use_lite) {
@@ -498,7 +518,8 @@ UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int n
 
 // Unpacks segment-query record k: the query, the camera-side MIS state, the
 // path weight before the segment and the packed pixel / camera path length.
-UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& weight, unsigned& pk)
+UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& weight, unsigned& pk, unsigned& path,
+                           unsigned& key)
 {
     const float4* r = c_params.seg_queue[k].q;
     const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]), q2 = __ldg(&r[2]), q3 = __ldg(&r[3]);
@@ -529,7 +550,16 @@ UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& we
     cw.d_bpt_b = q6.z;
     cw.d_pde_a = q6.w;
     cw.d_pde_b = q7.x;
+    path = fbits(q7.y);
+    key = fbits(q7.z);
 }
+
+// True if the contribution with event key `key` of camera path `path` is one
+// the reference makes (no deferred connection of the path failed before it).
+UPBP_D bool event_kept(unsigned path, unsigned key) { return key < c_params.path_err[path]; }
+
+// Step of BPT connection k of a vertex (keys stay below the point merges).
+UPBP_D unsigned bpt_step(unsigned k) { return min(kEvBpt + k, kEvPoint - 1u); }
 
 // Adds c into pixel px of the camera image (pixel 0xffffff: no pixel).
 UPBP_D void splat_camera(unsigned px, float3 c)
@@ -554,8 +584,9 @@ __global__ void __launch_bounds__(128) segment_query_kernel()
         QuerySeg q;
         StateWeights cw;
         float3 weight;
-        unsigned pk;
-        load_seg_query(k, q, cw, weight, pk);
+        unsigned pk, path, key;
+        load_seg_query(k, q, cw, weight, pk, path, key);
+        if (!event_kept(path, key)) continue;
         const float3 est = kBb1d ? query_bb1d(q, cw) : query_pb2d(q, cw);
         const float norm = kBb1d ? p.bb1d_normalization : p.pb2d_normalization;
         splat_camera(pk >> 8, weight * norm * est);
@@ -688,8 +719,9 @@ __global__ void __launch_bounds__(128) bb1d_eval_kernel()
         QuerySeg q;
         StateWeights cw;
         float3 weight;
-        unsigned pk;
-        load_seg_query(qb.x, q, cw, weight, pk);
+        unsigned pk, path, key;
+        load_seg_query(qb.x, q, cw, weight, pk, path, key);
+        if (!event_kept(path, key)) continue;
         Beam lb;
         load_beam(p.beams + qb.y, lb);
         const float3 est = eval_bb1d(q, cw, lb, g.x, g.y, g.z, g.w);
@@ -708,7 +740,7 @@ __global__ void __launch_bounds__(128) point_query_kernel()
     for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const unsigned k = p.pt_order ? __ldg(&p.pt_order[j]) : j;
         const float4 q8 = __ldg(&p.pt_queue[k].q8);
-        if (!(fbits(q8.y) & kKind)) continue;
+        if (!(fbits(q8.y) & kKind) || !event_kept(fbits(q8.z), fbits(q8.w))) continue;
         LightVertex cv;
         load_vertex(&p.pt_queue[k].v, cv);
         float3 c;
@@ -720,12 +752,7 @@ __global__ void __launch_bounds__(128) point_query_kernel()
                 query_points(p.med_map, cv.hit, p.radius_pp3d, p.radius_pp3d_2, cv.path_length, cv.w, cv.bsdf, true);
         else
             c = cv.thr * p.bp2d_normalization * query_bp2d(cv.hit, cv.path_length, cv.w, cv.bsdf);
-        if ((c.x != 0.f || c.y != 0.f || c.z != 0.f) && fbits(q8.x) != 0xffffffu) {
-            const unsigned px = fbits(q8.x);
-            atomicAdd(&p.cam_fb[3 * px + 0], c.x);
-            atomicAdd(&p.cam_fb[3 * px + 1], c.y);
-            atomicAdd(&p.cam_fb[3 * px + 2], c.z);
-        }
+        splat_camera(fbits(q8.x), c);
     }
 }
 
@@ -734,6 +761,7 @@ struct CameraLane {
     PathState s;
     Rng rng;
     float3 color;
+    unsigned path;    // the pixel the path was generated for (its random stream)
     unsigned target;  // pixel the sample lands in, kNoPixel if off screen
     unsigned ret;     // status of a failed step (0: none)
     bool origin_in_medium;
@@ -742,10 +770,39 @@ struct CameraLane {
 
 constexpr unsigned kNoPixel = 0xffffffu;
 
+// Appends the camera vertex of deferred connections; returns its record
+// index (past the capacity the record is counted but not written, and the
+// host grows the queue and repeats the camera pass).
+UPBP_D unsigned store_conn_vertex(float3 hit, const PathState& s, const Bsdf& bsdf, float3 frame_src, bool behind,
+                                  unsigned pixel, unsigned path)
+{
+    const DeviceParams& p = c_params;
+    const unsigned k = warp_reserve1(&p.queue_count[3]);
+    if (k >= p.conn_capacity) return k;
+    ConnVertexRec* r = p.conn_vertices + k;
+    store_vertex(&r->v, hit, s.throughput, s.path_length, bsdf.in_medium(), behind, bsdf, frame_src, s.sw.w);
+    r->q8 = make_float4(ubits(pixel), ubits((unsigned)s.stack.size), ubits(path), ubits(s.path_length));
+    for (int i = 0; i < s.stack.size; i++) r->stack[i] = make_int2(s.stack.el[i].mat, s.stack.el[i].med);
+    return k;
+}
+
+// The boundary stack of a connection vertex (priorities from the materials,
+// as every push computes them).
+UPBP_D void load_conn_stack(const ConnVertexRec* r, unsigned size, BoundaryStack& st)
+{
+    for (unsigned i = 0; i < size; i++) {
+        const int2 e = r->stack[i];
+        st.el[i] = Boundary{e.x, e.y};
+        st.pri[i] = boundary_priority(e.x);
+    }
+    st.size = (int)size;
+}
+
 // Starts the camera subpath of `pixel`; false if it ended already.
 UPBP_D bool camera_path_begin(CameraLane& c, unsigned pixel)
 {
     const DeviceParams& p = c_params;
+    c.path = pixel;
     c.rng.init(p.iteration + p.iteration_offset, pixel, 1u);
     float2 screen;
     c.ret = generate_camera_sample(screen, pixel, c.s, c.rng);
@@ -787,7 +844,7 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
         const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
         const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
         emit_segment_queries(ro, rd, segs, nseg, lsegs, nlseg, use_lite, qflags, s.path_length, s.sw, s.throughput,
-                             target);
+                             target, c.path);
     }
     if (!hit) {
         if (s.path_length < p.min_path_length) return false;
@@ -842,43 +899,44 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
         return false;
     }
     if (s.path_length >= p.max_path_length) return false;
-    if (p.do_bpt && !bsdf.delta() && s.path_length + 1 >= p.min_path_length && p.light_count > 0 &&
-        (bsdf.in_medium() || !only_spec_surf)) {
-        float3 c;
-        ret = direct_illumination(c, s, hitpoint, bsdf, rng, segs);
-        if (ret) return false;
-        color += s.throughput * c;
-    }
-    if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || !only_spec_surf)) {
-        bool behind = false;
+    // NEE and BPT connections: the samples are drawn here, from this path's
+    // random stream and in the reference's order; their occlusion rays are
+    // traced by nee_connect_kernel and bpt_connect_kernel, one per thread.
+    const bool connect = p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || !only_spec_surf);
+    NeeSample ns;
+    bool nee = false;
+    if (connect && s.path_length + 1 >= p.min_path_length && p.light_count > 0)
+        nee = nee_sample(ns, hitpoint, bsdf, rng);
+    unsigned nv = 0, lp = 0;
+    bool behind = false;
+    if (connect) {
         if (bsdf.in_medium() && s.stack.size > 0) {
             const int mid = s.stack.top().mat;
             if (mid >= 0 && p.materials[mid].real) behind = true;
         }
-        const int lp = int(rng.uniform() * p.light_subpath_count);
-        const unsigned nv = p.path_vertex_count[lp];
-        const LightVertexRec* base = p.vertices + (size_t)lp * p.slots_per_path;
-        bool err = false;
-        count_work(kCtrVertexLoads, nv);
-        for (unsigned k = 0; k < nv; k++) {
-            LightVertex lv;
-            load_vertex(base + k, lv);
-            const unsigned plen = lv.path_length + 1 + s.path_length;
-            if (plen > p.max_path_length) break;
-            const bool too_short = plen < p.min_path_length;
-            const bool diff_media = lv.bsdf.in_medium() && bsdf.in_medium() && lv.bsdf.id != bsdf.id &&
-                                    (lv.behind_surf || behind);
-            if (!(too_short || diff_media)) {
-                float3 c;
-                ret = connect_vertices(c, lv, bsdf, hitpoint, s, rng, segs);
-                if (ret) {
-                    err = true;
-                    break;
-                }
-                color += s.throughput * lv.thr * c;
+        lp = (unsigned)int(rng.uniform() * p.light_subpath_count);
+        nv = p.path_vertex_count[lp];
+    }
+    if ((nee || nv > 0) && target != kNoPixel) {
+        const float3 frame_src = bsdf.on_surface() ? isect.shading_normal : rd;
+        const unsigned v = store_conn_vertex(hitpoint, s, bsdf, frame_src, behind, target, c.path);
+        if (nee) {
+            const unsigned k = warp_reserve1(&p.queue_count[4]);
+            if (k < p.nee_capacity && v < p.conn_capacity) {
+                float4* q = p.nee_queue[k].q;
+                q[0] = make_float4(hitpoint.x, hitpoint.y, hitpoint.z, ns.dist);
+                q[1] = make_float4(ns.dir.x, ns.dir.y, ns.dir.z, ubits(v));
+                q[2] = make_float4(ns.rad.x, ns.rad.y, ns.rad.z, ns.k);
+                q[3] = make_float4(ns.f.x, ns.f.y, ns.f.z, ns.w_light);
+                q[4] = make_float4(ns.a, ns.rpdf, ns.sin_theta, ubits(bsdf.in_medium() ? 1u : 0u));
             }
         }
-        if (err) return false;
+        if (nv > 0) {
+            const unsigned k = warp_reserve(&p.queue_count[5], nv);
+            if (v < p.conn_capacity)
+                for (unsigned i = 0; i < nv && k + i < p.bpt_capacity; i++)
+                    p.bpt_pairs[k + i] = make_uint2(v, lp * p.slots_per_path + i);
+        }
     }
     {
         unsigned mask = 0;
@@ -887,13 +945,14 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
         if (p.build_pp3d && p.n_medium > 0 && bsdf.in_medium() && !bsdf.delta()) mask |= kQueryPp3d;
         if (p.build_bp2d && p.n_beams > 0 && bsdf.in_medium()) mask |= kQueryBp2d;
         if (mask) {
-            const unsigned k = atomicAdd(&p.queue_count[1], 1u);
+            const unsigned k = warp_reserve1(&p.queue_count[1]);
             if (k < p.pt_capacity) {
                 PointQueryRec* rec = p.pt_queue + k;
                 const float3 frame_src = bsdf.on_surface() ? isect.shading_normal : rd;
                 store_vertex(&rec->v, hitpoint, s.throughput, s.path_length, bsdf.in_medium(), false, bsdf,
                              frame_src, s.sw.w);
-                rec->q8 = make_float4(ubits(target), ubits(mask), 0.f, 0.f);
+                rec->q8 = make_float4(ubits(target), ubits(mask), ubits(c.path),
+                                      ubits(event_key(s.path_length, kEvPoint)));
             }
         }
     }
@@ -915,15 +974,12 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     return true;
 }
 
-// Ends a camera subpath: its status and its emitter-hit / NEE / BPT colour.
+// Ends a camera subpath: its status and its emitter-hit colour, which
+// k_resolve_camera adds once the deferred connections of the path are done.
 UPBP_D void camera_path_end(const CameraLane& c)
 {
     if (c.ret) flag_status(c.ret);
-    if (c.target == kNoPixel) return;
-    float* fb = c_params.cam_fb + 3 * (size_t)c.target;
-    atomicAdd(fb + 0, c.color.x);
-    atomicAdd(fb + 1, c.color.y);
-    atomicAdd(fb + 2, c.color.z);
+    c_params.path_color[c.path] = make_float4(c.color.x, c.color.y, c.color.z, ubits(c.target));
 }
 
 // Camera pass (extend): persistent warps, one camera subpath per lane.  Path
@@ -962,6 +1018,131 @@ __global__ void __launch_bounds__(128, 4) camera_pass_kernel()
         if (active && !camera_path_bounce(c, segs, lsegs)) {
             camera_path_end(c);
             active = false;
+        }
+    }
+}
+
+// Deferred NEE: one light sample per thread -- occlusion ray through the
+// media, MIS weight, throughput.  The contribution is kept per sample until
+// k_resolve_camera knows whether an earlier step of the path failed.
+__global__ void __launch_bounds__(128) nee_connect_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned n = min(p.queue_count[4], p.nee_capacity);
+    VolSeg segs[kMaxVolSegments];
+    BoundaryStack st;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const float4* q = p.nee_queue[j].q;
+        const float4 q0 = __ldg(&q[0]), q1 = __ldg(&q[1]), q2 = __ldg(&q[2]), q3 = __ldg(&q[3]), q4 = __ldg(&q[4]);
+        NeeSample ns;
+        const float3 hit = xyz(q0);
+        ns.dist = q0.w;
+        ns.dir = xyz(q1);
+        ns.rad = xyz(q2);
+        ns.k = q2.w;
+        ns.f = xyz(q3);
+        ns.w_light = q3.w;
+        ns.a = q4.x;
+        ns.rpdf = q4.y;
+        ns.sin_theta = q4.z;
+        const bool in_medium = (fbits(q4.w) & 1u) != 0;
+        const ConnVertexRec* cr = p.conn_vertices + fbits(q1.w);
+        const float4 thr = __ldg(&cr->v.q[1]), w2 = __ldg(&cr->v.q[2]), w3 = __ldg(&cr->v.q[3]);
+        const float4 q8 = __ldg(&cr->q8);
+        VertexWeights wc;
+        wc.d_shared = w2.x;
+        wc.d_bpt = w2.y;
+        wc.d_pde = w2.z;
+        wc.for_inv = w2.w;
+        wc.rev_inv = w3.x;
+        wc.for_ratio = w3.y;
+        wc.rev_ratio = w3.z;
+        wc.prev_in_medium = (fbits(w3.w) >> 28) & 1u;
+        wc.prev_specular = (fbits(w3.w) >> 29) & 1u;
+        load_conn_stack(cr, fbits(q8.y), st);
+        float3 c;
+        const unsigned e = nee_finish(c, ns, hit, in_medium, st, wc, segs);
+        if (e) {
+            // the reference ends the camera path at a failed step
+            flag_status(e);
+            atomicMin(&p.path_err[fbits(q8.z)], event_key(fbits(q8.w), kEvNee));
+            c = v3(0.f);
+        }
+        const float3 col = xyz(thr) * c;
+        p.nee_color[j] = make_float4(col.x, col.y, col.z, 0.f);
+    }
+}
+
+// Deferred BPT: one (camera vertex, light vertex) pair per thread -- the
+// path-length and media checks of the connection loop, then the connection
+// with its occlusion ray; the contribution is kept per pair like NEE's.
+__global__ void __launch_bounds__(128) bpt_connect_kernel()
+{
+    const DeviceParams& p = c_params;
+    const unsigned n = min(p.queue_count[5], p.bpt_capacity);
+    VolSeg segs[kMaxVolSegments];
+    PathState ps;
+    unsigned loads = 0;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint2 pr = __ldg(&p.bpt_pairs[j]);
+        const ConnVertexRec* cr = p.conn_vertices + pr.x;
+        p.bpt_color[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        LightVertex lv, cv;
+        load_vertex(p.vertices + pr.y, lv);
+        loads++;
+        load_vertex(&cr->v, cv);
+        const unsigned plen = lv.path_length + 1 + cv.path_length;
+        if (plen > p.max_path_length || plen < p.min_path_length) continue;
+        const bool diff_media = lv.bsdf.in_medium() && cv.bsdf.in_medium() && lv.bsdf.id != cv.bsdf.id &&
+                                (lv.behind_surf || cv.behind_surf);
+        if (diff_media) continue;
+        const float4 q8 = __ldg(&cr->q8);
+        load_conn_stack(cr, fbits(q8.y), ps.stack);
+        ps.sw.w = cv.w;
+        Rng unused;
+        unused.state = unused.inc = 0;  // occlusion rays draw no random numbers
+        float3 c;
+        const unsigned e = connect_vertices(c, lv, cv.bsdf, cv.hit, ps, unused, segs);
+        if (e) {
+            // the reference ends the camera path at a failed connection
+            flag_status(e);
+            atomicMin(&p.path_err[fbits(q8.z)], event_key(fbits(q8.w), bpt_step(pr.y % p.slots_per_path)));
+            continue;
+        }
+        const float3 col = cv.thr * lv.thr * c;
+        p.bpt_color[j] = make_float4(col.x, col.y, col.z, 0.f);
+    }
+    count_work(kCtrVertexLoads, loads);
+}
+
+// Adds the deferred connections and the emitter-hit colours into the camera
+// image, each only if no earlier step of its camera path failed: NEE samples,
+// then BPT pairs, then one colour per camera path.
+__global__ void __launch_bounds__(256) k_resolve_camera()
+{
+    const DeviceParams& p = c_params;
+    const unsigned nn = min(p.queue_count[4], p.nee_capacity);
+    const unsigned nb = min(p.queue_count[5], p.bpt_capacity);
+    const unsigned total = nn + nb + p.screen_pixel_count;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        if (j < nn) {
+            const float4 c = p.nee_color[j];
+            if (c.x == 0.f && c.y == 0.f && c.z == 0.f) continue;
+            const float4 q8 = __ldg(&p.conn_vertices[fbits(__ldg(&p.nee_queue[j].q[1]).w)].q8);
+            if (event_kept(fbits(q8.z), event_key(fbits(q8.w), kEvNee))) splat_camera(fbits(q8.x), xyz(c));
+        } else if (j < nn + nb) {
+            const unsigned k = j - nn;
+            const float4 c = p.bpt_color[k];
+            if (c.x == 0.f && c.y == 0.f && c.z == 0.f) continue;
+            const uint2 pr = __ldg(&p.bpt_pairs[k]);
+            const float4 q8 = __ldg(&p.conn_vertices[pr.x].q8);
+            if (event_kept(fbits(q8.z), event_key(fbits(q8.w), bpt_step(pr.y % p.slots_per_path))))
+                splat_camera(fbits(q8.x), xyz(c));
+        } else {
+            const unsigned path = j - nn - nb;
+            const float4 c = p.path_color[path];
+            // an emitter hit ends its path, after every connection of the path
+            if (p.path_err[path] == ~0u) splat_camera(fbits(c.w), xyz(c));
         }
     }
 }

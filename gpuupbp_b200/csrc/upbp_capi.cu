@@ -20,8 +20,11 @@ using namespace upbp;
 
 constexpr int kEventRing = 64;
 // events per iteration: start, light done, maps done, then one after each
-// camera-side kernel kind (extend, pb2d, bb1d, surf, pp3d, bp2d)
+// camera-side kernel kind (extend, nee, bpt, pb2d, bb1d, surf, pp3d, bp2d)
 constexpr int kEvPerIter = 3 + (kKernCount - 1);
+// camera-side kernel kinds in launch order (one event after each)
+constexpr int kCamOrder[kKernCount - 1] = {kKernCameraExtend, kKernNee, kKernBpt, kKernPb2d,
+                                           kKernBb1d,         kKernSurf, kKernPp3d, kKernBp2d};
 
 namespace {
 
@@ -40,6 +43,17 @@ cudaError_t dalloc(T** p, size_t n)
     *p = nullptr;
     if (n == 0) n = 1;
     return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+}
+
+// Reallocates *p for at least n elements (n + n/4) when n exceeds cap;
+// the old contents are dropped.
+template <class T>
+cudaError_t grow(T** p, unsigned& cap, unsigned n)
+{
+    if (n <= cap) return cudaSuccess;
+    cudaFree(*p);
+    cap = n + n / 4;
+    return dalloc(p, cap);
 }
 
 template <class T>
@@ -125,12 +139,21 @@ struct upbp_ctx {
     unsigned last_chunks = 0;
     unsigned long long* d_work = nullptr;   // kKernCount x kCtrCount
     unsigned launches = 0;
+    size_t h2d_iter = 0, d2h_iter = 0;
     SegQueryRec* d_seg_queue = nullptr;
     PointQueryRec* d_pt_queue = nullptr;
     unsigned seg_capacity = 0, pt_capacity = 0;
     unsigned* d_qcount = nullptr;
     float* d_cam_fb = nullptr;
-    unsigned h_qcount[2] = {0, 0};
+    unsigned h_qcount[6] = {0, 0, 0, 0, 0, 0};
+    // deferred NEE / BPT connections of the camera pass
+    ConnVertexRec* d_conn = nullptr;
+    NeeRec* d_nee = nullptr;
+    uint2* d_bpt = nullptr;
+    float4 *d_nee_color = nullptr, *d_bpt_color = nullptr;
+    unsigned conn_capacity = 0, nee_capacity = 0, bpt_capacity = 0;
+    unsigned* d_path_err = nullptr;
+    float4* d_path_color = nullptr;
     // BB1D hit list (search -> evaluation)
     uint2* d_hit_qb = nullptr;
     float4* d_hit_geom = nullptr;
@@ -545,6 +568,16 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     c->pt_capacity = std::max(1024u, 3 * P.screen_pixel_count);
     UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
     UPBP_CK(dalloc(&c->d_pt_queue, c->pt_capacity));
+    c->conn_capacity = std::max(1024u, 2 * P.screen_pixel_count);
+    c->nee_capacity = std::max(1024u, 2 * P.screen_pixel_count);
+    c->bpt_capacity = std::max(1024u, 2 * P.screen_pixel_count);
+    UPBP_CK(dalloc(&c->d_conn, c->conn_capacity));
+    UPBP_CK(dalloc(&c->d_nee, c->nee_capacity));
+    UPBP_CK(dalloc(&c->d_bpt, c->bpt_capacity));
+    UPBP_CK(dalloc(&c->d_nee_color, c->nee_capacity));
+    UPBP_CK(dalloc(&c->d_bpt_color, c->bpt_capacity));
+    UPBP_CK(dalloc(&c->d_path_err, P.screen_pixel_count));
+    UPBP_CK(dalloc(&c->d_path_color, P.screen_pixel_count));
     UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
@@ -578,6 +611,16 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     P.pt_queue = c->d_pt_queue;
     P.pt_capacity = c->pt_capacity;
     P.queue_count = c->d_qcount;
+    P.conn_vertices = c->d_conn;
+    P.conn_capacity = c->conn_capacity;
+    P.nee_queue = c->d_nee;
+    P.nee_capacity = c->nee_capacity;
+    P.bpt_pairs = c->d_bpt;
+    P.bpt_capacity = c->bpt_capacity;
+    P.nee_color = c->d_nee_color;
+    P.bpt_color = c->d_bpt_color;
+    P.path_err = c->d_path_err;
+    P.path_color = c->d_path_color;
     P.hit_count = c->d_hit_count;
     P.cam_fb = c->d_cam_fb;
     UPBP_CK(cudaStreamSynchronize(c->st));
@@ -597,9 +640,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
     UPBP_CK(cudaMemsetAsync(c->d_work, 0, (size_t)kKernCount * kCtrCount * sizeof(unsigned long long), c->st));
     unsigned launches = 0;
+    size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
     P.work = c->d_work;
     auto set_work = [&](int kern) -> cudaError_t {
         unsigned long long* w = c->d_work + (size_t)kern * kCtrCount;
+        h2d += sizeof(w);
         return cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st);
     };
     UPBP_CK(set_work(kKernLight));
@@ -642,12 +687,14 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         P.iteration = (unsigned)iteration;
         // [0] vertices [1] surface [2] medium [3] beams [4] next light path to hand out
         UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned), c->st));
+        h2d += sizeof(P);
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
         if (L > 0) {
             light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>();
             launches++;
         }
         UPBP_CK(cudaGetLastError());
+        d2h += 4 * sizeof(unsigned);
         UPBP_CK(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaStreamSynchronize(c->st));
         std::memcpy(found, c->h_counters, sizeof(found));
@@ -696,6 +743,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         size_t tb = c->scan_temp_bytes;
         UPBP_CK(cub::DeviceScan::ExclusiveSum(c->d_scan_temp, tb, c->d_chunk_counts, c->d_chunk_offsets, (int)nb, c->st));
         unsigned tail[2] = {0, 0};
+        d2h += 2 * sizeof(unsigned);
         UPBP_CK(cudaMemcpyAsync(&tail[0], c->d_chunk_offsets + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaMemcpyAsync(&tail[1], c->d_chunk_counts + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaStreamSynchronize(c->st));
@@ -723,10 +771,13 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
     UPBP_CK(cudaEventRecord(ev[2], c->st));
     if (P.trace_camera_paths) {
-        // extend: tracing, emitter hits, NEE and BPT; queues the range queries
+        // extend: tracing, emitter hits, NEE and BPT sampling; queues the
+        // range queries and the connections
         for (int attempt = 0; attempt < 2; attempt++) {
-            // [0] segment queries, [1] point queries, [2] next pixel to hand out
-            UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 3 * sizeof(unsigned), c->st));
+            // [0] segment queries [1] point queries [2] next pixel to hand out
+            // [3] connection vertices [4] NEE samples [5] BPT pairs
+            UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 6 * sizeof(unsigned), c->st));
+            h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
             UPBP_CK(set_work(kKernCameraExtend));
             UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
@@ -735,32 +786,69 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                                  c->st>>>();
             launches++;
             UPBP_CK(cudaGetLastError());
-            UPBP_CK(cudaMemcpyAsync(c->h_qcount, c->d_qcount, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+            d2h += 6 * sizeof(unsigned);
+            UPBP_CK(cudaMemcpyAsync(c->h_qcount, c->d_qcount, 6 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
             UPBP_CK(cudaStreamSynchronize(c->st));
-            if (c->h_qcount[0] <= c->seg_capacity && c->h_qcount[1] <= c->pt_capacity) break;
+            const unsigned* q = c->h_qcount;
+            if (q[0] <= c->seg_capacity && q[1] <= c->pt_capacity && q[3] <= c->conn_capacity &&
+                q[4] <= c->nee_capacity && q[5] <= c->bpt_capacity)
+                break;
             // a queue overflowed: grow it and render the camera pass again (the
             // pass is a pure function of the iteration, so the rerun is exact)
-            if (c->h_qcount[0] > c->seg_capacity) {
-                cudaFree(c->d_seg_queue);
-                c->seg_capacity = c->h_qcount[0] + c->h_qcount[0] / 4;
-                UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
-            }
-            if (c->h_qcount[1] > c->pt_capacity) {
-                cudaFree(c->d_pt_queue);
-                c->pt_capacity = c->h_qcount[1] + c->h_qcount[1] / 4;
-                UPBP_CK(dalloc(&c->d_pt_queue, c->pt_capacity));
+            unsigned nee_cap = c->nee_capacity, bpt_cap = c->bpt_capacity;
+            if (grow(&c->d_seg_queue, c->seg_capacity, q[0]) != cudaSuccess ||
+                grow(&c->d_pt_queue, c->pt_capacity, q[1]) != cudaSuccess ||
+                grow(&c->d_conn, c->conn_capacity, q[3]) != cudaSuccess ||
+                grow(&c->d_nee, c->nee_capacity, q[4]) != cudaSuccess ||
+                grow(&c->d_bpt, c->bpt_capacity, q[5]) != cudaSuccess ||
+                grow(&c->d_nee_color, nee_cap, q[4]) != cudaSuccess ||
+                grow(&c->d_bpt_color, bpt_cap, q[5]) != cudaSuccess) {
+                upbp_host::set_error("camera-pass queue allocation failed");
+                return UPBP_ERR_CUDA;
             }
             P.seg_queue = c->d_seg_queue;
             P.seg_capacity = c->seg_capacity;
             P.pt_queue = c->d_pt_queue;
             P.pt_capacity = c->pt_capacity;
+            P.conn_vertices = c->d_conn;
+            P.conn_capacity = c->conn_capacity;
+            P.nee_queue = c->d_nee;
+            P.nee_capacity = c->nee_capacity;
+            P.bpt_pairs = c->d_bpt;
+            P.bpt_capacity = c->bpt_capacity;
+            P.nee_color = c->d_nee_color;
+            P.bpt_color = c->d_bpt_color;
             UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
         }
     }
     UPBP_CK(cudaEventRecord(ev[3], c->st));
+    auto grid_for = [](unsigned n) { return std::max(1u, std::min((n + 127) / 128, 148u * 64u)); };
+    // deferred NEE and BPT connections, then the colours of every camera path
+    // whose steps all succeeded (the query kernels below check the same)
+    const unsigned nnee = P.trace_camera_paths ? std::min(c->h_qcount[4], c->nee_capacity) : 0;
+    const unsigned nbpt = P.trace_camera_paths ? std::min(c->h_qcount[5], c->bpt_capacity) : 0;
+    if (P.trace_camera_paths)
+        UPBP_CK(cudaMemsetAsync(c->d_path_err, 0xff, P.screen_pixel_count * sizeof(unsigned), c->st));
+    if (nnee > 0) {
+        UPBP_CK(set_work(kKernNee));
+        nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaEventRecord(ev[4], c->st));
+    if (nbpt > 0) {
+        UPBP_CK(set_work(kKernBpt));
+        bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>();
+        launches++;
+    }
+    if (P.trace_camera_paths) {
+        k_resolve_camera<<<std::max(1u, std::min((nnee + nbpt + P.screen_pixel_count + 255) / 256, 148u * 32u)), 256, 0,
+                           c->st>>>();
+        launches++;
+    }
+    UPBP_CK(cudaGetLastError());
+    UPBP_CK(cudaEventRecord(ev[5], c->st));
     const unsigned nseg = std::min(c->h_qcount[0], c->seg_capacity);
     const unsigned npt = std::min(c->h_qcount[1], c->pt_capacity);
-    auto grid_for = [](unsigned n) { return std::max(1u, std::min((n + 127) / 128, 148u * 64u)); };
     const bool run_pb2d = P.trace_camera_paths && P.build_pb2d && P.n_medium > 0 && nseg > 0;
     const bool run_bb1d = P.trace_camera_paths && P.build_bb1d && P.n_beams > 0 && nseg > 0;
     const bool run_surf = P.trace_camera_paths && P.build_surf && P.n_surface > 0 && npt > 0;
@@ -775,6 +863,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         P.seg_order = so;
         P.pt_order = po;
         launches += (so ? 1 : 0) + (po ? 1 : 0);
+        h2d += sizeof(P);
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
     }
     if (run_pb2d) {
@@ -782,7 +871,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         segment_query_kernel<false><<<grid_for(nseg), 128, 0, c->st>>>();
         launches++;
     }
-    UPBP_CK(cudaEventRecord(ev[4], c->st));
+    UPBP_CK(cudaEventRecord(ev[6], c->st));
     if (run_bb1d) {
         // search: (query, beam) pairs into the hit list; a list that was too
         // small is grown and the search repeated (it is a pure function of
@@ -796,10 +885,12 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             P.hit_qb = c->d_hit_qb;
             P.hit_geom = c->d_hit_geom;
             P.hit_capacity = c->hit_capacity;
+            h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
             bb1d_search_kernel<<<c->search_grid, 128, 0, c->st>>>();
             launches++;
             UPBP_CK(cudaGetLastError());
+            d2h += 2 * sizeof(unsigned);
             UPBP_CK(cudaMemcpyAsync(c->h_hit_count, c->d_hit_count, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                     c->st));
             UPBP_CK(cudaStreamSynchronize(c->st));
@@ -812,30 +903,32 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             launches++;
         }
     }
-    UPBP_CK(cudaEventRecord(ev[5], c->st));
+    UPBP_CK(cudaEventRecord(ev[7], c->st));
     if (run_surf) {
         UPBP_CK(set_work(kKernSurf));
         point_query_kernel<kQuerySurf><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
-    UPBP_CK(cudaEventRecord(ev[6], c->st));
+    UPBP_CK(cudaEventRecord(ev[8], c->st));
     if (run_pp3d) {
         UPBP_CK(set_work(kKernPp3d));
         point_query_kernel<kQueryPp3d><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
-    UPBP_CK(cudaEventRecord(ev[7], c->st));
+    UPBP_CK(cudaEventRecord(ev[9], c->st));
     if (run_bp2d) {
         UPBP_CK(set_work(kKernBp2d));
         point_query_kernel<kQueryBp2d><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
     UPBP_CK(cudaGetLastError());
-    UPBP_CK(cudaEventRecord(ev[8], c->st));
+    UPBP_CK(cudaEventRecord(ev[10], c->st));
     k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
                                                                          (unsigned)npx);
     launches++;
     c->launches = launches;
+    c->h2d_iter = h2d;
+    c->d2h_iter = d2h;
     UPBP_CK(cudaGetLastError());
     c->iterations++;
     c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
@@ -881,7 +974,7 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     o->scene_radius = c->P.scene_radius;
     unsigned long long work[kKernCount * kCtrCount];
     UPBP_CK(cudaMemcpy(work, c->d_work, sizeof(work), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < kKernCount && k < 7; k++)
+    for (int k = 0; k < kKernCount && k < UPBP_KERNEL_KINDS; k++)
         for (int i = 0; i < kCtrCount && i < 8; i++) o->work[k][i] = work[k * kCtrCount + i];
     for (int i = 0; i < kCtrCount && i < 8; i++) {
         o->work_light[i] = work[i];
@@ -891,6 +984,8 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     }
     o->segment_queries = c->h_qcount[0];
     o->point_queries = c->h_qcount[1];
+    o->nee_samples = c->h_qcount[4];
+    o->bpt_pairs = c->h_qcount[5];
     o->beam_chunks = c->last_chunks;
     o->radius[0] = c->P.radius_bb1d;
     o->radius[1] = c->P.radius_bp2d;
@@ -898,8 +993,8 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     o->radius[3] = c->P.radius_pp3d;
     o->radius[4] = c->P.radius_surf;
     o->radius[5] = c->P.rad_beam;
-    o->h2d_bytes = c->P.trace_light_paths ? 2 * sizeof(DeviceParams) : sizeof(DeviceParams);
-    o->d2h_bytes = c->P.trace_light_paths ? 4 * sizeof(unsigned) + (c->last_chunks ? 2 * sizeof(unsigned) : 0) : 0;
+    o->h2d_bytes = (uint32_t)c->h2d_iter;
+    o->d2h_bytes = (uint32_t)c->d2h_iter;
     o->kernel_launches = c->launches;
     // per-pass times: the last iteration, and sums over the iterations run
     // since the previous stats call (up to the event ring size)
@@ -907,7 +1002,8 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
         cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
         float t[kEvPerIter - 1];
         for (int e = 0; e + 1 < kEvPerIter; e++) UPBP_CK(cudaEventElapsedTime(&t[e], ev[e], ev[e + 1]));
-        const float cam = t[2] + t[3] + t[4] + t[5] + t[6] + t[7];
+        float cam = 0.f;
+        for (int e = 2; e + 1 < kEvPerIter; e++) cam += t[e];
         if (k == 0) {
             o->ms_light = t[0];
             o->ms_build = t[1];
@@ -917,7 +1013,7 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
         o->ms_build_sum += t[1];
         o->ms_camera_sum += cam;
         o->ms_kernel_sum[kKernLight] += t[0];
-        for (int kk = 1; kk < kKernCount; kk++) o->ms_kernel_sum[kk] += t[1 + kk];
+        for (int i = 0; i < kKernCount - 1; i++) o->ms_kernel_sum[kCamOrder[i]] += t[2 + i];
         o->timed_iterations++;
     }
     c->ev_pending = 0;
@@ -1055,7 +1151,8 @@ extern "C" void upbp_destroy(upbp_ctx* c)
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
                     c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
-                    c->d_qcount, c->d_hit_count, c->d_hit_qb, c->d_hit_geom, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
+                    c->d_qcount, c->d_conn, c->d_nee, c->d_bpt, c->d_nee_color, c->d_bpt_color,
+                    c->d_path_err, c->d_path_color, c->d_hit_count, c->d_hit_qb, c->d_hit_geom, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
                     c->d_sort[0][2], c->d_sort[0][3], c->d_sort[1][0], c->d_sort[1][1], c->d_sort[1][2],
                     c->d_sort[1][3], c->d_sort_temp};
     for (void* b : bufs)

@@ -123,16 +123,39 @@ struct BeamRec {
 //   q0: origin.xyz, dmin   q1: direction.xyz, dmax
 //   q2: weight.xyz (path throughput x attenuation before the segment), medium id bits
 //   q3: ray_sample_for_pdf, ray_sample_rev_pdf, sampling flags bits, pixel << 8 | camera path length
-//   q4..q7: camera StateWeights in the beam record layout (BeamRec q4..q7)
+//   q4..q7: camera StateWeights in the beam record layout (BeamRec q4..q7);
+//   q7.y camera path bits, q7.z event key bits
 struct SegQueryRec {
     float4 q[8];
 };
 // Point query (SURF / PP3D / BP2D at one camera vertex): a LightVertexRec
 // of the camera vertex (throughput, weights, BSDF) plus
-//   q8: pixel bits, estimator mask bits (1 SURF, 2 PP3D, 4 BP2D), -, -
+//   q8: pixel bits, estimator mask bits (1 SURF, 2 PP3D, 4 BP2D), camera path bits, event key bits
 struct PointQueryRec {
     LightVertexRec v;
     float4 q8;
+};
+
+// Camera vertex of deferred connections (NEE and BPT occlusion rays run in
+// their own kernels): the vertex in the light-vertex layout (behind-surface
+// bit included), then
+//   q8: pixel bits, boundary-stack size bits, camera path bits, bounce bits
+//   stack[i] = (material, medium) of the camera path's boundary stack at the
+//   vertex, bottom first; the priorities follow from the materials.
+constexpr int kConnStack = 20;
+struct ConnVertexRec {
+    LightVertexRec v;
+    float4 q8;
+    int2 stack[kConnStack];
+};
+// Next-event estimation sample whose occlusion ray is still to be traced:
+//   q0: vertex position.xyz, distance to the light sample
+//   q1: direction to the light.xyz, camera-vertex record index bits
+//   q2: light radiance.xyz, cos_to_light / (pick * direct_pdf_w)
+//   q3: BSDF value.xyz, w_light = bsdf pdf / (pick * direct_pdf_w)
+//   q4: emission_pdf_w * cos_to_light / (direct_pdf_w * cos_at_light), reverse bsdf pdf, sin theta, flag bits
+struct NeeRec {
+    float4 q[5];
 };
 
 // Point map: BVH over light-vertex positions in leaf order.
@@ -212,6 +235,7 @@ struct DeviceParams {
     PointQueryRec* pt_queue;
     unsigned pt_capacity;
     unsigned* queue_count;            // [0] segment queries [1] point queries [2] next camera pixel
+                                      // [3] connection vertices [4] NEE samples [5] BPT pairs
     const unsigned* seg_order;        // processing order of segment queries (Morton order of the midpoint)
     const unsigned* pt_order;         // processing order of point queries (Morton order of the position)
     float* cam_fb;                    // camera-pass image, W*H*3
@@ -222,7 +246,29 @@ struct DeviceParams {
     float4* hit_geom;                 // (distance, sin theta, t along the query, t along the beam)
     unsigned hit_capacity;
     unsigned* hit_count;              // [0] hits found (may exceed capacity), [1] next query to hand out
+
+    // deferred camera-side connections; counts in queue_count[3..5]
+    ConnVertexRec* conn_vertices;
+    unsigned conn_capacity;
+    NeeRec* nee_queue;
+    unsigned nee_capacity;
+    uint2* bpt_pairs;                 // (camera-vertex record, light-vertex slot)
+    unsigned bpt_capacity;
+    float4* nee_color;                // contribution of each NEE sample (after its occlusion ray)
+    float4* bpt_color;                // contribution of each BPT pair
+    // Per camera path (index = the pixel it was generated for): the first
+    // event key at which a deferred connection failed (~0: none), and the
+    // emitter-hit colour of the path with its target pixel.  A failed step
+    // ends a path in the reference, so contributions with a later key drop.
+    unsigned* path_err;
+    float4* path_color;
 };
+
+// Event keys order the contributions of a camera path as the reference's
+// path loop makes them: bounce * 256 + step, step = 1 segment merges (PB2D,
+// BB1D), 2 NEE, 3 + k BPT connection k, 255 point merges (SURF, PP3D, BP2D).
+enum : unsigned { kEvSegment = 1u, kEvNee = 2u, kEvBpt = 3u, kEvPoint = 255u };
+UPBP_HD unsigned event_key(unsigned bounce, unsigned step) { return bounce * 256u + step; }
 
 // Launch parameters of the running pass, uploaded before each launch.
 __constant__ DeviceParams c_params;
@@ -233,7 +279,8 @@ UPBP_D unsigned long long* c_work_ptr() { return c_work; }
 
 // Kernel kinds of an iteration, for work counters and timing.
 enum : int {
-    kKernLight = 0, kKernCameraExtend, kKernPb2d, kKernBb1d, kKernSurf, kKernPp3d, kKernBp2d, kKernCount
+    kKernLight = 0, kKernCameraExtend, kKernPb2d, kKernBb1d, kKernSurf, kKernPp3d, kKernBp2d, kKernNee, kKernBpt,
+    kKernCount
 };
 
 }  // namespace upbp

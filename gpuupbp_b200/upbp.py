@@ -55,12 +55,14 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint32), ("h2d_bytes", ctypes.c_uint32), ("d2h_bytes", ctypes.c_uint32),
         ("ms_light_sum", ctypes.c_double), ("ms_build_sum", ctypes.c_double), ("ms_camera_sum", ctypes.c_double),
         ("timed_iterations", ctypes.c_uint32), ("radius", ctypes.c_float * 6),
-        ("work", (ctypes.c_uint64 * 8) * 7), ("ms_kernel_sum", ctypes.c_double * 7),
+        ("work", (ctypes.c_uint64 * 8) * 9), ("ms_kernel_sum", ctypes.c_double * 9),
         ("segment_queries", ctypes.c_uint32), ("point_queries", ctypes.c_uint32),
+        ("nee_samples", ctypes.c_uint32), ("bpt_pairs", ctypes.c_uint32),
     ]
 
 
-KERNELS = ["light_pass", "camera_extend", "pb2d_query", "bb1d_query", "surf_query", "pp3d_query", "bp2d_query"]
+KERNELS = ["light_pass", "camera_extend", "pb2d_query", "bb1d_query", "surf_query", "pp3d_query", "bp2d_query",
+           "nee_connect", "bpt_connect"]
 
 
 WORK_NAMES = ["nodes", "tris", "rays", "point_cand", "point_hit", "beam_cand", "beam_hit", "vertex_loads"]

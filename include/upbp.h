@@ -151,12 +151,14 @@ typedef struct upbp_scene_desc {
 typedef struct upbp_scene upbp_scene;   /* host scene owned by the library */
 typedef struct upbp_ctx upbp_ctx;       /* device renderer state */
 
+#define UPBP_KERNEL_KINDS 9
+
 typedef struct upbp_stats {
     uint32_t light_vertices, surface_vertices, medium_vertices, light_beams;
     uint32_t light_paths, camera_paths;
     uint32_t status;              /* OR of UPBP_STATUS_* seen so far */
     uint32_t iterations_done;
-    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events; camera = extend + query kernels */
+    double ms_light, ms_build, ms_camera;   /* last iteration, CUDA events; camera = extend, connection and query kernels */
     uint64_t triangle_count;
     double scene_radius;
     /* Work counters of the last iteration, light pass then camera pass, in
@@ -167,8 +169,8 @@ typedef struct upbp_stats {
     uint64_t work_camera[8];
     uint32_t beam_chunks;         /* leaves of the last beam map */
     uint32_t kernel_launches;     /* this library's kernel launches in the last iteration */
-    uint32_t h2d_bytes;           /* host->device bytes of the last iteration (launch parameters) */
-    uint32_t d2h_bytes;           /* device->host bytes of the last iteration (counters) */
+    uint32_t h2d_bytes;           /* host->device bytes of the last iteration (launch parameters, counter pointers) */
+    uint32_t d2h_bytes;           /* device->host bytes of the last iteration (counters that size the next launches) */
     /* Pass times summed over the iterations run since the previous
      * upbp_get_stats call (at most the last 64), and their count. */
     double ms_light_sum, ms_build_sum, ms_camera_sum;
@@ -177,11 +179,12 @@ typedef struct upbp_stats {
      * radius used for the beam map (max of bb1d and bp2d when enabled). */
     float radius[6];
     /* Per kernel kind -- light pass, camera extend, PB2D, BB1D, SURF, PP3D,
-     * BP2D queries -- work counters of the last iteration and kernel times
-     * summed like the pass times above. */
-    uint64_t work[7][8];
-    double ms_kernel_sum[7];
+     * BP2D queries, NEE and BPT connections -- work counters of the last
+     * iteration and kernel times summed like the pass times above. */
+    uint64_t work[UPBP_KERNEL_KINDS][8];
+    double ms_kernel_sum[UPBP_KERNEL_KINDS];
     uint32_t segment_queries, point_queries;   /* query records of the last camera pass */
+    uint32_t nee_samples, bpt_pairs;           /* deferred connections of the last camera pass */
 } upbp_stats;
 
 /* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
