@@ -598,36 +598,92 @@ __global__ void __launch_bounds__(128) segment_query_kernel()
 // run inside one walk per thread, both leave most lanes of a warp idle.
 //
 // bb1d_search_kernel: persistent warps walk the beam map with one query per
-// lane, one node or leaf per step; a lane whose query is finished takes the
+// lane, one internal node per step; a lane whose query is finished takes the
 // next one in Morton order from a global counter, so lanes stay busy until
-// the queue is empty.  Accepted (query, beam) pairs are gathered per warp in
-// shared memory and written out 32 at a time (one atomic per 32 hits).  When
-// the list is full the pairs past the capacity are dropped but still counted,
-// and the host grows the list and repeats the search.
+// the queue is empty.  A child that is a leaf is not visited: its (query,
+// chunk) pair goes into a per-warp ring in shared memory, and whenever 32
+// pairs are waiting all lanes run the exact leaf test on one pair each, so
+// the expensive test never runs on a partly idle warp.  Accepted (query,
+// beam) pairs are gathered the same way and written out 32 at a time (one
+// atomic per 32 hits).  When the list is full the pairs past the capacity are
+// dropped but still counted, and the host grows the list and repeats the
+// search.
 constexpr int kSearchWarps = 4;
+constexpr unsigned kCandRing = 128;  // > 31 waiting + 64 new pairs per step
+
+struct SearchWarp {
+    uint2 cand[kCandRing];  // (segment-query record, beam-map leaf)
+    uint2 hit_qb[64];
+    float4 hit_geom[64];
+};
+
+// Leaf tests of the 32 (or, at the end, fewer) oldest waiting pairs, one per
+// lane; accepted pairs go to the hit buffer, which is flushed by 32.
+UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
+                              unsigned& cand, unsigned& hits)
+{
+    const DeviceParams& p = c_params;
+    const unsigned below = (1u << lane) - 1u;
+    __syncwarp();
+    BeamSegHit h;
+    bool hit = false;
+    uint2 pr = make_uint2(0u, 0u);
+    if (lane < count) {
+        pr = w.cand[(head + lane) % kCandRing];
+        const float4* r = p.seg_queue[pr.x].q;
+        const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
+        const int med = (int)fbits(__ldg(&r[2]).w);
+        hit = beam_chunk_vs_segment(p.beam_map, (int)pr.y, xyz(q0), xyz(q1), q0.w, q1.w, p.radius_bb1d_2,
+                                    p.do_bp2d != 0, med, cand, h);
+    }
+    head += count;
+    const unsigned hm = __ballot_sync(~0u, hit);
+    if (hit) {
+        const unsigned pos = hfill + __popc(hm & below);
+        w.hit_qb[pos] = make_uint2(pr.x, h.beam);
+        w.hit_geom[pos] = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
+        hits++;
+    }
+    hfill += __popc(hm);
+    if (hfill >= 32) {
+        __syncwarp();
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(&p.hit_count[0], 32u);
+        base = __shfl_sync(~0u, base, 0);
+        if (base + lane < p.hit_capacity) {
+            p.hit_qb[base + lane] = w.hit_qb[lane];
+            p.hit_geom[base + lane] = w.hit_geom[lane];
+        }
+        __syncwarp();
+        if (lane + 32 < hfill) {
+            w.hit_qb[lane] = w.hit_qb[lane + 32];
+            w.hit_geom[lane] = w.hit_geom[lane + 32];
+        }
+        hfill -= 32;
+    }
+    __syncwarp();
+}
 
 __global__ void __launch_bounds__(128) bb1d_search_kernel()
 {
     const DeviceParams& p = c_params;
-    __shared__ uint2 s_qb[kSearchWarps][64];
-    __shared__ float4 s_geom[kSearchWarps][64];
-    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ SearchWarp s_warp[kSearchWarps];
+    SearchWarp& w = s_warp[threadIdx.x >> 5];
+    const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const unsigned n = min(p.queue_count[0], p.seg_capacity);
     const BvhView bvh = p.beam_map.bvh;
     const float pad = beam_map_pad(p.rad_beam);
-    const float r2 = p.radius_bb1d_2;
-    const bool need_mask = p.do_bp2d != 0;
     WalkState s;
     s.node = kWalkDone;
-    float3 o = v3(0.f), d = v3(0.f), inv = v3(0.f);
+    float3 o = v3(0.f), inv = v3(0.f);
     float tmin = 0.f, tmax = 0.f;
-    int med = 0;
     unsigned qk = 0;
     bool exhausted = false, overflow = false;
-    unsigned fill = 0;  // same value in every lane
+    unsigned head = 0, tail = 0, hfill = 0;  // same values in every lane
     unsigned visits = 0, cand = 0, hits = 0;
     for (;;) {
+        int c0 = -1, c1 = -1;  // leaves reached this step
         const bool idle = s.node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
@@ -643,61 +699,67 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
                     const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
                     o = xyz(q0);
                     tmin = q0.w;
-                    d = xyz(q1);
                     tmax = q1.w;
-                    med = (int)fbits(__ldg(&r[2]).w);
-                    inv = safe_inv(d);
+                    inv = safe_inv(xyz(q1));
                     walk_begin(s, bvh);
+                    if (s.node < 0 && s.node != kWalkDone) {  // a one-leaf map
+                        c0 = ~s.node;
+                        s.node = kWalkDone;
+                    }
                 } else {
                     exhausted = true;
                 }
             }
         }
-        if (__all_sync(~0u, s.node == kWalkDone)) break;
-        BeamSegHit h;
-        bool hit = false;
         if (s.node != kWalkDone) {
-            const int leaf = walk_step(
-                s, bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
-                overflow, visits);
-            if (leaf >= 0) hit = beam_chunk_vs_segment(p.beam_map, leaf, o, d, tmin, tmax, r2, need_mask, med, cand, h);
-        }
-        const unsigned hm = __ballot_sync(~0u, hit);
-        if (hm) {
-            if (hit) {
-                const unsigned pos = fill + __popc(hm & below);
-                s_qb[warp][pos] = make_uint2(qk, h.beam);
-                s_geom[warp][pos] = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
-                hits++;
+            // one internal node: leaf children become pairs, internal ones are visited
+            visits++;
+            const NodeBoxes nb = load_node(bvh.nodes, s.node);
+            const bool hl = slab(nb.llo, nb.lhi, pad, o, inv, tmin, tmax);
+            const bool hr = slab(nb.rlo, nb.rhi, pad, o, inv, tmin, tmax);
+            int next = -1, other = -1;
+            if (hl) {
+                if (nb.l < 0)
+                    c0 = ~nb.l;
+                else
+                    next = nb.l;
             }
-            fill += __popc(hm);
-            if (fill >= 32) {
-                __syncwarp();
-                unsigned base = 0;
-                if (lane == 0) base = atomicAdd(&p.hit_count[0], 32u);
-                base = __shfl_sync(~0u, base, 0);
-                if (base + lane < p.hit_capacity) {
-                    p.hit_qb[base + lane] = s_qb[warp][lane];
-                    p.hit_geom[base + lane] = s_geom[warp][lane];
-                }
-                __syncwarp();
-                if (lane + 32 < fill) {
-                    s_qb[warp][lane] = s_qb[warp][lane + 32];
-                    s_geom[warp][lane] = s_geom[warp][lane + 32];
-                }
-                fill -= 32;
-                __syncwarp();
+            if (hr) {
+                if (nb.r < 0)
+                    c1 = ~nb.r;
+                else if (next < 0)
+                    next = nb.r;
+                else
+                    other = nb.r;
             }
+            if (other >= 0) {
+                if (s.sp < kStackDepth)
+                    s.stack[s.sp++] = other;
+                else
+                    overflow = true;
+            }
+            if (next >= 0)
+                s.node = next;
+            else
+                walk_pop(s);
         }
+        const unsigned m0 = __ballot_sync(~0u, c0 >= 0), m1 = __ballot_sync(~0u, c1 >= 0);
+        if (c0 >= 0) w.cand[(tail + __popc(m0 & below)) % kCandRing] = make_uint2(qk, (unsigned)c0);
+        tail += __popc(m0);
+        if (c1 >= 0) w.cand[(tail + __popc(m1 & below)) % kCandRing] = make_uint2(qk, (unsigned)c1);
+        tail += __popc(m1);
+        while (tail - head >= 32) search_test_pairs(w, head, 32, hfill, lane, cand, hits);
+        if (__all_sync(~0u, exhausted && s.node == kWalkDone)) break;
     }
+    if (tail != head) search_test_pairs(w, head, tail - head, hfill, lane, cand, hits);
     __syncwarp();
-    if (fill) {
+    if (hfill) {
         unsigned base = 0;
-        if (lane == 0) base = atomicAdd(&p.hit_count[0], fill);
+        if (lane == 0) base = atomicAdd(&p.hit_count[0], hfill);
         base = __shfl_sync(~0u, base, 0);
-        if (lane < fill && base + lane < p.hit_capacity) {
-            p.hit_qb[base + lane] = s_qb[warp][lane];
-            p.hit_geom[base + lane] = s_geom[warp][lane];
+        if (lane < hfill && base + lane < p.hit_capacity) {
+            p.hit_qb[base + lane] = w.hit_qb[lane];
+            p.hit_geom[base + lane] = w.hit_geom[lane];
         }
     }
     count_work(kCtrNodes, visits);
@@ -1025,7 +1087,7 @@ __global__ void __launch_bounds__(128, 4) camera_pass_kernel()
 // Deferred NEE: one light sample per thread -- occlusion ray through the
 // media, MIS weight, throughput.  The contribution is kept per sample until
 // k_resolve_camera knows whether an earlier step of the path failed.
-__global__ void __launch_bounds__(128) nee_connect_kernel()
+__global__ void __launch_bounds__(128, 4) nee_connect_kernel()
 {
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[4], p.nee_capacity);
@@ -1076,7 +1138,7 @@ __global__ void __launch_bounds__(128) nee_connect_kernel()
 // Deferred BPT: one (camera vertex, light vertex) pair per thread -- the
 // path-length and media checks of the connection loop, then the connection
 // with its occlusion ray; the contribution is kept per pair like NEE's.
-__global__ void __launch_bounds__(128) bpt_connect_kernel()
+__global__ void __launch_bounds__(128, 4) bpt_connect_kernel()
 {
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[5], p.bpt_capacity);
