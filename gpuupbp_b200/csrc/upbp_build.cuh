@@ -63,11 +63,6 @@ struct BoxSource {
     const uint2* chunks;      // kind 3: (beam index, chunk k | chunk count << 16)
 };
 
-// Parameter range [t0, t1) of chunk k of n along a beam of length len.  Both
-// neighbours evaluate the shared boundary with the same expression, so the
-// chunks partition [0, len) exactly.
-UPBP_HD float chunk_t(float len, unsigned k, unsigned n) { return k >= n ? len : len * (float)k / (float)n; }
-
 UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
 {
     if (s.kind == 0) {
@@ -90,15 +85,7 @@ UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
     } else {
         const uint2 ch = s.chunks[i];
         const float4 a = s.beams[ch.x].q[0], b = s.beams[ch.x].q[1];
-        const unsigned k = ch.y & 0xffffu, n = ch.y >> 16;
-        const float t0 = chunk_t(a.w, k, n), t1 = chunk_t(a.w, k + 1, n);
-        const float3 o = xyz(a) + xyz(b) * t0, e = xyz(a) + xyz(b) * t1;
-        lo = make_float3(fminf(o.x, e.x), fminf(o.y, e.y), fminf(o.z, e.z));
-        hi = make_float3(fmaxf(o.x, e.x), fmaxf(o.y, e.y), fmaxf(o.z, e.z));
-        // cover the rounding of o + d t at both ends
-        const float3 ext = (hi - lo) * 1e-6f + v3(1e-6f * (fabsf(lo.x) + fabsf(lo.y) + fabsf(lo.z) + 1e-3f));
-        lo = lo - ext;
-        hi = hi + ext;
+        chunk_box(xyz(a), xyz(b), a.w, ch.y & 0xffffu, ch.y >> 16, lo, hi);
     }
 }
 
@@ -179,7 +166,8 @@ __global__ void k_hierarchy(const unsigned* keys, int n, BvhNode* nodes, int* pa
     const int gamma = i + s * d + min(d, 0);
     const int left = (min(i, j) == gamma) ? ~gamma : gamma;
     const int right = (max(i, j) == gamma + 1) ? ~(gamma + 1) : gamma + 1;
-    nodes[i].link = make_int4(left, right, 0, 0);
+    // z, w: primitives under the left and right child
+    nodes[i].link = make_int4(left, right, gamma - min(i, j) + 1, max(i, j) - gamma);
     if (left < 0)
         parent_leaf[~left] = i;
     else
@@ -235,6 +223,20 @@ __global__ void k_refit(BoxSource s, int n, const unsigned* vals, BvhNode* nodes
         child = node;
         node = parent_internal[node];
     }
+}
+
+// Turns every child subtree of at most leaf_max (<= kLeafMaxCount)
+// primitives into one leaf over its contiguous primitive range.  Runs after
+// the refit, which needs the binary tree; the collapsed subtrees' nodes stay
+// in memory, unreferenced.
+__global__ void k_collapse(int n, BvhNode* nodes, int leaf_max)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int4 k = nodes[i].link;
+    if (k.x >= 0 && k.z <= leaf_max) k.x = leaf_link(k.x - k.z + 1, k.z);
+    if (k.y >= 0 && k.w <= leaf_max) k.y = leaf_link(k.y, k.w);
+    nodes[i].link = k;
 }
 
 // Leaf-order payloads.
@@ -293,7 +295,8 @@ __global__ void k_chunk_expand(const unsigned* counts, const unsigned* offsets, 
 }
 
 // Leaf payload of the chunked beam map: (origin, length), (direction, bits),
-// (t0, t1, medium id bits) where bits = beam index | BB1D-eligible << 31.
+// (t0, t1, medium id bits, chunk k | chunk count << 16) where bits = beam
+// index | BB1D-eligible << 31.
 __global__ void k_gather_chunks(const uint2* chunks, const BeamRec* beams, const unsigned* vals, unsigned n,
                                 unsigned bb1d_paths, float4* out)
 {
@@ -307,7 +310,7 @@ __global__ void k_gather_chunks(const uint2* chunks, const BeamRec* beams, const
     const unsigned k = ch.y & 0xffffu, c = ch.y >> 16;
     out[3 * s] = q0;
     out[3 * s + 1] = make_float4(q1.x, q1.y, q1.z, __uint_as_float(bits));
-    out[3 * s + 2] = make_float4(chunk_t(q0.w, k, c), chunk_t(q0.w, k + 1, c), q1.w, 0.f);  // z: medium id bits
+    out[3 * s + 2] = make_float4(chunk_t(q0.w, k, c), chunk_t(q0.w, k + 1, c), q1.w, __uint_as_float(ch.y));
 }
 
 // Scratch owned by a context, sized for the largest build it will run.
@@ -323,10 +326,12 @@ struct BuildScratch {
 
 // Builds an LBVH over n boxes from `src` into `nodes` (n-1 entries); on
 // return `sorted_vals` points at the leaf order (primitive index per leaf).
+// With leaf_max > 1 a leaf covers up to leaf_max consecutive primitives.
 inline cudaError_t build_lbvh(const BoxSource& src, unsigned n, BvhNode* nodes, BuildScratch& sc, cudaStream_t st,
-                              const unsigned** sorted_vals)
+                              const unsigned** sorted_vals, int leaf_max = 1)
 {
     if (n == 0) return cudaSuccess;
+    if (n > kMaxBvhPrimitives || leaf_max > kLeafMaxCount) return cudaErrorInvalidValue;  // leaf-link encoding limits
     const unsigned init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     cudaError_t e = cudaMemcpyAsync(sc.ord6, init, sizeof(init), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
@@ -345,6 +350,7 @@ inline cudaError_t build_lbvh(const BoxSource& src, unsigned n, BvhNode* nodes, 
         e = cudaMemsetAsync(sc.flags, 0, sizeof(unsigned) * (n - 1), st);
         if (e != cudaSuccess) return e;
         k_refit<<<grid, bs, 0, st>>>(src, (int)n, vb.Current(), nodes, sc.parent_internal, sc.parent_leaf, sc.flags);
+        if (leaf_max > 1) k_collapse<<<(n - 1 + bs - 1) / bs, bs, 0, st>>>((int)n, nodes, leaf_max);
     }
     return cudaGetLastError();
 }

@@ -111,7 +111,10 @@ UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& l
     unsigned visits = 0;
     for (;;) {
         if (node < 0) {
-            if (!leaf(~node)) {
+            const int first = leaf_first(node), cnt = leaf_count(node);
+            bool go = true;
+            for (int i = 0; i < cnt && go; i++) go = leaf(first + i);
+            if (!go) {
                 count_work(kCtrNodes, visits);
                 return ok;
             }
@@ -167,15 +170,20 @@ UPBP_D void walk_begin(WalkState& s, const BvhView& bvh)
 UPBP_D void walk_pop(WalkState& s) { s.node = s.sp > 0 ? s.stack[--s.sp] : kWalkDone; }
 
 // One step of a walk with s.node != kWalkDone.  Returns the sorted index of
-// the leaf this step reached, or -1 after an internal node.
+// the primitive this step reached (one per step through a leaf), or -1 after
+// an internal node.
 template <class BoxTest>
 UPBP_D int walk_step(WalkState& s, const BvhView& bvh, float pad, BoxTest&& test_box, bool& overflow,
                      unsigned& visits)
 {
     const int node = s.node;
     if (node < 0) {
-        walk_pop(s);
-        return ~node;
+        const int first = leaf_first(node), cnt = leaf_count(node);
+        if (cnt > 1)
+            s.node = leaf_link(first + 1, cnt - 1);
+        else
+            walk_pop(s);
+        return first;
     }
     visits++;
     const NodeBoxes nb = load_node(bvh.nodes, node);
@@ -234,16 +242,18 @@ UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float
     unsigned visits = 0, tests = 0;
     for (;;) {
         if (node < 0) {
-            float t, u, v;
-            const int s = ~node;
-            tests++;
-            if (tri_intersect(tv.tri, s, o, d, t, u, v) && t >= tmin && t <= best) {
-                best = t;
-                hit.t = t;
-                hit.u = u;
-                hit.v = v;
-                hit.prim = __float_as_int(__ldg(&tv.tri[3 * s]).w);
-                found = true;
+            const int first = leaf_first(node), cnt = leaf_count(node);
+            for (int s = first; s < first + cnt; s++) {
+                float t, u, v;
+                tests++;
+                if (tri_intersect(tv.tri, s, o, d, t, u, v) && t >= tmin && t <= best) {
+                    best = t;
+                    hit.t = t;
+                    hit.u = u;
+                    hit.v = v;
+                    hit.prim = __float_as_int(__ldg(&tv.tri[3 * s]).w);
+                    found = true;
+                }
             }
         } else {
             visits++;

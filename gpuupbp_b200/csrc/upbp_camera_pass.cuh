@@ -609,10 +609,10 @@ __global__ void __launch_bounds__(128) segment_query_kernel()
 // dropped but still counted, and the host grows the list and repeats the
 // search.
 constexpr int kSearchWarps = 4;
-constexpr unsigned kCandRing = 128;  // > 31 waiting + 64 new pairs per step
+constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
 
 struct SearchWarp {
-    uint2 cand[kCandRing];  // (segment-query record, beam-map leaf)
+    uint2 cand[kCandRing];  // (segment-query record, beam-map leaf | own-leaf bit << 31)
     uint2 hit_qb[64];
     float4 hit_geom[64];
 };
@@ -633,8 +633,9 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
         const float4* r = p.seg_queue[pr.x].q;
         const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
         const int med = (int)fbits(__ldg(&r[2]).w);
-        hit = beam_chunk_vs_segment(p.beam_map, (int)pr.y, xyz(q0), xyz(q1), q0.w, q1.w, p.radius_bb1d_2,
-                                    p.do_bp2d != 0, med, cand, h);
+        hit = beam_chunk_vs_segment(p.beam_map, (int)(pr.y & 0x7fffffffu), xyz(q0), xyz(q1), q0.w, q1.w,
+                                    p.radius_bb1d_2, beam_map_pad(p.rad_beam), (pr.y >> 31) != 0, p.do_bp2d != 0, med,
+                                    cand, h);
     }
     head += count;
     const unsigned hm = __ballot_sync(~0u, hit);
@@ -683,7 +684,7 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
     unsigned head = 0, tail = 0, hfill = 0;  // same values in every lane
     unsigned visits = 0, cand = 0, hits = 0;
     for (;;) {
-        int c0 = -1, c1 = -1;  // leaves reached this step
+        int f0 = 0, n0 = 0, f1 = 0, n1 = 0;  // leaves (first primitive, count) reached this step
         const bool idle = s.node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
@@ -703,7 +704,8 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
                     inv = safe_inv(xyz(q1));
                     walk_begin(s, bvh);
                     if (s.node < 0 && s.node != kWalkDone) {  // a one-leaf map
-                        c0 = ~s.node;
+                        f0 = leaf_first(s.node);
+                        n0 = leaf_count(s.node);
                         s.node = kWalkDone;
                     }
                 } else {
@@ -719,15 +721,18 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
             const bool hr = slab(nb.rlo, nb.rhi, pad, o, inv, tmin, tmax);
             int next = -1, other = -1;
             if (hl) {
-                if (nb.l < 0)
-                    c0 = ~nb.l;
-                else
+                if (nb.l < 0) {
+                    f0 = leaf_first(nb.l);
+                    n0 = leaf_count(nb.l);
+                } else {
                     next = nb.l;
+                }
             }
             if (hr) {
-                if (nb.r < 0)
-                    c1 = ~nb.r;
-                else if (next < 0)
+                if (nb.r < 0) {
+                    f1 = leaf_first(nb.r);
+                    n1 = leaf_count(nb.r);
+                } else if (next < 0)
                     next = nb.r;
                 else
                     other = nb.r;
@@ -743,12 +748,21 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
             else
                 walk_pop(s);
         }
-        const unsigned m0 = __ballot_sync(~0u, c0 >= 0), m1 = __ballot_sync(~0u, c1 >= 0);
-        if (c0 >= 0) w.cand[(tail + __popc(m0 & below)) % kCandRing] = make_uint2(qk, (unsigned)c0);
-        tail += __popc(m0);
-        if (c1 >= 0) w.cand[(tail + __popc(m1 & below)) % kCandRing] = make_uint2(qk, (unsigned)c1);
-        tail += __popc(m1);
-        while (tail - head >= 32) search_test_pairs(w, head, 32, hfill, lane, cand, hits);
+        // the primitives of the reached leaves become pairs, one per lane and
+        // round; 32 waiting pairs are tested at once
+        const int npend = n0 + n1;
+        for (int i = 0; __any_sync(~0u, i < npend); i++) {
+            const bool has = i < npend;
+            const unsigned m = __ballot_sync(~0u, has);
+            if (has) {
+                // bit 31: the pair's chunk is a leaf of its own, whose box the walk tested
+                const bool single = i < n0 ? n0 == 1 : n1 == 1;
+                w.cand[(tail + __popc(m & below)) % kCandRing] =
+                    make_uint2(qk, (unsigned)(i < n0 ? f0 + i : f1 + i - n0) | (single ? 0x80000000u : 0u));
+            }
+            tail += __popc(m);
+            if (tail - head >= 32) search_test_pairs(w, head, 32, hfill, lane, cand, hits);
+        }
         if (__all_sync(~0u, exhausted && s.node == kWalkDone)) break;
     }
     if (tail != head) search_test_pairs(w, head, tail - head, hfill, lane, cand, hits);

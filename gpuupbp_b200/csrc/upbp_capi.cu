@@ -19,6 +19,11 @@
 using namespace upbp;
 
 constexpr int kEventRing = 64;
+// Leaves of the beam map hold up to kBeamLeafMax chunks.  More chunks per
+// leaf mean fewer node visits (dependent loads) but more pair tests, and a
+// chunk reached through a shared leaf must test its own box before it may
+// report a beam; on the media workload single-chunk leaves are fastest.
+constexpr int kBeamLeafMax = 1;
 // events per iteration: start, light done, maps done, then one after each
 // camera-side kernel kind (extend, nee, bpt, pb2d, bb1d, surf, pp3d, bp2d)
 constexpr int kEvPerIter = 3 + (kKernCount - 1);
@@ -462,6 +467,13 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         P.scene_center = (hi + lo) * .5f;
         P.scene_radius = std::sqrt(r2) * .5f;
         P.inv_radius_sqr = 1.f / (P.scene_radius * P.scene_radius);
+        // largest coordinate magnitude the range queries see (scene and camera)
+        const float3 co = cam.origin;
+        const float mag = std::max(std::max(std::fabs(P.scene_center.x), std::fabs(P.scene_center.y)),
+                                   std::fabs(P.scene_center.z)) + P.scene_radius;
+        const float coord = std::max(mag, std::max(std::max(std::fabs(co.x), std::fabs(co.y)), std::fabs(co.z)));
+        P.cull_eps = 1e-6f * coord;
+        P.beam_cull_eps = 1e-4f * coord;
     }
 
     // configuration (renderer_init.cpp:681-925)
@@ -756,12 +768,12 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         src.beams = c->d_beams;
         src.chunks = c->d_chunks;
         const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
+        UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order, kBeamLeafMax));
         k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
                                                                   P.bb1d_used_light_subpath_count, c->d_beam_seg);
         P.beam_map.bvh.count = nchunks;
         c->last_chunks = nchunks;
-        launches += 2 + (nchunks > 1 ? 4 : 2) + 1;
+        launches += 2 + (nchunks > 1 ? (kBeamLeafMax > 1 ? 5 : 4) : 2) + 1;
     }
     UPBP_CK(cudaGetLastError());
     P.n_surface = found[1];

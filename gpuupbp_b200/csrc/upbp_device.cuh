@@ -72,13 +72,23 @@ struct DCamera {
 };
 
 // Two-wide BVH node: both children's boxes + child links.  A link >= 0 is an
-// internal node, a link < 0 is ~(leaf position in the sorted primitive order).
+// internal node, a link < 0 is a leaf: ~(first | (count - 1) << 27) for the
+// `count` consecutive primitives (count 1 unless the tree was built with
+// multi-primitive leaves) from position `first` of the sorted order.  z and
+// w count the primitives under the left and right child.
 struct BvhNode {
     float4 a;   // left.lo.xyz, left.hi.x
     float4 b;   // left.hi.yz, right.lo.xy
     float4 c;   // right.lo.z, right.hi.xyz
-    int4 link;  // left, right, -, -
+    int4 link;  // left, right, left count, right count
 };
+
+constexpr int kLeafShift = 27;
+constexpr int kLeafMaxCount = 16;
+constexpr unsigned kMaxBvhPrimitives = 1u << kLeafShift;
+UPBP_HD int leaf_link(int first, int count) { return ~(first | ((count - 1) << kLeafShift)); }
+UPBP_HD int leaf_first(int link) { return (~link) & ((1 << kLeafShift) - 1); }
+UPBP_HD int leaf_count(int link) { return ((~link) >> kLeafShift) + 1; }
 
 struct BvhView {
     const BvhNode* nodes;
@@ -167,11 +177,39 @@ struct PointMap {
 
 // Beam map: BVH over beam chunks (sub-segments of each beam) in leaf order.
 //   seg[3i] = (origin.xyz, length), seg[3i+1] = (direction.xyz, beam index bits),
-//   seg[3i+2] = (t0, t1) of the beam chunk this leaf covers, beam medium id bits
+//   seg[3i+2] = (t0, t1) of the beam chunk this leaf covers, beam medium id
+//   bits, chunk index | chunk count << 16 bits
 struct BeamMap {
     BvhView bvh;
     const float4* seg;
 };
+
+// Parameter range [t0, t1) of chunk k of n along a beam of length len.  Both
+// neighbours evaluate the shared boundary with the same expression, so the
+// chunks partition [0, len) exactly.
+UPBP_HD float chunk_t(float len, unsigned k, unsigned n) { return k >= n ? len : len * (float)k / (float)n; }
+
+// Box of chunk k of n of the beam (o, d, len): the beam-map builder's leaf
+// box, widened to cover the rounding of o + d t at both ends.
+UPBP_HD void chunk_box(float3 o, float3 d, float len, unsigned k, unsigned n, float3& lo, float3& hi)
+{
+    const float t0 = chunk_t(len, k, n), t1 = chunk_t(len, k + 1, n);
+    const float3 a = o + d * t0, e = o + d * t1;
+    lo = make_float3(fminf(a.x, e.x), fminf(a.y, e.y), fminf(a.z, e.z));
+    hi = make_float3(fmaxf(a.x, e.x), fmaxf(a.y, e.y), fmaxf(a.z, e.z));
+    const float3 ext = (hi - lo) * 1e-6f + v3(1e-6f * (fabsf(lo.x) + fabsf(lo.y) + fabsf(lo.z) + 1e-3f));
+    lo = lo - ext;
+    hi = hi + ext;
+}
+
+// Chunk of n holding parameter t of a beam of length len (t in [0, len)).
+UPBP_HD unsigned chunk_of(float t, float len, unsigned n)
+{
+    unsigned k = (unsigned)fminf(fmaxf(t / len * (float)n, 0.f), (float)(n - 1));
+    while (k > 0 && t < chunk_t(len, k, n)) k--;
+    while (k + 1 < n && t >= chunk_t(len, k + 1, n)) k++;
+    return k;
+}
 
 struct DeviceParams {
     // scene
@@ -186,6 +224,11 @@ struct DeviceParams {
     DCamera camera;
     float3 scene_center;
     float scene_radius, inv_radius_sqr;
+    // Margins of the range queries' box culling beyond the radius: cull_eps
+    // covers the rounding of box tests at the scene's coordinate magnitude;
+    // beam_cull_eps (BB1D) also covers the predicate's error in t1 for
+    // nearly parallel lines.
+    float cull_eps, beam_cull_eps;
     TriView real;
     TriView imag;
 

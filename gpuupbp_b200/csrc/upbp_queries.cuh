@@ -15,7 +15,7 @@ namespace upbp {
 template <class F>
 UPBP_D void points_in_radius(const PointMap& map, float3 x, float r, float r2, F&& f)
 {
-    const float pad = r * 1.0001f + 1e-7f;
+    const float pad = r * 1.0001f + c_params.cull_eps;
     unsigned cand = 0, hits = 0;
     const bool ok = bvh_walk(
         map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
@@ -40,7 +40,7 @@ UPBP_D void points_near_segment(const PointMap& map, float3 o, float3 d, float t
                                 F&& f)
 {
     const float3 inv = safe_inv(d);
-    const float pad = r * 1.0001f + 1e-7f;
+    const float pad = r * 1.0001f + c_params.cull_eps;
     unsigned cand = 0, hits = 0;
     const bool ok = bvh_walk(
         map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
@@ -71,12 +71,33 @@ struct BeamSegHit {
     float dist, sin_theta, t1, t2;
 };
 
+// Segment [tmin, tmax] of (o, d) vs chunk k of n of a beam, with the box
+// test of the beam-map walk (same box, same dilation).
+UPBP_D bool chunk_reached(float3 bo, float3 bd, float len, unsigned k, unsigned n, float pad, float3 o, float3 d,
+                          float tmin, float tmax)
+{
+    float3 lo, hi;
+    chunk_box(bo, bd, len, k, n, lo, hi);
+    return slab(lo, hi, pad, o, safe_inv(d), tmin, tmax);
+}
+
 // The BB1D test of one beam-map leaf against a query segment: the path mask,
-// the medium filter, the exact beam-beam predicate and the rule that only
-// the chunk holding the beam's closest point reports it.  cand counts the
-// leaves that reach the predicate.
+// the medium filter and the exact beam-beam predicate, which looks at the
+// whole beam, so every chunk of an accepted beam passes it; one of them
+// reports the beam.  That is the chunk holding the beam's closest point t2
+// when the walk reaches its box.  The predicate's t2 can be far from the
+// true closest point (it divides by d1.d2, which is tiny for nearly
+// perpendicular lines), and then the chunk holding it can lie outside the
+// query's reach: in that case the first chunk of the beam whose box the query
+// reaches reports instead (a check that is only needed when the computed
+// closest points are far apart).  A chunk whose own box passes the walk's box test
+// is always visited, so exactly one chunk reports each accepted beam, and
+// the set equals a test of every beam (a chunk reached only as part of a
+// leaf of several chunks never reports).  cand counts the leaves that reach
+// the predicate; pad is the walk's box dilation; own_box tells that the walk
+// reached this chunk through a leaf of its own (so its box passed).
 UPBP_D bool beam_chunk_vs_segment(const BeamMap& map, int i, float3 o, float3 d, float tmin, float tmax, float r2,
-                                  bool need_mask, int med, unsigned& cand, BeamSegHit& h)
+                                  float pad, bool own_box, bool need_mask, int med, unsigned& cand, BeamSegHit& h)
 {
     const float4 s1 = __ldg(&map.seg[3 * i + 1]);
     const unsigned bits = fbits(s1.w);
@@ -85,17 +106,35 @@ UPBP_D bool beam_chunk_vs_segment(const BeamMap& map, int i, float3 o, float3 d,
     if (med >= 0 && (int)fbits(s2.z) != med) return false;
     const float4 s0 = __ldg(&map.seg[3 * i]);
     cand++;
-    if (pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, h.dist, h.sin_theta, h.t1, h.t2) &&
-        h.t2 >= s2.x && h.t2 < s2.y) {
-        h.beam = bits & 0x7fffffffu;
-        return true;
-    }
-    return false;
+    if (!pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, h.dist, h.sin_theta, h.t1, h.t2)) return false;
+    h.beam = bits & 0x7fffffffu;
+    const bool mine = h.t2 >= s2.x && h.t2 < s2.y;
+    const float3 bo = xyz(s0), bd = xyz(s1);
+    // Usual case: the computed closest points lie within the dilation of each
+    // other (less a rounding margin), so the query passes through the dilated
+    // own box of the chunk holding t2 at t1, and the walk reached that chunk.
+    const float3 gap = (o + d * h.t1) - (bo + bd * h.t2);
+    const float inner = pad - 2.f * c_params.cull_eps;
+    if (inner > 0.f && dot(gap, gap) <= inner * inner) return mine;
+    const unsigned kc = fbits(s2.w), k = kc & 0xffffu, n = kc >> 16;
+    // a leaf of several chunks is visited when any of its chunks is in
+    // reach, so this chunk's own box decides, as for every other chunk
+    if (!own_box && !chunk_reached(bo, bd, s0.w, k, n, pad, o, d, tmin, tmax)) return false;
+    if (mine) return true;
+    if (chunk_reached(bo, bd, s0.w, chunk_of(h.t2, s0.w, n), n, pad, o, d, tmin, tmax)) return false;
+    for (unsigned j = 0; j < k; j++)
+        if (chunk_reached(bo, bd, s0.w, j, n, pad, o, d, tmin, tmax)) return false;
+    return true;
 }
 
-// Box dilation of beam-map walks: the beam radius with a small margin, so
-// rounding in the box test never drops a leaf the predicate accepts.
-UPBP_D float beam_map_pad(float pad_r) { return pad_r * 1.0001f + 1e-7f; }
+// Box dilation of BB1D beam-map walks: the beam radius with a margin for the
+// box tests' rounding and for the predicate's error in t1 on nearly parallel
+// lines: for 1 - dd^2 >= 1e-5 (the predicate rejects flatter pairs) t1 is off
+// by at most ~2.4e-7 |coordinates| / (1 - dd^2), so the query point at the
+// computed t1 can lie up to ~8e-5 |coordinates| farther from the beam than
+// the line distance.  With beam_cull_eps the walk reaches every beam the
+// predicate accepts.
+UPBP_D float beam_map_pad(float pad_r) { return pad_r * 1.0001f + c_params.beam_cull_eps; }
 
 template <class F>
 UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmin, float tmax, float pad_r, float r2,
@@ -112,7 +151,7 @@ UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmi
             s, map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
             overflow, visits);
         BeamSegHit h;
-        if (leaf >= 0 && beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, need_mask, med, cand, h)) {
+        if (leaf >= 0 && beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, pad, false, need_mask, med, cand, h)) {
             hits++;
             f(h.beam, h.dist, h.sin_theta, h.t1, h.t2);
         }
@@ -128,7 +167,7 @@ UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmi
 template <class F>
 UPBP_D void beams_near_point(const BeamMap& map, float3 x, float pad_r, float r2, F&& f)
 {
-    const float pad = pad_r * 1.0001f + 1e-7f;
+    const float pad = pad_r * 1.0001f + c_params.cull_eps;
     unsigned cand = 0, hits = 0;
     const bool ok = bvh_walk(
         map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },

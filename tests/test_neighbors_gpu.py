@@ -91,3 +91,76 @@ def test_neighbour_sets_equal_brute_force(scene_dir, workload, tiny, args):
     n = _check(r, 4, q, lambda qq: neighbors.beams_near_point(beams, qq[:3], np.float32(rb2) ** 2))
     assert n > 50
     r.close()
+
+
+def _media_renderer(scene_dir):
+    return _renderer(scene_dir, "media_field", True,
+                     ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "12", "-r", "64x64"])
+
+
+def _beam_frames(beams, rb1, rng, n):
+    long_ = beams[beams[:, 3] > 8 * rb1]
+    assert len(long_) > 100
+    b = long_[rng.integers(0, len(long_), n)].astype(np.float64)
+    d2 = b[:, 4:7] / np.linalg.norm(b[:, 4:7], axis=1, keepdims=True)
+    a = rng.normal(size=(n, 3))
+    u = a - d2 * np.sum(a * d2, axis=1, keepdims=True)
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    mid = b[:, :3] + d2 * (b[:, 3] * rng.uniform(0.2, 0.8, n))[:, None]
+    return d2, u, np.cross(d2, u), mid
+
+
+def test_bb1d_near_parallel_queries_equal_brute_force(scene_dir):
+    """BB1D queries almost parallel to a beam (1 - dd^2 from 1.5e-5 up) at a
+    distance just under the radius, on the media scene whose coordinates are
+    large against the radius: the predicate's t1 carries its largest error
+    there.  The set must equal brute force."""
+    r = _media_renderer(scene_dir)
+    rb1 = np.float32(r.stats()["radius"][0])
+    beams = r.photons(2)
+    rng = np.random.default_rng(23)
+    n = 2000
+    d2, u, v, mid = _beam_frames(beams, rb1, rng, n)
+    sin2 = 10.0 ** rng.uniform(np.log10(1.5e-5), -3.0, n)
+    d1 = np.sqrt(1.0 - sin2)[:, None] * d2 + np.sqrt(sin2)[:, None] * u
+    centre = mid + v * (float(rb1) * rng.uniform(0.5, 0.999, n))[:, None]
+    half = 20.0 * float(rb1)
+    q = np.zeros((n, 8), np.float32)
+    q[:, :3] = centre - d1 * half
+    q[:, 3:6] = d1
+    q[:, 7] = 2 * half
+    # half of the segments end short of the closest approach, by up to the
+    # size of the predicate's error in t1, where only that error accepts them
+    short = np.arange(n) % 2 == 1
+    extent = float(np.abs(beams[:, :3]).max())
+    q[short, 7] = half - rng.uniform(0.0, 0.02 * extent, short.sum())
+    nonempty = _check(r, 3, q, lambda qq: neighbors.beams_near_segment(beams, qq, rb1 ** 2))
+    assert nonempty > n // 4
+    r.close()
+
+
+def test_bb1d_near_perpendicular_queries_equal_brute_force(scene_dir):
+    """BB1D queries almost perpendicular to a beam (|d1.d2| from 1e-7 to
+    1e-2).  The predicate computes the beam's closest point by dividing by
+    d1.d2, so it can land far from where the query passes; the beam must
+    still be reported once, exactly as brute force reports it."""
+    r = _media_renderer(scene_dir)
+    rb1 = np.float32(r.stats()["radius"][0])
+    beams = r.photons(2)
+    rng = np.random.default_rng(29)
+    n = 3000
+    d2, u, v, mid = _beam_frames(beams, rb1, rng, n)
+    eps = 10.0 ** rng.uniform(-7.0, -2.0, n) * rng.choice([-1.0, 1.0], n)
+    d1 = u + eps[:, None] * d2
+    d1 /= np.linalg.norm(d1, axis=1, keepdims=True)
+    w = np.cross(d1, d2)
+    w /= np.linalg.norm(w, axis=1, keepdims=True)
+    centre = mid + w * (float(rb1) * rng.uniform(0.0, 0.999, n))[:, None]
+    half = float(rb1) * rng.uniform(2.0, 10.0, n)
+    q = np.zeros((n, 8), np.float32)
+    q[:, :3] = centre - d1 * half[:, None]
+    q[:, 3:6] = d1
+    q[:, 7] = 2 * half
+    nonempty = _check(r, 3, q, lambda qq: neighbors.beams_near_segment(beams, qq, rb1 ** 2))
+    assert nonempty > n // 4
+    r.close()
