@@ -611,10 +611,16 @@ __global__ void __launch_bounds__(128) segment_query_kernel()
 constexpr int kSearchWarps = 4;
 constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
 
+// The top kSmemStack entries of each lane's traversal stack live in shared
+// memory (column per lane, so lanes never share a bank); deeper entries go
+// to local memory.  Local memory competes with the beam map for L1.
+constexpr int kSmemStack = 16;
+
 struct SearchWarp {
     uint2 cand[kCandRing];  // (segment-query record, beam-map leaf | own-leaf bit << 31)
     uint2 hit_qb[64];
     float4 hit_geom[64];
+    int stack[kSmemStack][32];
 };
 
 // Leaf tests of the 32 (or, at the end, fewer) oldest waiting pairs, one per
@@ -675,8 +681,8 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
     const unsigned n = min(p.queue_count[0], p.seg_capacity);
     const BvhView bvh = p.beam_map.bvh;
     const float pad = beam_map_pad(p.rad_beam);
-    WalkState s;
-    s.node = kWalkDone;
+    int node = kWalkDone, sp = 0;
+    int deep[kStackDepth - kSmemStack];
     float3 o = v3(0.f), inv = v3(0.f);
     float tmin = 0.f, tmax = 0.f;
     unsigned qk = 0;
@@ -685,7 +691,7 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
     unsigned visits = 0, cand = 0, hits = 0;
     for (;;) {
         int f0 = 0, n0 = 0, f1 = 0, n1 = 0;  // leaves (first primitive, count) reached this step
-        const bool idle = s.node == kWalkDone;
+        const bool idle = node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
             const int leader = __ffs(want) - 1;
@@ -702,21 +708,21 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
                     tmin = q0.w;
                     tmax = q1.w;
                     inv = safe_inv(xyz(q1));
-                    walk_begin(s, bvh);
-                    if (s.node < 0 && s.node != kWalkDone) {  // a one-leaf map
-                        f0 = leaf_first(s.node);
-                        n0 = leaf_count(s.node);
-                        s.node = kWalkDone;
+                    sp = 0;
+                    node = bvh.count > 1 ? 0 : kWalkDone;
+                    if (bvh.count == 1) {  // a one-leaf map
+                        f0 = 0;
+                        n0 = 1;
                     }
                 } else {
                     exhausted = true;
                 }
             }
         }
-        if (s.node != kWalkDone) {
+        if (node != kWalkDone) {
             // one internal node: leaf children become pairs, internal ones are visited
             visits++;
-            const NodeBoxes nb = load_node(bvh.nodes, s.node);
+            const NodeBoxes nb = load_node(bvh.nodes, node);
             const bool hl = slab(nb.llo, nb.lhi, pad, o, inv, tmin, tmax);
             const bool hr = slab(nb.rlo, nb.rhi, pad, o, inv, tmin, tmax);
             int next = -1, other = -1;
@@ -738,15 +744,21 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
                     other = nb.r;
             }
             if (other >= 0) {
-                if (s.sp < kStackDepth)
-                    s.stack[s.sp++] = other;
+                if (sp < kSmemStack)
+                    w.stack[sp++][lane] = other;
+                else if (sp < kStackDepth)
+                    deep[sp++ - kSmemStack] = other;
                 else
                     overflow = true;
             }
-            if (next >= 0)
-                s.node = next;
-            else
-                walk_pop(s);
+            if (next >= 0) {
+                node = next;
+            } else if (sp > 0) {
+                --sp;
+                node = sp < kSmemStack ? w.stack[sp][lane] : deep[sp - kSmemStack];
+            } else {
+                node = kWalkDone;
+            }
         }
         // the primitives of the reached leaves become pairs, one per lane and
         // round; 32 waiting pairs are tested at once
@@ -763,7 +775,7 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
             tail += __popc(m);
             if (tail - head >= 32) search_test_pairs(w, head, 32, hfill, lane, cand, hits);
         }
-        if (__all_sync(~0u, exhausted && s.node == kWalkDone)) break;
+        if (__all_sync(~0u, exhausted && node == kWalkDone)) break;
     }
     if (tail != head) search_test_pairs(w, head, tail - head, hfill, lane, cand, hits);
     __syncwarp();
