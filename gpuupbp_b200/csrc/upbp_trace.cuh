@@ -133,7 +133,9 @@ UPBP_D bool init_boundary_stack(BoundaryStack& s)
 // a medium scattering point was found (result.dist), `segs` holds the medium
 // segments up to that point (with sampling pdfs) and `lsegs` the segments up
 // to the next real surface.  Returns a status bit (0 on success).
-UPBP_D unsigned intersect_scene(bool& hit, float3 ro, float3 rd, Isect& result, BoundaryStack& bstack,
+// Kept out of line: inlined into every caller it made the path kernels too large
+// for the instruction cache.
+__device__ __noinline__ unsigned intersect_scene(bool& hit, float3 ro, float3 rd, Isect& result, BoundaryStack& bstack,
                                 unsigned options, unsigned sflags, VolSeg* segs, int& nseg, LiteSeg* lsegs,
                                 int& nlseg, Rng& rng)
 {
