@@ -117,8 +117,8 @@ def algorithmic_bytes(work: dict, extra: float = 0.0) -> float:
 
 # Bytes of the query records each camera-side kernel writes or reads.
 SEG_RECORD, POINT_RECORD = 128, 144
-# BB1D hit-list entry (query, beam, distance, sin theta, t1, t2), written by
-# the search kernel and read by the evaluation kernel.
+# PB2D / BB1D hit-list entry (query, neighbour, 4 floats), written by the
+# search kernel and read by the evaluation kernel.
 HIT_RECORD = 24
 # Deferred connections: an NEE sample reads its 80 B record and 64 B of its
 # camera vertex and writes a 16 B contribution; a BPT pair reads its 8 B
@@ -134,9 +134,10 @@ def kernel_rooflines(st: dict, pixels: int) -> dict:
     nseg, npt = st["segment_queries"], st["point_queries"]
     nnee, npairs = st["nee_samples"], st["bpt_pairs"]
     hits = st["work"]["bb1d_query"]["beam_hit"]
+    pb2d_hits = st["work"]["pb2d_query"]["point_hit"]
     extra = {"light_pass": 0.0,
              "camera_extend": 12.0 * pixels + SEG_RECORD * nseg + POINT_RECORD * npt,
-             "pb2d_query": SEG_RECORD * nseg, "bb1d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * hits,
+             "pb2d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * pb2d_hits, "bb1d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * hits,
              "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt, "bp2d_query": POINT_RECORD * npt,
              "nee_connect": NEE_BYTES * nnee, "bpt_connect": PAIR_BYTES * npairs}
     out = {}

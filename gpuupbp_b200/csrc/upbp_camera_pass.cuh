@@ -424,32 +424,6 @@ UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& w
     return mis * unweighted;
 }
 
-UPBP_D float3 query_pb2d(const QuerySeg& q, const StateWeights& cw)
-{
-    const DeviceParams& p = c_params;
-    float3 acc = v3(0.f);
-    points_near_segment(p.med_map, q.o, q.d, q.dmin, q.dmax, p.radius_pb2d, p.radius_pb2d_2,
-                        [&](unsigned slot, float dist, float rad2) {
-                            LightVertex lv;
-                            load_vertex(p.vertices + slot, lv);
-                            acc += eval_pb2d(q, cw, lv, dist, rad2);
-                        });
-    return acc;
-}
-
-UPBP_D float3 query_bb1d(const QuerySeg& q, const StateWeights& cw)
-{
-    const DeviceParams& p = c_params;
-    float3 acc = v3(0.f);
-    beams_near_segment(p.beam_map, q.o, q.d, q.dmin, q.dmax, p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0, q.med,
-                       [&](unsigned b, float bb, float st, float t1, float t2) {
-                           Beam lb;
-                           load_beam(p.beams + b, lb);
-                           acc += eval_bb1d(q, cw, lb, bb, st, t1, t2);
-                       });
-    return acc;
-}
-
 UPBP_D float3 query_bp2d(float3 x, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb)
 {
     const DeviceParams& p = c_params;
@@ -572,32 +546,13 @@ UPBP_D void splat_camera(unsigned px, float3 c)
     }
 }
 
-// PB2D (kBb1d = false) or BB1D (kBb1d = true) for one segment-query record
-// per thread; adds weight * normalization * estimate into the camera image.
-template <bool kBb1d>
-__global__ void __launch_bounds__(128) segment_query_kernel()
-{
-    const DeviceParams& p = c_params;
-    const unsigned n = min(*p.queue_count, p.seg_capacity);
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const unsigned k = p.seg_order ? __ldg(&p.seg_order[j]) : j;
-        QuerySeg q;
-        StateWeights cw;
-        float3 weight;
-        unsigned pk, path, key;
-        load_seg_query(k, q, cw, weight, pk, path, key);
-        if (!event_kept(path, key)) continue;
-        const float3 est = kBb1d ? query_bb1d(q, cw) : query_pb2d(q, cw);
-        const float norm = kBb1d ? p.bb1d_normalization : p.pb2d_normalization;
-        splat_camera(pk >> 8, weight * norm * est);
-    }
-}
-
-// BB1D in two kernels.  A long query segment crosses hundreds of beam chunks
-// and a short one a few, and every accepted beam costs a full MIS evaluation;
-// run inside one walk per thread, both leave most lanes of a warp idle.
+// BB1D and PB2D in two kernels each.  A long query segment crosses hundreds
+// of beam chunks (or photons) and a short one a few, and every accepted
+// neighbour costs a full MIS evaluation; run inside one walk per thread, both
+// leave most lanes of a warp idle.
 //
-// bb1d_search_kernel: persistent warps walk the beam map with one query per
+// segment_search_kernel<kBeams>: persistent warps walk the beam map (BB1D)
+// or the medium photon map (PB2D) with one query per
 // lane, one internal node per step; a lane whose query is finished takes the
 // next one in Morton order from a global counter, so lanes stay busy until
 // the queue is empty.  A child that is a leaf is not visited: its (query,
@@ -624,31 +579,47 @@ struct SearchWarp {
 };
 
 // Leaf tests of the 32 (or, at the end, fewer) oldest waiting pairs, one per
-// lane; accepted pairs go to the hit buffer, which is flushed by 32.
+// lane; accepted pairs go to the hit buffer, which is flushed by 32.  A hit
+// is (query, beam) + (distance, sin theta, t1, t2) for BB1D and (query,
+// light-vertex slot) + (distance along the query, squared radius) for PB2D.
+template <bool kBeams>
 UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
                               unsigned& cand, unsigned& hits)
 {
     const DeviceParams& p = c_params;
     const unsigned below = (1u << lane) - 1u;
     __syncwarp();
-    BeamSegHit h;
     bool hit = false;
     uint2 pr = make_uint2(0u, 0u);
+    unsigned id = 0;
+    float4 geom = make_float4(0.f, 0.f, 0.f, 0.f);
     if (lane < count) {
         pr = w.cand[(head + lane) % kCandRing];
         const float4* r = p.seg_queue[pr.x].q;
         const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
-        const int med = (int)fbits(__ldg(&r[2]).w);
-        hit = beam_chunk_vs_segment(p.beam_map, (int)(pr.y & 0x7fffffffu), xyz(q0), xyz(q1), q0.w, q1.w,
-                                    p.radius_bb1d_2, beam_map_pad(p.rad_beam), (pr.y >> 31) != 0, p.do_bp2d != 0, med,
-                                    cand, h);
+        if (kBeams) {
+            BeamSegHit h;
+            const int med = (int)fbits(__ldg(&r[2]).w);
+            hit = beam_chunk_vs_segment(p.beam_map, (int)(pr.y & 0x7fffffffu), xyz(q0), xyz(q1), q0.w, q1.w,
+                                        p.radius_bb1d_2, beam_map_pad(p.rad_beam), (pr.y >> 31) != 0, p.do_bp2d != 0,
+                                        med, cand, h);
+            id = h.beam;
+            geom = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
+        } else {
+            const float4 pp = __ldg(&p.med_map.pos[pr.y & 0x7fffffffu]);
+            float dist, rad2;
+            cand++;
+            hit = pred_ray_disc(xyz(q0), xyz(q1), q0.w, q1.w, xyz(pp), p.radius_pb2d_2, dist, rad2);
+            id = fbits(pp.w);
+            geom = make_float4(dist, rad2, 0.f, 0.f);
+        }
     }
     head += count;
     const unsigned hm = __ballot_sync(~0u, hit);
     if (hit) {
         const unsigned pos = hfill + __popc(hm & below);
-        w.hit_qb[pos] = make_uint2(pr.x, h.beam);
-        w.hit_geom[pos] = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
+        w.hit_qb[pos] = make_uint2(pr.x, id);
+        w.hit_geom[pos] = geom;
         hits++;
     }
     hfill += __popc(hm);
@@ -671,7 +642,8 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(128) bb1d_search_kernel()
+template <bool kBeams>
+__global__ void __launch_bounds__(128) segment_search_kernel()
 {
     const DeviceParams& p = c_params;
     __shared__ SearchWarp s_warp[kSearchWarps];
@@ -679,8 +651,8 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
     const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const unsigned n = min(p.queue_count[0], p.seg_capacity);
-    const BvhView bvh = p.beam_map.bvh;
-    const float pad = beam_map_pad(p.rad_beam);
+    const BvhView bvh = kBeams ? p.beam_map.bvh : p.med_map.bvh;
+    const float pad = kBeams ? beam_map_pad(p.rad_beam) : p.radius_pb2d * 1.0001f + p.cull_eps;
     int node = kWalkDone, sp = 0;
     int deep[kStackDepth - kSmemStack];
     float3 o = v3(0.f), inv = v3(0.f);
@@ -773,11 +745,11 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
                     make_uint2(qk, (unsigned)(i < n0 ? f0 + i : f1 + i - n0) | (single ? 0x80000000u : 0u));
             }
             tail += __popc(m);
-            if (tail - head >= 32) search_test_pairs(w, head, 32, hfill, lane, cand, hits);
+            if (tail - head >= 32) search_test_pairs<kBeams>(w, head, 32, hfill, lane, cand, hits);
         }
         if (__all_sync(~0u, exhausted && node == kWalkDone)) break;
     }
-    if (tail != head) search_test_pairs(w, head, tail - head, hfill, lane, cand, hits);
+    if (tail != head) search_test_pairs<kBeams>(w, head, tail - head, hfill, lane, cand, hits);
     __syncwarp();
     if (hfill) {
         unsigned base = 0;
@@ -789,15 +761,16 @@ __global__ void __launch_bounds__(128) bb1d_search_kernel()
         }
     }
     count_work(kCtrNodes, visits);
-    count_work(kCtrBeamCand, cand);
-    count_work(kCtrBeamHit, hits);
+    count_work(kBeams ? kCtrBeamCand : kCtrPointCand, cand);
+    count_work(kBeams ? kCtrBeamHit : kCtrPointHit, hits);
     if (overflow) flag_status(kErrTraversalStack);
 }
 
-// bb1d_eval_kernel: one accepted (query, beam) pair per thread, so every lane
-// runs the same MIS evaluation; adds weight * normalization * estimate into
-// the camera image.
-__global__ void __launch_bounds__(128) bb1d_eval_kernel()
+// segment_eval_kernel<kBeams>: one accepted pair per thread, so every lane
+// runs the same MIS evaluation (eval_bb1d or eval_pb2d); adds weight *
+// normalization * estimate into the camera image.
+template <bool kBeams>
+__global__ void __launch_bounds__(128) segment_eval_kernel()
 {
     const DeviceParams& p = c_params;
     const unsigned n = min(p.hit_count[0], p.hit_capacity);
@@ -810,10 +783,17 @@ __global__ void __launch_bounds__(128) bb1d_eval_kernel()
         unsigned pk, path, key;
         load_seg_query(qb.x, q, cw, weight, pk, path, key);
         if (!event_kept(path, key)) continue;
-        Beam lb;
-        load_beam(p.beams + qb.y, lb);
-        const float3 est = eval_bb1d(q, cw, lb, g.x, g.y, g.z, g.w);
-        splat_camera(pk >> 8, weight * p.bb1d_normalization * est);
+        float3 est;
+        if (kBeams) {
+            Beam lb;
+            load_beam(p.beams + qb.y, lb);
+            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, g.x, g.y, g.z, g.w);
+        } else {
+            LightVertex lv;
+            load_vertex(p.vertices + qb.y, lv);
+            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, g.x, g.y);
+        }
+        splat_camera(pk >> 8, weight * est);
     }
 }
 

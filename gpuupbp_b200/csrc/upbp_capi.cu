@@ -165,7 +165,7 @@ struct upbp_ctx {
     unsigned hit_capacity = 0;
     unsigned* d_hit_count = nullptr;
     unsigned h_hit_count[2] = {0, 0};
-    int search_grid = 0;
+    int search_grid = 0, search_grid_pb2d = 0;
     int camera_grid = 0;   // resident blocks of the persistent camera pass
     int light_grid = 0;    // resident blocks of the persistent light pass
     // Morton sort of the query records: keys/values and their alternates per queue
@@ -569,8 +569,10 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         int dev = 0, sms = 0, per_sm = 0;
         UPBP_CK(cudaGetDevice(&dev));
         UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb1d_search_kernel, 128, 0));
+        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, segment_search_kernel<true>, 128, 0));
         c->search_grid = std::max(1, sms * std::max(1, per_sm));
+        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, segment_search_kernel<false>, 128, 0));
+        c->search_grid_pb2d = std::max(1, sms * std::max(1, per_sm));
         UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, camera_pass_kernel, 128, 0));
         c->camera_grid = std::max(1, sms * std::max(1, per_sm));
         UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light_pass_kernel, 128, 0));
@@ -878,28 +880,26 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         h2d += sizeof(P);
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
     }
-    if (run_pb2d) {
-        UPBP_CK(set_work(kKernPb2d));
-        segment_query_kernel<false><<<grid_for(nseg), 128, 0, c->st>>>();
-        launches++;
-    }
-    UPBP_CK(cudaEventRecord(ev[6], c->st));
-    if (run_bb1d) {
-        // search: (query, beam) pairs into the hit list; a list that was too
-        // small is grown and the search repeated (it is a pure function of
-        // the queries and the beam map)
-        UPBP_CK(set_work(kKernBb1d));
+    // PB2D and BB1D: search (query, neighbour) pairs into the hit list, then
+    // evaluate them; a list that was too small is grown and the search
+    // repeated (it is a pure function of the queries and the map)
+    auto segment_estimator = [&](bool beams) -> int {
+        const int kern = beams ? kKernBb1d : kKernPb2d;
+        UPBP_CK(set_work(kern));
         if (c->hit_capacity == 0 && ensure_hits(c, (size_t)nseg * 32) != UPBP_OK) return UPBP_ERR_CUDA;
         for (int attempt = 0; attempt < 2; attempt++) {
             UPBP_CK(cudaMemsetAsync(c->d_hit_count, 0, 2 * sizeof(unsigned), c->st));
-            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernBb1d * kCtrCount, 0,
-                                    kCtrCount * sizeof(unsigned long long), c->st));
+            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kern * kCtrCount, 0, kCtrCount * sizeof(unsigned long long),
+                                    c->st));
             P.hit_qb = c->d_hit_qb;
             P.hit_geom = c->d_hit_geom;
             P.hit_capacity = c->hit_capacity;
             h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-            bb1d_search_kernel<<<c->search_grid, 128, 0, c->st>>>();
+            if (beams)
+                segment_search_kernel<true><<<c->search_grid, 128, 0, c->st>>>();
+            else
+                segment_search_kernel<false><<<c->search_grid_pb2d, 128, 0, c->st>>>();
             launches++;
             UPBP_CK(cudaGetLastError());
             d2h += 2 * sizeof(unsigned);
@@ -911,10 +911,18 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         }
         const unsigned nh = std::min(c->h_hit_count[0], c->hit_capacity);
         if (nh > 0) {
-            bb1d_eval_kernel<<<grid_for(nh), 128, 0, c->st>>>();
+            if (beams)
+                segment_eval_kernel<true><<<grid_for(nh), 128, 0, c->st>>>();
+            else
+                segment_eval_kernel<false><<<grid_for(nh), 128, 0, c->st>>>();
             launches++;
         }
-    }
+        UPBP_CK(cudaGetLastError());
+        return UPBP_OK;
+    };
+    if (run_pb2d && segment_estimator(false) != UPBP_OK) return UPBP_ERR_CUDA;
+    UPBP_CK(cudaEventRecord(ev[6], c->st));
+    if (run_bb1d && segment_estimator(true) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[7], c->st));
     if (run_surf) {
         UPBP_CK(set_work(kKernSurf));
