@@ -61,6 +61,7 @@ struct BoxSource {
     const BeamRec* beams;     // kind 2
     unsigned bb1d_paths;      // kind 2: beams of paths below this index serve BB1D
     const uint2* chunks;      // kind 3: (beam index, chunk k | chunk count << 16)
+    float dilate;             // kinds 1, 3: leaf boxes grown by this much (the maps' query radius)
 };
 
 UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
@@ -77,6 +78,7 @@ UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
     } else if (s.kind == 1) {
         const float3 p = xyz(s.vertices[s.slots[i]].q[0]);
         lo = hi = p;
+        dilate_box(lo, hi, s.dilate);
     } else if (s.kind == 2) {
         const float4 a = s.beams[i].q[0], b = s.beams[i].q[1];
         const float3 o = xyz(a), e = xyz(a) + xyz(b) * a.w;
@@ -86,6 +88,7 @@ UPBP_D void source_box(const BoxSource& s, unsigned i, float3& lo, float3& hi)
         const uint2 ch = s.chunks[i];
         const float4 a = s.beams[ch.x].q[0], b = s.beams[ch.x].q[1];
         chunk_box(xyz(a), xyz(b), a.w, ch.y & 0xffffu, ch.y >> 16, lo, hi);
+        dilate_box(lo, hi, s.dilate);
     }
 }
 

@@ -58,23 +58,28 @@ UPBP_D unsigned warp_reserve1(unsigned* counter)
 
 UPBP_D float3 safe_inv(float3 d) { return make_float3(1.f / d.x, 1.f / d.y, 1.f / d.z); }
 
-// Segment [tmin, tmax] vs box [lo - pad, hi + pad].  Axes with a zero
-// direction component produce NaN/inf slabs, which fminf/fmaxf drop or
-// reject, so the test never misses a box the segment touches.
-UPBP_D bool slab(float3 lo, float3 hi, float pad, float3 o, float3 inv, float tmin, float tmax)
+// Inverse direction and origin * inverse direction of a ray, the inputs of
+// slab().
+UPBP_D float3 oinv_of(float3 o, float3 inv) { return make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z); }
+
+// Segment [tmin, tmax] of the ray o + t d vs box [lo, hi], with inv = 1/d and
+// oinv = o * inv per ray: one multiply-add per plane.  An axis with a zero
+// direction component yields NaN or infinite bounds, which fminf/fmaxf drop
+// or which never reject, so the test never misses a box the segment touches.
+// The photon maps' boxes already include the query radius (BoxSource.dilate).
+UPBP_D bool slab(float3 lo, float3 hi, float3 inv, float3 oinv, float tmin, float tmax)
 {
-    const float tx0 = (lo.x - pad - o.x) * inv.x, tx1 = (hi.x + pad - o.x) * inv.x;
-    const float ty0 = (lo.y - pad - o.y) * inv.y, ty1 = (hi.y + pad - o.y) * inv.y;
-    const float tz0 = (lo.z - pad - o.z) * inv.z, tz1 = (hi.z + pad - o.z) * inv.z;
+    const float tx0 = fmaf(lo.x, inv.x, -oinv.x), tx1 = fmaf(hi.x, inv.x, -oinv.x);
+    const float ty0 = fmaf(lo.y, inv.y, -oinv.y), ty1 = fmaf(hi.y, inv.y, -oinv.y);
+    const float tz0 = fmaf(lo.z, inv.z, -oinv.z), tz1 = fmaf(hi.z, inv.z, -oinv.z);
     const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
     const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
     return tn <= tf;
 }
 
-UPBP_D bool inside(float3 lo, float3 hi, float pad, float3 x)
+UPBP_D bool inside(float3 lo, float3 hi, float3 x)
 {
-    return x.x >= lo.x - pad && x.x <= hi.x + pad && x.y >= lo.y - pad && x.y <= hi.y + pad && x.z >= lo.z - pad &&
-           x.z <= hi.z + pad;
+    return x.x >= lo.x && x.x <= hi.x && x.y >= lo.y && x.y <= hi.y && x.z >= lo.z && x.z <= hi.z;
 }
 
 struct NodeBoxes {
@@ -101,7 +106,7 @@ UPBP_D NodeBoxes load_node(const BvhNode* nodes, int i)
 // leaf(sorted_index) which returns false to stop.  Returns false if the
 // traversal stack overflowed.
 template <class BoxTest, class Leaf>
-UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& leaf)
+UPBP_D bool bvh_walk(const BvhView& bvh, BoxTest&& test_box, Leaf&& leaf)
 {
     if (bvh.count == 0) return true;
     int stack[kStackDepth];
@@ -121,8 +126,8 @@ UPBP_D bool bvh_walk(const BvhView& bvh, float pad, BoxTest&& test_box, Leaf&& l
         } else {
             visits++;
             const NodeBoxes nb = load_node(bvh.nodes, node);
-            const bool hl = test_box(nb.llo, nb.lhi, pad);
-            const bool hr = test_box(nb.rlo, nb.rhi, pad);
+            const bool hl = test_box(nb.llo, nb.lhi);
+            const bool hr = test_box(nb.rlo, nb.rhi);
             if (hl && hr) {
                 if (sp < kStackDepth) {
                     stack[sp++] = nb.r;
@@ -173,8 +178,7 @@ UPBP_D void walk_pop(WalkState& s) { s.node = s.sp > 0 ? s.stack[--s.sp] : kWalk
 // the primitive this step reached (one per step through a leaf), or -1 after
 // an internal node.
 template <class BoxTest>
-UPBP_D int walk_step(WalkState& s, const BvhView& bvh, float pad, BoxTest&& test_box, bool& overflow,
-                     unsigned& visits)
+UPBP_D int walk_step(WalkState& s, const BvhView& bvh, BoxTest&& test_box, bool& overflow, unsigned& visits)
 {
     const int node = s.node;
     if (node < 0) {
@@ -187,8 +191,8 @@ UPBP_D int walk_step(WalkState& s, const BvhView& bvh, float pad, BoxTest&& test
     }
     visits++;
     const NodeBoxes nb = load_node(bvh.nodes, node);
-    const bool hl = test_box(nb.llo, nb.lhi, pad);
-    const bool hr = test_box(nb.rlo, nb.rhi, pad);
+    const bool hl = test_box(nb.llo, nb.lhi);
+    const bool hr = test_box(nb.rlo, nb.rhi);
     if (hl && hr) {
         if (s.sp < kStackDepth)
             s.stack[s.sp++] = nb.r;
@@ -303,8 +307,8 @@ UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tm
     unsigned tests = 0;
     count_work(kCtrRays, 1u);
     const bool ok = bvh_walk(
-        tv.bvh, 0.f,
-        [&](float3 lo, float3 hi, float) {
+        tv.bvh,
+        [&](float3 lo, float3 hi) {
             const float3 t0 = (lo - o) * inv, t1 = (hi - o) * inv;
             const float n = fmaxf(fmaxf(fminf(t0.x, t1.x), fminf(t0.y, t1.y)), fmaxf(fminf(t0.z, t1.z), tmin));
             const float fa = fminf(fminf(fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y)), fminf(fmaxf(t0.z, t1.z), tmax));

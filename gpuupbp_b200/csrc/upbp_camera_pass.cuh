@@ -215,11 +215,11 @@ UPBP_D float3 eval_point_merge(const LightVertex& lv, unsigned cam_len, const Ve
     return mis * f * lv.thr;
 }
 
-UPBP_D float3 query_points(const PointMap& map, float3 x, float r, float r2, unsigned cam_len, const VertexWeights& wc,
+UPBP_D float3 query_points(const PointMap& map, float3 x, float r2, unsigned cam_len, const VertexWeights& wc,
                            const Bsdf& cb, bool medium)
 {
     float3 acc = v3(0.f);
-    points_in_radius(map, x, r, r2, [&](unsigned slot) {
+    points_in_radius(map, x, r2, [&](unsigned slot) {
         LightVertex lv;
         load_vertex(c_params.vertices + slot, lv);
         acc += eval_point_merge(lv, cam_len, wc, cb, medium);
@@ -428,7 +428,7 @@ UPBP_D float3 query_bp2d(float3 x, unsigned cam_len, const VertexWeights& wc, co
 {
     const DeviceParams& p = c_params;
     float3 acc = v3(0.f);
-    beams_near_point(p.beam_map, x, p.rad_beam, p.radius_bp2d_2, [&](unsigned b, float dist, float rad2) {
+    beams_near_point(p.beam_map, x, p.radius_bp2d_2, [&](unsigned b, float dist, float rad2) {
         Beam lb;
         load_beam(p.beams + b, lb);
         acc += eval_bp2d(lb, cam_len, wc, cb, dist, rad2);
@@ -601,7 +601,7 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
             BeamSegHit h;
             const int med = (int)fbits(__ldg(&r[2]).w);
             hit = beam_chunk_vs_segment(p.beam_map, (int)(pr.y & 0x7fffffffu), xyz(q0), xyz(q1), q0.w, q1.w,
-                                        p.radius_bb1d_2, beam_map_pad(p.rad_beam), (pr.y >> 31) != 0, p.do_bp2d != 0,
+                                        p.radius_bb1d_2, (pr.y >> 31) != 0, p.do_bp2d != 0,
                                         med, cand, h);
             id = h.beam;
             geom = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
@@ -652,10 +652,10 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
     const unsigned below = (1u << lane) - 1u;
     const unsigned n = min(p.queue_count[0], p.seg_capacity);
     const BvhView bvh = kBeams ? p.beam_map.bvh : p.med_map.bvh;
-    const float pad = kBeams ? beam_map_pad(p.rad_beam) : p.radius_pb2d * 1.0001f + p.cull_eps;
+
     int node = kWalkDone, sp = 0;
     int deep[kStackDepth - kSmemStack];
-    float3 o = v3(0.f), inv = v3(0.f);
+    float3 inv = v3(0.f), oinv = v3(0.f);
     float tmin = 0.f, tmax = 0.f;
     unsigned qk = 0;
     bool exhausted = false, overflow = false;
@@ -676,10 +676,10 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
                     qk = p.seg_order ? __ldg(&p.seg_order[j]) : j;
                     const float4* r = p.seg_queue[qk].q;
                     const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
-                    o = xyz(q0);
                     tmin = q0.w;
                     tmax = q1.w;
                     inv = safe_inv(xyz(q1));
+                    oinv = oinv_of(xyz(q0), inv);
                     sp = 0;
                     node = bvh.count > 1 ? 0 : kWalkDone;
                     if (bvh.count == 1) {  // a one-leaf map
@@ -695,8 +695,8 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
             // one internal node: leaf children become pairs, internal ones are visited
             visits++;
             const NodeBoxes nb = load_node(bvh.nodes, node);
-            const bool hl = slab(nb.llo, nb.lhi, pad, o, inv, tmin, tmax);
-            const bool hr = slab(nb.rlo, nb.rhi, pad, o, inv, tmin, tmax);
+            const bool hl = slab(nb.llo, nb.lhi, inv, oinv, tmin, tmax);
+            const bool hr = slab(nb.rlo, nb.rhi, inv, oinv, tmin, tmax);
             int next = -1, other = -1;
             if (hl) {
                 if (nb.l < 0) {
@@ -814,10 +814,10 @@ __global__ void __launch_bounds__(128) point_query_kernel()
         float3 c;
         if (kKind == kQuerySurf)
             c = cv.thr * p.surf_normalization *
-                query_points(p.surf_map, cv.hit, p.radius_surf, p.radius_surf_2, cv.path_length, cv.w, cv.bsdf, false);
+                query_points(p.surf_map, cv.hit, p.radius_surf_2, cv.path_length, cv.w, cv.bsdf, false);
         else if (kKind == kQueryPp3d)
             c = cv.thr * p.pp3d_normalization *
-                query_points(p.med_map, cv.hit, p.radius_pp3d, p.radius_pp3d_2, cv.path_length, cv.w, cv.bsdf, true);
+                query_points(p.med_map, cv.hit, p.radius_pp3d_2, cv.path_length, cv.w, cv.bsdf, true);
         else
             c = cv.thr * p.bp2d_normalization * query_bp2d(cv.hit, cv.path_length, cv.w, cv.bsdf);
         splat_camera(fbits(q8.x), c);

@@ -85,21 +85,21 @@ __global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* co
     };
     switch (kind) {
     case 0:
-        points_in_radius(p.surf_map, x, p.radius_surf, p.radius_surf_2, [&](unsigned s) { rec(s); });
+        points_in_radius(p.surf_map, x, p.radius_surf_2, [&](unsigned s) { rec(s); });
         break;
     case 1:
-        points_in_radius(p.med_map, x, p.radius_pp3d, p.radius_pp3d_2, [&](unsigned s) { rec(s); });
+        points_in_radius(p.med_map, x, p.radius_pp3d_2, [&](unsigned s) { rec(s); });
         break;
     case 2:
-        points_near_segment(p.med_map, x, d, r[6], r[7], p.radius_pb2d, p.radius_pb2d_2,
+        points_near_segment(p.med_map, x, d, r[6], r[7], p.radius_pb2d_2,
                             [&](unsigned s, float, float) { rec(s); });
         break;
     case 3:
-        beams_near_segment(p.beam_map, x, d, r[6], r[7], p.rad_beam, p.radius_bb1d_2, p.do_bp2d != 0, -1,
+        beams_near_segment(p.beam_map, x, d, r[6], r[7], p.radius_bb1d_2, p.do_bp2d != 0, -1,
                            [&](unsigned b, float, float, float, float) { rec(b); });
         break;
     default:
-        beams_near_point(p.beam_map, x, p.rad_beam, p.radius_bp2d_2, [&](unsigned b, float, float) { rec(b); });
+        beams_near_point(p.beam_map, x, p.radius_bp2d_2, [&](unsigned b, float, float) { rec(b); });
         break;
     }
     counts[i] = k;
@@ -727,12 +727,16 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     const unsigned nb = std::min(found[3], c->beam_capacity);
     P.surf_map = PointMap{BvhView{c->d_surf_nodes, 0}, c->d_surf_pos};
     P.med_map = PointMap{BvhView{c->d_med_nodes, 0}, c->d_med_pos};
-    P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg};
+    // beam-map boxes: the beam radius (BB1D and BP2D), the box tests' rounding
+    // and the BB1D predicate's t1 error on nearly parallel lines
+    const float beam_dilate = P.rad_beam * 1.0001f + P.beam_cull_eps;
+    P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg, beam_dilate};
     if (P.build_surf && ns > 0) {
         BoxSource src{};
         src.kind = 1;
         src.slots = c->d_idx_s;
         src.vertices = c->d_vertices;
+        src.dilate = P.radius_surf * 1.0001f + P.cull_eps;
         const unsigned* order = nullptr;
         UPBP_CK(build_lbvh(src, ns, c->d_surf_nodes, c->sc, c->st, &order));
         k_gather_points<<<(ns + 255) / 256, 256, 0, c->st>>>(c->d_idx_s, c->d_vertices, order, ns, c->d_surf_pos);
@@ -744,6 +748,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         src.kind = 1;
         src.slots = c->d_idx_m;
         src.vertices = c->d_vertices;
+        src.dilate = P.rad_point_med * 1.0001f + P.cull_eps;  // PP3D and PB2D
         const unsigned* order = nullptr;
         UPBP_CK(build_lbvh(src, nm, c->d_med_nodes, c->sc, c->st, &order));
         k_gather_points<<<(nm + 255) / 256, 256, 0, c->st>>>(c->d_idx_m, c->d_vertices, order, nm, c->d_med_pos);
@@ -763,12 +768,13 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(cudaStreamSynchronize(c->st));
         const unsigned nchunks = tail[0] + tail[1];
         if (ensure_chunks(c, nchunks) != UPBP_OK) return UPBP_ERR_CUDA;
-        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg};
+        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg, beam_dilate};
         k_chunk_expand<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_chunk_counts, c->d_chunk_offsets, nb, c->d_chunks);
         BoxSource src{};
         src.kind = 3;
         src.beams = c->d_beams;
         src.chunks = c->d_chunks;
+        src.dilate = beam_dilate;
         const unsigned* order = nullptr;
         UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order, kBeamLeafMax));
         k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,

@@ -182,6 +182,7 @@ struct PointMap {
 struct BeamMap {
     BvhView bvh;
     const float4* seg;
+    float dilate;  // the leaf boxes' dilation (BoxSource.dilate of the build)
 };
 
 // Parameter range [t0, t1) of chunk k of n along a beam of length len.  Both
@@ -200,6 +201,15 @@ UPBP_HD void chunk_box(float3 o, float3 d, float len, unsigned k, unsigned n, fl
     const float3 ext = (hi - lo) * 1e-6f + v3(1e-6f * (fabsf(lo.x) + fabsf(lo.y) + fabsf(lo.z) + 1e-3f));
     lo = lo - ext;
     hi = hi + ext;
+}
+
+// A photon map's leaf box: the primitive's box dilated by the largest query
+// radius (plus rounding margins) of the map, so the walks test boxes as
+// they are.  The same expression builds the box and re-tests it.
+UPBP_HD void dilate_box(float3& lo, float3& hi, float d)
+{
+    lo = lo - v3(d);
+    hi = hi + v3(d);
 }
 
 // Chunk of n holding parameter t of a beam of length len (t in [0, len)).
@@ -224,10 +234,13 @@ struct DeviceParams {
     DCamera camera;
     float3 scene_center;
     float scene_radius, inv_radius_sqr;
-    // Margins of the range queries' box culling beyond the radius: cull_eps
+    // Margins of the photon maps' box dilation beyond the radius: cull_eps
     // covers the rounding of box tests at the scene's coordinate magnitude;
-    // beam_cull_eps (BB1D) also covers the predicate's error in t1 for
-    // nearly parallel lines.
+    // beam_cull_eps (beam map) also covers the BB1D predicate's error in t1:
+    // for 1 - dd^2 >= 1e-5 (the predicate rejects flatter pairs) t1 is off by
+    // at most ~2.4e-7 |coordinates| / (1 - dd^2), so the query point at the
+    // computed t1 can lie up to ~8e-5 |coordinates| farther from the beam than
+    // the line distance.
     float cull_eps, beam_cull_eps;
     TriView real;
     TriView imag;

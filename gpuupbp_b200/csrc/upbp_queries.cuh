@@ -1,5 +1,6 @@
 // Range queries over the per-iteration photon maps.  Each walker visits the
-// BVH leaves whose box, dilated by the query radius, the query touches, and
+// BVH leaves whose box (built dilated by the map's largest query radius) the
+// query touches, and
 // calls f for every photon or beam that passes the estimator's exact
 // predicate; the neighbour set is therefore defined by the predicate alone
 // (the reference's OptiX intersection programs apply the same predicates,
@@ -13,12 +14,11 @@ namespace upbp {
 
 // Photons within radius r of x (SURF, PP3D): f(vertex slot).
 template <class F>
-UPBP_D void points_in_radius(const PointMap& map, float3 x, float r, float r2, F&& f)
+UPBP_D void points_in_radius(const PointMap& map, float3 x, float r2, F&& f)
 {
-    const float pad = r * 1.0001f + c_params.cull_eps;
     unsigned cand = 0, hits = 0;
     const bool ok = bvh_walk(
-        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
+        map.bvh, [&](float3 lo, float3 hi) { return inside(lo, hi, x); },
         [&](int i) {
             const float4 pp = __ldg(&map.pos[i]);
             cand++;
@@ -36,14 +36,12 @@ UPBP_D void points_in_radius(const PointMap& map, float3 x, float r, float r2, F
 // Photons whose disc of radius r the query segment (o, d, (tmin, tmax))
 // crosses (PB2D): f(vertex slot, distance along the query, squared radius).
 template <class F>
-UPBP_D void points_near_segment(const PointMap& map, float3 o, float3 d, float tmin, float tmax, float r, float r2,
-                                F&& f)
+UPBP_D void points_near_segment(const PointMap& map, float3 o, float3 d, float tmin, float tmax, float r2, F&& f)
 {
-    const float3 inv = safe_inv(d);
-    const float pad = r * 1.0001f + c_params.cull_eps;
+    const float3 inv = safe_inv(d), oinv = oinv_of(o, inv);
     unsigned cand = 0, hits = 0;
     const bool ok = bvh_walk(
-        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
+        map.bvh, [&](float3 lo, float3 hi) { return slab(lo, hi, inv, oinv, tmin, tmax); },
         [&](int i) {
             const float4 pp = __ldg(&map.pos[i]);
             float dist, rad2;
@@ -72,13 +70,15 @@ struct BeamSegHit {
 };
 
 // Segment [tmin, tmax] of (o, d) vs chunk k of n of a beam, with the box
-// test of the beam-map walk (same box, same dilation).
-UPBP_D bool chunk_reached(float3 bo, float3 bd, float len, unsigned k, unsigned n, float pad, float3 o, float3 d,
+// test of the beam-map walk (same box, same dilation, same arithmetic).
+UPBP_D bool chunk_reached(float3 bo, float3 bd, float len, unsigned k, unsigned n, float dilate, float3 o, float3 d,
                           float tmin, float tmax)
 {
     float3 lo, hi;
     chunk_box(bo, bd, len, k, n, lo, hi);
-    return slab(lo, hi, pad, o, safe_inv(d), tmin, tmax);
+    dilate_box(lo, hi, dilate);
+    const float3 inv = safe_inv(d);
+    return slab(lo, hi, inv, oinv_of(o, inv), tmin, tmax);
 }
 
 // The BB1D test of one beam-map leaf against a query segment: the path mask,
@@ -94,10 +94,10 @@ UPBP_D bool chunk_reached(float3 bo, float3 bd, float len, unsigned k, unsigned 
 // is always visited, so exactly one chunk reports each accepted beam, and
 // the set equals a test of every beam (a chunk reached only as part of a
 // leaf of several chunks never reports).  cand counts the leaves that reach
-// the predicate; pad is the walk's box dilation; own_box tells that the walk
-// reached this chunk through a leaf of its own (so its box passed).
+// the predicate; own_box tells that the walk reached this chunk through a
+// leaf of its own (so its box passed).
 UPBP_D bool beam_chunk_vs_segment(const BeamMap& map, int i, float3 o, float3 d, float tmin, float tmax, float r2,
-                                  float pad, bool own_box, bool need_mask, int med, unsigned& cand, BeamSegHit& h)
+                                  bool own_box, bool need_mask, int med, unsigned& cand, BeamSegHit& h)
 {
     const float4 s1 = __ldg(&map.seg[3 * i + 1]);
     const unsigned bits = fbits(s1.w);
@@ -114,44 +114,33 @@ UPBP_D bool beam_chunk_vs_segment(const BeamMap& map, int i, float3 o, float3 d,
     // other (less a rounding margin), so the query passes through the dilated
     // own box of the chunk holding t2 at t1, and the walk reached that chunk.
     const float3 gap = (o + d * h.t1) - (bo + bd * h.t2);
-    const float inner = pad - 2.f * c_params.cull_eps;
+    const float inner = map.dilate - 2.f * c_params.cull_eps;
     if (inner > 0.f && dot(gap, gap) <= inner * inner) return mine;
     const unsigned kc = fbits(s2.w), k = kc & 0xffffu, n = kc >> 16;
     // a leaf of several chunks is visited when any of its chunks is in
     // reach, so this chunk's own box decides, as for every other chunk
-    if (!own_box && !chunk_reached(bo, bd, s0.w, k, n, pad, o, d, tmin, tmax)) return false;
+    if (!own_box && !chunk_reached(bo, bd, s0.w, k, n, map.dilate, o, d, tmin, tmax)) return false;
     if (mine) return true;
-    if (chunk_reached(bo, bd, s0.w, chunk_of(h.t2, s0.w, n), n, pad, o, d, tmin, tmax)) return false;
+    if (chunk_reached(bo, bd, s0.w, chunk_of(h.t2, s0.w, n), n, map.dilate, o, d, tmin, tmax)) return false;
     for (unsigned j = 0; j < k; j++)
-        if (chunk_reached(bo, bd, s0.w, j, n, pad, o, d, tmin, tmax)) return false;
+        if (chunk_reached(bo, bd, s0.w, j, n, map.dilate, o, d, tmin, tmax)) return false;
     return true;
 }
 
-// Box dilation of BB1D beam-map walks: the beam radius with a margin for the
-// box tests' rounding and for the predicate's error in t1 on nearly parallel
-// lines: for 1 - dd^2 >= 1e-5 (the predicate rejects flatter pairs) t1 is off
-// by at most ~2.4e-7 |coordinates| / (1 - dd^2), so the query point at the
-// computed t1 can lie up to ~8e-5 |coordinates| farther from the beam than
-// the line distance.  With beam_cull_eps the walk reaches every beam the
-// predicate accepts.
-UPBP_D float beam_map_pad(float pad_r) { return pad_r * 1.0001f + c_params.beam_cull_eps; }
-
 template <class F>
-UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmin, float tmax, float pad_r, float r2,
+UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmin, float tmax, float r2,
                                bool need_mask, int med, F&& f)
 {
-    const float3 inv = safe_inv(d);
-    const float pad = beam_map_pad(pad_r);
+    const float3 inv = safe_inv(d), oinv = oinv_of(o, inv);
     unsigned cand = 0, hits = 0, visits = 0;
     bool overflow = false;
     WalkState s;
     walk_begin(s, map.bvh);
     while (s.node != kWalkDone) {
         const int leaf = walk_step(
-            s, map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return slab(lo, hi, pd, o, inv, tmin, tmax); },
-            overflow, visits);
+            s, map.bvh, [&](float3 lo, float3 hi) { return slab(lo, hi, inv, oinv, tmin, tmax); }, overflow, visits);
         BeamSegHit h;
-        if (leaf >= 0 && beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, pad, false, need_mask, med, cand, h)) {
+        if (leaf >= 0 && beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, false, need_mask, med, cand, h)) {
             hits++;
             f(h.beam, h.dist, h.sin_theta, h.t1, h.t2);
         }
@@ -165,12 +154,11 @@ UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmi
 // Photon beams whose disc of radius sqrt(r2) contains x (BP2D):
 // f(beam index, distance along the beam, squared radius).
 template <class F>
-UPBP_D void beams_near_point(const BeamMap& map, float3 x, float pad_r, float r2, F&& f)
+UPBP_D void beams_near_point(const BeamMap& map, float3 x, float r2, F&& f)
 {
-    const float pad = pad_r * 1.0001f + c_params.cull_eps;
     unsigned cand = 0, hits = 0;
     const bool ok = bvh_walk(
-        map.bvh, pad, [&](float3 lo, float3 hi, float pd) { return inside(lo, hi, pd, x); },
+        map.bvh, [&](float3 lo, float3 hi) { return inside(lo, hi, x); },
         [&](int i) {
             const float4 s0 = __ldg(&map.seg[3 * i]), s1 = __ldg(&map.seg[3 * i + 1]);
             const float4 s2 = __ldg(&map.seg[3 * i + 2]);
