@@ -191,14 +191,25 @@ struct BeamMap {
 UPBP_HD float chunk_t(float len, unsigned k, unsigned n) { return k >= n ? len : len * (float)k / (float)n; }
 
 // Box of chunk k of n of the beam (o, d, len): the beam-map builder's leaf
-// box, widened to cover the rounding of o + d t at both ends.
-UPBP_HD void chunk_box(float3 o, float3 d, float len, unsigned k, unsigned n, float3& lo, float3& hi)
+// box, widened to cover the rounding of o + d t at both ends.  Written with
+// round-to-nearest intrinsics (no fused multiply-add), so the build and the
+// BB1D reporting rule compute the same box bit for bit.
+UPBP_D float3 rn_axpy(float3 o, float3 d, float t)
+{
+    return make_float3(__fadd_rn(o.x, __fmul_rn(d.x, t)), __fadd_rn(o.y, __fmul_rn(d.y, t)),
+                       __fadd_rn(o.z, __fmul_rn(d.z, t)));
+}
+
+UPBP_D void chunk_box(float3 o, float3 d, float len, unsigned k, unsigned n, float3& lo, float3& hi)
 {
     const float t0 = chunk_t(len, k, n), t1 = chunk_t(len, k + 1, n);
-    const float3 a = o + d * t0, e = o + d * t1;
+    const float3 a = rn_axpy(o, d, t0), e = rn_axpy(o, d, t1);
     lo = make_float3(fminf(a.x, e.x), fminf(a.y, e.y), fminf(a.z, e.z));
     hi = make_float3(fmaxf(a.x, e.x), fmaxf(a.y, e.y), fmaxf(a.z, e.z));
-    const float3 ext = (hi - lo) * 1e-6f + v3(1e-6f * (fabsf(lo.x) + fabsf(lo.y) + fabsf(lo.z) + 1e-3f));
+    const float m = __fmul_rn(1e-6f, __fadd_rn(__fadd_rn(__fadd_rn(fabsf(lo.x), fabsf(lo.y)), fabsf(lo.z)), 1e-3f));
+    const float3 ext = make_float3(__fadd_rn(__fmul_rn(__fsub_rn(hi.x, lo.x), 1e-6f), m),
+                                   __fadd_rn(__fmul_rn(__fsub_rn(hi.y, lo.y), 1e-6f), m),
+                                   __fadd_rn(__fmul_rn(__fsub_rn(hi.z, lo.z), 1e-6f), m));
     lo = lo - ext;
     hi = hi + ext;
 }
