@@ -645,6 +645,7 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
 template <bool kBeams>
 __global__ void __launch_bounds__(128) segment_search_kernel()
 {
+    begin_kernel(kBeams ? kKernBb1d : kKernPb2d);
     const DeviceParams& p = c_params;
     __shared__ SearchWarp s_warp[kSearchWarps];
     SearchWarp& w = s_warp[threadIdx.x >> 5];
@@ -803,6 +804,7 @@ enum : unsigned { kQuerySurf = 1u, kQueryPp3d = 2u, kQueryBp2d = 4u };
 template <unsigned kKind>
 __global__ void __launch_bounds__(128) point_query_kernel()
 {
+    begin_kernel(kKind == kQuerySurf ? kKernSurf : (kKind == kQueryPp3d ? kKernPp3d : kKernBp2d));
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[1], p.pt_capacity);
     for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
@@ -1058,6 +1060,7 @@ UPBP_D void camera_path_end(const CameraLane& c)
 // alone, so the assignment of pixels to lanes does not change any path.
 __global__ void __launch_bounds__(128, 4) camera_pass_kernel()
 {
+    begin_kernel(kKernCameraExtend);
     const DeviceParams& p = c_params;
     VolSeg segs[kMaxVolSegments];
     LiteSeg lsegs[kMaxVolSegments];
@@ -1095,6 +1098,7 @@ __global__ void __launch_bounds__(128, 4) camera_pass_kernel()
 // k_resolve_camera knows whether an earlier step of the path failed.
 __global__ void __launch_bounds__(128, 4) nee_connect_kernel()
 {
+    begin_kernel(kKernNee);
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[4], p.nee_capacity);
     VolSeg segs[kMaxVolSegments];
@@ -1146,6 +1150,7 @@ __global__ void __launch_bounds__(128, 4) nee_connect_kernel()
 // with its occlusion ray; the contribution is kept per pair like NEE's.
 __global__ void __launch_bounds__(128, 4) bpt_connect_kernel()
 {
+    begin_kernel(kKernBpt);
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[5], p.bpt_capacity);
     VolSeg segs[kMaxVolSegments];

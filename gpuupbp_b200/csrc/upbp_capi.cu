@@ -24,12 +24,17 @@ constexpr int kEventRing = 64;
 // chunk reached through a shared leaf must test its own box before it may
 // report a beam; on the media workload single-chunk leaves are fastest.
 constexpr int kBeamLeafMax = 1;
-// events per iteration: start, light done, maps done, then one after each
-// camera-side kernel kind (extend, nee, bpt, pb2d, bb1d, surf, pp3d, bp2d)
-constexpr int kEvPerIter = 3 + (kKernCount - 1);
-// camera-side kernel kinds in launch order (one event after each)
-constexpr int kCamOrder[kKernCount - 1] = {kKernCameraExtend, kKernNee, kKernBpt, kKernPb2d,
-                                           kKernBb1d,         kKernSurf, kKernPp3d, kKernBp2d};
+// Events per iteration: 0 start, 1 light pass done, 2 photon maps done, 3
+// extend, 4 NEE, 5 BPT + resolve, 6 query sort, 7 SURF, 8 PP3D, 9 BP2D,
+// 10 PB2D, 11 BB1D, 12 iteration done.  Each kernel kind's time is one
+// interval.
+constexpr int kEvPerIter = 13;
+struct EvInterval {
+    int kind, from, to;
+};
+constexpr EvInterval kKindInterval[kKernCount] = {
+    {kKernLight, 0, 1}, {kKernCameraExtend, 2, 3}, {kKernNee, 3, 4},   {kKernBpt, 4, 5},  {kKernSurf, 6, 7},
+    {kKernPp3d, 7, 8},  {kKernBp2d, 8, 9},         {kKernPb2d, 9, 10}, {kKernBb1d, 10, 11}};
 
 namespace {
 
@@ -73,6 +78,7 @@ cudaError_t dupload(T** p, const T* h, size_t n, cudaStream_t st)
 // Query record: x y z dx dy dz tmin tmax (points use x y z only).
 __global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* counts, unsigned* ids, unsigned cap)
 {
+    begin_kernel(kKernLight);
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const DeviceParams& p = c_params;
@@ -656,12 +662,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     unsigned launches = 0;
     size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
     P.work = c->d_work;
-    auto set_work = [&](int kern) -> cudaError_t {
-        unsigned long long* w = c->d_work + (size_t)kern * kCtrCount;
+    {
+        unsigned long long* w = c->d_work;
         h2d += sizeof(w);
-        return cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st);
-    };
-    UPBP_CK(set_work(kKernLight));
+        UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
+    }
     unsigned found[4] = {0, 0, 0, 0};
     if (P.trace_light_paths) {
         // radius schedule and MIS factors (renderer.cpp:57-119)
@@ -799,8 +804,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 6 * sizeof(unsigned), c->st));
             h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-            UPBP_CK(set_work(kKernCameraExtend));
-            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
+                UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
                                     kCtrCount * sizeof(unsigned long long), c->st));
             camera_pass_kernel<<<std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128), 128, 0,
                                  c->st>>>();
@@ -850,13 +854,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     if (P.trace_camera_paths)
         UPBP_CK(cudaMemsetAsync(c->d_path_err, 0xff, P.screen_pixel_count * sizeof(unsigned), c->st));
     if (nnee > 0) {
-        UPBP_CK(set_work(kKernNee));
         nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>();
         launches++;
     }
     UPBP_CK(cudaEventRecord(ev[4], c->st));
     if (nbpt > 0) {
-        UPBP_CK(set_work(kKernBpt));
         bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>();
         launches++;
     }
@@ -891,7 +893,6 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     // repeated (it is a pure function of the queries and the map)
     auto segment_estimator = [&](bool beams) -> int {
         const int kern = beams ? kKernBb1d : kKernPb2d;
-        UPBP_CK(set_work(kern));
         if (c->hit_capacity == 0 && ensure_hits(c, (size_t)nseg * 32) != UPBP_OK) return UPBP_ERR_CUDA;
         for (int attempt = 0; attempt < 2; attempt++) {
             UPBP_CK(cudaMemsetAsync(c->d_hit_count, 0, 2 * sizeof(unsigned), c->st));
@@ -926,32 +927,33 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(cudaGetLastError());
         return UPBP_OK;
     };
-    if (run_pb2d && segment_estimator(false) != UPBP_OK) return UPBP_ERR_CUDA;
+    // (Running the point merges on a second stream beside PB2D/BB1D gained
+    // nothing: all of these walks wait on the same L1/L2 latency.)
     UPBP_CK(cudaEventRecord(ev[6], c->st));
-    if (run_bb1d && segment_estimator(true) != UPBP_OK) return UPBP_ERR_CUDA;
-    UPBP_CK(cudaEventRecord(ev[7], c->st));
     if (run_surf) {
-        UPBP_CK(set_work(kKernSurf));
         point_query_kernel<kQuerySurf><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
-    UPBP_CK(cudaEventRecord(ev[8], c->st));
+    UPBP_CK(cudaEventRecord(ev[7], c->st));
     if (run_pp3d) {
-        UPBP_CK(set_work(kKernPp3d));
         point_query_kernel<kQueryPp3d><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
-    UPBP_CK(cudaEventRecord(ev[9], c->st));
+    UPBP_CK(cudaEventRecord(ev[8], c->st));
     if (run_bp2d) {
-        UPBP_CK(set_work(kKernBp2d));
         point_query_kernel<kQueryBp2d><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
     UPBP_CK(cudaGetLastError());
+    UPBP_CK(cudaEventRecord(ev[9], c->st));
+    if (run_pb2d && segment_estimator(false) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[10], c->st));
+    if (run_bb1d && segment_estimator(true) != UPBP_OK) return UPBP_ERR_CUDA;
+    UPBP_CK(cudaEventRecord(ev[11], c->st));
     k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
                                                                          (unsigned)npx);
     launches++;
+    UPBP_CK(cudaEventRecord(ev[12], c->st));
     c->launches = launches;
     c->h2d_iter = h2d;
     c->d2h_iter = d2h;
@@ -1026,20 +1028,23 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
     // since the previous stats call (up to the event ring size)
     for (unsigned k = 0; k < c->ev_pending; k++) {
         cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
-        float t[kEvPerIter - 1];
-        for (int e = 0; e + 1 < kEvPerIter; e++) UPBP_CK(cudaEventElapsedTime(&t[e], ev[e], ev[e + 1]));
-        float cam = 0.f;
-        for (int e = 2; e + 1 < kEvPerIter; e++) cam += t[e];
+        float light, build, cam;
+        UPBP_CK(cudaEventElapsedTime(&light, ev[0], ev[1]));
+        UPBP_CK(cudaEventElapsedTime(&build, ev[1], ev[2]));
+        UPBP_CK(cudaEventElapsedTime(&cam, ev[2], ev[12]));
         if (k == 0) {
-            o->ms_light = t[0];
-            o->ms_build = t[1];
+            o->ms_light = light;
+            o->ms_build = build;
             o->ms_camera = cam;
         }
-        o->ms_light_sum += t[0];
-        o->ms_build_sum += t[1];
+        o->ms_light_sum += light;
+        o->ms_build_sum += build;
         o->ms_camera_sum += cam;
-        o->ms_kernel_sum[kKernLight] += t[0];
-        for (int i = 0; i < kKernCount - 1; i++) o->ms_kernel_sum[kCamOrder[i]] += t[2 + i];
+        for (const EvInterval& iv : kKindInterval) {
+            float t;
+            UPBP_CK(cudaEventElapsedTime(&t, ev[iv.from], ev[iv.to]));
+            o->ms_kernel_sum[iv.kind] += t;
+        }
         o->timed_iterations++;
     }
     c->ev_pending = 0;

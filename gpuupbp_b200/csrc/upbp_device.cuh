@@ -339,10 +339,21 @@ UPBP_HD unsigned event_key(unsigned bounce, unsigned step) { return bounce * 256
 
 // Launch parameters of the running pass, uploaded before each launch.
 __constant__ DeviceParams c_params;
-// Work-counter set of the running kernel (one set per kernel kind).
+// Work counters of every kernel kind (kKernCount sets of kCtrCount), set
+// once per iteration.  Each counting kernel records its kind in shared
+// memory at entry, so kernels of different kinds may run concurrently.
 __constant__ unsigned long long* c_work;
+__shared__ int s_kernel_kind;
 
-UPBP_D unsigned long long* c_work_ptr() { return c_work; }
+// Records the running kernel's kind; every thread of the block calls it
+// first, before any early return.
+UPBP_D void begin_kernel(int kind)
+{
+    if (threadIdx.x == 0) s_kernel_kind = kind;
+    __syncthreads();
+}
+
+UPBP_D unsigned long long* c_work_ptr() { return c_work + (size_t)s_kernel_kind * kCtrCount; }
 
 // Kernel kinds of an iteration, for work counters and timing.
 enum : int {

@@ -290,6 +290,7 @@ UPBP_D void light_path_end(const LightLane& l)
 // vertex slots depend on its index alone.
 __global__ void __launch_bounds__(128, 4) light_pass_kernel()
 {
+    begin_kernel(kKernLight);
     const DeviceParams& p = c_params;
     VolSeg segs[kMaxVolSegments];
     LiteSeg lsegs[kMaxVolSegments];
