@@ -117,9 +117,9 @@ def algorithmic_bytes(work: dict, extra: float = 0.0) -> float:
 
 # Bytes of the query records each camera-side kernel writes or reads.
 SEG_RECORD, POINT_RECORD = 128, 144
-# PB2D / BB1D hit-list entry (query, neighbour, 4 floats), written by the
+# PB2D / BB1D hit-list entry (query record, neighbour), written by the
 # search kernel and read by the evaluation kernel.
-HIT_RECORD = 24
+HIT_RECORD = 8
 # Deferred connections: an NEE sample reads its 80 B record and 64 B of its
 # camera vertex and writes a 16 B contribution; a BPT pair reads its 8 B
 # pair and 144 B of its camera vertex and writes 16 B (the light vertex is

@@ -574,14 +574,13 @@ constexpr int kSmemStack = 16;
 struct SearchWarp {
     uint2 cand[kCandRing];  // (segment-query record, beam-map leaf | own-leaf bit << 31)
     uint2 hit_qb[64];
-    float4 hit_geom[64];
     int stack[kSmemStack][32];
 };
 
 // Leaf tests of the 32 (or, at the end, fewer) oldest waiting pairs, one per
 // lane; accepted pairs go to the hit buffer, which is flushed by 32.  A hit
-// is (query, beam) + (distance, sin theta, t1, t2) for BB1D and (query,
-// light-vertex slot) + (distance along the query, squared radius) for PB2D.
+// is (query record, beam) for BB1D and (query record, light-vertex slot) for
+// PB2D; the evaluation recomputes the pair's geometry.
 template <bool kBeams>
 UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
                               unsigned& cand, unsigned& hits)
@@ -592,7 +591,6 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     bool hit = false;
     uint2 pr = make_uint2(0u, 0u);
     unsigned id = 0;
-    float4 geom = make_float4(0.f, 0.f, 0.f, 0.f);
     if (lane < count) {
         pr = w.cand[(head + lane) % kCandRing];
         const float4* r = p.seg_queue[pr.x].q;
@@ -604,14 +602,12 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
                                         p.radius_bb1d_2, (pr.y >> 31) != 0, p.do_bp2d != 0,
                                         med, cand, h);
             id = h.beam;
-            geom = make_float4(h.dist, h.sin_theta, h.t1, h.t2);
         } else {
             const float4 pp = __ldg(&p.med_map.pos[pr.y & 0x7fffffffu]);
             float dist, rad2;
             cand++;
             hit = pred_ray_disc(xyz(q0), xyz(q1), q0.w, q1.w, xyz(pp), p.radius_pb2d_2, dist, rad2);
             id = fbits(pp.w);
-            geom = make_float4(dist, rad2, 0.f, 0.f);
         }
     }
     head += count;
@@ -619,7 +615,6 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     if (hit) {
         const unsigned pos = hfill + __popc(hm & below);
         w.hit_qb[pos] = make_uint2(pr.x, id);
-        w.hit_geom[pos] = geom;
         hits++;
     }
     hfill += __popc(hm);
@@ -630,12 +625,10 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
         base = __shfl_sync(~0u, base, 0);
         if (base + lane < p.hit_capacity) {
             p.hit_qb[base + lane] = w.hit_qb[lane];
-            p.hit_geom[base + lane] = w.hit_geom[lane];
         }
         __syncwarp();
         if (lane + 32 < hfill) {
             w.hit_qb[lane] = w.hit_qb[lane + 32];
-            w.hit_geom[lane] = w.hit_geom[lane + 32];
         }
         hfill -= 32;
     }
@@ -758,7 +751,6 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
         base = __shfl_sync(~0u, base, 0);
         if (lane < hfill && base + lane < p.hit_capacity) {
             p.hit_qb[base + lane] = w.hit_qb[lane];
-            p.hit_geom[base + lane] = w.hit_geom[lane];
         }
     }
     count_work(kCtrNodes, visits);
@@ -777,7 +769,6 @@ __global__ void __launch_bounds__(128) segment_eval_kernel()
     const unsigned n = min(p.hit_count[0], p.hit_capacity);
     for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const uint2 qb = __ldg(&p.hit_qb[j]);
-        const float4 g = __ldg(&p.hit_geom[j]);
         QuerySeg q;
         StateWeights cw;
         float3 weight;
@@ -785,14 +776,22 @@ __global__ void __launch_bounds__(128) segment_eval_kernel()
         load_seg_query(qb.x, q, cw, weight, pk, path, key);
         if (!event_kept(path, key)) continue;
         float3 est;
+        // the pair's geometry: the search's predicate again, on the same
+        // floats, so the values are the ones it accepted (a hit stores 8 bytes)
         if (kBeams) {
             Beam lb;
             load_beam(p.beams + qb.y, lb);
-            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, g.x, g.y, g.z, g.w);
+            float dist, sin_theta, t1, t2;
+            if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta, t1,
+                                t2))
+                continue;
+            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
         } else {
             LightVertex lv;
             load_vertex(p.vertices + qb.y, lv);
-            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, g.x, g.y);
+            float dist, rad2;
+            if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) continue;
+            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
         }
         splat_camera(pk >> 8, weight * est);
     }

@@ -167,7 +167,6 @@ struct upbp_ctx {
     float4* d_path_color = nullptr;
     // BB1D hit list (search -> evaluation)
     uint2* d_hit_qb = nullptr;
-    float4* d_hit_geom = nullptr;
     unsigned hit_capacity = 0;
     unsigned* d_hit_count = nullptr;
     unsigned h_hit_count[2] = {0, 0};
@@ -380,19 +379,16 @@ int ensure_chunks(upbp_ctx* c, unsigned n)
     return UPBP_OK;
 }
 
-// Room for n BB1D hits (24 bytes each).
+// Room for n PB2D / BB1D hits (8 bytes each).
 int ensure_hits(upbp_ctx* c, size_t n)
 {
     if (n <= c->hit_capacity) return UPBP_OK;
     const size_t cap = std::min<size_t>(std::max<size_t>(n + n / 4, 1u << 20), 0x7fffffffu);
     UPBP_CK(cudaStreamSynchronize(c->st));
     cudaFree(c->d_hit_qb);
-    cudaFree(c->d_hit_geom);
     c->d_hit_qb = nullptr;
-    c->d_hit_geom = nullptr;
     c->hit_capacity = 0;
     UPBP_CK(dalloc(&c->d_hit_qb, cap));
-    UPBP_CK(dalloc(&c->d_hit_geom, cap));
     c->hit_capacity = (unsigned)cap;
     return UPBP_OK;
 }
@@ -899,7 +895,6 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kern * kCtrCount, 0, kCtrCount * sizeof(unsigned long long),
                                     c->st));
             P.hit_qb = c->d_hit_qb;
-            P.hit_geom = c->d_hit_geom;
             P.hit_capacity = c->hit_capacity;
             h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
@@ -1183,7 +1178,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
                     c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
                     c->d_qcount, c->d_conn, c->d_nee, c->d_bpt, c->d_nee_color, c->d_bpt_color,
-                    c->d_path_err, c->d_path_color, c->d_hit_count, c->d_hit_qb, c->d_hit_geom, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
+                    c->d_path_err, c->d_path_color, c->d_hit_count, c->d_hit_qb, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
                     c->d_sort[0][2], c->d_sort[0][3], c->d_sort[1][0], c->d_sort[1][1], c->d_sort[1][2],
                     c->d_sort[1][3], c->d_sort_temp};
     for (void* b : bufs)

@@ -310,7 +310,6 @@ struct DeviceParams {
     // BB1D hit list: the search kernel appends every (segment query, beam)
     // pair the predicate accepts; the evaluation kernel consumes the list.
     uint2* hit_qb;                    // (segment-query record index, beam index)
-    float4* hit_geom;                 // (distance, sin theta, t along the query, t along the beam)
     unsigned hit_capacity;
     unsigned* hit_count;              // [0] hits found (may exceed capacity), [1] next query to hand out
 
