@@ -215,18 +215,6 @@ UPBP_D float3 eval_point_merge(const LightVertex& lv, unsigned cam_len, const Ve
     return mis * f * lv.thr;
 }
 
-UPBP_D float3 query_points(const PointMap& map, float3 x, float r2, unsigned cam_len, const VertexWeights& wc,
-                           const Bsdf& cb, bool medium)
-{
-    float3 acc = v3(0.f);
-    points_in_radius(map, x, r2, [&](unsigned slot) {
-        LightVertex lv;
-        load_vertex(c_params.vertices + slot, lv);
-        acc += eval_point_merge(lv, cam_len, wc, cb, medium);
-    });
-    return acc;
-}
-
 struct QuerySeg {
     float3 o, d;
     float dmin, dmax;
@@ -424,18 +412,6 @@ UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& w
     return mis * unweighted;
 }
 
-UPBP_D float3 query_bp2d(float3 x, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb)
-{
-    const DeviceParams& p = c_params;
-    float3 acc = v3(0.f);
-    beams_near_point(p.beam_map, x, p.radius_bp2d_2, [&](unsigned b, float dist, float rad2) {
-        Beam lb;
-        load_beam(p.beams + b, lb);
-        acc += eval_bp2d(lb, cam_len, wc, cb, dist, rad2);
-    });
-    return acc;
-}
-
 // Emits one segment-query record per scattering medium segment of a camera
 // ray, with the attenuation and sampling pdfs accumulated over the segments
 // before it (the segment loop of eval_pb2d_segments / eval_bb1d_segments,
@@ -546,42 +522,60 @@ UPBP_D void splat_camera(unsigned px, float3 c)
     }
 }
 
-// BB1D and PB2D in two kernels each.  A long query segment crosses hundreds
-// of beam chunks (or photons) and a short one a few, and every accepted
-// neighbour costs a full MIS evaluation; run inside one walk per thread, both
-// leave most lanes of a warp idle.
+// PB2D, BB1D and BP2D as range queries, each in two kernels.
+// A long query segment crosses hundreds of beam chunks (or photons) and a
+// short one a few, and every accepted neighbour costs a full MIS evaluation;
+// run inside one walk per thread, both leave most lanes of a warp idle.
 //
-// segment_search_kernel<kBeams>: persistent warps walk the beam map (BB1D)
-// or the medium photon map (PB2D) with one query per
-// lane, one internal node per step; a lane whose query is finished takes the
-// next one in Morton order from a global counter, so lanes stay busy until
-// the queue is empty.  A child that is a leaf is not visited: its (query,
-// chunk) pair goes into a per-warp ring in shared memory, and whenever 32
-// pairs are waiting all lanes run the exact leaf test on one pair each, so
-// the expensive test never runs on a partly idle warp.  Accepted (query,
-// beam) pairs are gathered the same way and written out 32 at a time (one
-// atomic per 32 hits).  When the list is full the pairs past the capacity are
-// dropped but still counted, and the host grows the list and repeats the
-// search.
+// range_search_kernel<kMode>: persistent warps walk a photon map with one
+// query per lane, one internal node per step; a lane whose query is finished
+// takes the next one in Morton order from a global counter, so lanes stay
+// busy until the queue is empty.  A child that is a leaf is not visited: its
+// (query, primitive) pair goes into a per-warp ring in shared memory, and
+// whenever 32 pairs are waiting all lanes run the exact leaf test on one pair
+// each, so the test never runs on a partly idle warp.  Accepted pairs are
+// gathered the same way and written out 32 at a time (one atomic per 32
+// hits).  When the list is full the pairs past the capacity are dropped but
+// still counted, and the host grows the list and repeats the search.
+//
+// range_eval_kernel<kMode>: one accepted pair per thread; recomputes the
+// pair's geometry with the same predicate, evaluates the estimator with its
+// MIS weight and adds it into the camera image.
+enum : int { kModePb2d = 0, kModeBb1d, kModeBp2d, kRangeModes };
+template <int kMode> struct RangeMode {
+    static_assert(kMode >= 0 && kMode < kRangeModes, "range-query mode");
+    static constexpr bool seg = kMode != kModeBp2d;  // segment queries (else point queries)
+    static constexpr bool beams = kMode != kModePb2d;  // beam map (else medium photon map)
+    static constexpr int kern = kMode == kModePb2d ? kKernPb2d : kMode == kModeBb1d ? kKernBb1d : kKernBp2d;
+};
+
+enum : unsigned { kQuerySurf = 1u, kQueryPp3d = 2u, kQueryBp2d = 4u };
+
+template <int kMode>
+UPBP_D const BvhView& range_map_bvh()
+{
+    const DeviceParams& p = c_params;
+    return RangeMode<kMode>::beams ? p.beam_map.bvh : p.med_map.bvh;
+}
+
 constexpr int kSearchWarps = 4;
 constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
 
 // The top kSmemStack entries of each lane's traversal stack live in shared
 // memory (column per lane, so lanes never share a bank); deeper entries go
-// to local memory.  Local memory competes with the beam map for L1.
+// to local memory.  Local memory competes with the photon maps for L1.
 constexpr int kSmemStack = 16;
 
 struct SearchWarp {
-    uint2 cand[kCandRing];  // (segment-query record, beam-map leaf | own-leaf bit << 31)
+    uint2 cand[kCandRing];  // (query record, map leaf | own-leaf bit << 31)
     uint2 hit_qb[64];
     int stack[kSmemStack][32];
 };
 
 // Leaf tests of the 32 (or, at the end, fewer) oldest waiting pairs, one per
 // lane; accepted pairs go to the hit buffer, which is flushed by 32.  A hit
-// is (query record, beam) for BB1D and (query record, light-vertex slot) for
-// PB2D; the evaluation recomputes the pair's geometry.
-template <bool kBeams>
+// is (query record, beam) or (query record, light-vertex slot).
+template <int kMode>
 UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
                               unsigned& cand, unsigned& hits)
 {
@@ -593,21 +587,34 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     unsigned id = 0;
     if (lane < count) {
         pr = w.cand[(head + lane) % kCandRing];
-        const float4* r = p.seg_queue[pr.x].q;
-        const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
-        if (kBeams) {
-            BeamSegHit h;
-            const int med = (int)fbits(__ldg(&r[2]).w);
-            hit = beam_chunk_vs_segment(p.beam_map, (int)(pr.y & 0x7fffffffu), xyz(q0), xyz(q1), q0.w, q1.w,
-                                        p.radius_bb1d_2, (pr.y >> 31) != 0, p.do_bp2d != 0,
-                                        med, cand, h);
-            id = h.beam;
+        const unsigned leaf = pr.y & 0x7fffffffu;
+        if constexpr (RangeMode<kMode>::seg) {
+            const float4* r = p.seg_queue[pr.x].q;
+            const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
+            if constexpr (kMode == kModeBb1d) {
+                BeamSegHit h;
+                const int med = (int)fbits(__ldg(&r[2]).w);
+                hit = beam_chunk_vs_segment(p.beam_map, (int)leaf, xyz(q0), xyz(q1), q0.w, q1.w, p.radius_bb1d_2,
+                                            (pr.y >> 31) != 0, p.do_bp2d != 0, med, cand, h);
+                id = h.beam;
+            } else {
+                const float4 pp = __ldg(&p.med_map.pos[leaf]);
+                float dist, rad2;
+                cand++;
+                hit = pred_ray_disc(xyz(q0), xyz(q1), q0.w, q1.w, xyz(pp), p.radius_pb2d_2, dist, rad2);
+                id = fbits(pp.w);
+            }
         } else {
-            const float4 pp = __ldg(&p.med_map.pos[pr.y & 0x7fffffffu]);
+            // BP2D: beams_near_point's leaf test, the chunk holding the
+            // beam's closest point reports it
+            const float3 x = xyz(__ldg(&p.pt_queue[pr.x].v.q[0]));
+            const float4 s0 = __ldg(&p.beam_map.seg[3 * leaf]), s1 = __ldg(&p.beam_map.seg[3 * leaf + 1]);
+            const float4 s2 = __ldg(&p.beam_map.seg[3 * leaf + 2]);
             float dist, rad2;
             cand++;
-            hit = pred_ray_disc(xyz(q0), xyz(q1), q0.w, q1.w, xyz(pp), p.radius_pb2d_2, dist, rad2);
-            id = fbits(pp.w);
+            hit = pred_ray_disc(xyz(s0), xyz(s1), 0.f, s0.w, x, p.radius_bp2d_2, dist, rad2) && dist >= s2.x &&
+                  dist < s2.y;
+            id = fbits(s1.w) & 0x7fffffffu;
         }
     }
     head += count;
@@ -623,40 +630,36 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(&p.hit_count[0], 32u);
         base = __shfl_sync(~0u, base, 0);
-        if (base + lane < p.hit_capacity) {
-            p.hit_qb[base + lane] = w.hit_qb[lane];
-        }
+        if (base + lane < p.hit_capacity) p.hit_qb[base + lane] = w.hit_qb[lane];
         __syncwarp();
-        if (lane + 32 < hfill) {
-            w.hit_qb[lane] = w.hit_qb[lane + 32];
-        }
+        if (lane + 32 < hfill) w.hit_qb[lane] = w.hit_qb[lane + 32];
         hfill -= 32;
     }
     __syncwarp();
 }
 
-template <bool kBeams>
-__global__ void __launch_bounds__(128) segment_search_kernel()
+template <int kMode>
+__global__ void __launch_bounds__(128) range_search_kernel()
 {
-    begin_kernel(kBeams ? kKernBb1d : kKernPb2d);
+    using M = RangeMode<kMode>;
+    begin_kernel(M::kern);
     const DeviceParams& p = c_params;
     __shared__ SearchWarp s_warp[kSearchWarps];
     SearchWarp& w = s_warp[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    const unsigned n = min(p.queue_count[0], p.seg_capacity);
-    const BvhView bvh = kBeams ? p.beam_map.bvh : p.med_map.bvh;
-
+    const unsigned n = M::seg ? min(p.queue_count[0], p.seg_capacity) : min(p.queue_count[1], p.pt_capacity);
+    const BvhView bvh = range_map_bvh<kMode>();
     int node = kWalkDone, sp = 0;
     int deep[kStackDepth - kSmemStack];
-    float3 inv = v3(0.f), oinv = v3(0.f);
+    float3 inv = v3(0.f), oinv = v3(0.f), x = v3(0.f);
     float tmin = 0.f, tmax = 0.f;
     unsigned qk = 0;
     bool exhausted = false, overflow = false;
     unsigned head = 0, tail = 0, hfill = 0;  // same values in every lane
     unsigned visits = 0, cand = 0, hits = 0;
     for (;;) {
-        int f0 = 0, n0 = 0, f1 = 0, n1 = 0;  // leaves (first primitive, count) reached this step
+        int lf[2] = {0, 0}, ln[2] = {0, 0};  // leaves (first primitive, count) reached this step
         const bool idle = node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
@@ -666,22 +669,33 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
             base = __shfl_sync(~0u, base, leader);
             if (idle && !exhausted) {
                 const unsigned j = base + __popc(want & below);
-                if (j < n) {
-                    qk = p.seg_order ? __ldg(&p.seg_order[j]) : j;
-                    const float4* r = p.seg_queue[qk].q;
-                    const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
-                    tmin = q0.w;
-                    tmax = q1.w;
-                    inv = safe_inv(xyz(q1));
-                    oinv = oinv_of(xyz(q0), inv);
+                bool take = j < n;
+                exhausted = !take;
+                if (take) {
+                    if constexpr (M::seg) {
+                        qk = p.seg_order ? __ldg(&p.seg_order[j]) : j;
+                        const float4* r = p.seg_queue[qk].q;
+                        const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
+                        tmin = q0.w;
+                        tmax = q1.w;
+                        inv = safe_inv(xyz(q1));
+                        oinv = oinv_of(xyz(q0), inv);
+                    } else {
+                        // point queries of other estimators, or of camera paths
+                        // that failed earlier, are skipped
+                        qk = p.pt_order ? __ldg(&p.pt_order[j]) : j;
+                        const float4 q8 = __ldg(&p.pt_queue[qk].q8);
+                        take = (fbits(q8.y) & kQueryBp2d) && event_kept(fbits(q8.z), fbits(q8.w));
+                        x = xyz(__ldg(&p.pt_queue[qk].v.q[0]));
+                    }
+                }
+                if (take) {
                     sp = 0;
                     node = bvh.count > 1 ? 0 : kWalkDone;
                     if (bvh.count == 1) {  // a one-leaf map
-                        f0 = 0;
-                        n0 = 1;
+                        lf[0] = 0;
+                        ln[0] = 1;
                     }
-                } else {
-                    exhausted = true;
                 }
             }
         }
@@ -689,25 +703,32 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
             // one internal node: leaf children become pairs, internal ones are visited
             visits++;
             const NodeBoxes nb = load_node(bvh.nodes, node);
-            const bool hl = slab(nb.llo, nb.lhi, inv, oinv, tmin, tmax);
-            const bool hr = slab(nb.rlo, nb.rhi, inv, oinv, tmin, tmax);
+            bool hl, hr;
+            if constexpr (M::seg) {
+                hl = slab(nb.llo, nb.lhi, inv, oinv, tmin, tmax);
+                hr = slab(nb.rlo, nb.rhi, inv, oinv, tmin, tmax);
+            } else {
+                hl = inside(nb.llo, nb.lhi, x);
+                hr = inside(nb.rlo, nb.rhi, x);
+            }
             int next = -1, other = -1;
             if (hl) {
                 if (nb.l < 0) {
-                    f0 = leaf_first(nb.l);
-                    n0 = leaf_count(nb.l);
+                    lf[0] = leaf_first(nb.l);
+                    ln[0] = leaf_count(nb.l);
                 } else {
                     next = nb.l;
                 }
             }
             if (hr) {
                 if (nb.r < 0) {
-                    f1 = leaf_first(nb.r);
-                    n1 = leaf_count(nb.r);
-                } else if (next < 0)
+                    lf[1] = leaf_first(nb.r);
+                    ln[1] = leaf_count(nb.r);
+                } else if (next < 0) {
                     next = nb.r;
-                else
+                } else {
                     other = nb.r;
+                }
             }
             if (other >= 0) {
                 if (sp < kSmemStack)
@@ -728,100 +749,107 @@ __global__ void __launch_bounds__(128) segment_search_kernel()
         }
         // the primitives of the reached leaves become pairs, one per lane and
         // round; 32 waiting pairs are tested at once
-        const int npend = n0 + n1;
+        const int npend = ln[0] + ln[1];
         for (int i = 0; __any_sync(~0u, i < npend); i++) {
             const bool has = i < npend;
             const unsigned m = __ballot_sync(~0u, has);
             if (has) {
-                // bit 31: the pair's chunk is a leaf of its own, whose box the walk tested
-                const bool single = i < n0 ? n0 == 1 : n1 == 1;
+                const bool second = i >= ln[0];
+                const int first = second ? lf[1] : lf[0], k = second ? i - ln[0] : i;
+                const int cnt = second ? ln[1] : ln[0];
+                // bit 31: the pair's primitive is a leaf of its own, whose box the walk tested
                 w.cand[(tail + __popc(m & below)) % kCandRing] =
-                    make_uint2(qk, (unsigned)(i < n0 ? f0 + i : f1 + i - n0) | (single ? 0x80000000u : 0u));
+                    make_uint2(qk, (unsigned)(first + k) | (cnt == 1 ? 0x80000000u : 0u));
             }
             tail += __popc(m);
-            if (tail - head >= 32) search_test_pairs<kBeams>(w, head, 32, hfill, lane, cand, hits);
+            if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits);
         }
         if (__all_sync(~0u, exhausted && node == kWalkDone)) break;
     }
-    if (tail != head) search_test_pairs<kBeams>(w, head, tail - head, hfill, lane, cand, hits);
+    if (tail != head) search_test_pairs<kMode>(w, head, tail - head, hfill, lane, cand, hits);
     __syncwarp();
     if (hfill) {
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(&p.hit_count[0], hfill);
         base = __shfl_sync(~0u, base, 0);
-        if (lane < hfill && base + lane < p.hit_capacity) {
-            p.hit_qb[base + lane] = w.hit_qb[lane];
-        }
+        if (lane < hfill && base + lane < p.hit_capacity) p.hit_qb[base + lane] = w.hit_qb[lane];
     }
     count_work(kCtrNodes, visits);
-    count_work(kBeams ? kCtrBeamCand : kCtrPointCand, cand);
-    count_work(kBeams ? kCtrBeamHit : kCtrPointHit, hits);
+    count_work(M::beams ? kCtrBeamCand : kCtrPointCand, cand);
+    count_work(M::beams ? kCtrBeamHit : kCtrPointHit, hits);
     if (overflow) flag_status(kErrTraversalStack);
 }
 
-// segment_eval_kernel<kBeams>: one accepted pair per thread, so every lane
-// runs the same MIS evaluation (eval_bb1d or eval_pb2d); adds weight *
-// normalization * estimate into the camera image.
-template <bool kBeams>
-__global__ void __launch_bounds__(128) segment_eval_kernel()
+template <int kMode>
+__global__ void __launch_bounds__(128) range_eval_kernel()
 {
+    using M = RangeMode<kMode>;
     const DeviceParams& p = c_params;
     const unsigned n = min(p.hit_count[0], p.hit_capacity);
     for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const uint2 qb = __ldg(&p.hit_qb[j]);
-        QuerySeg q;
-        StateWeights cw;
-        float3 weight;
-        unsigned pk, path, key;
-        load_seg_query(qb.x, q, cw, weight, pk, path, key);
-        if (!event_kept(path, key)) continue;
-        float3 est;
-        // the pair's geometry: the search's predicate again, on the same
-        // floats, so the values are the ones it accepted (a hit stores 8 bytes)
-        if (kBeams) {
+        if constexpr (M::seg) {
+            QuerySeg q;
+            StateWeights cw;
+            float3 weight;
+            unsigned pk, path, key;
+            load_seg_query(qb.x, q, cw, weight, pk, path, key);
+            if (!event_kept(path, key)) continue;
+            float3 est;
+            if constexpr (kMode == kModeBb1d) {
+                Beam lb;
+                load_beam(p.beams + qb.y, lb);
+                float dist, sin_theta, t1, t2;
+                if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta,
+                                    t1, t2))
+                    continue;
+                est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
+            } else {
+                LightVertex lv;
+                load_vertex(p.vertices + qb.y, lv);
+                float dist, rad2;
+                if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) continue;
+                est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
+            }
+            splat_camera(pk >> 8, weight * est);
+        } else {
+            const float4 q8 = __ldg(&p.pt_queue[qb.x].q8);
+            LightVertex cv;
+            load_vertex(&p.pt_queue[qb.x].v, cv);
             Beam lb;
             load_beam(p.beams + qb.y, lb);
-            float dist, sin_theta, t1, t2;
-            if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta, t1,
-                                t2))
-                continue;
-            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
-        } else {
-            LightVertex lv;
-            load_vertex(p.vertices + qb.y, lv);
             float dist, rad2;
-            if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) continue;
-            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
+            if (!pred_ray_disc(lb.o, lb.d, 0.f, lb.length, cv.hit, p.radius_bp2d_2, dist, rad2)) continue;
+            splat_camera(fbits(q8.x),
+                         cv.thr * p.bp2d_normalization * eval_bp2d(lb, cv.path_length, cv.w, cv.bsdf, dist, rad2));
         }
-        splat_camera(pk >> 8, weight * est);
     }
 }
 
-enum : unsigned { kQuerySurf = 1u, kQueryPp3d = 2u, kQueryBp2d = 4u };
-
-// SURF, PP3D or BP2D (kKind) for one point-query record.
-template <unsigned kKind>
-__global__ void __launch_bounds__(128) point_query_kernel()
+// SURF and PP3D for one point-query record per thread, evaluated inline:
+// their walks are short and their hits few, so the search / evaluation split
+// (kept for PB2D, BB1D and BP2D) costs more than it saves here.
+template <bool medium>
+__global__ void __launch_bounds__(128) point_merge_kernel()
 {
-    begin_kernel(kKind == kQuerySurf ? kKernSurf : (kKind == kQueryPp3d ? kKernPp3d : kKernBp2d));
+    begin_kernel(medium ? kKernPp3d : kKernSurf);
     const DeviceParams& p = c_params;
+    const PointMap& map = medium ? p.med_map : p.surf_map;
+    const float r2 = medium ? p.radius_pp3d_2 : p.radius_surf_2;
     const unsigned n = min(p.queue_count[1], p.pt_capacity);
     for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const unsigned k = p.pt_order ? __ldg(&p.pt_order[j]) : j;
         const float4 q8 = __ldg(&p.pt_queue[k].q8);
-        if (!(fbits(q8.y) & kKind) || !event_kept(fbits(q8.z), fbits(q8.w))) continue;
+        if (!(fbits(q8.y) & (medium ? kQueryPp3d : kQuerySurf)) || !event_kept(fbits(q8.z), fbits(q8.w))) continue;
         LightVertex cv;
         load_vertex(&p.pt_queue[k].v, cv);
-        float3 c;
-        if (kKind == kQuerySurf)
-            c = cv.thr * p.surf_normalization *
-                query_points(p.surf_map, cv.hit, p.radius_surf_2, cv.path_length, cv.w, cv.bsdf, false);
-        else if (kKind == kQueryPp3d)
-            c = cv.thr * p.pp3d_normalization *
-                query_points(p.med_map, cv.hit, p.radius_pp3d_2, cv.path_length, cv.w, cv.bsdf, true);
-        else
-            c = cv.thr * p.bp2d_normalization * query_bp2d(cv.hit, cv.path_length, cv.w, cv.bsdf);
-        splat_camera(fbits(q8.x), c);
+        float3 acc = v3(0.f);
+        points_in_radius(map, cv.hit, r2, [&](unsigned slot) {
+            LightVertex lv;
+            load_vertex(p.vertices + slot, lv);
+            acc += eval_point_merge(lv, cv.path_length, cv.w, cv.bsdf, medium);
+        });
+        splat_camera(fbits(q8.x), cv.thr * (medium ? p.pp3d_normalization : p.surf_normalization) * acc);
     }
 }
 

@@ -170,7 +170,7 @@ struct upbp_ctx {
     unsigned hit_capacity = 0;
     unsigned* d_hit_count = nullptr;
     unsigned h_hit_count[2] = {0, 0};
-    int search_grid = 0, search_grid_pb2d = 0;
+    int search_grid[kRangeModes] = {};  // per range-query mode (kModePb2d ...)
     int camera_grid = 0;   // resident blocks of the persistent camera pass
     int light_grid = 0;    // resident blocks of the persistent light pass
     // Morton sort of the query records: keys/values and their alternates per queue
@@ -571,10 +571,13 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         int dev = 0, sms = 0, per_sm = 0;
         UPBP_CK(cudaGetDevice(&dev));
         UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, segment_search_kernel<true>, 128, 0));
-        c->search_grid = std::max(1, sms * std::max(1, per_sm));
-        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, segment_search_kernel<false>, 128, 0));
-        c->search_grid_pb2d = std::max(1, sms * std::max(1, per_sm));
+        const void* search[kRangeModes] = {(const void*)range_search_kernel<kModePb2d>,
+                                           (const void*)range_search_kernel<kModeBb1d>,
+                                           (const void*)range_search_kernel<kModeBp2d>};
+        for (int m = 0; m < kRangeModes; m++) {
+            UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search[m], 128, 0));
+            c->search_grid[m] = std::max(1, sms * std::max(1, per_sm));
+        }
         UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, camera_pass_kernel, 128, 0));
         c->camera_grid = std::max(1, sms * std::max(1, per_sm));
         UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light_pass_kernel, 128, 0));
@@ -884,24 +887,26 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         h2d += sizeof(P);
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
     }
-    // PB2D and BB1D: search (query, neighbour) pairs into the hit list, then
+    // The estimators: search (query, neighbour) pairs into the hit list, then
     // evaluate them; a list that was too small is grown and the search
     // repeated (it is a pure function of the queries and the map)
-    auto segment_estimator = [&](bool beams) -> int {
-        const int kern = beams ? kKernBb1d : kKernPb2d;
-        if (c->hit_capacity == 0 && ensure_hits(c, (size_t)nseg * 32) != UPBP_OK) return UPBP_ERR_CUDA;
+    auto estimator = [&](int mode) -> int {
+        static constexpr int kKern[kRangeModes] = {kKernPb2d, kKernBb1d, kKernBp2d};
+        if (c->hit_capacity == 0 && ensure_hits(c, (size_t)std::max(nseg, npt) * 32) != UPBP_OK) return UPBP_ERR_CUDA;
         for (int attempt = 0; attempt < 2; attempt++) {
             UPBP_CK(cudaMemsetAsync(c->d_hit_count, 0, 2 * sizeof(unsigned), c->st));
-            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kern * kCtrCount, 0, kCtrCount * sizeof(unsigned long long),
-                                    c->st));
+            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKern[mode] * kCtrCount, 0,
+                                    kCtrCount * sizeof(unsigned long long), c->st));
             P.hit_qb = c->d_hit_qb;
             P.hit_capacity = c->hit_capacity;
             h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-            if (beams)
-                segment_search_kernel<true><<<c->search_grid, 128, 0, c->st>>>();
-            else
-                segment_search_kernel<false><<<c->search_grid_pb2d, 128, 0, c->st>>>();
+            const int g = c->search_grid[mode];
+            switch (mode) {
+            case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(); break;
+            case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(); break;
+            default: range_search_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(); break;
+            }
             launches++;
             UPBP_CK(cudaGetLastError());
             d2h += 2 * sizeof(unsigned);
@@ -913,37 +918,33 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         }
         const unsigned nh = std::min(c->h_hit_count[0], c->hit_capacity);
         if (nh > 0) {
-            if (beams)
-                segment_eval_kernel<true><<<grid_for(nh), 128, 0, c->st>>>();
-            else
-                segment_eval_kernel<false><<<grid_for(nh), 128, 0, c->st>>>();
+            const unsigned g = grid_for(nh);
+            switch (mode) {
+            case kModePb2d: range_eval_kernel<kModePb2d><<<g, 128, 0, c->st>>>(); break;
+            case kModeBb1d: range_eval_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(); break;
+            default: range_eval_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(); break;
+            }
             launches++;
         }
         UPBP_CK(cudaGetLastError());
         return UPBP_OK;
     };
-    // (Running the point merges on a second stream beside PB2D/BB1D gained
-    // nothing: all of these walks wait on the same L1/L2 latency.)
     UPBP_CK(cudaEventRecord(ev[6], c->st));
     if (run_surf) {
-        point_query_kernel<kQuerySurf><<<grid_for(npt), 128, 0, c->st>>>();
+        point_merge_kernel<false><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
     UPBP_CK(cudaEventRecord(ev[7], c->st));
     if (run_pp3d) {
-        point_query_kernel<kQueryPp3d><<<grid_for(npt), 128, 0, c->st>>>();
+        point_merge_kernel<true><<<grid_for(npt), 128, 0, c->st>>>();
         launches++;
     }
     UPBP_CK(cudaEventRecord(ev[8], c->st));
-    if (run_bp2d) {
-        point_query_kernel<kQueryBp2d><<<grid_for(npt), 128, 0, c->st>>>();
-        launches++;
-    }
-    UPBP_CK(cudaGetLastError());
+    if (run_bp2d && estimator(kModeBp2d) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[9], c->st));
-    if (run_pb2d && segment_estimator(false) != UPBP_OK) return UPBP_ERR_CUDA;
+    if (run_pb2d && estimator(kModePb2d) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[10], c->st));
-    if (run_bb1d && segment_estimator(true) != UPBP_OK) return UPBP_ERR_CUDA;
+    if (run_bb1d && estimator(kModeBb1d) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[11], c->st));
     k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
                                                                          (unsigned)npx);
