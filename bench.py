@@ -242,7 +242,8 @@ def run_b200(args) -> dict | None:
     top = max(kernels, key=lambda k: kernels[k]["ms"])
     b_top, top_ms = kernels[top]["bytes"], kernels[top]["ms"]
     achieved = kernels[top]["gbs"]
-    traffic = profiled_traffic() if top == "bb1d_query" else None
+    # the committed capture is scaled to the default resolution only
+    traffic = profiled_traffic() if top == "bb1d_query" and tuple(args.res) == tuple(RES) else None
     total_paths = paths_per_iter * args.steps * world
     value = total_paths / (ms * 1e-3)
     e2e = total_paths / (ms_e2e * 1e-3)
