@@ -10,6 +10,12 @@ photon-map builds, camera pass).
 Metric: paths/s = (camera + light subpaths per iteration) x iterations / time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload media_field|dense_beams]
+
+`--workload dense_beams` times the dense-beam stress case instead (1920x1080,
+one thick medium in a 500k-triangle enclosure, path length 16, beams from
+the first 600 000 light paths: about 2M beams and 4-5M photon points per
+iteration); the headline line is the default workload.
 
 N > 1 runs under torchrun, one rank per GPU; rank r renders iterations
 r, r+N, ... (iterations are independent given the seed), so the scaling is
@@ -33,12 +39,20 @@ sys.path.insert(0, HERE)
 SCENE_DIR = os.environ.get("UPBP_SCENE_DIR", "/tmp/upbp_scenes")
 RES = (1280, 720)
 TECH = "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d"
-PATH_LENGTH = 12
 METRIC = "paths/s (camera + light subpaths per second), plain UPBP render iterations"
 
+# name: (resolution, path length, further flags, scene description)
+WORKLOADS = {
+    "media_field": (RES, 12, [], "20 displaced icosphere media (1.64M tris)"),
+    "dense_beams": ((1920, 1080), 16, ["-r_initial_bb1d", "-0.004", "-r_initial_bp2d", "-0.004", "-pbc", "600000"],
+                    "one thick medium (sigma_s 5, g 0.9) in a displaced-box enclosure (0.5M tris), "
+                    "beam radius 0.004 x scene radius, beams from the first 600000 light paths"),
+}
 
-def workload_args(scene_path: str, res=RES) -> list[str]:
-    return ["-s", "-1", scene_path, "-a", TECH, "-l", str(PATH_LENGTH), "-r", f"{res[0]}x{res[1]}"]
+
+def workload_args(scene_path: str, res=RES, workload: str = "media_field") -> list[str]:
+    _, length, extra, _ = WORKLOADS[workload]
+    return ["-s", "-1", scene_path, "-a", TECH, "-l", str(length), "-r", f"{res[0]}x{res[1]}"] + extra
 
 
 def measured_peaks() -> dict:
@@ -138,7 +152,8 @@ def kernel_rooflines(st: dict, pixels: int) -> dict:
     extra = {"light_pass": 0.0,
              "camera_extend": 12.0 * pixels + SEG_RECORD * nseg + POINT_RECORD * npt,
              "pb2d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * pb2d_hits, "bb1d_query": SEG_RECORD * nseg + HIT_RECORD * 2 * hits,
-             "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt, "bp2d_query": POINT_RECORD * npt,
+             "surf_query": POINT_RECORD * npt, "pp3d_query": POINT_RECORD * npt,
+             "bp2d_query": POINT_RECORD * npt + HIT_RECORD * 2 * st["work"]["bp2d_query"]["beam_hit"],
              "nee_connect": NEE_BYTES * nnee, "bpt_connect": PAIR_BYTES * npairs}
     out = {}
     for k, w in st["work"].items():
@@ -182,11 +197,11 @@ def run_b200(args) -> dict | None:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
         pg = dist
-    scene = scenes.write_workload("media_field", SCENE_DIR) if rank == 0 else None
+    scene = scenes.write_workload(args.workload, SCENE_DIR) if rank == 0 else None
     if pg is not None:
         pg.barrier()
-        scene = scenes.write_workload("media_field", SCENE_DIR)
-    r = upbp.Renderer(workload_args(scene, args.res))
+        scene = scenes.write_workload(args.workload, SCENE_DIR)
+    r = upbp.Renderer(workload_args(scene, args.res, args.workload))
     paths_per_iter = r.config.res_x * r.config.res_y + int(r.config.path_count_per_iter)
     stream = torch.cuda.ExternalStream(r.stream_handle())
     # rank r renders iterations r, r+N, ...
@@ -243,7 +258,8 @@ def run_b200(args) -> dict | None:
     b_top, top_ms = kernels[top]["bytes"], kernels[top]["ms"]
     achieved = kernels[top]["gbs"]
     # the committed capture is scaled to the default resolution only
-    traffic = profiled_traffic() if top == "bb1d_query" and tuple(args.res) == tuple(RES) else None
+    traffic = (profiled_traffic() if top == "bb1d_query" and args.workload == "media_field" and tuple(args.res) == RES
+               else None)
     total_paths = paths_per_iter * args.steps * world
     value = total_paths / (ms * 1e-3)
     e2e = total_paths / (ms_e2e * 1e-3)
@@ -251,11 +267,11 @@ def run_b200(args) -> dict | None:
         "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, OBJ/MTL/AUX)",
-        "config": {"workload": f"media_field: {args.res[0]}x{args.res[1]}, 20 displaced icosphere media (1.64M tris), "
-                               "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d, path length 12, 1 light path per pixel",
+        "config": {"workload": f"{args.workload}: {args.res[0]}x{args.res[1]}, {WORKLOADS[args.workload][3]}, "
+                               f"{TECH}, path length {WORKLOADS[args.workload][1]}, 1 light path per pixel",
                    "triangles": int(st["triangle_count"]), "light_paths_per_iter": int(r.config.path_count_per_iter),
                    "camera_paths_per_iter": pixels, "parallelism": f"iterations sharded over {world} rank(s)",
-                   "l2": "inputs larger than L2 (scene BVH + triangle data ~300 MB, photon records per iteration)"},
+                   "l2": "inputs larger than L2 (scene BVH + triangle data, photon records per iteration)"},
         "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": int(st_e2e["h2d_bytes"]),
                 "d2h_bytes_per_step": int(st_e2e["d2h_bytes"]) + pixels * 12,
                 "wall_s": wall_e2e},
@@ -274,18 +290,25 @@ def run_b200(args) -> dict | None:
     return out
 
 
-def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iters: int | None = None) -> dict:
+def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iters: int | None = None,
+                         workload: str = "media_field") -> dict:
     """Times the reference's render loop on host cores on a bounded sample of
-    the workload: the same scene, estimators and path length at 160x90
-    pixels (1/64 of the pixels, one light path per pixel).  Iterations run
-    until `seconds` have been timed or `max_iters` iterations were timed."""
+    the workload: the same scene, estimators and path length at 1/8 of the
+    width and height (1/64 of the pixels, one light path per pixel).
+    Iterations run until `seconds` have been timed or `max_iters` iterations
+    were timed."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     import ref_cpu
     from gpuupbp_b200 import scenes
 
-    scene = scenes.write_workload("media_field", SCENE_DIR)
-    res = (160, 90)
-    r = ref_cpu.RefRenderer(workload_args(scene, res), threads=threads)
+    scene = scenes.write_workload(workload, SCENE_DIR)
+    full = WORKLOADS[workload][0]
+    res = (full[0] // 8, full[1] // 8)
+    args = workload_args(scene, res, workload)
+    if "-pbc" in args:  # the same fraction of beam-storing light paths
+        i = args.index("-pbc") + 1
+        args[i] = str(max(1, int(float(args[i]) / 64)))
+    r = ref_cpu.RefRenderer(args, threads=threads)
     for w in range(warmup):
         r.run_iteration(w)
     it, n, t = warmup, 0, 0.0
@@ -299,7 +322,7 @@ def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iter
     paths = (res[0] * res[1] + st["light_paths"]) * n
     r.close()
     return {"value": paths / t, "unit": "paths/s", "cores": threads, "kind": "reference",
-            "sample": f"media_field scene at {res[0]}x{res[1]} (1/64 of the pixels), {n} timed iteration(s), "
+            "sample": f"{workload} scene at {res[0]}x{res[1]} (1/64 of the pixels), {n} timed iteration(s), "
                       f"{t:.1f} s on {threads} host threads"}
 
 
@@ -311,22 +334,27 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--res", default=f"{RES[0]}x{RES[1]}",
-                    help="image size WxH; smaller sizes are for profiling captures, not bench lines")
+    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS))
+    ap.add_argument("--res", default=None,
+                    help="image size WxH (default: the workload's); smaller sizes are for profiling captures, "
+                         "not bench lines")
     args = ap.parse_args()
-    args.res = tuple(int(v) for v in args.res.lower().split("x"))
+    args.res = (tuple(int(v) for v in args.res.lower().split("x")) if args.res
+                else tuple(WORKLOADS[args.workload][0]))
     threads = os.cpu_count() or 1
     world, rank, _ = dist_env()
     if args.impl == "reference":
         if rank != 0:
             return
         # each step is one bounded iteration of the reference loop
-        s2 = run_reference_sample(seconds=1e9, threads=threads, warmup=args.warmup, max_iters=args.steps)
+        s2 = run_reference_sample(seconds=1e9, threads=threads, warmup=args.warmup, max_iters=args.steps,
+                                  workload=args.workload)
         v = s2["value"]
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "paths/s", "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                          "config": {"workload": "media_field (reference CPU build, 160x90 sample per step)"},
+                          "config": {"workload": f"{args.workload} (reference CPU build, 1/64-pixel sample per "
+                                                 "step)"},
                           "cpu_baseline": s2, "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0,
                                                       "d2h_bytes_per_step": 0}}))
         return
@@ -335,7 +363,7 @@ def main():
         return
     if not args.no_cpu_baseline and world == 1:
         try:
-            out["cpu_baseline"] = run_reference_sample(args.cpu_seconds, threads)
+            out["cpu_baseline"] = run_reference_sample(args.cpu_seconds, threads, workload=args.workload)
         except Exception as e:  # the oracle build is absent
             out["cpu_baseline"] = {"value": None, "unit": "paths/s", "cores": threads, "kind": "reference",
                                    "sample": f"unavailable: {e}"}

@@ -535,8 +535,11 @@ UPBP_D void splat_camera(unsigned px, float3 c)
 // whenever 32 pairs are waiting all lanes run the exact leaf test on one pair
 // each, so the test never runs on a partly idle warp.  Accepted pairs are
 // gathered the same way and written out 32 at a time (one atomic per 32
-// hits).  When the list is full the pairs past the capacity are dropped but
-// still counted, and the host grows the list and repeats the search.
+// hits).  A search covers one round of the query order: once the hit list
+// is 3/4 full no lane takes a new query, the lanes finish the queries they
+// hold, and the host evaluates the list and starts the next round where this
+// one stopped.  Pairs past the capacity are dropped but still counted, and
+// such a round is repeated.
 //
 // range_eval_kernel<kMode>: one accepted pair per thread; recomputes the
 // pair's geometry with the same predicate, evaluates the estimator with its
@@ -559,6 +562,7 @@ UPBP_D const BvhView& range_map_bvh()
 }
 
 constexpr int kSearchWarps = 4;
+constexpr unsigned kNoQuery = 0xffffffffu;  // no more queries in this round
 constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
 
 // The top kSmemStack entries of each lane's traversal stack live in shared
@@ -572,12 +576,57 @@ struct SearchWarp {
     int stack[kSmemStack][32];
 };
 
+// The estimate of one accepted (query, neighbour) pair: the predicate's
+// geometry recomputed, the estimator with its MIS weight, added into the
+// camera image.
+template <int kMode>
+UPBP_D void eval_range_hit(uint2 qb)
+{
+    using M = RangeMode<kMode>;
+    const DeviceParams& p = c_params;
+    if constexpr (M::seg) {
+        QuerySeg q;
+        StateWeights cw;
+        float3 weight;
+        unsigned pk, path, key;
+        load_seg_query(qb.x, q, cw, weight, pk, path, key);
+        if (!event_kept(path, key)) return;
+        float3 est;
+        if constexpr (kMode == kModeBb1d) {
+            Beam lb;
+            load_beam(p.beams + qb.y, lb);
+            float dist, sin_theta, t1, t2;
+            if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta,
+                                t1, t2))
+                return;
+            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
+        } else {
+            LightVertex lv;
+            load_vertex(p.vertices + qb.y, lv);
+            float dist, rad2;
+            if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) return;
+            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
+        }
+        splat_camera(pk >> 8, weight * est);
+    } else {
+        const float4 q8 = __ldg(&p.pt_queue[qb.x].q8);
+        LightVertex cv;
+        load_vertex(&p.pt_queue[qb.x].v, cv);
+        Beam lb;
+        load_beam(p.beams + qb.y, lb);
+        float dist, rad2;
+        if (!pred_ray_disc(lb.o, lb.d, 0.f, lb.length, cv.hit, p.radius_bp2d_2, dist, rad2)) return;
+        splat_camera(fbits(q8.x),
+                     cv.thr * p.bp2d_normalization * eval_bp2d(lb, cv.path_length, cv.w, cv.bsdf, dist, rad2));
+    }
+}
+
 // Leaf tests of the 32 (or, at the end, fewer) oldest waiting pairs, one per
 // lane; accepted pairs go to the hit buffer, which is flushed by 32.  A hit
 // is (query record, beam) or (query record, light-vertex slot).
 template <int kMode>
 UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
-                              unsigned& cand, unsigned& hits)
+                              unsigned& cand, unsigned& hits, unsigned long long& seen)
 {
     const DeviceParams& p = c_params;
     const unsigned below = (1u << lane) - 1u;
@@ -627,9 +676,10 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     hfill += __popc(hm);
     if (hfill >= 32) {
         __syncwarp();
-        unsigned base = 0;
-        if (lane == 0) base = atomicAdd(&p.hit_count[0], 32u);
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&p.hit_state->total, 32ull);
         base = __shfl_sync(~0u, base, 0);
+        seen = base + 32;
         if (base + lane < p.hit_capacity) p.hit_qb[base + lane] = w.hit_qb[lane];
         __syncwarp();
         if (lane + 32 < hfill) w.hit_qb[lane] = w.hit_qb[lane + 32];
@@ -648,7 +698,10 @@ __global__ void __launch_bounds__(128) range_search_kernel()
     SearchWarp& w = s_warp[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    const unsigned n = M::seg ? min(p.queue_count[0], p.seg_capacity) : min(p.queue_count[1], p.pt_capacity);
+    // this round's range of the processing order, within the queue
+    const unsigned nq = M::seg ? min(p.queue_count[0], p.seg_capacity) : min(p.queue_count[1], p.pt_capacity);
+    const unsigned n = min(p.query_end, nq) - min(p.query_begin, min(p.query_end, nq));
+    unsigned long long seen = 0;  // hit total after this warp's last flush
     const BvhView bvh = range_map_bvh<kMode>();
     int node = kWalkDone, sp = 0;
     int deep[kStackDepth - kSmemStack];
@@ -663,13 +716,18 @@ __global__ void __launch_bounds__(128) range_search_kernel()
         const bool idle = node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
+            // no new queries once the hit list is 3/4 full, as far as this
+            // warp saw at its last flush of hits (no extra load of the
+            // counter, which every flush and request updates)
             const int leader = __ffs(want) - 1;
-            unsigned base = 0;
-            if ((int)lane == leader) base = atomicAdd(&p.hit_count[1], (unsigned)__popc(want));
+            unsigned base = kNoQuery;
+            if ((int)lane == leader && seen < p.hit_soft_limit)
+                base = atomicAdd(&p.hit_state->fetched, (unsigned)__popc(want));
             base = __shfl_sync(~0u, base, leader);
             if (idle && !exhausted) {
-                const unsigned j = base + __popc(want & below);
-                bool take = j < n;
+                const unsigned r = base + __popc(want & below);
+                bool take = base != kNoQuery && r < n;
+                const unsigned j = p.query_begin + r;
                 exhausted = !take;
                 if (take) {
                     if constexpr (M::seg) {
@@ -762,15 +820,15 @@ __global__ void __launch_bounds__(128) range_search_kernel()
                     make_uint2(qk, (unsigned)(first + k) | (cnt == 1 ? 0x80000000u : 0u));
             }
             tail += __popc(m);
-            if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits);
+            if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);
         }
         if (__all_sync(~0u, exhausted && node == kWalkDone)) break;
     }
-    if (tail != head) search_test_pairs<kMode>(w, head, tail - head, hfill, lane, cand, hits);
+    if (tail != head) search_test_pairs<kMode>(w, head, tail - head, hfill, lane, cand, hits, seen);
     __syncwarp();
     if (hfill) {
-        unsigned base = 0;
-        if (lane == 0) base = atomicAdd(&p.hit_count[0], hfill);
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&p.hit_state->total, (unsigned long long)hfill);
         base = __shfl_sync(~0u, base, 0);
         if (lane < hfill && base + lane < p.hit_capacity) p.hit_qb[base + lane] = w.hit_qb[lane];
     }
@@ -783,47 +841,10 @@ __global__ void __launch_bounds__(128) range_search_kernel()
 template <int kMode>
 __global__ void __launch_bounds__(128) range_eval_kernel()
 {
-    using M = RangeMode<kMode>;
     const DeviceParams& p = c_params;
-    const unsigned n = min(p.hit_count[0], p.hit_capacity);
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const uint2 qb = __ldg(&p.hit_qb[j]);
-        if constexpr (M::seg) {
-            QuerySeg q;
-            StateWeights cw;
-            float3 weight;
-            unsigned pk, path, key;
-            load_seg_query(qb.x, q, cw, weight, pk, path, key);
-            if (!event_kept(path, key)) continue;
-            float3 est;
-            if constexpr (kMode == kModeBb1d) {
-                Beam lb;
-                load_beam(p.beams + qb.y, lb);
-                float dist, sin_theta, t1, t2;
-                if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta,
-                                    t1, t2))
-                    continue;
-                est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
-            } else {
-                LightVertex lv;
-                load_vertex(p.vertices + qb.y, lv);
-                float dist, rad2;
-                if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) continue;
-                est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
-            }
-            splat_camera(pk >> 8, weight * est);
-        } else {
-            const float4 q8 = __ldg(&p.pt_queue[qb.x].q8);
-            LightVertex cv;
-            load_vertex(&p.pt_queue[qb.x].v, cv);
-            Beam lb;
-            load_beam(p.beams + qb.y, lb);
-            float dist, rad2;
-            if (!pred_ray_disc(lb.o, lb.d, 0.f, lb.length, cv.hit, p.radius_bp2d_2, dist, rad2)) continue;
-            splat_camera(fbits(q8.x),
-                         cv.thr * p.bp2d_normalization * eval_bp2d(lb, cv.path_length, cv.w, cv.bsdf, dist, rad2));
-        }
-    }
+    const unsigned n = (unsigned)min(p.hit_state->total, (unsigned long long)p.hit_capacity);
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        eval_range_hit<kMode>(__ldg(&p.hit_qb[j]));
 }
 
 // SURF and PP3D for one point-query record per thread, evaluated inline:

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -165,11 +166,14 @@ struct upbp_ctx {
     unsigned conn_capacity = 0, nee_capacity = 0, bpt_capacity = 0;
     unsigned* d_path_err = nullptr;
     float4* d_path_color = nullptr;
-    // BB1D hit list (search -> evaluation)
+    // range-query hit list (search -> evaluation), round counters, and a
+    // copy of one kernel kind's work counters for a round that is repeated
     uint2* d_hit_qb = nullptr;
     unsigned hit_capacity = 0;
-    unsigned* d_hit_count = nullptr;
-    unsigned h_hit_count[2] = {0, 0};
+    size_t max_hits = 0;  // largest list: kMaxHits, or UPBP_MAX_HITS entries when that is smaller
+    HitState* d_hit_state = nullptr;
+    HitState h_hit_state = {};
+    unsigned long long* d_work_saved = nullptr;
     int search_grid[kRangeModes] = {};  // per range-query mode (kModePb2d ...)
     int camera_grid = 0;   // resident blocks of the persistent camera pass
     int light_grid = 0;    // resident blocks of the persistent light pass
@@ -379,11 +383,15 @@ int ensure_chunks(upbp_ctx* c, unsigned n)
     return UPBP_OK;
 }
 
-// Room for n PB2D / BB1D hits (8 bytes each).
+// Largest range-query hit list (8 bytes per entry, 17 GB); an iteration
+// with more hits runs its searches in rounds.
+constexpr size_t kMaxHits = size_t(1) << 31;
+
+// Room for n range-query hits (n + n/4, within 2^20 .. max_hits).
 int ensure_hits(upbp_ctx* c, size_t n)
 {
-    if (n <= c->hit_capacity) return UPBP_OK;
-    const size_t cap = std::min<size_t>(std::max<size_t>(n + n / 4, 1u << 20), 0x7fffffffu);
+    if (n <= c->hit_capacity || c->hit_capacity >= c->max_hits) return UPBP_OK;
+    const size_t cap = std::min<size_t>(std::max<size_t>(n + n / 4, 1u << 20), c->max_hits);
     UPBP_CK(cudaStreamSynchronize(c->st));
     cudaFree(c->d_hit_qb);
     c->d_hit_qb = nullptr;
@@ -565,7 +573,13 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     UPBP_CK(dalloc(&c->d_status, 1));
     UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
     UPBP_CK(dalloc(&c->d_qcount, 8));
-    UPBP_CK(dalloc(&c->d_hit_count, 2));
+    UPBP_CK(dalloc(&c->d_hit_state, 1));
+    UPBP_CK(dalloc(&c->d_work_saved, kCtrCount));
+    c->max_hits = kMaxHits;
+    if (const char* e = std::getenv("UPBP_MAX_HITS")) {
+        const long long v = std::atoll(e);
+        if (v > 0) c->max_hits = std::min<size_t>((size_t)v, kMaxHits);
+    }
     UPBP_CK(dalloc(&c->d_cam_fb, npx));
     {
         int dev = 0, sms = 0, per_sm = 0;
@@ -640,7 +654,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     P.bpt_color = c->d_bpt_color;
     P.path_err = c->d_path_err;
     P.path_color = c->d_path_color;
-    P.hit_count = c->d_hit_count;
+    P.hit_state = c->d_hit_state;
     P.cam_fb = c->d_cam_fb;
     UPBP_CK(cudaStreamSynchronize(c->st));
     *out = c;
@@ -888,17 +902,30 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
     }
     // The estimators: search (query, neighbour) pairs into the hit list, then
-    // evaluate them; a list that was too small is grown and the search
-    // repeated (it is a pure function of the queries and the map)
-    auto estimator = [&](int mode) -> int {
+    // evaluate them, in rounds over the query order.  A round stops handing
+    // out queries when the list is 3/4 full; if the queries in flight then
+    // overflow it, the round is repeated (the search is a pure function of
+    // the queries and the map) with a larger list or a shorter range.  A list
+    // that needed more than one round is grown for the next estimator and
+    // iteration (up to max_hits).
+    auto estimator = [&](int mode, unsigned nq) -> int {
         static constexpr int kKern[kRangeModes] = {kKernPb2d, kKernBb1d, kKernBp2d};
+        unsigned long long* work = c->d_work + (size_t)kKern[mode] * kCtrCount;
+        const size_t work_bytes = kCtrCount * sizeof(unsigned long long);
         if (c->hit_capacity == 0 && ensure_hits(c, (size_t)std::max(nseg, npt) * 32) != UPBP_OK) return UPBP_ERR_CUDA;
-        for (int attempt = 0; attempt < 2; attempt++) {
-            UPBP_CK(cudaMemsetAsync(c->d_hit_count, 0, 2 * sizeof(unsigned), c->st));
-            UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKern[mode] * kCtrCount, 0,
-                                    kCtrCount * sizeof(unsigned long long), c->st));
+        UPBP_CK(cudaMemsetAsync(work, 0, work_bytes, c->st));
+        unsigned long long found = 0;
+        unsigned begin = 0, span = nq;  // span: longest range of a round, halved after an overflow
+        int repeats = 0;
+        while (begin < nq) {
+            const unsigned end = begin + std::min(span, nq - begin);
+            UPBP_CK(cudaMemsetAsync(c->d_hit_state, 0, sizeof(HitState), c->st));
+            UPBP_CK(cudaMemcpyAsync(c->d_work_saved, work, work_bytes, cudaMemcpyDeviceToDevice, c->st));
             P.hit_qb = c->d_hit_qb;
             P.hit_capacity = c->hit_capacity;
+            P.hit_soft_limit = c->hit_capacity - c->hit_capacity / 4;
+            P.query_begin = begin;
+            P.query_end = end;
             h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
             const int g = c->search_grid[mode];
@@ -909,24 +936,43 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             }
             launches++;
             UPBP_CK(cudaGetLastError());
-            d2h += 2 * sizeof(unsigned);
-            UPBP_CK(cudaMemcpyAsync(c->h_hit_count, c->d_hit_count, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
-                                    c->st));
+            d2h += sizeof(HitState);
+            UPBP_CK(cudaMemcpyAsync(&c->h_hit_state, c->d_hit_state, sizeof(HitState), cudaMemcpyDeviceToHost, c->st));
             UPBP_CK(cudaStreamSynchronize(c->st));
-            if (c->h_hit_count[0] <= c->hit_capacity) break;
-            if (ensure_hits(c, c->h_hit_count[0]) != UPBP_OK) return UPBP_ERR_CUDA;
-        }
-        const unsigned nh = std::min(c->h_hit_count[0], c->hit_capacity);
-        if (nh > 0) {
-            const unsigned g = grid_for(nh);
-            switch (mode) {
-            case kModePb2d: range_eval_kernel<kModePb2d><<<g, 128, 0, c->st>>>(); break;
-            case kModeBb1d: range_eval_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(); break;
-            default: range_eval_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(); break;
+            const unsigned long long total = c->h_hit_state.total;
+            const unsigned done = (unsigned)std::min<unsigned long long>(c->h_hit_state.fetched, end - begin);
+            if (total > c->hit_capacity || done == 0) {
+                if (++repeats > 64) {  // repeats of one round
+                    upbp_host::set_error("range search made no progress");
+                    return UPBP_ERR_CUDA;
+                }
+                UPBP_CK(cudaMemcpyAsync(work, c->d_work_saved, work_bytes, cudaMemcpyDeviceToDevice, c->st));
+                if (c->hit_capacity < c->max_hits) {
+                    if (ensure_hits(c, (size_t)std::min<unsigned long long>(total, c->max_hits)) != UPBP_OK)
+                        return UPBP_ERR_CUDA;
+                } else {
+                    span = std::max(1u, std::min(done, end - begin) / 2);
+                }
+                continue;
             }
-            launches++;
+            if (total > 0) {
+                const unsigned g2 = grid_for((unsigned)total);
+                switch (mode) {
+                case kModePb2d: range_eval_kernel<kModePb2d><<<g2, 128, 0, c->st>>>(); break;
+                case kModeBb1d: range_eval_kernel<kModeBb1d><<<g2, 128, 0, c->st>>>(); break;
+                default: range_eval_kernel<kModeBp2d><<<g2, 128, 0, c->st>>>(); break;
+                }
+                launches++;
+                UPBP_CK(cudaGetLastError());
+            }
+            found += total;
+            begin += done;
+            repeats = 0;
+            span = span > nq / 2 ? nq : 2 * span;
         }
-        UPBP_CK(cudaGetLastError());
+        if (found > c->hit_capacity - c->hit_capacity / 4 &&
+            ensure_hits(c, (size_t)std::min<unsigned long long>(found + found / 8, c->max_hits)) != UPBP_OK)
+            return UPBP_ERR_CUDA;
         return UPBP_OK;
     };
     UPBP_CK(cudaEventRecord(ev[6], c->st));
@@ -940,11 +986,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         launches++;
     }
     UPBP_CK(cudaEventRecord(ev[8], c->st));
-    if (run_bp2d && estimator(kModeBp2d) != UPBP_OK) return UPBP_ERR_CUDA;
+    if (run_bp2d && estimator(kModeBp2d, npt) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[9], c->st));
-    if (run_pb2d && estimator(kModePb2d) != UPBP_OK) return UPBP_ERR_CUDA;
+    if (run_pb2d && estimator(kModePb2d, nseg) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[10], c->st));
-    if (run_bb1d && estimator(kModeBb1d) != UPBP_OK) return UPBP_ERR_CUDA;
+    if (run_bb1d && estimator(kModeBb1d, nseg) != UPBP_OK) return UPBP_ERR_CUDA;
     UPBP_CK(cudaEventRecord(ev[11], c->st));
     k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
                                                                          (unsigned)npx);
@@ -1179,7 +1225,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
                     c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
                     c->d_qcount, c->d_conn, c->d_nee, c->d_bpt, c->d_nee_color, c->d_bpt_color,
-                    c->d_path_err, c->d_path_color, c->d_hit_count, c->d_hit_qb, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
+                    c->d_path_err, c->d_path_color, c->d_hit_state, c->d_work_saved, c->d_hit_qb, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],
                     c->d_sort[0][2], c->d_sort[0][3], c->d_sort[1][0], c->d_sort[1][1], c->d_sort[1][2],
                     c->d_sort[1][3], c->d_sort_temp};
     for (void* b : bufs)

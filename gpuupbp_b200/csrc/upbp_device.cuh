@@ -232,6 +232,15 @@ UPBP_HD unsigned chunk_of(float t, float len, unsigned n)
     return k;
 }
 
+// Counters of one range-search round: hits found (may exceed the hit list's
+// capacity; 64-bit, a dense iteration finds billions) and queries handed out
+// (may exceed the round's range by the last requests).
+struct HitState {
+    unsigned long long total;
+    unsigned fetched;
+    unsigned pad;
+};
+
 struct DeviceParams {
     // scene
     const DMaterial* materials;
@@ -307,11 +316,17 @@ struct DeviceParams {
     const unsigned* pt_order;         // processing order of point queries (Morton order of the position)
     float* cam_fb;                    // camera-pass image, W*H*3
 
-    // BB1D hit list: the search kernel appends every (segment query, beam)
-    // pair the predicate accepts; the evaluation kernel consumes the list.
-    uint2* hit_qb;                    // (segment-query record index, beam index)
+    // Range-query hit list (PB2D, BB1D, BP2D): a search round appends every
+    // (query, neighbour) pair the predicate accepts for the queries
+    // [query_begin, query_end) of the processing order; the evaluation kernel
+    // consumes the list.  A round stops handing out queries once
+    // hit_soft_limit hits were found, so that the queries in flight still
+    // fit; the host runs rounds until every query was handed out.
+    uint2* hit_qb;                    // (query record index, beam index or light-vertex slot)
     unsigned hit_capacity;
-    unsigned* hit_count;              // [0] hits found (may exceed capacity), [1] next query to hand out
+    unsigned query_begin, query_end;
+    unsigned long long hit_soft_limit;
+    HitState* hit_state;
 
     // deferred camera-side connections; counts in queue_count[3..5]
     ConnVertexRec* conn_vertices;

@@ -199,7 +199,11 @@ int upbp_scene_load_predefined(int scene_id, uint32_t res_x, uint32_t res_y, upb
 const upbp_scene_desc* upbp_scene_get_desc(const upbp_scene* scene);
 void upbp_scene_free(upbp_scene* scene);
 
-/* Replaces: Renderer::init (gpuupbp/renderer/renderer_init.cpp:675-929). */
+/* Replaces: Renderer::init (gpuupbp/renderer/renderer_init.cpp:675-929).
+ * The range-query hit list grows with the work up to 2^31 entries (8 bytes
+ * each); an iteration with more hits runs its searches in rounds.  The
+ * environment variable UPBP_MAX_HITS, read here, sets a smaller limit
+ * (entries) for hosts with less device memory to spare. */
 int upbp_create(const upbp_scene_desc* scene, const upbp_config* config, upbp_ctx** out);
 /* Replaces: Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
  * Renders iteration `iteration` and adds it to the device accumulation. */

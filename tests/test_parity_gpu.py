@@ -62,3 +62,32 @@ def test_accumulation_is_the_mean_of_iterations(scene_dir):
     st = r.stats()
     assert st["iterations_done"] == 3 and st["status"] == 0
     r.close()
+
+
+def test_search_rounds_match_one_round(scene_dir, monkeypatch):
+    """A hit list far smaller than an iteration's hits makes every range
+    search run in many rounds (with repeated rounds after overflows): each
+    query must still be searched exactly once, so the work counters equal
+    those of a single round and the image equals it up to the order of the
+    float additions."""
+    from gpuupbp_b200 import upbp
+    path = scenes.write_workload("box_medium", scene_dir)
+    args = command_line("box_all_bp2d", path)
+    runs = []
+    for limit in (None, "512"):
+        if limit is None:
+            monkeypatch.delenv("UPBP_MAX_HITS", raising=False)
+        else:
+            monkeypatch.setenv("UPBP_MAX_HITS", limit)
+        r = upbp.Renderer(args)
+        r.run_iteration(0)
+        runs.append((r.iteration_image(), r.stats()))
+        r.close()
+    monkeypatch.delenv("UPBP_MAX_HITS", raising=False)
+    (img1, st1), (img2, st2) = runs
+    for k in ("pb2d_query", "bb1d_query", "bp2d_query"):
+        assert st1["work"][k] == st2["work"][k], k
+    assert st1["work"]["bb1d_query"]["beam_hit"] > 4 * 512
+    assert st2["kernel_launches"] > st1["kernel_launches"] + 8
+    assert np.allclose(img1, img2, rtol=1e-4, atol=1e-6)
+    assert st2["status"] == st1["status"]
