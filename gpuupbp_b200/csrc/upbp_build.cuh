@@ -242,6 +242,67 @@ __global__ void k_collapse(int n, BvhNode* nodes, int leaf_max)
     nodes[i].link = k;
 }
 
+// Smallest biased exponent e (1..254) with origin + 255 * 2^(e-127) >= hi
+// in the decoder's arithmetic.
+UPBP_D unsigned qnode_exponent(float origin, float hi)
+{
+    const float t = (hi - origin) * (1.f / 255.f);
+    unsigned e = t > 0.f ? ((__float_as_uint(t) >> 23) & 0xffu) + 1u : 1u;
+    e = min(max(e, 1u), 254u);
+    while (e < 254u && __fmaf_rn(255.f, qnode_step(e), origin) < hi) e++;
+    return e;
+}
+
+// Byte q with origin + q * step <= v (lower plane) or >= v (upper plane),
+// as tight as the step allows; v lies in [origin, origin + 255 * step].
+UPBP_D unsigned qnode_quantize(float v, float origin, float step, bool upper)
+{
+    const float f = (v - origin) / step;
+    int q = upper ? (int)ceilf(f) : (int)floorf(f);
+    q = min(max(q, 0), 255);
+    // at most 255 steps: q = 0 decodes to origin <= v, q = 255 to >= hi >= v
+    if (upper) {
+        while (q < 255 && __fmaf_rn((float)q, step, origin) < v) q++;
+    } else {
+        while (q > 0 && __fmaf_rn((float)q, step, origin) > v) q--;
+    }
+    return (unsigned)q;
+}
+
+// Compressed copy of the n - 1 internal nodes of a tree built with
+// one-primitive leaves (every child link is gamma or gamma + 1).
+__global__ void k_quantize(const BvhNode* nodes, int n_internal, QNode* q)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_internal) return;
+    const float4 a = nodes[i].a, b = nodes[i].b, c = nodes[i].c;
+    const int4 k = nodes[i].link;
+    const float lo[2][3] = {{a.x, a.y, a.z}, {b.z, b.w, c.x}};
+    const float hi[2][3] = {{a.w, b.x, b.y}, {c.y, c.z, c.w}};
+    float org[3], step[3];
+    unsigned ebits = 0;
+    for (int ax = 0; ax < 3; ax++) {
+        org[ax] = fminf(lo[0][ax], lo[1][ax]);
+        const unsigned e = qnode_exponent(org[ax], fmaxf(hi[0][ax], hi[1][ax]));
+        step[ax] = qnode_step(e);
+        ebits |= e << (8 * ax);
+    }
+    unsigned bytes[12];
+    for (int ch = 0; ch < 2; ch++)
+        for (int ax = 0; ax < 3; ax++) {
+            bytes[6 * ch + ax] = qnode_quantize(lo[ch][ax], org[ax], step[ax], false);
+            bytes[6 * ch + 3 + ax] = qnode_quantize(hi[ch][ax], org[ax], step[ax], true);
+        }
+    uint4 w;
+    w.x = bytes[0] | bytes[1] << 8 | bytes[2] << 16 | bytes[3] << 24;
+    w.y = bytes[4] | bytes[5] << 8 | bytes[6] << 16 | bytes[7] << 24;
+    w.z = bytes[8] | bytes[9] << 8 | bytes[10] << 16 | bytes[11] << 24;
+    const unsigned g = (unsigned)(k.x < 0 ? leaf_first(k.x) : k.x);
+    w.w = g | (k.x < 0 ? 1u << 30 : 0u) | (k.y < 0 ? 1u << 31 : 0u);
+    q[i].a = make_float4(org[0], org[1], org[2], __uint_as_float(ebits));
+    q[i].b = w;
+}
+
 // Leaf-order payloads.
 __global__ void k_gather_tris(const float4* tri, const unsigned* vals, unsigned n, float4* out)
 {

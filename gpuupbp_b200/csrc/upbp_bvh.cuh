@@ -102,6 +102,25 @@ UPBP_D NodeBoxes load_node(const BvhNode* nodes, int i)
     return r;
 }
 
+// A compressed node decoded into the children's boxes (each containing the
+// exact box) and links in BvhNode form.
+UPBP_D NodeBoxes load_qnode(const QNode* q, int i)
+{
+    const float4 a = __ldg(&q[i].a);
+    const uint4 b = __ldg(&q[i].b);
+    const unsigned e = __float_as_uint(a.w);
+    const float sx = qnode_step(e & 0xffu), sy = qnode_step((e >> 8) & 0xffu), sz = qnode_step((e >> 16) & 0xffu);
+    NodeBoxes r;
+    r.llo = make_float3(qnode_plane(b.x, 0, sx, a.x), qnode_plane(b.x, 1, sy, a.y), qnode_plane(b.x, 2, sz, a.z));
+    r.lhi = make_float3(qnode_plane(b.x, 3, sx, a.x), qnode_plane(b.y, 0, sy, a.y), qnode_plane(b.y, 1, sz, a.z));
+    r.rlo = make_float3(qnode_plane(b.y, 2, sx, a.x), qnode_plane(b.y, 3, sy, a.y), qnode_plane(b.z, 0, sz, a.z));
+    r.rhi = make_float3(qnode_plane(b.z, 1, sx, a.x), qnode_plane(b.z, 2, sy, a.y), qnode_plane(b.z, 3, sz, a.z));
+    const int g = (int)(b.w & 0x3fffffffu);
+    r.l = (b.w >> 30) & 1u ? leaf_link(g, 1) : g;
+    r.r = (b.w >> 31) ? leaf_link(g + 1, 1) : g + 1;
+    return r;
+}
+
 // Visits every leaf whose box (dilated by pad) passes `test_box`; calls
 // leaf(sorted_index) which returns false to stop.  Returns false if the
 // traversal stack overflowed.

@@ -571,7 +571,7 @@ constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
 constexpr int kSmemStack = 16;
 
 struct SearchWarp {
-    uint2 cand[kCandRing];  // (query record, map leaf | own-leaf bit << 31)
+    uint2 cand[kCandRing];  // (query record, map leaf)
     uint2 hit_qb[64];
     int stack[kSmemStack][32];
 };
@@ -636,7 +636,7 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     unsigned id = 0;
     if (lane < count) {
         pr = w.cand[(head + lane) % kCandRing];
-        const unsigned leaf = pr.y & 0x7fffffffu;
+        const unsigned leaf = pr.y;
         if constexpr (RangeMode<kMode>::seg) {
             const float4* r = p.seg_queue[pr.x].q;
             const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
@@ -644,7 +644,7 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
                 BeamSegHit h;
                 const int med = (int)fbits(__ldg(&r[2]).w);
                 hit = beam_chunk_vs_segment(p.beam_map, (int)leaf, xyz(q0), xyz(q1), q0.w, q1.w, p.radius_bb1d_2,
-                                            (pr.y >> 31) != 0, p.do_bp2d != 0, med, cand, h);
+                                            false, p.do_bp2d != 0, med, cand, h);
                 id = h.beam;
             } else {
                 const float4 pp = __ldg(&p.med_map.pos[leaf]);
@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(128) range_search_kernel()
         if (node != kWalkDone) {
             // one internal node: leaf children become pairs, internal ones are visited
             visits++;
-            const NodeBoxes nb = load_node(bvh.nodes, node);
+            const NodeBoxes nb = load_qnode(bvh.qnodes, node);
             bool hl, hr;
             if constexpr (M::seg) {
                 hl = slab(nb.llo, nb.lhi, inv, oinv, tmin, tmax);
@@ -815,9 +815,9 @@ __global__ void __launch_bounds__(128) range_search_kernel()
                 const bool second = i >= ln[0];
                 const int first = second ? lf[1] : lf[0], k = second ? i - ln[0] : i;
                 const int cnt = second ? ln[1] : ln[0];
-                // bit 31: the pair's primitive is a leaf of its own, whose box the walk tested
-                w.cand[(tail + __popc(m & below)) % kCandRing] =
-                    make_uint2(qk, (unsigned)(first + k) | (cnt == 1 ? 0x80000000u : 0u));
+                // the walk tests compressed boxes, which contain the exact ones:
+                // the leaf test re-checks a chunk's own box where it matters
+                w.cand[(tail + __popc(m & below)) % kCandRing] = make_uint2(qk, (unsigned)(first + k));
             }
             tail += __popc(m);
             if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);

@@ -142,6 +142,7 @@ struct upbp_ctx {
     double* d_acc = nullptr;
     unsigned* d_status = nullptr;
     BvhNode *d_surf_nodes = nullptr, *d_med_nodes = nullptr, *d_beam_nodes = nullptr;
+    QNode *d_med_qnodes = nullptr, *d_beam_qnodes = nullptr;  // compressed copies for the range searches
     float4 *d_surf_pos = nullptr, *d_med_pos = nullptr, *d_beam_seg = nullptr;
     unsigned *d_chunk_counts = nullptr, *d_chunk_offsets = nullptr;
     uint2* d_chunks = nullptr;
@@ -369,9 +370,11 @@ int ensure_chunks(upbp_ctx* c, unsigned n)
     if (cap > c->chunk_capacity) {
         cudaFree(c->d_chunks);
         cudaFree(c->d_beam_nodes);
+        cudaFree(c->d_beam_qnodes);
         cudaFree(c->d_beam_seg);
         UPBP_CK(dalloc(&c->d_chunks, cap));
         UPBP_CK(dalloc(&c->d_beam_nodes, cap));
+        UPBP_CK(dalloc(&c->d_beam_qnodes, cap));
         UPBP_CK(dalloc(&c->d_beam_seg, 3 * (size_t)cap));
         c->chunk_capacity = cap;
     }
@@ -613,6 +616,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
     UPBP_CK(dalloc(&c->d_path_color, P.screen_pixel_count));
     UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
+    UPBP_CK(dalloc(&c->d_med_qnodes, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_med_pos, c->vertex_capacity));
     UPBP_CK(dalloc(&c->d_chunk_counts, c->beam_capacity));
@@ -744,11 +748,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
     const unsigned nm = std::min(found[2], c->vertex_capacity);
     const unsigned nb = std::min(found[3], c->beam_capacity);
     P.surf_map = PointMap{BvhView{c->d_surf_nodes, 0}, c->d_surf_pos};
-    P.med_map = PointMap{BvhView{c->d_med_nodes, 0}, c->d_med_pos};
+    P.med_map = PointMap{BvhView{c->d_med_nodes, 0, c->d_med_qnodes}, c->d_med_pos};
     // beam-map boxes: the beam radius (BB1D and BP2D), the box tests' rounding
     // and the BB1D predicate's t1 error on nearly parallel lines
     const float beam_dilate = P.rad_beam * 1.0001f + P.beam_cull_eps;
-    P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg, beam_dilate};
+    P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0, c->d_beam_qnodes}, c->d_beam_seg, beam_dilate};
     if (P.build_surf && ns > 0) {
         BoxSource src{};
         src.kind = 1;
@@ -770,7 +774,8 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         const unsigned* order = nullptr;
         UPBP_CK(build_lbvh(src, nm, c->d_med_nodes, c->sc, c->st, &order));
         k_gather_points<<<(nm + 255) / 256, 256, 0, c->st>>>(c->d_idx_m, c->d_vertices, order, nm, c->d_med_pos);
-        launches += (nm > 1 ? 4 : 2) + 1;
+        if (nm > 1) k_quantize<<<(nm - 1 + 255) / 256, 256, 0, c->st>>>(c->d_med_nodes, (int)nm - 1, c->d_med_qnodes);
+        launches += (nm > 1 ? 5 : 2) + 1;
         P.med_map.bvh.count = nm;
     }
     if ((P.build_bb1d || P.build_bp2d) && nb > 0) {
@@ -786,7 +791,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(cudaStreamSynchronize(c->st));
         const unsigned nchunks = tail[0] + tail[1];
         if (ensure_chunks(c, nchunks) != UPBP_OK) return UPBP_ERR_CUDA;
-        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0}, c->d_beam_seg, beam_dilate};
+        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0, c->d_beam_qnodes}, c->d_beam_seg, beam_dilate};
         k_chunk_expand<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_chunk_counts, c->d_chunk_offsets, nb, c->d_chunks);
         BoxSource src{};
         src.kind = 3;
@@ -797,9 +802,13 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order, kBeamLeafMax));
         k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
                                                                   P.bb1d_used_light_subpath_count, c->d_beam_seg);
+        static_assert(kBeamLeafMax == 1, "compressed nodes need one-primitive leaves");
+        if (nchunks > 1)
+            k_quantize<<<(nchunks - 1 + 255) / 256, 256, 0, c->st>>>(c->d_beam_nodes, (int)nchunks - 1,
+                                                                     c->d_beam_qnodes);
         P.beam_map.bvh.count = nchunks;
         c->last_chunks = nchunks;
-        launches += 2 + (nchunks > 1 ? (kBeamLeafMax > 1 ? 5 : 4) : 2) + 1;
+        launches += 2 + (nchunks > 1 ? 5 : 2) + 1;
     }
     UPBP_CK(cudaGetLastError());
     P.n_surface = found[1];
@@ -1222,7 +1231,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
-                    c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
+                    c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_med_qnodes, c->d_beam_qnodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,
                     c->d_chunk_counts, c->d_chunk_offsets, c->d_chunks, c->d_scan_temp, c->d_work,
                     c->d_qcount, c->d_conn, c->d_nee, c->d_bpt, c->d_nee_color, c->d_bpt_color,
                     c->d_path_err, c->d_path_color, c->d_hit_state, c->d_work_saved, c->d_hit_qb, c->d_cam_fb, c->d_seg_queue, c->d_pt_queue, c->d_sort[0][0], c->d_sort[0][1],

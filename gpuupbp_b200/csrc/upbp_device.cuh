@@ -90,9 +90,33 @@ UPBP_HD int leaf_link(int first, int count) { return ~(first | ((count - 1) << k
 UPBP_HD int leaf_first(int link) { return (~link) & ((1 << kLeafShift) - 1); }
 UPBP_HD int leaf_count(int link) { return ((~link) >> kLeafShift) + 1; }
 
+// Compressed two-wide node of a photon map, 32 bytes (half a BvhNode), for
+// walks that are bound by the L1's per-lane sector lookups: the node's box
+// origin and a power-of-two step per axis, both children's boxes as 8-bit
+// multiples of the step (lower planes rounded down, upper planes up, with
+// the decoder's own arithmetic, so each stored box contains the exact one),
+// and the children of a Karras hierarchy of one-primitive leaves, which are
+// always gamma and gamma + 1: link = gamma | left-is-leaf << 30 |
+// right-is-leaf << 31.
+struct __align__(32) QNode {
+    float4 a;  // origin.xyz; w: biased step exponents x | y << 8 | z << 16
+    uint4 b;   // plane bytes: left lo xyz, left hi xyz, right lo xyz, right hi xyz; w: link
+};
+
+// Step 2^(e - 127) of a biased exponent byte e in 1..254.
+UPBP_D float qnode_step(unsigned e) { return __uint_as_float(e << 23); }
+
+// Plane `byte` of a QNode word: origin + q * step with q the byte (the one
+// rounding of the decoder; the encoder checks its bytes with it).
+UPBP_D float qnode_plane(unsigned word, int byte, float step, float origin)
+{
+    return __fmaf_rn((float)((word >> (8 * byte)) & 0xffu), step, origin);
+}
+
 struct BvhView {
     const BvhNode* nodes;
     unsigned count;          // primitives
+    const QNode* qnodes;     // the same hierarchy compressed (photon maps), or nullptr
 };
 
 // Triangles in BVH leaf order: v0 (w = original index bits), e1, e2.
