@@ -91,7 +91,10 @@ UPBP_HD int leaf_first(int link) { return (~link) & ((1 << kLeafShift) - 1); }
 UPBP_HD int leaf_count(int link) { return ((~link) >> kLeafShift) + 1; }
 
 // Compressed two-wide node of a photon map, 32 bytes (half a BvhNode), for
-// walks that are bound by the L1's per-lane sector lookups: the node's box
+// the range searches, which were bound by the L1's lookups (lanes of a warp
+// read nodes at unrelated addresses and each lane's 16-byte part of a load is
+// looked up separately; the path kernels, bound by divergence, stay on
+// BvhNodes, where decoding cost more than it saved): the node's box
 // origin and a power-of-two step per axis, both children's boxes as 8-bit
 // multiples of the step (lower planes rounded down, upper planes up, with
 // the decoder's own arithmetic, so each stored box contains the exact one),
