@@ -123,10 +123,13 @@ class ClockSampler:
 # framebuffer read-modify-write per pixel.
 BYTES_PER_WORK = {"nodes": 64, "tris": 48, "rays": 72, "point_cand": 16, "point_hit": 128, "beam_cand": 48,
                   "beam_hit": 128, "vertex_loads": 128}
+# The PB2D, BB1D and BP2D searches walk the maps' 32-byte compressed nodes.
+COMPRESSED_NODE_KERNELS = ("pb2d_query", "bb1d_query", "bp2d_query")
 
 
-def algorithmic_bytes(work: dict, extra: float = 0.0) -> float:
-    return float(sum(BYTES_PER_WORK[k] * v for k, v in work.items())) + extra
+def algorithmic_bytes(work: dict, extra: float = 0.0, node_bytes: int = 64) -> float:
+    per = dict(BYTES_PER_WORK, nodes=node_bytes)
+    return float(sum(per[k] * v for k, v in work.items())) + extra
 
 
 # Bytes of the query records each camera-side kernel writes or reads.
@@ -158,7 +161,7 @@ def kernel_rooflines(st: dict, pixels: int) -> dict:
     out = {}
     for k, w in st["work"].items():
         t = ms[k] / n
-        b = algorithmic_bytes(w, extra[k])
+        b = algorithmic_bytes(w, extra[k], 32 if k in COMPRESSED_NODE_KERNELS else 64)
         out[k] = {"ms": t, "bytes": b, "gbs": (b / (t * 1e-3) / 1e9) if t > 0 else 0.0}
     return out
 
