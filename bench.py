@@ -166,6 +166,23 @@ def kernel_rooflines(st: dict, pixels: int) -> dict:
     return out
 
 
+def iteration_bytes(st: dict, pixels: int) -> float:
+    """Algorithmic bytes of one whole iteration with implementation-independent
+    record sizes: rays (node visits x 32 B + triangle tests x 40 B), stored
+    light vertices 80 B and beams 128 B (written and read), query candidates x
+    their record (photon 80 B, beam 128 B), BPT connections 80 B, photon-map
+    builds (8-byte key/value + one 32-byte node per primitive), pixels 12 B
+    (written and read)."""
+    w = st["work"]
+    rays = sum(w[k]["nodes"] * 32 + w[k]["tris"] * 40
+               for k in ("light_pass", "camera_extend", "nee_connect", "bpt_connect"))
+    cand = sum(w[k]["point_cand"] * 80 + w[k]["beam_cand"] * 128
+               for k in ("surf_query", "pp3d_query", "pb2d_query", "bb1d_query", "bp2d_query"))
+    build = (st["surface_vertices"] + st["medium_vertices"] + st["beam_chunks"]) * (8 + 32)
+    return float(rays + st["light_vertices"] * 80 * 2 + st["light_beams"] * 128 * 2 + cand + st["bpt_pairs"] * 80
+                 + build + pixels * 12 * 2)
+
+
 def profiled_traffic() -> float | None:
     """DRAM bytes per iteration of the BB1D kernels from the committed ncu summary."""
     p = os.path.join(HERE, "profiles", "bb1d_query_media_field.md")
@@ -263,6 +280,10 @@ def run_b200(args) -> dict | None:
     # the committed capture is scaled to the default resolution only
     traffic = (profiled_traffic() if top == "bb1d_query" and args.workload == "media_field" and tuple(args.res) == RES
                else None)
+    b_iter = iteration_bytes(st, pixels)
+    iteration_roofline = {"bound": "hbm", "achieved": b_iter / (ms / args.steps * 1e-3) / 1e9, "peak": hbm,
+                          "unit": "GB/s", "frac": b_iter / (ms / args.steps * 1e-3) / 1e9 / hbm,
+                          "algorithmic_bytes_per_step": b_iter, "peak_source": peak_src}
     total_paths = paths_per_iter * args.steps * world
     value = total_paths / (ms * 1e-3)
     e2e = total_paths / (ms_e2e * 1e-3)
@@ -282,6 +303,7 @@ def run_b200(args) -> dict | None:
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes_per_launch": b_top, "launch_ms": top_ms},
+        "iteration_roofline": iteration_roofline,
         "kernels": kernels,
         "clocks": clk.summary(),
         "passes_ms": {"light": st["ms_light_sum"] / max(1, st["timed_iterations"]),
