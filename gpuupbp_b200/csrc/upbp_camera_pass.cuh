@@ -642,9 +642,8 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
             const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
             if constexpr (kMode == kModeBb1d) {
                 BeamSegHit h;
-                const int med = (int)fbits(__ldg(&r[2]).w);
                 hit = beam_chunk_vs_segment(p.beam_map, (int)leaf, xyz(q0), xyz(q1), q0.w, q1.w, p.radius_bb1d_2,
-                                            false, p.do_bp2d != 0, med, cand, h);
+                                            false, p.do_bp2d != 0, -1, &r[2], cand, h);
                 id = h.beam;
             } else {
                 const float4 pp = __ldg(&p.med_map.pos[leaf]);
@@ -658,11 +657,12 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
             // beam's closest point reports it
             const float3 x = xyz(__ldg(&p.pt_queue[pr.x].v.q[0]));
             const float4 s0 = __ldg(&p.beam_map.seg[3 * leaf]), s1 = __ldg(&p.beam_map.seg[3 * leaf + 1]);
-            const float4 s2 = __ldg(&p.beam_map.seg[3 * leaf + 2]);
             float dist, rad2;
             cand++;
-            hit = pred_ray_disc(xyz(s0), xyz(s1), 0.f, s0.w, x, p.radius_bp2d_2, dist, rad2) && dist >= s2.x &&
-                  dist < s2.y;
+            if (pred_ray_disc(xyz(s0), xyz(s1), 0.f, s0.w, x, p.radius_bp2d_2, dist, rad2)) {
+                const float4 s2 = __ldg(&p.beam_map.seg[3 * leaf + 2]);  // the chunk's range, for accepted pairs only
+                hit = dist >= s2.x && dist < s2.y;
+            }
             id = fbits(s1.w) & 0x7fffffffu;
         }
     }

@@ -95,18 +95,23 @@ UPBP_D bool chunk_reached(float3 bo, float3 bd, float len, unsigned k, unsigned 
 // the set equals a test of every beam (a chunk reached only as part of a
 // leaf of several chunks never reports).  cand counts the leaves that reach
 // the predicate; own_box tells that the walk reached this chunk through a
-// leaf of its own (so its box passed).
+// leaf of its own (so its box passed).  The query's medium is `med`, or,
+// when med_src is set, med_src->w: read, like the chunk's medium and range,
+// only for pairs the predicate accepts (three of four are rejected, and each
+// record read is one more L1 lookup per lane).
 UPBP_D bool beam_chunk_vs_segment(const BeamMap& map, int i, float3 o, float3 d, float tmin, float tmax, float r2,
-                                  bool own_box, bool need_mask, int med, unsigned& cand, BeamSegHit& h)
+                                  bool own_box, bool need_mask, int med, const float4* med_src, unsigned& cand,
+                                  BeamSegHit& h)
 {
     const float4 s1 = __ldg(&map.seg[3 * i + 1]);
     const unsigned bits = fbits(s1.w);
     if (need_mask && !(bits >> 31)) return false;
-    const float4 s2 = __ldg(&map.seg[3 * i + 2]);
-    if (med >= 0 && (int)fbits(s2.z) != med) return false;
     const float4 s0 = __ldg(&map.seg[3 * i]);
     cand++;
     if (!pred_beam_beam(o, d, tmin, tmax, xyz(s0), xyz(s1), s0.w, r2, h.dist, h.sin_theta, h.t1, h.t2)) return false;
+    const float4 s2 = __ldg(&map.seg[3 * i + 2]);
+    if (med_src) med = (int)fbits(__ldg(med_src).w);
+    if (med >= 0 && (int)fbits(s2.z) != med) return false;
     h.beam = bits & 0x7fffffffu;
     const bool mine = h.t2 >= s2.x && h.t2 < s2.y;
     const float3 bo = xyz(s0), bd = xyz(s1);
@@ -140,7 +145,8 @@ UPBP_D void beams_near_segment(const BeamMap& map, float3 o, float3 d, float tmi
         const int leaf = walk_step(
             s, map.bvh, [&](float3 lo, float3 hi) { return slab(lo, hi, inv, oinv, tmin, tmax); }, overflow, visits);
         BeamSegHit h;
-        if (leaf >= 0 && beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, false, need_mask, med, cand, h)) {
+        if (leaf >= 0 &&
+            beam_chunk_vs_segment(map, leaf, o, d, tmin, tmax, r2, false, need_mask, med, nullptr, cand, h)) {
             hits++;
             f(h.beam, h.dist, h.sin_theta, h.t1, h.t2);
         }
