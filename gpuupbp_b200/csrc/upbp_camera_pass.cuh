@@ -7,6 +7,8 @@
 // functs_bp2d.cuh:51-229).
 #pragma once
 
+#include <type_traits>
+
 #include "upbp_build.cuh"
 #include "upbp_queries.cuh"
 
@@ -550,6 +552,9 @@ template <int kMode> struct RangeMode {
     static constexpr bool seg = kMode != kModeBp2d;  // segment queries (else point queries)
     static constexpr bool beams = kMode != kModePb2d;  // beam map (else medium photon map)
     static constexpr int kern = kMode == kModePb2d ? kKernPb2d : kMode == kModeBb1d ? kKernBb1d : kKernBp2d;
+    // query geometry of waiting pairs in shared memory (long BB1D queries;
+    // the short PB2D and BP2D ones refill lanes too often for its flushes)
+    static constexpr bool shared_geo = kMode == kModeBb1d;
 };
 
 enum : unsigned { kQuerySurf = 1u, kQueryPp3d = 2u, kQueryBp2d = 4u };
@@ -570,11 +575,24 @@ constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
 // to local memory.  Local memory competes with the photon maps for L1.
 constexpr int kSmemStack = 16;
 
+// A waiting pair names the lane whose query it belongs to in the top bits of
+// its leaf word (leaf indices stay below 2^kLeafShift).  With shared_geo the
+// lane's query geometry sits in shared memory, so a pair test reads only the
+// map's record from global memory; a lane then overwrites its geometry only
+// when no pair is waiting.
+constexpr unsigned kPairLeafMask = (1u << kLeafShift) - 1u;
+
 struct SearchWarp {
-    uint2 cand[kCandRing];  // (query record, map leaf)
+    uint2 cand[kCandRing];  // (query record, map leaf | owner lane << kLeafShift)
     uint2 hit_qb[64];
     int stack[kSmemStack][32];
 };
+struct SearchWarpGeo : SearchWarp {
+    float4 qgeo[2][32];     // per lane: (origin, tmin), (direction, tmax)
+};
+template <int kMode>
+using SearchWarpOf = std::conditional_t<RangeMode<kMode>::shared_geo, SearchWarpGeo, SearchWarp>;
+static_assert(kLeafShift + 5 <= 32, "owner lane bits");
 
 // The estimate of one accepted (query, neighbour) pair: the predicate's
 // geometry recomputed, the estimator with its MIS weight, added into the
@@ -625,7 +643,7 @@ UPBP_D void eval_range_hit(uint2 qb)
 // lane; accepted pairs go to the hit buffer, which is flushed by 32.  A hit
 // is (query record, beam) or (query record, light-vertex slot).
 template <int kMode>
-UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
+UPBP_D void search_test_pairs(SearchWarpOf<kMode>& w, unsigned& head, unsigned count, unsigned& hfill, unsigned lane,
                               unsigned& cand, unsigned& hits, unsigned long long& seen)
 {
     const DeviceParams& p = c_params;
@@ -636,10 +654,17 @@ UPBP_D void search_test_pairs(SearchWarp& w, unsigned& head, unsigned count, uns
     unsigned id = 0;
     if (lane < count) {
         pr = w.cand[(head + lane) % kCandRing];
-        const unsigned leaf = pr.y;
+        const unsigned leaf = pr.y & kPairLeafMask, owner = pr.y >> kLeafShift;
         if constexpr (RangeMode<kMode>::seg) {
             const float4* r = p.seg_queue[pr.x].q;
-            const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]);
+            float4 q0, q1;
+            if constexpr (RangeMode<kMode>::shared_geo) {
+                q0 = w.qgeo[0][owner];
+                q1 = w.qgeo[1][owner];
+            } else {
+                q0 = __ldg(&r[0]);
+                q1 = __ldg(&r[1]);
+            }
             if constexpr (kMode == kModeBb1d) {
                 BeamSegHit h;
                 hit = beam_chunk_vs_segment(p.beam_map, (int)leaf, xyz(q0), xyz(q1), q0.w, q1.w, p.radius_bb1d_2,
@@ -694,8 +719,8 @@ __global__ void __launch_bounds__(128) range_search_kernel()
     using M = RangeMode<kMode>;
     begin_kernel(M::kern);
     const DeviceParams& p = c_params;
-    __shared__ SearchWarp s_warp[kSearchWarps];
-    SearchWarp& w = s_warp[threadIdx.x >> 5];
+    __shared__ SearchWarpOf<kMode> s_warp[kSearchWarps];
+    SearchWarpOf<kMode>& w = s_warp[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     // this round's range of the processing order, within the queue
@@ -716,6 +741,10 @@ __global__ void __launch_bounds__(128) range_search_kernel()
         const bool idle = node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
+            // a lane that takes a new query overwrites its geometry: test the
+            // pairs still waiting first
+            if (M::shared_geo && tail != head)
+                search_test_pairs<kMode>(w, head, tail - head, hfill, lane, cand, hits, seen);
             // no new queries once the hit list is 3/4 full, as far as this
             // warp saw at its last flush of hits (no extra load of the
             // counter, which every flush and request updates)
@@ -738,6 +767,10 @@ __global__ void __launch_bounds__(128) range_search_kernel()
                         tmax = q1.w;
                         inv = safe_inv(xyz(q1));
                         oinv = oinv_of(xyz(q0), inv);
+                        if constexpr (M::shared_geo) {
+                            w.qgeo[0][lane] = q0;
+                            w.qgeo[1][lane] = q1;
+                        }
                     } else {
                         // point queries of other estimators, or of camera paths
                         // that failed earlier, are skipped
@@ -817,7 +850,8 @@ __global__ void __launch_bounds__(128) range_search_kernel()
                 const int cnt = second ? ln[1] : ln[0];
                 // the walk tests compressed boxes, which contain the exact ones:
                 // the leaf test re-checks a chunk's own box where it matters
-                w.cand[(tail + __popc(m & below)) % kCandRing] = make_uint2(qk, (unsigned)(first + k));
+                w.cand[(tail + __popc(m & below)) % kCandRing] =
+                    make_uint2(qk, (unsigned)(first + k) | (lane << kLeafShift));
             }
             tail += __popc(m);
             if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);
