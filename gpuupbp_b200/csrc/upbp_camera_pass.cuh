@@ -470,12 +470,12 @@ UPBP_D void emit_segment_queries(float3 ro, float3 rd, const VolSeg* segs, int n
 
 // Unpacks segment-query record k: the query, the camera-side MIS state, the
 // path weight before the segment and the packed pixel / camera path length.
-UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& weight, unsigned& pk, unsigned& path,
+template <class Fetch>
+UPBP_D void read_seg_query(Fetch&& r, QuerySeg& q, StateWeights& cw, float3& weight, unsigned& pk, unsigned& path,
                            unsigned& key)
 {
-    const float4* r = c_params.seg_queue[k].q;
-    const float4 q0 = __ldg(&r[0]), q1 = __ldg(&r[1]), q2 = __ldg(&r[2]), q3 = __ldg(&r[3]);
-    const float4 q4 = __ldg(&r[4]), q5 = __ldg(&r[5]), q6 = __ldg(&r[6]), q7 = __ldg(&r[7]);
+    const float4 q0 = r(0), q1 = r(1), q2 = r(2), q3 = r(3);
+    const float4 q4 = r(4), q5 = r(5), q6 = r(6), q7 = r(7);
     q.o = xyz(q0);
     q.dmin = q0.w;
     q.d = xyz(q1);
@@ -504,6 +504,13 @@ UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& we
     cw.d_pde_b = q7.x;
     path = fbits(q7.y);
     key = fbits(q7.z);
+}
+
+UPBP_D void load_seg_query(unsigned k, QuerySeg& q, StateWeights& cw, float3& weight, unsigned& pk, unsigned& path,
+                           unsigned& key)
+{
+    const float4* r = c_params.seg_queue[k].q;
+    read_seg_query([&](int i) { return __ldg(&r[i]); }, q, cw, weight, pk, path, key);
 }
 
 // True if the contribution with event key `key` of camera path `path` is one
@@ -596,9 +603,11 @@ static_assert(kLeafShift + 5 <= 32, "owner lane bits");
 
 // The estimate of one accepted (query, neighbour) pair: the predicate's
 // geometry recomputed, the estimator with its MIS weight, added into the
-// camera image.
-template <int kMode>
-UPBP_D void eval_range_hit(uint2 qb)
+// camera image.  fq(i) and fn(i) return float4 i of the query's record
+// (segment query, or a point query's camera vertex) and of the neighbour's
+// (beam or light vertex).
+template <int kMode, class FQ, class FN>
+UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
 {
     using M = RangeMode<kMode>;
     const DeviceParams& p = c_params;
@@ -607,12 +616,12 @@ UPBP_D void eval_range_hit(uint2 qb)
         StateWeights cw;
         float3 weight;
         unsigned pk, path, key;
-        load_seg_query(qb.x, q, cw, weight, pk, path, key);
+        read_seg_query(fq, q, cw, weight, pk, path, key);
         if (!event_kept(path, key)) return;
         float3 est;
         if constexpr (kMode == kModeBb1d) {
             Beam lb;
-            load_beam(p.beams + qb.y, lb);
+            read_beam(fn, lb);
             float dist, sin_theta, t1, t2;
             if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta,
                                 t1, t2))
@@ -620,7 +629,7 @@ UPBP_D void eval_range_hit(uint2 qb)
             est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
         } else {
             LightVertex lv;
-            load_vertex(p.vertices + qb.y, lv);
+            read_vertex(fn, lv);
             float dist, rad2;
             if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) return;
             est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
@@ -629,9 +638,9 @@ UPBP_D void eval_range_hit(uint2 qb)
     } else {
         const float4 q8 = __ldg(&p.pt_queue[qb.x].q8);
         LightVertex cv;
-        load_vertex(&p.pt_queue[qb.x].v, cv);
+        read_vertex(fq, cv);
         Beam lb;
-        load_beam(p.beams + qb.y, lb);
+        read_beam(fn, lb);
         float dist, rad2;
         if (!pred_ray_disc(lb.o, lb.d, 0.f, lb.length, cv.hit, p.radius_bp2d_2, dist, rad2)) return;
         splat_camera(fbits(q8.x),
@@ -872,13 +881,57 @@ __global__ void __launch_bounds__(128) range_search_kernel()
     if (overflow) flag_status(kErrTraversalStack);
 }
 
+// The 128-byte records of a warp's 32 hits, read together: eight lanes load
+// one record as consecutive 16-byte pieces (four records per instruction, a
+// coalesced access each, instead of eight lookups per lane at unrelated
+// addresses, which kept the L1 busy), then every lane takes its own record
+// from shared memory (rows padded to 144 bytes, so the eight lanes of a
+// quarter-warp read different banks).  rec is this lane's record.
+constexpr int kEvalWarps = 4;
+UPBP_D void gather_records(const float4* rec, float4 (&out)[8], float4 (*s)[9], unsigned lane)
+{
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const unsigned r = 4u * k + (lane >> 3);
+        const auto rp = reinterpret_cast<const float4*>(
+            __shfl_sync(~0u, reinterpret_cast<unsigned long long>(rec), (int)r));
+        s[r][lane & 7u] = __ldg(rp + (lane & 7u));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = s[lane][i];
+}
+
+// One warp per 32 consecutive hits; lanes past the end read the warp's
+// first hit's records and evaluate nothing.
 template <int kMode>
 __global__ void __launch_bounds__(128) range_eval_kernel()
 {
+    using M = RangeMode<kMode>;
     const DeviceParams& p = c_params;
+    __shared__ float4 s_rec[kEvalWarps][32][9];
+    float4(*s)[9] = s_rec[threadIdx.x >> 5];
+    const unsigned lane = threadIdx.x & 31u;
     const unsigned n = (unsigned)min(p.hit_state->total, (unsigned long long)p.hit_capacity);
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-        eval_range_hit<kMode>(__ldg(&p.hit_qb[j]));
+    for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
+        const unsigned j = base + lane;
+        const uint2 qb = __ldg(&p.hit_qb[j < n ? j : base]);
+        const float4* qrec;
+        const float4* nrec;
+        if constexpr (M::seg)
+            qrec = p.seg_queue[qb.x].q;
+        else
+            qrec = p.pt_queue[qb.x].v.q;
+        if constexpr (M::beams)
+            nrec = p.beams[qb.y].q;
+        else
+            nrec = p.vertices[qb.y].q;
+        float4 qa[8], na[8];
+        gather_records(qrec, qa, s, lane);
+        gather_records(nrec, na, s, lane);
+        if (j < n) eval_range_hit<kMode>(qb, [&](int i) { return qa[i]; }, [&](int i) { return na[i]; });
+    }
 }
 
 // SURF and PP3D for one point-query record per thread, evaluated inline:

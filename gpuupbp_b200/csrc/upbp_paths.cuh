@@ -157,11 +157,13 @@ struct LightVertex {
     VertexWeights w;
 };
 
-UPBP_D void load_vertex(const LightVertexRec* rec, LightVertex& v)
+// A light-vertex record unpacked; q(i) returns float4 i of the record (read
+// from global memory, or from registers after a warp's gather).
+template <class Fetch>
+UPBP_D void read_vertex(Fetch&& q, LightVertex& v)
 {
-    const float4* q = rec->q;
-    const float4 q0 = __ldg(&q[0]), q1 = __ldg(&q[1]), q2 = __ldg(&q[2]), q3 = __ldg(&q[3]);
-    const float4 q4 = __ldg(&q[4]), q5 = __ldg(&q[5]);
+    const float4 q0 = q(0), q1 = q(1), q2 = q(2), q3 = q(3);
+    const float4 q4 = q(4), q5 = q(5);
     const unsigned meta = fbits(q0.w), ids = fbits(q3.w);
     v.hit = xyz(q0);
     v.thr = xyz(q1);
@@ -183,7 +185,7 @@ UPBP_D void load_vertex(const LightVertexRec* rec, LightVertex& v)
     b.cont_prob = q1.w;
     b.frame.set_from_z(xyz(q4));
     if (b.on_surface()) {
-        const float4 q6 = __ldg(&q[6]), q7 = __ldg(&q[7]);
+        const float4 q6 = q(6), q7 = q(7);
         b.ior = q4.w;
         b.local_dir_fix = xyz(q5);
         b.cos_fix_geom = q5.w;
@@ -201,6 +203,12 @@ UPBP_D void load_vertex(const LightVertexRec* rec, LightVertex& v)
         b.scatter_pos = !is_black_or_negative(m.scattering);
     }
 }
+
+UPBP_D void load_vertex(const LightVertexRec* rec, LightVertex& v)
+{
+    read_vertex([&](int i) { return __ldg(&rec->q[i]); }, v);
+}
+
 
 struct Beam {
     float3 o, d;
@@ -228,11 +236,12 @@ UPBP_D void store_beam(BeamRec* rec, const Beam& b)
     q[7] = make_float4(b.sw.d_pde_b, 0.f, 0.f, 0.f);
 }
 
-UPBP_D void load_beam(const BeamRec* rec, Beam& b)
+// A beam record unpacked; q(i) returns float4 i of the record.
+template <class Fetch>
+UPBP_D void read_beam(Fetch&& q, Beam& b)
 {
-    const float4* q = rec->q;
-    const float4 q0 = __ldg(&q[0]), q1 = __ldg(&q[1]), q2 = __ldg(&q[2]), q3 = __ldg(&q[3]);
-    const float4 q4 = __ldg(&q[4]), q5 = __ldg(&q[5]), q6 = __ldg(&q[6]), q7 = __ldg(&q[7]);
+    const float4 q0 = q(0), q1 = q(1), q2 = q(2), q3 = q(3);
+    const float4 q4 = q(4), q5 = q(5), q6 = q(6), q7 = q(7);
     b.o = xyz(q0);
     b.length = q0.w;
     b.d = xyz(q1);
@@ -259,6 +268,11 @@ UPBP_D void load_beam(const BeamRec* rec, Beam& b)
     b.sw.d_bpt_b = q6.z;
     b.sw.d_pde_a = q6.w;
     b.sw.d_pde_b = q7.x;
+}
+
+UPBP_D void load_beam(const BeamRec* rec, Beam& b)
+{
+    read_beam([&](int i) { return __ldg(&rec->q[i]); }, b);
 }
 
 // ---------------------------------------------------------------- exact predicates
