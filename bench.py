@@ -308,7 +308,8 @@ def run_b200(args) -> dict | None:
         "clocks": clk.summary(),
         "passes_ms": {"light": st["ms_light_sum"] / max(1, st["timed_iterations"]),
                       "build": st["ms_build_sum"] / max(1, st["timed_iterations"]), "camera": cam_ms},
-        "work": st["work"], "queries": {"segment": st["segment_queries"], "point": st["point_queries"]},
+        "work": st["work"], "queries": {"segment": st["segment_queries"], "point": st["point_queries"],
+                    "nee_samples": st["nee_samples"], "bpt_pairs": st["bpt_pairs"]},
         "status": int(st["status"]), "wall_s": wall,
     }
     r.close()

@@ -746,7 +746,9 @@ __global__ void __launch_bounds__(128) range_search_kernel()
     unsigned head = 0, tail = 0, hfill = 0;  // same values in every lane
     unsigned visits = 0, cand = 0, hits = 0;
     for (;;) {
-        int lf[2] = {0, 0}, ln[2] = {0, 0};  // leaves (first primitive, count) reached this step
+        // primitives of the leaf children reached this step (a compressed
+        // node's leaves hold one primitive each), -1 for none
+        int leaf0 = -1, leaf1 = -1;
         const bool idle = node == kWalkDone;
         const unsigned want = __ballot_sync(~0u, idle && !exhausted);
         if (want) {
@@ -793,8 +795,7 @@ __global__ void __launch_bounds__(128) range_search_kernel()
                     sp = 0;
                     node = bvh.count > 1 ? 0 : kWalkDone;
                     if (bvh.count == 1) {  // a one-leaf map
-                        lf[0] = 0;
-                        ln[0] = 1;
+                        leaf0 = 0;
                     }
                 }
             }
@@ -814,16 +815,14 @@ __global__ void __launch_bounds__(128) range_search_kernel()
             int next = -1, other = -1;
             if (hl) {
                 if (nb.l < 0) {
-                    lf[0] = leaf_first(nb.l);
-                    ln[0] = leaf_count(nb.l);
+                    leaf0 = leaf_first(nb.l);
                 } else {
                     next = nb.l;
                 }
             }
             if (hr) {
                 if (nb.r < 0) {
-                    lf[1] = leaf_first(nb.r);
-                    ln[1] = leaf_count(nb.r);
+                    leaf1 = leaf_first(nb.r);
                 } else if (next < 0) {
                     next = nb.r;
                 } else {
@@ -847,21 +846,16 @@ __global__ void __launch_bounds__(128) range_search_kernel()
                 node = kWalkDone;
             }
         }
-        // the primitives of the reached leaves become pairs, one per lane and
-        // round; 32 waiting pairs are tested at once
-        const int npend = ln[0] + ln[1];
-        for (int i = 0; __any_sync(~0u, i < npend); i++) {
-            const bool has = i < npend;
-            const unsigned m = __ballot_sync(~0u, has);
-            if (has) {
-                const bool second = i >= ln[0];
-                const int first = second ? lf[1] : lf[0], k = second ? i - ln[0] : i;
-                const int cnt = second ? ln[1] : ln[0];
-                // the walk tests compressed boxes, which contain the exact ones:
-                // the leaf test re-checks a chunk's own box where it matters
-                w.cand[(tail + __popc(m & below)) % kCandRing] =
-                    make_uint2(qk, (unsigned)(first + k) | (lane << kLeafShift));
-            }
+        // each reached leaf becomes a waiting pair, in two rounds (a lane adds
+        // up to two); 32 waiting pairs are tested at once.  The walk tests
+        // compressed boxes, which contain the exact ones: the leaf test
+        // re-checks a chunk's own box where it matters.
+#pragma unroll 1
+        for (int side = 0; side < 2; side++) {
+            const int lv = side ? leaf1 : leaf0;
+            const unsigned m = __ballot_sync(~0u, lv >= 0);
+            if (lv >= 0)
+                w.cand[(tail + __popc(m & below)) % kCandRing] = make_uint2(qk, (unsigned)lv | (lane << kLeafShift));
             tail += __popc(m);
             if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);
         }
