@@ -10,8 +10,10 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
+#include "host/upbp_sah.h"
 #include "host/upbp_scene.h"
 #include "upbp_build.cuh"
 #include "upbp_camera_pass.cuh"
@@ -267,23 +269,51 @@ int upload_geometry(upbp_ctx* c, const upbp_scene_desc* s, bool real, Geometry& 
         rec.push_back(make_int2(m, s->tri_light[i]));
     }
     g.count = (unsigned)rec.size();
-    float4* unsorted = nullptr;
-    UPBP_CK(dupload(&unsorted, tri.data(), tri.size(), c->st));
     UPBP_CK(dupload(&g.normals, nrm.data(), nrm.size(), c->st));
     UPBP_CK(dupload(&g.record, rec.data(), rec.size(), c->st));
     UPBP_CK(dalloc(&g.nodes, g.count > 1 ? g.count - 1 : 1));
-    UPBP_CK(dalloc(&g.tri, 3 * (size_t)std::max(1u, g.count)));
-    if (g.count > 0) {
-        BoxSource src{};
-        src.kind = 0;
-        src.tri = unsorted;
-        const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, g.count, g.nodes, c->sc, c->st, &order));
-        k_gather_tris<<<(g.count + 255) / 256, 256, 0, c->st>>>(unsorted, order, g.count, g.tri);
-        UPBP_CK(cudaGetLastError());
+    // Static scene: a binned-SAH tree built once on the host (the photon maps
+    // are rebuilt every iteration as GPU LBVHs).  Triangle boxes as the
+    // device intersects them: v0, v0 + e1, v0 + e2, slightly widened.
+    std::vector<float> boxes(6 * (size_t)g.count);
+    for (unsigned i = 0; i < g.count; i++) {
+        const float4 v0 = tri[3 * (size_t)i], e1 = tri[3 * (size_t)i + 1], e2 = tri[3 * (size_t)i + 2];
+        const float px[3] = {v0.x, v0.x + e1.x, v0.x + e2.x}, py[3] = {v0.y, v0.y + e1.y, v0.y + e2.y},
+                    pz[3] = {v0.z, v0.z + e1.z, v0.z + e2.z};
+        float lo[3] = {std::min({px[0], px[1], px[2]}), std::min({py[0], py[1], py[2]}), std::min({pz[0], pz[1], pz[2]})};
+        float hi[3] = {std::max({px[0], px[1], px[2]}), std::max({py[0], py[1], py[2]}), std::max({pz[0], pz[1], pz[2]})};
+        const float mag = 1e-7f * (std::fabs(lo[0]) + std::fabs(lo[1]) + std::fabs(lo[2]) + 1e-3f);
+        for (int k = 0; k < 3; k++) {
+            const float ext = (hi[k] - lo[k]) * 1e-6f + mag;
+            boxes[6 * (size_t)i + k] = lo[k] - ext;
+            boxes[6 * (size_t)i + 3 + k] = hi[k] + ext;
+        }
     }
+    std::vector<float4> leaf_tri(3 * (size_t)std::max(1u, g.count));
+    if (g.count == 1) {
+        leaf_tri[0] = tri[0];
+        leaf_tri[1] = tri[1];
+        leaf_tri[2] = tri[2];
+    } else if (g.count > 1) {
+        std::vector<uint32_t> order(g.count);
+        std::vector<float> words(16 * (size_t)(g.count - 1));
+        const int threads = (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+        upbp_host::sah_build(boxes.data(), g.count, words.data(), order.data(), threads);
+        for (unsigned k = 0; k < g.count; k++) {
+            const unsigned i = order[k];
+            float4 a = tri[3 * (size_t)i];
+            const int orig = (int)i;  // original triangle index (normals, records)
+            std::memcpy(&a.w, &orig, sizeof(orig));
+            leaf_tri[3 * (size_t)k] = a;
+            leaf_tri[3 * (size_t)k + 1] = tri[3 * (size_t)i + 1];
+            leaf_tri[3 * (size_t)k + 2] = tri[3 * (size_t)i + 2];
+        }
+        static_assert(sizeof(BvhNode) == 16 * sizeof(float), "node layout");
+        UPBP_CK(cudaMemcpy(g.nodes, words.data(), words.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (g.count == 1) leaf_tri[0].w = 0.f;  // original index 0
+    UPBP_CK(dupload(&g.tri, leaf_tri.data(), leaf_tri.size(), c->st));
     UPBP_CK(cudaStreamSynchronize(c->st));
-    cudaFree(unsorted);
     return UPBP_OK;
 }
 
