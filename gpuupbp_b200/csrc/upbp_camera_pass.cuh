@@ -1187,7 +1187,7 @@ UPBP_D void camera_path_end(const CameraLane& c)
 // the next pixel from a global counter instead of idling until the longest
 // path of its warp is done.  Each pixel's random stream depends on the pixel
 // alone, so the assignment of pixels to lanes does not change any path.
-__global__ void __launch_bounds__(128, 4) camera_pass_kernel()
+__global__ void __launch_bounds__(128, 8) camera_pass_kernel()
 {
     begin_kernel(kKernCameraExtend);
     const DeviceParams& p = c_params;
@@ -1225,7 +1225,7 @@ __global__ void __launch_bounds__(128, 4) camera_pass_kernel()
 // Deferred NEE: one light sample per thread -- occlusion ray through the
 // media, MIS weight, throughput.  The contribution is kept per sample until
 // k_resolve_camera knows whether an earlier step of the path failed.
-__global__ void __launch_bounds__(128, 4) nee_connect_kernel()
+__global__ void __launch_bounds__(128, 8) nee_connect_kernel()
 {
     begin_kernel(kKernNee);
     const DeviceParams& p = c_params;
@@ -1277,7 +1277,7 @@ __global__ void __launch_bounds__(128, 4) nee_connect_kernel()
 // Deferred BPT: one (camera vertex, light vertex) pair per thread -- the
 // path-length and media checks of the connection loop, then the connection
 // with its occlusion ray; the contribution is kept per pair like NEE's.
-__global__ void __launch_bounds__(128, 4) bpt_connect_kernel()
+__global__ void __launch_bounds__(128, 8) bpt_connect_kernel()
 {
     begin_kernel(kKernBpt);
     const DeviceParams& p = c_params;

@@ -288,7 +288,7 @@ UPBP_D void light_path_end(const LightLane& l)
 // path ended takes the next path index from a global counter (counters[4]),
 // as the camera pass does with pixels.  Each path's random stream and
 // vertex slots depend on its index alone.
-__global__ void __launch_bounds__(128, 4) light_pass_kernel()
+__global__ void __launch_bounds__(128, 8) light_pass_kernel()
 {
     begin_kernel(kKernLight);
     const DeviceParams& p = c_params;
