@@ -900,7 +900,7 @@ UPBP_D void gather_records(const float4* rec, float4 (&out)[8], float4 (*s)[9], 
 // One warp per 32 consecutive hits; lanes past the end read the warp's
 // first hit's records and evaluate nothing.
 template <int kMode>
-__global__ void __launch_bounds__(128) range_eval_kernel()
+__global__ void __launch_bounds__(128, 7) range_eval_kernel()
 {
     using M = RangeMode<kMode>;
     const DeviceParams& p = c_params;
