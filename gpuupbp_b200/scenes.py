@@ -128,6 +128,7 @@ class SceneBuilder:
     media: list = field(default_factory=list)
     camera: Camera | None = None
     global_medium: str | None = None
+    aux_lights: list = field(default_factory=list)  # AUX light lines (light_point, light_directional, ...)
 
     def add(self, material: str, verts, faces, normals=None):
         self.groups.append((material, np.asarray(verts, np.float64), np.asarray(faces, np.int64),
@@ -199,6 +200,8 @@ class SceneBuilder:
                     fa.write("ior %.6f\n" % m.ior)
             if self.global_medium is not None:
                 fa.write(f"globalMediumId {self.global_medium}\n")
+            for line in self.aux_lights:
+                fa.write(line + "\n")
 
 
 def _box_walls(sb: SceneBuilder, rng: np.random.Generator, lo=-0.5, hi=0.5):
@@ -317,7 +320,18 @@ def dense_beams(seed: int = 5, tiny: bool = False) -> SceneBuilder:
     return sb
 
 
-WORKLOADS = {"box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams}
+def media_field_lights(seed: int = 2, tiny: bool = False) -> SceneBuilder:
+    """The media field with the AUX light types beside its area lights: a
+    point light, a directional light and a constant background."""
+    sb = media_field(seed, tiny)
+    sb.aux_lights += ["light_point 1.5 4.0 3.0 30.0 25.0 20.0",
+                      "light_directional -0.3 -1.0 -0.4 0.8 0.9 1.0",
+                      "light_background_constant 0.15 0.2 0.3"]
+    return sb
+
+
+WORKLOADS = {"box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
+             "media_field_lights": media_field_lights}
 
 
 def write_workload(name: str, out_dir: str, seed: int | None = None, tiny: bool = False) -> str:

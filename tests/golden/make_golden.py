@@ -2,7 +2,10 @@
 parity case rendered by the reference's own render loop compiled for the CPU
 (oracle/_ref/libupbp_ref_cpu.so, built by `make -C oracle`).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
+
+With case names, only those cases are rendered and merged into the existing
+fixtures.
 """
 import json
 import os
@@ -23,9 +26,17 @@ from gpuupbp_b200 import scenes  # noqa: E402
 
 
 def main():
+    only = sys.argv[1:]
     out, meta = {}, {}
+    if only:
+        with np.load(os.path.join(HERE, "oracle_images.npz")) as old:
+            out = {k: old[k] for k in old.files if k.split("/")[0] not in only}
+        with open(os.path.join(HERE, "oracle_counts.json")) as f:
+            meta = {k: v for k, v in json.load(f).items() if k not in only}
     with tempfile.TemporaryDirectory() as tmp:
         for name, (workload, tiny, _, iters) in CASES.items():
+            if only and name not in only:
+                continue
             path = scenes.write_workload(workload, tmp, tiny=tiny)
             r = ref_cpu.RefRenderer(command_line(name, path), threads=0)
             meta[name] = []
