@@ -320,6 +320,26 @@ def dense_beams(seed: int = 5, tiny: bool = False) -> SceneBuilder:
     return sb
 
 
+def glass_box(seed: int = 3, tiny: bool = False) -> SceneBuilder:
+    """The unit box with specular and glossy materials: a real glass sphere
+    (mirror 1, ior 1.5) holding a medium, a Phong back wall, beside the
+    imaginary fog sphere."""
+    rng = np.random.default_rng(seed)
+    sb = box_medium(seed, tiny)
+    sb.groups = [g for g in sb.groups if g[0] != "fog_boundary"]
+    v, f = icosphere(1 if tiny else 3)
+    sb.add("fog_boundary", v * 0.18 + np.array([-0.2, -0.25, -0.15]), f, v)
+    sb.media.append(Medium("smoke", absorption=(0.3, 0.2, 0.1), scattering=(1.5, 1.5, 1.5), g=-0.2))
+    sb.materials.append(Material("glass", real=True, priority=2, medium="smoke", mirror=(1.0, 1.0, 1.0), ior=1.5))
+    sb.add("glass", v * 0.16 + np.array([0.18, -0.2, -0.2]), f, v)
+    gloss = Material("gloss", kd=tuple(float(x) for x in rng.uniform(0.2, 0.4, 3)), ks=(0.4, 0.4, 0.4), ns=40.0)
+    sb.materials.append(gloss)
+    qv, qf = grid_quad(1)
+    p = np.stack([qv[:, 0] * 0.98 - 0.49, qv[:, 1] * 0.98 - 0.49, np.full(len(qv), -0.49)], 1)
+    sb.add("gloss", p, qf, np.repeat(np.array([[0.0, 0.0, 1.0]]), len(p), 0))
+    return sb
+
+
 def media_field_lights(seed: int = 2, tiny: bool = False) -> SceneBuilder:
     """The media field with the AUX light types beside its area lights: a
     point light, a directional light and a constant background."""
@@ -331,7 +351,7 @@ def media_field_lights(seed: int = 2, tiny: bool = False) -> SceneBuilder:
 
 
 WORKLOADS = {"box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
-             "media_field_lights": media_field_lights}
+             "media_field_lights": media_field_lights, "glass_box": glass_box}
 
 
 def write_workload(name: str, out_dir: str, seed: int | None = None, tiny: bool = False) -> str:

@@ -28,6 +28,8 @@ CASES = {
                      ["-a", "upbp_all", "-pbc", "300", "-ioff", "3", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "media_field_tiny": ("media_field", True,
                          ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "12", "-r", "64x36"], 1),
+    "glass_tiny": ("glass_box", True, ["-a", "upbp_all", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "glass_speconly": ("glass_box", True, ["-a", "upbp_all", "-speconly", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "lights_tiny": ("media_field_lights", True,
                     ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "48x32"], 1),
     "dense_beams_tiny": ("dense_beams", True,
