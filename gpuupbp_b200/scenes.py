@@ -340,6 +340,17 @@ def glass_box(seed: int = 3, tiny: bool = False) -> SceneBuilder:
     return sb
 
 
+def fog_box(seed: int = 4, tiny: bool = False) -> SceneBuilder:
+    """The unit box filled with a thin global medium (globalMediumId; the
+    camera starts in it) around the fog sphere, whose medium continues paths
+    with probability 0.7 (continuation_probability)."""
+    sb = box_medium(seed, tiny)
+    sb.media[0].continuation = 0.7
+    sb.media.append(Medium("air", absorption=(0.05, 0.08, 0.1), scattering=(0.3, 0.3, 0.3), g=0.5))
+    sb.global_medium = "air"
+    return sb
+
+
 def media_field_lights(seed: int = 2, tiny: bool = False) -> SceneBuilder:
     """The media field with the AUX light types beside its area lights: a
     point light, a directional light and a constant background."""
@@ -351,7 +362,7 @@ def media_field_lights(seed: int = 2, tiny: bool = False) -> SceneBuilder:
 
 
 WORKLOADS = {"box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
-             "media_field_lights": media_field_lights, "glass_box": glass_box}
+             "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box}
 
 
 def write_workload(name: str, out_dir: str, seed: int | None = None, tiny: bool = False) -> str:
