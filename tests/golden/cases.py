@@ -33,6 +33,7 @@ CASES = {
     "glass_ignorespec": ("glass_box", True, ["-a", "upbp_all", "-ignorespec", "1", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "box_short_beams": ("box_medium", False, ["-a", "upbp_all", "-qbt", "S", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "box_long_beams": ("box_medium", False, ["-a", "upbp_all", "-pbt", "L", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_pcpi": ("box_medium", False, ["-a", "upbp_all", "-pcpi", "500", "-l", "8", "-r", "32x32"] + BOX_R, 2),
     "fog_global": ("fog_box", True, ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "lights_tiny": ("media_field_lights", True,
                     ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "48x32"], 1),
