@@ -230,6 +230,9 @@ def run_b200(args) -> dict | None:
         r.run_iteration(next(its))
     r.stats()  # drain the event ring
 
+    # the step's result is read into page-locked host memory the caller owns
+    result = torch.empty((r.height, r.width, 3), dtype=torch.float32, pin_memory=True).numpy()
+
     def timed(steps: int, readback: bool):
         if pg is not None:
             pg.barrier()
@@ -240,7 +243,7 @@ def run_b200(args) -> dict | None:
         for _ in range(steps):
             r.run_iteration(next(its))
             if readback:
-                r.iteration_image()  # device->host of this step's result
+                r.iteration_image(out=result)  # device->host of this step's result
         t1.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall

@@ -150,9 +150,14 @@ class Renderer:
         _check(load_library().upbp_run_iteration(self._ctx, iteration), f"iteration {iteration}")
         self.iterations += 1
 
-    def iteration_image(self) -> np.ndarray:
-        """The last iteration's image, (H, W, 3) float32."""
-        out = np.empty((self.height, self.width, 3), np.float32)
+    def iteration_image(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The last iteration's image, (H, W, 3) float32: a new array, or
+        `out` (C-contiguous float32 of that shape, e.g. page-locked memory
+        the caller reuses every iteration) filled and returned."""
+        if out is None:
+            out = np.empty((self.height, self.width, 3), np.float32)
+        elif out.dtype != np.float32 or out.shape != (self.height, self.width, 3) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape (H, W, 3)")
         _check(load_library().upbp_read_iteration(self._ctx, out.ctypes.data), "read")
         return out
 
