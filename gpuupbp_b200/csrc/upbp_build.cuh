@@ -228,20 +228,6 @@ __global__ void k_refit(BoxSource s, int n, const unsigned* vals, BvhNode* nodes
     }
 }
 
-// Turns every child subtree of at most leaf_max (<= kLeafMaxCount)
-// primitives into one leaf over its contiguous primitive range.  Runs after
-// the refit, which needs the binary tree; the collapsed subtrees' nodes stay
-// in memory, unreferenced.
-__global__ void k_collapse(int n, BvhNode* nodes, int leaf_max)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
-    int4 k = nodes[i].link;
-    if (k.x >= 0 && k.z <= leaf_max) k.x = leaf_link(k.x - k.z + 1, k.z);
-    if (k.y >= 0 && k.w <= leaf_max) k.y = leaf_link(k.y, k.w);
-    nodes[i].link = k;
-}
-
 // Smallest biased exponent e (1..254) with origin + 255 * 2^(e-127) >= hi
 // in the decoder's arithmetic.
 UPBP_D unsigned qnode_exponent(float origin, float hi)
@@ -388,14 +374,15 @@ struct BuildScratch {
     size_t temp_bytes = 0;
 };
 
-// Builds an LBVH over n boxes from `src` into `nodes` (n-1 entries); on
-// return `sorted_vals` points at the leaf order (primitive index per leaf).
-// With leaf_max > 1 a leaf covers up to leaf_max consecutive primitives.
+// Builds an LBVH over n boxes from `src` into `nodes` (n-1 entries, one
+// primitive per leaf; the children of node i are gamma and gamma + 1, as the
+// compressed nodes require); on return `sorted_vals` points at the leaf order
+// (primitive index per leaf).
 inline cudaError_t build_lbvh(const BoxSource& src, unsigned n, BvhNode* nodes, BuildScratch& sc, cudaStream_t st,
-                              const unsigned** sorted_vals, int leaf_max = 1)
+                              const unsigned** sorted_vals)
 {
     if (n == 0) return cudaSuccess;
-    if (n > kMaxBvhPrimitives || leaf_max > kLeafMaxCount) return cudaErrorInvalidValue;  // leaf-link encoding limits
+    if (n > kMaxBvhPrimitives) return cudaErrorInvalidValue;  // leaf-link encoding limit
     const unsigned init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     cudaError_t e = cudaMemcpyAsync(sc.ord6, init, sizeof(init), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
@@ -414,7 +401,6 @@ inline cudaError_t build_lbvh(const BoxSource& src, unsigned n, BvhNode* nodes, 
         e = cudaMemsetAsync(sc.flags, 0, sizeof(unsigned) * (n - 1), st);
         if (e != cudaSuccess) return e;
         k_refit<<<grid, bs, 0, st>>>(src, (int)n, vb.Current(), nodes, sc.parent_internal, sc.parent_leaf, sc.flags);
-        if (leaf_max > 1) k_collapse<<<(n - 1 + bs - 1) / bs, bs, 0, st>>>((int)n, nodes, leaf_max);
     }
     return cudaGetLastError();
 }

@@ -22,11 +22,6 @@
 using namespace upbp;
 
 constexpr int kEventRing = 64;
-// Leaves of the beam map hold up to kBeamLeafMax chunks.  More chunks per
-// leaf mean fewer node visits (dependent loads) but more pair tests, and a
-// chunk reached through a shared leaf must test its own box before it may
-// report a beam; on the media workload single-chunk leaves are fastest.
-constexpr int kBeamLeafMax = 1;
 // Events per iteration: 0 start, 1 light pass done, 2 photon maps done, 3
 // extend, 4 NEE, 5 BPT + resolve, 6 query sort, 7 SURF, 8 PP3D, 9 BP2D,
 // 10 PB2D, 11 BB1D, 12 iteration done.  Each kernel kind's time is one
@@ -829,10 +824,9 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         src.chunks = c->d_chunks;
         src.dilate = beam_dilate;
         const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order, kBeamLeafMax));
+        UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
         k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
                                                                   P.bb1d_used_light_subpath_count, c->d_beam_seg);
-        static_assert(kBeamLeafMax == 1, "compressed nodes need one-primitive leaves");
         if (nchunks > 1)
             k_quantize<<<(nchunks - 1 + 255) / 256, 256, 0, c->st>>>(c->d_beam_nodes, (int)nchunks - 1,
                                                                      c->d_beam_qnodes);

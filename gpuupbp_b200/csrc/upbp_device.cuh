@@ -84,7 +84,6 @@ struct BvhNode {
 };
 
 constexpr int kLeafShift = 27;
-constexpr int kLeafMaxCount = 16;
 constexpr unsigned kMaxBvhPrimitives = 1u << kLeafShift;
 UPBP_HD int leaf_link(int first, int count) { return ~(first | ((count - 1) << kLeafShift)); }
 UPBP_HD int leaf_first(int link) { return (~link) & ((1 << kLeafShift) - 1); }
