@@ -73,9 +73,10 @@ struct DCamera {
 
 // Two-wide BVH node: both children's boxes + child links.  A link >= 0 is an
 // internal node, a link < 0 is a leaf: ~(first | (count - 1) << 27) for the
-// `count` consecutive primitives (count 1 unless the tree was built with
-// multi-primitive leaves) from position `first` of the sorted order.  z and
-// w count the primitives under the left and right child.
+// `count` consecutive primitives (every tree here is built with one
+// primitive per leaf; the walks accept longer leaves) from position `first`
+// of the sorted order.  z and w count the primitives under the left and right
+// child.
 struct BvhNode {
     float4 a;   // left.lo.xyz, left.hi.x
     float4 b;   // left.hi.yz, right.lo.xy
@@ -143,7 +144,7 @@ struct LightVertexRec {
     float4 q[8];
 };
 
-// Photon beam record: 7 x 16 B.
+// Photon beam record: 8 x 16 B.
 //   q0: origin.xyz, length        q1: direction.xyz, medium id bits
 //   q2: throughput at origin.xyz, ray_sample_for_pdf
 //   q3: ray_sample_rev_pdf, sampling flags bits, path index bits, path length bits
