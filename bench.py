@@ -64,17 +64,23 @@ def measured_peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    """nvidia-smi clock / throttle-reason samples, started before the warm-up
+    (nvidia-smi's start-up stalls the host's CUDA calls for a while on a
+    freshly booted machine) and summarised over the samples taken inside the
+    timed region."""
 
-    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    QUERY = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.lines = []
 
-    def __enter__(self):
+    def start(self):
+        import atexit
+        atexit.register(self.stop)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
@@ -83,8 +89,7 @@ class ClockSampler:
             self.proc = None
         return self
 
-    def __exit__(self, *exc):
-        self.lines = []
+    def stop(self):
         if self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
@@ -94,15 +99,25 @@ class ClockSampler:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
             self.lines = [ln for ln in out.splitlines() if ln.strip()]
-        return False
+            self.proc = None
 
-    def summary(self) -> dict:
+    def summary(self, t0: float | None = None, t1: float | None = None) -> dict:
+        """Median SM clock and active throttle reasons of the samples taken
+        between wall-clock times t0 and t1 (all samples when not given)."""
+        import datetime
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
+        for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
+            if len(parts) < 8:
                 continue
+            try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                ts = None
+            if t0 is not None and ts is not None and not (t0 - 0.25 <= ts <= t1 + 0.25):
+                continue
+            parts = parts[1:]
             try:
                 sm.append(float(parts[0]))
                 mx = float(parts[1])
@@ -224,29 +239,36 @@ def run_b200(args) -> dict | None:
     r = upbp.Renderer(workload_args(scene, args.res, args.workload))
     paths_per_iter = r.config.res_x * r.config.res_y + int(r.config.path_count_per_iter)
     stream = torch.cuda.ExternalStream(r.stream_handle())
-    # rank r renders iterations r, r+N, ...
-    its = iter(range(rank, 10 ** 9, world))
-    for _ in range(args.warmup):
-        r.run_iteration(next(its))
+    # rank r renders iterations r, r+N, ...; the device-timed and the
+    # end-to-end runs render the same iterations (the radius schedule shrinks
+    # with the iteration index, so later iterations are cheaper)
+    clk = ClockSampler(local).start()
+    for k in range(args.warmup):
+        r.run_iteration(rank + world * k)
+    timed_iterations = [rank + world * (args.warmup + k) for k in range(args.steps)]
     r.stats()  # drain the event ring
 
     # the step's result is read into page-locked host memory the caller owns
     result = torch.empty((r.height, r.width, 3), dtype=torch.float32, pin_memory=True).numpy()
 
-    def timed(steps: int, readback: bool):
+    window = []
+
+    def timed(iterations: list, readback: bool):
         if pg is not None:
             pg.barrier()
         torch.cuda.synchronize()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        window.append(time.time())
         t0.record(stream)
         wall = time.perf_counter()
-        for _ in range(steps):
-            r.run_iteration(next(its))
+        for it in iterations:
+            r.run_iteration(it)
             if readback:
                 r.iteration_image(out=result)  # device->host of this step's result
         t1.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall
+        window.append(time.time())
         ms = t0.elapsed_time(t1)
         if pg is not None:
             t = torch.tensor([ms], device="cuda")
@@ -254,10 +276,10 @@ def run_b200(args) -> dict | None:
             ms = float(t.item())
         return ms, wall
 
-    with ClockSampler(local) as clk:
-        ms, wall = timed(args.steps, False)
+    ms, wall = timed(timed_iterations, False)
+    clk.stop()
     st = r.stats()
-    ms_e2e, wall_e2e = timed(args.steps, True)
+    ms_e2e, wall_e2e = timed(timed_iterations, True)
     st_e2e = r.stats()
 
     # final reduction of the accumulated images over ranks (output time, untimed)
@@ -308,7 +330,7 @@ def run_b200(args) -> dict | None:
                      "traffic": traffic, "algorithmic_bytes_per_launch": b_top, "launch_ms": top_ms},
         "iteration_roofline": iteration_roofline,
         "kernels": kernels,
-        "clocks": clk.summary(),
+        "clocks": clk.summary(window[0], window[1]),
         "passes_ms": {"light": st["ms_light_sum"] / max(1, st["timed_iterations"]),
                       "build": st["ms_build_sum"] / max(1, st["timed_iterations"]), "camera": cam_ms},
         "work": st["work"], "queries": {"segment": st["segment_queries"], "point": st["point_queries"],
