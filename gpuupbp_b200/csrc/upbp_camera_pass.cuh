@@ -536,8 +536,9 @@ UPBP_D void splat_camera(unsigned px, float3 c)
 // short one a few, and every accepted neighbour costs a full MIS evaluation;
 // run inside one walk per thread, both leave most lanes of a warp idle.
 //
-// range_search_kernel<kMode>: persistent warps walk a photon map with one
-// query per lane, one internal node per step; a lane whose query is finished
+// range_search_kernel<kMode>: persistent warps walk a photon map's compressed
+// nodes (QNode) with one query per lane, one internal node per step; a lane
+// whose query is finished
 // takes the next one in Morton order from a global counter, so lanes stay
 // busy until the queue is empty.  A child that is a leaf is not visited: its
 // (query, primitive) pair goes into a per-warp ring in shared memory, and
@@ -550,9 +551,10 @@ UPBP_D void splat_camera(unsigned px, float3 c)
 // one stopped.  Pairs past the capacity are dropped but still counted, and
 // such a round is repeated.
 //
-// range_eval_kernel<kMode>: one accepted pair per thread; recomputes the
-// pair's geometry with the same predicate, evaluates the estimator with its
-// MIS weight and adds it into the camera image.
+// range_eval_kernel<kMode>: one accepted pair per thread, the records of a
+// warp's 32 pairs read together (gather_records); recomputes the pair's
+// geometry with the same predicate, evaluates the estimator with its MIS
+// weight and adds it into the camera image.
 enum : int { kModePb2d = 0, kModeBb1d, kModeBp2d, kRangeModes };
 template <int kMode> struct RangeMode {
     static_assert(kMode >= 0 && kMode < kRangeModes, "range-query mode");
