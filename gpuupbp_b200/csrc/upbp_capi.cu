@@ -411,9 +411,11 @@ int ensure_chunks(upbp_ctx* c, unsigned n)
     return UPBP_OK;
 }
 
-// Largest range-query hit list (8 bytes per entry, 17 GB); an iteration
-// with more hits runs its searches in rounds.
-constexpr size_t kMaxHits = size_t(1) << 31;
+// Largest range-query hit list (8 bytes per entry, 34 GB, allocated only
+// when an iteration finds that many pairs); an iteration with more hits runs
+// its searches in rounds, each ending with a drain of the longest queries
+// in flight.  The evaluation's grid-stride index stays below 2^32.
+constexpr size_t kMaxHits = (size_t(1) << 32) - (size_t(1) << 21);
 
 // Room for n range-query hits (n + n/4, within 2^20 .. max_hits).
 int ensure_hits(upbp_ctx* c, size_t n)

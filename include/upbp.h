@@ -200,8 +200,8 @@ const upbp_scene_desc* upbp_scene_get_desc(const upbp_scene* scene);
 void upbp_scene_free(upbp_scene* scene);
 
 /* Replaces: Renderer::init (gpuupbp/renderer/renderer_init.cpp:675-929).
- * The range-query hit list grows with the work up to 2^31 entries (8 bytes
- * each); an iteration with more hits runs its searches in rounds.  The
+ * The range-query hit list grows with the work up to 2^32 - 2^21 entries (8
+ * bytes each); an iteration with more hits runs its searches in rounds.  The
  * environment variable UPBP_MAX_HITS, read here, sets a smaller limit
  * (entries) for hosts with less device memory to spare. */
 int upbp_create(const upbp_scene_desc* scene, const upbp_config* config, upbp_ctx** out);
