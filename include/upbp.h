@@ -203,7 +203,9 @@ void upbp_scene_free(upbp_scene* scene);
  * The range-query hit list grows with the work up to 2^32 - 2^21 entries (8
  * bytes each); an iteration with more hits runs its searches in rounds.  The
  * environment variable UPBP_MAX_HITS, read here, sets a smaller limit
- * (entries) for hosts with less device memory to spare. */
+ * (entries) for hosts with less device memory to spare; it must exceed the
+ * neighbours of any single query, or upbp_run_iteration fails with
+ * UPBP_ERR_CUDA ("range search made no progress"). */
 int upbp_create(const upbp_scene_desc* scene, const upbp_config* config, upbp_ctx** out);
 /* Replaces: Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
  * Renders iteration `iteration` and adds it to the device accumulation. */
