@@ -91,3 +91,27 @@ def test_search_rounds_match_one_round(scene_dir, monkeypatch):
     assert st2["kernel_launches"] > st1["kernel_launches"] + 8
     assert np.allclose(img1, img2, rtol=1e-4, atol=1e-6)
     assert st2["status"] == st1["status"]
+
+
+def test_executable_renders_the_reference_image(scene_dir, tmp_path):
+    """The upbp executable (the reference's main on the C ABI): same command
+    line, iterations accumulated and averaged, EXR written; the image equals
+    the mean of the reference's per-iteration golden images up to half
+    precision and the parity bar."""
+    import subprocess
+
+    from test_host_cpu import read_exr_half
+    gold = np.load(os.path.join(GOLDEN, "oracle_images.npz"))
+    case = "box_tiny_all"
+    workload, tiny, _, iters = CASES[case]
+    path = scenes.write_workload(workload, scene_dir, tiny=tiny)
+    out = tmp_path / "box.exr"
+    exe = os.path.join(ROOT, "gpuupbp_b200", "upbp")
+    r = subprocess.run([exe] + command_line(case, path) + ["-i", str(iters), "-o", str(out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    img = read_exr_half(str(out))
+    ref = np.mean([gold[f"{case}/{it}"] for it in range(iters)], axis=0).astype(np.float16).astype(np.float32)
+    rel = np.abs(img - ref) / (np.abs(ref) + 1e-3)
+    assert float(np.mean(np.all(rel < 2e-3, axis=-1))) >= 0.97
+    assert abs(img.mean() - ref.mean()) / (abs(ref.mean()) + 1e-6) <= 5e-3
