@@ -34,6 +34,13 @@ CASES = {
     "box_short_beams": ("box_medium", False, ["-a", "upbp_all", "-qbt", "S", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "box_long_beams": ("box_medium", False, ["-a", "upbp_all", "-pbt", "L", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "box_pcpi": ("box_medium", False, ["-a", "upbp_all", "-pcpi", "500", "-l", "8", "-r", "32x32"] + BOX_R, 2),
+    "box_shading_normals": ("box_medium", False, ["-a", "upbp_all", "-sn", "-l", "8", "-r", "32x32"] + BOX_R, 1),
+    "box_radii": ("box_medium", False,
+                  ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "32x32",
+                   "-r_initial_surf", "-0.03", "-r_alpha_surf", "0.6", "-r_initial_pp3d", "-0.012",
+                   "-r_alpha_pp3d", "0.8", "-r_initial_pb2d", "-0.015", "-r_alpha_pb2d", "0.7",
+                   "-r_initial_bb1d", "-0.008", "-r_alpha_bb1d", "0.9", "-r_initial_bp2d", "-0.01",
+                   "-r_alpha_bp2d", "0.5"], 3),
     "fog_global": ("fog_box", True, ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "lights_tiny": ("media_field_lights", True,
                     ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "48x32"], 1),
