@@ -63,241 +63,243 @@ void print_usage(const char* prog)
 
 extern "C" int upbp_parse_command_line(int argc, const char** argv, upbp_config* out)
 {
-    if (!out) return UPBP_ERR_ARGS;
-    upbp_config c{};
-    c.scene_id = 0;
-    c.algorithm_flags = UPBP_BPT | UPBP_SURF | UPBP_PP3D | UPBP_PB2D | UPBP_BB1D;
-    c.iteration_count = 1;
-    c.max_time = -1.f;
-    c.res_x = c.res_y = 256;
-    c.max_path_length = 10;
-    c.min_path_length = 0;
-    c.path_count_per_iter = -1.f;
-    c.query_beam_type = UPBP_LONG_BEAM;
-    c.photon_beam_type = UPBP_SHORT_BEAM;
-    c.surf_radius_initial = -0.0015f;
-    c.surf_radius_alpha = 0.75f;
-    c.pp3d_radius_initial = c.pb2d_radius_initial = c.bb1d_radius_initial = c.bp2d_radius_initial = -0.001f;
-    c.pp3d_radius_alpha = c.pb2d_radius_alpha = c.bb1d_radius_alpha = c.bp2d_radius_alpha = 1.f;
-    c.bb1d_used_light_subpath_count = -1.f;
-    c.use_shading_normal = 1;
-    std::ostringstream extra;
-    bool set_alpha[5] = {false, false, false, false, false};  // surf pp3d pb2d bb1d bp2d
-    bool set_init[5] = {false, false, false, false, false};
-    float* alphas[5] = {&c.surf_radius_alpha, &c.pp3d_radius_alpha, &c.pb2d_radius_alpha, &c.bb1d_radius_alpha,
-                        &c.bp2d_radius_alpha};
-    float* inits[5] = {&c.surf_radius_initial, &c.pp3d_radius_initial, &c.pb2d_radius_initial, &c.bb1d_radius_initial,
-                       &c.bp2d_radius_initial};
-    const char* tech_names[5] = {"surf", "pp3d", "pb2d", "bb1d", "bp2d"};
+    return upbp_host::abi_guard([&]() -> int {
+        if (!out) return UPBP_ERR_ARGS;
+        upbp_config c{};
+        c.scene_id = 0;
+        c.algorithm_flags = UPBP_BPT | UPBP_SURF | UPBP_PP3D | UPBP_PB2D | UPBP_BB1D;
+        c.iteration_count = 1;
+        c.max_time = -1.f;
+        c.res_x = c.res_y = 256;
+        c.max_path_length = 10;
+        c.min_path_length = 0;
+        c.path_count_per_iter = -1.f;
+        c.query_beam_type = UPBP_LONG_BEAM;
+        c.photon_beam_type = UPBP_SHORT_BEAM;
+        c.surf_radius_initial = -0.0015f;
+        c.surf_radius_alpha = 0.75f;
+        c.pp3d_radius_initial = c.pb2d_radius_initial = c.bb1d_radius_initial = c.bp2d_radius_initial = -0.001f;
+        c.pp3d_radius_alpha = c.pb2d_radius_alpha = c.bb1d_radius_alpha = c.bp2d_radius_alpha = 1.f;
+        c.bb1d_used_light_subpath_count = -1.f;
+        c.use_shading_normal = 1;
+        std::ostringstream extra;
+        bool set_alpha[5] = {false, false, false, false, false};  // surf pp3d pb2d bb1d bp2d
+        bool set_init[5] = {false, false, false, false, false};
+        float* alphas[5] = {&c.surf_radius_alpha, &c.pp3d_radius_alpha, &c.pb2d_radius_alpha, &c.bb1d_radius_alpha,
+                            &c.bp2d_radius_alpha};
+        float* inits[5] = {&c.surf_radius_initial, &c.pp3d_radius_initial, &c.pb2d_radius_initial, &c.bb1d_radius_initial,
+                           &c.bp2d_radius_initial};
+        const char* tech_names[5] = {"surf", "pp3d", "pb2d", "bb1d", "bp2d"};
 
-    auto fail = [&](const std::string& msg) {
-        std::fprintf(stderr, "%s, please see help (-h)\n", msg.c_str());
-        upbp_host::set_error(msg);
-        return UPBP_ERR_ARGS;
-    };
-
-    for (int i = 1; i < argc; i++) {
-        const std::string a = argv[i];
-        if (a == "-h" || a == "--help" || a == "/?" || a == "-hf" || a == "--help_full" || a == "/??") {
-            print_usage(argv[0]);
-            return UPBP_HELP;
-        }
-        if (a.empty() || a[0] != '-') continue;
-        auto need = [&](const char* opt) -> const char* {
-            if (i + 1 >= argc) return nullptr;
-            (void)opt;
-            return argv[++i];
+        auto fail = [&](const std::string& msg) {
+            std::fprintf(stderr, "%s, please see help (-h)\n", msg.c_str());
+            upbp_host::set_error(msg);
+            return UPBP_ERR_ARGS;
         };
-        if (a == "-s") {
-            const char* v = need("-s");
-            if (!v) return fail("missing argument of -s option");
-            char* end = nullptr;
-            long id = std::strtol(v, &end, 10);
-            if (end == v || id >= 41 || id < -1) return fail("invalid argument of -s option");
-            if (id == 3 || id == 4 || id == 9 || id == 10) return fail("scenes 3, 4, 9, and 10 cannot be rendered with UPBP");
-            c.scene_id = (int)id;
-            if (id == -1) {
-                const char* f = need("-s");
-                if (!f) return fail("missing file name argument of -s option");
-                copy_str(c.scene_path, sizeof(c.scene_path), f);
+
+        for (int i = 1; i < argc; i++) {
+            const std::string a = argv[i];
+            if (a == "-h" || a == "--help" || a == "/?" || a == "-hf" || a == "--help_full" || a == "/??") {
+                print_usage(argv[0]);
+                return UPBP_HELP;
             }
-        } else if (a == "-a") {
-            const char* v = need("-a");
-            if (!v) return fail("missing argument of -a option");
-            const std::string alg = v;
-            if (alg == "upbp_all") {
-                c.algorithm_flags |= UPBP_BPT | UPBP_SURF | UPBP_PP3D | UPBP_PB2D | UPBP_BB1D;
-            } else if (alg.size() >= 8 && alg.compare(0, 4, "upbp") == 0 && (alg[4] == '+' || alg[4] == '_')) {
-                c.algorithm_flags = 0;
-                if (alg[4] == '+') c.algorithm_flags |= UPBP_BPT | UPBP_SURF;
-                std::stringstream ss(alg.substr(5));
-                std::string t;
-                while (std::getline(ss, t, '+')) {
-                    if (t == "bpt") c.algorithm_flags |= UPBP_BPT;
-                    else if (t == "surf") c.algorithm_flags |= UPBP_SURF;
-                    else if (t == "pp3d") c.algorithm_flags |= UPBP_PP3D;
-                    else if (t == "pb2d") c.algorithm_flags |= UPBP_PB2D;
-                    else if (t == "bb1d") c.algorithm_flags |= UPBP_BB1D;
-                    else if (t == "bp2d") c.algorithm_flags |= UPBP_BP2D;
-                    else return fail("invalid argument of -a option");
+            if (a.empty() || a[0] != '-') continue;
+            auto need = [&](const char* opt) -> const char* {
+                if (i + 1 >= argc) return nullptr;
+                (void)opt;
+                return argv[++i];
+            };
+            if (a == "-s") {
+                const char* v = need("-s");
+                if (!v) return fail("missing argument of -s option");
+                char* end = nullptr;
+                long id = std::strtol(v, &end, 10);
+                if (end == v || id >= 41 || id < -1) return fail("invalid argument of -s option");
+                if (id == 3 || id == 4 || id == 9 || id == 10) return fail("scenes 3, 4, 9, and 10 cannot be rendered with UPBP");
+                c.scene_id = (int)id;
+                if (id == -1) {
+                    const char* f = need("-s");
+                    if (!f) return fail("missing file name argument of -s option");
+                    copy_str(c.scene_path, sizeof(c.scene_path), f);
                 }
-            }
-        } else if (a == "-l") {
-            const char* v = need("-l");
-            if (!v) return fail("missing argument of -l option");
-            char* end = nullptr;
-            long l = std::strtol(v, &end, 10);
-            if (end == v || l < 1) return fail("invalid argument of -l option");
-            c.max_path_length = (uint32_t)l;
-        } else if (a == "-t") {
-            const char* v = need("-t");
-            if (!v) return fail("missing argument of -t option");
-            char* end = nullptr;
-            double t = std::strtod(v, &end);
-            if (end == v || t < 0) return fail("invalid argument of -t option");
-            c.max_time = (float)t;
-            extra << "_t" << v;
-        } else if (a == "-i") {
-            const char* v = need("-i");
-            if (!v) return fail("missing argument of -i option");
-            char* end = nullptr;
-            long n = std::strtol(v, &end, 10);
-            if (end == v || n < 1) return fail("invalid argument of -i option");
-            c.iteration_count = (int)n;
-        } else if (a == "-o") {
-            const char* v = need("-o");
-            if (!v || !*v) return fail("invalid argument of -o option");
-            copy_str(c.output_name, sizeof(c.output_name), v);
-        } else if (a == "-r") {
-            const char* v = need("-r");
-            if (!v) return fail("missing argument of -r option");
-            int w = -1, h = -1;
-            std::sscanf(v, "%dx%d", &w, &h);
-            if (w <= 0 || h <= 0) return fail("invalid argument of -r option");
-            c.res_x = (uint32_t)w;
-            c.res_y = (uint32_t)h;
-            extra << "_r" << v;
-        } else if (a == "-r_alpha" || a == "-r_initial") {
-            const bool is_alpha = a == "-r_alpha";
-            const char* v = need(a.c_str());
-            if (!v) return fail("missing argument of " + a + " option");
-            float x = 0.f;
-            std::sscanf(v, "%f", &x);
-            if (is_alpha ? (x <= 0.f) : (x == 0.f)) return fail("invalid argument of " + a + " option");
-            for (int k = 0; k < 5; k++) {
-                if (is_alpha && !set_alpha[k]) *alphas[k] = x;
-                if (!is_alpha && !set_init[k]) *inits[k] = x;
-            }
-            extra << (is_alpha ? "_ralpha" : "_rinit") << v;
-        } else if (a.compare(0, 9, "-r_alpha_") == 0 || a.compare(0, 11, "-r_initial_") == 0) {
-            const bool is_alpha = a.compare(0, 9, "-r_alpha_") == 0;
-            const std::string tech = a.substr(is_alpha ? 9 : 11);
-            int k = -1;
-            for (int t = 0; t < 5; t++)
-                if (tech == tech_names[t]) k = t;
-            if (k < 0) return fail("invalid option \"" + a + "\"");
-            const char* v = need(a.c_str());
-            if (!v) return fail("missing argument of " + a + " option");
-            float x = 0.f;
-            std::sscanf(v, "%f", &x);
-            if (is_alpha ? (x <= 0.f) : (x == 0.f)) return fail("invalid argument of " + a + " option");
-            if (is_alpha) {
-                *alphas[k] = x;
-                set_alpha[k] = true;
-                extra << "_ralpha" << tech << v;
+            } else if (a == "-a") {
+                const char* v = need("-a");
+                if (!v) return fail("missing argument of -a option");
+                const std::string alg = v;
+                if (alg == "upbp_all") {
+                    c.algorithm_flags |= UPBP_BPT | UPBP_SURF | UPBP_PP3D | UPBP_PB2D | UPBP_BB1D;
+                } else if (alg.size() >= 8 && alg.compare(0, 4, "upbp") == 0 && (alg[4] == '+' || alg[4] == '_')) {
+                    c.algorithm_flags = 0;
+                    if (alg[4] == '+') c.algorithm_flags |= UPBP_BPT | UPBP_SURF;
+                    std::stringstream ss(alg.substr(5));
+                    std::string t;
+                    while (std::getline(ss, t, '+')) {
+                        if (t == "bpt") c.algorithm_flags |= UPBP_BPT;
+                        else if (t == "surf") c.algorithm_flags |= UPBP_SURF;
+                        else if (t == "pp3d") c.algorithm_flags |= UPBP_PP3D;
+                        else if (t == "pb2d") c.algorithm_flags |= UPBP_PB2D;
+                        else if (t == "bb1d") c.algorithm_flags |= UPBP_BB1D;
+                        else if (t == "bp2d") c.algorithm_flags |= UPBP_BP2D;
+                        else return fail("invalid argument of -a option");
+                    }
+                }
+            } else if (a == "-l") {
+                const char* v = need("-l");
+                if (!v) return fail("missing argument of -l option");
+                char* end = nullptr;
+                long l = std::strtol(v, &end, 10);
+                if (end == v || l < 1) return fail("invalid argument of -l option");
+                c.max_path_length = (uint32_t)l;
+            } else if (a == "-t") {
+                const char* v = need("-t");
+                if (!v) return fail("missing argument of -t option");
+                char* end = nullptr;
+                double t = std::strtod(v, &end);
+                if (end == v || t < 0) return fail("invalid argument of -t option");
+                c.max_time = (float)t;
+                extra << "_t" << v;
+            } else if (a == "-i") {
+                const char* v = need("-i");
+                if (!v) return fail("missing argument of -i option");
+                char* end = nullptr;
+                long n = std::strtol(v, &end, 10);
+                if (end == v || n < 1) return fail("invalid argument of -i option");
+                c.iteration_count = (int)n;
+            } else if (a == "-o") {
+                const char* v = need("-o");
+                if (!v || !*v) return fail("invalid argument of -o option");
+                copy_str(c.output_name, sizeof(c.output_name), v);
+            } else if (a == "-r") {
+                const char* v = need("-r");
+                if (!v) return fail("missing argument of -r option");
+                int w = -1, h = -1;
+                std::sscanf(v, "%dx%d", &w, &h);
+                if (w <= 0 || h <= 0) return fail("invalid argument of -r option");
+                c.res_x = (uint32_t)w;
+                c.res_y = (uint32_t)h;
+                extra << "_r" << v;
+            } else if (a == "-r_alpha" || a == "-r_initial") {
+                const bool is_alpha = a == "-r_alpha";
+                const char* v = need(a.c_str());
+                if (!v) return fail("missing argument of " + a + " option");
+                float x = 0.f;
+                std::sscanf(v, "%f", &x);
+                if (is_alpha ? (x <= 0.f) : (x == 0.f)) return fail("invalid argument of " + a + " option");
+                for (int k = 0; k < 5; k++) {
+                    if (is_alpha && !set_alpha[k]) *alphas[k] = x;
+                    if (!is_alpha && !set_init[k]) *inits[k] = x;
+                }
+                extra << (is_alpha ? "_ralpha" : "_rinit") << v;
+            } else if (a.compare(0, 9, "-r_alpha_") == 0 || a.compare(0, 11, "-r_initial_") == 0) {
+                const bool is_alpha = a.compare(0, 9, "-r_alpha_") == 0;
+                const std::string tech = a.substr(is_alpha ? 9 : 11);
+                int k = -1;
+                for (int t = 0; t < 5; t++)
+                    if (tech == tech_names[t]) k = t;
+                if (k < 0) return fail("invalid option \"" + a + "\"");
+                const char* v = need(a.c_str());
+                if (!v) return fail("missing argument of " + a + " option");
+                float x = 0.f;
+                std::sscanf(v, "%f", &x);
+                if (is_alpha ? (x <= 0.f) : (x == 0.f)) return fail("invalid argument of " + a + " option");
+                if (is_alpha) {
+                    *alphas[k] = x;
+                    set_alpha[k] = true;
+                    extra << "_ralpha" << tech << v;
+                } else {
+                    *inits[k] = x;
+                    set_init[k] = true;
+                    extra << "_rinit" << tech << v;
+                }
+            } else if (a == "-previous") {
+                c.algorithm_flags |= UPBP_PREVIOUS;
+                extra << "_prev";
+            } else if (a == "-compatible") {
+                c.algorithm_flags |= UPBP_COMPATIBLE;
+                extra << "_comp";
+            } else if (a == "-speconly") {
+                c.algorithm_flags |= UPBP_SPECULAR_ONLY;
+                extra << "_speconly";
+            } else if (a == "-ignorespec") {
+                const char* v = need("-ignorespec");
+                if (!v) return fail("missing argument of -ignorespec option");
+                if (std::string(v) == "1") c.ignore_fully_spec_paths = 1;
+                else if (std::string(v) == "0") c.ignore_fully_spec_paths = 0;
+                else return fail("invalid argument of -ignorespec option");
+            } else if (a == "-qbt" || a == "-pbt") {
+                const char* v = need(a.c_str());
+                if (!v) return fail("missing argument of " + a + " option");
+                const int t = (v[0] == 'L' || v[0] == 'l') ? UPBP_LONG_BEAM : UPBP_SHORT_BEAM;
+                if (a == "-qbt") c.query_beam_type = t;
+                else c.photon_beam_type = t;
+            } else if (a == "-pbc") {
+                const char* v = need("-pbc");
+                if (!v) return fail("missing argument of -pbc option");
+                float x = 0.f;
+                std::sscanf(v, "%f", &x);
+                if (x == 0.f) return fail("invalid argument of -pbc option");
+                c.bb1d_used_light_subpath_count = x;
+                extra << "_pbc" << v;
+            } else if (a == "-continuous_output") {
+                const char* v = need(a.c_str());
+                if (!v) return fail("missing argument of -continuous_output option");
+                char* end = nullptr;
+                long n = std::strtol(v, &end, 10);
+                if (end == v) return fail("invalid argument of -continuous_output option");
+                c.continuous_output = (int)n;
+            } else if (a == "-pcpi") {
+                const char* v = need("-pcpi");
+                if (!v) return fail("missing argument of -pcpi option");
+                float x = 0.f;
+                std::sscanf(v, "%f", &x);
+                if (std::floor(x) == 0.f) return fail("invalid argument of -pcpi option");
+                c.path_count_per_iter = x;
+                extra << "_pcpi" << v;
+            } else if (a == "-sn") {
+                const char* v = need("-sn");
+                if (!v) return fail("missing argument of -sn option");
+                int x = 1;
+                std::sscanf(v, "%d", &x);
+                c.use_shading_normal = x == 0 ? 0 : 1;
+                extra << "_sn" << v;
+            } else if (a == "-assert") {
+                c.gpu_assert = 1;
+                extra << "_assert";
+            } else if (a == "-ioff") {
+                const char* v = need("-ioff");
+                if (!v) return fail("missing argument of -ioff option");
+                char* end = nullptr;
+                long long n = std::strtoll(v, &end, 10);
+                if (end == v || n < 0) return fail("invalid argument of -ioff option");
+                c.iteration_offset = (uint64_t)n;
+            } else if (a == "-log") {
+                c.do_log = 1;
+                extra << "_log";
             } else {
-                *inits[k] = x;
-                set_init[k] = true;
-                extra << "_rinit" << tech << v;
+                return fail("invalid option \"" + a + "\"");
             }
-        } else if (a == "-previous") {
-            c.algorithm_flags |= UPBP_PREVIOUS;
-            extra << "_prev";
-        } else if (a == "-compatible") {
-            c.algorithm_flags |= UPBP_COMPATIBLE;
-            extra << "_comp";
-        } else if (a == "-speconly") {
-            c.algorithm_flags |= UPBP_SPECULAR_ONLY;
-            extra << "_speconly";
-        } else if (a == "-ignorespec") {
-            const char* v = need("-ignorespec");
-            if (!v) return fail("missing argument of -ignorespec option");
-            if (std::string(v) == "1") c.ignore_fully_spec_paths = 1;
-            else if (std::string(v) == "0") c.ignore_fully_spec_paths = 0;
-            else return fail("invalid argument of -ignorespec option");
-        } else if (a == "-qbt" || a == "-pbt") {
-            const char* v = need(a.c_str());
-            if (!v) return fail("missing argument of " + a + " option");
-            const int t = (v[0] == 'L' || v[0] == 'l') ? UPBP_LONG_BEAM : UPBP_SHORT_BEAM;
-            if (a == "-qbt") c.query_beam_type = t;
-            else c.photon_beam_type = t;
-        } else if (a == "-pbc") {
-            const char* v = need("-pbc");
-            if (!v) return fail("missing argument of -pbc option");
-            float x = 0.f;
-            std::sscanf(v, "%f", &x);
-            if (x == 0.f) return fail("invalid argument of -pbc option");
-            c.bb1d_used_light_subpath_count = x;
-            extra << "_pbc" << v;
-        } else if (a == "-continuous_output") {
-            const char* v = need(a.c_str());
-            if (!v) return fail("missing argument of -continuous_output option");
-            char* end = nullptr;
-            long n = std::strtol(v, &end, 10);
-            if (end == v) return fail("invalid argument of -continuous_output option");
-            c.continuous_output = (int)n;
-        } else if (a == "-pcpi") {
-            const char* v = need("-pcpi");
-            if (!v) return fail("missing argument of -pcpi option");
-            float x = 0.f;
-            std::sscanf(v, "%f", &x);
-            if (std::floor(x) == 0.f) return fail("invalid argument of -pcpi option");
-            c.path_count_per_iter = x;
-            extra << "_pcpi" << v;
-        } else if (a == "-sn") {
-            const char* v = need("-sn");
-            if (!v) return fail("missing argument of -sn option");
-            int x = 1;
-            std::sscanf(v, "%d", &x);
-            c.use_shading_normal = x == 0 ? 0 : 1;
-            extra << "_sn" << v;
-        } else if (a == "-assert") {
-            c.gpu_assert = 1;
-            extra << "_assert";
-        } else if (a == "-ioff") {
-            const char* v = need("-ioff");
-            if (!v) return fail("missing argument of -ioff option");
-            char* end = nullptr;
-            long long n = std::strtoll(v, &end, 10);
-            if (end == v || n < 0) return fail("invalid argument of -ioff option");
-            c.iteration_offset = (uint64_t)n;
-        } else if (a == "-log") {
-            c.do_log = 1;
-            extra << "_log";
-        } else {
-            return fail("invalid option \"" + a + "\"");
         }
-    }
-    if (c.path_count_per_iter < 0)
-        c.path_count_per_iter = std::floor(-c.path_count_per_iter * (float)c.res_x * (float)c.res_y);
-    else
-        c.path_count_per_iter = std::floor(c.path_count_per_iter);
-    if (c.output_name[0] == 0) {
-        std::string name;
-        if (c.scene_id > -1) {
-            name = "s" + two_digits(c.scene_id);
-        } else {
-            const std::string p = c.scene_path;
-            const size_t sl = p.find_last_of("\\/");
-            const size_t dot = p.find_last_of('.');
-            const size_t b = sl == std::string::npos ? 0 : sl + 1;
-            name = "s-" + p.substr(b, dot == std::string::npos ? std::string::npos : dot - b);
+        if (c.path_count_per_iter < 0)
+            c.path_count_per_iter = std::floor(-c.path_count_per_iter * (float)c.res_x * (float)c.res_y);
+        else
+            c.path_count_per_iter = std::floor(c.path_count_per_iter);
+        if (c.output_name[0] == 0) {
+            std::string name;
+            if (c.scene_id > -1) {
+                name = "s" + two_digits(c.scene_id);
+            } else {
+                const std::string p = c.scene_path;
+                const size_t sl = p.find_last_of("\\/");
+                const size_t dot = p.find_last_of('.');
+                const size_t b = sl == std::string::npos ? 0 : sl + 1;
+                name = "s-" + p.substr(b, dot == std::string::npos ? std::string::npos : dot - b);
+            }
+            copy_str(c.output_name, sizeof(c.output_name), name + default_suffix(c, extra.str()));
         }
-        copy_str(c.output_name, sizeof(c.output_name), name + default_suffix(c, extra.str()));
-    }
-    std::string on = c.output_name;
-    const std::string ext = on.size() > 4 ? on.substr(on.size() - 4) : "";
-    if (ext != ".bmp" && ext != ".exr") copy_str(c.output_name, sizeof(c.output_name), on + ".exr");
-    *out = c;
-    return UPBP_OK;
+        std::string on = c.output_name;
+        const std::string ext = on.size() > 4 ? on.substr(on.size() - 4) : "";
+        if (ext != ".bmp" && ext != ".exr") copy_str(c.output_name, sizeof(c.output_name), on + ".exr");
+        *out = c;
+        return UPBP_OK;
+    });
 }

@@ -74,64 +74,66 @@ void attr(std::vector<uint8_t>& b, const char* name, const char* type, const std
 
 extern "C" int upbp_write_exr(const char* path, const float* rgb, uint32_t w, uint32_t h)
 {
-    if (!path || !rgb || w == 0 || h == 0) return UPBP_ERR_ARGS;
-    std::vector<uint8_t> out;
-    put_u32(out, 20000630u);  // magic
-    put_u32(out, 2u);         // version 2, scanline
-    {
-        std::vector<uint8_t> ch;
-        for (const char* name : {"B", "G", "R"}) {
-            put_str(ch, name);
-            put_i32(ch, 1);  // HALF
-            ch.push_back(0);  // pLinear
+    return upbp_host::abi_guard([&]() -> int {
+        if (!path || !rgb || w == 0 || h == 0) return UPBP_ERR_ARGS;
+        std::vector<uint8_t> out;
+        put_u32(out, 20000630u);  // magic
+        put_u32(out, 2u);         // version 2, scanline
+        {
+            std::vector<uint8_t> ch;
+            for (const char* name : {"B", "G", "R"}) {
+                put_str(ch, name);
+                put_i32(ch, 1);  // HALF
+                ch.push_back(0);  // pLinear
+                ch.push_back(0);
+                ch.push_back(0);
+                ch.push_back(0);
+                put_i32(ch, 1);  // x sampling
+                put_i32(ch, 1);  // y sampling
+            }
             ch.push_back(0);
-            ch.push_back(0);
-            ch.push_back(0);
-            put_i32(ch, 1);  // x sampling
-            put_i32(ch, 1);  // y sampling
+            attr(out, "channels", "chlist", ch);
         }
-        ch.push_back(0);
-        attr(out, "channels", "chlist", ch);
-    }
-    attr(out, "compression", "compression", std::vector<uint8_t>{0});
-    std::vector<uint8_t> box;
-    put_i32(box, 0);
-    put_i32(box, 0);
-    put_i32(box, (int32_t)w - 1);
-    put_i32(box, (int32_t)h - 1);
-    attr(out, "dataWindow", "box2i", box);
-    attr(out, "displayWindow", "box2i", box);
-    attr(out, "lineOrder", "lineOrder", std::vector<uint8_t>{0});
-    std::vector<uint8_t> one;
-    put_f32(one, 1.f);
-    attr(out, "pixelAspectRatio", "float", one);
-    std::vector<uint8_t> center;
-    put_f32(center, 0.f);
-    put_f32(center, 0.f);
-    attr(out, "screenWindowCenter", "v2f", center);
-    attr(out, "screenWindowWidth", "float", one);
-    out.push_back(0);  // end of header
-    const uint32_t row_bytes = w * 3u * 2u;
-    const uint64_t table_pos = out.size();
-    const uint64_t first_block = table_pos + 8ull * h;
-    for (uint32_t y = 0; y < h; y++) put_u64(out, first_block + (uint64_t)y * (8ull + row_bytes));
-    for (uint32_t y = 0; y < h; y++) {
-        put_i32(out, (int32_t)y);
-        put_u32(out, row_bytes);
-        for (int c : {2, 1, 0}) {  // B, G, R
-            for (uint32_t x = 0; x < w; x++) {
-                const uint16_t hv = to_half(rgb[3 * ((size_t)y * w + x) + c]);
-                out.push_back((uint8_t)(hv & 0xff));
-                out.push_back((uint8_t)(hv >> 8));
+        attr(out, "compression", "compression", std::vector<uint8_t>{0});
+        std::vector<uint8_t> box;
+        put_i32(box, 0);
+        put_i32(box, 0);
+        put_i32(box, (int32_t)w - 1);
+        put_i32(box, (int32_t)h - 1);
+        attr(out, "dataWindow", "box2i", box);
+        attr(out, "displayWindow", "box2i", box);
+        attr(out, "lineOrder", "lineOrder", std::vector<uint8_t>{0});
+        std::vector<uint8_t> one;
+        put_f32(one, 1.f);
+        attr(out, "pixelAspectRatio", "float", one);
+        std::vector<uint8_t> center;
+        put_f32(center, 0.f);
+        put_f32(center, 0.f);
+        attr(out, "screenWindowCenter", "v2f", center);
+        attr(out, "screenWindowWidth", "float", one);
+        out.push_back(0);  // end of header
+        const uint32_t row_bytes = w * 3u * 2u;
+        const uint64_t table_pos = out.size();
+        const uint64_t first_block = table_pos + 8ull * h;
+        for (uint32_t y = 0; y < h; y++) put_u64(out, first_block + (uint64_t)y * (8ull + row_bytes));
+        for (uint32_t y = 0; y < h; y++) {
+            put_i32(out, (int32_t)y);
+            put_u32(out, row_bytes);
+            for (int c : {2, 1, 0}) {  // B, G, R
+                for (uint32_t x = 0; x < w; x++) {
+                    const uint16_t hv = to_half(rgb[3 * ((size_t)y * w + x) + c]);
+                    out.push_back((uint8_t)(hv & 0xff));
+                    out.push_back((uint8_t)(hv >> 8));
+                }
             }
         }
-    }
-    FILE* f = std::fopen(path, "wb");
-    if (!f) {
-        upbp_host::set_error(std::string("could not write ") + path);
-        return UPBP_ERR_IO;
-    }
-    const size_t n = std::fwrite(out.data(), 1, out.size(), f);
-    std::fclose(f);
-    return n == out.size() ? UPBP_OK : UPBP_ERR_IO;
+        FILE* f = std::fopen(path, "wb");
+        if (!f) {
+            upbp_host::set_error(std::string("could not write ") + path);
+            return UPBP_ERR_IO;
+        }
+        const size_t n = std::fwrite(out.data(), 1, out.size(), f);
+        std::fclose(f);
+        return n == out.size() ? UPBP_OK : UPBP_ERR_IO;
+    });
 }

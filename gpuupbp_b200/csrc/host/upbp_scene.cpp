@@ -290,157 +290,117 @@ using namespace upbp_host;
 
 extern "C" int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_t res_y, upbp_scene** out)
 {
-    if (!obj_path || !out || res_x == 0 || res_y == 0) return UPBP_ERR_ARGS;
-    const std::string path = obj_path;
-    std::ifstream f(path);
-    if (!f) {
-        set_error("could not open " + path);
-        return UPBP_ERR_IO;
-    }
-    std::vector<float> v, vn;
-    std::vector<ObjMat> mats;
-    std::vector<ObjMed> meds;
-    std::vector<Tri> tris;
-    std::vector<int> group_mat_order;  // material of each usemtl group in order
-    int cur_mat = -1;
-    std::string line;
-    while (std::getline(f, line)) {
-        std::istringstream ss(line);
-        std::string key;
-        if (!(ss >> key) || key[0] == '#') continue;
-        if (key == "v") {
-            float x[3];
-            read3(ss, x);
-            v.insert(v.end(), x, x + 3);
-        } else if (key == "vn") {
-            float x[3];
-            read3(ss, x);
-            vn.insert(vn.end(), x, x + 3);
-        } else if (key == "mtllib") {
-            std::string name;
-            ss >> name;
-            if (!read_mtl(dir_of(path) + name, mats)) return UPBP_ERR_IO;
-        } else if (key == "usemtl") {
-            std::string name;
-            ss >> name;
-            cur_mat = find_mat(mats, name);
-            if (cur_mat < 0) {
-                set_error("material not found: " + name);
-                return UPBP_ERR_SCENE;
-            }
-        } else if (key == "f") {
-            if (cur_mat < 0) {
-                set_error("face before usemtl");
-                return UPBP_ERR_SCENE;
-            }
-            std::vector<std::string> toks;
-            std::string t;
-            while (ss >> t) toks.push_back(t);
-            if (toks.size() < 3) continue;
-            int fv[3], fn[3];
-            const int fmt = parse_fv(toks[0], fv[0], fn[0]);
-            parse_fv(toks[1], fv[1], fn[1]);
-            parse_fv(toks[2], fv[2], fn[2]);
-            const bool has_n = fmt == 2 || fmt == 3;
-            Tri tr;
-            for (int k = 0; k < 3; k++) {
-                tr.v[k] = fv[k] - 1;
-                tr.n[k] = has_n ? fn[k] - 1 : -1;
-            }
-            tr.mat = cur_mat;
-            tris.push_back(tr);
-            for (size_t k = 3; k < toks.size(); k++) {
-                int nv, nn;
-                parse_fv(toks[k], nv, nn);
-                Tri t2;
-                t2.v[0] = tris.back().v[0];
-                t2.n[0] = tris.back().n[0];
-                t2.v[1] = tris.back().v[2];
-                t2.n[1] = tris.back().n[2];
-                t2.v[2] = nv - 1;
-                t2.n[2] = has_n ? nn - 1 : -1;
-                t2.mat = cur_mat;
-                tris.push_back(t2);
-            }
+    return upbp_host::abi_guard([&]() -> int {
+        if (!obj_path || !out || res_x == 0 || res_y == 0) return UPBP_ERR_ARGS;
+        const std::string path = obj_path;
+        std::ifstream f(path);
+        if (!f) {
+            set_error("could not open " + path);
+            return UPBP_ERR_IO;
         }
-    }
-
-    // AUX file
-    std::ifstream fa(path + ".aux");
-    if (!fa) {
-        set_error("could not open " + path + ".aux");
-        return UPBP_ERR_IO;
-    }
-    float tm[4][3] = {{0}};
-    float fov_rad = 0.f, focal = 1.f;
-    int cam_mat = -1;
-    int global_med = -1;
-    std::vector<AuxLight> aux_lights;
-    ObjMat* mat = nullptr;
-    int med = -1;
-    while (std::getline(fa, line)) {
-        std::istringstream ss(line);
-        std::string key;
-        if (!(ss >> key) || key[0] == '#') continue;
-        if (key.compare(0, 6, "TM_ROW") == 0 && key.size() == 7) {
-            const int r = key[6] - '0';
-            if (r >= 0 && r < 4) read3(ss, tm[r]);
-        } else if (key == "CAMERA_FOV") {
-            ss >> fov_rad;
-        } else if (key == "CAMERA_TDIST") {
-            ss >> focal;
-        } else if (key == "CAMERA_MATERIAL") {
-            std::string name;
-            ss >> name;
-            cam_mat = find_mat(mats, name);
-            if (cam_mat < 0) {
-                set_error("material not found: " + name);
-                return UPBP_ERR_SCENE;
-            }
-        } else if (key == "CAMERA_RESOLUTION_X" || key == "CAMERA_RESOLUTION_Y") {
-            // the command line decides the resolution
-        } else if (key == "material") {
-            std::string name;
-            ss >> name;
-            const int m = find_mat(mats, name);
-            if (m < 0) {
-                set_error("material not found: " + name);
-                return UPBP_ERR_SCENE;
-            }
-            mat = &mats[m];
-        } else if (key == "medium") {
-            std::string name;
-            ss >> name;
-            med = find_or_add_med(meds, name);
-        } else if (key == "mediumId" || key == "mirror" || key == "ior" || key == "priority" ||
-                   key == "geometryType" || key == "Ke" || key == "enclosingMatId") {
-            if (!mat) {
-                set_error("using " + key + " option without material selection");
-                return UPBP_ERR_SCENE;
-            }
-            if (key == "mediumId") {
+        std::vector<float> v, vn;
+        std::vector<ObjMat> mats;
+        std::vector<ObjMed> meds;
+        std::vector<Tri> tris;
+        std::vector<int> group_mat_order;  // material of each usemtl group in order
+        int cur_mat = -1;
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream ss(line);
+            std::string key;
+            if (!(ss >> key) || key[0] == '#') continue;
+            if (key == "v") {
+                float x[3];
+                read3(ss, x);
+                v.insert(v.end(), x, x + 3);
+            } else if (key == "vn") {
+                float x[3];
+                read3(ss, x);
+                vn.insert(vn.end(), x, x + 3);
+            } else if (key == "mtllib") {
                 std::string name;
                 ss >> name;
-                mat->medium = find_or_add_med(meds, name);
-            } else if (key == "mirror") {
-                read3(ss, mat->mirror);
-            } else if (key == "ior") {
-                ss >> mat->ior;
-            } else if (key == "priority") {
-                ss >> mat->priority;
-            } else if (key == "geometryType") {
-                std::string g;
-                ss >> g;
-                if (!g.empty() && g[0] == 'r') mat->real = true;
-                else if (!g.empty() && g[0] == 'i') mat->real = false;
-                else {
-                    set_error("unknown geometry type");
+                if (!read_mtl(dir_of(path) + name, mats)) return UPBP_ERR_IO;
+            } else if (key == "usemtl") {
+                std::string name;
+                ss >> name;
+                cur_mat = find_mat(mats, name);
+                if (cur_mat < 0) {
+                    set_error("material not found: " + name);
                     return UPBP_ERR_SCENE;
                 }
-            } else if (key == "Ke") {
-                read3(ss, mat->ke);
-                mat->emissive = mat->ke[0] > 0.f || mat->ke[1] > 0.f || mat->ke[2] > 0.f;
-            } else {
+            } else if (key == "f") {
+                if (cur_mat < 0) {
+                    set_error("face before usemtl");
+                    return UPBP_ERR_SCENE;
+                }
+                std::vector<std::string> toks;
+                std::string t;
+                while (ss >> t) toks.push_back(t);
+                if (toks.size() < 3) continue;
+                int fv[3], fn[3];
+                const int fmt = parse_fv(toks[0], fv[0], fn[0]);
+                parse_fv(toks[1], fv[1], fn[1]);
+                parse_fv(toks[2], fv[2], fn[2]);
+                const bool has_n = fmt == 2 || fmt == 3;
+                Tri tr;
+                for (int k = 0; k < 3; k++) {
+                    tr.v[k] = fv[k] - 1;
+                    tr.n[k] = has_n ? fn[k] - 1 : -1;
+                }
+                tr.mat = cur_mat;
+                tris.push_back(tr);
+                for (size_t k = 3; k < toks.size(); k++) {
+                    int nv, nn;
+                    parse_fv(toks[k], nv, nn);
+                    Tri t2;
+                    t2.v[0] = tris.back().v[0];
+                    t2.n[0] = tris.back().n[0];
+                    t2.v[1] = tris.back().v[2];
+                    t2.n[1] = tris.back().n[2];
+                    t2.v[2] = nv - 1;
+                    t2.n[2] = has_n ? nn - 1 : -1;
+                    t2.mat = cur_mat;
+                    tris.push_back(t2);
+                }
+            }
+        }
+
+        // AUX file
+        std::ifstream fa(path + ".aux");
+        if (!fa) {
+            set_error("could not open " + path + ".aux");
+            return UPBP_ERR_IO;
+        }
+        float tm[4][3] = {{0}};
+        float fov_rad = 0.f, focal = 1.f;
+        int cam_mat = -1;
+        int global_med = -1;
+        std::vector<AuxLight> aux_lights;
+        ObjMat* mat = nullptr;
+        int med = -1;
+        while (std::getline(fa, line)) {
+            std::istringstream ss(line);
+            std::string key;
+            if (!(ss >> key) || key[0] == '#') continue;
+            if (key.compare(0, 6, "TM_ROW") == 0 && key.size() == 7) {
+                const int r = key[6] - '0';
+                if (r >= 0 && r < 4) read3(ss, tm[r]);
+            } else if (key == "CAMERA_FOV") {
+                ss >> fov_rad;
+            } else if (key == "CAMERA_TDIST") {
+                ss >> focal;
+            } else if (key == "CAMERA_MATERIAL") {
+                std::string name;
+                ss >> name;
+                cam_mat = find_mat(mats, name);
+                if (cam_mat < 0) {
+                    set_error("material not found: " + name);
+                    return UPBP_ERR_SCENE;
+                }
+            } else if (key == "CAMERA_RESOLUTION_X" || key == "CAMERA_RESOLUTION_Y") {
+                // the command line decides the resolution
+            } else if (key == "material") {
                 std::string name;
                 ss >> name;
                 const int m = find_mat(mats, name);
@@ -448,198 +408,242 @@ extern "C" int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_
                     set_error("material not found: " + name);
                     return UPBP_ERR_SCENE;
                 }
-                mat->enclosing = m;
-            }
-        } else if (key == "g" || key == "absorption" || key == "scattering" || key == "emission" ||
-                   key == "continuation_probability") {
-            if (med < 0) {
-                set_error("using " + key + " option without medium selection");
-                return UPBP_ERR_SCENE;
-            }
-            ObjMed& m = meds[med];
-            if (key == "g") ss >> m.g;
-            else if (key == "absorption") read3(ss, m.absorption);
-            else if (key == "scattering") read3(ss, m.scattering);
-            else if (key == "emission") read3(ss, m.emission);
-            else ss >> m.cont;
-        } else if (key == "globalMediumId") {
-            std::string name;
-            ss >> name;
-            global_med = find_or_add_med(meds, name);
-        } else if (key == "light_point" || key == "light_directional") {
-            AuxLight l;
-            l.type = key == "light_point" ? UPBP_LIGHT_POINT : UPBP_LIGHT_DIRECTIONAL;
-            read3(ss, l.pos);
-            read3(ss, l.emission);
-            aux_lights.push_back(l);
-        } else if (key == "light_background_constant") {
-            AuxLight l;
-            l.type = UPBP_LIGHT_BACKGROUND;
-            read3(ss, l.emission);
-            aux_lights.push_back(l);
-        } else if (key == "light_background_em") {
-            set_error("environment-map background lights are not supported");
-            return UPBP_ERR_SCENE;
-        }
-    }
-
-    upbp_scene* sc = new upbp_scene();
-    sc->desc.background_light = -1;
-    // lights from the AUX file first
-    for (const AuxLight& al : aux_lights) {
-        upbp_light L{};
-        L.type = al.type;
-        L.mat_id = L.med_id = -1;
-        L.scale = 1.f;
-        std::memcpy(L.intensity, al.emission, sizeof(L.intensity));
-        std::memcpy(L.position, al.pos, sizeof(L.position));
-        if (al.type == UPBP_LIGHT_BACKGROUND) {
-            if (sc->desc.background_light < 0) sc->desc.background_light = (int32_t)sc->lights.size();
-        }
-        sc->lights.push_back(L);
-    }
-    // triangles (file order), one area light per emissive triangle
-    const size_t nt = tris.size();
-    sc->verts.resize(9 * nt);
-    sc->normals.resize(12 * nt);
-    sc->tri_material.resize(nt);
-    sc->tri_light.resize(nt);
-    float bmin[3] = {1e36f, 1e36f, 1e36f}, bmax[3] = {-1e36f, -1e36f, -1e36f};
-    for (size_t k = 0; k < nt; k++) {
-        const Tri& t = tris[k];
-        F3 p[3];
-        for (int j = 0; j < 3; j++) {
-            const int vi = t.v[j];
-            if (vi < 0 || 3 * (size_t)vi + 2 >= v.size()) {
-                delete sc;
-                set_error("face references a missing vertex");
-                return UPBP_ERR_SCENE;
-            }
-            p[j] = {v[3 * vi], v[3 * vi + 1], v[3 * vi + 2]};
-            sc->verts[9 * k + 3 * j + 0] = p[j].x;
-            sc->verts[9 * k + 3 * j + 1] = p[j].y;
-            sc->verts[9 * k + 3 * j + 2] = p[j].z;
-            const float* q = &p[j].x;
-            for (int a = 0; a < 3; a++) {
-                bmin[a] = std::fmin(bmin[a], q[a]);
-                bmax[a] = std::fmax(bmax[a], q[a]);
-            }
-        }
-        F3 face = fnormalize(fcross(fsub(p[1], p[0]), fsub(p[2], p[0])));
-        F3 n[3];
-        if (t.n[0] >= 0 && t.n[1] >= 0 && t.n[2] >= 0) {
-            for (int j = 0; j < 3; j++) {
-                const int ni = t.n[j];
-                if (3 * (size_t)ni + 2 >= vn.size()) {
-                    delete sc;
-                    set_error("face references a missing normal");
+                mat = &mats[m];
+            } else if (key == "medium") {
+                std::string name;
+                ss >> name;
+                med = find_or_add_med(meds, name);
+            } else if (key == "mediumId" || key == "mirror" || key == "ior" || key == "priority" ||
+                       key == "geometryType" || key == "Ke" || key == "enclosingMatId") {
+                if (!mat) {
+                    set_error("using " + key + " option without material selection");
                     return UPBP_ERR_SCENE;
                 }
-                n[j] = {vn[3 * ni], vn[3 * ni + 1], vn[3 * ni + 2]};
+                if (key == "mediumId") {
+                    std::string name;
+                    ss >> name;
+                    mat->medium = find_or_add_med(meds, name);
+                } else if (key == "mirror") {
+                    read3(ss, mat->mirror);
+                } else if (key == "ior") {
+                    ss >> mat->ior;
+                } else if (key == "priority") {
+                    ss >> mat->priority;
+                } else if (key == "geometryType") {
+                    std::string g;
+                    ss >> g;
+                    if (!g.empty() && g[0] == 'r') mat->real = true;
+                    else if (!g.empty() && g[0] == 'i') mat->real = false;
+                    else {
+                        set_error("unknown geometry type");
+                        return UPBP_ERR_SCENE;
+                    }
+                } else if (key == "Ke") {
+                    read3(ss, mat->ke);
+                    mat->emissive = mat->ke[0] > 0.f || mat->ke[1] > 0.f || mat->ke[2] > 0.f;
+                } else {
+                    std::string name;
+                    ss >> name;
+                    const int m = find_mat(mats, name);
+                    if (m < 0) {
+                        set_error("material not found: " + name);
+                        return UPBP_ERR_SCENE;
+                    }
+                    mat->enclosing = m;
+                }
+            } else if (key == "g" || key == "absorption" || key == "scattering" || key == "emission" ||
+                       key == "continuation_probability") {
+                if (med < 0) {
+                    set_error("using " + key + " option without medium selection");
+                    return UPBP_ERR_SCENE;
+                }
+                ObjMed& m = meds[med];
+                if (key == "g") ss >> m.g;
+                else if (key == "absorption") read3(ss, m.absorption);
+                else if (key == "scattering") read3(ss, m.scattering);
+                else if (key == "emission") read3(ss, m.emission);
+                else ss >> m.cont;
+            } else if (key == "globalMediumId") {
+                std::string name;
+                ss >> name;
+                global_med = find_or_add_med(meds, name);
+            } else if (key == "light_point" || key == "light_directional") {
+                AuxLight l;
+                l.type = key == "light_point" ? UPBP_LIGHT_POINT : UPBP_LIGHT_DIRECTIONAL;
+                read3(ss, l.pos);
+                read3(ss, l.emission);
+                aux_lights.push_back(l);
+            } else if (key == "light_background_constant") {
+                AuxLight l;
+                l.type = UPBP_LIGHT_BACKGROUND;
+                read3(ss, l.emission);
+                aux_lights.push_back(l);
+            } else if (key == "light_background_em") {
+                set_error("environment-map background lights are not supported");
+                return UPBP_ERR_SCENE;
             }
-            const F3 mdl{(n[0].x + n[1].x + n[2].x) / 3.f, (n[0].y + n[1].y + n[2].y) / 3.f,
-                         (n[0].z + n[1].z + n[2].z) / 3.f};
-            if (fdot(face, mdl) < 0.f) face = fneg(face);
-        } else {
-            n[0] = n[1] = n[2] = face;
         }
-        for (int j = 0; j < 3; j++) {
-            sc->normals[12 * k + 3 * j + 0] = n[j].x;
-            sc->normals[12 * k + 3 * j + 1] = n[j].y;
-            sc->normals[12 * k + 3 * j + 2] = n[j].z;
-        }
-        sc->normals[12 * k + 9] = face.x;
-        sc->normals[12 * k + 10] = face.y;
-        sc->normals[12 * k + 11] = face.z;
-        sc->tri_material[k] = t.mat;
-        sc->tri_light[k] = -1;
-        const ObjMat& m = mats[t.mat];
-        if (m.emissive) {
+
+        upbp_scene* sc = new upbp_scene();
+        sc->desc.background_light = -1;
+        // lights from the AUX file first
+        for (const AuxLight& al : aux_lights) {
             upbp_light L{};
-            L.type = UPBP_LIGHT_AREA;
-            L.mat_id = m.enclosing < 0 ? -1 : m.enclosing;
-            L.med_id = L.mat_id < 0 ? -1 : mats[L.mat_id].medium;
-            for (int a = 0; a < 3; a++) {
-                L.p0[a] = (&p[0].x)[a];
-                L.p1[a] = (&p[1].x)[a];
-                L.p2[a] = (&p[2].x)[a];
-                L.intensity[a] = m.ke[a];
-            }
+            L.type = al.type;
+            L.mat_id = L.med_id = -1;
             L.scale = 1.f;
-            sc->tri_light[k] = (int32_t)sc->lights.size();
+            std::memcpy(L.intensity, al.emission, sizeof(L.intensity));
+            std::memcpy(L.position, al.pos, sizeof(L.position));
+            if (al.type == UPBP_LIGHT_BACKGROUND) {
+                if (sc->desc.background_light < 0) sc->desc.background_light = (int32_t)sc->lights.size();
+            }
             sc->lights.push_back(L);
         }
-    }
-    // materials
-    for (const ObjMat& m : mats) {
-        upbp_material M{};
-        std::memcpy(M.diffuse, m.kd, sizeof(M.diffuse));
-        std::memcpy(M.phong, m.ks, sizeof(M.phong));
-        std::memcpy(M.mirror, m.mirror, sizeof(M.mirror));
-        M.ior = m.ior;
-        M.phong_exponent = m.ns;
-        M.priority = m.priority;
-        M.real = m.real ? 1 : 0;
-        if (m.ns == 0.f) M.phong[0] = M.phong[1] = M.phong[2] = 0.f;
-        M.medium = m.medium;
-        sc->materials.push_back(M);
-    }
-    // media; continuation probability from albedo unless given
-    for (const ObjMed& m : meds) {
-        upbp_medium M{};
-        std::memcpy(M.absorption, m.absorption, sizeof(M.absorption));
-        std::memcpy(M.emission, m.emission, sizeof(M.emission));
-        std::memcpy(M.scattering, m.scattering, sizeof(M.scattering));
-        M.mean_cosine = m.g;
-        float cp = m.cont;
-        if (cp == -1.f) {
-            float al[3];
-            for (int a = 0; a < 3; a++) al[a] = m.scattering[a] / (m.scattering[a] + m.absorption[a]);
-            const float mx = std::fmax(al[0], std::fmax(al[1], al[2]));
-            if (std::isnan(mx) || std::isinf(mx)) cp = 1.f;
-            else cp = mx > .8f ? mx : .8f;
+        // triangles (file order), one area light per emissive triangle
+        const size_t nt = tris.size();
+        sc->verts.resize(9 * nt);
+        sc->normals.resize(12 * nt);
+        sc->tri_material.resize(nt);
+        sc->tri_light.resize(nt);
+        float bmin[3] = {1e36f, 1e36f, 1e36f}, bmax[3] = {-1e36f, -1e36f, -1e36f};
+        for (size_t k = 0; k < nt; k++) {
+            const Tri& t = tris[k];
+            F3 p[3];
+            for (int j = 0; j < 3; j++) {
+                const int vi = t.v[j];
+                if (vi < 0 || 3 * (size_t)vi + 2 >= v.size()) {
+                    delete sc;
+                    set_error("face references a missing vertex");
+                    return UPBP_ERR_SCENE;
+                }
+                p[j] = {v[3 * vi], v[3 * vi + 1], v[3 * vi + 2]};
+                sc->verts[9 * k + 3 * j + 0] = p[j].x;
+                sc->verts[9 * k + 3 * j + 1] = p[j].y;
+                sc->verts[9 * k + 3 * j + 2] = p[j].z;
+                const float* q = &p[j].x;
+                for (int a = 0; a < 3; a++) {
+                    bmin[a] = std::fmin(bmin[a], q[a]);
+                    bmax[a] = std::fmax(bmax[a], q[a]);
+                }
+            }
+            F3 face = fnormalize(fcross(fsub(p[1], p[0]), fsub(p[2], p[0])));
+            F3 n[3];
+            if (t.n[0] >= 0 && t.n[1] >= 0 && t.n[2] >= 0) {
+                for (int j = 0; j < 3; j++) {
+                    const int ni = t.n[j];
+                    if (3 * (size_t)ni + 2 >= vn.size()) {
+                        delete sc;
+                        set_error("face references a missing normal");
+                        return UPBP_ERR_SCENE;
+                    }
+                    n[j] = {vn[3 * ni], vn[3 * ni + 1], vn[3 * ni + 2]};
+                }
+                const F3 mdl{(n[0].x + n[1].x + n[2].x) / 3.f, (n[0].y + n[1].y + n[2].y) / 3.f,
+                             (n[0].z + n[1].z + n[2].z) / 3.f};
+                if (fdot(face, mdl) < 0.f) face = fneg(face);
+            } else {
+                n[0] = n[1] = n[2] = face;
+            }
+            for (int j = 0; j < 3; j++) {
+                sc->normals[12 * k + 3 * j + 0] = n[j].x;
+                sc->normals[12 * k + 3 * j + 1] = n[j].y;
+                sc->normals[12 * k + 3 * j + 2] = n[j].z;
+            }
+            sc->normals[12 * k + 9] = face.x;
+            sc->normals[12 * k + 10] = face.y;
+            sc->normals[12 * k + 11] = face.z;
+            sc->tri_material[k] = t.mat;
+            sc->tri_light[k] = -1;
+            const ObjMat& m = mats[t.mat];
+            if (m.emissive) {
+                upbp_light L{};
+                L.type = UPBP_LIGHT_AREA;
+                L.mat_id = m.enclosing < 0 ? -1 : m.enclosing;
+                L.med_id = L.mat_id < 0 ? -1 : mats[L.mat_id].medium;
+                for (int a = 0; a < 3; a++) {
+                    L.p0[a] = (&p[0].x)[a];
+                    L.p1[a] = (&p[1].x)[a];
+                    L.p2[a] = (&p[2].x)[a];
+                    L.intensity[a] = m.ke[a];
+                }
+                L.scale = 1.f;
+                sc->tri_light[k] = (int32_t)sc->lights.size();
+                sc->lights.push_back(L);
+            }
         }
-        M.continuation_prob = cp;
-        sc->media.push_back(M);
-    }
-    if (global_med < 0) {
-        upbp_medium M{};
-        M.continuation_prob = 1.f;
-        sc->media.push_back(M);
-        sc->desc.global_medium = (int32_t)sc->media.size() - 1;
-    } else {
-        sc->desc.global_medium = global_med;
-    }
-    // camera (rows: right, up, -forward, position; fill_camera_info)
-    upbp_camera_desc& cd = sc->desc.camera;
-    for (int a = 0; a < 3; a++) {
-        cd.origin[a] = tm[3][a];
-        cd.target[a] = tm[3][a] - tm[2][a];
-        cd.roll[a] = tm[1][a];
-    }
-    const float rl = 1.f / std::sqrt(cd.roll[0] * cd.roll[0] + cd.roll[1] * cd.roll[1] + cd.roll[2] * cd.roll[2]);
-    for (int a = 0; a < 3; a++) cd.roll[a] *= rl;
-    cd.horizontal_fov_deg = fov_rad * 57.295779f;
-    cd.focal_dist = focal;
-    cd.mat_id = cam_mat < 0 ? -1 : cam_mat;
-    cd.med_id = cd.mat_id < 0 ? -1 : mats[cd.mat_id].medium;
-    sc->desc.res_x = res_x;
-    sc->desc.res_y = res_y;
-    for (int a = 0; a < 3; a++) {
-        sc->desc.bbox_min[a] = bmin[a];
-        sc->desc.bbox_max[a] = bmax[a];
-    }
-    sc->finalize();
-    *out = sc;
-    return UPBP_OK;
+        // materials
+        for (const ObjMat& m : mats) {
+            upbp_material M{};
+            std::memcpy(M.diffuse, m.kd, sizeof(M.diffuse));
+            std::memcpy(M.phong, m.ks, sizeof(M.phong));
+            std::memcpy(M.mirror, m.mirror, sizeof(M.mirror));
+            M.ior = m.ior;
+            M.phong_exponent = m.ns;
+            M.priority = m.priority;
+            M.real = m.real ? 1 : 0;
+            if (m.ns == 0.f) M.phong[0] = M.phong[1] = M.phong[2] = 0.f;
+            M.medium = m.medium;
+            sc->materials.push_back(M);
+        }
+        // media; continuation probability from albedo unless given
+        for (const ObjMed& m : meds) {
+            upbp_medium M{};
+            std::memcpy(M.absorption, m.absorption, sizeof(M.absorption));
+            std::memcpy(M.emission, m.emission, sizeof(M.emission));
+            std::memcpy(M.scattering, m.scattering, sizeof(M.scattering));
+            M.mean_cosine = m.g;
+            float cp = m.cont;
+            if (cp == -1.f) {
+                float al[3];
+                for (int a = 0; a < 3; a++) al[a] = m.scattering[a] / (m.scattering[a] + m.absorption[a]);
+                const float mx = std::fmax(al[0], std::fmax(al[1], al[2]));
+                if (std::isnan(mx) || std::isinf(mx)) cp = 1.f;
+                else cp = mx > .8f ? mx : .8f;
+            }
+            M.continuation_prob = cp;
+            sc->media.push_back(M);
+        }
+        if (global_med < 0) {
+            upbp_medium M{};
+            M.continuation_prob = 1.f;
+            sc->media.push_back(M);
+            sc->desc.global_medium = (int32_t)sc->media.size() - 1;
+        } else {
+            sc->desc.global_medium = global_med;
+        }
+        // camera (rows: right, up, -forward, position; fill_camera_info)
+        upbp_camera_desc& cd = sc->desc.camera;
+        for (int a = 0; a < 3; a++) {
+            cd.origin[a] = tm[3][a];
+            cd.target[a] = tm[3][a] - tm[2][a];
+            cd.roll[a] = tm[1][a];
+        }
+        const float rl = 1.f / std::sqrt(cd.roll[0] * cd.roll[0] + cd.roll[1] * cd.roll[1] + cd.roll[2] * cd.roll[2]);
+        for (int a = 0; a < 3; a++) cd.roll[a] *= rl;
+        cd.horizontal_fov_deg = fov_rad * 57.295779f;
+        cd.focal_dist = focal;
+        cd.mat_id = cam_mat < 0 ? -1 : cam_mat;
+        cd.med_id = cd.mat_id < 0 ? -1 : mats[cd.mat_id].medium;
+        sc->desc.res_x = res_x;
+        sc->desc.res_y = res_y;
+        for (int a = 0; a < 3; a++) {
+            sc->desc.bbox_min[a] = bmin[a];
+            sc->desc.bbox_max[a] = bmax[a];
+        }
+        sc->finalize();
+        *out = sc;
+        return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_scene_load_predefined(int scene_id, uint32_t, uint32_t, upbp_scene** out)
 {
-    (void)scene_id;
-    (void)out;
-    set_error("predefined Cornell-box scenes (-s 0..40) are not available in this build; use -s -1 <file.obj>");
-    return UPBP_ERR_ARGS;
+    return upbp_host::abi_guard([&]() -> int {
+        (void)scene_id;
+        (void)out;
+        set_error("predefined Cornell-box scenes (-s 0..40) are not available in this build; use -s -1 <file.obj>");
+        return UPBP_ERR_ARGS;
+    });
 }
 
 extern "C" const upbp_scene_desc* upbp_scene_get_desc(const upbp_scene* scene) { return scene ? &scene->desc : nullptr; }

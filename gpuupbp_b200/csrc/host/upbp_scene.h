@@ -2,6 +2,8 @@
 // the camera set-up shared by the loader and the device context.
 #pragma once
 
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -29,5 +31,25 @@ struct CameraMatrices {
 CameraMatrices camera_setup(const upbp_camera_desc& c, float res_x, float res_y);
 
 void set_error(const std::string& msg);
+
+// Runs the body of a C entry point and turns a C++ exception (a failed host
+// allocation, a thread that could not start) into UPBP_ERR_HOST with its
+// message: no exception crosses the C ABI.
+template <class F>
+int abi_guard(F&& body) noexcept
+{
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        set_error("out of host memory");
+    } catch (const std::exception& e) {
+        try {
+            set_error(std::string("host error: ") + e.what());
+        } catch (...) {
+        }
+    } catch (...) {
+    }
+    return UPBP_ERR_HOST;
+}
 
 }  // namespace upbp_host

@@ -435,754 +435,768 @@ int ensure_hits(upbp_ctx* c, size_t n)
 
 extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upbp_ctx** out)
 {
-    if (!s || !cfg || !out) return UPBP_ERR_ARGS;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        upbp_host::set_error("no CUDA device");
-        return UPBP_ERR_NO_DEVICE;
-    }
-    if (s->material_count == 0 || s->medium_count == 0 || s->global_medium < 0 ||
-        (uint32_t)s->global_medium >= s->medium_count) {
-        upbp_host::set_error("scene has no materials or no valid global medium");
-        return UPBP_ERR_SCENE;
-    }
-    for (uint32_t i = 0; i < s->triangle_count; i++)
-        if (s->tri_material[i] < 0 || (uint32_t)s->tri_material[i] >= s->material_count) {
-            upbp_host::set_error("triangle material index out of range");
+    return upbp_host::abi_guard([&]() -> int {
+        if (!s || !cfg || !out) return UPBP_ERR_ARGS;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            upbp_host::set_error("no CUDA device");
+            return UPBP_ERR_NO_DEVICE;
+        }
+        if (s->material_count == 0 || s->medium_count == 0 || s->global_medium < 0 ||
+            (uint32_t)s->global_medium >= s->medium_count) {
+            upbp_host::set_error("scene has no materials or no valid global medium");
             return UPBP_ERR_SCENE;
         }
-    upbp_ctx* c = new upbp_ctx();
-    c->cfg = *cfg;
-    DeviceParams& P = c->P;
-    UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
-    for (auto& slot : c->ev_ring)
-        for (auto& e : slot) UPBP_CK(cudaEventCreate(&e));
+        for (uint32_t i = 0; i < s->triangle_count; i++)
+            if (s->tri_material[i] < 0 || (uint32_t)s->tri_material[i] >= s->material_count) {
+                upbp_host::set_error("triangle material index out of range");
+                return UPBP_ERR_SCENE;
+            }
+        upbp_ctx* c = new upbp_ctx();
+        c->cfg = *cfg;
+        DeviceParams& P = c->P;
+        UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        for (auto& slot : c->ev_ring)
+            for (auto& e : slot) UPBP_CK(cudaEventCreate(&e));
 
-    // scene records
-    std::vector<DMaterial> mats(s->material_count);
-    for (uint32_t i = 0; i < s->material_count; i++) {
-        const upbp_material& m = s->materials[i];
-        mats[i].diffuse = make_float3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
-        mats[i].phong = make_float3(m.phong[0], m.phong[1], m.phong[2]);
-        mats[i].phong_exponent = m.phong_exponent;
-        mats[i].mirror = make_float3(m.mirror[0], m.mirror[1], m.mirror[2]);
-        mats[i].ior = m.ior;
-        mats[i].priority = m.priority;
-        mats[i].real = m.real;
-        mats[i].medium = m.medium;
-    }
-    std::vector<DMedium> meds(s->medium_count);
-    for (uint32_t i = 0; i < s->medium_count; i++) init_medium(meds[i], s->media[i]);
-    std::vector<DLight> lights(std::max(1u, s->light_count));
-    for (uint32_t i = 0; i < s->light_count; i++) init_light(lights[i], s->lights[i]);
-    UPBP_CK(dupload(&c->d_mat, mats.data(), mats.size(), c->st));
-    UPBP_CK(dupload(&c->d_med, meds.data(), meds.size(), c->st));
-    UPBP_CK(dupload(&c->d_lights, lights.data(), lights.size(), c->st));
-    P.materials = c->d_mat;
-    P.material_count = (int)s->material_count;
-    P.media = c->d_med;
-    P.medium_count = (int)s->medium_count;
-    P.global_medium = s->global_medium;
-    P.lights = c->d_lights;
-    P.light_count = (int)s->light_count;
-    P.background_light = s->background_light;
-
-    // camera and scene sphere (scene_loader.hpp:65-71)
-    const upbp_host::CameraMatrices cm = upbp_host::camera_setup(s->camera, (float)cfg->res_x, (float)cfg->res_y);
-    DCamera& cam = P.camera;
-    cam.origin = make_float3(cm.origin[0], cm.origin[1], cm.origin[2]);
-    cam.direction = make_float3(cm.direction[0], cm.direction[1], cm.direction[2]);
-    cam.res_x = (float)cfg->res_x;
-    cam.res_y = (float)cfg->res_y;
-    std::memcpy(cam.raster_to_world, cm.raster_to_world, sizeof(cam.raster_to_world));
-    std::memcpy(cam.world_to_raster, cm.world_to_raster, sizeof(cam.world_to_raster));
-    cam.image_plane_dist = cm.image_plane_dist;
-    cam.mat_id = s->camera.mat_id;
-    cam.med_id = s->camera.med_id;
-    {
-        const float3 lo = make_float3(s->bbox_min[0], s->bbox_min[1], s->bbox_min[2]);
-        const float3 hi = make_float3(s->bbox_max[0], s->bbox_max[1], s->bbox_max[2]);
-        float r2 = dot(hi - lo, hi - lo);
-        if (r2 == 0.f || r2 > kInfinity) r2 = 1.f;
-        P.scene_center = (hi + lo) * .5f;
-        P.scene_radius = std::sqrt(r2) * .5f;
-        P.inv_radius_sqr = 1.f / (P.scene_radius * P.scene_radius);
-        // largest coordinate magnitude the range queries see (scene and camera)
-        const float3 co = cam.origin;
-        const float mag = std::max(std::max(std::fabs(P.scene_center.x), std::fabs(P.scene_center.y)),
-                                   std::fabs(P.scene_center.z)) + P.scene_radius;
-        const float coord = std::max(mag, std::max(std::max(std::fabs(co.x), std::fabs(co.y)), std::fabs(co.z)));
-        P.cull_eps = 1e-6f * coord;
-        P.beam_cull_eps = 1e-4f * coord;
-    }
-
-    // configuration (renderer_init.cpp:681-925)
-    const uint32_t flags = cfg->algorithm_flags;
-    P.trace_light_paths = flags != 0;
-    P.trace_camera_paths = flags != 0;
-    P.do_bpt = (flags & kBpt) != 0;
-    P.do_bb1d = (flags & kBb1d) != 0;
-    P.do_bp2d = (flags & kBp2d) != 0;
-    P.do_pb2d = (flags & kPb2d) != 0;
-    P.do_pp3d = (flags & kPp3d) != 0;
-    P.do_surf = (flags & kSurf) != 0;
-    if (flags & kSpecularOnly) {
-        P.trace_light_paths = 0;
-        P.trace_camera_paths = 1;
-        P.do_bpt = P.do_bb1d = P.do_bp2d = P.do_pb2d = P.do_pp3d = P.do_surf = 0;
-    }
-    P.connect_to_camera_from_surf = (flags & (kPrevious | kCompatible)) == 0;
-    P.screen_pixel_count = cfg->res_x * cfg->res_y;
-    const unsigned L = (unsigned)cfg->path_count_per_iter;
-    P.light_subpath_count = L;
-    c->bb1d_used = cfg->bb1d_used_light_subpath_count;
-    if (c->bb1d_used < 0.f) c->bb1d_used = std::floor(-c->bb1d_used * (float)L);
-    c->r0[0] = relative_radius(cfg->bb1d_radius_initial, P.scene_radius);
-    c->r0[1] = relative_radius(cfg->bp2d_radius_initial, P.scene_radius);
-    c->r0[2] = relative_radius(cfg->pb2d_radius_initial, P.scene_radius);
-    c->r0[3] = relative_radius(cfg->pp3d_radius_initial, P.scene_radius);
-    c->r0[4] = relative_radius(cfg->surf_radius_initial, P.scene_radius);
-
-    const unsigned slots = cfg->max_path_length > 1 ? cfg->max_path_length - 1 : 1;
-    const unsigned beams_per_path = cfg->max_path_length > 2 ? cfg->max_path_length - 2 : 0;
-    unsigned beam_paths = 0;
-    if (P.do_bb1d) beam_paths = std::max(beam_paths, (unsigned)c->bb1d_used);
-    if (P.do_bp2d) beam_paths = std::max(beam_paths, L);
-    c->vertex_capacity = L * slots;
-    c->beam_capacity = beam_paths * beams_per_path;
-    P.slots_per_path = slots;
-    P.beam_capacity = c->beam_capacity;
-
-    const bool merging = cfg->max_path_length > 1;
-    P.build_bb1d = P.trace_light_paths && merging && P.do_bb1d;
-    P.build_bp2d = P.trace_light_paths && merging && P.do_bp2d;
-    P.build_pb2d = P.trace_light_paths && merging && P.do_pb2d;
-    P.build_pp3d = P.trace_light_paths && merging && P.do_pp3d;
-    P.build_surf = P.trace_light_paths && merging && P.do_surf;
-    P.iteration_offset = cfg->iteration_offset;
-    P.min_path_length = cfg->min_path_length;
-    P.max_path_length = cfg->max_path_length;
-    P.photon_beam_type = cfg->photon_beam_type;
-    P.camera_beam_type = cfg->query_beam_type;
-    P.subpath_count_bpt = float(P.do_bpt);
-    P.subpath_count_bb1d = float(P.do_bb1d) * c->bb1d_used;
-    P.subpath_count_bp2d = float(P.do_bp2d) * L;
-    P.subpath_count_pb2d = float(P.do_pb2d) * L;
-    P.subpath_count_pp3d = float(P.do_pp3d) * L;
-    P.subpath_count_surf = float(P.do_surf) * L;
-    P.ignore_fully_spec_paths = cfg->ignore_fully_spec_paths;
-    P.estimator_techniques = flags;
-    P.bb1d_used_light_subpath_count = (unsigned)c->bb1d_used;
-    P.use_shading_normal = cfg->use_shading_normal;
-    P.res_x = cfg->res_x;
-    P.res_y = cfg->res_y;
-
-    // buffers
-    unsigned n_real = 0, n_imag = 0;
-    for (uint32_t i = 0; i < s->triangle_count; i++) (s->materials[s->tri_material[i]].real ? n_real : n_imag)++;
-    c->triangles = s->triangle_count;
-    if (alloc_scratch(c->sc, std::max({n_real, n_imag, c->vertex_capacity, c->beam_capacity})) != UPBP_OK) {
-        upbp_destroy(c);
-        return UPBP_ERR_CUDA;
-    }
-    if (upload_geometry(c, s, true, c->real) != UPBP_OK || upload_geometry(c, s, false, c->imag) != UPBP_OK) {
-        upbp_destroy(c);
-        return UPBP_ERR_CUDA;
-    }
-    P.real = TriView{BvhView{c->real.nodes, c->real.count}, c->real.tri, c->real.normals, c->real.record};
-    P.imag = TriView{BvhView{c->imag.nodes, c->imag.count}, c->imag.tri, c->imag.normals, c->imag.record};
-    const size_t npx = (size_t)P.screen_pixel_count * 3;
-    UPBP_CK(dalloc(&c->d_vertices, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_path_count, std::max(1u, L)));
-    UPBP_CK(dalloc(&c->d_counters, 8));
-    UPBP_CK(dalloc(&c->d_idx_s, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_idx_m, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_beams, c->beam_capacity));
-    UPBP_CK(dalloc(&c->d_fb, npx));
-    UPBP_CK(dalloc(&c->d_acc, npx));
-    UPBP_CK(dalloc(&c->d_status, 1));
-    UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
-    UPBP_CK(dalloc(&c->d_qcount, 8));
-    UPBP_CK(dalloc(&c->d_hit_state, 1));
-    UPBP_CK(dalloc(&c->d_work_saved, kCtrCount));
-    c->max_hits = kMaxHits;
-    if (const char* e = std::getenv("UPBP_MAX_HITS")) {
-        const long long v = std::atoll(e);
-        if (v > 0) c->max_hits = std::min<size_t>((size_t)v, kMaxHits);
-    }
-    UPBP_CK(dalloc(&c->d_cam_fb, npx));
-    {
-        int dev = 0, sms = 0, per_sm = 0;
-        UPBP_CK(cudaGetDevice(&dev));
-        UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const void* search[kRangeModes] = {(const void*)range_search_kernel<kModePb2d>,
-                                           (const void*)range_search_kernel<kModeBb1d>,
-                                           (const void*)range_search_kernel<kModeBp2d>};
-        for (int m = 0; m < kRangeModes; m++) {
-            UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search[m], 128, 0));
-            c->search_grid[m] = std::max(1, sms * std::max(1, per_sm));
+        // scene records
+        std::vector<DMaterial> mats(s->material_count);
+        for (uint32_t i = 0; i < s->material_count; i++) {
+            const upbp_material& m = s->materials[i];
+            mats[i].diffuse = make_float3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+            mats[i].phong = make_float3(m.phong[0], m.phong[1], m.phong[2]);
+            mats[i].phong_exponent = m.phong_exponent;
+            mats[i].mirror = make_float3(m.mirror[0], m.mirror[1], m.mirror[2]);
+            mats[i].ior = m.ior;
+            mats[i].priority = m.priority;
+            mats[i].real = m.real;
+            mats[i].medium = m.medium;
         }
-        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, camera_pass_kernel, 128, 0));
-        c->camera_grid = std::max(1, sms * std::max(1, per_sm));
-        UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light_pass_kernel, 128, 0));
-        c->light_grid = std::max(1, sms * std::max(1, per_sm));
-    }
-    c->seg_capacity = std::max(1024u, 4 * P.screen_pixel_count);
-    c->pt_capacity = std::max(1024u, 3 * P.screen_pixel_count);
-    UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
-    UPBP_CK(dalloc(&c->d_pt_queue, c->pt_capacity));
-    c->conn_capacity = std::max(1024u, 2 * P.screen_pixel_count);
-    c->nee_capacity = std::max(1024u, 2 * P.screen_pixel_count);
-    c->bpt_capacity = std::max(1024u, 2 * P.screen_pixel_count);
-    UPBP_CK(dalloc(&c->d_conn, c->conn_capacity));
-    UPBP_CK(dalloc(&c->d_nee, c->nee_capacity));
-    UPBP_CK(dalloc(&c->d_bpt, c->bpt_capacity));
-    UPBP_CK(dalloc(&c->d_nee_color, c->nee_capacity));
-    UPBP_CK(dalloc(&c->d_bpt_color, c->bpt_capacity));
-    UPBP_CK(dalloc(&c->d_path_err, P.screen_pixel_count));
-    UPBP_CK(dalloc(&c->d_path_color, P.screen_pixel_count));
-    UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_med_qnodes, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_med_pos, c->vertex_capacity));
-    UPBP_CK(dalloc(&c->d_chunk_counts, c->beam_capacity));
-    UPBP_CK(dalloc(&c->d_chunk_offsets, c->beam_capacity));
-    {
-        size_t bytes = 0;
-        UPBP_CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->d_chunk_counts, c->d_chunk_offsets,
-                                              (int)std::max(1u, c->beam_capacity)));
-        c->scan_temp_bytes = bytes;
-        UPBP_CK(cudaMalloc(&c->d_scan_temp, std::max<size_t>(bytes, 16)));
-    }
-    if (ensure_chunks(c, std::max(1u, c->beam_capacity) * 4) != UPBP_OK) {
-        upbp_destroy(c);
-        return UPBP_ERR_CUDA;
-    }
-    UPBP_CK(cudaMemsetAsync(c->d_acc, 0, npx * sizeof(double), c->st));
-    UPBP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->st));
-    UPBP_CK(cudaMemsetAsync(c->d_path_count, 0, sizeof(unsigned) * std::max(1u, L), c->st));
-    P.vertices = c->d_vertices;
-    P.path_vertex_count = c->d_path_count;
-    P.counters = c->d_counters;
-    P.idx_surface = c->d_idx_s;
-    P.idx_medium = c->d_idx_m;
-    P.beams = c->d_beams;
-    P.framebuffer = c->d_fb;
-    P.status = c->d_status;
-    P.seg_queue = c->d_seg_queue;
-    P.seg_capacity = c->seg_capacity;
-    P.pt_queue = c->d_pt_queue;
-    P.pt_capacity = c->pt_capacity;
-    P.queue_count = c->d_qcount;
-    P.conn_vertices = c->d_conn;
-    P.conn_capacity = c->conn_capacity;
-    P.nee_queue = c->d_nee;
-    P.nee_capacity = c->nee_capacity;
-    P.bpt_pairs = c->d_bpt;
-    P.bpt_capacity = c->bpt_capacity;
-    P.nee_color = c->d_nee_color;
-    P.bpt_color = c->d_bpt_color;
-    P.path_err = c->d_path_err;
-    P.path_color = c->d_path_color;
-    P.hit_state = c->d_hit_state;
-    P.cam_fb = c->d_cam_fb;
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    *out = c;
-    return UPBP_OK;
+        std::vector<DMedium> meds(s->medium_count);
+        for (uint32_t i = 0; i < s->medium_count; i++) init_medium(meds[i], s->media[i]);
+        std::vector<DLight> lights(std::max(1u, s->light_count));
+        for (uint32_t i = 0; i < s->light_count; i++) init_light(lights[i], s->lights[i]);
+        UPBP_CK(dupload(&c->d_mat, mats.data(), mats.size(), c->st));
+        UPBP_CK(dupload(&c->d_med, meds.data(), meds.size(), c->st));
+        UPBP_CK(dupload(&c->d_lights, lights.data(), lights.size(), c->st));
+        P.materials = c->d_mat;
+        P.material_count = (int)s->material_count;
+        P.media = c->d_med;
+        P.medium_count = (int)s->medium_count;
+        P.global_medium = s->global_medium;
+        P.lights = c->d_lights;
+        P.light_count = (int)s->light_count;
+        P.background_light = s->background_light;
+
+        // camera and scene sphere (scene_loader.hpp:65-71)
+        const upbp_host::CameraMatrices cm = upbp_host::camera_setup(s->camera, (float)cfg->res_x, (float)cfg->res_y);
+        DCamera& cam = P.camera;
+        cam.origin = make_float3(cm.origin[0], cm.origin[1], cm.origin[2]);
+        cam.direction = make_float3(cm.direction[0], cm.direction[1], cm.direction[2]);
+        cam.res_x = (float)cfg->res_x;
+        cam.res_y = (float)cfg->res_y;
+        std::memcpy(cam.raster_to_world, cm.raster_to_world, sizeof(cam.raster_to_world));
+        std::memcpy(cam.world_to_raster, cm.world_to_raster, sizeof(cam.world_to_raster));
+        cam.image_plane_dist = cm.image_plane_dist;
+        cam.mat_id = s->camera.mat_id;
+        cam.med_id = s->camera.med_id;
+        {
+            const float3 lo = make_float3(s->bbox_min[0], s->bbox_min[1], s->bbox_min[2]);
+            const float3 hi = make_float3(s->bbox_max[0], s->bbox_max[1], s->bbox_max[2]);
+            float r2 = dot(hi - lo, hi - lo);
+            if (r2 == 0.f || r2 > kInfinity) r2 = 1.f;
+            P.scene_center = (hi + lo) * .5f;
+            P.scene_radius = std::sqrt(r2) * .5f;
+            P.inv_radius_sqr = 1.f / (P.scene_radius * P.scene_radius);
+            // largest coordinate magnitude the range queries see (scene and camera)
+            const float3 co = cam.origin;
+            const float mag = std::max(std::max(std::fabs(P.scene_center.x), std::fabs(P.scene_center.y)),
+                                       std::fabs(P.scene_center.z)) + P.scene_radius;
+            const float coord = std::max(mag, std::max(std::max(std::fabs(co.x), std::fabs(co.y)), std::fabs(co.z)));
+            P.cull_eps = 1e-6f * coord;
+            P.beam_cull_eps = 1e-4f * coord;
+        }
+
+        // configuration (renderer_init.cpp:681-925)
+        const uint32_t flags = cfg->algorithm_flags;
+        P.trace_light_paths = flags != 0;
+        P.trace_camera_paths = flags != 0;
+        P.do_bpt = (flags & kBpt) != 0;
+        P.do_bb1d = (flags & kBb1d) != 0;
+        P.do_bp2d = (flags & kBp2d) != 0;
+        P.do_pb2d = (flags & kPb2d) != 0;
+        P.do_pp3d = (flags & kPp3d) != 0;
+        P.do_surf = (flags & kSurf) != 0;
+        if (flags & kSpecularOnly) {
+            P.trace_light_paths = 0;
+            P.trace_camera_paths = 1;
+            P.do_bpt = P.do_bb1d = P.do_bp2d = P.do_pb2d = P.do_pp3d = P.do_surf = 0;
+        }
+        P.connect_to_camera_from_surf = (flags & (kPrevious | kCompatible)) == 0;
+        P.screen_pixel_count = cfg->res_x * cfg->res_y;
+        const unsigned L = (unsigned)cfg->path_count_per_iter;
+        P.light_subpath_count = L;
+        c->bb1d_used = cfg->bb1d_used_light_subpath_count;
+        if (c->bb1d_used < 0.f) c->bb1d_used = std::floor(-c->bb1d_used * (float)L);
+        c->r0[0] = relative_radius(cfg->bb1d_radius_initial, P.scene_radius);
+        c->r0[1] = relative_radius(cfg->bp2d_radius_initial, P.scene_radius);
+        c->r0[2] = relative_radius(cfg->pb2d_radius_initial, P.scene_radius);
+        c->r0[3] = relative_radius(cfg->pp3d_radius_initial, P.scene_radius);
+        c->r0[4] = relative_radius(cfg->surf_radius_initial, P.scene_radius);
+
+        const unsigned slots = cfg->max_path_length > 1 ? cfg->max_path_length - 1 : 1;
+        const unsigned beams_per_path = cfg->max_path_length > 2 ? cfg->max_path_length - 2 : 0;
+        unsigned beam_paths = 0;
+        if (P.do_bb1d) beam_paths = std::max(beam_paths, (unsigned)c->bb1d_used);
+        if (P.do_bp2d) beam_paths = std::max(beam_paths, L);
+        c->vertex_capacity = L * slots;
+        c->beam_capacity = beam_paths * beams_per_path;
+        P.slots_per_path = slots;
+        P.beam_capacity = c->beam_capacity;
+
+        const bool merging = cfg->max_path_length > 1;
+        P.build_bb1d = P.trace_light_paths && merging && P.do_bb1d;
+        P.build_bp2d = P.trace_light_paths && merging && P.do_bp2d;
+        P.build_pb2d = P.trace_light_paths && merging && P.do_pb2d;
+        P.build_pp3d = P.trace_light_paths && merging && P.do_pp3d;
+        P.build_surf = P.trace_light_paths && merging && P.do_surf;
+        P.iteration_offset = cfg->iteration_offset;
+        P.min_path_length = cfg->min_path_length;
+        P.max_path_length = cfg->max_path_length;
+        P.photon_beam_type = cfg->photon_beam_type;
+        P.camera_beam_type = cfg->query_beam_type;
+        P.subpath_count_bpt = float(P.do_bpt);
+        P.subpath_count_bb1d = float(P.do_bb1d) * c->bb1d_used;
+        P.subpath_count_bp2d = float(P.do_bp2d) * L;
+        P.subpath_count_pb2d = float(P.do_pb2d) * L;
+        P.subpath_count_pp3d = float(P.do_pp3d) * L;
+        P.subpath_count_surf = float(P.do_surf) * L;
+        P.ignore_fully_spec_paths = cfg->ignore_fully_spec_paths;
+        P.estimator_techniques = flags;
+        P.bb1d_used_light_subpath_count = (unsigned)c->bb1d_used;
+        P.use_shading_normal = cfg->use_shading_normal;
+        P.res_x = cfg->res_x;
+        P.res_y = cfg->res_y;
+
+        // buffers
+        unsigned n_real = 0, n_imag = 0;
+        for (uint32_t i = 0; i < s->triangle_count; i++) (s->materials[s->tri_material[i]].real ? n_real : n_imag)++;
+        c->triangles = s->triangle_count;
+        if (alloc_scratch(c->sc, std::max({n_real, n_imag, c->vertex_capacity, c->beam_capacity})) != UPBP_OK) {
+            upbp_destroy(c);
+            return UPBP_ERR_CUDA;
+        }
+        if (upload_geometry(c, s, true, c->real) != UPBP_OK || upload_geometry(c, s, false, c->imag) != UPBP_OK) {
+            upbp_destroy(c);
+            return UPBP_ERR_CUDA;
+        }
+        P.real = TriView{BvhView{c->real.nodes, c->real.count}, c->real.tri, c->real.normals, c->real.record};
+        P.imag = TriView{BvhView{c->imag.nodes, c->imag.count}, c->imag.tri, c->imag.normals, c->imag.record};
+        const size_t npx = (size_t)P.screen_pixel_count * 3;
+        UPBP_CK(dalloc(&c->d_vertices, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_path_count, std::max(1u, L)));
+        UPBP_CK(dalloc(&c->d_counters, 8));
+        UPBP_CK(dalloc(&c->d_idx_s, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_idx_m, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_beams, c->beam_capacity));
+        UPBP_CK(dalloc(&c->d_fb, npx));
+        UPBP_CK(dalloc(&c->d_acc, npx));
+        UPBP_CK(dalloc(&c->d_status, 1));
+        UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
+        UPBP_CK(dalloc(&c->d_qcount, 8));
+        UPBP_CK(dalloc(&c->d_hit_state, 1));
+        UPBP_CK(dalloc(&c->d_work_saved, kCtrCount));
+        c->max_hits = kMaxHits;
+        if (const char* e = std::getenv("UPBP_MAX_HITS")) {
+            const long long v = std::atoll(e);
+            if (v > 0) c->max_hits = std::min<size_t>((size_t)v, kMaxHits);
+        }
+        UPBP_CK(dalloc(&c->d_cam_fb, npx));
+        {
+            int dev = 0, sms = 0, per_sm = 0;
+            UPBP_CK(cudaGetDevice(&dev));
+            UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const void* search[kRangeModes] = {(const void*)range_search_kernel<kModePb2d>,
+                                               (const void*)range_search_kernel<kModeBb1d>,
+                                               (const void*)range_search_kernel<kModeBp2d>};
+            for (int m = 0; m < kRangeModes; m++) {
+                UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search[m], 128, 0));
+                c->search_grid[m] = std::max(1, sms * std::max(1, per_sm));
+            }
+            UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, camera_pass_kernel, 128, 0));
+            c->camera_grid = std::max(1, sms * std::max(1, per_sm));
+            UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light_pass_kernel, 128, 0));
+            c->light_grid = std::max(1, sms * std::max(1, per_sm));
+        }
+        c->seg_capacity = std::max(1024u, 4 * P.screen_pixel_count);
+        c->pt_capacity = std::max(1024u, 3 * P.screen_pixel_count);
+        UPBP_CK(dalloc(&c->d_seg_queue, c->seg_capacity));
+        UPBP_CK(dalloc(&c->d_pt_queue, c->pt_capacity));
+        c->conn_capacity = std::max(1024u, 2 * P.screen_pixel_count);
+        c->nee_capacity = std::max(1024u, 2 * P.screen_pixel_count);
+        c->bpt_capacity = std::max(1024u, 2 * P.screen_pixel_count);
+        UPBP_CK(dalloc(&c->d_conn, c->conn_capacity));
+        UPBP_CK(dalloc(&c->d_nee, c->nee_capacity));
+        UPBP_CK(dalloc(&c->d_bpt, c->bpt_capacity));
+        UPBP_CK(dalloc(&c->d_nee_color, c->nee_capacity));
+        UPBP_CK(dalloc(&c->d_bpt_color, c->bpt_capacity));
+        UPBP_CK(dalloc(&c->d_path_err, P.screen_pixel_count));
+        UPBP_CK(dalloc(&c->d_path_color, P.screen_pixel_count));
+        UPBP_CK(dalloc(&c->d_surf_nodes, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_med_nodes, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_med_qnodes, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_surf_pos, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_med_pos, c->vertex_capacity));
+        UPBP_CK(dalloc(&c->d_chunk_counts, c->beam_capacity));
+        UPBP_CK(dalloc(&c->d_chunk_offsets, c->beam_capacity));
+        {
+            size_t bytes = 0;
+            UPBP_CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->d_chunk_counts, c->d_chunk_offsets,
+                                                  (int)std::max(1u, c->beam_capacity)));
+            c->scan_temp_bytes = bytes;
+            UPBP_CK(cudaMalloc(&c->d_scan_temp, std::max<size_t>(bytes, 16)));
+        }
+        if (ensure_chunks(c, std::max(1u, c->beam_capacity) * 4) != UPBP_OK) {
+            upbp_destroy(c);
+            return UPBP_ERR_CUDA;
+        }
+        UPBP_CK(cudaMemsetAsync(c->d_acc, 0, npx * sizeof(double), c->st));
+        UPBP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->st));
+        UPBP_CK(cudaMemsetAsync(c->d_path_count, 0, sizeof(unsigned) * std::max(1u, L), c->st));
+        P.vertices = c->d_vertices;
+        P.path_vertex_count = c->d_path_count;
+        P.counters = c->d_counters;
+        P.idx_surface = c->d_idx_s;
+        P.idx_medium = c->d_idx_m;
+        P.beams = c->d_beams;
+        P.framebuffer = c->d_fb;
+        P.status = c->d_status;
+        P.seg_queue = c->d_seg_queue;
+        P.seg_capacity = c->seg_capacity;
+        P.pt_queue = c->d_pt_queue;
+        P.pt_capacity = c->pt_capacity;
+        P.queue_count = c->d_qcount;
+        P.conn_vertices = c->d_conn;
+        P.conn_capacity = c->conn_capacity;
+        P.nee_queue = c->d_nee;
+        P.nee_capacity = c->nee_capacity;
+        P.bpt_pairs = c->d_bpt;
+        P.bpt_capacity = c->bpt_capacity;
+        P.nee_color = c->d_nee_color;
+        P.bpt_color = c->d_bpt_color;
+        P.path_err = c->d_path_err;
+        P.path_color = c->d_path_color;
+        P.hit_state = c->d_hit_state;
+        P.cam_fb = c->d_cam_fb;
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        *out = c;
+        return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
 {
-    if (!c || iteration < 0) return UPBP_ERR_ARGS;
-    DeviceParams& P = c->P;
-    const upbp_config& cfg = c->cfg;
-    const unsigned L = P.light_subpath_count;
-    const size_t npx = (size_t)P.screen_pixel_count * 3;
-    cudaEvent_t* ev = c->ev_ring[c->iterations % kEventRing];
-    UPBP_CK(cudaEventRecord(ev[0], c->st));
-    UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
-    UPBP_CK(cudaMemsetAsync(c->d_work, 0, (size_t)kKernCount * kCtrCount * sizeof(unsigned long long), c->st));
-    unsigned launches = 0;
-    size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
-    P.work = c->d_work;
-    {
-        unsigned long long* w = c->d_work;
-        h2d += sizeof(w);
-        UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
-    }
-    unsigned found[4] = {0, 0, 0, 0};
-    if (P.trace_light_paths) {
-        // radius schedule and MIS factors (renderer.cpp:57-119)
-        const float eff = 1.f + (float)iteration;
-        float r_bb1d = c->r0[0] * powf(1.f + (float)iteration * c->bb1d_used / (float)L, cfg.bb1d_radius_alpha - 1.f);
-        r_bb1d = fmaxf(r_bb1d, 1e-7f);
-        float r_bp2d = fmaxf(c->r0[1] * powf(eff, (cfg.bp2d_radius_alpha - 1.f) * .5f), 1e-7f);
-        float r_pb2d = fmaxf(c->r0[2] * powf(eff, (cfg.pb2d_radius_alpha - 1.f) * .5f), 1e-7f);
-        float r_pp3d = fmaxf(c->r0[3] * powf(eff, (cfg.pp3d_radius_alpha - 1.f) * (1.f / 3.f)), 1e-7f);
-        float r_surf = fmaxf(c->r0[4] * powf(eff, (cfg.surf_radius_alpha - 1.f) * .5f), 1e-7f);
-        P.mis_factor_bb1d = .5f * r_bb1d * P.subpath_count_bb1d;
-        P.mis_factor_bp2d = (kPi * (r_bp2d * r_bp2d)) * P.subpath_count_bp2d;
-        P.mis_factor_pb2d = (kPi * (r_pb2d * r_pb2d)) * P.subpath_count_pb2d;
-        P.mis_factor_pp3d = (4.f / 3.f) * (kPi * (r_pp3d * r_pp3d * r_pp3d)) * P.subpath_count_pp3d;
-        P.mis_factor_surf = (kPi * (r_surf * r_surf)) * P.subpath_count_surf;
-        P.bb1d_normalization = 1.f / c->bb1d_used;
-        P.bp2d_normalization = 1.f / (float)L;
-        P.pb2d_normalization = 1.f / (float)L;
-        P.pp3d_normalization = 1.f / P.mis_factor_pp3d;
-        P.surf_normalization = 1.f / P.mis_factor_surf;
-        P.radius_bb1d = r_bb1d;
-        P.radius_bp2d = r_bp2d;
-        P.radius_pb2d = r_pb2d;
-        P.radius_pp3d = r_pp3d;
-        P.radius_surf = r_surf;
-        P.rad_point_med = 0.f;
-        if (P.do_pp3d) P.rad_point_med = std::max(P.rad_point_med, r_pp3d);
-        if (P.do_pb2d) P.rad_point_med = std::max(P.rad_point_med, r_pb2d);
-        P.rad_beam = 0.f;
-        if (P.do_bb1d) P.rad_beam = std::max(P.rad_beam, r_bb1d);
-        if (P.do_bp2d) P.rad_beam = std::max(P.rad_beam, r_bp2d);
-        P.radius_bb1d_2 = r_bb1d * r_bb1d;
-        P.radius_bp2d_2 = r_bp2d * r_bp2d;
-        P.radius_pb2d_2 = r_pb2d * r_pb2d;
-        P.radius_pp3d_2 = r_pp3d * r_pp3d;
-        P.radius_surf_2 = r_surf * r_surf;
-        P.iteration = (unsigned)iteration;
-        // [0] vertices [1] surface [2] medium [3] beams [4] next light path to hand out
-        UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned), c->st));
-        h2d += sizeof(P);
-        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-        if (L > 0) {
-            light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>();
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || iteration < 0) return UPBP_ERR_ARGS;
+        DeviceParams& P = c->P;
+        const upbp_config& cfg = c->cfg;
+        const unsigned L = P.light_subpath_count;
+        const size_t npx = (size_t)P.screen_pixel_count * 3;
+        cudaEvent_t* ev = c->ev_ring[c->iterations % kEventRing];
+        UPBP_CK(cudaEventRecord(ev[0], c->st));
+        UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
+        UPBP_CK(cudaMemsetAsync(c->d_work, 0, (size_t)kKernCount * kCtrCount * sizeof(unsigned long long), c->st));
+        unsigned launches = 0;
+        size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
+        P.work = c->d_work;
+        {
+            unsigned long long* w = c->d_work;
+            h2d += sizeof(w);
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
+        }
+        unsigned found[4] = {0, 0, 0, 0};
+        if (P.trace_light_paths) {
+            // radius schedule and MIS factors (renderer.cpp:57-119)
+            const float eff = 1.f + (float)iteration;
+            float r_bb1d = c->r0[0] * powf(1.f + (float)iteration * c->bb1d_used / (float)L, cfg.bb1d_radius_alpha - 1.f);
+            r_bb1d = fmaxf(r_bb1d, 1e-7f);
+            float r_bp2d = fmaxf(c->r0[1] * powf(eff, (cfg.bp2d_radius_alpha - 1.f) * .5f), 1e-7f);
+            float r_pb2d = fmaxf(c->r0[2] * powf(eff, (cfg.pb2d_radius_alpha - 1.f) * .5f), 1e-7f);
+            float r_pp3d = fmaxf(c->r0[3] * powf(eff, (cfg.pp3d_radius_alpha - 1.f) * (1.f / 3.f)), 1e-7f);
+            float r_surf = fmaxf(c->r0[4] * powf(eff, (cfg.surf_radius_alpha - 1.f) * .5f), 1e-7f);
+            P.mis_factor_bb1d = .5f * r_bb1d * P.subpath_count_bb1d;
+            P.mis_factor_bp2d = (kPi * (r_bp2d * r_bp2d)) * P.subpath_count_bp2d;
+            P.mis_factor_pb2d = (kPi * (r_pb2d * r_pb2d)) * P.subpath_count_pb2d;
+            P.mis_factor_pp3d = (4.f / 3.f) * (kPi * (r_pp3d * r_pp3d * r_pp3d)) * P.subpath_count_pp3d;
+            P.mis_factor_surf = (kPi * (r_surf * r_surf)) * P.subpath_count_surf;
+            P.bb1d_normalization = 1.f / c->bb1d_used;
+            P.bp2d_normalization = 1.f / (float)L;
+            P.pb2d_normalization = 1.f / (float)L;
+            P.pp3d_normalization = 1.f / P.mis_factor_pp3d;
+            P.surf_normalization = 1.f / P.mis_factor_surf;
+            P.radius_bb1d = r_bb1d;
+            P.radius_bp2d = r_bp2d;
+            P.radius_pb2d = r_pb2d;
+            P.radius_pp3d = r_pp3d;
+            P.radius_surf = r_surf;
+            P.rad_point_med = 0.f;
+            if (P.do_pp3d) P.rad_point_med = std::max(P.rad_point_med, r_pp3d);
+            if (P.do_pb2d) P.rad_point_med = std::max(P.rad_point_med, r_pb2d);
+            P.rad_beam = 0.f;
+            if (P.do_bb1d) P.rad_beam = std::max(P.rad_beam, r_bb1d);
+            if (P.do_bp2d) P.rad_beam = std::max(P.rad_beam, r_bp2d);
+            P.radius_bb1d_2 = r_bb1d * r_bb1d;
+            P.radius_bp2d_2 = r_bp2d * r_bp2d;
+            P.radius_pb2d_2 = r_pb2d * r_pb2d;
+            P.radius_pp3d_2 = r_pp3d * r_pp3d;
+            P.radius_surf_2 = r_surf * r_surf;
+            P.iteration = (unsigned)iteration;
+            // [0] vertices [1] surface [2] medium [3] beams [4] next light path to hand out
+            UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned), c->st));
+            h2d += sizeof(P);
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+            if (L > 0) {
+                light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>();
+                launches++;
+            }
+            UPBP_CK(cudaGetLastError());
+            d2h += 4 * sizeof(unsigned);
+            UPBP_CK(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            std::memcpy(found, c->h_counters, sizeof(found));
+            if (found[3] > c->beam_capacity) {
+                // the reference prints the same warning and continues (renderer.cpp:188-195)
+                std::fprintf(stderr, "error: device finds more beams than memory allocated\n");
+            }
+        } else {
+            P.iteration = (unsigned)iteration;
+        }
+        UPBP_CK(cudaEventRecord(ev[1], c->st));
+
+        // photon maps (renderer.cpp:206-307 builds OptiX structures here)
+        const unsigned ns = std::min(found[1], c->vertex_capacity);
+        const unsigned nm = std::min(found[2], c->vertex_capacity);
+        const unsigned nb = std::min(found[3], c->beam_capacity);
+        P.surf_map = PointMap{BvhView{c->d_surf_nodes, 0}, c->d_surf_pos};
+        P.med_map = PointMap{BvhView{c->d_med_nodes, 0, c->d_med_qnodes}, c->d_med_pos};
+        // beam-map boxes: the beam radius (BB1D and BP2D), the box tests' rounding
+        // and the BB1D predicate's t1 error on nearly parallel lines
+        const float beam_dilate = P.rad_beam * 1.0001f + P.beam_cull_eps;
+        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0, c->d_beam_qnodes}, c->d_beam_seg, beam_dilate};
+        if (P.build_surf && ns > 0) {
+            BoxSource src{};
+            src.kind = 1;
+            src.slots = c->d_idx_s;
+            src.vertices = c->d_vertices;
+            src.dilate = P.radius_surf * 1.0001f + P.cull_eps;
+            const unsigned* order = nullptr;
+            UPBP_CK(build_lbvh(src, ns, c->d_surf_nodes, c->sc, c->st, &order));
+            k_gather_points<<<(ns + 255) / 256, 256, 0, c->st>>>(c->d_idx_s, c->d_vertices, order, ns, c->d_surf_pos);
+            launches += (ns > 1 ? 4 : 2) + 1;
+            P.surf_map.bvh.count = ns;
+        }
+        if ((P.build_pb2d || P.build_pp3d) && nm > 0) {
+            BoxSource src{};
+            src.kind = 1;
+            src.slots = c->d_idx_m;
+            src.vertices = c->d_vertices;
+            src.dilate = P.rad_point_med * 1.0001f + P.cull_eps;  // PP3D and PB2D
+            const unsigned* order = nullptr;
+            UPBP_CK(build_lbvh(src, nm, c->d_med_nodes, c->sc, c->st, &order));
+            k_gather_points<<<(nm + 255) / 256, 256, 0, c->st>>>(c->d_idx_m, c->d_vertices, order, nm, c->d_med_pos);
+            if (nm > 1) k_quantize<<<(nm - 1 + 255) / 256, 256, 0, c->st>>>(c->d_med_nodes, (int)nm - 1, c->d_med_qnodes);
+            launches += (nm > 1 ? 5 : 2) + 1;
+            P.med_map.bvh.count = nm;
+        }
+        if ((P.build_bb1d || P.build_bp2d) && nb > 0) {
+            // split beams into chunks of about 6 beam radii, at most 64 per beam
+            const float chunk_len = 6.f * P.rad_beam;
+            k_chunk_counts<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_beams, nb, chunk_len, 64u, c->d_chunk_counts);
+            size_t tb = c->scan_temp_bytes;
+            UPBP_CK(cub::DeviceScan::ExclusiveSum(c->d_scan_temp, tb, c->d_chunk_counts, c->d_chunk_offsets, (int)nb, c->st));
+            unsigned tail[2] = {0, 0};
+            d2h += 2 * sizeof(unsigned);
+            UPBP_CK(cudaMemcpyAsync(&tail[0], c->d_chunk_offsets + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+            UPBP_CK(cudaMemcpyAsync(&tail[1], c->d_chunk_counts + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            const unsigned nchunks = tail[0] + tail[1];
+            if (ensure_chunks(c, nchunks) != UPBP_OK) return UPBP_ERR_CUDA;
+            P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0, c->d_beam_qnodes}, c->d_beam_seg, beam_dilate};
+            k_chunk_expand<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_chunk_counts, c->d_chunk_offsets, nb, c->d_chunks);
+            BoxSource src{};
+            src.kind = 3;
+            src.beams = c->d_beams;
+            src.chunks = c->d_chunks;
+            src.dilate = beam_dilate;
+            const unsigned* order = nullptr;
+            UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
+            k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
+                                                                      P.bb1d_used_light_subpath_count, c->d_beam_seg);
+            if (nchunks > 1)
+                k_quantize<<<(nchunks - 1 + 255) / 256, 256, 0, c->st>>>(c->d_beam_nodes, (int)nchunks - 1,
+                                                                         c->d_beam_qnodes);
+            P.beam_map.bvh.count = nchunks;
+            c->last_chunks = nchunks;
+            launches += 2 + (nchunks > 1 ? 5 : 2) + 1;
+        }
+        UPBP_CK(cudaGetLastError());
+        P.n_surface = found[1];
+        P.n_medium = found[2];
+        P.n_beams = found[3];
+
+        UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
+        UPBP_CK(cudaEventRecord(ev[2], c->st));
+        if (P.trace_camera_paths) {
+            // extend: tracing, emitter hits, NEE and BPT sampling; queues the
+            // range queries and the connections
+            for (int attempt = 0; attempt < 2; attempt++) {
+                // [0] segment queries [1] point queries [2] next pixel to hand out
+                // [3] connection vertices [4] NEE samples [5] BPT pairs
+                UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 6 * sizeof(unsigned), c->st));
+                h2d += sizeof(P);
+                UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+                    UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
+                                        kCtrCount * sizeof(unsigned long long), c->st));
+                camera_pass_kernel<<<std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128), 128, 0,
+                                     c->st>>>();
+                launches++;
+                UPBP_CK(cudaGetLastError());
+                d2h += 6 * sizeof(unsigned);
+                UPBP_CK(cudaMemcpyAsync(c->h_qcount, c->d_qcount, 6 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+                UPBP_CK(cudaStreamSynchronize(c->st));
+                const unsigned* q = c->h_qcount;
+                if (q[0] <= c->seg_capacity && q[1] <= c->pt_capacity && q[3] <= c->conn_capacity &&
+                    q[4] <= c->nee_capacity && q[5] <= c->bpt_capacity)
+                    break;
+                // a queue overflowed: grow it and render the camera pass again (the
+                // pass is a pure function of the iteration, so the rerun is exact)
+                unsigned nee_cap = c->nee_capacity, bpt_cap = c->bpt_capacity;
+                if (grow(&c->d_seg_queue, c->seg_capacity, q[0]) != cudaSuccess ||
+                    grow(&c->d_pt_queue, c->pt_capacity, q[1]) != cudaSuccess ||
+                    grow(&c->d_conn, c->conn_capacity, q[3]) != cudaSuccess ||
+                    grow(&c->d_nee, c->nee_capacity, q[4]) != cudaSuccess ||
+                    grow(&c->d_bpt, c->bpt_capacity, q[5]) != cudaSuccess ||
+                    grow(&c->d_nee_color, nee_cap, q[4]) != cudaSuccess ||
+                    grow(&c->d_bpt_color, bpt_cap, q[5]) != cudaSuccess) {
+                    upbp_host::set_error("camera-pass queue allocation failed");
+                    return UPBP_ERR_CUDA;
+                }
+                P.seg_queue = c->d_seg_queue;
+                P.seg_capacity = c->seg_capacity;
+                P.pt_queue = c->d_pt_queue;
+                P.pt_capacity = c->pt_capacity;
+                P.conn_vertices = c->d_conn;
+                P.conn_capacity = c->conn_capacity;
+                P.nee_queue = c->d_nee;
+                P.nee_capacity = c->nee_capacity;
+                P.bpt_pairs = c->d_bpt;
+                P.bpt_capacity = c->bpt_capacity;
+                P.nee_color = c->d_nee_color;
+                P.bpt_color = c->d_bpt_color;
+                UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
+            }
+        }
+        UPBP_CK(cudaEventRecord(ev[3], c->st));
+        auto grid_for = [](unsigned n) { return std::max(1u, std::min((n + 127) / 128, 148u * 64u)); };
+        // deferred NEE and BPT connections, then the colours of every camera path
+        // whose steps all succeeded (the query kernels below check the same)
+        const unsigned nnee = P.trace_camera_paths ? std::min(c->h_qcount[4], c->nee_capacity) : 0;
+        const unsigned nbpt = P.trace_camera_paths ? std::min(c->h_qcount[5], c->bpt_capacity) : 0;
+        if (P.trace_camera_paths)
+            UPBP_CK(cudaMemsetAsync(c->d_path_err, 0xff, P.screen_pixel_count * sizeof(unsigned), c->st));
+        if (nnee > 0) {
+            nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>();
+            launches++;
+        }
+        UPBP_CK(cudaEventRecord(ev[4], c->st));
+        if (nbpt > 0) {
+            bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>();
+            launches++;
+        }
+        if (P.trace_camera_paths) {
+            k_resolve_camera<<<std::max(1u, std::min((nnee + nbpt + P.screen_pixel_count + 255) / 256, 148u * 32u)), 256, 0,
+                               c->st>>>();
             launches++;
         }
         UPBP_CK(cudaGetLastError());
-        d2h += 4 * sizeof(unsigned);
-        UPBP_CK(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-        UPBP_CK(cudaStreamSynchronize(c->st));
-        std::memcpy(found, c->h_counters, sizeof(found));
-        if (found[3] > c->beam_capacity) {
-            // the reference prints the same warning and continues (renderer.cpp:188-195)
-            std::fprintf(stderr, "error: device finds more beams than memory allocated\n");
-        }
-    } else {
-        P.iteration = (unsigned)iteration;
-    }
-    UPBP_CK(cudaEventRecord(ev[1], c->st));
-
-    // photon maps (renderer.cpp:206-307 builds OptiX structures here)
-    const unsigned ns = std::min(found[1], c->vertex_capacity);
-    const unsigned nm = std::min(found[2], c->vertex_capacity);
-    const unsigned nb = std::min(found[3], c->beam_capacity);
-    P.surf_map = PointMap{BvhView{c->d_surf_nodes, 0}, c->d_surf_pos};
-    P.med_map = PointMap{BvhView{c->d_med_nodes, 0, c->d_med_qnodes}, c->d_med_pos};
-    // beam-map boxes: the beam radius (BB1D and BP2D), the box tests' rounding
-    // and the BB1D predicate's t1 error on nearly parallel lines
-    const float beam_dilate = P.rad_beam * 1.0001f + P.beam_cull_eps;
-    P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0, c->d_beam_qnodes}, c->d_beam_seg, beam_dilate};
-    if (P.build_surf && ns > 0) {
-        BoxSource src{};
-        src.kind = 1;
-        src.slots = c->d_idx_s;
-        src.vertices = c->d_vertices;
-        src.dilate = P.radius_surf * 1.0001f + P.cull_eps;
-        const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, ns, c->d_surf_nodes, c->sc, c->st, &order));
-        k_gather_points<<<(ns + 255) / 256, 256, 0, c->st>>>(c->d_idx_s, c->d_vertices, order, ns, c->d_surf_pos);
-        launches += (ns > 1 ? 4 : 2) + 1;
-        P.surf_map.bvh.count = ns;
-    }
-    if ((P.build_pb2d || P.build_pp3d) && nm > 0) {
-        BoxSource src{};
-        src.kind = 1;
-        src.slots = c->d_idx_m;
-        src.vertices = c->d_vertices;
-        src.dilate = P.rad_point_med * 1.0001f + P.cull_eps;  // PP3D and PB2D
-        const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, nm, c->d_med_nodes, c->sc, c->st, &order));
-        k_gather_points<<<(nm + 255) / 256, 256, 0, c->st>>>(c->d_idx_m, c->d_vertices, order, nm, c->d_med_pos);
-        if (nm > 1) k_quantize<<<(nm - 1 + 255) / 256, 256, 0, c->st>>>(c->d_med_nodes, (int)nm - 1, c->d_med_qnodes);
-        launches += (nm > 1 ? 5 : 2) + 1;
-        P.med_map.bvh.count = nm;
-    }
-    if ((P.build_bb1d || P.build_bp2d) && nb > 0) {
-        // split beams into chunks of about 6 beam radii, at most 64 per beam
-        const float chunk_len = 6.f * P.rad_beam;
-        k_chunk_counts<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_beams, nb, chunk_len, 64u, c->d_chunk_counts);
-        size_t tb = c->scan_temp_bytes;
-        UPBP_CK(cub::DeviceScan::ExclusiveSum(c->d_scan_temp, tb, c->d_chunk_counts, c->d_chunk_offsets, (int)nb, c->st));
-        unsigned tail[2] = {0, 0};
-        d2h += 2 * sizeof(unsigned);
-        UPBP_CK(cudaMemcpyAsync(&tail[0], c->d_chunk_offsets + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-        UPBP_CK(cudaMemcpyAsync(&tail[1], c->d_chunk_counts + nb - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-        UPBP_CK(cudaStreamSynchronize(c->st));
-        const unsigned nchunks = tail[0] + tail[1];
-        if (ensure_chunks(c, nchunks) != UPBP_OK) return UPBP_ERR_CUDA;
-        P.beam_map = BeamMap{BvhView{c->d_beam_nodes, 0, c->d_beam_qnodes}, c->d_beam_seg, beam_dilate};
-        k_chunk_expand<<<(nb + 255) / 256, 256, 0, c->st>>>(c->d_chunk_counts, c->d_chunk_offsets, nb, c->d_chunks);
-        BoxSource src{};
-        src.kind = 3;
-        src.beams = c->d_beams;
-        src.chunks = c->d_chunks;
-        src.dilate = beam_dilate;
-        const unsigned* order = nullptr;
-        UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
-        k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
-                                                                  P.bb1d_used_light_subpath_count, c->d_beam_seg);
-        if (nchunks > 1)
-            k_quantize<<<(nchunks - 1 + 255) / 256, 256, 0, c->st>>>(c->d_beam_nodes, (int)nchunks - 1,
-                                                                     c->d_beam_qnodes);
-        P.beam_map.bvh.count = nchunks;
-        c->last_chunks = nchunks;
-        launches += 2 + (nchunks > 1 ? 5 : 2) + 1;
-    }
-    UPBP_CK(cudaGetLastError());
-    P.n_surface = found[1];
-    P.n_medium = found[2];
-    P.n_beams = found[3];
-
-    UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
-    UPBP_CK(cudaEventRecord(ev[2], c->st));
-    if (P.trace_camera_paths) {
-        // extend: tracing, emitter hits, NEE and BPT sampling; queues the
-        // range queries and the connections
-        for (int attempt = 0; attempt < 2; attempt++) {
-            // [0] segment queries [1] point queries [2] next pixel to hand out
-            // [3] connection vertices [4] NEE samples [5] BPT pairs
-            UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 6 * sizeof(unsigned), c->st));
+        UPBP_CK(cudaEventRecord(ev[5], c->st));
+        const unsigned nseg = std::min(c->h_qcount[0], c->seg_capacity);
+        const unsigned npt = std::min(c->h_qcount[1], c->pt_capacity);
+        const bool run_pb2d = P.trace_camera_paths && P.build_pb2d && P.n_medium > 0 && nseg > 0;
+        const bool run_bb1d = P.trace_camera_paths && P.build_bb1d && P.n_beams > 0 && nseg > 0;
+        const bool run_surf = P.trace_camera_paths && P.build_surf && P.n_surface > 0 && npt > 0;
+        const bool run_pp3d = P.trace_camera_paths && P.build_pp3d && P.n_medium > 0 && npt > 0;
+        const bool run_bp2d = P.trace_camera_paths && P.build_bp2d && P.n_beams > 0 && npt > 0;
+        // Morton order of the query records for coherent traversal
+        {
+            const unsigned* so = nullptr;
+            const unsigned* po = nullptr;
+            if ((run_pb2d || run_bb1d) && sort_queries(c, 0, nseg, &so) != UPBP_OK) return UPBP_ERR_CUDA;
+            if ((run_surf || run_pp3d || run_bp2d) && sort_queries(c, 1, npt, &po) != UPBP_OK) return UPBP_ERR_CUDA;
+            P.seg_order = so;
+            P.pt_order = po;
+            launches += (so ? 1 : 0) + (po ? 1 : 0);
             h2d += sizeof(P);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-                UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
-                                    kCtrCount * sizeof(unsigned long long), c->st));
-            camera_pass_kernel<<<std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128), 128, 0,
-                                 c->st>>>();
-            launches++;
-            UPBP_CK(cudaGetLastError());
-            d2h += 6 * sizeof(unsigned);
-            UPBP_CK(cudaMemcpyAsync(c->h_qcount, c->d_qcount, 6 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-            UPBP_CK(cudaStreamSynchronize(c->st));
-            const unsigned* q = c->h_qcount;
-            if (q[0] <= c->seg_capacity && q[1] <= c->pt_capacity && q[3] <= c->conn_capacity &&
-                q[4] <= c->nee_capacity && q[5] <= c->bpt_capacity)
-                break;
-            // a queue overflowed: grow it and render the camera pass again (the
-            // pass is a pure function of the iteration, so the rerun is exact)
-            unsigned nee_cap = c->nee_capacity, bpt_cap = c->bpt_capacity;
-            if (grow(&c->d_seg_queue, c->seg_capacity, q[0]) != cudaSuccess ||
-                grow(&c->d_pt_queue, c->pt_capacity, q[1]) != cudaSuccess ||
-                grow(&c->d_conn, c->conn_capacity, q[3]) != cudaSuccess ||
-                grow(&c->d_nee, c->nee_capacity, q[4]) != cudaSuccess ||
-                grow(&c->d_bpt, c->bpt_capacity, q[5]) != cudaSuccess ||
-                grow(&c->d_nee_color, nee_cap, q[4]) != cudaSuccess ||
-                grow(&c->d_bpt_color, bpt_cap, q[5]) != cudaSuccess) {
-                upbp_host::set_error("camera-pass queue allocation failed");
-                return UPBP_ERR_CUDA;
-            }
-            P.seg_queue = c->d_seg_queue;
-            P.seg_capacity = c->seg_capacity;
-            P.pt_queue = c->d_pt_queue;
-            P.pt_capacity = c->pt_capacity;
-            P.conn_vertices = c->d_conn;
-            P.conn_capacity = c->conn_capacity;
-            P.nee_queue = c->d_nee;
-            P.nee_capacity = c->nee_capacity;
-            P.bpt_pairs = c->d_bpt;
-            P.bpt_capacity = c->bpt_capacity;
-            P.nee_color = c->d_nee_color;
-            P.bpt_color = c->d_bpt_color;
-            UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
         }
-    }
-    UPBP_CK(cudaEventRecord(ev[3], c->st));
-    auto grid_for = [](unsigned n) { return std::max(1u, std::min((n + 127) / 128, 148u * 64u)); };
-    // deferred NEE and BPT connections, then the colours of every camera path
-    // whose steps all succeeded (the query kernels below check the same)
-    const unsigned nnee = P.trace_camera_paths ? std::min(c->h_qcount[4], c->nee_capacity) : 0;
-    const unsigned nbpt = P.trace_camera_paths ? std::min(c->h_qcount[5], c->bpt_capacity) : 0;
-    if (P.trace_camera_paths)
-        UPBP_CK(cudaMemsetAsync(c->d_path_err, 0xff, P.screen_pixel_count * sizeof(unsigned), c->st));
-    if (nnee > 0) {
-        nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>();
-        launches++;
-    }
-    UPBP_CK(cudaEventRecord(ev[4], c->st));
-    if (nbpt > 0) {
-        bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>();
-        launches++;
-    }
-    if (P.trace_camera_paths) {
-        k_resolve_camera<<<std::max(1u, std::min((nnee + nbpt + P.screen_pixel_count + 255) / 256, 148u * 32u)), 256, 0,
-                           c->st>>>();
-        launches++;
-    }
-    UPBP_CK(cudaGetLastError());
-    UPBP_CK(cudaEventRecord(ev[5], c->st));
-    const unsigned nseg = std::min(c->h_qcount[0], c->seg_capacity);
-    const unsigned npt = std::min(c->h_qcount[1], c->pt_capacity);
-    const bool run_pb2d = P.trace_camera_paths && P.build_pb2d && P.n_medium > 0 && nseg > 0;
-    const bool run_bb1d = P.trace_camera_paths && P.build_bb1d && P.n_beams > 0 && nseg > 0;
-    const bool run_surf = P.trace_camera_paths && P.build_surf && P.n_surface > 0 && npt > 0;
-    const bool run_pp3d = P.trace_camera_paths && P.build_pp3d && P.n_medium > 0 && npt > 0;
-    const bool run_bp2d = P.trace_camera_paths && P.build_bp2d && P.n_beams > 0 && npt > 0;
-    // Morton order of the query records for coherent traversal
-    {
-        const unsigned* so = nullptr;
-        const unsigned* po = nullptr;
-        if ((run_pb2d || run_bb1d) && sort_queries(c, 0, nseg, &so) != UPBP_OK) return UPBP_ERR_CUDA;
-        if ((run_surf || run_pp3d || run_bp2d) && sort_queries(c, 1, npt, &po) != UPBP_OK) return UPBP_ERR_CUDA;
-        P.seg_order = so;
-        P.pt_order = po;
-        launches += (so ? 1 : 0) + (po ? 1 : 0);
-        h2d += sizeof(P);
-        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-    }
-    // The estimators: search (query, neighbour) pairs into the hit list, then
-    // evaluate them, in rounds over the query order.  A round stops handing
-    // out queries when the list is 3/4 full; if the queries in flight then
-    // overflow it, the round is repeated (the search is a pure function of
-    // the queries and the map) with a larger list or a shorter range.  A list
-    // that needed more than one round is grown for the next estimator and
-    // iteration (up to max_hits).
-    auto estimator = [&](int mode, unsigned nq) -> int {
-        static constexpr int kKern[kRangeModes] = {kKernPb2d, kKernBb1d, kKernBp2d};
-        unsigned long long* work = c->d_work + (size_t)kKern[mode] * kCtrCount;
-        const size_t work_bytes = kCtrCount * sizeof(unsigned long long);
-        if (c->hit_capacity == 0 && ensure_hits(c, (size_t)std::max(nseg, npt) * 32) != UPBP_OK) return UPBP_ERR_CUDA;
-        UPBP_CK(cudaMemsetAsync(work, 0, work_bytes, c->st));
-        unsigned long long found = 0;
-        unsigned begin = 0, span = nq;  // span: longest range of a round, halved after an overflow
-        int repeats = 0;
-        while (begin < nq) {
-            const unsigned end = begin + std::min(span, nq - begin);
-            UPBP_CK(cudaMemsetAsync(c->d_hit_state, 0, sizeof(HitState), c->st));
-            UPBP_CK(cudaMemcpyAsync(c->d_work_saved, work, work_bytes, cudaMemcpyDeviceToDevice, c->st));
-            P.hit_qb = c->d_hit_qb;
-            P.hit_capacity = c->hit_capacity;
-            P.hit_soft_limit = c->hit_capacity - c->hit_capacity / 4;
-            P.query_begin = begin;
-            P.query_end = end;
-            h2d += sizeof(P);
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
-            const int g = c->search_grid[mode];
-            switch (mode) {
-            case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(); break;
-            case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(); break;
-            default: range_search_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(); break;
-            }
-            launches++;
-            UPBP_CK(cudaGetLastError());
-            d2h += sizeof(HitState);
-            UPBP_CK(cudaMemcpyAsync(&c->h_hit_state, c->d_hit_state, sizeof(HitState), cudaMemcpyDeviceToHost, c->st));
-            UPBP_CK(cudaStreamSynchronize(c->st));
-            const unsigned long long total = c->h_hit_state.total;
-            const unsigned done = (unsigned)std::min<unsigned long long>(c->h_hit_state.fetched, end - begin);
-            if (total > c->hit_capacity || done == 0) {
-                if (++repeats > 64) {  // repeats of one round
-                    upbp_host::set_error("range search made no progress");
-                    return UPBP_ERR_CUDA;
-                }
-                UPBP_CK(cudaMemcpyAsync(work, c->d_work_saved, work_bytes, cudaMemcpyDeviceToDevice, c->st));
-                if (c->hit_capacity < c->max_hits) {
-                    if (ensure_hits(c, (size_t)std::min<unsigned long long>(total, c->max_hits)) != UPBP_OK)
-                        return UPBP_ERR_CUDA;
-                } else {
-                    span = std::max(1u, std::min(done, end - begin) / 2);
-                }
-                continue;
-            }
-            if (total > 0) {
-                const unsigned g2 = grid_for((unsigned)total);
+        // The estimators: search (query, neighbour) pairs into the hit list, then
+        // evaluate them, in rounds over the query order.  A round stops handing
+        // out queries when the list is 3/4 full; if the queries in flight then
+        // overflow it, the round is repeated (the search is a pure function of
+        // the queries and the map) with a larger list or a shorter range.  A list
+        // that needed more than one round is grown for the next estimator and
+        // iteration (up to max_hits).
+        auto estimator = [&](int mode, unsigned nq) -> int {
+            static constexpr int kKern[kRangeModes] = {kKernPb2d, kKernBb1d, kKernBp2d};
+            unsigned long long* work = c->d_work + (size_t)kKern[mode] * kCtrCount;
+            const size_t work_bytes = kCtrCount * sizeof(unsigned long long);
+            if (c->hit_capacity == 0 && ensure_hits(c, (size_t)std::max(nseg, npt) * 32) != UPBP_OK) return UPBP_ERR_CUDA;
+            UPBP_CK(cudaMemsetAsync(work, 0, work_bytes, c->st));
+            unsigned long long found = 0;
+            unsigned begin = 0, span = nq;  // span: longest range of a round, halved after an overflow
+            int repeats = 0;
+            while (begin < nq) {
+                const unsigned end = begin + std::min(span, nq - begin);
+                UPBP_CK(cudaMemsetAsync(c->d_hit_state, 0, sizeof(HitState), c->st));
+                UPBP_CK(cudaMemcpyAsync(c->d_work_saved, work, work_bytes, cudaMemcpyDeviceToDevice, c->st));
+                P.hit_qb = c->d_hit_qb;
+                P.hit_capacity = c->hit_capacity;
+                P.hit_soft_limit = c->hit_capacity - c->hit_capacity / 4;
+                P.query_begin = begin;
+                P.query_end = end;
+                h2d += sizeof(P);
+                UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+                const int g = c->search_grid[mode];
                 switch (mode) {
-                case kModePb2d: range_eval_kernel<kModePb2d><<<g2, 128, 0, c->st>>>(); break;
-                case kModeBb1d: range_eval_kernel<kModeBb1d><<<g2, 128, 0, c->st>>>(); break;
-                default: range_eval_kernel<kModeBp2d><<<g2, 128, 0, c->st>>>(); break;
+                case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(); break;
+                case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(); break;
+                default: range_search_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(); break;
                 }
                 launches++;
                 UPBP_CK(cudaGetLastError());
+                d2h += sizeof(HitState);
+                UPBP_CK(cudaMemcpyAsync(&c->h_hit_state, c->d_hit_state, sizeof(HitState), cudaMemcpyDeviceToHost, c->st));
+                UPBP_CK(cudaStreamSynchronize(c->st));
+                const unsigned long long total = c->h_hit_state.total;
+                const unsigned done = (unsigned)std::min<unsigned long long>(c->h_hit_state.fetched, end - begin);
+                if (total > c->hit_capacity || done == 0) {
+                    if (++repeats > 64) {  // repeats of one round
+                        upbp_host::set_error("range search made no progress");
+                        return UPBP_ERR_CUDA;
+                    }
+                    UPBP_CK(cudaMemcpyAsync(work, c->d_work_saved, work_bytes, cudaMemcpyDeviceToDevice, c->st));
+                    if (c->hit_capacity < c->max_hits) {
+                        if (ensure_hits(c, (size_t)std::min<unsigned long long>(total, c->max_hits)) != UPBP_OK)
+                            return UPBP_ERR_CUDA;
+                    } else {
+                        span = std::max(1u, std::min(done, end - begin) / 2);
+                    }
+                    continue;
+                }
+                if (total > 0) {
+                    const unsigned g2 = grid_for((unsigned)total);
+                    switch (mode) {
+                    case kModePb2d: range_eval_kernel<kModePb2d><<<g2, 128, 0, c->st>>>(); break;
+                    case kModeBb1d: range_eval_kernel<kModeBb1d><<<g2, 128, 0, c->st>>>(); break;
+                    default: range_eval_kernel<kModeBp2d><<<g2, 128, 0, c->st>>>(); break;
+                    }
+                    launches++;
+                    UPBP_CK(cudaGetLastError());
+                }
+                found += total;
+                begin += done;
+                repeats = 0;
+                span = span > nq / 2 ? nq : 2 * span;
             }
-            found += total;
-            begin += done;
-            repeats = 0;
-            span = span > nq / 2 ? nq : 2 * span;
+            if (found > c->hit_capacity - c->hit_capacity / 4 &&
+                ensure_hits(c, (size_t)std::min<unsigned long long>(found + found / 8, c->max_hits)) != UPBP_OK)
+                return UPBP_ERR_CUDA;
+            return UPBP_OK;
+        };
+        UPBP_CK(cudaEventRecord(ev[6], c->st));
+        if (run_surf) {
+            point_merge_kernel<false><<<grid_for(npt), 128, 0, c->st>>>();
+            launches++;
         }
-        if (found > c->hit_capacity - c->hit_capacity / 4 &&
-            ensure_hits(c, (size_t)std::min<unsigned long long>(found + found / 8, c->max_hits)) != UPBP_OK)
-            return UPBP_ERR_CUDA;
+        UPBP_CK(cudaEventRecord(ev[7], c->st));
+        if (run_pp3d) {
+            point_merge_kernel<true><<<grid_for(npt), 128, 0, c->st>>>();
+            launches++;
+        }
+        UPBP_CK(cudaEventRecord(ev[8], c->st));
+        if (run_bp2d && estimator(kModeBp2d, npt) != UPBP_OK) return UPBP_ERR_CUDA;
+        UPBP_CK(cudaEventRecord(ev[9], c->st));
+        if (run_pb2d && estimator(kModePb2d, nseg) != UPBP_OK) return UPBP_ERR_CUDA;
+        UPBP_CK(cudaEventRecord(ev[10], c->st));
+        if (run_bb1d && estimator(kModeBb1d, nseg) != UPBP_OK) return UPBP_ERR_CUDA;
+        UPBP_CK(cudaEventRecord(ev[11], c->st));
+        k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
+                                                                             (unsigned)npx);
+        launches++;
+        UPBP_CK(cudaEventRecord(ev[12], c->st));
+        c->launches = launches;
+        c->h2d_iter = h2d;
+        c->d2h_iter = d2h;
+        UPBP_CK(cudaGetLastError());
+        c->iterations++;
+        c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
         return UPBP_OK;
-    };
-    UPBP_CK(cudaEventRecord(ev[6], c->st));
-    if (run_surf) {
-        point_merge_kernel<false><<<grid_for(npt), 128, 0, c->st>>>();
-        launches++;
-    }
-    UPBP_CK(cudaEventRecord(ev[7], c->st));
-    if (run_pp3d) {
-        point_merge_kernel<true><<<grid_for(npt), 128, 0, c->st>>>();
-        launches++;
-    }
-    UPBP_CK(cudaEventRecord(ev[8], c->st));
-    if (run_bp2d && estimator(kModeBp2d, npt) != UPBP_OK) return UPBP_ERR_CUDA;
-    UPBP_CK(cudaEventRecord(ev[9], c->st));
-    if (run_pb2d && estimator(kModePb2d, nseg) != UPBP_OK) return UPBP_ERR_CUDA;
-    UPBP_CK(cudaEventRecord(ev[10], c->st));
-    if (run_bb1d && estimator(kModeBb1d, nseg) != UPBP_OK) return UPBP_ERR_CUDA;
-    UPBP_CK(cudaEventRecord(ev[11], c->st));
-    k_finish_iteration<<<(unsigned)((npx + 255) / 256), 256, 0, c->st>>>(c->d_fb, c->d_cam_fb, c->d_acc,
-                                                                         (unsigned)npx);
-    launches++;
-    UPBP_CK(cudaEventRecord(ev[12], c->st));
-    c->launches = launches;
-    c->h2d_iter = h2d;
-    c->d2h_iter = d2h;
-    UPBP_CK(cudaGetLastError());
-    c->iterations++;
-    c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
-    return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_accumulate_to_host(upbp_ctx* c, float* rgb, double scale)
 {
-    if (!c || !rgb) return UPBP_ERR_ARGS;
-    const size_t n = (size_t)c->P.screen_pixel_count * 3;
-    std::vector<double> tmp(n);
-    UPBP_CK(cudaMemcpyAsync(tmp.data(), c->d_acc, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    for (size_t i = 0; i < n; i++) rgb[i] += (float)(scale * tmp[i]);
-    return UPBP_OK;
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !rgb) return UPBP_ERR_ARGS;
+        const size_t n = (size_t)c->P.screen_pixel_count * 3;
+        std::vector<double> tmp(n);
+        UPBP_CK(cudaMemcpyAsync(tmp.data(), c->d_acc, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        for (size_t i = 0; i < n; i++) rgb[i] += (float)(scale * tmp[i]);
+        return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_read_iteration(upbp_ctx* c, float* rgb)
 {
-    if (!c || !rgb) return UPBP_ERR_ARGS;
-    const size_t n = (size_t)c->P.screen_pixel_count * 3;
-    UPBP_CK(cudaMemcpyAsync(rgb, c->d_fb, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    return UPBP_OK;
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !rgb) return UPBP_ERR_ARGS;
+        const size_t n = (size_t)c->P.screen_pixel_count * 3;
+        UPBP_CK(cudaMemcpyAsync(rgb, c->d_fb, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
 {
-    if (!c || !o) return UPBP_ERR_ARGS;
-    std::memset(o, 0, sizeof(*o));
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    unsigned status = 0;
-    UPBP_CK(cudaMemcpy(&status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    o->light_vertices = c->h_counters[0];
-    o->surface_vertices = c->h_counters[1];
-    o->medium_vertices = c->h_counters[2];
-    o->light_beams = c->h_counters[3];
-    o->light_paths = c->P.light_subpath_count;
-    o->camera_paths = c->P.screen_pixel_count;
-    o->status = status;
-    o->iterations_done = c->iterations;
-    o->triangle_count = c->triangles;
-    o->scene_radius = c->P.scene_radius;
-    unsigned long long work[kKernCount * kCtrCount];
-    UPBP_CK(cudaMemcpy(work, c->d_work, sizeof(work), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < kKernCount && k < UPBP_KERNEL_KINDS; k++)
-        for (int i = 0; i < kCtrCount && i < 8; i++) o->work[k][i] = work[k * kCtrCount + i];
-    for (int i = 0; i < kCtrCount && i < 8; i++) {
-        o->work_light[i] = work[i];
-        unsigned long long cam = 0;
-        for (int k = 1; k < kKernCount; k++) cam += work[k * kCtrCount + i];
-        o->work_camera[i] = cam;
-    }
-    o->segment_queries = c->h_qcount[0];
-    o->point_queries = c->h_qcount[1];
-    o->nee_samples = c->h_qcount[4];
-    o->bpt_pairs = c->h_qcount[5];
-    o->beam_chunks = c->last_chunks;
-    o->radius[0] = c->P.radius_bb1d;
-    o->radius[1] = c->P.radius_bp2d;
-    o->radius[2] = c->P.radius_pb2d;
-    o->radius[3] = c->P.radius_pp3d;
-    o->radius[4] = c->P.radius_surf;
-    o->radius[5] = c->P.rad_beam;
-    o->h2d_bytes = (uint32_t)c->h2d_iter;
-    o->d2h_bytes = (uint32_t)c->d2h_iter;
-    o->kernel_launches = c->launches;
-    // per-pass times: the last iteration, and sums over the iterations run
-    // since the previous stats call (up to the event ring size)
-    for (unsigned k = 0; k < c->ev_pending; k++) {
-        cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
-        float light, build, cam;
-        UPBP_CK(cudaEventElapsedTime(&light, ev[0], ev[1]));
-        UPBP_CK(cudaEventElapsedTime(&build, ev[1], ev[2]));
-        UPBP_CK(cudaEventElapsedTime(&cam, ev[2], ev[12]));
-        if (k == 0) {
-            o->ms_light = light;
-            o->ms_build = build;
-            o->ms_camera = cam;
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !o) return UPBP_ERR_ARGS;
+        std::memset(o, 0, sizeof(*o));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        unsigned status = 0;
+        UPBP_CK(cudaMemcpy(&status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        o->light_vertices = c->h_counters[0];
+        o->surface_vertices = c->h_counters[1];
+        o->medium_vertices = c->h_counters[2];
+        o->light_beams = c->h_counters[3];
+        o->light_paths = c->P.light_subpath_count;
+        o->camera_paths = c->P.screen_pixel_count;
+        o->status = status;
+        o->iterations_done = c->iterations;
+        o->triangle_count = c->triangles;
+        o->scene_radius = c->P.scene_radius;
+        unsigned long long work[kKernCount * kCtrCount];
+        UPBP_CK(cudaMemcpy(work, c->d_work, sizeof(work), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < kKernCount && k < UPBP_KERNEL_KINDS; k++)
+            for (int i = 0; i < kCtrCount && i < 8; i++) o->work[k][i] = work[k * kCtrCount + i];
+        for (int i = 0; i < kCtrCount && i < 8; i++) {
+            o->work_light[i] = work[i];
+            unsigned long long cam = 0;
+            for (int k = 1; k < kKernCount; k++) cam += work[k * kCtrCount + i];
+            o->work_camera[i] = cam;
         }
-        o->ms_light_sum += light;
-        o->ms_build_sum += build;
-        o->ms_camera_sum += cam;
-        for (const EvInterval& iv : kKindInterval) {
-            float t;
-            UPBP_CK(cudaEventElapsedTime(&t, ev[iv.from], ev[iv.to]));
-            o->ms_kernel_sum[iv.kind] += t;
+        o->segment_queries = c->h_qcount[0];
+        o->point_queries = c->h_qcount[1];
+        o->nee_samples = c->h_qcount[4];
+        o->bpt_pairs = c->h_qcount[5];
+        o->beam_chunks = c->last_chunks;
+        o->radius[0] = c->P.radius_bb1d;
+        o->radius[1] = c->P.radius_bp2d;
+        o->radius[2] = c->P.radius_pb2d;
+        o->radius[3] = c->P.radius_pp3d;
+        o->radius[4] = c->P.radius_surf;
+        o->radius[5] = c->P.rad_beam;
+        o->h2d_bytes = (uint32_t)c->h2d_iter;
+        o->d2h_bytes = (uint32_t)c->d2h_iter;
+        o->kernel_launches = c->launches;
+        // per-pass times: the last iteration, and sums over the iterations run
+        // since the previous stats call (up to the event ring size)
+        for (unsigned k = 0; k < c->ev_pending; k++) {
+            cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
+            float light, build, cam;
+            UPBP_CK(cudaEventElapsedTime(&light, ev[0], ev[1]));
+            UPBP_CK(cudaEventElapsedTime(&build, ev[1], ev[2]));
+            UPBP_CK(cudaEventElapsedTime(&cam, ev[2], ev[12]));
+            if (k == 0) {
+                o->ms_light = light;
+                o->ms_build = build;
+                o->ms_camera = cam;
+            }
+            o->ms_light_sum += light;
+            o->ms_build_sum += build;
+            o->ms_camera_sum += cam;
+            for (const EvInterval& iv : kKindInterval) {
+                float t;
+                UPBP_CK(cudaEventElapsedTime(&t, ev[iv.from], ev[iv.to]));
+                o->ms_kernel_sum[iv.kind] += t;
+            }
+            o->timed_iterations++;
         }
-        o->timed_iterations++;
-    }
-    c->ev_pending = 0;
-    return UPBP_OK;
+        c->ev_pending = 0;
+        return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_debug_photons(upbp_ctx* c, int kind, float* out, uint32_t capacity, uint32_t* count)
 {
-    if (!c || !count || kind < 0 || kind > 2) return UPBP_ERR_ARGS;
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    if (kind < 2) {
-        const PointMap& m = kind == 0 ? c->P.surf_map : c->P.med_map;
-        *count = m.bvh.count;
-        const unsigned n = std::min(m.bvh.count, capacity);
-        if (out && n) UPBP_CK(cudaMemcpy(out, m.pos, n * sizeof(float4), cudaMemcpyDeviceToHost));
-        return UPBP_OK;
-    }
-    const unsigned nb = std::min(c->h_counters[3], c->beam_capacity);
-    *count = (c->P.build_bb1d || c->P.build_bp2d) ? nb : 0;
-    const unsigned n = std::min(*count, capacity);
-    if (out && n) {
-        std::vector<BeamRec> tmp(n);
-        UPBP_CK(cudaMemcpy(tmp.data(), c->d_beams, n * sizeof(BeamRec), cudaMemcpyDeviceToHost));
-        for (unsigned i = 0; i < n; i++) {
-            const float4 q0 = tmp[i].q[0], q1 = tmp[i].q[1], q3 = tmp[i].q[3];
-            float* o = out + 8 * (size_t)i;
-            o[0] = q0.x;
-            o[1] = q0.y;
-            o[2] = q0.z;
-            o[3] = q0.w;
-            o[4] = q1.x;
-            o[5] = q1.y;
-            o[6] = q1.z;
-            std::memcpy(&o[7], &q3.z, 4);  // path index bits
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !count || kind < 0 || kind > 2) return UPBP_ERR_ARGS;
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        if (kind < 2) {
+            const PointMap& m = kind == 0 ? c->P.surf_map : c->P.med_map;
+            *count = m.bvh.count;
+            const unsigned n = std::min(m.bvh.count, capacity);
+            if (out && n) UPBP_CK(cudaMemcpy(out, m.pos, n * sizeof(float4), cudaMemcpyDeviceToHost));
+            return UPBP_OK;
         }
-    }
-    return UPBP_OK;
+        const unsigned nb = std::min(c->h_counters[3], c->beam_capacity);
+        *count = (c->P.build_bb1d || c->P.build_bp2d) ? nb : 0;
+        const unsigned n = std::min(*count, capacity);
+        if (out && n) {
+            std::vector<BeamRec> tmp(n);
+            UPBP_CK(cudaMemcpy(tmp.data(), c->d_beams, n * sizeof(BeamRec), cudaMemcpyDeviceToHost));
+            for (unsigned i = 0; i < n; i++) {
+                const float4 q0 = tmp[i].q[0], q1 = tmp[i].q[1], q3 = tmp[i].q[3];
+                float* o = out + 8 * (size_t)i;
+                o[0] = q0.x;
+                o[1] = q0.y;
+                o[2] = q0.z;
+                o[3] = q0.w;
+                o[4] = q1.x;
+                o[5] = q1.y;
+                o[6] = q1.z;
+                std::memcpy(&o[7], &q3.z, 4);  // path index bits
+            }
+        }
+        return UPBP_OK;
+    });
 }
 
 extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uint32_t n, uint32_t* counts,
                                 uint32_t* ids, uint32_t ids_per_query)
 {
-    if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
-    if (n == 0) return UPBP_OK;
-    float* dq = nullptr;
-    unsigned *dc = nullptr, *di = nullptr;
-    UPBP_CK(dalloc(&dq, 8 * (size_t)n));
-    UPBP_CK(dalloc(&dc, n));
-    UPBP_CK(dalloc(&di, (size_t)n * std::max(1u, ids_per_query)));
-    UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
-    UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
-    k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
-    UPBP_CK(cudaGetLastError());
-    UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-    if (ids && ids_per_query)
-        UPBP_CK(cudaMemcpyAsync(ids, di, (size_t)n * ids_per_query * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    cudaFree(dq);
-    cudaFree(dc);
-    cudaFree(di);
-    return UPBP_OK;
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
+        if (n == 0) return UPBP_OK;
+        float* dq = nullptr;
+        unsigned *dc = nullptr, *di = nullptr;
+        UPBP_CK(dalloc(&dq, 8 * (size_t)n));
+        UPBP_CK(dalloc(&dc, n));
+        UPBP_CK(dalloc(&di, (size_t)n * std::max(1u, ids_per_query)));
+        UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
+        k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
+        UPBP_CK(cudaGetLastError());
+        UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        if (ids && ids_per_query)
+            UPBP_CK(cudaMemcpyAsync(ids, di, (size_t)n * ids_per_query * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        cudaFree(dq);
+        cudaFree(dc);
+        cudaFree(di);
+        return UPBP_OK;
+    });
 }
 
 // ---- neighbour-set query without device allocation --------------------
@@ -1210,42 +1224,44 @@ unsigned char* g_scratch_addr[64] = {};  // device address of g_query_scratch, p
 extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queries, uint32_t n, uint32_t* counts,
                                        uint32_t* ids, uint32_t ids_per_query)
 {
-    if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
-    if (n > kStaticQueryMax || ids_per_query > kStaticIdsMax) {
-        upbp_host::set_error("upbp_debug_query_static: at most " + std::to_string(kStaticQueryMax) +
-                             " queries and " + std::to_string(kStaticIdsMax) + " ids per query");
-        return UPBP_ERR_ARGS;
-    }
-    if (n == 0) return UPBP_OK;
-    int dev = 0;
-    UPBP_CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return UPBP_ERR_ARGS;
-    unsigned char* base = nullptr;
-    {
-        // first call on a device: resolve the array's device address (the
-        // host-side symbol is only a stand-in and must never reach a kernel)
-        std::lock_guard<std::mutex> lk(g_scratch_mu);
-        if (!g_scratch_addr[dev]) {
-            void* ptr = nullptr;
-            UPBP_CK(cudaGetSymbolAddress(&ptr, g_query_scratch));
-            g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
+        if (n > kStaticQueryMax || ids_per_query > kStaticIdsMax) {
+            upbp_host::set_error("upbp_debug_query_static: at most " + std::to_string(kStaticQueryMax) +
+                                 " queries and " + std::to_string(kStaticIdsMax) + " ids per query");
+            return UPBP_ERR_ARGS;
         }
-        base = g_scratch_addr[dev];
-    }
-    float* dq = reinterpret_cast<float*>(base);
-    unsigned* dc = reinterpret_cast<unsigned*>(base + kStaticQueryBytes);
-    unsigned* di = reinterpret_cast<unsigned*>(base + kStaticQueryBytes + kStaticCountBytes);
-    const size_t id_bytes = (size_t)n * ids_per_query * sizeof(unsigned);
-    UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
-    // the array keeps the previous call's ids; clear this call's id slots
-    if (id_bytes) UPBP_CK(cudaMemsetAsync(di, 0, id_bytes, c->st));
-    UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
-    k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
-    UPBP_CK(cudaGetLastError());
-    UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-    if (ids && id_bytes) UPBP_CK(cudaMemcpyAsync(ids, di, id_bytes, cudaMemcpyDeviceToHost, c->st));
-    UPBP_CK(cudaStreamSynchronize(c->st));
-    return UPBP_OK;
+        if (n == 0) return UPBP_OK;
+        int dev = 0;
+        UPBP_CK(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return UPBP_ERR_ARGS;
+        unsigned char* base = nullptr;
+        {
+            // first call on a device: resolve the array's device address (the
+            // host-side symbol is only a stand-in and must never reach a kernel)
+            std::lock_guard<std::mutex> lk(g_scratch_mu);
+            if (!g_scratch_addr[dev]) {
+                void* ptr = nullptr;
+                UPBP_CK(cudaGetSymbolAddress(&ptr, g_query_scratch));
+                g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
+            }
+            base = g_scratch_addr[dev];
+        }
+        float* dq = reinterpret_cast<float*>(base);
+        unsigned* dc = reinterpret_cast<unsigned*>(base + kStaticQueryBytes);
+        unsigned* di = reinterpret_cast<unsigned*>(base + kStaticQueryBytes + kStaticCountBytes);
+        const size_t id_bytes = (size_t)n * ids_per_query * sizeof(unsigned);
+        UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+        // the array keeps the previous call's ids; clear this call's id slots
+        if (id_bytes) UPBP_CK(cudaMemsetAsync(di, 0, id_bytes, c->st));
+        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
+        k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
+        UPBP_CK(cudaGetLastError());
+        UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        if (ids && id_bytes) UPBP_CK(cudaMemcpyAsync(ids, di, id_bytes, cudaMemcpyDeviceToHost, c->st));
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        return UPBP_OK;
+    });
 }
 
 extern "C" void* upbp_get_stream(upbp_ctx* c) { return c ? (void*)c->st : nullptr; }

@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libupbp_b200.so")
 
 UPBP_OK, UPBP_HELP = 0, 1
-ERRORS = {-1: "invalid arguments", -2: "I/O error", -3: "CUDA error", -4: "no CUDA device", -5: "invalid scene"}
+ERRORS = {-1: "invalid arguments", -2: "I/O error", -3: "CUDA error", -4: "no CUDA device", -5: "invalid scene",
+          -6: "host error"}
 STATUS_BITS = {1: "boundary stack", 2: "intersection array", 4: "volume segment array", 8: "intersection stack",
                16: "beam capacity", 32: "traversal stack"}
 

@@ -33,6 +33,7 @@ extern "C" {
 #define UPBP_ERR_CUDA (-3)       /* a CUDA call failed; see upbp_last_error */
 #define UPBP_ERR_NO_DEVICE (-4)  /* no CUDA device / extension not usable */
 #define UPBP_ERR_SCENE (-5)      /* scene description is inconsistent */
+#define UPBP_ERR_HOST (-6)       /* host memory or thread failure; see upbp_last_error */
 #define UPBP_HELP 1              /* the command line asked for help */
 
 /* Device status bits, the reference's RETURN_WITH_ERR codes
