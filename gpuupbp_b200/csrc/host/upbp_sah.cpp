@@ -42,6 +42,14 @@ struct Box {
     }
 };
 
+// Bin of a centroid coordinate: 0 .. kBins-1, also for NaN or values outside
+// the bounds (a float-to-int conversion of those is undefined).
+int bin_of(float c, float lo, float scale)
+{
+    const float f = (c - lo) * scale;
+    return f > 0.f ? std::min(kBins - 1, (int)std::min(f, (float)kBins)) : 0;
+}
+
 struct Build {
     const float* box;         // 6 floats per primitive
     std::vector<float> cen;   // 3 floats per primitive
@@ -90,7 +98,7 @@ void build(Build& b, uint32_t a, uint32_t e, uint32_t slot, int depth)
             for (auto& x : bins) x.reset();
             for (uint32_t i = a; i < e; i++) {
                 const uint32_t p = b.idx[i];
-                const int k = std::min(kBins - 1, (int)((b.cen[3 * (size_t)p + ax] - cb.lo[ax]) * scale));
+                const int k = bin_of(b.cen[3 * (size_t)p + ax], cb.lo[ax], scale);
                 bins[k].grow(b.box + 6 * (size_t)p, b.box + 6 * (size_t)p + 3);
                 counts[k]++;
             }
@@ -125,7 +133,7 @@ void build(Build& b, uint32_t a, uint32_t e, uint32_t slot, int depth)
         const float lo = cb.lo[best_axis], scale = kBins / (cb.hi[best_axis] - cb.lo[best_axis]);
         const float* cen = b.cen.data();
         const uint32_t* it = std::partition(b.idx + a, b.idx + e, [&](uint32_t p) {
-            return std::min(kBins - 1, (int)((cen[3 * (size_t)p + best_axis] - lo) * scale)) <= best_bin;
+            return bin_of(cen[3 * (size_t)p + best_axis], lo, scale) <= best_bin;
         });
         mid = (uint32_t)(it - b.idx);
         if (mid == a || mid == e) mid = a + m / 2;

@@ -101,6 +101,17 @@ def test_sah_tree_is_valid(harness, n, seed):
     check_tree(boxes, nodes, links, order)
 
 
+def test_sah_tolerates_nan_boxes(harness):
+    """A NaN box (a malformed vertex) still lands in exactly one leaf."""
+    rng = np.random.default_rng(5)
+    n = 200
+    c = rng.random((n, 3)) * 4
+    boxes = np.concatenate([c - 0.05, c + 0.05], axis=1).astype(np.float32)
+    boxes[[3, 77]] = np.nan
+    nodes, links, order = run(harness, boxes)
+    assert sorted(order.tolist()) == list(range(n))
+
+
 def test_sah_coincident_centroids(harness):
     """All centroids equal: the builder falls back to middle splits."""
     n = 300
