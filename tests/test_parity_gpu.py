@@ -67,9 +67,12 @@ def test_accumulation_is_the_mean_of_iterations(scene_dir):
 def test_search_rounds_match_one_round(scene_dir, monkeypatch):
     """A hit list far smaller than an iteration's hits makes every range
     search run in many rounds (with repeated rounds after overflows): each
-    query must still be searched exactly once, so the work counters equal
+    query must still be searched exactly once, so the accepted pairs equal
     those of a single round and the image equals it up to the order of the
-    float additions."""
+    float additions.  (Node visits are not compared: the light pass appends
+    photons and beams in an order that varies from run to run, and Morton-code
+    ties follow that order, so two renderers can build different trees; the
+    accepted pairs do not depend on the tree.)"""
     from gpuupbp_b200 import upbp
     path = scenes.write_workload("box_medium", scene_dir)
     args = command_line("box_all_bp2d", path)
@@ -85,8 +88,8 @@ def test_search_rounds_match_one_round(scene_dir, monkeypatch):
         r.close()
     monkeypatch.delenv("UPBP_MAX_HITS", raising=False)
     (img1, st1), (img2, st2) = runs
-    for k in ("pb2d_query", "bb1d_query", "bp2d_query"):
-        assert st1["work"][k] == st2["work"][k], k
+    for k, field in (("pb2d_query", "point_hit"), ("bb1d_query", "beam_hit"), ("bp2d_query", "beam_hit")):
+        assert st1["work"][k][field] == st2["work"][k][field], k
     assert st1["work"]["bb1d_query"]["beam_hit"] > 4 * 512
     assert st2["kernel_launches"] > st1["kernel_launches"] + 8
     assert np.allclose(img1, img2, rtol=1e-4, atol=1e-6)
