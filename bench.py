@@ -13,9 +13,15 @@ Metric: paths/s = (camera + light subpaths per iteration) x iterations / time.
                     [--workload media_field|dense_beams]
 
 `--workload dense_beams` times the dense-beam stress case instead (1920x1080,
-one thick medium in a 500k-triangle enclosure, path length 16, beams from
-the first 600 000 light paths: about 2M beams and 4-5M photon points per
-iteration); the headline line is the default workload.
+one thick medium in a 500k-triangle enclosure, path length 16, BB1D over the
+beams of the first 600 000 light paths, about 2M, BP2D over all, about 7M,
+and 4-5M photon points per iteration); the headline line is the default
+workload.
+
+`value` is timed with CUDA events on the library's stream, inputs resident;
+`e2e` renders the same iterations through the C ABI and reads every
+iteration's image back into page-locked host memory.  nvidia-smi samples the
+clocks during the timed region.
 
 N > 1 runs under torchrun, one rank per GPU; rank r renders iterations
 r, r+N, ... (iterations are independent given the seed), so the scaling is
