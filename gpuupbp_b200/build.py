@@ -21,7 +21,8 @@ HOST_CXX = "/usr/bin/g++"   # system toolchain (dynamic libstdc++)
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompiler", "-fPIC", "-diag-suppress", "549,550"]
 
 DEVICE_SOURCES = ["upbp_capi.cu"]
-HOST_SOURCES = ["host/upbp_cli.cpp", "host/upbp_scene.cpp", "host/upbp_exr.cpp", "host/upbp_sah.cpp"]
+HOST_SOURCES = ["host/upbp_cli.cpp", "host/upbp_scene.cpp", "host/upbp_predef.cpp", "host/upbp_exr.cpp",
+                "host/upbp_sah.cpp"]
 
 
 def _sources():

@@ -50,7 +50,10 @@ void print_usage(const char* prog)
 {
     std::printf("\nUsage: %s [ -s <scene_id> | -a <algorithm> | -l <path length> |\n", prog);
     std::printf("           -t <time> | -i <iteration> | -o <output_name> ]\n\n");
-    std::printf("    -s  -1 <file.obj>  OBJ scene (with <file.obj>.aux); predefined ids 0..40\n");
+    std::printf("    -s  <scene_id> selects the scene (default 0):\n");
+    std::printf("        -1    <file.obj>: OBJ scene (with <file.obj>.aux)\n");
+    for (int i = 0; i < upbp_host::predefined_scene_count(); i++)
+        std::printf("        %-2d    %s\n", i, upbp_host::predefined_scene_name(i, true));
     std::printf("    -a  upbp_<tech>[+<tech>]* | upbp+<tech>... | upbp_all (tech=bpt|surf|pp3d|pb2d|bb1d|bp2d)\n");
     std::printf("    -l  maximum path length (default 10)   -i iterations (default 1)   -t seconds\n");
     std::printf("    -o  output name (.exr or .bmp)          -r WIDTHxHEIGHT (default 256x256)\n");
@@ -114,7 +117,7 @@ extern "C" int upbp_parse_command_line(int argc, const char** argv, upbp_config*
                 if (!v) return fail("missing argument of -s option");
                 char* end = nullptr;
                 long id = std::strtol(v, &end, 10);
-                if (end == v || id >= 41 || id < -1) return fail("invalid argument of -s option");
+                if (end == v || id >= upbp_host::predefined_scene_count() || id < -1) return fail("invalid argument of -s option");
                 if (id == 3 || id == 4 || id == 9 || id == 10) return fail("scenes 3, 4, 9, and 10 cannot be rendered with UPBP");
                 c.scene_id = (int)id;
                 if (id == -1) {

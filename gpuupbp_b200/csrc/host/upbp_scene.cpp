@@ -284,6 +284,9 @@ void upbp_scene::finalize()
     desc.media = media.data();
     desc.light_count = (uint32_t)lights.size();
     desc.lights = lights.data();
+    desc.sphere_count = (uint32_t)sph_material.size();
+    desc.spheres = spheres.data();
+    desc.sph_material = sph_material.data();
 }
 
 using namespace upbp_host;
@@ -636,13 +639,18 @@ extern "C" int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_
     });
 }
 
-extern "C" int upbp_scene_load_predefined(int scene_id, uint32_t, uint32_t, upbp_scene** out)
+extern "C" int upbp_scene_load_predefined(int scene_id, uint32_t res_x, uint32_t res_y, upbp_scene** out)
 {
     return upbp_host::abi_guard([&]() -> int {
-        (void)scene_id;
-        (void)out;
-        set_error("predefined Cornell-box scenes (-s 0..40) are not available in this build; use -s -1 <file.obj>");
-        return UPBP_ERR_ARGS;
+        if (!out || res_x == 0 || res_y == 0) return UPBP_ERR_ARGS;
+        upbp_scene* sc = new upbp_scene();
+        const int rc = build_predefined(scene_id, res_x, res_y, *sc);
+        if (rc != UPBP_OK) {
+            delete sc;
+            return rc;
+        }
+        *out = sc;
+        return UPBP_OK;
     });
 }
 

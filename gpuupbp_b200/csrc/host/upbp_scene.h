@@ -12,6 +12,8 @@
 struct upbp_scene {
     std::vector<float> verts, normals;
     std::vector<int32_t> tri_material, tri_light;
+    std::vector<float> spheres;  // centre xyz, radius
+    std::vector<int32_t> sph_material;
     std::vector<upbp_material> materials;
     std::vector<upbp_medium> media;
     std::vector<upbp_light> lights;
@@ -31,6 +33,11 @@ struct CameraMatrices {
 CameraMatrices camera_setup(const upbp_camera_desc& c, float res_x, float res_y);
 
 void set_error(const std::string& msg);
+
+// The reference's predefined Cornell-box scenes (-s 0..40).
+int predefined_scene_count();
+const char* predefined_scene_name(int id, bool long_name);
+int build_predefined(int id, uint32_t res_x, uint32_t res_y, upbp_scene& sc);
 
 // Runs the body of a C entry point and turns a C++ exception (a failed host
 // allocation, a thread that could not start) into UPBP_ERR_HOST with its

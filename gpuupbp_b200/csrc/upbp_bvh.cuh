@@ -248,20 +248,68 @@ UPBP_D bool tri_intersect(const float4* tri, int s, float3 o, float3 d, float& t
 }
 
 struct TriHit {
-    float t, u, v;
-    int prim;  // original triangle index
+    float t, u, v;  // sphere hits: (u, v, w) is the normal
+    float w;
+    int prim;       // original triangle index; ~index for a sphere
 };
 
-// Closest triangle hit with t in [tmin, tmax]; ordered traversal, near child first.
-UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float tmax, TriHit& hit, bool& overflow)
+// Ray-sphere roots as the reference's sphere intersection program finds them
+// (gpuupbp/kernel/intersector.cu:35-97): the near root of the unit-direction
+// quadratic, refined once by solving again from its own point when it lies
+// farther than the radius, and the far root of the (refined) solve.  Normals
+// are (point - centre) / radius.  False when the ray misses the sphere.
+UPBP_D bool sphere_roots(float4 s, float3 ro, float3 rd, float& t1, float3& n1, float& t2, float3& n2)
 {
-    if (tv.bvh.count == 0) return false;
+    const float radius = s.w;
+    const float3 o = ro - make_float3(s.x, s.y, s.z);
+    const float l = 1.f / length(rd);
+    const float3 d = rd * l;
+    float b = dot(o, d);
+    float c = dot(o, o) - radius * radius;
+    float disc = b * b - c;
+    if (!(disc > 0.f)) return false;
+    float sdisc = sqrtf(disc);
+    const float root1 = -b - sdisc;
+    float root11 = 0.f;
+    const bool refine = fabsf(root1) > radius;
+    if (refine) {
+        const float3 o1 = o + root1 * d;
+        b = dot(o1, d);
+        c = dot(o1, o1) - radius * radius;
+        disc = b * b - c;
+        if (disc > 0.f) {
+            sdisc = sqrtf(disc);
+            root11 = -b - sdisc;
+        }
+    }
+    const float inv_r = 1.f / radius;
+    t1 = (root1 + root11) * l;
+    n1 = (o + (root1 + root11) * d) * inv_r;
+    const float root2 = (-b + sdisc) + (refine ? root1 : 0.f);
+    t2 = root2 * l;
+    n2 = (o + root2 * d) * inv_r;
+    return true;
+}
+
+UPBP_D void sphere_hit(TriHit& h, float t, float3 n, int k)
+{
+    h.t = t;
+    h.u = n.x;
+    h.v = n.y;
+    h.w = n.z;
+    h.prim = ~k;
+}
+
+// Closest triangle hit with t in [tmin, best] (updates best); ordered
+// traversal, near child first.
+UPBP_D bool closest_triangle(const TriView& tv, float3 o, float3 d, float tmin, float& best, TriHit& hit,
+                             bool& overflow)
+{
+    bool found = false;
     const float3 inv = safe_inv(d);
     int stack[kStackDepth];
     int sp = 0;
     int node = tv.bvh.count > 1 ? 0 : ~0;
-    bool found = false;
-    float best = tmax;
     unsigned visits = 0, tests = 0;
     for (;;) {
         if (node < 0) {
@@ -313,17 +361,47 @@ UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float
     }
     count_work(kCtrNodes, visits);
     count_work(kCtrTris, tests);
+    return found;
+}
+
+// Closest triangle hit with t in [tmin, tmax], or closer sphere hit with t in
+// (tmin, tmax): a sphere reports its near root when that lies in range, else
+// its far root.  The spheres are tested after the tree, so that nothing of
+// theirs is live during the walk.
+UPBP_D bool closest_hit(const TriView& tv, float3 o, float3 d, float tmin, float tmax, TriHit& hit, bool& overflow)
+{
+    bool found = false;
+    float best = tmax;
+    if (tv.bvh.count > 0) found = closest_triangle(tv, o, d, tmin, best, hit, overflow);
+    for (int k = 0; k < tv.sphere_count; k++) {
+        float t1, t2;
+        float3 n1, n2;
+        if (!sphere_roots(__ldg(&tv.spheres[k]), o, d, t1, n1, t2, n2)) continue;
+        if (t1 > tmin && t1 < best) {
+            best = t1;
+            sphere_hit(hit, t1, n1, k);
+            found = true;
+        } else if (t2 > tmin && t2 < best) {
+            best = t2;
+            sphere_hit(hit, t2, n2, k);
+            found = true;
+        }
+    }
+    count_work(kCtrTris, (unsigned)tv.sphere_count);
     count_work(kCtrRays, 1u);
     return found;
 }
 
-// Every triangle hit with t in [tmin, tmax]; calls f(hit) for each, f returns
+// Every triangle hit with t in [tmin, tmax], then every sphere root with t in
+// (tmin, tmax) (near root first: the reference's any-hit program ignores
+// each hit, so both roots are reported); calls f(hit) for each, f returns
 // false to stop.
 template <class F>
 UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tmax, F&& f)
 {
     const float3 inv = safe_inv(d);
     unsigned tests = 0;
+    bool go = true;
     count_work(kCtrRays, 1u);
     const bool ok = bvh_walk(
         tv.bvh,
@@ -342,10 +420,26 @@ UPBP_D bool all_hits(const TriView& tv, float3 o, float3 d, float tmin, float tm
                 h.u = u;
                 h.v = v;
                 h.prim = __float_as_int(__ldg(&tv.tri[3 * s]).w);
-                return f(h);
+                go = f(h);
+                return go;
             }
             return true;
         });
+    for (int k = 0; k < tv.sphere_count && go; k++) {
+        float t1, t2;
+        float3 n1, n2;
+        tests++;
+        if (!sphere_roots(__ldg(&tv.spheres[k]), o, d, t1, n1, t2, n2)) continue;
+        TriHit h;
+        if (t1 > tmin && t1 < tmax) {
+            sphere_hit(h, t1, n1, k);
+            go = f(h);
+        }
+        if (go && t2 > tmin && t2 < tmax) {
+            sphere_hit(h, t2, n2, k);
+            go = f(h);
+        }
+    }
     count_work(kCtrTris, tests);
     return ok;
 }

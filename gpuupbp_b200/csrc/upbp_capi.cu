@@ -115,6 +115,9 @@ struct Geometry {
     float4* normals = nullptr;
     int2* record = nullptr;
     unsigned count = 0;
+    float4* spheres = nullptr;  // centre, radius
+    int* sph_mat = nullptr;
+    unsigned sph_count = 0;
 };
 
 }  // namespace
@@ -264,6 +267,27 @@ int upload_geometry(upbp_ctx* c, const upbp_scene_desc* s, bool real, Geometry& 
         rec.push_back(make_int2(m, s->tri_light[i]));
     }
     g.count = (unsigned)rec.size();
+    // Spheres of this class.  The reference hands OptiX a box per sphere and
+    // recovers centre and radius from it (intersector.cu:37-42); the same
+    // round trip here gives the same floats.
+    std::vector<float4> sph;
+    std::vector<int> sph_mat;
+    for (uint32_t i = 0; i < s->sphere_count; i++) {
+        const int m = s->sph_material[i];
+        if ((s->materials[m].real != 0) != real) continue;
+        const float* q = s->spheres + 4 * (size_t)i;
+        const float r = q[3];
+        const float lo[3] = {q[0] - r, q[1] - r, q[2] - r}, hi[3] = {q[0] + r, q[1] + r, q[2] + r};
+        float cen[3];
+        for (int k = 0; k < 3; k++) cen[k] = lo[k] + .5f * (hi[k] - lo[k]);
+        sph.push_back(make_float4(cen[0], cen[1], cen[2], (hi[0] - lo[0]) * .5f));
+        sph_mat.push_back(m);
+    }
+    g.sph_count = (unsigned)sph.size();
+    if (g.sph_count) {
+        UPBP_CK(dupload(&g.spheres, sph.data(), sph.size(), c->st));
+        UPBP_CK(dupload(&g.sph_mat, sph_mat.data(), sph_mat.size(), c->st));
+    }
     UPBP_CK(dupload(&g.normals, nrm.data(), nrm.size(), c->st));
     UPBP_CK(dupload(&g.record, rec.data(), rec.size(), c->st));
     UPBP_CK(dalloc(&g.nodes, g.count > 1 ? g.count - 1 : 1));
@@ -452,6 +476,18 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
                 upbp_host::set_error("triangle material index out of range");
                 return UPBP_ERR_SCENE;
             }
+        if (s->sphere_count > UPBP_MAX_SPHERES) {
+            upbp_host::set_error("more than UPBP_MAX_SPHERES spheres");
+            return UPBP_ERR_SCENE;
+        }
+        for (uint32_t i = 0; i < s->sphere_count; i++) {
+            const float r = s->spheres[4 * (size_t)i + 3];
+            if (s->sph_material[i] < 0 || (uint32_t)s->sph_material[i] >= s->material_count || !(r > 0.f) ||
+                !std::isfinite(r)) {
+                upbp_host::set_error("sphere with a material index out of range or a radius not positive");
+                return UPBP_ERR_SCENE;
+            }
+        }
         upbp_ctx* c = new upbp_ctx();
         c->cfg = *cfg;
         DeviceParams& P = c->P;
@@ -590,8 +626,10 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
             upbp_destroy(c);
             return UPBP_ERR_CUDA;
         }
-        P.real = TriView{BvhView{c->real.nodes, c->real.count}, c->real.tri, c->real.normals, c->real.record};
-        P.imag = TriView{BvhView{c->imag.nodes, c->imag.count}, c->imag.tri, c->imag.normals, c->imag.record};
+        P.real = TriView{BvhView{c->real.nodes, c->real.count}, c->real.tri, c->real.normals, c->real.record,
+                         c->real.spheres, c->real.sph_mat, (int)c->real.sph_count};
+        P.imag = TriView{BvhView{c->imag.nodes, c->imag.count}, c->imag.tri, c->imag.normals, c->imag.record,
+                         c->imag.spheres, c->imag.sph_mat, (int)c->imag.sph_count};
         const size_t npx = (size_t)P.screen_pixel_count * 3;
         UPBP_CK(dalloc(&c->d_vertices, c->vertex_capacity));
         UPBP_CK(dalloc(&c->d_path_count, std::max(1u, L)));
@@ -1271,6 +1309,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     if (!c) return;
     if (c->st) cudaStreamSynchronize(c->st);
     void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
+                    c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_med_qnodes, c->d_beam_qnodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,

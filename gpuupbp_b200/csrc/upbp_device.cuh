@@ -128,6 +128,12 @@ struct TriView {
     const float4* tri;       // 3 float4 per triangle
     const float4* normals;   // 4 float4 per triangle (n0, n1, n2, face), original order
     const int2* record;      // (material, light) per triangle, original order
+    // Analytic spheres of this class, tested one by one (the predefined
+    // scenes have at most seven): centre and radius as the reference
+    // recovers them from the sphere's box, and the material.
+    const float4* spheres;
+    const int* sph_mat;
+    int sphere_count;
 };
 
 // Light vertex record: 8 x 16 B, one per stored light-subpath vertex, placed

@@ -160,6 +160,13 @@ UPBP_D bool light_path_begin(LightLane& l, unsigned path_idx)
     l.stored = 0;
     l.my_slots = p.vertices + (size_t)path_idx * p.slots_per_path;
     l.origin_in_medium = false;
+    if (p.light_count == 0) {
+        // A scene without lights (an emitting medium only): no light subpaths.
+        // The reference samples lights[0] of its empty light array here
+        // (functs_light.cuh:93).
+        l.ret = 0;
+        return false;
+    }
     l.ret = generate_light_sample(l.s, l.rng);
     if (l.s.is_infinite_light && p.media[p.global_medium].has_attenuation) {
         // the reference ends such a path before tracing it, without an error

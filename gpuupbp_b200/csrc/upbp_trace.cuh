@@ -101,9 +101,22 @@ UPBP_D bool is_real_material(int mat) { return mat >= 0 && c_params.materials[ma
 
 UPBP_D void flag_status(unsigned bits) { atomicOr(c_params.status, bits); }
 
-// Fills surface data of a triangle hit (intersector.cu fill_isect).
+// Fills surface data of a triangle or sphere hit (intersector.cu fill_isect;
+// a sphere's shading normal is its geometric normal and it is no emitter).
 UPBP_D void fill_hit(const TriView& tv, const TriHit& h, float3 ray_dir, Isect& r)
 {
+    if (h.prim < 0) {
+        const int mat = __ldg(&tv.sph_mat[~h.prim]);
+        const float3 nrm = make_float3(h.u, h.v, h.w);
+        r.dist = h.t;
+        r.mat = mat;
+        r.med = c_params.materials[mat].medium;
+        r.light = -1;
+        r.normal = nrm;
+        r.enter = dot(nrm, ray_dir) < 0.f;
+        r.shading_normal = nrm;
+        return;
+    }
     const float4* n = tv.normals + 4 * (size_t)h.prim;
     const float3 face = xyz(__ldg(&n[3]));
     float3 sn;

@@ -62,6 +62,44 @@ class Stats(ctypes.Structure):
     ]
 
 
+F3 = ctypes.c_float * 3
+
+
+class MaterialDesc(ctypes.Structure):
+    _fields_ = [("diffuse", F3), ("phong", F3), ("phong_exponent", ctypes.c_float), ("mirror", F3),
+                ("ior", ctypes.c_float), ("priority", ctypes.c_int), ("real", ctypes.c_int), ("medium", ctypes.c_int)]
+
+
+class MediumDesc(ctypes.Structure):
+    _fields_ = [("absorption", F3), ("emission", F3), ("scattering", F3), ("continuation_prob", ctypes.c_float),
+                ("mean_cosine", ctypes.c_float)]
+
+
+class LightDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("mat_id", ctypes.c_int), ("med_id", ctypes.c_int), ("p0", F3), ("p1", F3),
+                ("p2", F3), ("intensity", F3), ("position", F3), ("scale", ctypes.c_float)]
+
+
+class CameraDesc(ctypes.Structure):
+    _fields_ = [("origin", F3), ("target", F3), ("roll", F3), ("horizontal_fov_deg", ctypes.c_float),
+                ("focal_dist", ctypes.c_float), ("mat_id", ctypes.c_int), ("med_id", ctypes.c_int)]
+
+
+class SceneDesc(ctypes.Structure):
+    """upbp_scene_desc (include/upbp.h)."""
+    _fields_ = [
+        ("triangle_count", ctypes.c_uint32), ("verts", ctypes.POINTER(ctypes.c_float)),
+        ("normals", ctypes.POINTER(ctypes.c_float)), ("tri_material", ctypes.POINTER(ctypes.c_int32)),
+        ("tri_light", ctypes.POINTER(ctypes.c_int32)), ("material_count", ctypes.c_uint32),
+        ("materials", ctypes.POINTER(MaterialDesc)), ("medium_count", ctypes.c_uint32),
+        ("media", ctypes.POINTER(MediumDesc)), ("global_medium", ctypes.c_int32), ("light_count", ctypes.c_uint32),
+        ("lights", ctypes.POINTER(LightDesc)), ("background_light", ctypes.c_int32), ("camera", CameraDesc),
+        ("res_x", ctypes.c_uint32), ("res_y", ctypes.c_uint32), ("bbox_min", F3), ("bbox_max", F3),
+        ("sphere_count", ctypes.c_uint32), ("spheres", ctypes.POINTER(ctypes.c_float)),
+        ("sph_material", ctypes.POINTER(ctypes.c_int32)),
+    ]
+
+
 KERNELS = ["light_pass", "camera_extend", "pb2d_query", "bb1d_query", "surf_query", "pp3d_query", "bp2d_query",
            "nee_connect", "bpt_connect"]
 
@@ -91,7 +129,7 @@ def load_library(path: str = LIB_PATH):
     L.upbp_scene_load_obj.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, P(VP)]
     L.upbp_scene_load_predefined.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, P(VP)]
     L.upbp_scene_get_desc.argtypes = [VP]
-    L.upbp_scene_get_desc.restype = VP
+    L.upbp_scene_get_desc.restype = P(SceneDesc)
     L.upbp_scene_free.argtypes = [VP]
     L.upbp_create.argtypes = [VP, P(Config), P(VP)]
     L.upbp_run_iteration.argtypes = [VP, ctypes.c_int]
@@ -127,6 +165,43 @@ def parse_command_line(args: list[str]) -> Config:
         raise UpbpError("help requested")
     _check(rc, "command line")
     return cfg
+
+
+def load_scene(args: list[str]) -> dict:
+    """The scene a command line names (-s <id> or -s -1 <file.obj>), loaded
+    by the library on the host, as numpy arrays and record lists."""
+    L = load_library()
+    c = parse_command_line(args)
+    sc = ctypes.c_void_p()
+    if c.scene_id < 0:
+        rc = L.upbp_scene_load_obj(c.scene_path, c.res_x, c.res_y, ctypes.byref(sc))
+    else:
+        rc = L.upbp_scene_load_predefined(c.scene_id, c.res_x, c.res_y, ctypes.byref(sc))
+    _check(rc, "scene")
+    try:
+        d = L.upbp_scene_get_desc(sc).contents
+        nt, ns = d.triangle_count, d.sphere_count
+
+        def arr(ptr, n, dt):
+            return np.ctypeslib.as_array(ptr, (n,)).astype(dt).copy() if n else np.zeros(0, dt)
+
+        def recs(ptr, n):
+            return [{k: (list(getattr(ptr[i], k)) if isinstance(getattr(ptr[i], k), ctypes.Array)
+                         else getattr(ptr[i], k)) for k, _ in ptr[i]._fields_} for i in range(n)]
+
+        return {
+            "verts": arr(d.verts, 9 * nt, np.float32).reshape(nt, 3, 3),
+            "normals": arr(d.normals, 12 * nt, np.float32).reshape(nt, 4, 3),
+            "tri_material": arr(d.tri_material, nt, np.int32), "tri_light": arr(d.tri_light, nt, np.int32),
+            "spheres": arr(d.spheres, 4 * ns, np.float32).reshape(ns, 4),
+            "sph_material": arr(d.sph_material, ns, np.int32),
+            "materials": recs(d.materials, d.material_count), "media": recs(d.media, d.medium_count),
+            "lights": recs(d.lights, d.light_count), "global_medium": d.global_medium,
+            "background_light": d.background_light,
+            "bbox_min": np.array(list(d.bbox_min), np.float32), "bbox_max": np.array(list(d.bbox_max), np.float32),
+        }
+    finally:
+        L.upbp_scene_free(sc)
 
 
 class Renderer:

@@ -147,7 +147,18 @@ typedef struct upbp_scene_desc {
     upbp_camera_desc camera;
     uint32_t res_x, res_y;
     float bbox_min[3], bbox_max[3];
+    /* Analytic spheres (the reference's Spheres, gpuupbp/shared/scene.h:62-75;
+     * only the predefined scenes have them): centre xyz and radius per
+     * sphere, and its material.  Real vs imaginary follows the material's
+     * `real` flag, as for triangles.  Spheres are never emitters (no loader
+     * of the reference gives them a light).  At most UPBP_MAX_SPHERES. */
+    uint32_t sphere_count;
+    const float* spheres;
+    const int32_t* sph_material;
 } upbp_scene_desc;
+
+#define UPBP_MAX_SPHERES 64
+#define UPBP_PREDEFINED_SCENES 41
 
 typedef struct upbp_scene upbp_scene;   /* host scene owned by the library */
 typedef struct upbp_ctx upbp_ctx;       /* device renderer state */

@@ -51,6 +51,8 @@ def lib():
         L.upbp_ref_iteration_count.restype = ctypes.c_int
         L.upbp_ref_describe.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         L.upbp_ref_describe.restype = ctypes.c_int
+        L.upbp_ref_scene_json.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
+        L.upbp_ref_scene_json.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -107,6 +109,16 @@ class RefRenderer:
         import json
         buf = ctypes.create_string_buffer(8192)
         lib().upbp_ref_describe(self._h, buf, len(buf))
+        return json.loads(buf.value.decode())
+
+    def scene(self) -> dict:
+        """Every record of the scene the reference's loader built: triangles
+        (3 vertices, face normal, (material, light)), sphere boxes (lo, hi,
+        (material, light)), materials, media, lights."""
+        import json
+        n = lib().upbp_ref_scene_json(self._h, None, 0)
+        buf = ctypes.create_string_buffer(n)
+        lib().upbp_ref_scene_json(self._h, buf, n)
         return json.loads(buf.value.decode())
 
     @staticmethod

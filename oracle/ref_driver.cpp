@@ -25,7 +25,9 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstring>
 #include <cstdio>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -677,6 +679,159 @@ int upbp_ref_describe(RefCtx* c, char* buf, int cap)
         s.record_count, cam.origin.x, cam.origin.y, cam.origin.z, cam.direction.x, cam.direction.y,
         cam.direction.z, cam.image_plane_dist, sc.scene_sphere.center.x, sc.scene_sphere.center.y,
         sc.scene_sphere.center.z, sc.scene_sphere.radius);
+}
+
+// JSON dump of every record of the loaded scene (triangles with their face
+// normals, sphere boxes, primitive records, materials, media, lights), for
+// the loader parity tests.  Returns the length the dump needs; writes it when
+// it fits in `cap` bytes.
+int upbp_ref_scene_json(RefCtx* c, char* buf, int cap)
+{
+    const OracleSetup& s = c->setup;
+    const Scene& sc = s.scene;
+    std::string o = "{";
+    auto num = [&](double v) {
+        char t[40];
+        snprintf(t, sizeof(t), "%.9g", v);
+        o += t;
+    };
+    auto f3 = [&](float3 v) {
+        o += "[";
+        num(v.x);
+        o += ",";
+        num(v.y);
+        o += ",";
+        num(v.z);
+        o += "]";
+    };
+    auto rec = [&](unsigned r) {
+        o += "[";
+        num(s.records[r].id_material);
+        o += ",";
+        num(s.records[r].id_light);
+        o += "]";
+    };
+    auto tris = [&](const char* name, const Triangles& t) {
+        o += std::string("\"") + name + "\": [";
+        for (unsigned i = 0; i < t.count; i++) {
+            if (i) o += ",";
+            o += "[";
+            for (int k = 0; k < 3; k++) {
+                f3(make_float3(t.verts[3 * i + k].x, t.verts[3 * i + k].y, t.verts[3 * i + k].z));
+                o += ",";
+            }
+            f3(t.norms[4 * i + 3]);
+            o += ",";
+            rec(t.records[i]);
+            o += "]";
+        }
+        o += "], ";
+    };
+    auto sphs = [&](const char* name, const Spheres& t) {
+        o += std::string("\"") + name + "\": [";
+        for (unsigned i = 0; i < t.count; i++) {
+            if (i) o += ",";
+            const OptixAabb& b = t.aabbs[i];
+            o += "[";
+            f3(make_float3(b.minX, b.minY, b.minZ));
+            o += ",";
+            f3(make_float3(b.maxX, b.maxY, b.maxZ));
+            o += ",";
+            rec(t.records[i]);
+            o += "]";
+        }
+        o += "], ";
+    };
+    tris("tri_real", sc.triangles_real);
+    tris("tri_imag", sc.triangles_imag);
+    sphs("sph_real", sc.spheres_real);
+    sphs("sph_imag", sc.spheres_imag);
+    o += "\"materials\": [";
+    for (unsigned i = 0; i < sc.mat_count; i++) {
+        const Material& m = sc.materials[i];
+        if (i) o += ",";
+        o += "[";
+        f3(m.diffuse_reflectance);
+        o += ",";
+        f3(m.phong_reflectance);
+        o += ",";
+        num(m.phong_exponent);
+        o += ",";
+        f3(m.mirror_reflectance);
+        o += ",";
+        num(m.ior);
+        o += ",";
+        num(m.priority);
+        o += ",";
+        num(m.real ? 1 : 0);
+        o += ",";
+        num(m.med_idx);
+        o += "]";
+    }
+    o += "], \"media\": [";
+    for (unsigned i = 0; i < sc.med_count; i++) {
+        const Medium& m = sc.media[i];
+        if (i) o += ",";
+        o += "[";
+        f3(m.absorption_coeff);
+        o += ",";
+        f3(m.emission_coeff);
+        o += ",";
+        f3(m.scattering_coeff);
+        o += ",";
+        num(m.continuation_prob);
+        o += ",";
+        num(m.mean_cosine);
+        o += "]";
+    }
+    // per light: type, material, medium, then (area) p0, e1, e2, intensity;
+    // (background) colour, scale; (directional) frame z, intensity; (point)
+    // position, intensity
+    o += "], \"lights\": [";
+    for (unsigned i = 0; i < sc.light_count; i++) {
+        const AbstractLight& l = sc.lights[i];
+        if (i) o += ",";
+        o += "[";
+        num((int)l.type);
+        o += ",";
+        num(l.mat_id);
+        o += ",";
+        num(l.med_id);
+        o += ",";
+        if (l.type == AREA) {
+            f3(l.area.p0);
+            o += ",";
+            f3(l.area.e1);
+            o += ",";
+            f3(l.area.e2);
+            o += ",";
+            f3(l.area.intensity);
+        } else if (l.type == BACKGROUND) {
+            f3(l.background.background_color);
+            o += ",";
+            num(l.background.scale);
+        } else if (l.type == DIRECTIONAL) {
+            f3(l.directional.frame.z);
+            o += ",";
+            f3(l.directional.intensity);
+        } else {
+            f3(l.point.position);
+            o += ",";
+            f3(l.point.intensity);
+        }
+        o += "]";
+    }
+    o += "], \"global_medium\": ";
+    num(sc.global_medium_idx);
+    o += ", \"background\": ";
+    num(sc.background_light_idx == UINT32_MAX ? -1 : (int)sc.background_light_idx);
+    o += ", \"scene_center\": ";
+    f3(sc.scene_sphere.center);
+    o += ", \"scene_radius\": ";
+    num(sc.scene_sphere.radius);
+    o += "}";
+    if ((int)o.size() < cap) std::memcpy(buf, o.c_str(), o.size() + 1);
+    return (int)o.size() + 1;
 }
 
 int upbp_ref_iteration_count(RefCtx* c) { return c->setup.iteration_count; }

@@ -50,5 +50,27 @@ CASES = {
 }
 
 
+# The reference's predefined Cornell-box scenes (-s <id>): analytic real and
+# imaginary spheres, point, directional (sun), background and facing lights,
+# global media, the imaginary box.  Workload "predef:<id>".
+PREDEF_ARGS = ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "32x32"]
+for _sid, _name in [(0, "abssph"), (1, "isosph"), (2, "mirsphinfisov"), (5, "ssssun"), (6, "ssspoint"),
+                    (7, "sssback"), (13, "nogeoisopt"), (17, "faceisosmall"), (21, "overgwi"), (22, "rovergwi"),
+                    (28, "overiwr"), (30, "woveriwr"), (31, "backg"), (35, "smallsb"), (39, "glasssphbck")]:
+    CASES[f"predef_{_sid:02d}_{_name}"] = (f"predef:{_sid}", True, PREDEF_ARGS, 1)
+
+
 def command_line(case: str, scene_path: str) -> list:
+    workload = CASES[case][0]
+    if workload.startswith("predef:"):
+        return ["-s", workload.split(":")[1]] + list(CASES[case][2])
     return ["-s", "-1", scene_path] + list(CASES[case][2])
+
+
+def prepare(case: str, scene_dir: str) -> list:
+    """The command line of a case, after writing its generated scene files
+    (predefined scenes need none)."""
+    from gpuupbp_b200 import scenes
+    workload, tiny, _, _ = CASES[case]
+    path = None if workload.startswith("predef:") else scenes.write_workload(workload, scene_dir, tiny=tiny)
+    return command_line(case, path)

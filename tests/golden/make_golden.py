@@ -21,8 +21,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 
 import ref_cpu  # noqa: E402
-from cases import CASES, command_line  # noqa: E402
-from gpuupbp_b200 import scenes  # noqa: E402
+from cases import CASES, prepare  # noqa: E402
 
 
 def main():
@@ -37,8 +36,7 @@ def main():
         for name, (workload, tiny, _, iters) in CASES.items():
             if only and name not in only:
                 continue
-            path = scenes.write_workload(workload, tmp, tiny=tiny)
-            r = ref_cpu.RefRenderer(command_line(name, path), threads=0)
+            r = ref_cpu.RefRenderer(prepare(name, tmp), threads=0)
             meta[name] = []
             for it in range(iters):
                 out[f"{name}/{it}"] = r.run_iteration(it)

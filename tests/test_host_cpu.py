@@ -78,33 +78,22 @@ def test_command_line_errors():
             upbp.parse_command_line(bad)
 
 
-class SceneDesc(ctypes.Structure):
-    _fields_ = [("triangle_count", ctypes.c_uint32), ("verts", ctypes.c_void_p), ("normals", ctypes.c_void_p),
-                ("tri_material", ctypes.c_void_p), ("tri_light", ctypes.c_void_p),
-                ("material_count", ctypes.c_uint32), ("materials", ctypes.c_void_p),
-                ("medium_count", ctypes.c_uint32), ("media", ctypes.c_void_p), ("global_medium", ctypes.c_int32),
-                ("light_count", ctypes.c_uint32), ("lights", ctypes.c_void_p), ("background_light", ctypes.c_int32),
-                ("cam_origin", ctypes.c_float * 3), ("cam_target", ctypes.c_float * 3), ("cam_roll", ctypes.c_float * 3),
-                ("cam_fov_deg", ctypes.c_float), ("cam_focal", ctypes.c_float), ("cam_mat", ctypes.c_int),
-                ("cam_med", ctypes.c_int), ("res_x", ctypes.c_uint32), ("res_y", ctypes.c_uint32),
-                ("bbox_min", ctypes.c_float * 3), ("bbox_max", ctypes.c_float * 3)]
-
-
 @pytest.mark.parametrize("workload", ["box_medium", "media_field", "dense_beams"])
 def test_scene_loader_matches_reference(workload, scene_dir, oracle_available):
     L = upbp.load_library()
     path = scenes.write_workload(workload, scene_dir, tiny=True)
     sc = ctypes.c_void_p()
     assert L.upbp_scene_load_obj(path.encode(), 40, 30, ctypes.byref(sc)) == 0
-    d = SceneDesc.from_address(L.upbp_scene_get_desc(sc))
-    mats = (ctypes.c_int32 * d.triangle_count).from_address(d.tri_material)
-    reals = [struct.unpack_from("i", ctypes.string_at(d.materials + 56 * m + 48, 4))[0] for m in range(d.material_count)]
+    d = L.upbp_scene_get_desc(sc).contents
+    mats = d.tri_material[:d.triangle_count]
+    reals = [d.materials[m].real for m in range(d.material_count)]
     n_real = sum(1 for i in range(d.triangle_count) if reals[mats[i]])
     info = dict(tris=d.triangle_count, real=n_real, lights=d.light_count, materials=d.material_count,
                 media=d.medium_count, global_medium=d.global_medium, background=d.background_light,
-                bmin=list(d.bbox_min), bmax=list(d.bbox_max), origin=list(d.cam_origin), fov=d.cam_fov_deg)
+                bmin=list(d.bbox_min), bmax=list(d.bbox_max), origin=list(d.camera.origin),
+                fov=d.camera.horizontal_fov_deg, spheres=d.sphere_count)
     L.upbp_scene_free(sc)
-    assert info["tris"] == scenes.WORKLOADS[workload](tiny=True).triangle_count()
+    assert info["tris"] == scenes.WORKLOADS[workload](tiny=True).triangle_count() and info["spheres"] == 0
     if not oracle_available:
         pytest.skip("oracle/_ref not built")
     import ref_cpu
@@ -132,7 +121,10 @@ def test_scene_loader_errors(tmp_path):
     bad.write_text("v 0 0 0\nf 1 2 3\n")
     (tmp_path / "bad.obj.aux").write_text("")
     assert L.upbp_scene_load_obj(str(bad).encode(), 8, 8, ctypes.byref(sc)) == -5
-    assert L.upbp_scene_load_predefined(0, 8, 8, ctypes.byref(sc)) == -1
+    assert L.upbp_scene_load_predefined(41, 8, 8, ctypes.byref(sc)) == -1
+    assert L.upbp_scene_load_predefined(0, 0, 8, ctypes.byref(sc)) == -1
+    assert L.upbp_scene_load_predefined(0, 8, 8, ctypes.byref(sc)) == 0
+    L.upbp_scene_free(sc)
 
 
 def read_exr_half(path):

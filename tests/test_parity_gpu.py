@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from cases import CASES, command_line
+from cases import CASES, command_line, prepare
 from gpuupbp_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -33,9 +33,8 @@ def test_image_parity_with_reference(case, scene_dir):
     from gpuupbp_b200 import upbp
     gold = np.load(os.path.join(GOLDEN, "oracle_images.npz"))
     counts = json.load(open(os.path.join(GOLDEN, "oracle_counts.json")))
-    workload, tiny, _, iters = CASES[case]
-    path = scenes.write_workload(workload, scene_dir, tiny=tiny)
-    r = upbp.Renderer(command_line(case, path))
+    iters = CASES[case][3]
+    r = upbp.Renderer(prepare(case, scene_dir))
     for it in range(iters):
         r.run_iteration(it)
         img = r.iteration_image()
@@ -62,6 +61,28 @@ def test_accumulation_is_the_mean_of_iterations(scene_dir):
     st = r.stats()
     assert st["iterations_done"] == 3 and st["status"] == 0
     r.close()
+
+
+def test_predefined_scene_without_lights():
+    """Predefined scene 10 (a glass sphere of emitting medium, no light): the
+    command line refuses it as the reference's does, the C API renders it.
+    No light subpaths are traced; the medium's emission reaches the camera."""
+    import ctypes
+    from gpuupbp_b200 import upbp
+    L = upbp.load_library()
+    cfg = upbp.parse_command_line(["-s", "0", "-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "32x32"])
+    sc, ctx = ctypes.c_void_p(), ctypes.c_void_p()
+    assert L.upbp_scene_load_predefined(10, 32, 32, ctypes.byref(sc)) == 0
+    assert L.upbp_create(L.upbp_scene_get_desc(sc), ctypes.byref(cfg), ctypes.byref(ctx)) == 0
+    assert L.upbp_run_iteration(ctx, 0) >= 0
+    img = np.zeros((32, 32, 3), np.float32)
+    assert L.upbp_read_iteration(ctx, img.ctypes.data) == 0
+    st = upbp.Stats()
+    assert L.upbp_get_stats(ctx, ctypes.byref(st)) == 0
+    L.upbp_destroy(ctx)
+    L.upbp_scene_free(sc)
+    assert st.status == 0 and st.light_vertices == 0 and st.light_beams == 0
+    assert np.isfinite(img).all() and img.max() > 0
 
 
 def test_search_rounds_match_one_round(scene_dir, monkeypatch):
