@@ -101,13 +101,26 @@ UPBP_D bool is_real_material(int mat) { return mat >= 0 && c_params.materials[ma
 
 UPBP_D void flag_status(unsigned bits) { atomicOr(c_params.status, bits); }
 
+// A sphere normal component as the reference's closest-hit and any-hit
+// programs read it back from the hit attributes (intersector.cu:130-132): the
+// attribute word holds the component's bits, __float_as_int is applied to the
+// word, so the word is first converted to float by value, and the int read
+// from that float's bits becomes the component.  The result is large and
+// positive for every nonzero component instead of the unit normal; it decides
+// `enter` and the shading frame at sphere hits, so it is kept for parity.
+UPBP_D float sphere_attribute_component(float x)
+{
+    return __int2float_rn(__float_as_int(__uint2float_rn(__float_as_uint(x))));
+}
+
 // Fills surface data of a triangle or sphere hit (intersector.cu fill_isect;
-// a sphere's shading normal is its geometric normal and it is no emitter).
+// a sphere's shading normal is its normal and it is no emitter).
 UPBP_D void fill_hit(const TriView& tv, const TriHit& h, float3 ray_dir, Isect& r)
 {
     if (h.prim < 0) {
         const int mat = __ldg(&tv.sph_mat[~h.prim]);
-        const float3 nrm = make_float3(h.u, h.v, h.w);
+        const float3 nrm = make_float3(sphere_attribute_component(h.u), sphere_attribute_component(h.v),
+                                       sphere_attribute_component(h.w));
         r.dist = h.t;
         r.mat = mat;
         r.med = c_params.materials[mat].medium;

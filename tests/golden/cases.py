@@ -60,6 +60,15 @@ for _sid, _name in [(0, "abssph"), (1, "isosph"), (2, "mirsphinfisov"), (5, "sss
     CASES[f"predef_{_sid:02d}_{_name}"] = (f"predef:{_sid}", True, PREDEF_ARGS, 1)
 
 
+# Per-pixel tolerance of the parity test where it is not 1e-3: scenes in which
+# every pixel sums many weak light-tracer splats from a scattering global or
+# enclosing medium.  There float rounding (fused multiply-adds on the GPU)
+# changes single contributions, moving pixels by up to 0.3% (1-2% on a few
+# dim ones) while the image sum agrees to 1e-6; the mean bar is tightened to
+# 1e-4 for them instead.
+PIXEL_TOL = {"predef_02_mirsphinfisov": 5e-3, "predef_35_smallsb": 5e-3}
+
+
 def command_line(case: str, scene_path: str) -> list:
     workload = CASES[case][0]
     if workload.startswith("predef:"):

@@ -6,14 +6,16 @@ float rounding (fused multiply-adds on the GPU) flips a comparison; such
 paths show up as a small set of differing pixels.
 
 Bar: vertex/beam counts equal; >= 97% of pixels agree to 1e-3 relative;
-mean image agrees to 5e-3 relative."""
+mean image agrees to 5e-3 relative.  The scenes in cases.PIXEL_TOL (every
+pixel a sum of weak light-tracer splats from a scattering medium) use their
+per-pixel tolerance there and a mean bar of 1e-4."""
 import json
 import os
 
 import numpy as np
 import pytest
 
-from cases import CASES, command_line, prepare
+from cases import CASES, PIXEL_TOL, command_line, prepare
 from gpuupbp_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -21,9 +23,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
-def compare(img, ref):
+def compare(img, ref, tol=1e-3):
     rel = np.abs(img - ref) / (np.abs(ref) + 1e-3)
-    frac = float(np.mean(np.all(rel < 1e-3, axis=-1)))
+    frac = float(np.mean(np.all(rel < tol, axis=-1)))
     mean_rel = float(np.abs(img.mean() - ref.mean()) / (abs(ref.mean()) + 1e-6))
     return frac, mean_rel
 
@@ -42,9 +44,9 @@ def test_image_parity_with_reference(case, scene_dir):
         got = {"vertices": st["light_vertices"], "surface": st["surface_vertices"],
                "medium": st["medium_vertices"], "beams": st["light_beams"]}
         assert got == counts[case][it]
-        frac, mean_rel = compare(img, gold[f"{case}/{it}"])
+        frac, mean_rel = compare(img, gold[f"{case}/{it}"], PIXEL_TOL.get(case, 1e-3))
         assert frac >= 0.97, (case, it, frac, mean_rel)
-        assert mean_rel <= 5e-3, (case, it, frac, mean_rel)
+        assert mean_rel <= (1e-4 if case in PIXEL_TOL else 5e-3), (case, it, frac, mean_rel)
         assert np.isfinite(img).all()
     r.close()
 
@@ -65,8 +67,9 @@ def test_accumulation_is_the_mean_of_iterations(scene_dir):
 
 def test_predefined_scene_without_lights():
     """Predefined scene 10 (a glass sphere of emitting medium, no light): the
-    command line refuses it as the reference's does, the C API renders it.
-    No light subpaths are traced; the medium's emission reaches the camera."""
+    command line refuses it as the reference's does (its camera paths never
+    add medium emission, so the scene renders black), the C API renders it.
+    No light subpaths are traced and nothing fails."""
     import ctypes
     from gpuupbp_b200 import upbp
     L = upbp.load_library()
@@ -82,7 +85,7 @@ def test_predefined_scene_without_lights():
     L.upbp_destroy(ctx)
     L.upbp_scene_free(sc)
     assert st.status == 0 and st.light_vertices == 0 and st.light_beams == 0
-    assert np.isfinite(img).all() and img.max() > 0
+    assert np.isfinite(img).all() and img.max() == 0
 
 
 def test_search_rounds_match_one_round(scene_dir, monkeypatch):
