@@ -22,7 +22,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompiler", "-f
 
 DEVICE_SOURCES = ["upbp_capi.cu"]
 HOST_SOURCES = ["host/upbp_cli.cpp", "host/upbp_scene.cpp", "host/upbp_predef.cpp", "host/upbp_exr.cpp",
-                "host/upbp_sah.cpp"]
+                "host/upbp_exr_read.cpp", "host/upbp_sah.cpp"]
 
 
 def _sources():
@@ -64,7 +64,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if verbose:
                 sys.stderr.write(r.stderr)
             objs.append(obj)
-        _run([NVCC] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", LIB] + objs + ["-lcudart"])
+        _run([NVCC] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", LIB] + objs + ["-lcudart", "-lz"])
         _run([NVCC] + ARCH + FLAGS + ["-o", EXE, "upbp_main.cpp", "-L" + HERE, "-lupbp_b200",
                                       "-Xlinker", "-rpath,$ORIGIN"])
     return LIB

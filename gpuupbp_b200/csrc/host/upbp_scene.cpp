@@ -84,6 +84,8 @@ struct Tri {
 struct AuxLight {
     int type;  // UPBP_LIGHT_*
     float pos[3] = {0, 0, 0}, emission[3] = {0, 0, 0};
+    std::string env_map;  // light_background_em: image file
+    float env_scale = 1.f, env_rotate = 0.f;
 };
 
 std::string dir_of(const std::string& p)
@@ -271,6 +273,42 @@ CameraMatrices camera_setup(const upbp_camera_desc& c, float res_x, float res_y)
 
 }  // namespace upbp_host
 
+namespace upbp_host {
+
+// The environment map of a background light: the image as the reference's
+// tinyexr_wrapper::load_image leaves it (tinyexr_wrapper.cpp:97-136): every
+// pixel times `scale`, columns shifted right by (int)(rotate * width) with
+// wrap-around.  Shifts outside [0, width] are refused (the reference would
+// write outside its image).
+int load_env_map(const std::string& path, float rotate, float scale, upbp_scene& sc)
+{
+    int w = 0, h = 0;
+    std::vector<float> in;
+    std::string err;
+    if (!read_exr_rgb(path, w, h, in, err)) {
+        set_error("environment map: " + err);
+        return UPBP_ERR_IO;
+    }
+    const int rot = (int)(rotate * (float)w);
+    if (rot < 0 || rot > w) {
+        set_error("environment map rotation must lie in [0, 1]");
+        return UPBP_ERR_SCENE;
+    }
+    sc.env_rgb.assign(in.size(), 0.f);
+    for (int j = 0; j < h; j++)
+        for (int i = 0; i < w; i++) {
+            int x = i + rot;
+            if (x >= w) x -= w;
+            for (int k = 0; k < 3; k++)
+                sc.env_rgb[3 * ((size_t)j * w + x) + k] = in[3 * ((size_t)j * w + i) + k] * scale;
+        }
+    sc.env_width = (uint32_t)w;
+    sc.env_height = (uint32_t)h;
+    return UPBP_OK;
+}
+
+}  // namespace upbp_host
+
 void upbp_scene::finalize()
 {
     desc.triangle_count = (uint32_t)tri_material.size();
@@ -284,6 +322,9 @@ void upbp_scene::finalize()
     desc.media = media.data();
     desc.light_count = (uint32_t)lights.size();
     desc.lights = lights.data();
+    desc.env_width = env_width;
+    desc.env_height = env_height;
+    desc.env_rgb = env_rgb.empty() ? nullptr : env_rgb.data();
     desc.sphere_count = (uint32_t)sph_material.size();
     desc.spheres = spheres.data();
     desc.sph_material = sph_material.data();
@@ -482,8 +523,17 @@ extern "C" int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_
                 read3(ss, l.emission);
                 aux_lights.push_back(l);
             } else if (key == "light_background_em") {
-                set_error("environment-map background lights are not supported");
-                return UPBP_ERR_SCENE;
+                // light_background_em <scale> <rotate> <file> (scene_loader_obj.cpp:582-591);
+                // a relative file name is relative to the OBJ file
+                AuxLight l;
+                l.type = UPBP_LIGHT_BACKGROUND;
+                std::string file;
+                if (!(ss >> l.env_scale >> l.env_rotate >> file)) {
+                    set_error("light_background_em needs <scale> <rotate> <file>");
+                    return UPBP_ERR_SCENE;
+                }
+                l.env_map = (file.size() > 1 && (file[1] == ':' || file[0] == '/')) ? file : dir_of(path) + file;
+                aux_lights.push_back(l);
             }
         }
 
@@ -498,7 +548,16 @@ extern "C" int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_
             std::memcpy(L.intensity, al.emission, sizeof(L.intensity));
             std::memcpy(L.position, al.pos, sizeof(L.position));
             if (al.type == UPBP_LIGHT_BACKGROUND) {
-                if (sc->desc.background_light < 0) sc->desc.background_light = (int32_t)sc->lights.size();
+                if (sc->desc.background_light < 0) {
+                    sc->desc.background_light = (int32_t)sc->lights.size();
+                    if (!al.env_map.empty()) {
+                        const int rc = load_env_map(al.env_map, al.env_rotate, al.env_scale, *sc);
+                        if (rc != UPBP_OK) {
+                            delete sc;
+                            return rc;
+                        }
+                    }
+                }
             }
             sc->lights.push_back(L);
         }

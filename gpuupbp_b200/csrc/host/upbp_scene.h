@@ -13,6 +13,8 @@ struct upbp_scene {
     std::vector<float> verts, normals;
     std::vector<int32_t> tri_material, tri_light;
     std::vector<float> spheres;  // centre xyz, radius
+    std::vector<float> env_rgb;  // environment map of the background light
+    uint32_t env_width = 0, env_height = 0;
     std::vector<int32_t> sph_material;
     std::vector<upbp_material> materials;
     std::vector<upbp_medium> media;
@@ -33,6 +35,10 @@ struct CameraMatrices {
 CameraMatrices camera_setup(const upbp_camera_desc& c, float res_x, float res_y);
 
 void set_error(const std::string& msg);
+
+// OpenEXR scanline image (NONE/RLE/ZIPS/ZIP, HALF/FLOAT) as RGB floats.
+bool read_exr_rgb(const std::string& path, int& width, int& height, std::vector<float>& rgb, std::string& err);
+int load_env_map(const std::string& path, float rotate, float scale, upbp_scene& sc);
 
 // The reference's predefined Cornell-box scenes (-s 0..40).
 int predefined_scene_count();

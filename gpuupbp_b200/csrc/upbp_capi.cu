@@ -130,6 +130,9 @@ struct upbp_ctx {
     unsigned ev_pending = 0;                   // iterations recorded since the last stats read
     DMaterial* d_mat = nullptr;
     DMedium* d_med = nullptr;
+    float4* d_env_img = nullptr;   // environment map and its sampling distribution
+    float* d_env_dist = nullptr;
+    float* d_env_row_int = nullptr;
     DLight* d_lights = nullptr;
     Geometry real, imag;
     LightVertexRec* d_vertices = nullptr;
@@ -249,6 +252,69 @@ void init_light(DLight& l, const upbp_light& in)
         l.position = make_float3(in.position[0], in.position[1], in.position[2]);
         l.intensity = I;
     }
+}
+
+// One piecewise-constant 1-D distribution over n values (init_distribution_1d,
+// gpuupbp/host/env_map.hpp): the function, then its cdf normalised by the
+// integral (uniform when the integral is 0); returns the integral.  Same
+// float operations as the reference, so sampling decisions agree.
+float env_distribution_1d(const float* f, int n, float* func, float* cdf)
+{
+    std::memcpy(func, f, (size_t)n * sizeof(float));
+    cdf[0] = 0.f;
+    for (int i = 1; i < n + 1; i++) cdf[i] = cdf[i - 1] + func[i - 1] / n;
+    const float integral = cdf[n];
+    if (integral == 0.f) {
+        for (int i = 1; i < n + 1; i++) cdf[i] = float(i) / float(n);
+    } else {
+        for (int i = 1; i < n + 1; i++) cdf[i] /= integral;
+    }
+    return integral;
+}
+
+// The environment map's image and sampling distribution on the device
+// (convert_image_to_pdf, gpuupbp/host/env_map.hpp): 2 * height columns x
+// height rows of luminance times the sine of the row's polar angle.
+int upload_env_map(upbp_ctx* c, const upbp_scene_desc* s)
+{
+    const int w = (int)s->env_width, h = (int)s->env_height;
+    if (h <= 0 || w < 2 * h) {
+        upbp_host::set_error("environment map must be at least twice as wide as high");
+        return UPBP_ERR_SCENE;
+    }
+    const int nu = 2 * h, nv = h;
+    std::vector<float4> img((size_t)w * h);
+    for (size_t i = 0; i < img.size(); i++)
+        img[i] = make_float4(s->env_rgb[3 * i], s->env_rgb[3 * i + 1], s->env_rgb[3 * i + 2], 0.f);
+    std::vector<float> lum((size_t)nu * nv);
+    for (int r = 0; r < nv; r++) {
+        const float v = (float)(r + .5f) / (float)nv;
+        const float st = std::sin(3.14159265358979323846f * v);
+        for (int col = 0; col < nu; col++) {
+            const float4 p = img[(size_t)r * w + col];
+            lum[(size_t)r * nu + col] = st * (0.212671f * p.x + 0.715160f * p.y + 0.072169f * p.z);
+        }
+    }
+    const size_t row = 2 * (size_t)nu + 1;
+    std::vector<float> dist(row * (nv + 1), 0.f), row_int(nv), marg(nv);
+    for (int r = 0; r < nv; r++)
+        row_int[r] = env_distribution_1d(&lum[(size_t)r * nu], nu, &dist[row * r], &dist[row * r + nu]);
+    for (int r = 0; r < nv; r++) marg[r] = row_int[r];
+    const float marg_int = env_distribution_1d(marg.data(), nv, &dist[row * nv], &dist[row * nv + nu]);
+    UPBP_CK(dupload(&c->d_env_img, img.data(), img.size(), c->st));
+    UPBP_CK(dupload(&c->d_env_dist, dist.data(), dist.size(), c->st));
+    UPBP_CK(dupload(&c->d_env_row_int, row_int.data(), row_int.size(), c->st));
+    DEnvMap& m = c->P.env;
+    m.img = c->d_env_img;
+    m.width = w;
+    m.height = h;
+    m.dist = c->d_env_dist;
+    m.row_int = c->d_env_row_int;
+    m.marg_int = marg_int;
+    m.nu = nu;
+    m.nv = nv;
+    m.norm = .5f * 0.318309886183790671538f * 0.318309886183790671538f;
+    return UPBP_OK;
 }
 
 int upload_geometry(upbp_ctx* c, const upbp_scene_desc* s, bool real, Geometry& g)
@@ -512,6 +578,14 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         for (uint32_t i = 0; i < s->medium_count; i++) init_medium(meds[i], s->media[i]);
         std::vector<DLight> lights(std::max(1u, s->light_count));
         for (uint32_t i = 0; i < s->light_count; i++) init_light(lights[i], s->lights[i]);
+        if (s->env_rgb && s->background_light >= 0 && (uint32_t)s->background_light < s->light_count) {
+            if (upload_env_map(c, s) != UPBP_OK) {
+                upbp_destroy(c);
+                return UPBP_ERR_CUDA;
+            }
+            lights[s->background_light].env = 1;
+            lights[s->background_light].scale = s->lights[s->background_light].scale;
+        }
         UPBP_CK(dupload(&c->d_mat, mats.data(), mats.size(), c->st));
         UPBP_CK(dupload(&c->d_med, meds.data(), meds.size(), c->st));
         UPBP_CK(dupload(&c->d_lights, lights.data(), lights.size(), c->st));
@@ -1309,7 +1383,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     if (!c) return;
     if (c->st) cudaStreamSynchronize(c->st);
     void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
-                    c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
+                    c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,
                     c->d_surf_nodes, c->d_med_nodes, c->d_beam_nodes, c->d_med_qnodes, c->d_beam_qnodes, c->d_surf_pos, c->d_med_pos, c->d_beam_seg,

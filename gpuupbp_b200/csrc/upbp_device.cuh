@@ -60,6 +60,22 @@ struct DLight {
     float3 intensity;       // area/point/directional; background colour * scale
     float inv_area;
     float3 position;        // point light
+    int env;                // background: radiance from the environment map
+    float scale;            // background: scale of the environment map's radiance
+};
+
+// Environment map of the background light (gpuupbp/shared/env_map.h): the
+// image and a piecewise-constant 2-D distribution over 2 * height columns x
+// height rows, row r holding nu function values then nu + 1 cdf values,
+// row nv the marginal over rows.
+struct DEnvMap {
+    const float4* img;      // width x height, rgb
+    int width, height;
+    const float* dist;      // (nv + 1) x (2 nu + 1)
+    const float* row_int;   // integral of each row's function
+    float marg_int;         // integral of the marginal
+    int nu, nv;
+    float norm;             // 1 / (2 pi^2)
 };
 
 struct DCamera {
@@ -284,6 +300,7 @@ struct DeviceParams {
     const DLight* lights;
     int light_count;
     int background_light;
+    DEnvMap env;
     DCamera camera;
     float3 scene_center;
     float scene_radius, inv_radius_sqr;

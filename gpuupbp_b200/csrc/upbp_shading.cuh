@@ -443,6 +443,98 @@ UPBP_D float3 bsdf_sample(const Bsdf& b, float r0, float r1, float r2, float3& d
 
 // ---------------------------------------------------------------- lights
 
+// Environment map (gpuupbp/kernel/env_map.cuh, distribution.cuh): lat-long
+// mapping, bilinear radiance lookup and sampling of the sin-weighted
+// luminance distribution, as piecewise-constant 1-D distributions (a
+// marginal over rows, a conditional per row) inverted by binary search.
+UPBP_D float3 env_dir(float u, float v)
+{
+    const float phi = u * 2.f * kPi, theta = v * kPi;
+    const float st = sinf(theta);
+    return make_float3(-st * cosf(phi), st * sinf(phi), cosf(theta));
+}
+
+UPBP_D float2 env_uv(float3 d)
+{
+    const float phi = (d.x != 0.f || d.y != 0.f) ? atan2f(d.y, d.x) : 0.f;
+    const float theta = acosf(d.z);
+    return make_float2(fminf(fmaxf(.5f - phi * .5f * kInvPi, 0.f), 1.f), fminf(fmaxf(theta * kInvPi, 0.f), 1.f));
+}
+
+UPBP_D float3 env_pixel(const DEnvMap& m, int x, int y) { return xyz(__ldg(&m.img[(size_t)y * m.width + x])); }
+
+UPBP_D float3 env_radiance(const DEnvMap& m, float u, float v)
+{
+    const float xf = u * m.width, yf = v * m.height;
+    const int x1 = min(max((int)xf, 0), m.width - 1), y1 = min(max((int)yf, 0), m.height - 1);
+    const int x2 = x1 == m.width - 1 ? x1 : x1 + 1, y2 = y1 == m.height - 1 ? y1 : y1 + 1;
+    const float tx = xf - (float)x1, ty = yf - (float)y1;
+    return (1.f - ty) * ((1.f - tx) * env_pixel(m, x1, y1) + tx * env_pixel(m, x2, y1)) +
+           ty * ((1.f - tx) * env_pixel(m, x1, y2) + tx * env_pixel(m, x2, y2));
+}
+
+// sin(theta) at the centre of the row holding v
+UPBP_D float env_sin_theta(float v, float height)
+{
+    const float row = v < 1.f ? (float)((int)(v * height)) : height - 1.f;
+    return sinf(kPi * (row + .5f) / height);
+}
+
+// Samples one 1-D distribution of n values (function at f, cdf at f + n... as
+// laid out by the host); returns the continuous coordinate in [0, 1).
+UPBP_D float env_sample_1d(const float* func, const float* cdf, int n, float integral, float u, float& pdf, int& off)
+{
+    int first = 0, len = n + 1;
+    while (len > 0) {  // last cdf entry <= u
+        const int half = len >> 1, mid = first + half;
+        if (__ldg(&cdf[mid]) <= u) {
+            first = mid + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
+    }
+    off = min(max(first - 1, 0), n - 1);
+    const float c0 = __ldg(&cdf[off]), c1 = __ldg(&cdf[off + 1]);
+    float du = u - c0;
+    if (c1 - c0 > 0.f) du /= (c1 - c0);
+    pdf = integral > 0.f ? __ldg(&func[off]) / integral : 0.f;
+    return ((float)off + du) / (float)n;
+}
+
+// Direction sampled from the map, its solid-angle pdf and radiance.
+UPBP_D float3 env_sample(const DEnvMap& m, float u0, float u1, float& pdf_w, float3& radiance)
+{
+    const size_t row = 2 * (size_t)m.nu + 1;
+    const float* marg = m.dist + row * m.nv;
+    float pv, pu;
+    int v;
+    const float fv = env_sample_1d(marg, marg + m.nu, m.nv, m.marg_int, u1, pv, v);
+    int unused;
+    const float* cond = m.dist + row * v;
+    const float fu = env_sample_1d(cond, cond + m.nu, m.nu, __ldg(&m.row_int[v]), u0, pu, unused);
+    pdf_w = m.norm * (pu * pv) / env_sin_theta(fv, (float)m.height);
+    radiance = env_radiance(m, fu, fv);
+    return env_dir(fu, fv);
+}
+
+// Radiance the map sends along -dir (dir points from the scene to the map)
+// and the solid-angle pdf of sampling dir; radiance 0 where that pdf is 0.
+UPBP_D float3 env_lookup(const DEnvMap& m, float3 dir, float& pdf_w)
+{
+    const float2 uv = env_uv(normalize(dir));
+    float3 radiance = env_radiance(m, uv.x, uv.y);
+    const int iu = min(max((int)(uv.x * m.nu), 0), m.nu - 1);
+    const int iv = min(max((int)(uv.y * m.nv), 0), m.nv - 1);
+    const float ri = __ldg(&m.row_int[iv]);
+    const size_t row = 2 * (size_t)m.nu + 1;
+    float p = 0.f;
+    if (ri * m.marg_int != 0.f) p = (__ldg(&m.dist[row * iv + iu]) * __ldg(&m.dist[row * m.nv + iv])) / (ri * m.marg_int);
+    pdf_w = m.norm * p / env_sin_theta(uv.y, (float)m.height);
+    if (pdf_w == 0.f) radiance = v3(0.f);
+    return radiance;
+}
+
 UPBP_D bool light_is_finite(const DLight& l) { return l.type == kLightArea || l.type == kLightPoint; }
 UPBP_D bool light_is_delta(const DLight& l) { return l.type == kLightDirectional || l.type == kLightPoint; }
 
@@ -467,11 +559,17 @@ UPBP_D float3 light_illuminate(const DLight& l, float3 x, float u0, float u1, fl
         return l.intensity;
     }
     case kLightBackground: {
-        dir_to_light = sample_uniform_sphere(u0, u1, &direct_pdf_w);
+        float3 radiance = l.intensity;
+        if (l.env) {
+            dir_to_light = env_sample(c_params.env, u0, u1, direct_pdf_w, radiance);
+            radiance = radiance * l.scale;
+        } else {
+            dir_to_light = sample_uniform_sphere(u0, u1, &direct_pdf_w);
+        }
         dist = kInfinity;
         emission_pdf_w = direct_pdf_w * kInvPi * c_params.inv_radius_sqr;
         cos_at_light = 1.f;
-        return l.intensity;
+        return radiance;
     }
     case kLightDirectional: {
         dir_to_light = -l.frame.z;
@@ -512,7 +610,13 @@ UPBP_D float3 light_emit(const DLight& l, float d0, float d1, float p0, float p1
     }
     case kLightBackground: {
         float fp;
-        dir = sample_uniform_sphere(d0, d1, &fp);
+        float3 radiance = l.intensity;
+        if (l.env) {
+            dir = -env_sample(c_params.env, d0, d1, fp, radiance);
+            radiance = radiance * l.scale;
+        } else {
+            dir = sample_uniform_sphere(d0, d1, &fp);
+        }
         const float2 xy = sample_concentric_disc(p0, p1);
         Frame f;
         f.set_from_z(dir);
@@ -520,7 +624,7 @@ UPBP_D float3 light_emit(const DLight& l, float d0, float d1, float p0, float p1
         emission_pdf_w = fp * kInvPi * c_params.inv_radius_sqr;
         direct_pdf_a = fp;
         cos_light = 1.f;
-        return l.intensity;
+        return radiance;
     }
     case kLightDirectional: {
         const float2 xy = sample_concentric_disc(p0, p1);
@@ -552,10 +656,12 @@ UPBP_D float3 light_radiance(const DLight& l, float3 ray_dir, float& direct_pdf_
         return l.intensity;
     }
     if (l.type == kLightBackground) {
-        const float fp = uniform_sphere_pdf();
+        float fp = uniform_sphere_pdf();
+        float3 radiance = l.intensity;
+        if (l.env) radiance = l.scale * env_lookup(c_params.env, ray_dir, fp);
         direct_pdf_a = fp;
         emission_pdf_w = fp * (kInvPi * c_params.inv_radius_sqr);
-        return l.intensity;
+        return radiance;
     }
     return v3(0.f);
 }

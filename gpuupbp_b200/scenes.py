@@ -129,6 +129,7 @@ class SceneBuilder:
     camera: Camera | None = None
     global_medium: str | None = None
     aux_lights: list = field(default_factory=list)  # AUX light lines (light_point, light_directional, ...)
+    env_map: tuple | None = None  # (H x W x 3 image, scale, rotate): a light_background_em written beside the OBJ
 
     def add(self, material: str, verts, faces, normals=None):
         self.groups.append((material, np.asarray(verts, np.float64), np.asarray(faces, np.int64),
@@ -202,6 +203,11 @@ class SceneBuilder:
                 fa.write(f"globalMediumId {self.global_medium}\n")
             for line in self.aux_lights:
                 fa.write(line + "\n")
+            if self.env_map is not None:
+                img, scale, rotate = self.env_map
+                name = os.path.basename(obj_path) + ".env.exr"
+                write_exr_float(os.path.join(os.path.dirname(obj_path), name), img)
+                fa.write(f"light_background_em {scale} {rotate} {name}\n")
 
 
 def _box_walls(sb: SceneBuilder, rng: np.random.Generator, lo=-0.5, hi=0.5):
@@ -361,7 +367,58 @@ def media_field_lights(seed: int = 2, tiny: bool = False) -> SceneBuilder:
     return sb
 
 
-WORKLOADS = {"box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
+def write_exr_float(path: str, img: np.ndarray):
+    """Writes an (H, W, 3) image as an uncompressed OpenEXR scanline file with
+    FLOAT channels B, G, R (OpenEXR file layout: magic, version, attributes,
+    offset table, one (y, size, B row, G row, R row) block per scanline)."""
+    import struct
+    img = np.ascontiguousarray(img, np.float32)
+    h, w = img.shape[:2]
+
+    def attr(name, typ, data):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(data)) + data
+
+    chl = b"".join(c.encode() + b"\0" + struct.pack("<iB3xii", 2, 0, 1, 1) for c in "BGR") + b"\0"
+    box = struct.pack("<iiii", 0, 0, w - 1, h - 1)
+    hdr = (struct.pack("<ii", 20000630, 2) + attr("channels", "chlist", chl) + attr("compression", "compression", b"\0")
+           + attr("dataWindow", "box2i", box) + attr("displayWindow", "box2i", box)
+           + attr("lineOrder", "lineOrder", b"\0") + attr("pixelAspectRatio", "float", struct.pack("<f", 1.0))
+           + attr("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0))
+           + attr("screenWindowWidth", "float", struct.pack("<f", 1.0)) + b"\0")
+    line = 12 * w
+    start = len(hdr) + 8 * h
+    offsets = struct.pack(f"<{h}Q", *[start + y * (8 + line) for y in range(h)])
+    blocks = b"".join(struct.pack("<ii", y, line) + img[y, :, 2].tobytes() + img[y, :, 1].tobytes()
+                      + img[y, :, 0].tobytes() for y in range(h))
+    with open(path, "wb") as f:
+        f.write(hdr + offsets + blocks)
+
+
+def sky_image(seed: int, width: int = 64) -> np.ndarray:
+    """A seeded lat-long sky (width x width/2): a blue gradient, noise and a
+    bright sun lobe, so importance sampling has a peak to find."""
+    rng = np.random.default_rng(seed)
+    h = width // 2
+    v = (np.arange(h) + 0.5) / h
+    u = (np.arange(width) + 0.5) / width
+    sky = np.zeros((h, width, 3), np.float32)
+    sky[...] = (0.3 + 0.5 * (1 - v))[:, None, None] * np.array([0.5, 0.7, 1.0], np.float32)
+    sky *= (1 + 0.2 * rng.random((h, width, 1))).astype(np.float32)
+    su, sv = rng.uniform(0.2, 0.8), rng.uniform(0.15, 0.35)
+    d2 = ((u[None, :] - su) * 2) ** 2 + (v[:, None] - sv) ** 2
+    sky += (40.0 * np.exp(-d2 / 0.002))[..., None].astype(np.float32) * np.array([1.0, 0.9, 0.7], np.float32)
+    return sky.astype(np.float32)
+
+
+def media_field_env(seed: int = 2, tiny: bool = False) -> SceneBuilder:
+    """The media field under an environment-map sky (light_background_em,
+    scale 0.8, rotated by a quarter turn) beside its area lights."""
+    sb = media_field(seed, tiny)
+    sb.env_map = (sky_image(seed + 100), 0.8, 0.25)
+    return sb
+
+
+WORKLOADS = {"media_field_env": media_field_env, "box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
              "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box}
 
 

@@ -97,6 +97,7 @@ class SceneDesc(ctypes.Structure):
         ("res_x", ctypes.c_uint32), ("res_y", ctypes.c_uint32), ("bbox_min", F3), ("bbox_max", F3),
         ("sphere_count", ctypes.c_uint32), ("spheres", ctypes.POINTER(ctypes.c_float)),
         ("sph_material", ctypes.POINTER(ctypes.c_int32)),
+        ("env_width", ctypes.c_uint32), ("env_height", ctypes.c_uint32), ("env_rgb", ctypes.POINTER(ctypes.c_float)),
     ]
 
 
@@ -199,6 +200,8 @@ def load_scene(args: list[str]) -> dict:
             "lights": recs(d.lights, d.light_count), "global_medium": d.global_medium,
             "background_light": d.background_light,
             "bbox_min": np.array(list(d.bbox_min), np.float32), "bbox_max": np.array(list(d.bbox_max), np.float32),
+            "env": (arr(d.env_rgb, 3 * d.env_width * d.env_height, np.float32).reshape(d.env_height, d.env_width, 3)
+                    if d.env_rgb else None),
         }
     finally:
         L.upbp_scene_free(sc)

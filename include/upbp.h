@@ -155,6 +155,14 @@ typedef struct upbp_scene_desc {
     uint32_t sphere_count;
     const float* spheres;
     const int32_t* sph_material;
+    /* Environment map of the background light `background_light`
+     * (light_background_em, gpuupbp/host/env_map.hpp): env_width x env_height
+     * RGB floats, rows top to bottom, already scaled and rotated as the
+     * reference's loader leaves them; NULL for a constant background.
+     * env_width must be at least 2 * env_height (the reference's sampling
+     * distribution spans 2 * height columns). */
+    uint32_t env_width, env_height;
+    const float* env_rgb;
 } upbp_scene_desc;
 
 #define UPBP_MAX_SPHERES 64

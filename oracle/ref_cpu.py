@@ -53,11 +53,24 @@ def lib():
         L.upbp_ref_describe.restype = ctypes.c_int
         L.upbp_ref_scene_json.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         L.upbp_ref_scene_json.restype = ctypes.c_int
+        L.upbp_ref_save_exr.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int]
+        L.upbp_ref_save_exr.restype = ctypes.c_int
         _lib = L
     return _lib
 
 
 _current = None
+
+
+def save_exr(path: str, rgb, half: bool, compression: int) -> None:
+    """Writes an (H, W, 3) float image with tinyexr's encoder (compression
+    0 none, 1 RLE, 2 ZIPS, 3 ZIP), for tests of the library's EXR reader."""
+    import numpy as np
+    a = np.ascontiguousarray(rgb, np.float32)
+    rc = lib().upbp_ref_save_exr(path.encode(), a.ctypes.data, a.shape[1], a.shape[0], int(half), compression)
+    if rc != 0:
+        raise RuntimeError(f"tinyexr could not write {path} (rc={rc})")
 
 
 class RefRenderer:

@@ -829,6 +829,19 @@ int upbp_ref_scene_json(RefCtx* c, char* buf, int cap)
     f3(sc.scene_sphere.center);
     o += ", \"scene_radius\": ";
     num(sc.scene_sphere.radius);
+    if (sc.has_env_map) {  // the environment map image as the loader left it
+        const Image& im = sc.env_map.img;
+        o += ", \"env\": [";
+        num(im.width);
+        o += ",";
+        num(im.height);
+        o += ",[";
+        for (int i = 0; i < im.width * im.height; i++) {
+            if (i) o += ",";
+            f3(im.data[i]);
+        }
+        o += "]]";
+    }
     o += "}";
     if ((int)o.size() < cap) std::memcpy(buf, o.c_str(), o.size() + 1);
     return (int)o.size() + 1;

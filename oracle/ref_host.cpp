@@ -54,3 +54,42 @@ void oracle_free_setup(OracleSetup* s)
     delete_scene_host(s->scene);
     free(s->records);
 }
+
+// Writes an RGB float image (rows top to bottom) with tinyexr's own encoder:
+// channels B, G, R stored as HALF (half != 0) or FLOAT with the given
+// compression (0 none, 1 RLE, 2 ZIPS, 3 ZIP).  Makes test files for the
+// library's EXR reader.  Returns tinyexr's status (0 on success).
+extern "C" int upbp_ref_save_exr(const char* path, const float* rgb, int w, int h, int half, int compression)
+{
+    std::vector<float> ch[3];
+    for (int k = 0; k < 3; k++) ch[k].resize((size_t)w * h);
+    for (size_t i = 0; i < (size_t)w * h; i++)
+        for (int k = 0; k < 3; k++) ch[k][i] = rgb[3 * i + k];
+    EXRHeader header;
+    InitEXRHeader(&header);
+    EXRImage image;
+    InitEXRImage(&image);
+    float* planes[3] = {ch[2].data(), ch[1].data(), ch[0].data()};  // B, G, R
+    image.images = reinterpret_cast<unsigned char**>(planes);
+    image.num_channels = 3;
+    image.width = w;
+    image.height = h;
+    EXRChannelInfo infos[3];
+    std::memset(infos, 0, sizeof(infos));
+    const char* names[3] = {"B", "G", "R"};
+    int types[3], requested[3];
+    for (int k = 0; k < 3; k++) {
+        std::strncpy(infos[k].name, names[k], 255);
+        types[k] = TINYEXR_PIXELTYPE_FLOAT;
+        requested[k] = half ? TINYEXR_PIXELTYPE_HALF : TINYEXR_PIXELTYPE_FLOAT;
+    }
+    header.num_channels = 3;
+    header.channels = infos;
+    header.pixel_types = types;
+    header.requested_pixel_types = requested;
+    header.compression_type = compression;
+    const char* err = nullptr;
+    const int ret = SaveEXRImageToFile(&image, &header, path, &err);
+    if (err) FreeEXRErrorMessage(err);
+    return ret;
+}

@@ -44,6 +44,8 @@ CASES = {
     "fog_global": ("fog_box", True, ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "32x32"] + BOX_R, 1),
     "lights_tiny": ("media_field_lights", True,
                     ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "48x32"], 1),
+    "env_tiny": ("media_field_env", True, ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "48x32"], 1),
+    "env_bpt": ("media_field_env", True, ["-a", "upbp_bpt", "-l", "6", "-r", "48x32"], 2),
     "dense_beams_tiny": ("dense_beams", True,
                          ["-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "16", "-r", "48x48",
                           "-r_initial_bb1d", "-0.004", "-r_initial_bp2d", "-0.004"], 1),
