@@ -3,7 +3,8 @@
 // CAMERA_FOV in radians, CAMERA_MATERIAL), materials (geometryType, priority,
 // mediumId, mirror, ior, Ke, enclosingMatId), media (absorption, scattering,
 // emission, g, continuation_probability), globalMediumId and the extra lights
-// (light_point, light_directional, light_background_constant).  One area
+// (light_point, light_directional, light_background_constant,
+// light_background_em with its OpenEXR environment map).  One area
 // light per emissive triangle; lights listed in the AUX file come first.
 // Also the camera matrices of gpuupbp/host/camera.hpp:33-76.
 #include <cmath>
