@@ -142,3 +142,26 @@ def test_executable_renders_the_reference_image(scene_dir, tmp_path):
     rel = np.abs(img - ref) / (np.abs(ref) + 1e-3)
     assert float(np.mean(np.all(rel < 2e-3, axis=-1))) >= 0.97
     assert abs(img.mean() - ref.mean()) / (abs(ref.mean()) + 1e-6) <= 5e-3
+
+
+def test_executable_renders_a_predefined_scene(tmp_path):
+    """`upbp -s 21 ...` (three overlapping glass, water and ice spheres under
+    the big area light) without -o: writes the reference's default output
+    name into the working directory, and the image is the golden one up to
+    half precision and the parity bar."""
+    import subprocess
+
+    from gpuupbp_b200 import upbp
+    from test_host_cpu import read_exr_half
+    case = "predef_21_overgwi"
+    args = command_line(case, None)
+    name = upbp.parse_command_line(args).output_name.decode()
+    assert name.startswith("s21_") and name.endswith(".exr")
+    exe = os.path.join(ROOT, "gpuupbp_b200", "upbp")
+    r = subprocess.run([exe] + args, capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    img = read_exr_half(str(tmp_path / name))
+    ref = np.load(os.path.join(GOLDEN, "oracle_images.npz"))[f"{case}/0"].astype(np.float16).astype(np.float32)
+    rel = np.abs(img - ref) / (np.abs(ref) + 1e-3)
+    assert float(np.mean(np.all(rel < 2e-3, axis=-1))) >= 0.97
+    assert abs(img.mean() - ref.mean()) / (abs(ref.mean()) + 1e-6) <= 5e-3
