@@ -214,7 +214,12 @@ int upbp_parse_command_line(int argc, const char** argv, upbp_config* out);
 /* Replaces: SceneLoader::load_from_obj (gpuupbp/misc/scene_loader_obj.cpp:926-1104)
  * with the reference's OBJ+MTL+AUX semantics. */
 int upbp_scene_load_obj(const char* obj_path, uint32_t res_x, uint32_t res_y, upbp_scene** out);
-/* Replaces: SceneLoader::load_predefined (gpuupbp/misc/scene_loader_predef.cpp:126). */
+/* Replaces: SceneLoader::load_predefined (gpuupbp/misc/scene_loader_predef.cpp:126).
+ * Builds predefined scene scene_id (0 .. UPBP_PREDEFINED_SCENES - 1, the
+ * reference's table in gpuupbp/misc/config.cpp:100-548) with the same
+ * records as the reference; UPBP_ERR_ARGS for other ids.  Scenes 3, 4, 9
+ * and 10 (emitting media, which the renderer does not add on camera paths)
+ * are built although the command line refuses them, as the reference's. */
 int upbp_scene_load_predefined(int scene_id, uint32_t res_x, uint32_t res_y, upbp_scene** out);
 const upbp_scene_desc* upbp_scene_get_desc(const upbp_scene* scene);
 void upbp_scene_free(upbp_scene* scene);
