@@ -20,14 +20,17 @@ workload.
 
 `value` is timed with CUDA events on the library's stream, inputs resident;
 `e2e` renders the same iterations through the C ABI and reads every
-iteration's image back into page-locked host memory.  nvidia-smi samples the
-clocks during the timed region.
+iteration's image back into page-locked host memory.  Each is the median of
+three windows of the same K iterations (all windows are in `repeats`).
+nvidia-smi samples the clocks through all six windows.
 
 N > 1 runs under torchrun, one rank per GPU; rank r renders iterations
 r, r+N, ... (iterations are independent given the seed), so the scaling is
 weak; value = all ranks' paths / max over ranks of the timed region.  The
 reference arm times the reference's own render loop compiled for the host
-cores (oracle/_ref/libupbp_ref_cpu.so) on a bounded sample of the workload.
+cores (oracle/_ref/libupbp_ref_cpu.so) on a bounded sample of the workload:
+1/64 of the camera paths with all of the light paths (media field), timed
+from the same iteration index as the B200 arm.
 """
 from __future__ import annotations
 
@@ -43,6 +46,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 SCENE_DIR = os.environ.get("UPBP_SCENE_DIR", "/tmp/upbp_scenes")
+# timed windows of K steps each; value and e2e are their medians
+REPEATS = 3
 RES = (1280, 720)
 TECH = "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d"
 METRIC = "paths/s (camera + light subpaths per second), plain UPBP render iterations"
@@ -282,11 +287,17 @@ def run_b200(args) -> dict | None:
             ms = float(t.item())
         return ms, wall
 
-    ms, wall = timed(timed_iterations, False)
-    clk.stop()
+    # three windows of the same K iterations each, device-timed then end to
+    # end; the clock sampler runs through all of them
+    runs = [timed(timed_iterations, False) for _ in range(REPEATS)]
     st = r.stats()
-    ms_e2e, wall_e2e = timed(timed_iterations, True)
+    runs_e2e = [timed(timed_iterations, True) for _ in range(REPEATS)]
     st_e2e = r.stats()
+    clk.stop()
+    ms = statistics.median(m for m, _ in runs)
+    ms_e2e = statistics.median(m for m, _ in runs_e2e)
+    wall = statistics.median(w for _, w in runs)
+    wall_e2e = statistics.median(w for _, w in runs_e2e)
 
     # final reduction of the accumulated images over ranks (output time, untimed)
     if pg is not None:
@@ -336,7 +347,10 @@ def run_b200(args) -> dict | None:
                      "traffic": traffic, "algorithmic_bytes_per_launch": b_top, "launch_ms": top_ms},
         "iteration_roofline": iteration_roofline,
         "kernels": kernels,
-        "clocks": clk.summary(window[0], window[1]),
+        "clocks": clk.summary(window[0], window[-1]),
+        "repeats": {"windows": REPEATS, "ms_per_step": [m / args.steps for m, _ in runs],
+                    "e2e_ms_per_step": [m / args.steps for m, _ in runs_e2e],
+                    "statistic": "median of the windows"},
         "passes_ms": {"light": st["ms_light_sum"] / max(1, st["timed_iterations"]),
                       "build": st["ms_build_sum"] / max(1, st["timed_iterations"]), "camera": cam_ms},
         "work": st["work"], "queries": {"segment": st["segment_queries"], "point": st["point_queries"],
@@ -347,24 +361,40 @@ def run_b200(args) -> dict | None:
     return out
 
 
-def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iters: int | None = None,
-                         workload: str = "media_field") -> dict:
-    """Times the reference's render loop on host cores on a bounded sample of
-    the workload: the same scene, estimators and path length at 1/8 of the
-    width and height (1/64 of the pixels, one light path per pixel).
-    Iterations run until `seconds` have been timed or `max_iters` iterations
-    were timed."""
-    sys.path.insert(0, os.path.join(HERE, "oracle"))
-    import ref_cpu
+def reference_sample_args(workload: str) -> tuple[list[str], tuple[int, int], int]:
+    """Command line of the reference's CPU sample of a workload: 1/8 of the
+    width and height (1/64 of the camera paths).  On the media field it keeps
+    every light path of the full-size workload (-pcpi = its pixel count),
+    so photon, beam and query densities are the benchmark's own.  The dense
+    beams keep 1/64 of the light paths (and of -pbc): at full density one
+    iteration of its CPU build takes minutes (86 s at 48x27 on 8 threads)."""
     from gpuupbp_b200 import scenes
 
     scene = scenes.write_workload(workload, SCENE_DIR)
     full = WORKLOADS[workload][0]
     res = (full[0] // 8, full[1] // 8)
     args = workload_args(scene, res, workload)
-    if "-pbc" in args:  # the same fraction of beam-storing light paths
-        i = args.index("-pbc") + 1
-        args[i] = str(max(1, int(float(args[i]) / 64)))
+    if workload == "media_field":
+        light_paths = full[0] * full[1]
+        args += ["-pcpi", str(light_paths)]
+    else:
+        light_paths = res[0] * res[1]
+        if "-pbc" in args:  # the same fraction of beam-storing light paths
+            i = args.index("-pbc") + 1
+            args[i] = str(max(1, int(float(args[i]) / 64)))
+    return args, res, light_paths
+
+
+def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iters: int | None = None,
+                         workload: str = "media_field") -> dict:
+    """Times the reference's render loop on host cores on a bounded sample of
+    the workload (reference_sample_args).  Iterations 0 .. warmup-1 run
+    untimed; the timed ones start at iteration `warmup`, as the B200 arm's
+    do, and run until `seconds` have been timed or `max_iters` iterations."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import ref_cpu
+
+    args, res, light_paths = reference_sample_args(workload)
     r = ref_cpu.RefRenderer(args, threads=threads)
     for w in range(warmup):
         r.run_iteration(w)
@@ -379,8 +409,9 @@ def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iter
     paths = (res[0] * res[1] + st["light_paths"]) * n
     r.close()
     return {"value": paths / t, "unit": "paths/s", "cores": threads, "kind": "reference",
-            "sample": f"{workload} scene at {res[0]}x{res[1]} (1/64 of the pixels), {n} timed iteration(s), "
-                      f"{t:.1f} s on {threads} host threads"}
+            "sample": f"{workload} scene at {res[0]}x{res[1]} (1/64 of the camera paths) with "
+                      f"{st['light_paths']} light paths per iteration, iterations {warmup}..{it - 1} timed "
+                      f"({t:.1f} s on {threads} host threads)"}
 
 
 def main():
@@ -410,8 +441,8 @@ def main():
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "paths/s", "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                          "config": {"workload": f"{args.workload} (reference CPU build, 1/64-pixel sample per "
-                                                 "step)"},
+                          "config": {"workload": f"{args.workload} (reference CPU build; per step one iteration "
+                                                 "of the sample in cpu_baseline.sample)"},
                           "cpu_baseline": s2, "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0,
                                                       "d2h_bytes_per_step": 0}}))
         return
@@ -420,7 +451,8 @@ def main():
         return
     if not args.no_cpu_baseline and world == 1:
         try:
-            out["cpu_baseline"] = run_reference_sample(args.cpu_seconds, threads, workload=args.workload)
+            out["cpu_baseline"] = run_reference_sample(args.cpu_seconds, threads, warmup=args.warmup,
+                                                       workload=args.workload)
         except Exception as e:  # the oracle build is absent
             out["cpu_baseline"] = {"value": None, "unit": "paths/s", "cores": threads, "kind": "reference",
                                    "sample": f"unavailable: {e}"}

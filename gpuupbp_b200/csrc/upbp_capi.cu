@@ -45,6 +45,64 @@ namespace {
         }                                                                                          \
     } while (0)
 
+// Makes device `dev` current for the scope of an entry point and restores
+// the caller's device after it: every call works on the device its context
+// was created on, whichever device the calling thread has current.
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != dev) err_ = cudaSetDevice(dev);
+        else prev_ = dev;
+        dev_ = dev;
+    }
+    ~DeviceGuard()
+    {
+        if (prev_ != dev_) cudaSetDevice(prev_);
+    }
+    cudaError_t error() const { return err_; }
+
+  private:
+    int prev_ = 0, dev_ = 0;
+    cudaError_t err_ = cudaSuccess;
+};
+
+// The launch-parameter bank (c_params, c_work) exists once per device and
+// process.  Contexts on one device take turns on it: a call that uploads
+// parameters holds the device's bank lock on the host for its whole
+// duration, makes its stream wait for the last use of the bank by another
+// context (an event on that context's stream), and records the event after
+// its own launches.  So contexts may be driven from several host threads;
+// their GPU work on the bank is serialised, never interleaved.
+constexpr int kMaxDevices = 64;
+struct ParamBank {
+    std::mutex mu;
+    cudaEvent_t last = nullptr;   // recorded after the latest use, on that user's stream
+    const void* owner = nullptr;  // context of the latest use
+};
+ParamBank g_bank[kMaxDevices];
+
+class BankUse {
+  public:
+    BankUse(const void* ctx, int dev, cudaStream_t st) : b_(g_bank[dev]), lk_(b_.mu), ctx_(ctx), st_(st)
+    {
+        if (b_.owner && b_.owner != ctx && b_.last) err_ = cudaStreamWaitEvent(st, b_.last, 0);
+    }
+    ~BankUse()
+    {
+        if (b_.last) cudaEventRecord(b_.last, st_);
+        b_.owner = ctx_;
+    }
+    cudaError_t error() const { return err_; }
+
+  private:
+    ParamBank& b_;
+    std::lock_guard<std::mutex> lk_;
+    const void* ctx_;
+    cudaStream_t st_;
+    cudaError_t err_ = cudaSuccess;
+};
+
 template <class T>
 cudaError_t dalloc(T** p, size_t n)
 {
@@ -76,7 +134,7 @@ cudaError_t dupload(T** p, const T* h, size_t n, cudaStream_t st)
 // Query record: x y z dx dy dz tmin tmax (points use x y z only).
 __global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* counts, unsigned* ids, unsigned cap)
 {
-    begin_kernel(kKernLight);
+    begin_kernel(kKernDebug);
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const DeviceParams& p = c_params;
@@ -125,7 +183,11 @@ struct Geometry {
 struct upbp_ctx {
     upbp_config cfg{};
     DeviceParams P{};
+    int dev = 0;                              // device the context was created on
     cudaStream_t st = nullptr;
+    unsigned* h_status = nullptr;             // page-locked copy of the iteration's status word
+    unsigned status_seen = 0;                 // OR of every iteration's status bits
+    unsigned char* static_scratch = nullptr;  // device address of the no-allocation query array
     cudaEvent_t ev_ring[kEventRing][kEvPerIter] = {};
     unsigned ev_pending = 0;                   // iterations recorded since the last stats read
     DMaterial* d_mat = nullptr;
@@ -523,6 +585,24 @@ int ensure_hits(upbp_ctx* c, size_t n)
 
 }  // namespace
 
+// ---- neighbour-set query without device allocation --------------------
+// upbp_debug_query stages the queries, counts and ids in buffers it
+// allocates and frees on every call.  Some callers cannot do that: a host
+// application that gives the renderer a fixed device-memory budget at
+// creation, or one whose other streams must not be stalled by the
+// device-wide synchronisation cudaFree implies.  upbp_debug_query_static
+// stages everything in one statically allocated device array instead.  The
+// array is shared by every call in the process: two calls whose copies or
+// kernels overlap on the GPU overwrite each other's data, so callers
+// serialise them.
+constexpr unsigned kStaticQueryMax = 4096;  // queries per call
+constexpr unsigned kStaticIdsMax = 256;     // ids per query
+constexpr size_t kStaticQueryBytes = (size_t)kStaticQueryMax * 8 * sizeof(float);
+constexpr size_t kStaticCountBytes = (size_t)kStaticQueryMax * sizeof(unsigned);
+constexpr size_t kStaticIdBytes = (size_t)kStaticQueryMax * kStaticIdsMax * sizeof(unsigned);
+// About 4.2 MB; every GPU that loads the library holds it until exit.
+static __device__ __align__(256) unsigned char g_query_scratch[kStaticQueryBytes + kStaticCountBytes + kStaticIdBytes];
+
 extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upbp_ctx** out)
 {
     return upbp_host::abi_guard([&]() -> int {
@@ -554,10 +634,32 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
                 return UPBP_ERR_SCENE;
             }
         }
+        int dev = 0;
+        UPBP_CK(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) {
+            upbp_host::set_error("device index beyond the library's limit of " + std::to_string(kMaxDevices));
+            return UPBP_ERR_NO_DEVICE;
+        }
+        {
+            ParamBank& b = g_bank[dev];
+            std::lock_guard<std::mutex> lk(b.mu);
+            if (!b.last) UPBP_CK(cudaEventCreateWithFlags(&b.last, cudaEventDisableTiming));
+        }
         upbp_ctx* c = new upbp_ctx();
         c->cfg = *cfg;
+        c->dev = dev;
         DeviceParams& P = c->P;
         UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        UPBP_CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_status), sizeof(unsigned)));
+        *c->h_status = 0;
+        {
+            // Set-up of the no-allocation query (upbp_debug_query_static):
+            // the static array's device address on this device.  Its host-side
+            // symbol is only a stand-in and must never reach a kernel.
+            void* ptr = nullptr;
+            UPBP_CK(cudaGetSymbolAddress(&ptr, g_query_scratch));
+            c->static_scratch = static_cast<unsigned char*>(ptr);
+        }
         for (auto& slot : c->ev_ring)
             for (auto& e : slot) UPBP_CK(cudaEventCreate(&e));
 
@@ -714,7 +816,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         UPBP_CK(dalloc(&c->d_fb, npx));
         UPBP_CK(dalloc(&c->d_acc, npx));
         UPBP_CK(dalloc(&c->d_status, 1));
-        UPBP_CK(dalloc(&c->d_work, (size_t)kKernCount * kCtrCount));
+        UPBP_CK(dalloc(&c->d_work, (size_t)kKernRows * kCtrCount));
         UPBP_CK(dalloc(&c->d_qcount, 8));
         UPBP_CK(dalloc(&c->d_hit_state, 1));
         UPBP_CK(dalloc(&c->d_work_saved, kCtrCount));
@@ -725,8 +827,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         }
         UPBP_CK(dalloc(&c->d_cam_fb, npx));
         {
-            int dev = 0, sms = 0, per_sm = 0;
-            UPBP_CK(cudaGetDevice(&dev));
+            int sms = 0, per_sm = 0;
             UPBP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             const void* search[kRangeModes] = {(const void*)range_search_kernel<kModePb2d>,
                                                (const void*)range_search_kernel<kModeBb1d>,
@@ -810,6 +911,10 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
 {
     return upbp_host::abi_guard([&]() -> int {
         if (!c || iteration < 0) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        BankUse bank(c, c->dev, c->st);
+        UPBP_CK(bank.error());
         DeviceParams& P = c->P;
         const upbp_config& cfg = c->cfg;
         const unsigned L = P.light_subpath_count;
@@ -818,6 +923,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(cudaEventRecord(ev[0], c->st));
         UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
         UPBP_CK(cudaMemsetAsync(c->d_work, 0, (size_t)kKernCount * kCtrCount * sizeof(unsigned long long), c->st));
+        UPBP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->st));  // this iteration's status bits
         unsigned launches = 0;
         size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
         P.work = c->d_work;
@@ -1146,13 +1252,19 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                                                                              (unsigned)npx);
         launches++;
         UPBP_CK(cudaEventRecord(ev[12], c->st));
+        // the iteration's device status bits, returned as the reference's
+        // run_iteration reports its failed paths (renderer.cpp:171-195)
+        d2h += sizeof(unsigned);
+        UPBP_CK(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         c->launches = launches;
         c->h2d_iter = h2d;
         c->d2h_iter = d2h;
         UPBP_CK(cudaGetLastError());
+        UPBP_CK(cudaStreamSynchronize(c->st));
         c->iterations++;
         c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
-        return UPBP_OK;
+        c->status_seen |= *c->h_status;
+        return (int)*c->h_status;
     });
 }
 
@@ -1160,6 +1272,8 @@ extern "C" int upbp_accumulate_to_host(upbp_ctx* c, float* rgb, double scale)
 {
     return upbp_host::abi_guard([&]() -> int {
         if (!c || !rgb) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
         const size_t n = (size_t)c->P.screen_pixel_count * 3;
         std::vector<double> tmp(n);
         UPBP_CK(cudaMemcpyAsync(tmp.data(), c->d_acc, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -1173,6 +1287,8 @@ extern "C" int upbp_read_iteration(upbp_ctx* c, float* rgb)
 {
     return upbp_host::abi_guard([&]() -> int {
         if (!c || !rgb) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
         const size_t n = (size_t)c->P.screen_pixel_count * 3;
         UPBP_CK(cudaMemcpyAsync(rgb, c->d_fb, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaStreamSynchronize(c->st));
@@ -1184,10 +1300,11 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
 {
     return upbp_host::abi_guard([&]() -> int {
         if (!c || !o) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
         std::memset(o, 0, sizeof(*o));
         UPBP_CK(cudaStreamSynchronize(c->st));
-        unsigned status = 0;
-        UPBP_CK(cudaMemcpy(&status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        const unsigned status = c->status_seen;
         o->light_vertices = c->h_counters[0];
         o->surface_vertices = c->h_counters[1];
         o->medium_vertices = c->h_counters[2];
@@ -1254,6 +1371,8 @@ extern "C" int upbp_debug_photons(upbp_ctx* c, int kind, float* out, uint32_t ca
 {
     return upbp_host::abi_guard([&]() -> int {
         if (!c || !count || kind < 0 || kind > 2) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
         UPBP_CK(cudaStreamSynchronize(c->st));
         if (kind < 2) {
             const PointMap& m = kind == 0 ? c->P.surf_map : c->P.med_map;
@@ -1291,15 +1410,23 @@ extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uin
     return upbp_host::abi_guard([&]() -> int {
         if (!c || !queries || !counts || kind < 0 || kind > 4) return UPBP_ERR_ARGS;
         if (n == 0) return UPBP_OK;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
         float* dq = nullptr;
         unsigned *dc = nullptr, *di = nullptr;
         UPBP_CK(dalloc(&dq, 8 * (size_t)n));
         UPBP_CK(dalloc(&dc, n));
         UPBP_CK(dalloc(&di, (size_t)n * std::max(1u, ids_per_query)));
         UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
-        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
-        k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
-        UPBP_CK(cudaGetLastError());
+        {
+            BankUse bank(c, c->dev, c->st);
+            UPBP_CK(bank.error());
+            unsigned long long* w = c->d_work;  // the query counts into its own row (kKernDebug)
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
+            k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
+            UPBP_CK(cudaGetLastError());
+        }
         UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         if (ids && ids_per_query)
             UPBP_CK(cudaMemcpyAsync(ids, di, (size_t)n * ids_per_query * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
@@ -1310,28 +1437,6 @@ extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uin
         return UPBP_OK;
     });
 }
-
-// ---- neighbour-set query without device allocation --------------------
-// upbp_debug_query stages the queries, counts and ids in buffers it
-// allocates and frees on every call.  Some callers cannot do that: a host
-// application that gives the renderer a fixed device-memory budget at
-// creation, or one whose other streams must not be stalled by the
-// device-wide synchronisation cudaFree implies.  This variant stages
-// everything in one statically allocated device array instead.  The array
-// is shared by every call in the process: two calls whose copies or kernels
-// overlap on the GPU overwrite each other's data, so callers serialise them.
-constexpr unsigned kStaticQueryMax = 4096;  // queries per call
-constexpr unsigned kStaticIdsMax = 256;     // ids per query
-constexpr size_t kStaticQueryBytes = (size_t)kStaticQueryMax * 8 * sizeof(float);
-constexpr size_t kStaticCountBytes = (size_t)kStaticQueryMax * sizeof(unsigned);
-constexpr size_t kStaticIdBytes = (size_t)kStaticQueryMax * kStaticIdsMax * sizeof(unsigned);
-// About 4.2 MB; every GPU that loads the library holds it until exit.
-static __device__ __align__(256) unsigned char g_query_scratch[kStaticQueryBytes + kStaticCountBytes + kStaticIdBytes];
-
-namespace {
-std::mutex g_scratch_mu;
-unsigned char* g_scratch_addr[64] = {};  // device address of g_query_scratch, per device
-}  // namespace
 
 extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queries, uint32_t n, uint32_t* counts,
                                        uint32_t* ids, uint32_t ids_per_query)
@@ -1344,21 +1449,11 @@ extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queri
             return UPBP_ERR_ARGS;
         }
         if (n == 0) return UPBP_OK;
-        int dev = 0;
-        UPBP_CK(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= 64) return UPBP_ERR_ARGS;
-        unsigned char* base = nullptr;
-        {
-            // first call on a device: resolve the array's device address (the
-            // host-side symbol is only a stand-in and must never reach a kernel)
-            std::lock_guard<std::mutex> lk(g_scratch_mu);
-            if (!g_scratch_addr[dev]) {
-                void* ptr = nullptr;
-                UPBP_CK(cudaGetSymbolAddress(&ptr, g_query_scratch));
-                g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
-            }
-            base = g_scratch_addr[dev];
-        }
+        // the context's device, whose address of the array upbp_create
+        // resolved; the kernel and copies run on the context's stream there
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        unsigned char* base = c->static_scratch;
         float* dq = reinterpret_cast<float*>(base);
         unsigned* dc = reinterpret_cast<unsigned*>(base + kStaticQueryBytes);
         unsigned* di = reinterpret_cast<unsigned*>(base + kStaticQueryBytes + kStaticCountBytes);
@@ -1366,9 +1461,15 @@ extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queri
         UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
         // the array keeps the previous call's ids; clear this call's id slots
         if (id_bytes) UPBP_CK(cudaMemsetAsync(di, 0, id_bytes, c->st));
-        UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
-        k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
-        UPBP_CK(cudaGetLastError());
+        {
+            BankUse bank(c, c->dev, c->st);
+            UPBP_CK(bank.error());
+            unsigned long long* w = c->d_work;  // the query counts into its own row (kKernDebug)
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
+            k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
+            UPBP_CK(cudaGetLastError());
+        }
         UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         if (ids && id_bytes) UPBP_CK(cudaMemcpyAsync(ids, di, id_bytes, cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaStreamSynchronize(c->st));
@@ -1378,10 +1479,20 @@ extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queri
 
 extern "C" void* upbp_get_stream(upbp_ctx* c) { return c ? (void*)c->st : nullptr; }
 
+extern "C" int upbp_get_device(const upbp_ctx* c) { return c ? c->dev : UPBP_ERR_ARGS; }
+
 extern "C" void upbp_destroy(upbp_ctx* c)
 {
     if (!c) return;
+    DeviceGuard dg(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
+    {
+        // the parameter bank no longer needs to wait for this context
+        ParamBank& b = g_bank[c->dev];
+        std::lock_guard<std::mutex> lk(b.mu);
+        if (b.owner == c) b.owner = nullptr;
+    }
+    if (c->h_status) cudaFreeHost(c->h_status);
     void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,

@@ -401,10 +401,12 @@ struct DeviceParams {
 enum : unsigned { kEvSegment = 1u, kEvNee = 2u, kEvBpt = 3u, kEvPoint = 255u };
 UPBP_HD unsigned event_key(unsigned bounce, unsigned step) { return bounce * 256u + step; }
 
-// Launch parameters of the running pass, uploaded before each launch.
+// Launch parameters of the running pass, uploaded before each launch.  One
+// bank per device: the host orders the uploads of different contexts on it
+// (ParamBank in upbp_capi.cu).
 __constant__ DeviceParams c_params;
-// Work counters of every kernel kind (kKernCount sets of kCtrCount), set
-// once per iteration.  Each counting kernel records its kind in shared
+// Work counters of every kernel kind (kKernRows sets of kCtrCount), set
+// before each pass.  Each counting kernel records its kind in shared
 // memory at entry, so kernels of different kinds may run concurrently.
 __constant__ unsigned long long* c_work;
 __shared__ int s_kernel_kind;
@@ -419,10 +421,12 @@ UPBP_D void begin_kernel(int kind)
 
 UPBP_D unsigned long long* c_work_ptr() { return c_work + (size_t)s_kernel_kind * kCtrCount; }
 
-// Kernel kinds of an iteration, for work counters and timing.
+// Kernel kinds of an iteration, for work counters and timing.  The
+// diagnostic neighbour queries count into a row of their own after the
+// iteration's rows (kKernDebug), so they never change an iteration's figures.
 enum : int {
     kKernLight = 0, kKernCameraExtend, kKernPb2d, kKernBb1d, kKernSurf, kKernPp3d, kKernBp2d, kKernNee, kKernBpt,
-    kKernCount
+    kKernCount, kKernDebug = kKernCount, kKernRows
 };
 
 }  // namespace upbp

@@ -57,14 +57,14 @@ int main(int argc, const char** argv)
         for (;;) {
             const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             if (el >= cfg.max_time) break;
-            if (upbp_run_iteration(ctx, iter) != UPBP_OK) break;
+            if (upbp_run_iteration(ctx, iter) < 0) break;  // > 0: status bits, the image is complete
             iter++;
             continuous(iter);
         }
     } else {
         int percent = -1;
         for (iter = 0; iter < cfg.iteration_count; iter++) {
-            if (upbp_run_iteration(ctx, iter) != UPBP_OK) {
+            if (upbp_run_iteration(ctx, iter) < 0) {  // > 0: status bits, the image is complete
                 std::fprintf(stderr, "iteration %d: %s\n", iter, upbp_last_error());
                 break;
             }

@@ -422,12 +422,23 @@ WORKLOADS = {"media_field_env": media_field_env, "box_medium": box_medium, "medi
              "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box}
 
 
+# Version of the generators' output: a change to any generator that changes
+# the files it writes must bump it, so that no directory serves files an
+# older generator left there.
+GENERATOR_VERSION = 2
+
+
 def write_workload(name: str, out_dir: str, seed: int | None = None, tiny: bool = False) -> str:
-    """Writes the named workload into out_dir and returns the .obj path."""
+    """Writes the named workload into out_dir and returns the .obj path.
+
+    The file name carries the workload, its size, the seed (`d` for the
+    workload's default) and the generator version, so files written for
+    other arguments or by another generator version are never reused."""
     os.makedirs(out_dir, exist_ok=True)
     fn = WORKLOADS[name]
-    sb = fn(tiny=tiny) if seed is None else fn(seed=seed, tiny=tiny)
-    path = os.path.join(out_dir, f"{name}{'_tiny' if tiny else ''}.obj")
+    stem = f"{name}{'_tiny' if tiny else ''}_s{'d' if seed is None else int(seed)}_g{GENERATOR_VERSION}"
+    path = os.path.join(out_dir, stem + ".obj")
     if not os.path.exists(path) or not os.path.exists(path + ".aux"):
-        sb.write(path)
+        sb = fn(tiny=tiny) if seed is None else fn(seed=seed, tiny=tiny)
+        sb.write(path)  # the .aux file, written last, marks a complete set
     return path

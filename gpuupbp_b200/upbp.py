@@ -112,7 +112,7 @@ WORK_NAMES = ["nodes", "tris", "rays", "point_cand", "point_hit", "beam_cand", "
 EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_predefined", "upbp_scene_get_desc",
            "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
            "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
-           "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static"]
+           "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device"]
 
 _lib = None
 
@@ -141,6 +141,7 @@ def load_library(path: str = LIB_PATH):
     L.upbp_write_exr.argtypes = [ctypes.c_char_p, VP, ctypes.c_uint32, ctypes.c_uint32]
     L.upbp_get_stream.argtypes = [VP]
     L.upbp_get_stream.restype = VP
+    L.upbp_get_device.argtypes = [VP]
     L.upbp_last_error.restype = ctypes.c_char_p
     L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]
     L.upbp_debug_query.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
@@ -225,9 +226,16 @@ class Renderer:
         self.width, self.height = c.res_x, c.res_y
         self.iterations = 0
 
-    def run_iteration(self, iteration: int):
-        _check(load_library().upbp_run_iteration(self._ctx, iteration), f"iteration {iteration}")
+    def run_iteration(self, iteration: int) -> int:
+        """Renders one iteration; returns its device status bits (0, or
+        UPBP_STATUS_* bits for paths ended early or beams dropped, as the
+        reference ends or drops them; the image is complete either way)."""
+        rc = load_library().upbp_run_iteration(self._ctx, iteration)
+        if rc < 0:
+            _check(rc, f"iteration {iteration}")
         self.iterations += 1
+        self.last_status = rc
+        return rc
 
     def iteration_image(self, out: np.ndarray | None = None) -> np.ndarray:
         """The last iteration's image, (H, W, 3) float32: a new array, or

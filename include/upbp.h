@@ -11,10 +11,19 @@
  * (gpuupbp/misc/scene_loader.hpp:44-76).  Each entry point below names the
  * reference interface it replaces.  Plain pointers and sizes only.
  *
- * Return codes: 0 ok; > 0 device status bits (UPBP_STATUS_*); < 0 host or
- * CUDA errors (UPBP_ERR_*).  No exception crosses the ABI.
- * Threading: one context per host thread; the caller owns host buffers, the
- * library owns device memory.
+ * Return codes: 0 ok; < 0 host or CUDA errors (UPBP_ERR_*);
+ * upbp_run_iteration returns > 0 when the iteration set device status bits
+ * (UPBP_STATUS_*: paths that the reference, too, ends early or beams it
+ * drops), and the iteration's image is complete all the same.  No
+ * exception crosses the ABI.
+ * Devices and threads: a context belongs to the device that was current at
+ * upbp_create; every entry point works on that device, whichever device the
+ * calling thread has current (and leaves the caller's current device as it
+ * was).  A context is driven by one host thread at a time; several contexts
+ * may be driven from several threads.  Contexts on one device share one
+ * launch-parameter bank, so the library runs their iterations one after the
+ * other on the GPU (a call waits for another context's call in progress).
+ * The caller owns host buffers, the library owns device memory.
  */
 #ifndef UPBP_B200_H
 #define UPBP_B200_H
@@ -233,7 +242,10 @@ void upbp_scene_free(upbp_scene* scene);
  * UPBP_ERR_CUDA ("range search made no progress"). */
 int upbp_create(const upbp_scene_desc* scene, const upbp_config* config, upbp_ctx** out);
 /* Replaces: Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
- * Renders iteration `iteration` and adds it to the device accumulation. */
+ * Renders iteration `iteration` and adds it to the device accumulation.
+ * Synchronous like the reference's: returns when the iteration's work on
+ * the device is done, with UPBP_OK, the iteration's UPBP_STATUS_* bits
+ * (> 0; upbp_stats.status keeps the OR over all iterations), or an error. */
 int upbp_run_iteration(upbp_ctx* ctx, int iteration);
 /* Replaces the D->H framebuffer copy + add_framebuffer of run_iteration
  * (renderer.cpp:381-392): adds scale * (device accumulation) into rgb. */
@@ -271,9 +283,10 @@ int upbp_debug_query(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, 
  * cudaFree).  No counterpart in the reference.  Allocates nothing: queries,
  * counts and ids are staged in one static device array of about 4.2 MB that
  * every GPU loading the library holds until exit.  Limits: n <= 4096 queries
- * and ids_per_query <= 256, otherwise UPBP_ERR_ARGS.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture.  All calls share the array:
+ * and ids_per_query <= 256, otherwise UPBP_ERR_ARGS.  The array's device
+ * address on the context's device is looked up once, in upbp_create (so a
+ * context created after a cudaDeviceReset gets the new one); the call
+ * itself resolves nothing.  All calls share the array:
  * calls that overlap on the GPU (several threads, or contexts on one device)
  * race and must be serialised by the caller.  Nothing in the array has to
  * start at zero: every call writes all n counts and clears its own n x
@@ -285,6 +298,8 @@ int upbp_debug_query_static(upbp_ctx* ctx, int kind, const float* queries, uint3
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */
 void* upbp_get_stream(upbp_ctx* ctx);
+/* The device index the context was created on (UPBP_ERR_ARGS for NULL). */
+int upbp_get_device(const upbp_ctx* ctx);
 
 const char* upbp_last_error(void);
 

@@ -1,0 +1,96 @@
+"""Parity at the benchmark configurations' real geometry and light-path
+density: the GPU renderer against the reference's own render loop compiled
+for the host cores (oracle/_ref), both run here on the same scene files,
+command line and random stream.
+
+* media_field_full: the 1.64M-triangle media field (20 displaced
+  icospheres of 81 920 triangles, path length 12, BPT and all five
+  estimators) with all 921 600 light paths of the 1280x720 benchmark, on a
+  160x90 camera, iterations 0 and 1.  Photon, beam and query densities are
+  the benchmark's; only the number of camera paths is smaller.  Rays that
+  cross more than eight imaginary boundaries end their path with
+  UPBP_STATUS_INTERSECTION_STACK in both programs every iteration.
+* box_256: the 256x256 box with the icosphere medium (subdivision 3, BPT +
+  SURF + PP3D + PB2D + BB1D, path length 8) at iterations 0, 7 and 15 of the
+  radius schedule.
+* dense_beams_crop: the 0.5M-triangle dense-beam enclosure with all
+  2 073 600 light paths of the 1920x1080 workload (path length 16, about 7M
+  beams and 10M photons), BB1D over the first 600 000 light paths, on a
+  32x18 camera.
+
+Per iteration: the light-vertex, surface, medium and beam counts equal; the
+device status bits equal the reference's failed-path codes (the reference
+counts RETURN_WITH_ERR codes, the GPU sets one bit per code); pixels agree
+as the small parity cases do (PIXEL_BAR of pixels within 1e-3 relative,
+image mean within MEAN_BAR).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from gpuupbp_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+BOX_R = ["-r_initial", "-0.02", "-r_alpha", "0.75"]
+ALL6 = "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d"
+
+# name: (workload, command line without the scene, iterations, pixel bar, mean bar)
+FULL = {
+    "media_field_full": ("media_field", ["-a", ALL6, "-l", "12", "-r", "160x90", "-pcpi", "921600"], [0, 1],
+                         0.99, 1e-3),
+    "box_256": ("box_medium", ["-a", "upbp_all", "-l", "8", "-r", "256x256"] + BOX_R, [0, 7, 15], 0.99, 1e-3),
+    "dense_beams_crop": ("dense_beams", ["-a", ALL6, "-l", "16", "-r", "32x18", "-pcpi", "2073600",
+                                         "-r_initial_bb1d", "-0.004", "-r_initial_bp2d", "-0.004",
+                                         "-pbc", "600000"], [0], 0.99, 1e-3),
+}
+
+# reference RETURN_WITH_ERR codes 1..4 (kernel/defs.cuh:39-48) -> UPBP_STATUS_* bits
+def _status_of_codes(delta):
+    return sum(1 << (code - 1) for code in range(1, 5) if delta[code] > 0)
+
+
+def _log(case, it, record):
+    path = os.environ.get("UPBP_PARITY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"case": case, "iteration": it, **record}) + "\n")
+
+
+@pytest.mark.parametrize("case", list(FULL))
+def test_full_size_parity_with_reference(case, scene_dir):
+    import ref_cpu
+    from gpuupbp_b200 import upbp
+    assert ref_cpu.available(), "oracle/_ref/libupbp_ref_cpu.so is not built (make -C oracle)"
+    workload, extra, iters, pixel_bar, mean_bar = FULL[case]
+    path = scenes.write_workload(workload, scene_dir)
+    args = ["-s", "-1", path] + extra
+    ref = ref_cpu.RefRenderer(args, threads=0)
+    want = []
+    for it in iters:
+        before = ref_cpu.RefRenderer.exception_counts()
+        img = ref.run_iteration(it)
+        delta = [a - b for a, b in zip(ref_cpu.RefRenderer.exception_counts(), before)]
+        st = ref.stats()
+        want.append((img, {k: st[k] for k in ("vertices", "surface", "medium", "beams")}, _status_of_codes(delta)))
+    ref.close()
+    r = upbp.Renderer(args)
+    for it, (ref_img, ref_counts, ref_status) in zip(iters, want):
+        status = r.run_iteration(it)
+        img = r.iteration_image()
+        st = r.stats()
+        got = {"vertices": st["light_vertices"], "surface": st["surface_vertices"],
+               "medium": st["medium_vertices"], "beams": st["light_beams"]}
+        rel = np.abs(img - ref_img) / (np.abs(ref_img) + 1e-3)
+        frac = float(np.mean(np.all(rel < 1e-3, axis=-1)))
+        mean_rel = float(abs(img.mean() - ref_img.mean()) / (abs(ref_img.mean()) + 1e-6))
+        _log(case, it, {"frac": frac, "mean_rel": mean_rel, "counts": got, "ref_counts": ref_counts,
+                        "status": status, "ref_status": ref_status})
+        assert got == ref_counts, (case, it)
+        assert status == ref_status, (case, it, status, ref_status)
+        assert np.isfinite(img).all()
+        assert frac >= pixel_bar, (case, it, frac, mean_rel)
+        assert mean_rel <= mean_bar, (case, it, frac, mean_rel)
+    r.close()

@@ -45,6 +45,9 @@ def test_image_parity_with_reference(case, scene_dir):
                "medium": st["medium_vertices"], "beams": st["light_beams"]}
         assert got == counts[case][it]
         frac, mean_rel = compare(img, gold[f"{case}/{it}"], PIXEL_TOL.get(case, 1e-3))
+        if os.environ.get("UPBP_PARITY_LOG"):
+            with open(os.environ["UPBP_PARITY_LOG"], "a") as f:
+                f.write(json.dumps({"case": case, "iteration": it, "frac": frac, "mean_rel": mean_rel}) + "\n")
         assert frac >= 0.97, (case, it, frac, mean_rel)
         assert mean_rel <= (1e-4 if case in PIXEL_TOL else 5e-3), (case, it, frac, mean_rel)
         assert np.isfinite(img).all()

@@ -7,7 +7,8 @@ its data in one static device array instead of per-call allocations.
 Checked through the C ABI against upbp_debug_query on the same queries, two
 calls in a row (the static array keeps the previous call's contents, so the
 second call shows that nothing stale leaks into its results).  Neighbour sets
-are integer results: they must be equal exactly.  The file is named to be
+are integer results: they must be equal exactly.  Neither query may change
+the last iteration's work counters.  The file is named to be
 collected last; it also passes when run alone in a fresh process.
 """
 import ctypes
@@ -63,6 +64,7 @@ def test_static_scratch_query_matches_allocating_query(tmp_path):
     r = upbp.Renderer(["-s", "-1", path, "-a", "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d", "-l", "8", "-r", "64x64",
                        "-r_initial", "-0.02"])
     r.run_iteration(0)
+    work_before = r.stats()["work"]
     rng = np.random.default_rng(5)
     for kind in KINDS:
         for call in range(2):
@@ -75,6 +77,9 @@ def test_static_scratch_query_matches_allocating_query(tmp_path):
             for i, c in enumerate(want_c):
                 assert np.array_equal(np.sort(got_i[i, :c]), np.sort(want_i[i, :c]))
                 assert not got_i[i, c:].any()  # slots beyond the count are cleared
+    # the queries count their work in a row of their own: the iteration's
+    # work counters read the same after them
+    assert r.stats()["work"] == work_before
     # sizes beyond the static array are refused, not truncated
     q = np.zeros((4097, 8), np.float32)
     counts = np.zeros(4097, np.uint32)
