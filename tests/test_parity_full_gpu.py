@@ -18,11 +18,21 @@ command line and random stream.
   beams and 10M photons), BB1D over the first 600 000 light paths, on a
   32x18 camera.
 
-Per iteration: the light-vertex, surface, medium and beam counts equal; the
-device status bits equal the reference's failed-path codes (the reference
-counts RETURN_WITH_ERR codes, the GPU sets one bit per code); pixels agree
-as the small parity cases do (PIXEL_BAR of pixels within 1e-3 relative,
-image mean within MEAN_BAR).
+Per iteration: the device status bits equal the reference's failed-path
+codes (the reference counts RETURN_WITH_ERR codes, the GPU sets one bit per
+code); the light-vertex, surface, medium and beam counts agree within
+COUNT_TOL relative; a fraction of the pixels (the case's pixel bar) agrees
+within 1e-3 relative, a larger one (the 1e-2 bar) within 1e-2, and the image
+mean within the case's mean bar.
+
+At these sizes the two programs do not take every decision alike: the GPU
+contracts multiplies and adds into fused operations and its expf/logf/sqrtf
+round differently from the host's, so a comparison that lands within a
+rounding error flips on a few of the millions of light paths (observed: 15
+of 498 205 light vertices of the media field, 103 of 10.5M in the dense
+enclosure).  A diverged light path moves every pixel its photons and beams
+reach by a small amount, which is why the pixel bars of the media field are
+below the small cases' while its mean agrees to 5e-5.
 """
 import json
 import os
@@ -37,14 +47,17 @@ pytestmark = pytest.mark.gpu
 BOX_R = ["-r_initial", "-0.02", "-r_alpha", "0.75"]
 ALL6 = "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d"
 
-# name: (workload, command line without the scene, iterations, pixel bar, mean bar)
+COUNT_TOL = 1e-4
+
+# name: (workload, command line without the scene, iterations, pixel bar at 1e-3, pixel bar at 1e-2, mean bar)
 FULL = {
     "media_field_full": ("media_field", ["-a", ALL6, "-l", "12", "-r", "160x90", "-pcpi", "921600"], [0, 1],
-                         0.99, 1e-3),
-    "box_256": ("box_medium", ["-a", "upbp_all", "-l", "8", "-r", "256x256"] + BOX_R, [0, 7, 15], 0.99, 1e-3),
+                         0.96, 0.99, 2e-4),
+    "box_256": ("box_medium", ["-a", "upbp_all", "-l", "8", "-r", "256x256"] + BOX_R, [0, 7, 15],
+                0.998, 0.999, 2e-5),
     "dense_beams_crop": ("dense_beams", ["-a", ALL6, "-l", "16", "-r", "32x18", "-pcpi", "2073600",
                                          "-r_initial_bb1d", "-0.004", "-r_initial_bp2d", "-0.004",
-                                         "-pbc", "600000"], [0], 0.99, 1e-3),
+                                         "-pbc", "600000"], [0], 0.995, 0.998, 5e-5),
 }
 
 # reference RETURN_WITH_ERR codes 1..4 (kernel/defs.cuh:39-48) -> UPBP_STATUS_* bits
@@ -64,7 +77,7 @@ def test_full_size_parity_with_reference(case, scene_dir):
     import ref_cpu
     from gpuupbp_b200 import upbp
     assert ref_cpu.available(), "oracle/_ref/libupbp_ref_cpu.so is not built (make -C oracle)"
-    workload, extra, iters, pixel_bar, mean_bar = FULL[case]
+    workload, extra, iters, pixel_bar, pixel_bar_2, mean_bar = FULL[case]
     path = scenes.write_workload(workload, scene_dir)
     args = ["-s", "-1", path] + extra
     ref = ref_cpu.RefRenderer(args, threads=0)
@@ -85,12 +98,14 @@ def test_full_size_parity_with_reference(case, scene_dir):
                "medium": st["medium_vertices"], "beams": st["light_beams"]}
         rel = np.abs(img - ref_img) / (np.abs(ref_img) + 1e-3)
         frac = float(np.mean(np.all(rel < 1e-3, axis=-1)))
+        frac_2 = float(np.mean(np.all(rel < 1e-2, axis=-1)))
         mean_rel = float(abs(img.mean() - ref_img.mean()) / (abs(ref_img.mean()) + 1e-6))
-        _log(case, it, {"frac": frac, "mean_rel": mean_rel, "counts": got, "ref_counts": ref_counts,
-                        "status": status, "ref_status": ref_status})
-        assert got == ref_counts, (case, it)
+        _log(case, it, {"frac": frac, "frac_1e-2": frac_2, "mean_rel": mean_rel, "counts": got,
+                        "ref_counts": ref_counts, "status": status, "ref_status": ref_status})
+        for k in got:
+            assert abs(got[k] - ref_counts[k]) <= COUNT_TOL * ref_counts[k], (case, it, k, got, ref_counts)
         assert status == ref_status, (case, it, status, ref_status)
         assert np.isfinite(img).all()
-        assert frac >= pixel_bar, (case, it, frac, mean_rel)
+        assert frac >= pixel_bar and frac_2 >= pixel_bar_2, (case, it, frac, frac_2, mean_rel)
         assert mean_rel <= mean_bar, (case, it, frac, mean_rel)
     r.close()
