@@ -29,6 +29,7 @@ UPBP_D unsigned generate_camera_sample(float2& screen, unsigned pixel, PathState
     const float3 wr = transform_point(cam.raster_to_world, make_float3(screen.x, screen.y, 0.f));
     s.origin = cam.origin;
     s.dir = normalize(wr - cam.origin);
+    UPBP_MISDBG(mis_origin(false, pixel, cam.origin, cam.direction, 0u));
     const float cos_at_cam = dot(cam.direction, s.dir);
     const float ip_dist = cam.image_plane_dist / cos_at_cam;
     const float camera_pdf_w = (ip_dist * ip_dist) / cos_at_cam;
@@ -50,7 +51,7 @@ UPBP_D unsigned generate_camera_sample(float2& screen, unsigned pixel, PathState
 }
 
 // Emitter hit, MIS Eq D.32/D.33 (functs_camera.cuh:107-165).
-UPBP_D float3 light_hit_radiance(const DLight& l, const PathState& s, float rs_rev)
+UPBP_D float3 light_hit_radiance(const DLight& l, const PathState& s, float rs_rev, float* w_out = nullptr)
 {
     const DeviceParams& p = c_params;
     if (s.is_specular_path && p.ignore_fully_spec_paths) return v3(0.f);
@@ -65,6 +66,7 @@ UPBP_D float3 light_hit_radiance(const DLight& l, const PathState& s, float rs_r
     const VertexWeights& wc = s.sw.w;
     const float bpt = !wc.prev_specular;
     const float w_camera = direct_pdf_a * bpt * wc.d_shared + emission_pdf_w * rs_rev * wc.d_bpt;
+    if (w_out) *w_out = 1.f / (0.f + 1.f + w_camera);
     return (1.f / (0.f + 1.f + w_camera)) * rad;
 }
 
@@ -75,6 +77,7 @@ UPBP_D float3 light_hit_radiance(const DLight& l, const PathState& s, float rs_r
 struct NeeSample {
     float3 dir, rad, f;
     float dist, k, w_light, a, rpdf, sin_theta;
+    UPBP_MISDBG(int light;)
 };
 
 UPBP_D bool nee_sample(NeeSample& ns, float3 hit, const Bsdf& bsdf, Rng& rng)
@@ -105,11 +108,12 @@ UPBP_D bool nee_sample(NeeSample& ns, float3 hit, const Bsdf& bsdf, Rng& rng)
     ns.k = cos_to_light / (pick * direct_pdf_w);
     ns.rpdf = rpdf;
     ns.sin_theta = sin_theta;
+    UPBP_MISDBG(ns.light = lid;)
     return true;
 }
 
 UPBP_D unsigned nee_finish(float3& contrib, const NeeSample& ns, float3 hit, bool in_medium, const BoundaryStack& stack,
-                           const VertexWeights& wc, VolSeg* segs)
+                           const VertexWeights& wc, VolSeg* segs, float* w_out = nullptr, int* nseg_out = nullptr)
 {
     contrib = v3(0.f);
     int nseg = 0;
@@ -119,17 +123,24 @@ UPBP_D unsigned nee_finish(float3& contrib, const NeeSample& ns, float3 hit, boo
     const unsigned st = occluded(occ, hit, ns.dir, ns.dist, stack, in_medium ? kOriginInMedium : 0u, segs, nseg, unused);
     if (st) return st;
     if (occ) return 0;
-    float n_rev = 1.f;
+    float n_rev = 1.f, n_for = 1.f;
     float3 att = v3(1.f);
     if (nseg > 0) {
         n_rev = seg_rev_pdf(segs, nseg);
+        n_for = seg_for_pdf(segs, nseg);
         att = seg_attenuation(segs, nseg);
         if (!is_positive(att)) return 0;
     }
     const float ft = pde_factor(in_medium, false, 1.f / n_rev, wc.rev_ratio, wc.for_inv, wc.for_ratio, ns.sin_theta);
     const float b = !wc.prev_specular;
     const float w_camera = ns.a * n_rev * (ft + b * wc.d_shared + (ns.rpdf / wc.rev_inv) * wc.d_bpt);
-    const float mis = 1.f / (ns.w_light + 1.f + w_camera);
+    // the reference's w_light omits the camera-side sampling pdf of the
+    // light ray's media (functs_camera.cuh:296); the emitter-hit weight of
+    // the same path includes it
+    const float w_light = c_params.mis_exact ? ns.w_light * n_for : ns.w_light;
+    const float mis = 1.f / (w_light + 1.f + w_camera);
+    if (w_out) *w_out = mis;
+    if (nseg_out) *nseg_out = nseg;
     contrib = (ns.k * (ns.rad * att * ns.f)) * mis;
     if (is_black_or_negative(contrib)) contrib = v3(0.f);
     return 0;
@@ -138,7 +149,7 @@ UPBP_D unsigned nee_finish(float3& contrib, const NeeSample& ns, float3 hit, boo
 // BPT connection of a camera and a light vertex, Eq 4.50/4.51
 // (functs_camera.cuh:349-527).
 UPBP_D unsigned connect_vertices(float3& contrib, const LightVertex& lv, const Bsdf& cb, float3 chit, const PathState& s,
-                                 Rng& rng, VolSeg* segs)
+                                 Rng& rng, VolSeg* segs, float* w_out = nullptr, int* nseg_out = nullptr)
 {
     contrib = v3(0.f);
     float3 dir = lv.hit - chit;
@@ -184,6 +195,8 @@ UPBP_D unsigned connect_vertices(float3& contrib, const LightVertex& lv, const B
     const float bt = !wc.prev_specular;
     const float w_camera = l_fpdf_a * rs_rev * (f_t + bt * wc.d_shared + (c_rpdf / wc.rev_inv) * wc.d_bpt);
     const float mis = 1.f / (w_light + 1.f + w_camera);
+    if (w_out) *w_out = mis;
+    if (nseg_out) *nseg_out = nseg;
     contrib = (g * cf * lf * att) * mis;
     if (is_black_or_negative(contrib)) contrib = v3(0.f);
     return 0;
@@ -192,7 +205,7 @@ UPBP_D unsigned connect_vertices(float3& contrib, const LightVertex& lv, const B
 // SURF / PP3D merge of a camera vertex with one photon, Eq 4.52/4.17/4.53
 // (functs_pp.cuh:44-136).
 UPBP_D float3 eval_point_merge(const LightVertex& lv, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb,
-                                bool medium)
+                                bool medium, float* w_out = nullptr)
 {
     const DeviceParams& p = c_params;
     const unsigned plen = lv.path_length + cam_len;
@@ -214,6 +227,7 @@ UPBP_D float3 eval_point_merge(const LightVertex& lv, unsigned cam_len, const Ve
     const float bt = !wc.prev_specular;
     const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
     const float mis = 1.f / (w_light + w_local + w_camera);
+    if (w_out) *w_out = mis;
     return mis * f * lv.thr;
 }
 
@@ -227,7 +241,8 @@ struct QuerySeg {
 };
 
 // PB2D: camera query beam x photon point (functs_pb2d.cuh:57-201).
-UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVertex& lv, float isect_dist, float rad2)
+UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVertex& lv, float isect_dist, float rad2,
+                        float* w_out = nullptr)
 {
     const DeviceParams& p = c_params;
     const unsigned plen = lv.path_length + q.cam_path_length;
@@ -278,12 +293,13 @@ UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVe
     const float bt = !wc.prev_specular;
     const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
     const float mis = 1.f / (w_light + w_local + w_camera);
+    if (w_out) *w_out = mis;
     return mis * unweighted;
 }
 
 // BB1D: camera query beam x photon beam (functs_bb1d.cuh:57-248).
 UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& lb, float bb_dist, float sin_theta,
-                        float tc, float tp)
+                        float tc, float tp, float* w_out = nullptr)
 {
     const DeviceParams& p = c_params;
     const unsigned plen = lb.path_length + q.cam_path_length;
@@ -333,9 +349,16 @@ UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& l
     wc.rev_inv = 1.f / rsr_c;
     wc.for_ratio = ratio;
     wc.rev_ratio = ratio;
-    // the reference multiplies by dist^2 except for first-segment beams of
-    // finite lights (functs_bb1d.cuh:191); kept for parity
-    if (!(lb.path_length == 1 && !lb.infinite)) wl.d_shared *= tp * tp;
+    {
+        // The reference multiplies by the squared distance from the beam's
+        // origin, and not for first-segment beams of finite lights
+        // (functs_bb1d.cuh:191), kept for parity.  The exact form (mis_exact)
+        // measures the distance from the light vertex and skips it only after
+        // an infinite light, as every other merge does.
+        const bool skip = lb.path_length == 1 && lb.infinite == (p.mis_exact != 0);
+        const float dl = tp + (p.mis_exact ? lb.origin_offset : 0.f);
+        if (!skip) wl.d_shared *= dl * dl;
+    }
     wl.d_shared /= rsf_p;
     wl.d_bpt /= rsf_p;
     wl.d_pde /= rsf_p;
@@ -356,12 +379,13 @@ UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& l
     const float bt = !wc.prev_specular;
     const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
     const float mis = 1.f / (w_light + w_local + w_camera);
+    if (w_out) *w_out = mis;
     return mis * unweighted;
 }
 
 // BP2D: photon beam x camera point (functs_bp2d.cuh:51-198).
 UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& wc, const Bsdf& cb, float isect_dist,
-                        float rad2)
+                        float rad2, float* w_out = nullptr)
 {
     const DeviceParams& p = c_params;
     const unsigned plen = lb.path_length + cam_len;
@@ -390,7 +414,11 @@ UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& w
     if (is_black_or_negative(f)) return v3(0.f);
     const float fpdf = ph * cb.cont_prob;
     const float rpdf = ph * m.cont_prob;
-    if (!(lb.path_length == 1 && lb.infinite)) wl.d_shared *= isect_dist * isect_dist;
+    // the reference measures the distance from the beam's origin, which lies
+    // past the light vertex when the beam starts at a medium boundary
+    // (functs_bp2d.cuh:137-140); the exact form measures it from the vertex
+    const float dl = p.mis_exact ? lb.origin_offset + isect_dist : isect_dist;
+    if (!(lb.path_length == 1 && lb.infinite)) wl.d_shared *= dl * dl;
     wl.d_shared /= rs_for;
     wl.d_bpt /= rs_for;
     wl.d_pde /= rs_for;
@@ -411,6 +439,7 @@ UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& w
     const float bt = !wc.prev_specular;
     const float w_camera = val * (wc.d_shared * bt * p.subpath_count_bpt + rpdf * wc.d_pde / wc.rev_inv);
     const float mis = 1.f / (w_light + w_local + w_camera);
+    if (w_out) *w_out = mis;
     return mis * unweighted;
 }
 
@@ -628,13 +657,25 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
             if (!pred_beam_beam(q.o, q.d, q.dmin, q.dmax, lb.o, lb.d, lb.length, p.radius_bb1d_2, dist, sin_theta,
                                 t1, t2))
                 return;
-            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2);
+            float w = -1.f;
+            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2, &w);
+            UPBP_MISDBG(if (w >= 0.f) {
+                MisEvent e{kMisBb1d, path, q.cam_path_length, lb.path_idx, lb.path_length, 0u, w,
+                           lb.o + lb.d * t2, q.o + q.d * t1, lb.origin_offset + t2, t1};
+                mis_event(e, nullptr, 0);
+            });
         } else {
             LightVertex lv;
             read_vertex(fn, lv);
             float dist, rad2;
             if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) return;
-            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2);
+            float w = -1.f;
+            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2, &w);
+            UPBP_MISDBG(if (w >= 0.f) {
+                MisEvent e{kMisPb2d, path, q.cam_path_length, qb.y / p.slots_per_path, lv.path_length, 0u, w,
+                           lv.hit, q.o + q.d * dist, 0.f, dist};
+                mis_event(e, nullptr, 0);
+            });
         }
         splat_camera(pk >> 8, weight * est);
     } else {
@@ -645,8 +686,14 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
         read_beam(fn, lb);
         float dist, rad2;
         if (!pred_ray_disc(lb.o, lb.d, 0.f, lb.length, cv.hit, p.radius_bp2d_2, dist, rad2)) return;
+        float w = -1.f;
         splat_camera(fbits(q8.x),
-                     cv.thr * p.bp2d_normalization * eval_bp2d(lb, cv.path_length, cv.w, cv.bsdf, dist, rad2));
+                     cv.thr * p.bp2d_normalization * eval_bp2d(lb, cv.path_length, cv.w, cv.bsdf, dist, rad2, &w));
+        UPBP_MISDBG(if (w >= 0.f) {
+            MisEvent e{kMisBp2d, fbits(q8.z), cv.path_length, lb.path_idx, lb.path_length, 0u, w,
+                       lb.o + lb.d * dist, cv.hit, lb.origin_offset + dist, 0.f};
+            mis_event(e, nullptr, 0);
+        });
     }
 }
 
@@ -951,7 +998,13 @@ __global__ void __launch_bounds__(128) point_merge_kernel()
         points_in_radius(map, cv.hit, r2, [&](unsigned slot) {
             LightVertex lv;
             load_vertex(p.vertices + slot, lv);
-            acc += eval_point_merge(lv, cv.path_length, cv.w, cv.bsdf, medium);
+            float w = -1.f;
+            acc += eval_point_merge(lv, cv.path_length, cv.w, cv.bsdf, medium, &w);
+            UPBP_MISDBG(if (w >= 0.f) {
+                MisEvent e{medium ? kMisPp3d : kMisSurf, fbits(q8.z), cv.path_length, slot / p.slots_per_path,
+                           lv.path_length, 0u, w, lv.hit, cv.hit, 0.f, 0.f};
+                mis_event(e, nullptr, 0);
+            });
         });
         splat_camera(fbits(q8.x), cv.thr * (medium ? p.pp3d_normalization : p.surf_normalization) * acc);
     }
@@ -1041,6 +1094,8 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
                           segs, nseg, lsegs, nlseg, rng);
     if (ret) return false;
+    UPBP_MISDBG(mis_ray(false, c.path, s.path_length, hit ? isect.dist : kInfinity,
+                        origin_in_medium ? kOriginInMedium : 0u, lsegs, nlseg));
     if ((p.build_pb2d && p.n_medium > 0) || (p.build_bb1d && p.n_beams > 0)) {
         const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;
         const bool use_lite = !(isect.on_surface() || p.camera_beam_type == kShortBeam || !hit);
@@ -1083,6 +1138,9 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
     const float3 hitpoint = ro + rd * isect.dist;
     origin_in_medium = isect.in_medium();
+    UPBP_MISDBG(mis_hit(false, c.path, s.path_length, hitpoint, isect.in_medium(),
+                        isect.in_medium() ? isect.med : isect.mat, isect.in_medium() ? v3(0.f) : isect.shading_normal,
+                        isect.in_medium() ? v3(0.f) : isect.normal, bsdf.delta(), bsdf.cont_prob));
     {
         const float d = bsdf.d_factor();
         w.d_shared *= isect.dist * isect.dist;
@@ -1096,7 +1154,16 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     }
     if (isect.light >= 0) {
         if (s.path_length < p.min_path_length) return false;
-        color += s.throughput * light_hit_radiance(p.lights[isect.light], s, rs_rev);
+        float wl = -1.f;
+        color += s.throughput * light_hit_radiance(p.lights[isect.light], s, rs_rev, &wl);
+        UPBP_MISDBG({
+            mis_hit_light(c.path, s.path_length, hitpoint, isect.light, isect.normal);
+            if (wl >= 0.f) {
+                MisEvent e{kMisEmitterHit, c.path, s.path_length, 0u, 0u, (unsigned)isect.light, wl, hitpoint, hitpoint,
+                           0.f, 0.f};
+                mis_event(e, nullptr, 0);
+            }
+        });
         return false;
     }
     if (s.path_length >= p.max_path_length) return false;
@@ -1129,7 +1196,8 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
                 q[1] = make_float4(ns.dir.x, ns.dir.y, ns.dir.z, ubits(v));
                 q[2] = make_float4(ns.rad.x, ns.rad.y, ns.rad.z, ns.k);
                 q[3] = make_float4(ns.f.x, ns.f.y, ns.f.z, ns.w_light);
-                q[4] = make_float4(ns.a, ns.rpdf, ns.sin_theta, ubits(bsdf.in_medium() ? 1u : 0u));
+                q[4] = make_float4(ns.a, ns.rpdf, ns.sin_theta,
+                                   ubits((bsdf.in_medium() ? 1u : 0u) UPBP_MISDBG(| ((unsigned)ns.light << 1))));
             }
         }
         if (nv > 0) {
@@ -1160,6 +1228,7 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     bool cont;
     ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
     if (ret || !cont) return false;
+    UPBP_MISDBG(if (s.sw.w.prev_specular) mis_specular(false, c.path, s.path_length));
     if (bsdf.on_surface()) {
         if (!s.sw.w.prev_specular && (only_spec_surf || (p.estimator_techniques & kSpecularOnly))) return false;
     } else {
@@ -1264,7 +1333,14 @@ __global__ void __launch_bounds__(128, 8) nee_connect_kernel()
         wc.prev_specular = (fbits(w3.w) >> 29) & 1u;
         load_conn_stack(cr, fbits(q8.y), st);
         float3 c;
-        const unsigned e = nee_finish(c, ns, hit, in_medium, st, wc, segs);
+        float w = -1.f;
+        int nseg = 0;
+        const unsigned e = nee_finish(c, ns, hit, in_medium, st, wc, segs, &w, &nseg);
+        UPBP_MISDBG(if (!e && w >= 0.f) {
+            MisEvent ev{kMisNee, fbits(q8.z), fbits(q8.w), 0u, 0u, fbits(q4.w) >> 1, w, hit + ns.dir * ns.dist, hit,
+                        0.f, 0.f};
+            mis_event(ev, segs, nseg);
+        });
         if (e) {
             // the reference ends the camera path at a failed step
             flag_status(e);
@@ -1306,7 +1382,14 @@ __global__ void __launch_bounds__(128, 8) bpt_connect_kernel()
         Rng unused;
         unused.state = unused.inc = 0;  // occlusion rays draw no random numbers
         float3 c;
-        const unsigned e = connect_vertices(c, lv, cv.bsdf, cv.hit, ps, unused, segs);
+        float w = -1.f;
+        int nseg = 0;
+        const unsigned e = connect_vertices(c, lv, cv.bsdf, cv.hit, ps, unused, segs, &w, &nseg);
+        UPBP_MISDBG(if (!e && w >= 0.f) {
+            MisEvent ev{kMisBpt, fbits(q8.z), fbits(q8.w), pr.y / p.slots_per_path, lv.path_length, 0u, w, lv.hit,
+                        cv.hit, 0.f, 0.f};
+            mis_event(ev, segs, nseg);
+        });
         if (e) {
             // the reference ends the camera path at a failed connection
             flag_status(e);

@@ -255,6 +255,7 @@ struct upbp_ctx {
     unsigned h_counters[4] = {0, 0, 0, 0};
     unsigned iterations = 0;
     uint64_t triangles = 0;
+    MisDebug mis{};  // MIS recording buffers (recording build only)
 };
 
 namespace {
@@ -787,6 +788,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         P.estimator_techniques = flags;
         P.bb1d_used_light_subpath_count = (unsigned)c->bb1d_used;
         P.use_shading_normal = cfg->use_shading_normal;
+        P.mis_exact = cfg->mis_exact != 0;
         P.res_x = cfg->res_x;
         P.res_y = cfg->res_y;
 
@@ -901,6 +903,20 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         P.path_color = c->d_path_color;
         P.hit_state = c->d_hit_state;
         P.cam_fb = c->d_cam_fb;
+#ifdef UPBP_MIS_DEBUG
+        {
+            MisDebug& m = c->mis;
+            m.max_verts = cfg->max_path_length + 1;
+            m.light_paths = L;
+            m.camera_paths = P.screen_pixel_count;
+            m.event_capacity = 1u << 20;
+            if (const char* e = std::getenv("UPBP_MIS_EVENTS")) m.event_capacity = (unsigned)std::max(1LL, std::atoll(e));
+            UPBP_CK(dalloc(&m.light, (size_t)L * m.max_verts * kMisVtxWords));
+            UPBP_CK(dalloc(&m.camera, (size_t)P.screen_pixel_count * m.max_verts * kMisVtxWords));
+            UPBP_CK(dalloc(&m.events, (size_t)m.event_capacity * kMisEvWords));
+            UPBP_CK(dalloc(&m.event_count, 1));
+        }
+#endif
         UPBP_CK(cudaStreamSynchronize(c->st));
         *out = c;
         return UPBP_OK;
@@ -932,6 +948,15 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             h2d += sizeof(w);
             UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
         }
+#ifdef UPBP_MIS_DEBUG
+        {
+            const MisDebug& m = c->mis;
+            UPBP_CK(cudaMemsetAsync(m.light, 0, (size_t)m.light_paths * m.max_verts * kMisVtxWords * sizeof(float4), c->st));
+            UPBP_CK(cudaMemsetAsync(m.camera, 0, (size_t)m.camera_paths * m.max_verts * kMisVtxWords * sizeof(float4), c->st));
+            UPBP_CK(cudaMemsetAsync(m.event_count, 0, sizeof(unsigned), c->st));
+            UPBP_CK(cudaMemcpyToSymbolAsync(c_misdbg, &m, sizeof(m), 0, cudaMemcpyHostToDevice, c->st));
+        }
+#endif
         unsigned found[4] = {0, 0, 0, 0};
         if (P.trace_light_paths) {
             // radius schedule and MIS factors (renderer.cpp:57-119)
@@ -1477,6 +1502,57 @@ extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queri
     });
 }
 
+// MIS records of the last iteration (recording build, libupbp_b200_misdbg.so):
+// which 0 light-subpath vertices, 1 camera-subpath vertices, 2 contributions,
+// 3 a header of kMisHeader floats (layout in include/upbp.h).
+constexpr int kMisHeader = 64;
+extern "C" int upbp_debug_mis_records(upbp_ctx* c, int which, float* out, uint64_t capacity, uint64_t* count)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !count || which < 0 || which > 3) return UPBP_ERR_ARGS;
+#ifndef UPBP_MIS_DEBUG
+        (void)out;
+        (void)capacity;
+        *count = 0;
+        upbp_host::set_error("MIS records are kept only by the recording build (libupbp_b200_misdbg.so)");
+        return UPBP_ERR_ARGS;
+#else
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        const MisDebug& m = c->mis;
+        unsigned nev = 0;
+        UPBP_CK(cudaMemcpy(&nev, m.event_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        const unsigned kept = std::min(nev, m.event_capacity);
+        if (which == 3) {
+            const DeviceParams& P = c->P;
+            float h[kMisHeader] = {};
+            const float vals[] = {(float)m.max_verts, (float)m.light_paths, (float)m.camera_paths, (float)nev,
+                                  (float)m.event_capacity, (float)kMisVtxWords, (float)kMisEvWords, (float)kMisSegs,
+                                  P.camera.origin.x, P.camera.origin.y, P.camera.origin.z, P.camera.direction.x,
+                                  P.camera.direction.y, P.camera.direction.z, P.camera.image_plane_dist,
+                                  (float)P.res_x, (float)P.res_y, P.mis_factor_surf, P.mis_factor_pp3d,
+                                  P.mis_factor_pb2d, P.mis_factor_bp2d, P.mis_factor_bb1d, P.subpath_count_bpt,
+                                  (float)P.light_subpath_count, (float)P.photon_beam_type, (float)P.camera_beam_type,
+                                  (float)P.light_count, (float)P.mis_exact, (float)P.connect_to_camera_from_surf,
+                                  (float)P.max_path_length, (float)P.min_path_length, P.scene_radius};
+            std::memcpy(h, vals, sizeof(vals));
+            *count = kMisHeader;
+            if (out) std::memcpy(out, h, sizeof(float) * std::min<uint64_t>(capacity, kMisHeader));
+            return UPBP_OK;
+        }
+        const float4* src = which == 0 ? m.light : which == 1 ? m.camera : m.events;
+        const uint64_t n4 = which == 0 ? (uint64_t)m.light_paths * m.max_verts * kMisVtxWords
+                            : which == 1 ? (uint64_t)m.camera_paths * m.max_verts * kMisVtxWords
+                                         : (uint64_t)kept * kMisEvWords;
+        *count = 4 * n4;
+        if (out && capacity) UPBP_CK(cudaMemcpy(out, src, sizeof(float) * std::min<uint64_t>(capacity, 4 * n4),
+                                                cudaMemcpyDeviceToHost));
+        return UPBP_OK;
+#endif
+    });
+}
+
 extern "C" void* upbp_get_stream(upbp_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 extern "C" int upbp_get_device(const upbp_ctx* c) { return c ? c->dev : UPBP_ERR_ARGS; }
@@ -1493,7 +1569,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
         if (b.owner == c) b.owner = nullptr;
     }
     if (c->h_status) cudaFreeHost(c->h_status);
-    void* bufs[] = {c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
+    void* bufs[] = {c->mis.light, c->mis.camera, c->mis.events, c->mis.event_count, c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,

@@ -172,7 +172,8 @@ struct LightVertexRec {
 //   q3: ray_sample_rev_pdf, sampling flags bits, path index bits, path length bits
 //   q4: d_shared, d_bpt, d_pde, ray_sample_for_pdf_inv
 //   q5: ray_sample_rev_pdf_inv, for_pdfs_ratio, rev_pdfs_ratio, bits (prev_in_medium | prev_specular<<1 | infinite<<2)
-//   q6: last_sin_theta, d_bpt_a, d_bpt_b, d_pde_a ; d_pde_b goes in q7.x
+//   q6: last_sin_theta, d_bpt_a, d_bpt_b, d_pde_a
+//   q7: d_pde_b, distance from the light vertex that traced the ray to the origin, 0, 0
 struct BeamRec {
     float4 q[8];
 };
@@ -326,6 +327,12 @@ struct DeviceParams {
     int connect_to_camera_from_surf, ignore_fully_spec_paths, use_shading_normal;
     unsigned estimator_techniques;
     unsigned screen_pixel_count, light_subpath_count, bb1d_used_light_subpath_count;
+    // 0: the reference's MIS weights; 1: weights equal to the full-path
+    // balance heuristic where the reference's recursion departs from it
+    // (photon-beam merges measure the light-side distance from the light
+    // vertex, first-segment BB1D beams of finite lights include it, and the
+    // NEE weight includes the media on the camera side of the light ray)
+    int mis_exact;
     unsigned res_x, res_y;
     unsigned long long iteration_offset;
 

@@ -9,7 +9,7 @@
 
 namespace upbp {
 
-UPBP_D unsigned generate_light_sample(PathState& s, Rng& rng)
+UPBP_D unsigned generate_light_sample(PathState& s, Rng& rng, unsigned path_idx)
 {
     const DeviceParams& p = c_params;
     const float lc = (float)p.light_count;
@@ -21,6 +21,7 @@ UPBP_D unsigned generate_light_sample(PathState& s, Rng& rng)
     emission_pdf_w /= lc;
     direct_pdf_a /= lc;
     s.throughput /= emission_pdf_w;
+    UPBP_MISDBG(mis_origin(true, path_idx, s.origin, l.frame.z, (unsigned)lid));
     s.path_length = 1;
     s.is_infinite_light = !light_is_finite(l);
     s.is_specular_path = false;
@@ -67,6 +68,7 @@ UPBP_D void add_beams(float3 ro, float3 rd, float3 throughput, unsigned path_len
             b.med = med;
             b.o = ro + rd * dmin;
             b.length = fminf(dmax - dmin, m.max_beam_length);
+            b.origin_offset = dmin;
             b.for_pdf = fpdf;
             b.rev_pdf = rpdf;
             b.flags = kEndInMedium | (i == 0 ? sflags : 0u);
@@ -92,7 +94,8 @@ UPBP_D void add_beams(float3 ro, float3 rd, float3 throughput, unsigned path_len
 }
 
 // Light tracing splat to the image plane (functs_light.cuh:251-388, Eq D.38).
-UPBP_D unsigned connect_to_camera(const PathState& s, float3 hit, const Bsdf& bsdf, Rng& rng, VolSeg* segs)
+UPBP_D unsigned connect_to_camera(const PathState& s, float3 hit, const Bsdf& bsdf, Rng& rng, VolSeg* segs,
+                                  unsigned path_idx)
 {
     const DeviceParams& p = c_params;
     const DCamera& cam = p.camera;
@@ -130,6 +133,10 @@ UPBP_D unsigned connect_to_camera(const PathState& s, float3 hit, const Bsdf& bs
     const float w_light = (camera_pdf_a / p.light_subpath_count) * rs_rev *
                           (f_s + bpt_s_sub_1 * wl.d_shared + (rpdf / wl.rev_inv) * wl.d_bpt);
     const float mis = 1.f / (w_light + 1.f);
+    UPBP_MISDBG({
+        MisEvent e{kMisLightTrace, 0u, 0u, path_idx, s.path_length, 0u, mis, hit, cam.origin, 0.f, 0.f};
+        mis_event(e, segs, nseg);
+    });
     const float s2i = 1.f / i2s;
     const float3 contrib = mis * s.throughput * f * att / (p.light_subpath_count * s2i);
     if (is_black_or_negative(contrib)) return 0;
@@ -167,7 +174,7 @@ UPBP_D bool light_path_begin(LightLane& l, unsigned path_idx)
         l.ret = 0;
         return false;
     }
-    l.ret = generate_light_sample(l.s, l.rng);
+    l.ret = generate_light_sample(l.s, l.rng, path_idx);
     if (l.s.is_infinite_light && p.media[p.global_medium].has_attenuation) {
         // the reference ends such a path before tracing it, without an error
         l.ret = 0;
@@ -200,6 +207,8 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
     ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
                           segs, nseg, lsegs, nlseg, rng);
     if (ret) return false;
+    UPBP_MISDBG(mis_ray(true, path_idx, s.path_length, hit ? isect.dist : kInfinity,
+                        origin_in_medium ? kOriginInMedium : 0u, lsegs, nlseg));
     if (store_beams)
         add_beams(ro, rd, s.throughput, s.path_length, origin_in_medium ? kOriginInMedium : 0u, segs, nseg, lsegs,
                   nlseg, path_idx, s);
@@ -238,6 +247,9 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
     if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;
     const float3 hitpoint = ro + rd * isect.dist;
     origin_in_medium = isect.in_medium();
+    UPBP_MISDBG(mis_hit(true, path_idx, s.path_length, hitpoint, isect.in_medium(),
+                        isect.in_medium() ? isect.med : isect.mat, isect.in_medium() ? v3(0.f) : isect.shading_normal,
+                        isect.in_medium() ? v3(0.f) : isect.normal, bsdf.delta(), bsdf.cont_prob));
     {
         const float d = bsdf.d_factor();
         if (!(s.path_length == 1 && s.is_infinite_light)) w.d_shared *= isect.dist * isect.dist;
@@ -272,7 +284,7 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
     }
     if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || p.connect_to_camera_from_surf)) {
         if (s.path_length + 1 >= p.min_path_length) {
-            ret = connect_to_camera(s, hitpoint, bsdf, rng, segs);
+            ret = connect_to_camera(s, hitpoint, bsdf, rng, segs, path_idx);
             if (ret) return false;
         }
     }
@@ -280,6 +292,7 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
     bool cont;
     ret = sample_scattering(cont, bsdf, hitpoint, isect, s, rng);
     if (ret || !cont) return false;
+    UPBP_MISDBG(if (s.sw.w.prev_specular) mis_specular(true, path_idx, s.path_length));
     s.path_length++;
     return true;
 }

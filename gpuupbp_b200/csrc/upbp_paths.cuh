@@ -4,6 +4,7 @@
 // path_weight.cuh:35-51 get_pde_factor, Eq 4.23).
 #pragma once
 
+#include "upbp_misdbg.cuh"
 #include "upbp_trace.cuh"
 
 namespace upbp {
@@ -218,6 +219,7 @@ struct Beam {
     float for_pdf, rev_pdf;
     unsigned flags, path_idx, path_length;
     bool infinite;
+    float origin_offset;  // distance from the light vertex that traced the ray to the beam's origin
     StateWeights sw;
 };
 
@@ -233,7 +235,7 @@ UPBP_D void store_beam(BeamRec* rec, const Beam& b)
     q[4] = make_float4(w.d_shared, w.d_bpt, w.d_pde, w.for_inv);
     q[5] = make_float4(w.rev_inv, w.for_ratio, w.rev_ratio, ubits(bits));
     q[6] = make_float4(b.sw.last_sin_theta, b.sw.d_bpt_a, b.sw.d_bpt_b, b.sw.d_pde_a);
-    q[7] = make_float4(b.sw.d_pde_b, 0.f, 0.f, 0.f);
+    q[7] = make_float4(b.sw.d_pde_b, b.origin_offset, 0.f, 0.f);
 }
 
 // A beam record unpacked; q(i) returns float4 i of the record.
@@ -268,6 +270,7 @@ UPBP_D void read_beam(Fetch&& q, Beam& b)
     b.sw.d_bpt_b = q6.z;
     b.sw.d_pde_a = q6.w;
     b.sw.d_pde_b = q7.x;
+    b.origin_offset = q7.y;
 }
 
 UPBP_D void load_beam(const BeamRec* rec, Beam& b)

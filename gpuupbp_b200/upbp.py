@@ -15,6 +15,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libupbp_b200.so")
+# the same ABI built with UPBP_MIS_DEBUG: records subpath vertices and MIS
+# weights for the FP64 full-path check (upbp_debug_mis_records)
+MISDBG_LIB_PATH = os.path.join(HERE, "libupbp_b200_misdbg.so")
 
 UPBP_OK, UPBP_HELP = 0, 1
 ERRORS = {-1: "invalid arguments", -2: "I/O error", -3: "CUDA error", -4: "no CUDA device", -5: "invalid scene",
@@ -42,6 +45,7 @@ class Config(ctypes.Structure):
         ("surf_radius_initial", ctypes.c_float), ("surf_radius_alpha", ctypes.c_float),
         ("continuous_output", ctypes.c_int), ("ignore_fully_spec_paths", ctypes.c_int), ("gpu_assert", ctypes.c_int),
         ("iteration_offset", ctypes.c_uint64), ("do_log", ctypes.c_int), ("use_shading_normal", ctypes.c_int),
+        ("mis_exact", ctypes.c_int),
     ]
 
 
@@ -112,16 +116,17 @@ WORK_NAMES = ["nodes", "tris", "rays", "point_cand", "point_hit", "beam_cand", "
 EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_predefined", "upbp_scene_get_desc",
            "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
            "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
-           "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device"]
+           "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device",
+           "upbp_debug_mis_records"]
 
-_lib = None
+_libs = {}
 
 
 def load_library(path: str = LIB_PATH):
-    """Loads libupbp_b200.so (raises if it was not built)."""
-    global _lib
-    if _lib is not None:
-        return _lib
+    """Loads libupbp_b200.so, or another build of the same ABI (raises if it
+    was not built)."""
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise UpbpError(f"{path} is missing: run gpuupbp_b200/build.py")
     L = ctypes.CDLL(path)
@@ -142,17 +147,18 @@ def load_library(path: str = LIB_PATH):
     L.upbp_get_stream.argtypes = [VP]
     L.upbp_get_stream.restype = VP
     L.upbp_get_device.argtypes = [VP]
+    L.upbp_debug_mis_records.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint64, P(ctypes.c_uint64)]
     L.upbp_last_error.restype = ctypes.c_char_p
     L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]
     L.upbp_debug_query.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
     L.upbp_debug_query_static.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
-    _lib = L
+    _libs[path] = L
     return L
 
 
-def _check(rc: int, what: str):
+def _check(rc: int, what: str, L=None):
     if rc != UPBP_OK:
-        msg = load_library().upbp_last_error().decode(errors="replace")
+        msg = (L or load_library()).upbp_last_error().decode(errors="replace")
         raise UpbpError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
 
 
@@ -211,8 +217,8 @@ def load_scene(args: list[str]) -> dict:
 class Renderer:
     """Drop-in for the reference's Renderer on a scene file + command line."""
 
-    def __init__(self, args: list[str]):
-        L = load_library()
+    def __init__(self, args: list[str], library: str = LIB_PATH):
+        L = self._L = load_library(library)
         self.config = parse_command_line(args)
         c = self.config
         self._scene = ctypes.c_void_p()
@@ -222,7 +228,7 @@ class Renderer:
             rc = L.upbp_scene_load_predefined(c.scene_id, c.res_x, c.res_y, ctypes.byref(self._scene))
         _check(rc, "scene")
         self._ctx = ctypes.c_void_p()
-        _check(L.upbp_create(L.upbp_scene_get_desc(self._scene), ctypes.byref(c), ctypes.byref(self._ctx)), "init")
+        _check(L.upbp_create(L.upbp_scene_get_desc(self._scene), ctypes.byref(c), ctypes.byref(self._ctx)), "init", L)
         self.width, self.height = c.res_x, c.res_y
         self.iterations = 0
 
@@ -230,9 +236,9 @@ class Renderer:
         """Renders one iteration; returns its device status bits (0, or
         UPBP_STATUS_* bits for paths ended early or beams dropped, as the
         reference ends or drops them; the image is complete either way)."""
-        rc = load_library().upbp_run_iteration(self._ctx, iteration)
+        rc = self._L.upbp_run_iteration(self._ctx, iteration)
         if rc < 0:
-            _check(rc, f"iteration {iteration}")
+            _check(rc, f"iteration {iteration}", self._L)
         self.iterations += 1
         self.last_status = rc
         return rc
@@ -245,13 +251,13 @@ class Renderer:
             out = np.empty((self.height, self.width, 3), np.float32)
         elif out.dtype != np.float32 or out.shape != (self.height, self.width, 3) or not out.flags.c_contiguous:
             raise ValueError("out must be a C-contiguous float32 array of shape (H, W, 3)")
-        _check(load_library().upbp_read_iteration(self._ctx, out.ctypes.data), "read")
+        _check(self._L.upbp_read_iteration(self._ctx, out.ctypes.data), "read")
         return out
 
     def accumulated(self, scale: float | None = None) -> np.ndarray:
         out = np.zeros((self.height, self.width, 3), np.float32)
         s = (1.0 / max(1, self.iterations)) if scale is None else scale
-        _check(load_library().upbp_accumulate_to_host(self._ctx, out.ctypes.data, s), "accumulate")
+        _check(self._L.upbp_accumulate_to_host(self._ctx, out.ctypes.data, s), "accumulate")
         return out
 
     def render(self, iterations: int, start: int = 0) -> np.ndarray:
@@ -261,7 +267,7 @@ class Renderer:
 
     def stats(self) -> dict:
         st = Stats()
-        _check(load_library().upbp_get_stats(self._ctx, ctypes.byref(st)), "stats")
+        _check(self._L.upbp_get_stats(self._ctx, ctypes.byref(st)), "stats")
         out = {k: getattr(st, k) for k, _ in Stats._fields_}
         out["work_light"] = dict(zip(WORK_NAMES, list(st.work_light)))
         out["work_camera"] = dict(zip(WORK_NAMES, list(st.work_camera)))
@@ -272,7 +278,7 @@ class Renderer:
 
     def photons(self, kind: int) -> np.ndarray:
         """Photon map contents of the last iteration (see upbp_debug_photons)."""
-        L = load_library()
+        L = self._L
         n = ctypes.c_uint32()
         _check(L.upbp_debug_photons(self._ctx, kind, None, 0, ctypes.byref(n)), "photons")
         width = 4 if kind < 2 else 8
@@ -286,15 +292,30 @@ class Renderer:
         q = np.ascontiguousarray(queries, np.float32).reshape(-1, 8)
         counts = np.zeros(len(q), np.uint32)
         ids = np.zeros((len(q), cap), np.uint32)
-        _check(load_library().upbp_debug_query(self._ctx, kind, q.ctypes.data, len(q), counts.ctypes.data,
+        _check(self._L.upbp_debug_query(self._ctx, kind, q.ctypes.data, len(q), counts.ctypes.data,
                                                ids.ctypes.data, cap), "query")
         return [ids[i, :min(int(c), cap)].copy() for i, c in enumerate(counts)], counts
 
+    def mis_records(self) -> dict:
+        """MIS records of the last iteration (recording build only):
+        header, light and camera subpath vertices, contributions, as float32
+        arrays (upbp_debug_mis_records)."""
+        out = {}
+        for which, name in ((3, "header"), (0, "light"), (1, "camera"), (2, "events")):
+            n = ctypes.c_uint64()
+            _check(self._L.upbp_debug_mis_records(self._ctx, which, None, 0, ctypes.byref(n)), "mis records", self._L)
+            a = np.zeros(n.value, np.float32)
+            if n.value:
+                _check(self._L.upbp_debug_mis_records(self._ctx, which, a.ctypes.data, n.value, ctypes.byref(n)),
+                       "mis records", self._L)
+            out[name] = a
+        return out
+
     def stream_handle(self) -> int:
-        return load_library().upbp_get_stream(self._ctx) or 0
+        return self._L.upbp_get_stream(self._ctx) or 0
 
     def close(self):
-        L = load_library()
+        L = self._L
         if getattr(self, "_ctx", None):
             L.upbp_destroy(self._ctx)
             self._ctx = None

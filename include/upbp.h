@@ -92,6 +92,15 @@ typedef struct upbp_config {
     uint64_t iteration_offset;
     int do_log;
     int use_shading_normal;
+    /* Not in the reference (command line -mis_exact): 1 makes the MIS
+     * weights equal the balance heuristic over the full path where the
+     * reference's recursion departs from it -- photon-beam merges (BB1D,
+     * BP2D) measure the light-side distance from the light vertex instead of
+     * the beam's origin, first-segment BB1D beams of finite lights convert to
+     * area measure like every other beam, and next-event estimation counts
+     * the camera-side sampling pdf of the media its light ray crosses.  0
+     * (the default) keeps the reference's weights. */
+    int mis_exact;
 } upbp_config;
 
 /* ------------------------------------------------------ scene records */
@@ -294,6 +303,25 @@ int upbp_debug_query(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, 
  * are returned as 0 whatever an earlier call left there. */
 int upbp_debug_query_static(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, uint32_t* counts,
                             uint32_t* ids, uint32_t ids_per_query);
+
+/* MIS records of the last iteration, for the FP64 full-path weight check
+ * (oracle/mis_fp64.py).  No counterpart in the reference.  Only the
+ * recording build of the library, libupbp_b200_misdbg.so (the same sources
+ * compiled with UPBP_MIS_DEBUG), keeps them; the production library returns
+ * UPBP_ERR_ARGS.  which: 0 light-subpath vertices and 1 camera-subpath
+ * vertices (per subpath max_verts records of vtx_words float4, see
+ * gpuupbp_b200/csrc/upbp_misdbg.cuh), 2 contributions (ev_words float4
+ * each: technique, the FP32 weight applied, the two subpaths and the points
+ * where they meet), 3 a header of 64 floats: max_verts, light paths, camera
+ * paths, contributions, capacity, vtx_words, ev_words, segments per record,
+ * camera origin xyz, direction xyz, image-plane distance, resolution x y,
+ * MIS factors surf pp3d pb2d bp2d bb1d, BPT subpath count, light subpaths,
+ * photon and query beam types, light count, mis_exact, light tracing from
+ * surfaces, max and min path length, scene radius.  *count receives the
+ * number of floats; at most `capacity` are written.  The recording build
+ * keeps up to 2^20 contributions per iteration (environment variable
+ * UPBP_MIS_EVENTS, read by upbp_create, sets another limit). */
+int upbp_debug_mis_records(upbp_ctx* ctx, int which, float* out, uint64_t capacity, uint64_t* count);
 
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */
