@@ -661,7 +661,7 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
             est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2, &w);
             UPBP_MISDBG(if (w >= 0.f) {
                 MisEvent e{kMisBb1d, path, q.cam_path_length, lb.path_idx, lb.path_length, 0u, w,
-                           lb.o + lb.d * t2, q.o + q.d * t1, lb.origin_offset + t2, t1};
+                           lb.o + lb.d * t2, q.o + q.d * t1, lb.origin_offset + t2, t1, lb.origin_offset};
                 mis_event(e, nullptr, 0);
             });
         } else {
@@ -691,7 +691,7 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
                      cv.thr * p.bp2d_normalization * eval_bp2d(lb, cv.path_length, cv.w, cv.bsdf, dist, rad2, &w));
         UPBP_MISDBG(if (w >= 0.f) {
             MisEvent e{kMisBp2d, fbits(q8.z), cv.path_length, lb.path_idx, lb.path_length, 0u, w,
-                       lb.o + lb.d * dist, cv.hit, lb.origin_offset + dist, 0.f};
+                       lb.o + lb.d * dist, cv.hit, lb.origin_offset + dist, 0.f, lb.origin_offset};
             mis_event(e, nullptr, 0);
         });
     }
@@ -1094,7 +1094,7 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
                           segs, nseg, lsegs, nlseg, rng);
     if (ret) return false;
-    UPBP_MISDBG(mis_ray(false, c.path, s.path_length, hit ? isect.dist : kInfinity,
+    UPBP_MISDBG(mis_ray(false, c.path, s.path_length, rd, hit ? isect.dist : kInfinity,
                         origin_in_medium ? kOriginInMedium : 0u, lsegs, nlseg));
     if ((p.build_pb2d && p.n_medium > 0) || (p.build_bb1d && p.n_beams > 0)) {
         const unsigned qflags = origin_in_medium ? kOriginInMedium : 0u;

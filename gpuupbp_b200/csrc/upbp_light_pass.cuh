@@ -207,7 +207,7 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
     ret = intersect_scene(hit, ro, rd, isect, s.stack, kSampleScattering, origin_in_medium ? kOriginInMedium : 0u,
                           segs, nseg, lsegs, nlseg, rng);
     if (ret) return false;
-    UPBP_MISDBG(mis_ray(true, path_idx, s.path_length, hit ? isect.dist : kInfinity,
+    UPBP_MISDBG(mis_ray(true, path_idx, s.path_length, rd, hit ? isect.dist : kInfinity,
                         origin_in_medium ? kOriginInMedium : 0u, lsegs, nlseg));
     if (store_beams)
         add_beams(ro, rd, s.throughput, s.path_length, origin_in_medium ? kOriginInMedium : 0u, segs, nseg, lsegs,

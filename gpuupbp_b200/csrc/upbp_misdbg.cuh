@@ -21,9 +21,10 @@ namespace upbp {
 //   w1: frame normal.xyz (shading normal; light normal at a light vertex), id bits (material / medium / light)
 //   w2: geometric normal.xyz, segment count bits
 //   w3: ray length to this vertex, trace flags bits (origin in medium), continuation probability, 0
-//   w4..: media segments of that ray (dmin, dmax, medium id bits, 0), up to kMisSegs, to the ray's real hit
+//   w4: direction of that ray.xyz, 0
+//   w5..: media segments of that ray (dmin, dmax, medium id bits, 0), up to kMisSegs, to the ray's real hit
 constexpr int kMisSegs = 10;
-constexpr int kMisVtxWords = 4 + kMisSegs;
+constexpr int kMisVtxWords = 5 + kMisSegs;
 enum : unsigned {
     kMisValid = 1u, kMisMedium = 2u, kMisSpecular = 4u, kMisDelta = 8u, kMisLight = 16u, kMisCamera = 32u,
     kMisMiss = 64u
@@ -31,7 +32,7 @@ enum : unsigned {
 
 // Contribution record: kMisEvWords float4.
 //   e0: technique bits, weight, camera path bits, camera vertex index bits
-//   e1: light path bits, light vertex index bits, light id bits (NEE), 0
+//   e1: light path bits, light vertex index bits, light id bits (NEE), photon beam's origin offset from its vertex
 //   e2: light-side point.xyz, distance along the photon beam from its vertex (beams)
 //   e3: camera-side point.xyz, distance along the query ray from its vertex (query beams)
 //   e4: connection-ray segment count bits, 0, 0, 0
@@ -76,7 +77,8 @@ UPBP_D void mis_origin(bool light, unsigned path, float3 pos, float3 n, unsigned
 // The ray that reaches vertex k: its media segments (up to the real hit) and
 // its length to the vertex (the hit, a sampled scattering distance, or
 // infinity for a miss).
-UPBP_D void mis_ray(bool light, unsigned path, unsigned k, float dist, unsigned sflags, const LiteSeg* lsegs, int nlseg)
+UPBP_D void mis_ray(bool light, unsigned path, unsigned k, float3 dir, float dist, unsigned sflags,
+                    const LiteSeg* lsegs, int nlseg)
 {
     float4* v = mis_vertex(light, path, k);
     if (!v) return;
@@ -84,7 +86,8 @@ UPBP_D void mis_ray(bool light, unsigned path, unsigned k, float dist, unsigned 
     v[0] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kMisMiss));
     v[2] = make_float4(0.f, 0.f, 0.f, __uint_as_float((unsigned)n));
     v[3] = make_float4(dist, __uint_as_float(sflags), 1.f, 0.f);
-    for (int i = 0; i < n; i++) v[4 + i] = make_float4(lsegs[i].dmin, lsegs[i].dmax, __uint_as_float((unsigned)lsegs[i].med), 0.f);
+    v[4] = make_float4(dir.x, dir.y, dir.z, 0.f);
+    for (int i = 0; i < n; i++) v[5 + i] = make_float4(lsegs[i].dmin, lsegs[i].dmax, __uint_as_float((unsigned)lsegs[i].med), 0.f);
 }
 
 // The vertex the ray reached: position, frame, ids and its scattering function.
@@ -121,6 +124,7 @@ struct MisEvent {
     float weight;
     float3 pl, pc;
     float tl, tc;
+    float offset;
 };
 
 UPBP_D void mis_event(const MisEvent& e, const VolSeg* segs, int nseg)
@@ -131,7 +135,7 @@ UPBP_D void mis_event(const MisEvent& e, const VolSeg* segs, int nseg)
     float4* r = d.events + (size_t)i * kMisEvWords;
     const int n = min(nseg, kMisSegs);
     r[0] = make_float4(__uint_as_float(e.tech), e.weight, __uint_as_float(e.cam_path), __uint_as_float(e.cam_k));
-    r[1] = make_float4(__uint_as_float(e.light_path), __uint_as_float(e.light_k), __uint_as_float(e.light_id), 0.f);
+    r[1] = make_float4(__uint_as_float(e.light_path), __uint_as_float(e.light_k), __uint_as_float(e.light_id), e.offset);
     r[2] = make_float4(e.pl.x, e.pl.y, e.pl.z, e.tl);
     r[3] = make_float4(e.pc.x, e.pc.y, e.pc.z, e.tc);
     r[4] = make_float4(__uint_as_float((unsigned)n), 0.f, 0.f, 0.f);

@@ -86,6 +86,7 @@ class Scene:
     def __init__(self, scene: dict, header: np.ndarray):
         h = [float(x) for x in header]
         self.max_verts, self.light_paths, self.camera_paths = int(h[0]), int(h[1]), int(h[2])
+        self.events_total, self.event_capacity = int(h[3]), int(h[4])
         self.vtx_words, self.ev_words, self.segs = int(h[5]), int(h[6]), int(h[7])
         self.cam_origin, self.cam_dir = _vec(h[8:11]), _vec(h[11:14])
         self.image_plane_dist = h[14]
@@ -130,8 +131,13 @@ class Scene:
         return abs(co) * INV_PI
 
     def surface_cont(self, mat: int) -> float:
+        """Continuation probability of a surface (reference
+        bsdf.cuh:143-177): the largest reflectance component plus the
+        transmitted Fresnel part; without a dielectric the Fresnel reflectance
+        is 1, so it is the largest diffuse (+ phong + mirror) component."""
         m = self.materials[mat]
-        return min(1.0, max(0.0, max(m["diffuse"]) + 1.0))  # no Fresnel term without a dielectric
+        r = [a + b + c for a, b, c in zip(m["diffuse"], m["phong"], m["mirror"])]
+        return min(1.0, max(0.0, max(r)))
 
     def hg_pdf(self, med: int, travel_in: np.ndarray, w_out: np.ndarray) -> float:
         g = self.media[med]["g"]
@@ -158,15 +164,16 @@ class PathVertex:
 def _edge_pdfs(scene: Scene, segs, length: float, a_medium: bool, b_medium: bool) -> tuple[float, float]:
     """(pr, pl) of an edge from a to b of the given length whose media
     segments (dmin, dmax, medium) are measured from a: pr samples b from a,
-    pl samples a from b."""
+    pl samples a from b.  The recorded segment ends are float32 distances of
+    the GPU's trace and the length is recomputed in float64, so the segments
+    touching the end points are recognised within 1e-5 of the length."""
     pr = pl = 1.0
-    for d0, d1, med in segs:
-        d1 = min(d1, length)
-        if d1 <= d0:
-            continue
+    tol = 1e-5 * (1.0 + length)
+    segs = sorted((d0, min(d1, length), m) for d0, d1, m in segs if min(d1, length) > d0)
+    for j, (d0, d1, med) in enumerate(segs):
         ln = d1 - d0
-        at_b = d1 >= length * (1 - 1e-6) - 1e-7
-        at_a = d0 <= 1e-7
+        at_b = j == len(segs) - 1 and d1 >= length - tol
+        at_a = j == 0 and d0 <= tol
         pr *= scene.seg_pdf(med, ln, b_medium and at_b)
         pl *= scene.seg_pdf(med, ln, a_medium and at_a)
     return pr, pl
@@ -174,13 +181,19 @@ def _edge_pdfs(scene: Scene, segs, length: float, a_medium: bool, b_medium: bool
 
 class FullPath:
     """A full path x_0..x_k with the media segments of each edge
-    (edges[i] joins x_i and x_{i+1}, segments measured from x_i), and the
-    index of the merged vertex (None for BPT techniques)."""
+    (edges[i] joins x_i and x_{i+1}, segments measured from x_i), the
+    index of the merged vertex (None for BPT techniques), and per edge the
+    traced ray's direction (from x_i toward x_{i+1}) and length where a
+    subpath traced it (None for connections: those are taken from the
+    positions, as the renderer takes them).  Traced rays keep their own
+    direction and length because a float32 position is too coarse for a
+    medium vertex sampled a few micrometres from the previous one."""
 
-    def __init__(self, scene: Scene, verts: list, edges: list, merge: int | None):
+    def __init__(self, scene: Scene, verts: list, edges: list, merge: int | None, geo: list | None = None):
         self.s, self.v, self.e, self.merge = scene, verts, edges, merge
         self.k = len(verts) - 1
-        assert len(edges) == self.k
+        self.geo = geo if geo is not None else [None] * self.k
+        assert len(edges) == self.k and len(self.geo) == self.k
 
     def ends(self, i: int):
         """The two points edge i joins: x_i's camera-side point when x_i is
@@ -193,8 +206,18 @@ class FullPath:
 
     def _toward(self, i: int, j: int):
         """Unit direction from x_i to its neighbour x_j along their edge."""
-        a, b = self.ends(min(i, j))
+        e = min(i, j)
+        if self.geo[e] is not None:
+            d = self.geo[e][0]
+            return d if j > i else -d
+        a, b = self.ends(e)
         return _norm(b - a)[0] if j > i else _norm(a - b)[0]
+
+    def _length(self, e: int) -> float:
+        if self.geo[e] is not None:
+            return self.geo[e][1]
+        a, b = self.ends(e)
+        return _norm(b - a)[1]
 
     def _dir_pdf(self, i: int, toward: int) -> float:
         """Directional pdf at x_i of the direction toward its neighbour
@@ -227,8 +250,7 @@ class FullPath:
         k, sc, v = self.k, self.s, self.v
         pr_e, pl_e, len_e = [], [], []
         for i in range(k):
-            a, b = self.ends(i)
-            d = _norm(b - a)[1]
+            d = self._length(i)
             pr, pl = _edge_pdfs(sc, self.e[i], d, v[i].kind == "medium", v[i + 1].kind == "medium")
             pr_e.append(pr)
             pl_e.append(pl)
@@ -263,9 +285,26 @@ class FullPath:
                  "bb1d": sc.mis_bb1d * sin_t * fo * ro}
         return sum(terms.values()) if which is None else terms.get(which, 0.0)
 
-    def weight(self, tech: int, split: int) -> float:
+    def weight(self, tech: int, split: int, reference: bool = False, beam_offset: float = 0.0) -> float:
         """Balance-heuristic weight of technique `tech` (BPT split s = `split`,
-        or a merge at vertex `split`)."""
+        or a merge at vertex `split`).
+
+        reference=True gives instead the weight the reference's recursion
+        computes, which departs from the balance heuristic in three places:
+        * next-event estimation: its ratio for the emitter-hit technique
+          leaves out the camera-side free-flight pdf of the light ray
+          (functs_camera.cuh:296), i.e. it divides p(s=0) by pl of edge 0;
+        * BP2D and BB1D: the light side's area-measure conversion at the
+          merged point uses its distance from the photon beam's origin, not
+          from the light vertex (functs_bp2d.cuh:137-140,
+          functs_bb1d.cuh:189-193), which scales the connection technique
+          that ends the light subpath at x_{m-1} by (t / (offset + t))^2
+          (t the distance along the beam, offset from the vertex to the
+          beam's origin);
+        * BB1D beams leaving the light (m = 1) of a finite light skip the
+          conversion altogether (functs_bb1d.cuh:191), a factor
+          1 / (offset + t)^2 on that technique.
+        The three change a path's weights so that they no longer sum to one."""
         k, v, sc = self.k, self.v, self.s
         fwd, rev, pr_e, pl_e = self.pdfs()
 
@@ -287,7 +326,18 @@ class FullPath:
         def pde_pdf(i: int, which: str | None = None) -> float:
             return math.prod(fwd[:i + 1]) * math.prod(rev[i:]) * self.factor(i, pr_e, pl_e, which)
 
-        total = sum(bpt_pdf(s) for s in range(k + 1)) + sum(pde_pdf(i) for i in range(1, k))
+        terms = [bpt_pdf(s) for s in range(k + 1)]
+        if reference:
+            if tech == NEE:
+                terms[0] /= pl_e[0]
+            elif tech in (BP2D, BB1D):
+                dl = self._length(split - 1)
+                t = dl - beam_offset
+                f = (t / dl) ** 2
+                if tech == BB1D and split == 1:
+                    f = 1.0 / (dl * dl)
+                terms[split] *= f
+        total = sum(terms) + sum(pde_pdf(i) for i in range(1, k))
         if tech in (EMITTER_HIT, NEE, BPT, LIGHT_TRACE):
             cur = bpt_pdf(split)
         else:
@@ -306,9 +356,10 @@ class Records:
         self.camera = rec["camera"].reshape(sc.camera_paths, sc.max_verts, sc.vtx_words, 4)
         self.events = rec["events"].reshape(-1, sc.ev_words, 4)
 
-    def _vertex(self, table, path: int, k: int) -> tuple[PathVertex, list, float]:
+    def _vertex(self, table, path: int, k: int):
         """Vertex k of a subpath, the segments of the ray that reached it
-        (measured from vertex k - 1) and that ray's length to it."""
+        (measured from vertex k - 1), that ray's length to it and its unit
+        direction."""
         r = table[path, k]
         flags = _bits(r[0, 3])
         if not flags & VTX_VALID:
@@ -324,9 +375,9 @@ class Records:
             kind = "surface"
         pv = PathVertex(kind, r[0, :3], normal=r[1, :3] if kind in ("light", "surface", "camera") else None,
                         ident=ident, specular=bool(flags & (VTX_SPECULAR | VTX_DELTA)))
-        nseg = _bits(r[2, 3])
-        segs = [(float(r[4 + j, 0]), float(r[4 + j, 1]), _bits(r[4 + j, 2])) for j in range(nseg)]
-        return pv, segs, float(r[3, 0])
+        d = r[4, :3].astype(np.float64)
+        n = float(np.linalg.norm(d))
+        return pv, self._ray_segments(table, path, k), float(r[3, 0]), (d / n if n > 0 else d)
 
     @staticmethod
     def _clip(segs, length):
@@ -348,75 +399,85 @@ class Records:
         conn = [(float(ev[5 + j, 0]), float(ev[5 + j, 1]), _bits(ev[5 + j, 2])) for j in range(nconn)]
 
         def camera_part(upto: int):
-            """Camera vertices z_upto .. z_0 in light-to-camera order, and the
-            edges between them (segments measured from the light side)."""
-            vs, es = [], []
+            """Camera vertices z_upto .. z_0 in light-to-camera order, the
+            edges between them (segments measured from the light side) and
+            their traced directions (light to camera) and lengths."""
+            vs, es, gs = [], [], []
             for j in range(upto, -1, -1):
-                pv, segs, dist = self._vertex(self.camera, cam_path, j)
+                pv, segs, dist, d = self._vertex(self.camera, cam_path, j)
                 vs.append(pv)
                 if j > 0:
-                    d = float(np.linalg.norm(pv.pc - self._vertex(self.camera, cam_path, j - 1)[0].pc))
-                    es.append(self._flip(self._clip(segs, d), d))
-            return vs, es
+                    es.append(self._flip(self._clip(segs, dist), dist))
+                    gs.append((-d, dist))
+            return vs, es, gs
 
         def light_part(upto: int):
-            vs, es = [], []
+            vs, es, gs = [], [], []
             for j in range(upto + 1):
-                pv, segs, dist = self._vertex(self.light, light_path, j)
+                pv, segs, dist, d = self._vertex(self.light, light_path, j)
                 vs.append(pv)
                 if j > 0:
-                    d = float(np.linalg.norm(pv.pl - vs[-2].pl))
-                    es.append(self._clip(segs, d))
-            return vs, es
+                    es.append(self._clip(segs, dist))
+                    gs.append((d, dist))
+            return vs, es, gs
 
         sc = self.sc
         if tech == EMITTER_HIT:
-            vs, es = camera_part(t)
-            return FullPath(sc, vs, es, None), tech, 0
+            vs, es, gs = camera_part(t)
+            return FullPath(sc, vs, es, None, gs), tech, 0
         if tech == NEE:
             light_id = _bits(ev[1, 2])
             lt = sc.lights[light_id]
             n = np.cross(_vec(lt["p1"]) - _vec(lt["p0"]), _vec(lt["p2"]) - _vec(lt["p0"]))
             lv = PathVertex("light", pl, normal=n, ident=light_id)
-            cvs, ces = camera_part(t)
+            cvs, ces, cgs = camera_part(t)
             d = float(np.linalg.norm(cvs[0].pc - pl))
-            return FullPath(sc, [lv] + cvs, [self._flip(self._clip(conn, d), d)] + ces, None), tech, 1
+            return FullPath(sc, [lv] + cvs, [self._flip(self._clip(conn, d), d)] + ces, None, [None] + cgs), tech, 1
         if tech == BPT:
-            lvs, les = light_part(s)
-            cvs, ces = camera_part(t)
+            lvs, les, lgs = light_part(s)
+            cvs, ces, cgs = camera_part(t)
             d = float(np.linalg.norm(cvs[0].pc - lvs[-1].pl))
-            return FullPath(sc, lvs + cvs, les + [self._flip(self._clip(conn, d), d)] + ces, None), tech, s + 1
+            return (FullPath(sc, lvs + cvs, les + [self._flip(self._clip(conn, d), d)] + ces, None, lgs + [None] + cgs),
+                    tech, s + 1)
         if tech == LIGHT_TRACE:
-            lvs, les = light_part(s)
+            lvs, les, lgs = light_part(s)
             cam = PathVertex("camera", sc.cam_origin)
             d = float(np.linalg.norm(sc.cam_origin - lvs[-1].pl))
-            return FullPath(sc, lvs + [cam], les + [self._clip(conn, d)], None), tech, s + 1
+            return FullPath(sc, lvs + [cam], les + [self._clip(conn, d)], None, lgs + [None]), tech, s + 1
         # merges: the light side up to the merged vertex (the photon y_s, or
         # the point at tl on the photon beam of the ray y_{s-1} -> y_s), the
         # camera side from it (the camera vertex z_t, or the point at tc on the
         # query ray z_{t-1} -> z_t)
         if tech in (SURF, PP3D, PB2D):
-            lvs, les = light_part(s)
+            lvs, les, lgs = light_part(s)
             photon = lvs[-1]
         else:
-            lvs, les = light_part(s - 1)
-            segs = self._ray_segments(self.light, light_path, s)
+            lvs, les, lgs = light_part(s - 1)
+            _, segs, _, d = self._vertex_ray(self.light, light_path, s)
             les.append(self._clip(segs, tl))
+            lgs.append((d, tl))
             photon = PathVertex("medium", pl, ident=self._medium_at(segs, tl))
             lvs.append(photon)
         if tech in (SURF, PP3D, BP2D):
-            cvs, ces = camera_part(t)
+            cvs, ces, cgs = camera_part(t)
             cam = cvs[0]
             cvs = cvs[1:]
         else:
-            cvs, ces = camera_part(t - 1)
-            segs = self._ray_segments(self.camera, cam_path, t)
+            cvs, ces, cgs = camera_part(t - 1)
+            _, segs, _, d = self._vertex_ray(self.camera, cam_path, t)
             ces = [self._flip(self._clip(segs, tc), tc)] + ces
+            cgs = [(-d, tc)] + cgs
             cam = PathVertex("medium", pc, ident=self._medium_at(segs, tc))
         # the camera side's scattering function at the merged vertex
         mv = PathVertex(cam.kind, photon.pl, cam.pc, normal=cam.normal, ident=cam.id, normal_l=photon.normal)
         m = len(lvs) - 1
-        return FullPath(sc, lvs[:-1] + [mv] + cvs, les + ces, m), tech, m
+        return FullPath(sc, lvs[:-1] + [mv] + cvs, les + ces, m, lgs + cgs), tech, m
+
+    def _vertex_ray(self, table, path, k):
+        """The ray that reached slot k (recorded even when it hit nothing)."""
+        r = table[path, k]
+        d = r[4, :3].astype(np.float64)
+        return None, self._ray_segments(table, path, k), float(r[3, 0]), d / np.linalg.norm(d)
 
     def _has(self, table, path, k) -> bool:
         return bool(_bits(table[path, k, 0, 3]) & VTX_VALID)
@@ -424,7 +485,7 @@ class Records:
     def _ray_segments(self, table, path, k):
         r = table[path, k]
         nseg = _bits(r[2, 3])
-        return [(float(r[4 + j, 0]), float(r[4 + j, 1]), _bits(r[4 + j, 2])) for j in range(nseg)]
+        return [(float(r[5 + j, 0]), float(r[5 + j, 1]), _bits(r[5 + j, 2])) for j in range(nseg)]
 
     @staticmethod
     def _medium_at(segs, t):
@@ -434,17 +495,22 @@ class Records:
                 return m
         return segs[-1][2]
 
-    def check(self, limit: int | None = None):
-        """(technique, GPU weight, FP64 weight) of every supported
-        contribution, and the count of unsupported ones."""
+    def check(self, limit: int | None = None, reference: bool | None = None):
+        """(technique, GPU weight, FP64 weight, full path length) of every
+        supported contribution, and the count of unsupported ones.  The FP64
+        weight is the balance heuristic, or the reference's form of it
+        (FullPath.weight) when the renderer ran without mis_exact (or
+        `reference` says so)."""
+        if reference is None:
+            reference = not self.sc.mis_exact
         out, skipped = [], 0
         evs = self.events if limit is None else self.events[:limit]
         for ev in evs:
             try:
                 fp, tech, split = self.full_path(ev)
-                w = fp.weight(tech, split)
+                w = fp.weight(tech, split, reference=reference, beam_offset=float(ev[1, 3]))
             except (NotImplementedError, KeyError):
                 skipped += 1
                 continue
-            out.append((tech, float(ev[0, 1]), w))
+            out.append((tech, float(ev[0, 1]), w, fp.k))
         return out, skipped

@@ -1,0 +1,98 @@
+"""Per-path MIS weights of the GPU renderer against the FP64 full-path
+oracle (oracle/mis_fp64.py).
+
+The recording build of the library (libupbp_b200_misdbg.so, the same
+sources compiled with UPBP_MIS_DEBUG) keeps, for one iteration, every
+subpath vertex with the media segments of the ray that reached it and every
+contribution with the FP32 weight the renderer applied.  The oracle rebuilds
+each contribution's full path and evaluates the balance heuristic over all
+of its vertices and techniques in float64.
+
+* With -mis_exact every weight of every technique (emitter hits, NEE, BPT,
+  light tracing, SURF, PP3D, PB2D, BB1D, BP2D) agrees with the FP64
+  balance heuristic within 1e-4 relative: on the 256x256 box scene's
+  geometry (config 1: diffuse box, icosphere medium, quad light; path length
+  8) and on the dense-beam enclosure at path length 16 (sigma_t 5.05), where
+  the FP32 recursion runs over up to 16 vertices.
+* Without it (the reference's weights, the default) every weight agrees
+  within 1e-4 with the oracle's statement of the reference's three
+  departures from the balance heuristic (FullPath.weight), and the
+  departures are real: weights of those techniques move by up to tens of
+  percent, and on such a path the weights of all techniques no longer sum to
+  one.
+"""
+import collections
+
+import numpy as np
+import pytest
+
+from gpuupbp_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+ALL6 = "upbp_bpt+surf+pp3d+pb2d+bb1d+bp2d"
+CASES = {
+    "box": ("box_medium", ["-a", ALL6, "-l", "8", "-r", "24x24", "-r_initial", "-0.02", "-r_alpha", "0.75"]),
+    "dense": ("dense_beams", ["-a", ALL6, "-l", "16", "-r", "16x16", "-r_initial_bb1d", "-0.004",
+                              "-r_initial_bp2d", "-0.004"]),
+}
+TOL = 1e-4
+
+
+def _records(case, scene_dir, exact, iteration=0):
+    import mis_fp64
+    from gpuupbp_b200 import upbp
+    workload, args = CASES[case]
+    full = ["-s", "-1", scenes.write_workload(workload, scene_dir)] + args + (["-mis_exact"] if exact else [])
+    r = upbp.Renderer(full, library=upbp.MISDBG_LIB_PATH)
+    r.run_iteration(iteration)
+    rec = r.mis_records()
+    r.close()
+    sc = upbp.load_scene(full)
+    return mis_fp64.Records(rec, {k: sc[k] for k in ("lights", "materials", "media")})
+
+
+def _by_technique(rows):
+    by = collections.defaultdict(list)
+    for tech, w_gpu, w_fp64, k in rows:
+        by[tech].append((w_gpu, w_fp64, k))
+    return {t: np.array(v) for t, v in by.items()}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_weights_equal_fp64_full_path_balance_heuristic(case, scene_dir):
+    import mis_fp64
+    rec = _records(case, scene_dir, exact=True)
+    assert int(rec.sc.mis_exact) == 1
+    assert rec.sc.events_total <= rec.sc.event_capacity  # no contribution was left unrecorded
+    rows, skipped = rec.check()
+    assert skipped == 0 and len(rows) > 5000
+    by = _by_technique(rows)
+    want = {mis_fp64.NEE, mis_fp64.BPT, mis_fp64.LIGHT_TRACE, mis_fp64.BB1D, mis_fp64.PB2D, mis_fp64.BP2D}
+    if case == "box":
+        want |= {mis_fp64.SURF, mis_fp64.EMITTER_HIT}
+    assert want <= set(by), sorted(by)
+    for tech, a in by.items():
+        rel = np.abs(a[:, 0] - a[:, 1]) / a[:, 1]
+        assert rel.max() <= TOL, (mis_fp64.TECH_NAMES[tech], rel.max(), int((rel > TOL).sum()), len(a))
+    if case == "dense":
+        # paths of up to 16 vertices are checked
+        assert max(int(a[:, 2].max()) for a in by.values()) >= 15
+
+
+def test_reference_weights_equal_the_oracles_statement_of_its_departures(scene_dir):
+    import mis_fp64
+    rec = _records("box", scene_dir, exact=False)
+    assert int(rec.sc.mis_exact) == 0
+    rows, skipped = rec.check()  # the reference's form
+    assert skipped == 0
+    by = _by_technique(rows)
+    for tech, a in by.items():
+        rel = np.abs(a[:, 0] - a[:, 1]) / a[:, 1]
+        assert rel.max() <= TOL, (mis_fp64.TECH_NAMES[tech], rel.max())
+    # and they are departures: against the balance heuristic the same
+    # weights differ, only in these three techniques
+    exact, _ = rec.check(reference=False)
+    moved = collections.Counter(t for t, wg, wo, k in exact if abs(wg - wo) > TOL * wo)
+    assert set(moved) <= {mis_fp64.NEE, mis_fp64.BB1D, mis_fp64.BP2D}
+    assert moved[mis_fp64.BB1D] > 100 and moved[mis_fp64.NEE] > 10
