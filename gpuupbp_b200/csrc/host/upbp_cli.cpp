@@ -60,6 +60,8 @@ void print_usage(const char* prog)
     std::printf("    -r_alpha[_surf|_pp3d|_pb2d|_bb1d|_bp2d] <a>  -r_initial[_...] <r> (negative: x scene radius)\n");
     std::printf("    -previous -compatible -speconly -ignorespec 0|1 -qbt S|L -pbt S|L -pbc <n>\n");
     std::printf("    -continuous_output <n> -pcpi <n> -sn 0|1 -assert -ioff <iter> -log\n");
+    std::printf("    -guide <n>   (this build only) learned proposal for scattering in media, trained during\n"
+                "                 the first n iterations\n");
     std::printf("    -mis_exact   (this build only) MIS weights of the full-path balance heuristic where the\n"
                 "                 reference's recursion departs from it (photon-beam distances, NEE through media)\n");
 }
@@ -280,6 +282,15 @@ extern "C" int upbp_parse_command_line(int argc, const char** argv, upbp_config*
             } else if (a == "-log") {
                 c.do_log = 1;
                 extra << "_log";
+            } else if (a == "-guide") {
+                // not in the reference: learned proposal for scattering in media
+                const char* v = need("-guide");
+                if (!v) return fail("missing argument of -guide option");
+                char* end = nullptr;
+                const long n = std::strtol(v, &end, 10);
+                if (end == v || n < 0) return fail("invalid argument of -guide option");
+                c.guide_train_iterations = (int)n;
+                extra << "_guide" << n;
             } else if (a == "-mis_exact") {
                 // not in the reference: full-path balance-heuristic weights
                 // where the reference's recursion departs from them

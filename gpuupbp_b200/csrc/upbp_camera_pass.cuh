@@ -269,7 +269,7 @@ UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVe
     const float ph = hg_pdf(-q.d, pdir, m.mean_cosine, &sin_theta);
     const float3 f = v3(ph);
     if (is_black_or_negative(f)) return v3(0.f);
-    const float fpdf = ph * m.cont_prob;
+    const float fpdf = guide_pdf_at(q.o + q.d * isect_dist, q.med, q.d, pdir, ph) * m.cont_prob;
     const float rpdf = ph * lv.bsdf.cont_prob;
     wc.d_shared *= isect_dist * isect_dist;
     wc.d_shared /= rs_for;
@@ -339,7 +339,7 @@ UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& l
     const float ph = hg_pdf(-q.d, -lb.d, m.mean_cosine, nullptr);
     const float3 f = v3(ph);
     if (is_black_or_negative(f)) return v3(0.f);
-    const float fpdf = ph * m.cont_prob;
+    const float fpdf = guide_pdf_at(q.o + q.d * tc, q.med, q.d, -lb.d, ph) * m.cont_prob;
     const float rpdf = ph * m.cont_prob;
     wc.d_shared *= tc * tc;
     wc.d_shared /= rsf_c;
@@ -412,7 +412,7 @@ UPBP_D float3 eval_bp2d(const Beam& lb, unsigned cam_len, const VertexWeights& w
     const float ph = hg_pdf(cdir, -lb.d, m.mean_cosine, &sin_theta);
     const float3 f = v3(ph);
     if (is_black_or_negative(f)) return v3(0.f);
-    const float fpdf = ph * cb.cont_prob;
+    const float fpdf = guide_pdf(cb, -cdir, -lb.d, ph) * cb.cont_prob;
     const float rpdf = ph * m.cont_prob;
     // the reference measures the distance from the beam's origin, which lies
     // past the light vertex when the beam starts at a medium boundary
@@ -1132,7 +1132,7 @@ UPBP_D bool camera_path_bounce(CameraLane& c, VolSeg* segs, LiteSeg* lsegs)
     if (isect.on_surface())
         bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, false, relative_ior(isect, s.stack));
     else
-        bsdf_setup_medium(bsdf, rd, isect.med, false);
+        bsdf_setup_medium(bsdf, rd, isect.med, false, ro + rd * isect.dist);
     if (!bsdf.valid()) return false;
     float ratio = 0.f;
     if (bsdf.in_medium()) ratio = 1.f / p.media[bsdf.id].min_pos_att;

@@ -167,6 +167,12 @@ __global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* co
     counts[i] = k;
 }
 
+}  // namespace
+
+#include "upbp_guide_train.cuh"
+
+namespace {
+
 struct Geometry {
     BvhNode* nodes = nullptr;
     float4* tri = nullptr;
@@ -256,6 +262,8 @@ struct upbp_ctx {
     unsigned iterations = 0;
     uint64_t triangles = 0;
     MisDebug mis{};  // MIS recording buffers (recording build only)
+    GuideState guide;  // learned proposal (guide.train_iterations > 0)
+    float3 bbox_lo{}, bbox_hi{};
 };
 
 namespace {
@@ -718,6 +726,8 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
             const float3 hi = make_float3(s->bbox_max[0], s->bbox_max[1], s->bbox_max[2]);
             float r2 = dot(hi - lo, hi - lo);
             if (r2 == 0.f || r2 > kInfinity) r2 = 1.f;
+            c->bbox_lo = lo;
+            c->bbox_hi = hi;
             P.scene_center = (hi + lo) * .5f;
             P.scene_radius = std::sqrt(r2) * .5f;
             P.inv_radius_sqr = 1.f / (P.scene_radius * P.scene_radius);
@@ -903,6 +913,46 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         P.path_color = c->d_path_color;
         P.hit_state = c->d_hit_state;
         P.cam_fb = c->d_cam_fb;
+        if (cfg->guide_train_iterations > 0) {
+            GuideState& g = c->guide;
+            g.train_iterations = cfg->guide_train_iterations;
+            // media slots: every scattering medium, up to the one-hot width
+            std::vector<int> slot(s->medium_count, -1);
+            std::vector<float> med_g(s->medium_count, 0.f);
+            for (uint32_t i = 0; i < s->medium_count; i++) {
+                med_g[i] = meds[i].mean_cosine;
+                if (meds[i].has_scattering && g.slots < kGuideMedia) slot[i] = g.slots++;
+            }
+            if (g.slots > 0) {
+                const unsigned rows = 1u << 18;
+                // cells per axis so that the table fits the batch buffers
+                // (cells^3 x 64 direction bins x slots rows), at most 12
+                g.cells = 12;
+                while (g.cells > 2 && (unsigned)g.cells * g.cells * g.cells * g.dir_res * g.dir_res * g.slots > rows)
+                    g.cells--;
+                g.table_rows = (unsigned)g.cells * g.cells * g.cells * g.dir_res * g.dir_res * g.slots;
+                const float3 ext = c->bbox_hi - c->bbox_lo;
+                g.ext = make_float3(fmaxf(ext.x, 1e-3f), fmaxf(ext.y, 1e-3f), fmaxf(ext.z, 1e-3f));
+                g.lo = c->bbox_lo;
+                UPBP_CK(dupload(&g.medium_slot, slot.data(), slot.size(), c->st));
+                UPBP_CK(dupload(&g.med_g, med_g.data(), med_g.size(), c->st));
+                UPBP_CK(guide_alloc_net(g.net, c->st));
+                std::vector<float> w0;
+                guide_init_params(w0);
+                UPBP_CK(guide_set_params(g.net, w0.data(), c->st));
+                UPBP_CK(guide_alloc_batch(g.batch, rows));
+                g.rec_capacity = 1u << 20;
+                UPBP_CK(dalloc(&g.recs, g.rec_capacity));
+                UPBP_CK(dalloc(&g.rec_count, 1));
+                UPBP_CK(cudaMemsetAsync(g.rec_count, 0, sizeof(unsigned), c->st));
+                for (auto& t : g.table) UPBP_CK(dalloc(&t, (size_t)g.table_rows * kGuideEntryWords));
+                P.guide_recs = g.recs;
+                P.guide_rec_count = g.rec_count;
+                P.guide_rec_capacity = g.rec_capacity;
+            } else {
+                g.train_iterations = 0;  // no scattering medium to guide in
+            }
+        }
 #ifdef UPBP_MIS_DEBUG
         {
             MisDebug& m = c->mis;
@@ -957,6 +1007,25 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             UPBP_CK(cudaMemcpyToSymbolAsync(c_misdbg, &m, sizeof(m), 0, cudaMemcpyHostToDevice, c->st));
         }
 #endif
+        GuideState& gs = c->guide;
+        const bool guide_training = gs.train_iterations > 0 && iteration < gs.train_iterations;
+        {
+            // the proposal table trained before this iteration began (none in
+            // the first): both passes of the iteration read the same one
+            GuideTable& t = P.guide;
+            t = GuideTable{};
+            if (gs.front >= 0) {
+                const float3 cell = make_float3(gs.ext.x / gs.cells, gs.ext.y / gs.cells, gs.ext.z / gs.cells);
+                t.entries = gs.table[gs.front];
+                t.lo = gs.lo;
+                t.inv_cell = make_float3(1.f / cell.x, 1.f / cell.y, 1.f / cell.z);
+                t.cells = gs.cells;
+                t.dir_res = gs.dir_res;
+                t.slots = gs.slots;
+                t.medium_slot = gs.medium_slot;
+            }
+            P.guide_collect = guide_training ? 1 : 0;
+        }
         unsigned found[4] = {0, 0, 0, 0};
         if (P.trace_light_paths) {
             // radius schedule and MIS factors (renderer.cpp:57-119)
@@ -1013,6 +1082,20 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             }
         } else {
             P.iteration = (unsigned)iteration;
+        }
+        if (guide_training) {
+            // train on every record collected so far, then bake the network
+            // into the back table, which the next iteration renders with
+            for (int k = 0; k < gs.steps_per_iteration; k++)
+                guide_train_step(c->st, gs, (unsigned)(iteration * gs.steps_per_iteration + k + 1));
+            const int back = gs.front == 0 ? 1 : 0;
+            guide_fill_table(c->st, gs, gs.table[back]);
+            UPBP_CK(cudaGetLastError());
+            UPBP_CK(cudaMemcpyAsync(gs.h_scal, gs.batch.scal, 2 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            gs.last_loss = gs.h_scal[0] / (float)gs.batch.rows;
+            gs.front_next = back;
+            launches += gs.steps_per_iteration * 16 + 3;
         }
         UPBP_CK(cudaEventRecord(ev[1], c->st));
 
@@ -1289,6 +1372,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         c->iterations++;
         c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
         c->status_seen |= *c->h_status;
+        if (guide_training) gs.front = gs.front_next;
         return (int)*c->h_status;
     });
 }
@@ -1553,6 +1637,72 @@ extern "C" int upbp_debug_mis_records(upbp_ctx* c, int which, float* out, uint64
     });
 }
 
+// State of the learned proposal: training iterations, Adam steps, last batch
+// loss, records collected, table rows, cells per axis, direction bins per
+// axis, media slots, table in use (-1 none).
+extern "C" int upbp_guide_info(upbp_ctx* c, float* out, uint32_t n)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !out) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        const GuideState& g = c->guide;
+        unsigned recs = 0;
+        if (g.rec_count) {
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            UPBP_CK(cudaMemcpy(&recs, g.rec_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        }
+        const float v[] = {(float)g.train_iterations, (float)g.net.steps, g.last_loss, (float)recs,
+                           (float)g.table_rows, (float)g.cells, (float)g.dir_res, (float)g.slots, (float)g.front};
+        for (uint32_t i = 0; i < n; i++) out[i] = i < sizeof(v) / sizeof(v[0]) ? v[i] : 0.f;
+        return UPBP_OK;
+    });
+}
+
+// One forward and backward pass of the proposal's network on given inputs,
+// for checking the tensor-core training kernels against a float64 restatement.
+extern "C" int upbp_guide_gradients(const float* params, const float* x, const float* t, uint32_t rows, float* grads,
+                                    float* outputs, float* loss)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!params || !x || !t || !grads || rows == 0) return UPBP_ERR_ARGS;
+        cudaStream_t st = nullptr;
+        UPBP_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        GuideNet net;
+        GuideBatch b;
+        int rc = UPBP_OK;
+        auto run = [&]() -> int {
+            UPBP_CK(guide_alloc_net(net, st));
+            UPBP_CK(guide_set_params(net, params, st));
+            UPBP_CK(guide_alloc_batch(b, rows));
+            std::vector<__half> xh((size_t)rows * kGuideInPad);
+            for (size_t i = 0; i < xh.size(); i++) xh[i] = __float2half(x[i]);
+            UPBP_CK(cudaMemcpyAsync(b.X, xh.data(), xh.size() * sizeof(__half), cudaMemcpyHostToDevice, st));
+            UPBP_CK(cudaMemcpyAsync(b.T, t, (size_t)rows * sizeof(float4), cudaMemcpyHostToDevice, st));
+            guide_forward(st, net, b, b.X, rows);
+            guide_loss(st, b, rows);
+            UPBP_CK(cudaMemsetAsync(net.grad, 0, kGuideParams * sizeof(float), st));
+            guide_backward(st, net, b, rows);
+            UPBP_CK(cudaGetLastError());
+            UPBP_CK(cudaMemcpyAsync(grads, net.grad, kGuideParams * sizeof(float), cudaMemcpyDeviceToHost, st));
+            if (outputs)
+                UPBP_CK(cudaMemcpyAsync(outputs, b.O, (size_t)rows * kGuideOutPad * sizeof(float),
+                                        cudaMemcpyDeviceToHost, st));
+            float scal[2];
+            UPBP_CK(cudaMemcpyAsync(scal, b.scal, sizeof(scal), cudaMemcpyDeviceToHost, st));
+            UPBP_CK(cudaStreamSynchronize(st));
+            if (loss) *loss = scal[0];
+            return UPBP_OK;
+        };
+        rc = run();
+        cudaStreamSynchronize(st);
+        guide_free_net(net);
+        guide_free_batch(b);
+        cudaStreamDestroy(st);
+        return rc;
+    });
+}
+
 extern "C" void* upbp_get_stream(upbp_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 extern "C" int upbp_get_device(const upbp_ctx* c) { return c ? c->dev : UPBP_ERR_ARGS; }
@@ -1582,6 +1732,14 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     for (void* b : bufs)
         if (b) cudaFree(b);
     free_scratch(c->sc);
+    {
+        GuideState& g = c->guide;
+        guide_free_net(g.net);
+        guide_free_batch(g.batch);
+        void* p[] = {g.recs, g.rec_count, g.table[0], g.table[1], g.medium_slot, g.med_g};
+        for (void* x : p)
+            if (x) cudaFree(x);
+    }
     for (auto& slot : c->ev_ring)
         for (auto& e : slot)
             if (e) cudaEventDestroy(e);

@@ -291,6 +291,23 @@ struct HitState {
     unsigned pad;
 };
 
+// Learned proposal table (upbp_guide.cuh): entries over cells^3 x dir_res^2
+// directions of travel x media slots; entries == nullptr: no guiding.
+struct GuideTable {
+    const float4* entries;
+    float3 lo, inv_cell;     // scene box and grid step
+    int cells, dir_res;      // cells per axis, direction bins per octahedral axis
+    int slots;               // media slots in the table
+    const int* medium_slot;  // medium id -> slot, -1 if not guided
+};
+
+// Training record of the learned proposal, one per medium vertex of a light
+// subpath.
+struct GuideRecord {
+    float4 a;  // position.xyz, medium bits
+    float4 b;  // direction of travel of the light subpath.xyz, throughput luminance
+};
+
 struct DeviceParams {
     // scene
     const DMaterial* materials;
@@ -400,6 +417,15 @@ struct DeviceParams {
     // ends a path in the reference, so contributions with a later key drop.
     unsigned* path_err;
     float4* path_color;
+
+    // learned proposal: the table camera subpaths sample and every
+    // camera-direction pdf reads; the light pass appends training records
+    // while guide_collect is set
+    GuideTable guide;
+    GuideRecord* guide_recs;
+    unsigned* guide_rec_count;
+    unsigned guide_rec_capacity;
+    int guide_collect;
 };
 
 // Event keys order the contributions of a camera path as the reference's

@@ -240,7 +240,7 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
         bsdf_setup_surface(bsdf, rd, isect.normal, isect.shading_normal, isect.mat, true, relative_ior(isect, s.stack));
     } else {
         frame_src = rd;
-        bsdf_setup_medium(bsdf, rd, isect.med, true);
+        bsdf_setup_medium(bsdf, rd, isect.med, true, ro + rd * isect.dist);
     }
     if (!bsdf.valid()) return false;
     float ratio = 0.f;
@@ -281,6 +281,14 @@ UPBP_D bool light_path_bounce(LightLane& l, VolSeg* segs, LiteSeg* lsegs)
                 p.idx_surface[k] = slot;
             }
         }
+    }
+    if (p.guide_collect && bsdf.in_medium()) {
+        // a training record of the learned proposal: where light arrives in
+        // the medium, from which direction, with how much throughput
+        const unsigned k = warp_reserve1(p.guide_rec_count);
+        if (k < p.guide_rec_capacity)
+            p.guide_recs[k] = GuideRecord{make_float4(hitpoint.x, hitpoint.y, hitpoint.z, ubits((unsigned)bsdf.id)),
+                                          make_float4(rd.x, rd.y, rd.z, luminance(s.throughput))};
     }
     if (p.do_bpt && !bsdf.delta() && (bsdf.in_medium() || p.connect_to_camera_from_surf)) {
         if (s.path_length + 1 >= p.min_path_length) {

@@ -196,12 +196,14 @@ UPBP_D void read_vertex(Fetch&& q, LightVertex& v)
         b.phong_prob = q7.y;
         b.refl_prob = q7.z;
         b.refr_prob = q7.w;
+        b.gcell = -1;
     } else {
         const DMedium& m = c_params.media[b.id];
         b.mean_cosine = q4.w;
         b.world_dir_fix = xyz(q5);
         b.scatter_coef = m.scattering;
         b.scatter_pos = !is_black_or_negative(m.scattering);
+        b.gcell = guide_cell(c_params.guide, v.hit, b.id);
     }
 }
 

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "upbp_device.cuh"
+#include "upbp_guide.cuh"
 
 namespace upbp {
 
@@ -194,6 +195,7 @@ struct Bsdf {
     float mean_cosine;
     float3 scatter_coef;
     bool scatter_pos;
+    int gcell;               // learned-proposal cell of a medium vertex (-1: phase function only)
 
     UPBP_D bool valid() const { return flags & kBsdfValid; }
     UPBP_D bool delta() const { return flags & kBsdfDelta; }
@@ -204,6 +206,23 @@ struct Bsdf {
     UPBP_D float d_factor() const { return on_surface() ? fabsf(local_dir_fix.z) : 1.f; }
     UPBP_D float3 dir_fix() const { return on_surface() ? frame.to_world(local_dir_fix) : world_dir_fix; }
 };
+
+// Pdf of a camera subpath scattering at a medium vertex from direction of
+// travel `travel` into `out`: the blend of the phase function (value hg) and
+// the learned mixture, or hg where the vertex is not guided.
+UPBP_D float guide_pdf(const Bsdf& b, float3 travel, float3 out, float hg)
+{
+    const float4* e = guide_entry(c_params.guide, b.gcell, travel);
+    return e ? .5f * hg + .5f * vmf_mix_pdf(e, out) : hg;
+}
+
+// The same at a point of medium `med` that is not a vertex (a query beam's
+// merge point).
+UPBP_D float guide_pdf_at(float3 x, int med, float3 travel, float3 out, float hg)
+{
+    const float4* e = guide_entry(c_params.guide, guide_cell(c_params.guide, x, med), travel);
+    return e ? .5f * hg + .5f * vmf_mix_pdf(e, out) : hg;
+}
 
 UPBP_D void bsdf_component_probs(Bsdf& b, const DMaterial& m)
 {
@@ -232,6 +251,7 @@ UPBP_D void bsdf_setup_surface(Bsdf& b, float3 ray_dir, float3 normal, float3 sh
                                bool from_light, float ior)
 {
     b.flags = from_light ? kBsdfFromLight : 0;
+    b.gcell = -1;
     const DMaterial& m = c_params.materials[mat_id];
     b.id = mat_id;
     b.frame.set_from_z(shading_normal);
@@ -248,12 +268,13 @@ UPBP_D void bsdf_setup_surface(Bsdf& b, float3 ray_dir, float3 normal, float3 sh
     b.flags |= kBsdfValid;
 }
 
-UPBP_D void bsdf_setup_medium(Bsdf& b, float3 ray_dir, int med_id, bool from_light)
+UPBP_D void bsdf_setup_medium(Bsdf& b, float3 ray_dir, int med_id, bool from_light, float3 x)
 {
     b.flags = (from_light ? kBsdfFromLight : 0) | kBsdfInMedium;
     const int idx = min(med_id, c_params.medium_count - 1);
     const DMedium& m = c_params.media[idx];
     b.id = idx;
+    b.gcell = guide_cell(c_params.guide, x, idx);
     b.world_dir_fix = -ray_dir;
     b.frame.set_from_z(-b.world_dir_fix);
     b.cont_prob = m.cont_prob;
@@ -326,8 +347,12 @@ UPBP_D float3 bsdf_eval(const Bsdf& b, float3 dir_gen, float& cos_gen, float* fp
         return v3(0.f);
     }
     const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, sin_theta);
-    if (fpdf) *fpdf = p;
-    if (rpdf) *rpdf = p;
+    // light subpaths sample the phase function; camera subpaths its blend
+    // with the learned proposal (the phase function is symmetric, so p is
+    // also its reverse pdf)
+    const bool light = b.from_light();
+    if (fpdf) *fpdf = light ? p : guide_pdf(b, -b.world_dir_fix, dir_gen, p);
+    if (rpdf) *rpdf = light ? guide_pdf(b, -dir_gen, b.world_dir_fix, p) : p;
     return b.scatter_coef * p;
 }
 
@@ -349,7 +374,11 @@ UPBP_D float bsdf_pdf(const Bsdf& b, float3 dir_gen, bool reverse)
         pdf_phong(b, m, lg, &fp, &rp);
         return reverse ? rp : fp;
     }
-    return hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, nullptr);
+    const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, nullptr);
+    // the camera side's pdfs use the learned proposal's blend (bsdf_eval)
+    if (b.from_light() == reverse) return reverse ? guide_pdf(b, -dir_gen, b.world_dir_fix, p)
+                                                  : guide_pdf(b, -b.world_dir_fix, dir_gen, p);
+    return p;
 }
 
 // Samples a direction (bsdf.cuh:571-658).
@@ -437,8 +466,21 @@ UPBP_D float3 bsdf_sample(const Bsdf& b, float r0, float r1, float r2, float3& d
         sin_theta = 0.f;
         return v3(0.f);
     }
-    hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
-    return b.scatter_coef * pdf;
+    const float4* e = b.from_light() ? nullptr : guide_entry(c_params.guide, b.gcell, -b.world_dir_fix);
+    if (!e) {
+        hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
+        return b.scatter_coef * pdf;
+    }
+    // blend of the phase function and the learned mixture, one half each:
+    // r2 picks the component (and, rescaled, the mixture's lobe)
+    if (r2 < .5f) {
+        hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
+    } else {
+        dir_gen = vmf_mix_sample(e, 2.f * r2 - 1.f, r0, r1);
+    }
+    const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, &sin_theta);
+    pdf = .5f * p + .5f * vmf_mix_pdf(e, dir_gen);
+    return b.scatter_coef * p;
 }
 
 // ---------------------------------------------------------------- lights

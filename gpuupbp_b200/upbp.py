@@ -45,7 +45,7 @@ class Config(ctypes.Structure):
         ("surf_radius_initial", ctypes.c_float), ("surf_radius_alpha", ctypes.c_float),
         ("continuous_output", ctypes.c_int), ("ignore_fully_spec_paths", ctypes.c_int), ("gpu_assert", ctypes.c_int),
         ("iteration_offset", ctypes.c_uint64), ("do_log", ctypes.c_int), ("use_shading_normal", ctypes.c_int),
-        ("mis_exact", ctypes.c_int),
+        ("mis_exact", ctypes.c_int), ("guide_train_iterations", ctypes.c_int),
     ]
 
 
@@ -117,7 +117,7 @@ EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_pr
            "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
            "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
            "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device",
-           "upbp_debug_mis_records"]
+           "upbp_debug_mis_records", "upbp_guide_info", "upbp_guide_gradients"]
 
 _libs = {}
 
@@ -147,6 +147,8 @@ def load_library(path: str = LIB_PATH):
     L.upbp_get_stream.argtypes = [VP]
     L.upbp_get_stream.restype = VP
     L.upbp_get_device.argtypes = [VP]
+    L.upbp_guide_info.argtypes = [VP, VP, ctypes.c_uint32]
+    L.upbp_guide_gradients.argtypes = [VP, VP, VP, ctypes.c_uint32, VP, VP, VP]
     L.upbp_debug_mis_records.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint64, P(ctypes.c_uint64)]
     L.upbp_last_error.restype = ctypes.c_char_p
     L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]

@@ -101,6 +101,15 @@ typedef struct upbp_config {
      * the camera-side sampling pdf of the media its light ray crosses.  0
      * (the default) keeps the reference's weights. */
     int mis_exact;
+    /* Not in the reference (command line -guide <n>): when n > 0, a learned
+     * proposal guides the scattering of camera subpaths in media -- an MLP
+     * (position under a 12-band frequency encoding, direction of travel,
+     * one-hot medium -> 8-lobe von Mises-Fisher mixture, blended 50/50 with
+     * Henyey-Greenstein), trained on the GPU from the light subpaths'
+     * medium vertices after the light passes of iterations 0..n-1 and used
+     * from iteration 1 on; its pdf enters every camera-direction pdf of the
+     * MIS recursion.  0 (the default): the plain method. */
+    int guide_train_iterations;
 } upbp_config;
 
 /* ------------------------------------------------------ scene records */
@@ -322,6 +331,23 @@ int upbp_debug_query_static(upbp_ctx* ctx, int kind, const float* queries, uint3
  * keeps up to 2^20 contributions per iteration (environment variable
  * UPBP_MIS_EVENTS, read by upbp_create, sets another limit). */
 int upbp_debug_mis_records(upbp_ctx* ctx, int which, float* out, uint64_t capacity, uint64_t* count);
+
+/* The learned proposal (upbp_config.guide_train_iterations; not in the
+ * reference).  upbp_guide_info writes up to n floats: training iterations,
+ * Adam steps taken, mean weighted loss of the last batch, training records
+ * collected, proposal-table rows, cells per axis, direction bins per axis,
+ * media slots, table in use (-1: none yet).
+ * upbp_guide_gradients runs the network's FP16 tensor-core forward and
+ * backward kernels once on the current device for given FP32 parameters
+ * (the layout of gpuupbp_b200/csrc/upbp_guide.cuh: four row-major [in][out]
+ * weight matrices 96x64, 64x64, 64x64, 64x48, then their biases), `rows`
+ * inputs of 96 floats and targets of 4 floats (unit direction, weight); it
+ * writes the gradient sums of the weighted negative log-likelihood (weights
+ * normalised to a batch mean of 1) with respect to every parameter, the
+ * rows x 48 outputs when `outputs` is not NULL, and the summed loss. */
+int upbp_guide_info(upbp_ctx* ctx, float* out, uint32_t n);
+int upbp_guide_gradients(const float* params, const float* x, const float* t, uint32_t rows, float* grads,
+                         float* outputs, float* loss);
 
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */
