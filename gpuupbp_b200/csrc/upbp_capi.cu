@@ -1661,11 +1661,16 @@ extern "C" int upbp_guide_info(upbp_ctx* c, float* out, uint32_t n)
 
 // One forward and backward pass of the proposal's network on given inputs,
 // for checking the tensor-core training kernels against a float64 restatement.
-extern "C" int upbp_guide_gradients(const float* params, const float* x, const float* t, uint32_t rows, float* grads,
-                                    float* outputs, float* loss)
+extern "C" int upbp_guide_gradients(const float* params, uint32_t n_params, const float* x, const float* t,
+                                    uint32_t rows, float* grads, float* outputs, float* loss)
 {
     return upbp_host::abi_guard([&]() -> int {
         if (!params || !x || !t || !grads || rows == 0) return UPBP_ERR_ARGS;
+        if (n_params != (uint32_t)kGuideParams) {
+            upbp_host::set_error("upbp_guide_gradients: the network has " + std::to_string(kGuideParams) +
+                                 " parameters");
+            return UPBP_ERR_ARGS;
+        }
         cudaStream_t st = nullptr;
         UPBP_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         GuideNet net;

@@ -47,13 +47,15 @@ constexpr int kGuideLayerOut[kGuideLayers] = {kGuideHidden, kGuideHidden, kGuide
 constexpr int kGuideWOff[kGuideLayers + 1] = {0, kGuideInPad * kGuideHidden,
                                               kGuideInPad * kGuideHidden + kGuideHidden * kGuideHidden,
                                               kGuideInPad * kGuideHidden + 2 * kGuideHidden * kGuideHidden,
-                                              kGuideInPad * kGuideHidden + 3 * kGuideHidden * kGuideHidden +
+                                              kGuideInPad * kGuideHidden + 2 * kGuideHidden * kGuideHidden +
                                                   kGuideHidden * kGuideOutPad};
 constexpr int kGuideWeights = kGuideWOff[kGuideLayers];
 constexpr int kGuideBOff[kGuideLayers + 1] = {0, kGuideHidden, 2 * kGuideHidden, 3 * kGuideHidden,
                                               3 * kGuideHidden + kGuideOutPad};
 constexpr int kGuideBiases = kGuideBOff[kGuideLayers];
 constexpr int kGuideParams = kGuideWeights + kGuideBiases;
+static_assert(kGuideWeights == 96 * 64 + 2 * 64 * 64 + 64 * 48 && kGuideParams == kGuideWeights + 240,
+              "parameter layout (the float64 restatement and the C ABI share it)");
 constexpr float kGuideKappaMin = 1e-2f, kGuideKappaMax = 2e3f;
 
 // Table entry: per lobe (mean xyz, kappa), the lobe's weight times its
@@ -344,7 +346,7 @@ __global__ void k_guide_batch(const GuideRecord* recs, const unsigned* rec_count
     const float z = 1.f - 2.f * u0, s = sqrtf(fmaxf(0.f, 1.f - z * z)), phi = 6.28318530717959f * u1;
     const float3 wi = make_float3(s * cosf(phi), s * sinf(phi), z);
     const float3 target = make_float3(-r.b.x, -r.b.y, -r.b.z);  // toward where the light came from
-    const float g = med_g[med];
+    const float g = slot >= 0 ? med_g[med] : 0.f;
     const float ct = dot(wi, target);
     const float g2 = g * g, d = 1.f + g2 - 2.f * g * ct;
     const float phase = fabsf(g) < 1e-3f ? 0.0795774715f : 0.0795774715f * (1.f - g2) / (d * sqrtf(d));

@@ -148,7 +148,7 @@ def load_library(path: str = LIB_PATH):
     L.upbp_get_stream.restype = VP
     L.upbp_get_device.argtypes = [VP]
     L.upbp_guide_info.argtypes = [VP, VP, ctypes.c_uint32]
-    L.upbp_guide_gradients.argtypes = [VP, VP, VP, ctypes.c_uint32, VP, VP, VP]
+    L.upbp_guide_gradients.argtypes = [VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32, VP, VP, VP]
     L.upbp_debug_mis_records.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint64, P(ctypes.c_uint64)]
     L.upbp_last_error.restype = ctypes.c_char_p
     L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]

@@ -340,14 +340,15 @@ int upbp_debug_mis_records(upbp_ctx* ctx, int which, float* out, uint64_t capaci
  * upbp_guide_gradients runs the network's FP16 tensor-core forward and
  * backward kernels once on the current device for given FP32 parameters
  * (the layout of gpuupbp_b200/csrc/upbp_guide.cuh: four row-major [in][out]
- * weight matrices 96x64, 64x64, 64x64, 64x48, then their biases), `rows`
+ * weight matrices 96x64, 64x64, 64x64, 64x48, then their biases; n_params
+ * must be their count, 17648, or UPBP_ERR_ARGS is returned), `rows`
  * inputs of 96 floats and targets of 4 floats (unit direction, weight); it
  * writes the gradient sums of the weighted negative log-likelihood (weights
  * normalised to a batch mean of 1) with respect to every parameter, the
  * rows x 48 outputs when `outputs` is not NULL, and the summed loss. */
 int upbp_guide_info(upbp_ctx* ctx, float* out, uint32_t n);
-int upbp_guide_gradients(const float* params, const float* x, const float* t, uint32_t rows, float* grads,
-                         float* outputs, float* loss);
+int upbp_guide_gradients(const float* params, uint32_t n_params, const float* x, const float* t, uint32_t rows,
+                         float* grads, float* outputs, float* loss);
 
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */

@@ -52,8 +52,11 @@ def test_tensor_core_training_kernels_match_float64():
     grads = np.zeros(len(P), np.float32)
     out = np.zeros((rows, G.OUT), np.float32)
     loss = ctypes.c_float()
-    assert L.upbp_guide_gradients(P.ctypes.data, X.ctypes.data, T.ctypes.data, rows, grads.ctypes.data,
+    assert L.upbp_guide_gradients(P.ctypes.data, len(P), X.ctypes.data, T.ctypes.data, rows, grads.ctypes.data,
                                   out.ctypes.data, ctypes.byref(loss)) == 0
+    # a parameter vector of another size is refused, not read past
+    assert L.upbp_guide_gradients(P.ctypes.data, len(P) - 1, X.ctypes.data, T.ctypes.data, rows, grads.ctypes.data,
+                                  out.ctypes.data, ctypes.byref(loss)) == -1
     O, loss64, g64 = G.forward_backward(P, X, T, fp16_like_gpu=True)
     # outputs: FP32 accumulation of FP16 products, same roundings of the
     # hidden activations
