@@ -772,10 +772,10 @@ UPBP_D void search_test_pairs(SearchWarpOf<kMode>& w, unsigned& head, unsigned c
 }
 
 template <int kMode>
-__global__ void __launch_bounds__(128) range_search_kernel()
+__global__ void __launch_bounds__(128) range_search_kernel(int slot)
 {
     using M = RangeMode<kMode>;
-    begin_kernel(M::kern);
+    begin_kernel(M::kern, slot);
     const DeviceParams& p = c_params;
     __shared__ SearchWarpOf<kMode> s_warp[kSearchWarps];
     SearchWarpOf<kMode>& w = s_warp[threadIdx.x >> 5];
@@ -949,9 +949,10 @@ UPBP_D void gather_records(const float4* rec, float4 (&out)[8], float4 (*s)[9], 
 // One warp per 32 consecutive hits; lanes past the end read the warp's
 // first hit's records and evaluate nothing.
 template <int kMode>
-__global__ void __launch_bounds__(128, 7) range_eval_kernel()
+__global__ void __launch_bounds__(128, 7) range_eval_kernel(int slot)
 {
     using M = RangeMode<kMode>;
+    begin_kernel(M::kern, slot);
     const DeviceParams& p = c_params;
     __shared__ float4 s_rec[kEvalWarps][32][9];
     float4(*s)[9] = s_rec[threadIdx.x >> 5];
@@ -981,9 +982,9 @@ __global__ void __launch_bounds__(128, 7) range_eval_kernel()
 // their walks are short and their hits few, so the search / evaluation split
 // (kept for PB2D, BB1D and BP2D) costs more than it saves here.
 template <bool medium>
-__global__ void __launch_bounds__(128) point_merge_kernel()
+__global__ void __launch_bounds__(128) point_merge_kernel(int slot)
 {
-    begin_kernel(medium ? kKernPp3d : kKernSurf);
+    begin_kernel(medium ? kKernPp3d : kKernSurf, slot);
     const DeviceParams& p = c_params;
     const PointMap& map = medium ? p.med_map : p.surf_map;
     const float r2 = medium ? p.radius_pp3d_2 : p.radius_surf_2;
@@ -1258,9 +1259,9 @@ UPBP_D void camera_path_end(const CameraLane& c)
 // the next pixel from a global counter instead of idling until the longest
 // path of its warp is done.  Each pixel's random stream depends on the pixel
 // alone, so the assignment of pixels to lanes does not change any path.
-__global__ void __launch_bounds__(128, 8) camera_pass_kernel()
+__global__ void __launch_bounds__(128, 8) camera_pass_kernel(int slot)
 {
-    begin_kernel(kKernCameraExtend);
+    begin_kernel(kKernCameraExtend, slot);
     const DeviceParams& p = c_params;
     VolSeg segs[kMaxVolSegments];
     LiteSeg lsegs[kMaxVolSegments];
@@ -1296,9 +1297,9 @@ __global__ void __launch_bounds__(128, 8) camera_pass_kernel()
 // Deferred NEE: one light sample per thread -- occlusion ray through the
 // media, MIS weight, throughput.  The contribution is kept per sample until
 // k_resolve_camera knows whether an earlier step of the path failed.
-__global__ void __launch_bounds__(128, 8) nee_connect_kernel()
+__global__ void __launch_bounds__(128, 8) nee_connect_kernel(int slot)
 {
-    begin_kernel(kKernNee);
+    begin_kernel(kKernNee, slot);
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[4], p.nee_capacity);
     VolSeg segs[kMaxVolSegments];
@@ -1355,9 +1356,9 @@ __global__ void __launch_bounds__(128, 8) nee_connect_kernel()
 // Deferred BPT: one (camera vertex, light vertex) pair per thread -- the
 // path-length and media checks of the connection loop, then the connection
 // with its occlusion ray; the contribution is kept per pair like NEE's.
-__global__ void __launch_bounds__(128, 8) bpt_connect_kernel()
+__global__ void __launch_bounds__(128, 8) bpt_connect_kernel(int slot)
 {
-    begin_kernel(kKernBpt);
+    begin_kernel(kKernBpt, slot);
     const DeviceParams& p = c_params;
     const unsigned n = min(p.queue_count[5], p.bpt_capacity);
     VolSeg segs[kMaxVolSegments];
@@ -1405,8 +1406,9 @@ __global__ void __launch_bounds__(128, 8) bpt_connect_kernel()
 // Adds the deferred connections and the emitter-hit colours into the camera
 // image, each only if no earlier step of its camera path failed: NEE samples,
 // then BPT pairs, then one colour per camera path.
-__global__ void __launch_bounds__(256) k_resolve_camera()
+__global__ void __launch_bounds__(256) k_resolve_camera(int slot)
 {
+    begin_kernel(kKernCameraExtend, slot);
     const DeviceParams& p = c_params;
     const unsigned nn = min(p.queue_count[4], p.nee_capacity);
     const unsigned nb = min(p.queue_count[5], p.bpt_capacity);
@@ -1438,8 +1440,9 @@ __global__ void __launch_bounds__(256) k_resolve_camera()
 // the scene's bounding cube), so the query kernels walk spatially coherent
 // warps through the photon maps.
 template <bool kSeg>
-__global__ void k_query_keys(unsigned n, unsigned* keys, unsigned* vals)
+__global__ void k_query_keys(int slot, unsigned n, unsigned* keys, unsigned* vals)
 {
+    begin_kernel(kKernCameraExtend, slot);
     const DeviceParams& p = c_params;
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;

@@ -67,41 +67,34 @@ class DeviceGuard {
     cudaError_t err_ = cudaSuccess;
 };
 
-// The launch-parameter bank (c_params, c_work) exists once per device and
-// process.  Contexts on one device take turns on it: a call that uploads
-// parameters holds the device's bank lock on the host for its whole
-// duration, makes its stream wait for the last use of the bank by another
-// context (an event on that context's stream), and records the event after
-// its own launches.  So contexts may be driven from several host threads;
-// their GPU work on the bank is serialised, never interleaved.
+// Parameter slots (c_slots, one per context) of each device: a context
+// takes the lowest free slot at upbp_create and returns it at upbp_destroy.
 constexpr int kMaxDevices = 64;
-struct ParamBank {
+struct SlotTable {
     std::mutex mu;
-    cudaEvent_t last = nullptr;   // recorded after the latest use, on that user's stream
-    const void* owner = nullptr;  // context of the latest use
+    bool used[kParamSlots] = {};
 };
-ParamBank g_bank[kMaxDevices];
+SlotTable g_slots[kMaxDevices];
 
-class BankUse {
-  public:
-    BankUse(const void* ctx, int dev, cudaStream_t st) : b_(g_bank[dev]), lk_(b_.mu), ctx_(ctx), st_(st)
-    {
-        if (b_.owner && b_.owner != ctx && b_.last) err_ = cudaStreamWaitEvent(st, b_.last, 0);
-    }
-    ~BankUse()
-    {
-        if (b_.last) cudaEventRecord(b_.last, st_);
-        b_.owner = ctx_;
-    }
-    cudaError_t error() const { return err_; }
+int take_slot(int dev)
+{
+    SlotTable& t = g_slots[dev];
+    std::lock_guard<std::mutex> lk(t.mu);
+    for (int i = 0; i < kParamSlots; i++)
+        if (!t.used[i]) {
+            t.used[i] = true;
+            return i;
+        }
+    return -1;
+}
 
-  private:
-    ParamBank& b_;
-    std::lock_guard<std::mutex> lk_;
-    const void* ctx_;
-    cudaStream_t st_;
-    cudaError_t err_ = cudaSuccess;
-};
+void give_slot(int dev, int slot)
+{
+    if (slot < 0) return;
+    SlotTable& t = g_slots[dev];
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.used[slot] = false;
+}
 
 template <class T>
 cudaError_t dalloc(T** p, size_t n)
@@ -132,9 +125,10 @@ cudaError_t dupload(T** p, const T* h, size_t n, cudaStream_t st)
 
 // Neighbour sets of n queries through the estimators' range-query walkers.
 // Query record: x y z dx dy dz tmin tmax (points use x y z only).
-__global__ void k_debug_query(int kind, const float* q, unsigned n, unsigned* counts, unsigned* ids, unsigned cap)
+__global__ void k_debug_query(int slot, int kind, const float* q, unsigned n, unsigned* counts, unsigned* ids,
+                              unsigned cap)
 {
-    begin_kernel(kKernDebug);
+    begin_kernel(kKernDebug, slot);
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const DeviceParams& p = c_params;
@@ -190,6 +184,7 @@ struct upbp_ctx {
     upbp_config cfg{};
     DeviceParams P{};
     int dev = 0;                              // device the context was created on
+    int slot = -1;                            // the context's launch-parameter slot on it
     cudaStream_t st = nullptr;
     unsigned* h_status = nullptr;             // page-locked copy of the iteration's status word
     unsigned status_seen = 0;                 // OR of every iteration's status bits
@@ -267,6 +262,14 @@ struct upbp_ctx {
 };
 
 namespace {
+
+// Uploads the context's launch parameters into its slot (stream-ordered
+// before the launches that read them).
+cudaError_t upload_params(upbp_ctx* c)
+{
+    return cudaMemcpyToSymbolAsync(c_slots, &c->P, sizeof(DeviceParams), sizeof(DeviceParams) * (size_t)c->slot,
+                                   cudaMemcpyHostToDevice, c->st);
+}
 
 void init_medium(DMedium& m, const upbp_medium& in)
 {
@@ -537,9 +540,9 @@ int sort_queries(upbp_ctx* c, int q, unsigned n, const unsigned** order)
     if (ensure_sort(c, q, n) != UPBP_OK) return UPBP_ERR_CUDA;
     unsigned** b = c->d_sort[q];
     if (q == 0)
-        k_query_keys<true><<<(n + 255) / 256, 256, 0, c->st>>>(n, b[0], b[2]);
+        k_query_keys<true><<<(n + 255) / 256, 256, 0, c->st>>>(c->slot, n, b[0], b[2]);
     else
-        k_query_keys<false><<<(n + 255) / 256, 256, 0, c->st>>>(n, b[0], b[2]);
+        k_query_keys<false><<<(n + 255) / 256, 256, 0, c->st>>>(c->slot, n, b[0], b[2]);
     UPBP_CK(cudaGetLastError());
     cub::DoubleBuffer<unsigned> kb(b[0], b[1]), vb(b[2], b[3]);
     size_t tb = c->sort_temp_bytes;
@@ -649,14 +652,15 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
             upbp_host::set_error("device index beyond the library's limit of " + std::to_string(kMaxDevices));
             return UPBP_ERR_NO_DEVICE;
         }
-        {
-            ParamBank& b = g_bank[dev];
-            std::lock_guard<std::mutex> lk(b.mu);
-            if (!b.last) UPBP_CK(cudaEventCreateWithFlags(&b.last, cudaEventDisableTiming));
+        const int slot = take_slot(dev);
+        if (slot < 0) {
+            upbp_host::set_error("more than " + std::to_string(kParamSlots) + " contexts on one device");
+            return UPBP_ERR_HOST;
         }
         upbp_ctx* c = new upbp_ctx();
         c->cfg = *cfg;
         c->dev = dev;
+        c->slot = slot;
         DeviceParams& P = c->P;
         UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         UPBP_CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_status), sizeof(unsigned)));
@@ -979,8 +983,6 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         if (!c || iteration < 0) return UPBP_ERR_ARGS;
         DeviceGuard dg(c->dev);
         UPBP_CK(dg.error());
-        BankUse bank(c, c->dev, c->st);
-        UPBP_CK(bank.error());
         DeviceParams& P = c->P;
         const upbp_config& cfg = c->cfg;
         const unsigned L = P.light_subpath_count;
@@ -993,11 +995,6 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         unsigned launches = 0;
         size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
         P.work = c->d_work;
-        {
-            unsigned long long* w = c->d_work;
-            h2d += sizeof(w);
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
-        }
 #ifdef UPBP_MIS_DEBUG
         {
             const MisDebug& m = c->mis;
@@ -1066,9 +1063,9 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             // [0] vertices [1] surface [2] medium [3] beams [4] next light path to hand out
             UPBP_CK(cudaMemsetAsync(c->d_counters, 0, 5 * sizeof(unsigned), c->st));
             h2d += sizeof(P);
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+            UPBP_CK(upload_params(c));
             if (L > 0) {
-                light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>();
+                light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>(c->slot);
                 launches++;
             }
             UPBP_CK(cudaGetLastError());
@@ -1180,11 +1177,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 // [3] connection vertices [4] NEE samples [5] BPT pairs
                 UPBP_CK(cudaMemsetAsync(c->d_qcount, 0, 6 * sizeof(unsigned), c->st));
                 h2d += sizeof(P);
-                UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+                UPBP_CK(upload_params(c));
                     UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
                                         kCtrCount * sizeof(unsigned long long), c->st));
                 camera_pass_kernel<<<std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128), 128, 0,
-                                     c->st>>>();
+                                     c->st>>>(c->slot);
                 launches++;
                 UPBP_CK(cudaGetLastError());
                 d2h += 6 * sizeof(unsigned);
@@ -1231,17 +1228,17 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         if (P.trace_camera_paths)
             UPBP_CK(cudaMemsetAsync(c->d_path_err, 0xff, P.screen_pixel_count * sizeof(unsigned), c->st));
         if (nnee > 0) {
-            nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>();
+            nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[4], c->st));
         if (nbpt > 0) {
-            bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>();
+            bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         if (P.trace_camera_paths) {
             k_resolve_camera<<<std::max(1u, std::min((nnee + nbpt + P.screen_pixel_count + 255) / 256, 148u * 32u)), 256, 0,
-                               c->st>>>();
+                               c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaGetLastError());
@@ -1263,7 +1260,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             P.pt_order = po;
             launches += (so ? 1 : 0) + (po ? 1 : 0);
             h2d += sizeof(P);
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+            UPBP_CK(upload_params(c));
         }
         // The estimators: search (query, neighbour) pairs into the hit list, then
         // evaluate them, in rounds over the query order.  A round stops handing
@@ -1291,12 +1288,12 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 P.query_begin = begin;
                 P.query_end = end;
                 h2d += sizeof(P);
-                UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &P, sizeof(P), 0, cudaMemcpyHostToDevice, c->st));
+                UPBP_CK(upload_params(c));
                 const int g = c->search_grid[mode];
                 switch (mode) {
-                case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(); break;
-                case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(); break;
-                default: range_search_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(); break;
+                case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(c->slot); break;
+                case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(c->slot); break;
+                default: range_search_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(c->slot); break;
                 }
                 launches++;
                 UPBP_CK(cudaGetLastError());
@@ -1322,9 +1319,9 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 if (total > 0) {
                     const unsigned g2 = grid_for((unsigned)total);
                     switch (mode) {
-                    case kModePb2d: range_eval_kernel<kModePb2d><<<g2, 128, 0, c->st>>>(); break;
-                    case kModeBb1d: range_eval_kernel<kModeBb1d><<<g2, 128, 0, c->st>>>(); break;
-                    default: range_eval_kernel<kModeBp2d><<<g2, 128, 0, c->st>>>(); break;
+                    case kModePb2d: range_eval_kernel<kModePb2d><<<g2, 128, 0, c->st>>>(c->slot); break;
+                    case kModeBb1d: range_eval_kernel<kModeBb1d><<<g2, 128, 0, c->st>>>(c->slot); break;
+                    default: range_eval_kernel<kModeBp2d><<<g2, 128, 0, c->st>>>(c->slot); break;
                     }
                     launches++;
                     UPBP_CK(cudaGetLastError());
@@ -1341,12 +1338,12 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         };
         UPBP_CK(cudaEventRecord(ev[6], c->st));
         if (run_surf) {
-            point_merge_kernel<false><<<grid_for(npt), 128, 0, c->st>>>();
+            point_merge_kernel<false><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[7], c->st));
         if (run_pp3d) {
-            point_merge_kernel<true><<<grid_for(npt), 128, 0, c->st>>>();
+            point_merge_kernel<true><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[8], c->st));
@@ -1527,15 +1524,10 @@ extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uin
         UPBP_CK(dalloc(&dc, n));
         UPBP_CK(dalloc(&di, (size_t)n * std::max(1u, ids_per_query)));
         UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
-        {
-            BankUse bank(c, c->dev, c->st);
-            UPBP_CK(bank.error());
-            unsigned long long* w = c->d_work;  // the query counts into its own row (kKernDebug)
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
-            k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
-            UPBP_CK(cudaGetLastError());
-        }
+        c->P.work = c->d_work;  // the query counts into its own row (kKernDebug)
+        UPBP_CK(upload_params(c));
+        k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(c->slot, kind, dq, n, dc, di, ids_per_query);
+        UPBP_CK(cudaGetLastError());
         UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         if (ids && ids_per_query)
             UPBP_CK(cudaMemcpyAsync(ids, di, (size_t)n * ids_per_query * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
@@ -1570,15 +1562,10 @@ extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queri
         UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
         // the array keeps the previous call's ids; clear this call's id slots
         if (id_bytes) UPBP_CK(cudaMemsetAsync(di, 0, id_bytes, c->st));
-        {
-            BankUse bank(c, c->dev, c->st);
-            UPBP_CK(bank.error());
-            unsigned long long* w = c->d_work;  // the query counts into its own row (kKernDebug)
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_work, &w, sizeof(w), 0, cudaMemcpyHostToDevice, c->st));
-            UPBP_CK(cudaMemcpyToSymbolAsync(c_params, &c->P, sizeof(c->P), 0, cudaMemcpyHostToDevice, c->st));
-            k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(kind, dq, n, dc, di, ids_per_query);
-            UPBP_CK(cudaGetLastError());
-        }
+        c->P.work = c->d_work;  // the query counts into its own row (kKernDebug)
+        UPBP_CK(upload_params(c));
+        k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(c->slot, kind, dq, n, dc, di, ids_per_query);
+        UPBP_CK(cudaGetLastError());
         UPBP_CK(cudaMemcpyAsync(counts, dc, n * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
         if (ids && id_bytes) UPBP_CK(cudaMemcpyAsync(ids, di, id_bytes, cudaMemcpyDeviceToHost, c->st));
         UPBP_CK(cudaStreamSynchronize(c->st));
@@ -1717,12 +1704,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     if (!c) return;
     DeviceGuard dg(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
-    {
-        // the parameter bank no longer needs to wait for this context
-        ParamBank& b = g_bank[c->dev];
-        std::lock_guard<std::mutex> lk(b.mu);
-        if (b.owner == c) b.owner = nullptr;
-    }
+    give_slot(c->dev, c->slot);
     if (c->h_status) cudaFreeHost(c->h_status);
     void* bufs[] = {c->mis.light, c->mis.camera, c->mis.events, c->mis.event_count, c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,

@@ -434,25 +434,33 @@ struct DeviceParams {
 enum : unsigned { kEvSegment = 1u, kEvNee = 2u, kEvBpt = 3u, kEvPoint = 255u };
 UPBP_HD unsigned event_key(unsigned bounce, unsigned step) { return bounce * 256u + step; }
 
-// Launch parameters of the running pass, uploaded before each launch.  One
-// bank per device: the host orders the uploads of different contexts on it
-// (ParamBank in upbp_capi.cu).
-__constant__ DeviceParams c_params;
-// Work counters of every kernel kind (kKernRows sets of kCtrCount), set
-// before each pass.  Each counting kernel records its kind in shared
-// memory at entry, so kernels of different kinds may run concurrently.
-__constant__ unsigned long long* c_work;
+// Launch parameters: one slot per context (kParamSlots per device), each
+// uploaded by its context before its launches on its own stream.  Every
+// kernel that reads them takes its context's slot as an argument and records
+// it in shared memory at entry; device code names the running kernel's
+// parameters c_params.  Contexts therefore run concurrently, each on its own
+// slot and stream.
+constexpr int kParamSlots = 48;
+__constant__ DeviceParams c_slots[kParamSlots];
+__shared__ int s_slot;
 __shared__ int s_kernel_kind;
+#define c_params (c_slots[s_slot])
 
-// Records the running kernel's kind; every thread of the block calls it
-// first, before any early return.
-UPBP_D void begin_kernel(int kind)
+// Records the running kernel's parameter slot and kind (for its work
+// counters); every thread of the block calls it first, before any early
+// return.
+UPBP_D void begin_kernel(int kind, int slot)
 {
-    if (threadIdx.x == 0) s_kernel_kind = kind;
+    if (threadIdx.x == 0) {
+        s_kernel_kind = kind;
+        s_slot = slot;
+    }
     __syncthreads();
 }
 
-UPBP_D unsigned long long* c_work_ptr() { return c_work + (size_t)s_kernel_kind * kCtrCount; }
+// Work counters of every kernel kind (kKernRows sets of kCtrCount at
+// c_params.work): the running kernel's set.
+UPBP_D unsigned long long* c_work_ptr() { return c_params.work + (size_t)s_kernel_kind * kCtrCount; }
 
 // Kernel kinds of an iteration, for work counters and timing.  The
 // diagnostic neighbour queries count into a row of their own after the

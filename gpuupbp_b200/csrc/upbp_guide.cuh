@@ -229,13 +229,16 @@ __global__ void __launch_bounds__(128) k_guide_gemm(GemmArgs g)
             for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
     const __half zero = __float2half(0.f);
     for (int k0 = kb; k0 < ke; k0 += kGemmBK) {
+        // consecutive threads read consecutive addresses of whichever
+        // operand dimension is contiguous in memory
+        const bool a_k_inner = g.sak == 1, b_k_inner = g.sbk == 1;
         for (int i = threadIdx.x; i < kGemmBM * kGemmBK; i += blockDim.x) {
-            const int r = i / kGemmBK, c = i % kGemmBK;
+            const int r = a_k_inner ? i / kGemmBK : i % kGemmBM, c = a_k_inner ? i % kGemmBK : i / kGemmBM;
             const int m = m0 + r, k = k0 + c;
             As[r][c] = (m < g.M && k < ke) ? g.A[m * g.sam + k * g.sak] : zero;
         }
         for (int i = threadIdx.x; i < kGemmBN * kGemmBK; i += blockDim.x) {
-            const int r = i / kGemmBK, c = i % kGemmBK;
+            const int r = b_k_inner ? i / kGemmBK : i % kGemmBN, c = b_k_inner ? i % kGemmBK : i / kGemmBN;
             const int n = n0 + r, k = k0 + c;
             Bs[r][c] = (n < g.N && k < ke) ? g.B[k * g.sbk + n * g.sbn] : zero;
         }

@@ -34,7 +34,7 @@ struct GuideBatch {
 
 struct GuideState {
     int train_iterations = 0;   // iterations whose light records train the network
-    int steps_per_iteration = 16;
+    int steps_per_iteration = 8;
     GuideNet net;
     GuideBatch batch;
     GuideRecord* recs = nullptr;

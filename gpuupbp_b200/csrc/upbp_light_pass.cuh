@@ -316,9 +316,9 @@ UPBP_D void light_path_end(const LightLane& l)
 // path ended takes the next path index from a global counter (counters[4]),
 // as the camera pass does with pixels.  Each path's random stream and
 // vertex slots depend on its index alone.
-__global__ void __launch_bounds__(128, 8) light_pass_kernel()
+__global__ void __launch_bounds__(128, 8) light_pass_kernel(int slot)
 {
-    begin_kernel(kKernLight);
+    begin_kernel(kKernLight, slot);
     const DeviceParams& p = c_params;
     VolSeg segs[kMaxVolSegments];
     LiteSeg lsegs[kMaxVolSegments];

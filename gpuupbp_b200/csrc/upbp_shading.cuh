@@ -210,18 +210,46 @@ struct Bsdf {
 // Pdf of a camera subpath scattering at a medium vertex from direction of
 // travel `travel` into `out`: the blend of the phase function (value hg) and
 // the learned mixture, or hg where the vertex is not guided.
+// Kept out of line: the unguided callers, the common case, pay only the
+// test of the cell.
+__device__ __noinline__ float guide_mix(int cell, float3 travel, float3 out, float hg)
+{
+    const float4* e = guide_entry(c_params.guide, cell, travel);
+    return e ? .5f * hg + .5f * vmf_mix_pdf(e, out) : hg;
+}
+
 UPBP_D float guide_pdf(const Bsdf& b, float3 travel, float3 out, float hg)
 {
-    const float4* e = guide_entry(c_params.guide, b.gcell, travel);
-    return e ? .5f * hg + .5f * vmf_mix_pdf(e, out) : hg;
+    return b.gcell < 0 ? hg : guide_mix(b.gcell, travel, out, hg);
 }
 
 // The same at a point of medium `med` that is not a vertex (a query beam's
 // merge point).
+__device__ __noinline__ float guide_mix_at(float3 x, int med, float3 travel, float3 out, float hg)
+{
+    return guide_mix(guide_cell(c_params.guide, x, med), travel, out, hg);
+}
+
 UPBP_D float guide_pdf_at(float3 x, int med, float3 travel, float3 out, float hg)
 {
-    const float4* e = guide_entry(c_params.guide, guide_cell(c_params.guide, x, med), travel);
-    return e ? .5f * hg + .5f * vmf_mix_pdf(e, out) : hg;
+    return c_params.guide.entries ? guide_mix_at(x, med, travel, out, hg) : hg;
+}
+
+// Samples the blend of the phase function and the learned mixture, one half
+// each: r2 picks the component (and, rescaled, the mixture's lobe).
+__device__ __noinline__ float3 guide_sample(const Bsdf& b, float r0, float r1, float r2, float3& dir_gen, float& pdf,
+                                            float& sin_theta)
+{
+    const float4* e = guide_entry(c_params.guide, b.gcell, -b.world_dir_fix);
+    if (!e || r2 < .5f) {
+        hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
+        if (!e) return b.scatter_coef * pdf;
+    } else {
+        dir_gen = vmf_mix_sample(e, 2.f * r2 - 1.f, r0, r1);
+    }
+    const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, &sin_theta);
+    pdf = .5f * p + .5f * vmf_mix_pdf(e, dir_gen);
+    return b.scatter_coef * p;
 }
 
 UPBP_D void bsdf_component_probs(Bsdf& b, const DMaterial& m)
@@ -466,21 +494,9 @@ UPBP_D float3 bsdf_sample(const Bsdf& b, float r0, float r1, float r2, float3& d
         sin_theta = 0.f;
         return v3(0.f);
     }
-    const float4* e = b.from_light() ? nullptr : guide_entry(c_params.guide, b.gcell, -b.world_dir_fix);
-    if (!e) {
-        hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
-        return b.scatter_coef * pdf;
-    }
-    // blend of the phase function and the learned mixture, one half each:
-    // r2 picks the component (and, rescaled, the mixture's lobe)
-    if (r2 < .5f) {
-        hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
-    } else {
-        dir_gen = vmf_mix_sample(e, 2.f * r2 - 1.f, r0, r1);
-    }
-    const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, &sin_theta);
-    pdf = .5f * p + .5f * vmf_mix_pdf(e, dir_gen);
-    return b.scatter_coef * p;
+    if (!b.from_light() && b.gcell >= 0) return guide_sample(b, r0, r1, r2, dir_gen, pdf, sin_theta);
+    hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
+    return b.scatter_coef * pdf;
 }
 
 // ---------------------------------------------------------------- lights

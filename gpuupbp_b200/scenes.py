@@ -418,6 +418,44 @@ def media_field_env(seed: int = 2, tiny: bool = False) -> SceneBuilder:
     return sb
 
 
+def batch_job(seed: int, tiny: bool = False) -> SceneBuilder:
+    """One job of the batched workload, drawn from its seed: a closed box with
+    a quad light and 1-3 randomly displaced icospheres bounding homogeneous
+    media (sigma_s in [0.1, 2], sigma_a in [0.01, 0.3], g in [-0.5, 0.8],
+    nested by priority), about log-uniform in [1k, 200k] triangles (each
+    sphere's subdivision the one nearest its share of the draw)."""
+    rng = np.random.default_rng(10_000 + seed)
+    sb = SceneBuilder()
+    _box_walls(sb, rng)
+    _quad_light(sb, "light", (0.0, 0.499, 0.0), 0.3)
+    media = int(rng.integers(1, 4))
+    target = math.exp(rng.uniform(math.log(1000.0), math.log(200000.0)))
+    for i in range(media):
+        share = max(target / media, 80.0)
+        sub = int(min(7, max(1, round(math.log(share / 20.0, 4)))))
+        if tiny:
+            sub = min(sub, 2)
+        v, f = icosphere(sub)
+        radius = rng.uniform(0.12, 0.28)
+        centre = rng.uniform(-0.45 + radius, 0.45 - radius, size=3)
+        v = displace(v, rng, amplitude=0.12) * radius + centre
+        name = f"m{i}"
+        ss, sa = float(rng.uniform(0.1, 2.0)), float(rng.uniform(0.01, 0.3))
+        sb.media.append(Medium(name, absorption=(sa, sa, sa), scattering=(ss, ss, ss), g=float(rng.uniform(-0.5, 0.8))))
+        sb.materials.append(Material(f"b{i}", real=False, priority=i + 1, medium=name))
+        sb.add(f"b{i}", v, f)
+    sb.camera = Camera(position=(0.0, 0.0, 0.45), target=(0.0, 0.0, -0.5), up=(0.0, 1.0, 0.0), hfov_deg=80.0)
+    return sb
+
+
+def batch_job_config(seed: int) -> dict:
+    """The view and path settings of batched job `seed`: resolution
+    uniform in {64^2, 128^2, 256^2, 512^2}, path length uniform in [4, 16]."""
+    rng = np.random.default_rng(20_000 + seed)
+    side = int(rng.choice([64, 128, 256, 512]))
+    return {"res": (side, side), "length": int(rng.integers(4, 17))}
+
+
 WORKLOADS = {"media_field_env": media_field_env, "box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
              "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box}
 
