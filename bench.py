@@ -414,6 +414,57 @@ def run_reference_sample(seconds: float, threads: int, warmup: int = 1, max_iter
                       f"({t:.1f} s on {threads} host threads)"}
 
 
+def run_batch_workload(args) -> dict:
+    """Config 3: 64 seeded jobs (resolution 64^2..512^2, path length 4..16,
+    1k..200k triangles of displaced icospheres bounding 1-3 media in a box),
+    rendered a batch iteration at a time through upbp_run_batch after the
+    batch autotuner chose workers and the per-job launch cap.  A step is one
+    iteration of every job; value = all jobs' camera + light subpaths per
+    second; the same jobs run one after another (one worker, no cap) give the
+    sequential figure beside it."""
+    import torch
+
+    from gpuupbp_b200 import batch
+    jobs = [batch.job_args(j, SCENE_DIR) for j in range(64)]
+    b = batch.Batch(jobs)
+    paths = b.paths_per_iteration()
+    tune = batch.autotune(b, 0, workers=(8, 16, 32), limits=(0, 148 * 2))
+    it = tune["next_iteration"]
+    for _ in range(args.warmup):
+        b.run_iteration(it)
+        it += 1
+    windows = []
+    for _ in range(REPEATS):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            b.run_iteration(it)
+            it += 1
+        torch.cuda.synchronize()
+        windows.append(time.perf_counter() - t0)
+    t = statistics.median(windows)
+    b.set_grid_limit(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run_iteration(it, workers=1)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    res = sorted({a[a.index("-r") + 1] for a in jobs})
+    lengths = [int(a[a.index("-l") + 1]) for a in jobs]
+    b.close()
+    return {"metric": "paths/s of a batch of 64 independent scene/view jobs", "value": paths * args.steps / t,
+            "unit": "paths/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded procedural jobs)",
+            "config": {"workload": "batch: 64 jobs, resolutions " + ",".join(res) +
+                                   f", path lengths {min(lengths)}..{max(lengths)}, upbp_all",
+                       "paths_per_step": paths, "timing": "wall clock around whole batch iterations, median of "
+                                                          f"{REPEATS} windows"},
+            "autotune": tune, "sequential": {"value": paths / t_seq, "unit": "paths/s",
+                                             "note": "the same jobs one after another, one worker, no launch cap"},
+            "repeats": {"s_per_window": windows}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -422,11 +473,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS) + ["batch"])
     ap.add_argument("--res", default=None,
                     help="image size WxH (default: the workload's); smaller sizes are for profiling captures, "
                          "not bench lines")
     args = ap.parse_args()
+    if args.workload == "batch":
+        print(json.dumps(run_batch_workload(args)))
+        return
     args.res = (tuple(int(v) for v in args.res.lower().split("x")) if args.res
                 else tuple(WORKLOADS[args.workload][0]))
     threads = os.cpu_count() or 1

@@ -242,7 +242,7 @@ struct QuerySeg {
 
 // PB2D: camera query beam x photon point (functs_pb2d.cuh:57-201).
 UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVertex& lv, float isect_dist, float rad2,
-                        float* w_out = nullptr)
+                        float* w_out = nullptr, bool guided = true)
 {
     const DeviceParams& p = c_params;
     const unsigned plen = lv.path_length + q.cam_path_length;
@@ -269,7 +269,7 @@ UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVe
     const float ph = hg_pdf(-q.d, pdir, m.mean_cosine, &sin_theta);
     const float3 f = v3(ph);
     if (is_black_or_negative(f)) return v3(0.f);
-    const float fpdf = guide_pdf_at(q.o + q.d * isect_dist, q.med, q.d, pdir, ph) * m.cont_prob;
+    const float fpdf = (guided ? guide_pdf_at(q.o + q.d * isect_dist, q.med, q.d, pdir, ph) : ph) * m.cont_prob;
     const float rpdf = ph * lv.bsdf.cont_prob;
     wc.d_shared *= isect_dist * isect_dist;
     wc.d_shared /= rs_for;
@@ -299,7 +299,7 @@ UPBP_D float3 eval_pb2d(const QuerySeg& q, const StateWeights& cw, const LightVe
 
 // BB1D: camera query beam x photon beam (functs_bb1d.cuh:57-248).
 UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& lb, float bb_dist, float sin_theta,
-                        float tc, float tp, float* w_out = nullptr)
+                        float tc, float tp, float* w_out = nullptr, bool guided = true)
 {
     const DeviceParams& p = c_params;
     const unsigned plen = lb.path_length + q.cam_path_length;
@@ -339,7 +339,7 @@ UPBP_D float3 eval_bb1d(const QuerySeg& q, const StateWeights& cw, const Beam& l
     const float ph = hg_pdf(-q.d, -lb.d, m.mean_cosine, nullptr);
     const float3 f = v3(ph);
     if (is_black_or_negative(f)) return v3(0.f);
-    const float fpdf = guide_pdf_at(q.o + q.d * tc, q.med, q.d, -lb.d, ph) * m.cont_prob;
+    const float fpdf = (guided ? guide_pdf_at(q.o + q.d * tc, q.med, q.d, -lb.d, ph) : ph) * m.cont_prob;
     const float rpdf = ph * m.cont_prob;
     wc.d_shared *= tc * tc;
     wc.d_shared /= rsf_c;
@@ -637,7 +637,7 @@ static_assert(kLeafShift + 5 <= 32, "owner lane bits");
 // camera image.  fq(i) and fn(i) return float4 i of the query's record
 // (segment query, or a point query's camera vertex) and of the neighbour's
 // (beam or light vertex).
-template <int kMode, class FQ, class FN>
+template <int kMode, bool kGuided, class FQ, class FN>
 UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
 {
     using M = RangeMode<kMode>;
@@ -658,7 +658,7 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
                                 t1, t2))
                 return;
             float w = -1.f;
-            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2, &w);
+            est = p.bb1d_normalization * eval_bb1d(q, cw, lb, dist, sin_theta, t1, t2, &w, kGuided);
             UPBP_MISDBG(if (w >= 0.f) {
                 MisEvent e{kMisBb1d, path, q.cam_path_length, lb.path_idx, lb.path_length, 0u, w,
                            lb.o + lb.d * t2, q.o + q.d * t1, lb.origin_offset + t2, t1, lb.origin_offset};
@@ -670,7 +670,7 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
             float dist, rad2;
             if (!pred_ray_disc(q.o, q.d, q.dmin, q.dmax, lv.hit, p.radius_pb2d_2, dist, rad2)) return;
             float w = -1.f;
-            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2, &w);
+            est = p.pb2d_normalization * eval_pb2d(q, cw, lv, dist, rad2, &w, kGuided);
             UPBP_MISDBG(if (w >= 0.f) {
                 MisEvent e{kMisPb2d, path, q.cam_path_length, qb.y / p.slots_per_path, lv.path_length, 0u, w,
                            lv.hit, q.o + q.d * dist, 0.f, dist};
@@ -682,6 +682,7 @@ UPBP_D void eval_range_hit(uint2 qb, FQ&& fq, FN&& fn)
         const float4 q8 = __ldg(&p.pt_queue[qb.x].q8);
         LightVertex cv;
         read_vertex(fq, cv);
+        if (!kGuided) cv.bsdf.gcell = -1;  // the unguided instantiation has no proposal code
         Beam lb;
         read_beam(fn, lb);
         float dist, rad2;
@@ -948,7 +949,9 @@ UPBP_D void gather_records(const float4* rec, float4 (&out)[8], float4 (*s)[9], 
 
 // One warp per 32 consecutive hits; lanes past the end read the warp's
 // first hit's records and evaluate nothing.
-template <int kMode>
+// kGuided: a learned-proposal table is in use (the unguided instantiation,
+// the common case, contains none of the proposal's code).
+template <int kMode, bool kGuided>
 __global__ void __launch_bounds__(128, 7) range_eval_kernel(int slot)
 {
     using M = RangeMode<kMode>;
@@ -974,14 +977,14 @@ __global__ void __launch_bounds__(128, 7) range_eval_kernel(int slot)
         float4 qa[8], na[8];
         gather_records(qrec, qa, s, lane);
         gather_records(nrec, na, s, lane);
-        if (j < n) eval_range_hit<kMode>(qb, [&](int i) { return qa[i]; }, [&](int i) { return na[i]; });
+        if (j < n) eval_range_hit<kMode, kGuided>(qb, [&](int i) { return qa[i]; }, [&](int i) { return na[i]; });
     }
 }
 
 // SURF and PP3D for one point-query record per thread, evaluated inline:
 // their walks are short and their hits few, so the search / evaluation split
 // (kept for PB2D, BB1D and BP2D) costs more than it saves here.
-template <bool medium>
+template <bool medium, bool kGuided>
 __global__ void __launch_bounds__(128) point_merge_kernel(int slot)
 {
     begin_kernel(medium ? kKernPp3d : kKernSurf, slot);
@@ -995,6 +998,7 @@ __global__ void __launch_bounds__(128) point_merge_kernel(int slot)
         if (!(fbits(q8.y) & (medium ? kQueryPp3d : kQuerySurf)) || !event_kept(fbits(q8.z), fbits(q8.w))) continue;
         LightVertex cv;
         load_vertex(&p.pt_queue[k].v, cv);
+        if (!kGuided) cv.bsdf.gcell = -1;  // the unguided instantiation has no proposal code
         float3 acc = v3(0.f);
         points_in_radius(map, cv.hit, r2, [&](unsigned slot) {
             LightVertex lv;

@@ -4,6 +4,7 @@
 // Renderer::init (gpuupbp/renderer/renderer_init.cpp:675-929) and
 // Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -244,6 +245,7 @@ struct upbp_ctx {
     int search_grid[kRangeModes] = {};  // per range-query mode (kModePb2d ...)
     int camera_grid = 0;   // resident blocks of the persistent camera pass
     int light_grid = 0;    // resident blocks of the persistent light pass
+    unsigned grid_limit = 0;  // cap on any launch's blocks (0: none), so that concurrent contexts share the SMs
     // Morton sort of the query records: keys/values and their alternates per queue
     unsigned* d_sort[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
     unsigned sort_capacity[2] = {0, 0};
@@ -262,6 +264,12 @@ struct upbp_ctx {
 };
 
 namespace {
+
+// Blocks of a launch under the context's grid limit (at least one).
+unsigned cap_grid(const upbp_ctx* c, unsigned blocks)
+{
+    return c->grid_limit ? std::max(1u, std::min(blocks, c->grid_limit)) : blocks;
+}
 
 // Uploads the context's launch parameters into its slot (stream-ordered
 // before the launches that read them).
@@ -1065,7 +1073,8 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             h2d += sizeof(P);
             UPBP_CK(upload_params(c));
             if (L > 0) {
-                light_pass_kernel<<<std::min<unsigned>(c->light_grid, (L + 127) / 128), 128, 0, c->st>>>(c->slot);
+                light_pass_kernel<<<cap_grid(c, std::min<unsigned>(c->light_grid, (L + 127) / 128)), 128, 0, c->st>>>(
+                    c->slot);
                 launches++;
             }
             UPBP_CK(cudaGetLastError());
@@ -1180,8 +1189,8 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 UPBP_CK(upload_params(c));
                     UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
                                         kCtrCount * sizeof(unsigned long long), c->st));
-                camera_pass_kernel<<<std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128), 128, 0,
-                                     c->st>>>(c->slot);
+                camera_pass_kernel<<<cap_grid(c, std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128)),
+                                     128, 0, c->st>>>(c->slot);
                 launches++;
                 UPBP_CK(cudaGetLastError());
                 d2h += 6 * sizeof(unsigned);
@@ -1220,7 +1229,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             }
         }
         UPBP_CK(cudaEventRecord(ev[3], c->st));
-        auto grid_for = [](unsigned n) { return std::max(1u, std::min((n + 127) / 128, 148u * 64u)); };
+        auto grid_for = [c](unsigned n) { return cap_grid(c, std::max(1u, std::min((n + 127) / 128, 148u * 64u))); };
         // deferred NEE and BPT connections, then the colours of every camera path
         // whose steps all succeeded (the query kernels below check the same)
         const unsigned nnee = P.trace_camera_paths ? std::min(c->h_qcount[4], c->nee_capacity) : 0;
@@ -1289,7 +1298,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 P.query_end = end;
                 h2d += sizeof(P);
                 UPBP_CK(upload_params(c));
-                const int g = c->search_grid[mode];
+                const int g = (int)cap_grid(c, (unsigned)c->search_grid[mode]);
                 switch (mode) {
                 case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(c->slot); break;
                 case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(c->slot); break;
@@ -1318,10 +1327,20 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 }
                 if (total > 0) {
                     const unsigned g2 = grid_for((unsigned)total);
+                    const bool gd = P.guide.entries != nullptr;
                     switch (mode) {
-                    case kModePb2d: range_eval_kernel<kModePb2d><<<g2, 128, 0, c->st>>>(c->slot); break;
-                    case kModeBb1d: range_eval_kernel<kModeBb1d><<<g2, 128, 0, c->st>>>(c->slot); break;
-                    default: range_eval_kernel<kModeBp2d><<<g2, 128, 0, c->st>>>(c->slot); break;
+                    case kModePb2d:
+                        if (gd) range_eval_kernel<kModePb2d, true><<<g2, 128, 0, c->st>>>(c->slot);
+                        else range_eval_kernel<kModePb2d, false><<<g2, 128, 0, c->st>>>(c->slot);
+                        break;
+                    case kModeBb1d:
+                        if (gd) range_eval_kernel<kModeBb1d, true><<<g2, 128, 0, c->st>>>(c->slot);
+                        else range_eval_kernel<kModeBb1d, false><<<g2, 128, 0, c->st>>>(c->slot);
+                        break;
+                    default:
+                        if (gd) range_eval_kernel<kModeBp2d, true><<<g2, 128, 0, c->st>>>(c->slot);
+                        else range_eval_kernel<kModeBp2d, false><<<g2, 128, 0, c->st>>>(c->slot);
+                        break;
                     }
                     launches++;
                     UPBP_CK(cudaGetLastError());
@@ -1338,12 +1357,14 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         };
         UPBP_CK(cudaEventRecord(ev[6], c->st));
         if (run_surf) {
-            point_merge_kernel<false><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            if (P.guide.entries) point_merge_kernel<false, true><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            else point_merge_kernel<false, false><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[7], c->st));
         if (run_pp3d) {
-            point_merge_kernel<true><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            if (P.guide.entries) point_merge_kernel<true, true><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            else point_merge_kernel<true, false><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[8], c->st));
@@ -1692,6 +1713,56 @@ extern "C" int upbp_guide_gradients(const float* params, uint32_t n_params, cons
         guide_free_batch(b);
         cudaStreamDestroy(st);
         return rc;
+    });
+}
+
+extern "C" int upbp_set_grid_limit(upbp_ctx* c, uint32_t max_blocks)
+{
+    if (!c) return UPBP_ERR_ARGS;
+    c->grid_limit = max_blocks;
+    return UPBP_OK;
+}
+
+// Batched rendering: one iteration of many contexts (jobs), each driven on
+// its own stream and parameter slot by one of `workers` host threads, so the
+// jobs' kernels and host synchronisations overlap instead of queueing.
+extern "C" int upbp_run_batch(upbp_ctx* const* ctxs, uint32_t n, int iteration, int workers)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!ctxs || n == 0 || iteration < 0) return UPBP_ERR_ARGS;
+        for (uint32_t i = 0; i < n; i++)
+            if (!ctxs[i]) return UPBP_ERR_ARGS;
+        const unsigned w = (unsigned)std::max(1, std::min<int>(workers > 0 ? workers : 16, (int)n));
+        std::atomic<uint32_t> next{0};
+        std::atomic<unsigned> status{0};
+        std::mutex mu;
+        int err = UPBP_OK;
+        std::string msg;
+        auto work = [&]() {
+            for (;;) {
+                const uint32_t j = next.fetch_add(1);
+                if (j >= n) return;
+                const int rc = upbp_run_iteration(ctxs[j], iteration);
+                if (rc < 0) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    if (err == UPBP_OK) {
+                        err = rc;
+                        msg = std::string("job ") + std::to_string(j) + ": " + upbp_last_error();
+                    }
+                } else {
+                    status.fetch_or((unsigned)rc);
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (unsigned k = 1; k < w; k++) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        if (err != UPBP_OK) {
+            upbp_host::set_error(msg);
+            return err;
+        }
+        return (int)status.load();
     });
 }
 

@@ -333,12 +333,29 @@ UPBP_HD unsigned guide_hash(unsigned x)
 
 UPBP_HD float guide_u01(unsigned h) { return (float)(h >> 8) * (1.f / 16777216.f); }
 
-__global__ void k_guide_batch(const GuideRecord* recs, const unsigned* rec_count, unsigned rec_capacity,
-                              unsigned batch, unsigned seed, float3 lo, float3 inv_ext, const float* med_g,
-                              const int* medium_slot, __half* X, float4* T)
+// Copies a block's rows of FP16 inputs from shared memory to X with 16-byte
+// stores (rows are 96 halves = 12 such stores).
+UPBP_D void guide_store_rows(const __half (*rows)[kGuideInPad], unsigned first, unsigned count, __half* X)
 {
-    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= batch) return;
+    __syncthreads();
+    const uint4* src = reinterpret_cast<const uint4*>(rows);
+    uint4* dst = reinterpret_cast<uint4*>(X + (size_t)first * kGuideInPad);
+    const unsigned n = count * (kGuideInPad / 8);
+    for (unsigned k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+}
+
+constexpr int kGuideRowsPerBlock = 128;
+
+__global__ void __launch_bounds__(kGuideRowsPerBlock) k_guide_batch(const GuideRecord* recs, const unsigned* rec_count,
+                                                                    unsigned rec_capacity, unsigned batch, unsigned seed,
+                                                                    float3 lo, float3 inv_ext, const float* med_g,
+                                                                    const int* medium_slot, __half* X, float4* T)
+{
+    __shared__ __align__(16) __half rows[kGuideRowsPerBlock][kGuideInPad];
+    const unsigned first = blockIdx.x * kGuideRowsPerBlock;
+    const unsigned i = first + threadIdx.x;
+    const unsigned count = min((unsigned)kGuideRowsPerBlock, batch - min(batch, first));
+    if (i < batch) {
     const unsigned nrec = min(*rec_count, rec_capacity);
     const unsigned h0 = guide_hash(seed * 0x9e3779b9u + i);
     const GuideRecord r = recs[guide_hash(h0) % max(nrec, 1u)];
@@ -355,8 +372,10 @@ __global__ void k_guide_batch(const GuideRecord* recs, const unsigned* rec_count
     const float phase = fabsf(g) < 1e-3f ? 0.0795774715f : 0.0795774715f * (1.f - g2) / (d * sqrtf(d));
     float in[kGuideInPad];
     guide_encode((xyz(r.a) - lo) * inv_ext, wi, slot, in);
-    for (int k = 0; k < kGuideInPad; k++) X[(size_t)i * kGuideInPad + k] = __float2half(in[k]);
+    for (int k = 0; k < kGuideInPad; k++) rows[threadIdx.x][k] = __float2half(in[k]);
     T[i] = make_float4(target.x, target.y, target.z, slot >= 0 ? r.b.w * phase : 0.f);
+    }
+    guide_store_rows(rows, first, count, X);
 }
 
 // Loss rows: -w log q(target) with q the vMF mixture of the row's output;
@@ -433,15 +452,20 @@ __global__ void k_guide_relu_mask(const __half* H, float* dH, __half* dH16, size
     }
 }
 
-// Bias gradient: column sums of dY [rows x cols].
-__global__ void k_guide_colsum(const __half* dY, unsigned rows, int cols, float* out)
+// Bias gradient: column sums of dY [rows x cols], cols <= 64: thread t of a
+// 256-thread block sums column t % 64 over every fourth row of the block's
+// rows (a warp reads 32 consecutive halves of one row), then the four
+// partial sums of a column meet in shared memory.
+__global__ void __launch_bounds__(256) k_guide_colsum(const __half* dY, unsigned rows, int cols, float* out)
 {
-    const int c = blockIdx.y;
+    __shared__ float part[4][64];
+    const int c = threadIdx.x & 63, q = threadIdx.x >> 6;
     float s = 0.f;
-    for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
-        s += __half2float(dY[(size_t)r * cols + c]);
-    for (int off = 16; off; off >>= 1) s += __shfl_down_sync(~0u, s, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&out[c], s);
+    if (c < cols)
+        for (unsigned r = blockIdx.x * 4 + q; r < rows; r += gridDim.x * 4) s += __half2float(dY[(size_t)r * cols + c]);
+    part[q][c] = s;
+    __syncthreads();
+    if (q == 0 && c < cols) atomicAdd(&out[c], part[0][c] + part[1][c] + part[2][c] + part[3][c]);
 }
 
 // Adam on the FP32 masters (gradients are batch sums: scaled by 1/batch),
@@ -468,8 +492,11 @@ __global__ void k_guide_table_inputs(int cells, int dir_res, int slots, float3 l
 {
     const unsigned per_slot = (unsigned)cells * cells * cells * dir_res * dir_res;
     const unsigned n = per_slot * slots;
-    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    __shared__ __align__(16) __half rows[kGuideRowsPerBlock][kGuideInPad];
+    const unsigned first = blockIdx.x * kGuideRowsPerBlock;
+    const unsigned i = first + threadIdx.x;
+    const unsigned count = min((unsigned)kGuideRowsPerBlock, n - min(n, first));
+    if (i < n) {
     const unsigned slot = i / per_slot, r = i % per_slot;
     const unsigned b = r % (dir_res * dir_res), c = r / (dir_res * dir_res);
     const unsigned ix = c % cells, iy = (c / cells) % cells, iz = c / (cells * cells);
@@ -477,7 +504,9 @@ __global__ void k_guide_table_inputs(int cells, int dir_res, int slots, float3 l
     const float3 d = oct_decode(make_float2(((b % dir_res) + .5f) / dir_res, ((b / dir_res) + .5f) / dir_res));
     float in[kGuideInPad];
     guide_encode((x - lo) * inv_ext, d, (int)slot, in);
-    for (int k = 0; k < kGuideInPad; k++) X[(size_t)i * kGuideInPad + k] = __float2half(in[k]);
+    for (int k = 0; k < kGuideInPad; k++) rows[threadIdx.x][k] = __float2half(in[k]);
+    }
+    guide_store_rows(rows, first, count, X);
 }
 
 // Network outputs -> table entries (lobe means and kappas, weights times

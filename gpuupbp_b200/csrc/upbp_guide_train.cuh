@@ -34,7 +34,7 @@ struct GuideBatch {
 
 struct GuideState {
     int train_iterations = 0;   // iterations whose light records train the network
-    int steps_per_iteration = 8;
+    int steps_per_iteration = 4;
     GuideNet net;
     GuideBatch batch;
     GuideRecord* recs = nullptr;
@@ -174,7 +174,7 @@ void guide_backward(cudaStream_t st, GuideNet& n, GuideBatch& b, unsigned rows)
         const __half* Hin = l == 0 ? b.X : b.H[l - 1];
         // dW_l = H_in^T dY, db_l = column sums of dY
         guide_gemm(st, Hin, 1, K, dY, ny, 1, gw + kGuideWOff[l], ny, K, ny, R, nullptr, 0, nullptr, true, split);
-        k_guide_colsum<<<dim3(64, ny), 256, 0, st>>>(dY, rows, ny, gb + kGuideBOff[l]);
+        k_guide_colsum<<<296, 256, 0, st>>>(dY, rows, ny, gb + kGuideBOff[l]);
         if (l == 0) break;
         // dH_in = (dY W_l^T) masked by the ReLU of H_in
         guide_gemm(st, dY, ny, 1, n.w16 + kGuideWOff[l], 1, ny, b.Hf, kGuideHidden, R, kGuideHidden, ny, nullptr, 0,
@@ -210,8 +210,8 @@ void guide_train_step(cudaStream_t st, GuideState& g, unsigned seed)
 {
     GuideBatch& b = g.batch;
     const float3 inv_ext = make_float3(1.f / g.ext.x, 1.f / g.ext.y, 1.f / g.ext.z);
-    k_guide_batch<<<(b.rows + 255) / 256, 256, 0, st>>>(g.recs, g.rec_count, g.rec_capacity, b.rows, seed, g.lo, inv_ext,
-                                                       g.med_g, g.medium_slot, b.X, b.T);
+    k_guide_batch<<<(b.rows + kGuideRowsPerBlock - 1) / kGuideRowsPerBlock, kGuideRowsPerBlock, 0, st>>>(
+        g.recs, g.rec_count, g.rec_capacity, b.rows, seed, g.lo, inv_ext, g.med_g, g.medium_slot, b.X, b.T);
     guide_forward(st, g.net, b, b.X, b.rows);
     guide_loss(st, b, b.rows);
     cudaMemsetAsync(g.net.grad, 0, kGuideParams * sizeof(float), st);
@@ -226,8 +226,8 @@ void guide_fill_table(cudaStream_t st, GuideState& g, float4* table)
     GuideBatch& b = g.batch;
     const float3 cell = make_float3(g.ext.x / g.cells, g.ext.y / g.cells, g.ext.z / g.cells);
     const float3 inv_ext = make_float3(1.f / g.ext.x, 1.f / g.ext.y, 1.f / g.ext.z);
-    k_guide_table_inputs<<<(g.table_rows + 255) / 256, 256, 0, st>>>(g.cells, g.dir_res, g.slots, g.lo, cell, inv_ext,
-                                                                    b.X);
+    k_guide_table_inputs<<<(g.table_rows + kGuideRowsPerBlock - 1) / kGuideRowsPerBlock, kGuideRowsPerBlock, 0, st>>>(
+        g.cells, g.dir_res, g.slots, g.lo, cell, inv_ext, b.X);
     guide_forward(st, g.net, b, b.X, g.table_rows);
     k_guide_table_entries<<<(g.table_rows + 255) / 256, 256, 0, st>>>(b.O, g.table_rows, table);
 }

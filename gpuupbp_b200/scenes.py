@@ -457,7 +457,8 @@ def batch_job_config(seed: int) -> dict:
 
 
 WORKLOADS = {"media_field_env": media_field_env, "box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
-             "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box}
+             "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box,
+             "batch_job": batch_job}
 
 
 # Version of the generators' output: a change to any generator that changes

@@ -117,7 +117,8 @@ EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_pr
            "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
            "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
            "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device",
-           "upbp_debug_mis_records", "upbp_guide_info", "upbp_guide_gradients"]
+           "upbp_debug_mis_records", "upbp_guide_info", "upbp_guide_gradients", "upbp_run_batch",
+           "upbp_set_grid_limit"]
 
 _libs = {}
 
@@ -147,6 +148,8 @@ def load_library(path: str = LIB_PATH):
     L.upbp_get_stream.argtypes = [VP]
     L.upbp_get_stream.restype = VP
     L.upbp_get_device.argtypes = [VP]
+    L.upbp_run_batch.argtypes = [VP, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
+    L.upbp_set_grid_limit.argtypes = [VP, ctypes.c_uint32]
     L.upbp_guide_info.argtypes = [VP, VP, ctypes.c_uint32]
     L.upbp_guide_gradients.argtypes = [VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32, VP, VP, VP]
     L.upbp_debug_mis_records.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint64, P(ctypes.c_uint64)]

@@ -350,6 +350,21 @@ int upbp_guide_info(upbp_ctx* ctx, float* out, uint32_t n);
 int upbp_guide_gradients(const float* params, uint32_t n_params, const float* x, const float* t, uint32_t rows,
                          float* grads, float* outputs, float* loss);
 
+/* Batched rendering of many independent jobs (config 3 of the benchmark
+ * spec; no counterpart in the reference, which renders one scene): each job
+ * is a context of its own (scene, view, configuration), and
+ * upbp_run_batch renders iteration `iteration` of all n of them
+ * concurrently -- `workers` host threads (0: 16) take jobs from a shared
+ * counter and drive each on the job's own stream and launch-parameter slot,
+ * so one job's kernels and host synchronisations overlap the others' -- and
+ * returns once every job's iteration is done: the OR of their status bits,
+ * or the first job's error.  upbp_set_grid_limit caps the blocks of any of a
+ * context's launches (0: no cap; the persistent kernels otherwise fill the
+ * GPU), so that kernels of concurrent jobs share the SMs; the batch
+ * autotuner in gpuupbp_b200/batch.py picks workers and the cap by timing. */
+int upbp_run_batch(upbp_ctx* const* ctxs, uint32_t n, int iteration, int workers);
+int upbp_set_grid_limit(upbp_ctx* ctx, uint32_t max_blocks);
+
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */
 void* upbp_get_stream(upbp_ctx* ctx);

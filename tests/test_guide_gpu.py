@@ -104,7 +104,7 @@ def test_training_lowers_the_loss(scene_dir):
         info = np.zeros(9, np.float32)
         r._L.upbp_guide_info(r._ctx, info.ctypes.data, 9)
         losses.append(float(info[2]))
-    assert info[1] == 4 * 8 and info[3] > 1000 and info[8] >= 0
+    assert info[1] == 4 * 4 and info[3] > 1000 and info[8] >= 0
     r.close()
     assert losses[-1] < losses[0] - 0.05, losses
 
