@@ -5,6 +5,7 @@
 // Renderer::run_iteration (gpuupbp/renderer/renderer.cpp:37-418).
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -68,34 +69,53 @@ class DeviceGuard {
     cudaError_t err_ = cudaSuccess;
 };
 
-// Parameter slots (c_slots, one per context) of each device: a context
-// takes the lowest free slot at upbp_create and returns it at upbp_destroy.
+// Parameter slots (c_slots) of each device.  A call that launches
+// parameter-reading kernels leases the lowest free slot for its duration
+// (every such call ends with a synchronisation of the context's stream, so
+// no kernel of it still reads the slot afterwards); any number of contexts
+// may exist, and up to kParamSlots of them run at once -- a further call
+// waits for a slot.
 constexpr int kMaxDevices = 64;
 struct SlotTable {
     std::mutex mu;
+    std::condition_variable freed;
     bool used[kParamSlots] = {};
 };
 SlotTable g_slots[kMaxDevices];
 
-int take_slot(int dev)
-{
-    SlotTable& t = g_slots[dev];
-    std::lock_guard<std::mutex> lk(t.mu);
-    for (int i = 0; i < kParamSlots; i++)
-        if (!t.used[i]) {
-            t.used[i] = true;
-            return i;
+class SlotLease {
+  public:
+    SlotLease(int dev, int& slot, cudaStream_t st) : t_(g_slots[dev]), slot_(slot), st_(st)
+    {
+        std::unique_lock<std::mutex> lk(t_.mu);
+        for (;;) {
+            for (int i = 0; i < kParamSlots; i++)
+                if (!t_.used[i]) {
+                    t_.used[i] = true;
+                    slot_ = i;
+                    return;
+                }
+            t_.freed.wait(lk);
         }
-    return -1;
-}
+    }
+    ~SlotLease()
+    {
+        // no kernel of the call may still read the slot (an error return
+        // skips the call's own final synchronisation)
+        cudaStreamSynchronize(st_);
+        {
+            std::lock_guard<std::mutex> lk(t_.mu);
+            t_.used[slot_] = false;
+            slot_ = -1;
+        }
+        t_.freed.notify_one();
+    }
 
-void give_slot(int dev, int slot)
-{
-    if (slot < 0) return;
-    SlotTable& t = g_slots[dev];
-    std::lock_guard<std::mutex> lk(t.mu);
-    t.used[slot] = false;
-}
+  private:
+    SlotTable& t_;
+    int& slot_;
+    cudaStream_t st_;
+};
 
 template <class T>
 cudaError_t dalloc(T** p, size_t n)
@@ -185,7 +205,7 @@ struct upbp_ctx {
     upbp_config cfg{};
     DeviceParams P{};
     int dev = 0;                              // device the context was created on
-    int slot = -1;                            // the context's launch-parameter slot on it
+    int slot = -1;                            // its launch-parameter slot during a call (SlotLease)
     cudaStream_t st = nullptr;
     unsigned* h_status = nullptr;             // page-locked copy of the iteration's status word
     unsigned status_seen = 0;                 // OR of every iteration's status bits
@@ -660,15 +680,9 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
             upbp_host::set_error("device index beyond the library's limit of " + std::to_string(kMaxDevices));
             return UPBP_ERR_NO_DEVICE;
         }
-        const int slot = take_slot(dev);
-        if (slot < 0) {
-            upbp_host::set_error("more than " + std::to_string(kParamSlots) + " contexts on one device");
-            return UPBP_ERR_HOST;
-        }
         upbp_ctx* c = new upbp_ctx();
         c->cfg = *cfg;
         c->dev = dev;
-        c->slot = slot;
         DeviceParams& P = c->P;
         UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         UPBP_CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_status), sizeof(unsigned)));
@@ -991,6 +1005,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         if (!c || iteration < 0) return UPBP_ERR_ARGS;
         DeviceGuard dg(c->dev);
         UPBP_CK(dg.error());
+        SlotLease lease(c->dev, c->slot, c->st);
         DeviceParams& P = c->P;
         const upbp_config& cfg = c->cfg;
         const unsigned L = P.light_subpath_count;
@@ -1546,6 +1561,7 @@ extern "C" int upbp_debug_query(upbp_ctx* c, int kind, const float* queries, uin
         UPBP_CK(dalloc(&di, (size_t)n * std::max(1u, ids_per_query)));
         UPBP_CK(cudaMemcpyAsync(dq, queries, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
         c->P.work = c->d_work;  // the query counts into its own row (kKernDebug)
+        SlotLease lease(c->dev, c->slot, c->st);
         UPBP_CK(upload_params(c));
         k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(c->slot, kind, dq, n, dc, di, ids_per_query);
         UPBP_CK(cudaGetLastError());
@@ -1584,6 +1600,7 @@ extern "C" int upbp_debug_query_static(upbp_ctx* c, int kind, const float* queri
         // the array keeps the previous call's ids; clear this call's id slots
         if (id_bytes) UPBP_CK(cudaMemsetAsync(di, 0, id_bytes, c->st));
         c->P.work = c->d_work;  // the query counts into its own row (kKernDebug)
+        SlotLease lease(c->dev, c->slot, c->st);
         UPBP_CK(upload_params(c));
         k_debug_query<<<(n + 127) / 128, 128, 0, c->st>>>(c->slot, kind, dq, n, dc, di, ids_per_query);
         UPBP_CK(cudaGetLastError());
@@ -1775,7 +1792,6 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     if (!c) return;
     DeviceGuard dg(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
-    give_slot(c->dev, c->slot);
     if (c->h_status) cudaFreeHost(c->h_status);
     void* bufs[] = {c->mis.light, c->mis.camera, c->mis.events, c->mis.event_count, c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,

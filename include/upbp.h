@@ -20,10 +20,11 @@
  * upbp_create; every entry point works on that device, whichever device the
  * calling thread has current (and leaves the caller's current device as it
  * was).  A context is driven by one host thread at a time; several contexts
- * may be driven from several threads.  Contexts on one device share one
- * launch-parameter bank, so the library runs their iterations one after the
- * other on the GPU (a call waits for another context's call in progress).
- * The caller owns host buffers, the library owns device memory.
+ * may be driven from several threads and then run concurrently on the GPU,
+ * each on its own stream: a call that launches kernels leases one of 48
+ * launch-parameter slots of the device for its duration (a 49th concurrent
+ * call waits for a slot).  The caller owns host buffers, the library owns
+ * device memory.
  */
 #ifndef UPBP_B200_H
 #define UPBP_B200_H
