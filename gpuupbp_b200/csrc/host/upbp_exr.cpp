@@ -4,6 +4,7 @@
 // layout specification: magic + version, attribute header, per-scanline
 // offset table, then one block per scanline (y, byte count, channel rows in
 // alphabetical channel order).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -136,4 +137,98 @@ extern "C" int upbp_write_exr(const char* path, const float* rgb, uint32_t w, ui
         std::fclose(f);
         return n == out.size() ? UPBP_OK : UPBP_ERR_IO;
     });
+}
+
+// ---- BMP and Radiance HDR (host/framebuffer.cpp:129-233 of the reference)
+
+// 24-bit BMP, rows bottom up, BGR bytes of pow(c, 1/gamma) * 255 clamped to
+// [0, 255] and truncated; no row padding, as the reference writes it (its
+// files are valid BMPs when the width is a multiple of 4).
+extern "C" int upbp_write_bmp(const char* path, const float* rgb, uint32_t w, uint32_t h, float gamma)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!path || !rgb || w == 0 || h == 0 || !(gamma > 0.f)) return UPBP_ERR_ARGS;
+        FILE* f = std::fopen(path, "wb");
+        if (!f) {
+            upbp_host::set_error(std::string("could not open ") + path);
+            return UPBP_ERR_IO;
+        }
+        auto u32 = [&](uint32_t v) { std::fwrite(&v, 4, 1, f); };
+        auto i32 = [&](int32_t v) { std::fwrite(&v, 4, 1, f); };
+        auto u16 = [&](uint16_t v) { std::fwrite(&v, 2, 1, f); };
+        const uint32_t header = 52;  // the reference's header struct (52 bytes) after "BM"
+        std::fwrite("BM", 1, 2, f);
+        u32(header + 2 + w * h * 3);
+        u32(0);
+        u32(header + 2);
+        u32(40);
+        i32((int32_t)w);
+        i32((int32_t)h);
+        u16(1);
+        u16(24);
+        u32(0);
+        u32(w * h * 3);
+        u32(2953);
+        u32(2953);
+        u32(0);
+        u32(0);
+        const float inv = 1.f / gamma;
+        std::vector<unsigned char> row((size_t)w * 3);
+        for (uint32_t y = 0; y < h; y++) {
+            const float* src = rgb + (size_t)(h - y - 1) * w * 3;
+            for (uint32_t x = 0; x < w; x++)
+                for (int c = 0; c < 3; c++) {
+                    const float v = std::pow(src[3 * x + 2 - c], inv) * 255.f;
+                    row[3 * x + c] = (unsigned char)std::min(255.f, std::max(0.f, v));
+                }
+            std::fwrite(row.data(), 1, row.size(), f);
+        }
+        const bool ok = std::fclose(f) == 0;
+        return ok ? UPBP_OK : UPBP_ERR_IO;
+    });
+}
+
+// Radiance RGBE: the "#?RADIANCE" header, -Y h +X w, then uncompressed
+// 4-byte pixels (mantissas scaled by frexp of the largest component).
+extern "C" int upbp_write_hdr(const char* path, const float* rgb, uint32_t w, uint32_t h)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!path || !rgb || w == 0 || h == 0) return UPBP_ERR_ARGS;
+        FILE* f = std::fopen(path, "wb");
+        if (!f) {
+            upbp_host::set_error(std::string("could not open ") + path);
+            return UPBP_ERR_IO;
+        }
+        std::fprintf(f, "#?RADIANCE\n# SmallUPBP\nFORMAT=32-bit_rle_rgbe\n\n-Y %u +X %u\n", h, w);
+        std::vector<unsigned char> px((size_t)w * h * 4, 0);
+        for (size_t i = 0; i < (size_t)w * h; i++) {
+            const float* c = rgb + 3 * i;
+            float v = std::max(c[0], std::max(c[1], c[2]));
+            if (v >= 1e-32f) {
+                int e;
+                v = float(std::frexp(v, &e) * 256.f / v);
+                px[4 * i + 0] = (unsigned char)(c[0] * v);
+                px[4 * i + 1] = (unsigned char)(c[1] * v);
+                px[4 * i + 2] = (unsigned char)(c[2] * v);
+                px[4 * i + 3] = (unsigned char)(e + 128);
+            }
+        }
+        std::fwrite(px.data(), 1, px.size(), f);
+        const bool ok = std::fclose(f) == 0;
+        return ok ? UPBP_OK : UPBP_ERR_IO;
+    });
+}
+
+// The reference's save(fb, name, gamma) (host/framebuffer.cpp:114-127): the
+// writer chosen by the name's last three characters.
+extern "C" int upbp_write_image(const char* path, const float* rgb, uint32_t w, uint32_t h, float gamma)
+{
+    if (!path) return UPBP_ERR_ARGS;
+    const std::string p = path;
+    const std::string ext = p.size() >= 3 ? p.substr(p.size() - 3) : "";
+    if (ext == "bmp") return upbp_write_bmp(path, rgb, w, h, gamma);
+    if (ext == "hdr") return upbp_write_hdr(path, rgb, w, h);
+    if (ext == "exr") return upbp_write_exr(path, rgb, w, h);
+    upbp_host::set_error("unknown image extension " + ext);
+    return UPBP_ERR_ARGS;
 }

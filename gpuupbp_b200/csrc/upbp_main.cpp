@@ -4,17 +4,63 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/upbp.h"
 
+// The reference saves with gamma 2.2 (framebuffer.hpp:66-70); the writer
+// follows the name's extension (exr, bmp or hdr).
 static int save_image(const std::string& name, const std::vector<float>& rgb, uint32_t w, uint32_t h)
 {
-    if (name.size() > 4 && name.substr(name.size() - 4) == ".exr") return upbp_write_exr(name.c_str(), rgb.data(), w, h);
-    std::fprintf(stderr, "only .exr output is written by this build (%s)\n", name.c_str());
-    return UPBP_ERR_ARGS;
+    const int rc = upbp_write_image(name.c_str(), rgb.data(), w, h, 2.2f);
+    if (rc != UPBP_OK) std::fprintf(stderr, "%s: %s\n", name.c_str(), upbp_last_error());
+    return rc;
 }
+
+// -log: one CSV row per iteration in <timestamp>_log.txt, the reference's
+// columns (misc/logger.cpp:32-86: scene, iter, light/build/camera time in
+// seconds, resolution, device memory used/free/total in MiB, core
+// utilisation -- 0, as the reference's without DBG_CORE_UTIL) and two more:
+// subpaths per second and range queries per second of the iteration.
+struct CsvLog {
+    FILE* f = nullptr;
+    explicit CsvLog(bool on)
+    {
+        if (!on) return;
+        char stamp[80];
+        const std::time_t t = std::time(nullptr);
+        std::strftime(stamp, sizeof(stamp), "%Y-%m-%d-%H-%M-%S", std::localtime(&t));
+        f = std::fopen((std::string(stamp) + "_log.txt").c_str(), "w");
+        if (f)
+            std::fprintf(f, "%40s,%6s,%12s,%12s,%12s,%12s,%12s,%12s,%12s,%12s,%12s,%12s,%12s,%12s\n", "scene", "iter",
+                         "lighttime", "buildtime", "cameratime", "res_x", "res_y", "mem_used", "mem_free", "mem_total",
+                         "light_util", "camera_util", "paths_per_s", "queries_per_s");
+    }
+    void row(const char* scene, int iter, upbp_ctx* ctx, uint32_t w, uint32_t h)
+    {
+        if (!f) return;
+        upbp_stats st;
+        if (upbp_get_stats(ctx, &st) != UPBP_OK) return;
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        const double mfree = fr / 1048576.0, mtot = tot / 1048576.0;
+        const double s = (st.ms_light + st.ms_build + st.ms_camera) * 1e-3;
+        const double paths = (double)st.light_paths + st.camera_paths;
+        const double queries = (double)st.segment_queries + st.point_queries;
+        std::fprintf(f, "%40s,%6d,%12g,%12g,%12g,%12u,%12u,%12g,%12g,%12g,%12g,%12g,%12g,%12g\n", scene, iter,
+                     st.ms_light * 1e-3, st.ms_build * 1e-3, st.ms_camera * 1e-3, w, h, mtot - mfree, mfree, mtot,
+                     0.0, 0.0, s > 0 ? paths / s : 0.0, s > 0 ? queries / s : 0.0);
+        std::fflush(f);
+    }
+    ~CsvLog()
+    {
+        if (f) std::fclose(f);
+    }
+};
 
 int main(int argc, const char** argv)
 {
@@ -42,6 +88,7 @@ int main(int argc, const char** argv)
     const uint32_t w = cfg.res_x, h = cfg.res_y;
     const std::string out = cfg.output_name;
     const std::string stem = out.substr(0, out.size() - 4), ext = out.substr(out.size() - 3);
+    CsvLog log(cfg.do_log != 0);
     auto t0 = std::chrono::steady_clock::now();
     int iter = 0;
     auto continuous = [&](int done) {
@@ -58,6 +105,7 @@ int main(int argc, const char** argv)
             const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             if (el >= cfg.max_time) break;
             if (upbp_run_iteration(ctx, iter) < 0) break;  // > 0: status bits, the image is complete
+            log.row(cfg.scene_path, iter, ctx, w, h);
             iter++;
             continuous(iter);
         }
@@ -68,6 +116,7 @@ int main(int argc, const char** argv)
                 std::fprintf(stderr, "iteration %d: %s\n", iter, upbp_last_error());
                 break;
             }
+            log.row(cfg.scene_path, iter, ctx, w, h);
             const int p = (int)((float)(iter + 1) / cfg.iteration_count * 100.f);
             if (p != percent) {
                 percent = p;

@@ -115,7 +115,8 @@ WORK_NAMES = ["nodes", "tris", "rays", "point_cand", "point_hit", "beam_cand", "
 # symbols declared in include/upbp.h
 EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_predefined", "upbp_scene_get_desc",
            "upbp_scene_free", "upbp_create", "upbp_run_iteration", "upbp_accumulate_to_host", "upbp_read_iteration",
-           "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_get_stream", "upbp_last_error",
+           "upbp_get_stats", "upbp_destroy", "upbp_write_exr", "upbp_write_bmp", "upbp_write_hdr",
+           "upbp_write_image", "upbp_get_stream", "upbp_last_error",
            "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device",
            "upbp_debug_mis_records", "upbp_guide_info", "upbp_guide_gradients", "upbp_run_batch",
            "upbp_set_grid_limit"]
@@ -145,6 +146,9 @@ def load_library(path: str = LIB_PATH):
     L.upbp_get_stats.argtypes = [VP, P(Stats)]
     L.upbp_destroy.argtypes = [VP]
     L.upbp_write_exr.argtypes = [ctypes.c_char_p, VP, ctypes.c_uint32, ctypes.c_uint32]
+    L.upbp_write_bmp.argtypes = [ctypes.c_char_p, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float]
+    L.upbp_write_hdr.argtypes = [ctypes.c_char_p, VP, ctypes.c_uint32, ctypes.c_uint32]
+    L.upbp_write_image.argtypes = [ctypes.c_char_p, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float]
     L.upbp_get_stream.argtypes = [VP]
     L.upbp_get_stream.restype = VP
     L.upbp_get_device.argtypes = [VP]
@@ -338,3 +342,9 @@ class Renderer:
 def write_exr(path: str, rgb: np.ndarray):
     a = np.ascontiguousarray(rgb, np.float32)
     _check(load_library().upbp_write_exr(path.encode(), a.ctypes.data, a.shape[1], a.shape[0]), "exr")
+
+
+def write_image(path: str, rgb: np.ndarray, gamma: float = 2.2):
+    """Writes an (H, W, 3) image as .exr, .bmp or .hdr by the name's extension."""
+    a = np.ascontiguousarray(rgb, np.float32)
+    _check(load_library().upbp_write_image(path.encode(), a.ctypes.data, a.shape[1], a.shape[0], gamma), "image")

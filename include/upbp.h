@@ -279,6 +279,17 @@ void upbp_destroy(upbp_ctx* ctx);
  * (gpuupbp/host/framebuffer.cpp:114-127, misc/tinyexr_wrapper.cpp:34-95):
  * half-float B,G,R channels, uncompressed scanlines. */
 int upbp_write_exr(const char* path, const float* rgb, uint32_t width, uint32_t height);
+/* Replaces: save_bmp (gpuupbp/host/framebuffer.cpp:129-202): 24-bit BGR,
+ * rows bottom up, bytes of min(255, max(0, pow(c, 1/gamma) * 255)) truncated,
+ * the reference's 52-byte header after "BM" and no row padding. */
+int upbp_write_bmp(const char* path, const float* rgb, uint32_t width, uint32_t height, float gamma);
+/* Replaces: save_hdr (gpuupbp/host/framebuffer.cpp:204-233): Radiance RGBE,
+ * uncompressed pixels after the "-Y h +X w" line. */
+int upbp_write_hdr(const char* path, const float* rgb, uint32_t width, uint32_t height);
+/* Replaces: save(fb, name, gamma) (gpuupbp/host/framebuffer.cpp:114-127):
+ * the writer chosen by the name's last three characters (bmp, hdr, exr);
+ * UPBP_ERR_ARGS for any other. */
+int upbp_write_image(const char* path, const float* rgb, uint32_t width, uint32_t height, float gamma);
 
 /* ---- diagnostics (no counterpart in the reference; used by the parity tests)
  * upbp_debug_photons: the last iteration's photon map contents.  kind 0/1:

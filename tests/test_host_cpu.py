@@ -165,3 +165,58 @@ def test_exr_writer_roundtrip(tmp_path):
     back = read_exr_half(str(p))
     expected = img.astype(np.float16)  # IEEE round to nearest even
     assert np.array_equal(back.view(np.uint16), expected.view(np.uint16))
+
+
+def test_bmp_writer_bytes(tmp_path):
+    """24-bit BMP as the reference's save_bmp writes it (framebuffer.cpp:129-202):
+    "BM", its 52-byte header, rows bottom up, BGR of pow(c, 1/gamma) * 255
+    clamped and truncated, no row padding."""
+    rng = np.random.default_rng(4)
+    h, w, gamma = 5, 6, 2.2
+    img = (rng.random((h, w, 3)) * 1.3 - 0.1).astype(np.float32)
+    p = tmp_path / "x.bmp"
+    upbp.write_image(str(p), img, gamma)
+    data = p.read_bytes()
+    assert data[:2] == b"BM" and len(data) == 54 + w * h * 3
+    fields = struct.unpack_from("<IIIIiihhIIIIII", data, 2)
+    assert fields == (54 + w * h * 3, 0, 54, 40, w, h, 1, 24, 0, w * h * 3, 2953, 2953, 0, 0)
+    with np.errstate(invalid="ignore"):
+        v = np.power(img.astype(np.float32), np.float32(1.0 / gamma)) * np.float32(255.0)
+    v = np.where(np.isnan(v), 0.0, np.clip(v, 0.0, 255.0)).astype(np.uint8)
+    expected = v[::-1, :, ::-1].tobytes()
+    got = np.frombuffer(data, np.uint8, offset=54)
+    # pow in float32 may differ from numpy's in the last ulp: at most one
+    # byte value apart, and almost always equal
+    diff = np.abs(got.astype(int) - np.frombuffer(expected, np.uint8).astype(int))
+    assert diff.max() <= 1 and (diff == 0).mean() > 0.95
+
+
+def test_hdr_writer_bytes(tmp_path):
+    """Radiance RGBE as the reference's save_hdr writes it (framebuffer.cpp:204-233)."""
+    rng = np.random.default_rng(5)
+    h, w = 4, 3
+    img = (rng.random((h, w, 3)) * 10.0).astype(np.float32)
+    img[0, 0] = 0.0
+    img[1, 1] = [1e-33, 0.0, 0.0]
+    p = tmp_path / "x.hdr"
+    upbp.write_image(str(p), img)
+    data = p.read_bytes()
+    head = b"#?RADIANCE\n# SmallUPBP\nFORMAT=32-bit_rle_rgbe\n\n-Y %d +X %d\n" % (h, w)
+    assert data.startswith(head) and len(data) == len(head) + 4 * w * h
+    px = np.frombuffer(data, np.uint8, offset=len(head)).reshape(h, w, 4)
+    for y in range(h):
+        for x in range(w):
+            c = img[y, x]
+            v = float(max(c))
+            if v < 1e-32:
+                assert (px[y, x] == 0).all()
+                continue
+            m, e = np.frexp(np.float32(v))
+            s = np.float32(m * np.float32(256.0) / np.float32(v))
+            assert list(px[y, x, :3]) == [int(np.float32(ch) * s) for ch in c]
+            assert px[y, x, 3] == e + 128
+
+
+def test_image_writer_refuses_unknown_extension(tmp_path):
+    with pytest.raises(upbp.UpbpError):
+        upbp.write_image(str(tmp_path / "x.png"), np.zeros((2, 2, 3), np.float32))

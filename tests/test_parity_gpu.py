@@ -15,6 +15,7 @@ take another branch after a fused multiply-add rounds differently and the
 pixels they reach move by more than 1e-3."""
 import json
 import os
+import struct
 
 import numpy as np
 import pytest
@@ -172,3 +173,29 @@ def test_executable_renders_a_predefined_scene(tmp_path):
     rel = np.abs(img - ref) / (np.abs(ref) + 1e-3)
     assert float(np.mean(np.all(rel < 2e-3, axis=-1))) >= PIXEL_BAR
     assert abs(img.mean() - ref.mean()) / (abs(ref.mean()) + 1e-6) <= 1e-3  # half-float output
+
+
+def test_executable_writes_bmp_and_log(scene_dir, tmp_path):
+    """`-o x.bmp -log`: a BMP (the reference's writer, gamma 2.2) and
+    <timestamp>_log.txt with a header and one CSV row per iteration in the
+    reference logger's columns plus subpaths/s and queries/s."""
+    import glob
+    import subprocess
+
+    case = "box_tiny_all"
+    workload, tiny, _, _ = CASES[case]
+    path = scenes.write_workload(workload, scene_dir, tiny=tiny)
+    exe = os.path.join(ROOT, "gpuupbp_b200", "upbp")
+    r = subprocess.run([exe] + command_line(case, path) + ["-i", "3", "-o", "box.bmp", "-log"],
+                       capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    data = (tmp_path / "box.bmp").read_bytes()
+    w, h = struct.unpack_from("<ii", data, 18)
+    assert data[:2] == b"BM" and len(data) == 54 + 3 * w * h and max(data[54:]) > 0
+    logs = glob.glob(str(tmp_path / "*_log.txt"))
+    assert len(logs) == 1
+    rows = [[c.strip() for c in line.split(",")] for line in open(logs[0]).read().splitlines()]
+    assert rows[0][:3] == ["scene", "iter", "lighttime"] and len(rows) == 4
+    for it, row in enumerate(rows[1:]):
+        assert len(row) == len(rows[0]) == 14 and int(row[1]) == it
+        assert float(row[2]) > 0 and float(row[4]) > 0 and int(row[5]) == w and float(row[12]) > 0
