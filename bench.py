@@ -10,13 +10,15 @@ photon-map builds, camera pass).
 Metric: paths/s = (camera + light subpaths per iteration) x iterations / time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload media_field|dense_beams]
+                    [--workload media_field|dense_beams|batch|guided]
 
 `--workload dense_beams` times the dense-beam stress case instead (1920x1080,
 one thick medium in a 500k-triangle enclosure, path length 16, BB1D over the
 beams of the first 600 000 light paths, about 2M, BP2D over all, about 7M,
-and 4-5M photon points per iteration); the headline line is the default
-workload.
+and 4-5M photon points per iteration); `--workload batch` times 64 seeded
+scene/view jobs rendered together (run_batch_workload); `--workload guided`
+compares the learned proposal with plain UPBP at equal device time
+(run_guided_workload).  The headline line is the default workload.
 
 `value` is timed with CUDA events on the library's stream, inputs resident;
 `e2e` renders the same iterations through the C ABI and reads every
@@ -428,7 +430,9 @@ def run_batch_workload(args) -> dict:
     jobs = [batch.job_args(j, SCENE_DIR) for j in range(64)]
     b = batch.Batch(jobs)
     paths = b.paths_per_iteration()
+    free0, total = torch.cuda.mem_get_info()
     tune = batch.autotune(b, 0, workers=(8, 16, 32), limits=(0, 148 * 2))
+    free1, _ = torch.cuda.mem_get_info()
     it = tune["next_iteration"]
     for _ in range(args.warmup):
         b.run_iteration(it)
@@ -460,9 +464,94 @@ def run_batch_workload(args) -> dict:
                                    f", path lengths {min(lengths)}..{max(lengths)}, upbp_all",
                        "paths_per_step": paths, "timing": "wall clock around whole batch iterations, median of "
                                                           f"{REPEATS} windows"},
+            "device_memory_gb": {"total": total / 1e9, "used_after_create": (total - free0) / 1e9,
+                                 "used_after_autotune": (total - free1) / 1e9},
             "autotune": tune, "sequential": {"value": paths / t_seq, "unit": "paths/s",
                                              "note": "the same jobs one after another, one worker, no launch cap"},
             "repeats": {"s_per_window": windows}}
+
+
+# FLOPs of the proposal's network per row: forward 2 x (96x64 + 64x64 + 64x64
+# + 64x48) multiply-adds; a training row adds the weight gradients (as many)
+# and the hidden gradients 2 x (48x64 + 64x64 + 64x64)
+GUIDE_FWD_FLOP = 2 * (96 * 64 + 64 * 64 + 64 * 64 + 64 * 48)
+GUIDE_TRAIN_FLOP = 2 * GUIDE_FWD_FLOP + 2 * (48 * 64 + 64 * 64 + 64 * 64)
+GUIDE_BATCH, GUIDE_STEPS_PER_ITERATION = 1 << 18, 4
+CONFIG1_ARGS = ["-a", "upbp_all", "-l", "8", "-r", "256x256", "-r_initial", "-0.02", "-r_alpha", "0.75"]
+
+
+def run_guided_workload(args) -> dict:
+    """Config 4: the learned proposal (-guide 8: trained online on the light
+    subpaths' medium records during the first 8 of 60 iterations) on config
+    1's scene -- the 256x256 box with the icosphere medium, BPT + SURF + PP3D
+    + PB2D + BB1D, path length 8, radius 0.01 x scene diameter shrinking with
+    alpha 0.75 -- against plain UPBP at equal device time.  Both are compared
+    by relMSE with a converged plain render of --ref-iterations iterations on
+    independent random streams.  value = relMSE(plain) / relMSE(guided) at
+    equal time (above 1: the proposal pays).  The training phase (4 fused
+    tcgen05 training steps of 2^18 rows and the table bake per training
+    iteration) is reported against the tensor peak."""
+    import numpy as np
+    import torch
+
+    from gpuupbp_b200 import quality, scenes, upbp
+    path = scenes.write_workload("box_medium", SCENE_DIR)
+    plain = ["-s", "-1", path] + CONFIG1_ARGS
+    guided = plain + ["-guide", "8"]
+    res = quality.equal_time(plain, guided, args.ref_iterations, 60)
+    # the training phase alone, from the library's own events
+    r = upbp.Renderer(guided)
+    r.stats()
+    for it in range(8):
+        r.run_iteration(it)
+    st = r.stats()
+    info = np.zeros(9, np.float32)
+    r._L.upbp_guide_info(r._ctx, info.ctypes.data, 9)
+    r.close()
+    torch.cuda.synchronize()
+    table_rows = int(info[4])
+    flop = GUIDE_STEPS_PER_ITERATION * GUIDE_BATCH * GUIDE_TRAIN_FLOP + table_rows * GUIDE_FWD_FLOP
+    ms = st["ms_guide_sum"] / max(1, st["timed_iterations"])
+    peaks = measured_peaks()
+    peak = peaks.get("bf16_tflops") or 1590.0
+    achieved = flop / (ms * 1e-3) / 1e12
+    return {"metric": "equal-time relMSE ratio, plain / guided UPBP (config 4)",
+            "value": res["relmse_ratio_plain_over_other"], "unit": "x", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32 render, f16 network with f32 accumulation", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": "guided: box_medium 256x256, upbp_all, path length 8, -guide 8, 60 iterations; "
+                                   f"reference {args.ref_iterations} plain iterations"},
+            "equal_time": res,
+            "guided_ms_per_iteration": res["other_ms"] / res["other_iterations"],
+            "plain_ms_per_iteration": res["plain_ms"] / res["plain_iterations"],
+            "training": {"ms_per_training_iteration": ms, "steps_per_iteration": GUIDE_STEPS_PER_ITERATION,
+                         "batch_rows": GUIDE_BATCH, "table_rows": table_rows, "final_loss": float(info[2]),
+                         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                                      "frac": achieved / peak, "peak_source": "measured" if peaks else "fallback",
+                                      "flop_per_iteration": flop}}}
+
+
+def run_batch_quality_workload(args) -> dict:
+    """Config 3's quality target: the guided, batched renderer against the
+    plain single-scene renderer at equal wall time, by relMSE per job
+    against each job's converged plain render (quality.batch_equal_time).
+    Jobs 0..--jobs-1 of the seeded 64 (a bounded sample of config 3, so that
+    the converged references -- --ref-iterations iterations of every job --
+    stay within minutes); the guided jobs train their proposal during the
+    first 8 of --method-iterations iterations.  value = mean relMSE of the
+    plain renderer / mean relMSE of the guided batch (above 1: the batched,
+    guided form wins)."""
+    from gpuupbp_b200 import batch, quality
+    jobs = [batch.job_args(j, SCENE_DIR) for j in range(args.jobs)]
+    res = quality.batch_equal_time(jobs, ["-guide", "8"], args.ref_iterations, args.method_iterations)
+    return {"metric": "equal-time relMSE ratio, plain single-scene / guided batched UPBP (config 3 sample)",
+            "value": res["relmse_ratio_plain_over_method"], "unit": "x", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded procedural jobs)",
+            "config": {"workload": f"batch_quality: jobs 0..{args.jobs - 1} of the 64 seeded config-3 jobs, "
+                                   f"upbp_all, guided (-guide 8) and batched vs plain one job at a time, "
+                                   f"{args.method_iterations} guided iterations, reference "
+                                   f"{args.ref_iterations} plain iterations per job",
+                       "timing": "wall clock of whole batch iterations"},
+            "equal_time": res}
 
 
 def main():
@@ -473,13 +562,26 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS) + ["batch", "batch_quality", "guided"])
+    ap.add_argument("--ref-iterations", type=int, default=None,
+                    help="iterations of the converged plain render the guided (default 4096) and batch_quality "
+                         "(default 192) workloads compare with")
+    ap.add_argument("--jobs", type=int, default=16, help="batch_quality: jobs of the seeded 64")
+    ap.add_argument("--method-iterations", type=int, default=24, help="batch_quality: guided batch iterations")
     ap.add_argument("--res", default=None,
                     help="image size WxH (default: the workload's); smaller sizes are for profiling captures, "
                          "not bench lines")
     args = ap.parse_args()
     if args.workload == "batch":
         print(json.dumps(run_batch_workload(args)))
+        return
+    if args.workload == "guided":
+        args.ref_iterations = args.ref_iterations or 4096
+        print(json.dumps(run_guided_workload(args)))
+        return
+    if args.workload == "batch_quality":
+        args.ref_iterations = args.ref_iterations or 192
+        print(json.dumps(run_batch_quality_workload(args)))
         return
     args.res = (tuple(int(v) for v in args.res.lower().split("x")) if args.res
                 else tuple(WORKLOADS[args.workload][0]))

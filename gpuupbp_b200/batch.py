@@ -64,18 +64,20 @@ class Batch:
 
 def autotune(batch: Batch, first_iteration: int, workers=(4, 8, 16, 32), limits=(0, 148 * 2)) -> dict:
     """Times one batch iteration for every (workers, grid limit) pair and
-    keeps the fastest; the iterations rendered while tuning are real ones
-    (first_iteration onward), so the caller continues after them.  Returns
-    the choice, its timings and the next iteration index."""
+    keeps the fastest; the jobs one after another (one worker, no cap) is
+    always among the candidates, so the choice is never slower than that.
+    The iterations rendered while tuning are real ones (first_iteration
+    onward), so the caller continues after them.  Returns the choice, its
+    timings and the next iteration index."""
     it = first_iteration
     timings = {}
-    for lim in limits:
+    pairs = [(1, 0)] + [(w, lim) for lim in limits for w in workers if (w, lim) != (1, 0)]
+    for w, lim in pairs:
         batch.set_grid_limit(lim)
-        for w in workers:
-            t0 = time.perf_counter()
-            batch.run_iteration(it, w)
-            timings[(w, lim)] = time.perf_counter() - t0
-            it += 1
+        t0 = time.perf_counter()
+        batch.run_iteration(it, w)
+        timings[(w, lim)] = time.perf_counter() - t0
+        it += 1
     best = min(timings, key=timings.get)
     batch.workers, _ = best
     batch.set_grid_limit(best[1])

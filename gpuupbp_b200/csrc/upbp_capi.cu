@@ -28,7 +28,7 @@ constexpr int kEventRing = 64;
 // extend, 4 NEE, 5 BPT + resolve, 6 query sort, 7 SURF, 8 PP3D, 9 BP2D,
 // 10 PB2D, 11 BB1D, 12 iteration done.  Each kernel kind's time is one
 // interval.
-constexpr int kEvPerIter = 13;
+constexpr int kEvPerIter = 14;  // [13]: end of the light pass, start of the proposal's training
 struct EvInterval {
     int kind, from, to;
 };
@@ -116,6 +116,29 @@ class SlotLease {
     int& slot_;
     cudaStream_t st_;
 };
+
+// Range-query hit lists are needed only while an iteration's searches run.
+// Contexts of a device borrow them from a pool for the duration of
+// upbp_run_iteration, so contexts driven by W threads at once hold at most W
+// lists (a 64-job batch would otherwise keep 64, each grown to its job's
+// largest iteration); a returned list keeps its size for the next borrower.
+// The pool's idle lists are freed with the device's last context, or to make
+// room when a list cannot grow.
+struct HitPool {
+    std::mutex mu;
+    std::vector<std::pair<uint2*, unsigned>> idle;  // (list, capacity in entries)
+    int contexts = 0;
+};
+HitPool g_hit_pool[kMaxDevices];
+
+// Frees the device's idle hit lists (the device must be current).
+void hit_pool_release_idle(int dev)
+{
+    HitPool& p = g_hit_pool[dev];
+    std::lock_guard<std::mutex> lk(p.mu);
+    for (auto& h : p.idle) cudaFree(h.first);
+    p.idle.clear();
+}
 
 template <class T>
 cudaError_t dalloc(T** p, size_t n)
@@ -258,6 +281,7 @@ struct upbp_ctx {
     // copy of one kernel kind's work counters for a round that is repeated
     uint2* d_hit_qb = nullptr;
     unsigned hit_capacity = 0;
+    size_t hit_want = 0;  // list size the last growth asked for (the pool's best fit)
     size_t max_hits = 0;  // largest list: kMaxHits, or UPBP_MAX_HITS entries when that is smaller
     HitState* d_hit_state = nullptr;
     HitState h_hit_state = {};
@@ -286,9 +310,51 @@ struct upbp_ctx {
 namespace {
 
 // Blocks of a launch under the context's grid limit (at least one).
+// Borrows the largest idle hit list of the context's device for one call
+// and returns it (after the call's kernels are done) at the end.
+class HitLease {
+  public:
+    explicit HitLease(upbp_ctx* c);
+    ~HitLease();
+
+  private:
+    upbp_ctx* c_;
+};
+
 unsigned cap_grid(const upbp_ctx* c, unsigned blocks)
 {
     return c->grid_limit ? std::max(1u, std::min(blocks, c->grid_limit)) : blocks;
+}
+
+HitLease::HitLease(upbp_ctx* c) : c_(c)
+{
+    // the smallest idle list that holds what the context's last iteration
+    // needed, else the largest (which then grows): a list is not freed and
+    // reallocated (a device-wide synchronisation) while one of the right
+    // size sits idle
+    HitPool& p = g_hit_pool[c->dev];
+    std::lock_guard<std::mutex> lk(p.mu);
+    if (p.idle.empty()) return;
+    auto pick = p.idle.end(), largest = p.idle.begin();
+    for (auto it = p.idle.begin(); it != p.idle.end(); ++it) {
+        if (it->second > largest->second) largest = it;
+        if (it->second >= c->hit_want && (pick == p.idle.end() || it->second < pick->second)) pick = it;
+    }
+    if (pick == p.idle.end()) pick = largest;
+    c->d_hit_qb = pick->first;
+    c->hit_capacity = pick->second;
+    p.idle.erase(pick);
+}
+
+HitLease::~HitLease()
+{
+    if (!c_->d_hit_qb) return;
+    cudaStreamSynchronize(c_->st);  // an error return skips the call's own final synchronisation
+    HitPool& p = g_hit_pool[c_->dev];
+    std::lock_guard<std::mutex> lk(p.mu);
+    p.idle.emplace_back(c_->d_hit_qb, c_->hit_capacity);
+    c_->d_hit_qb = nullptr;
+    c_->hit_capacity = 0;
 }
 
 // Uploads the context's launch parameters into its slot (stream-ordered
@@ -609,16 +675,34 @@ int ensure_chunks(upbp_ctx* c, unsigned n)
 // in flight.  The evaluation's grid-stride index stays below 2^32.
 constexpr size_t kMaxHits = (size_t(1) << 32) - (size_t(1) << 21);
 
-// Room for n range-query hits (n + n/4, within 2^20 .. max_hits).
+// Room for n range-query hits (n + n/4, within 2^20 .. max_hits).  When
+// the device has no room for that list, the pool's idle lists are freed and
+// then ever smaller lists tried, down to 2^20 entries: the context's limit
+// becomes the size obtained, and its searches run in more rounds.
 int ensure_hits(upbp_ctx* c, size_t n)
 {
     if (n <= c->hit_capacity || c->hit_capacity >= c->max_hits) return UPBP_OK;
-    const size_t cap = std::min<size_t>(std::max<size_t>(n + n / 4, 1u << 20), c->max_hits);
+    size_t cap = std::min<size_t>(std::max<size_t>(n + n / 4, 1u << 20), c->max_hits);
+    c->hit_want = std::max(c->hit_want, cap);
     UPBP_CK(cudaStreamSynchronize(c->st));
     cudaFree(c->d_hit_qb);
     c->d_hit_qb = nullptr;
     c->hit_capacity = 0;
-    UPBP_CK(dalloc(&c->d_hit_qb, cap));
+    bool pool_freed = false;
+    for (;;) {
+        const cudaError_t e = dalloc(&c->d_hit_qb, cap);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorMemoryAllocation) UPBP_CK(e);
+        (void)cudaGetLastError();  // an allocation failure is not sticky
+        if (!pool_freed) {
+            hit_pool_release_idle(c->dev);
+            pool_freed = true;
+            continue;
+        }
+        if (cap <= (1u << 20)) UPBP_CK(e);
+        cap = std::max<size_t>(cap / 2, 1u << 20);
+        c->max_hits = cap;
+    }
     c->hit_capacity = (unsigned)cap;
     return UPBP_OK;
 }
@@ -683,6 +767,10 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         upbp_ctx* c = new upbp_ctx();
         c->cfg = *cfg;
         c->dev = dev;
+        {
+            std::lock_guard<std::mutex> lk(g_hit_pool[dev].mu);
+            g_hit_pool[dev].contexts++;
+        }
         DeviceParams& P = c->P;
         UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         UPBP_CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_status), sizeof(unsigned)));
@@ -966,7 +1054,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
                 std::vector<float> w0;
                 guide_init_params(w0);
                 UPBP_CK(guide_set_params(g.net, w0.data(), c->st));
-                UPBP_CK(guide_alloc_batch(g.batch, rows));
+                UPBP_CK(guide_alloc_batch(g.batch, rows, false));
                 g.rec_capacity = 1u << 20;
                 UPBP_CK(dalloc(&g.recs, g.rec_capacity));
                 UPBP_CK(dalloc(&g.rec_count, 1));
@@ -1006,6 +1094,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         DeviceGuard dg(c->dev);
         UPBP_CK(dg.error());
         SlotLease lease(c->dev, c->slot, c->st);
+        HitLease hits(c);
         DeviceParams& P = c->P;
         const upbp_config& cfg = c->cfg;
         const unsigned L = P.light_subpath_count;
@@ -1104,19 +1193,23 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         } else {
             P.iteration = (unsigned)iteration;
         }
+        UPBP_CK(cudaEventRecord(ev[13], c->st));
         if (guide_training) {
             // train on every record collected so far, then bake the network
             // into the back table, which the next iteration renders with
             for (int k = 0; k < gs.steps_per_iteration; k++)
-                guide_train_step(c->st, gs, (unsigned)(iteration * gs.steps_per_iteration + k + 1));
+                UPBP_CK(guide_train_step(c->st, gs, (unsigned)(iteration * gs.steps_per_iteration + k + 1)));
             const int back = gs.front == 0 ? 1 : 0;
-            guide_fill_table(c->st, gs, gs.table[back]);
-            UPBP_CK(cudaGetLastError());
-            UPBP_CK(cudaMemcpyAsync(gs.h_scal, gs.batch.scal, 2 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+            UPBP_CK(guide_fill_table(c->st, gs, gs.table[back]));
+            UPBP_CK(cudaMemcpyAsync(gs.h_scal, gs.batch.scal, 3 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
             UPBP_CK(cudaStreamSynchronize(c->st));
+            if (reinterpret_cast<const unsigned&>(gs.h_scal[2]) != 0u) {
+                upbp_host::set_error("learned proposal: a tensor-core chain of the training kernels did not complete");
+                return UPBP_ERR_CUDA;
+            }
             gs.last_loss = gs.h_scal[0] / (float)gs.batch.rows;
             gs.front_next = back;
-            launches += gs.steps_per_iteration * 16 + 3;
+            launches += gs.steps_per_iteration * 3 + 1;
         }
         UPBP_CK(cudaEventRecord(ev[1], c->st));
 
@@ -1485,15 +1578,18 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
         // since the previous stats call (up to the event ring size)
         for (unsigned k = 0; k < c->ev_pending; k++) {
             cudaEvent_t* ev = c->ev_ring[(c->iterations - 1 - k) % kEventRing];
-            float light, build, cam;
-            UPBP_CK(cudaEventElapsedTime(&light, ev[0], ev[1]));
+            float light, guide, build, cam;
+            UPBP_CK(cudaEventElapsedTime(&light, ev[0], ev[13]));
+            UPBP_CK(cudaEventElapsedTime(&guide, ev[13], ev[1]));
             UPBP_CK(cudaEventElapsedTime(&build, ev[1], ev[2]));
             UPBP_CK(cudaEventElapsedTime(&cam, ev[2], ev[12]));
             if (k == 0) {
                 o->ms_light = light;
                 o->ms_build = build;
                 o->ms_camera = cam;
+                o->ms_guide = guide;
             }
+            o->ms_guide_sum += guide;
             o->ms_light_sum += light;
             o->ms_build_sum += build;
             o->ms_camera_sum += cam;
@@ -1704,23 +1800,35 @@ extern "C" int upbp_guide_gradients(const float* params, uint32_t n_params, cons
         auto run = [&]() -> int {
             UPBP_CK(guide_alloc_net(net, st));
             UPBP_CK(guide_set_params(net, params, st));
-            UPBP_CK(guide_alloc_batch(b, rows));
+            UPBP_CK(guide_alloc_batch(b, rows, true));
             std::vector<__half> xh((size_t)rows * kGuideInPad);
             for (size_t i = 0; i < xh.size(); i++) xh[i] = __float2half(x[i]);
             UPBP_CK(cudaMemcpyAsync(b.X, xh.data(), xh.size() * sizeof(__half), cudaMemcpyHostToDevice, st));
             UPBP_CK(cudaMemcpyAsync(b.T, t, (size_t)rows * sizeof(float4), cudaMemcpyHostToDevice, st));
-            guide_forward(st, net, b, b.X, rows);
-            guide_loss(st, b, rows);
+            UPBP_CK(cudaMemsetAsync(b.scal, 0, 3 * sizeof(float), st));
             UPBP_CK(cudaMemsetAsync(net.grad, 0, kGuideParams * sizeof(float), st));
-            guide_backward(st, net, b, rows);
-            UPBP_CK(cudaGetLastError());
-            UPBP_CK(cudaMemcpyAsync(grads, net.grad, kGuideParams * sizeof(float), cudaMemcpyDeviceToHost, st));
-            if (outputs)
-                UPBP_CK(cudaMemcpyAsync(outputs, b.O, (size_t)rows * kGuideOutPad * sizeof(float),
+            k_guide_weight_sum<<<148, 256, 0, st>>>(b.T, rows, b.scal + 1);
+            float* dout = nullptr;
+            if (outputs) UPBP_CK(dalloc(&dout, (size_t)rows * kGuideOutPad));
+            GuideTcArgs a = guide_tc_args(net, rows, b.scal);
+            a.X = b.X;
+            a.T = b.T;
+            a.O = dout;
+            const cudaError_t le = guide_tc_launch<kTcTrainRows>(st, a);
+            if (le == cudaSuccess && outputs)
+                UPBP_CK(cudaMemcpyAsync(outputs, dout, (size_t)rows * kGuideOutPad * sizeof(float),
                                         cudaMemcpyDeviceToHost, st));
-            float scal[2];
+            cudaStreamSynchronize(st);
+            if (dout) cudaFree(dout);
+            UPBP_CK(le);
+            UPBP_CK(cudaMemcpyAsync(grads, net.grad, kGuideParams * sizeof(float), cudaMemcpyDeviceToHost, st));
+            float scal[3];
             UPBP_CK(cudaMemcpyAsync(scal, b.scal, sizeof(scal), cudaMemcpyDeviceToHost, st));
             UPBP_CK(cudaStreamSynchronize(st));
+            if (reinterpret_cast<const unsigned&>(scal[2]) != 0u) {
+                upbp_host::set_error("upbp_guide_gradients: a tensor-core chain did not complete");
+                return UPBP_ERR_CUDA;
+            }
             if (loss) *loss = scal[0];
             return UPBP_OK;
         };
@@ -1750,6 +1858,38 @@ extern "C" int upbp_run_batch(upbp_ctx* const* ctxs, uint32_t n, int iteration, 
         for (uint32_t i = 0; i < n; i++)
             if (!ctxs[i]) return UPBP_ERR_ARGS;
         const unsigned w = (unsigned)std::max(1, std::min<int>(workers > 0 ? workers : 16, (int)n));
+        // Range-query hit lists: up to w of them are in use at once (one per
+        // worker, from the device's pool), each growing toward its job's
+        // need.  Each worker's list is held to an even share of half the
+        // device memory that is free or idle in the pool; a job that needs
+        // more runs its searches in rounds.  The contexts' own limits are
+        // restored afterwards.
+        std::vector<size_t> saved_max(n);
+        {
+            const int dev = ctxs[0]->dev;
+            DeviceGuard dg(dev);
+            UPBP_CK(dg.error());
+            size_t free_b = 0, total_b = 0;
+            UPBP_CK(cudaMemGetInfo(&free_b, &total_b));
+            size_t idle_b = 0;
+            {
+                std::lock_guard<std::mutex> lk(g_hit_pool[dev].mu);
+                for (auto& h : g_hit_pool[dev].idle) idle_b += (size_t)h.second * sizeof(uint2);
+            }
+            const size_t share = std::max<size_t>((free_b + idle_b) / 2 / w / sizeof(uint2), 1u << 20);
+            for (uint32_t i = 0; i < n; i++) {
+                saved_max[i] = ctxs[i]->max_hits;
+                if (ctxs[i]->dev == dev) ctxs[i]->max_hits = std::min(ctxs[i]->max_hits, share);
+            }
+        }
+        struct Restore {
+            upbp_ctx* const* c;
+            std::vector<size_t>& m;
+            ~Restore()
+            {
+                for (size_t i = 0; i < m.size(); i++) c[i]->max_hits = m[i];
+            }
+        } restore{ctxs, saved_max};
         std::atomic<uint32_t> next{0};
         std::atomic<unsigned> status{0};
         std::mutex mu;
@@ -1818,5 +1958,11 @@ extern "C" void upbp_destroy(upbp_ctx* c)
         for (auto& e : slot)
             if (e) cudaEventDestroy(e);
     if (c->st) cudaStreamDestroy(c->st);
+    bool last = false;
+    {
+        std::lock_guard<std::mutex> lk(g_hit_pool[c->dev].mu);
+        last = --g_hit_pool[c->dev].contexts == 0;
+    }
+    if (last) hit_pool_release_idle(c->dev);
     delete c;
 }

@@ -1,13 +1,13 @@
-// Host side of the learned proposal (kernels in upbp_guide.cuh): network
-// state, the training step (forward, loss, backward, Adam) as a sequence of
-// tensor-core GEMMs and element-wise kernels on the context's stream, and the
-// table the render kernels read.  Included by upbp_capi.cu after its
+// Host side of the learned proposal (kernels in upbp_guide.cuh and
+// upbp_guide_tc.cuh): network state, the training step (batch weight sum,
+// the fused tcgen05 forward / loss / backward kernel, Adam) on the context's
+// stream, and the table the render kernels read.  Included by upbp_capi.cu after its
 // allocation and error-check helpers.
 #pragma once
 
 #include <random>
 
-#include "upbp_guide.cuh"
+#include "upbp_guide_tc.cuh"
 
 namespace {
 
@@ -20,16 +20,14 @@ struct GuideNet {
     int steps = 0;           // Adam steps taken
 };
 
+// Buffers of one training step: the batch's own rows exist only in the
+// fused kernel's shared memory; X and T hold given rows (the gradient check
+// entry point).
 struct GuideBatch {
     unsigned rows = 0;
-    __half* X = nullptr;      // rows x kGuideInPad
-    __half* H[3] = {};        // rows x kGuideHidden, after ReLU
-    float* Hf = nullptr;      // rows x kGuideHidden scratch (FP32 GEMM output)
-    float* O = nullptr;       // rows x kGuideOutPad
-    __half* dO = nullptr;     // rows x kGuideOutPad
-    __half* dH = nullptr;     // rows x kGuideHidden
-    float4* T = nullptr;      // rows: target direction, weight
-    float* scal = nullptr;    // [0] weighted loss sum [1] weight sum
+    __half* X = nullptr;      // rows x kGuideInPad, given rows only
+    float4* T = nullptr;      // rows: target direction, weight; given rows only
+    float* scal = nullptr;    // [0] weighted loss sum [1] weight sum [2] error bits (unsigned)
 };
 
 struct GuideState {
@@ -50,28 +48,24 @@ struct GuideState {
     unsigned table_rows = 0;
     float3 lo{}, ext{};
     float last_loss = 0.f;
-    float h_scal[2] = {0.f, 0.f};
+    float h_scal[3] = {0.f, 0.f, 0.f};
     int front_next = -1;        // table the last training step filled
 };
 
-cudaError_t guide_alloc_batch(GuideBatch& b, unsigned rows)
+cudaError_t guide_alloc_batch(GuideBatch& b, unsigned rows, bool given_rows)
 {
     b.rows = rows;
     cudaError_t e;
-    if ((e = dalloc(&b.X, (size_t)rows * kGuideInPad)) != cudaSuccess) return e;
-    for (auto& h : b.H)
-        if ((e = dalloc(&h, (size_t)rows * kGuideHidden)) != cudaSuccess) return e;
-    if ((e = dalloc(&b.Hf, (size_t)rows * kGuideHidden)) != cudaSuccess) return e;
-    if ((e = dalloc(&b.O, (size_t)rows * kGuideOutPad)) != cudaSuccess) return e;
-    if ((e = dalloc(&b.dO, (size_t)rows * kGuideOutPad)) != cudaSuccess) return e;
-    if ((e = dalloc(&b.dH, (size_t)rows * kGuideHidden)) != cudaSuccess) return e;
-    if ((e = dalloc(&b.T, rows)) != cudaSuccess) return e;
-    return dalloc(&b.scal, 2);
+    if (given_rows) {
+        if ((e = dalloc(&b.X, (size_t)rows * kGuideInPad)) != cudaSuccess) return e;
+        if ((e = dalloc(&b.T, rows)) != cudaSuccess) return e;
+    }
+    return dalloc(&b.scal, 3);
 }
 
 void guide_free_batch(GuideBatch& b)
 {
-    void* p[] = {b.X, b.H[0], b.H[1], b.H[2], b.Hf, b.O, b.dO, b.dH, b.T, b.scal};
+    void* p[] = {b.X, b.T, b.scal};
     for (void* x : p)
         if (x) cudaFree(x);
     b = GuideBatch{};
@@ -131,60 +125,34 @@ cudaError_t guide_set_params(GuideNet& n, const float* w, cudaStream_t st)
     return cudaStreamSynchronize(st);  // h is a host temporary
 }
 
-void guide_gemm(cudaStream_t st, const __half* A, long long sam, long long sak, const __half* B, long long sbk,
-                long long sbn, float* C, int ldc, int M, int N, int K, const float* bias, int relu, __half* H,
-                bool accumulate, int split)
+// Launches one of the fused tcgen05 kernels: one CTA per SM (at most one
+// per tile), each with the kernel's shared-memory arrays.
+template <int MODE>
+cudaError_t guide_tc_launch(cudaStream_t st, const GuideTcArgs& a)
 {
-    GemmArgs g{A, sam, sak, B, sbk, sbn, C, ldc, M, N, K, 0, bias, relu, H, accumulate ? 1 : 0};
-    split = std::max(1, std::min(split, (K + kGemmBK - 1) / kGemmBK));
-    const int per = ((K + split - 1) / split + kGemmBK - 1) / kGemmBK * kGemmBK;
-    g.k_per_block = per;
-    split = (K + per - 1) / per;
-    dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + kGemmBN - 1) / kGemmBN, split);
-    k_guide_gemm<<<grid, 128, 0, st>>>(g);
+    int dev = 0, sms = 148;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_guide_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(GuideTcSmem))) != cudaSuccess)
+        return e;
+    const unsigned tiles = (a.rows + kTcRows - 1) / kTcRows;
+    k_guide_tc<MODE><<<std::max(1u, std::min(tiles, (unsigned)sms)), kTcThreads, sizeof(GuideTcSmem), st>>>(a);
+    return cudaGetLastError();
 }
 
-// Forward pass of `rows` inputs: H[0..2] (FP16, after ReLU) and O (FP32).
-void guide_forward(cudaStream_t st, const GuideNet& n, GuideBatch& b, const __half* X, unsigned rows)
+GuideTcArgs guide_tc_args(const GuideNet& n, unsigned rows, float* scal)
 {
-    const float* bias = n.w32 + kGuideWeights;
-    const __half* in = X;
-    for (int l = 0; l < 3; l++) {
-        const int K = kGuideLayerIn[l], N = kGuideLayerOut[l];
-        guide_gemm(st, in, K, 1, n.w16 + kGuideWOff[l], N, 1, b.Hf, N, (int)rows, N, K, bias + kGuideBOff[l], 1, b.H[l],
-                   false, 1);
-        in = b.H[l];
-    }
-    guide_gemm(st, in, kGuideHidden, 1, n.w16 + kGuideWOff[3], kGuideOutPad, 1, b.O, kGuideOutPad, (int)rows,
-               kGuideOutPad, kGuideHidden, bias + kGuideBOff[3], 0, nullptr, false, 1);
-}
-
-// Backward pass of the batch in b (after guide_forward and the loss's dO):
-// gradient sums into n.grad.
-void guide_backward(cudaStream_t st, GuideNet& n, GuideBatch& b, unsigned rows)
-{
-    const int R = (int)rows;
-    const int split = std::max(1, std::min(148, R / 1024));
-    float* gw = n.grad;
-    float* gb = n.grad + kGuideWeights;
-    const __half* dY = b.dO;
-    int ny = kGuideOutPad;
-    for (int l = kGuideLayers - 1; l >= 0; l--) {
-        const int K = kGuideLayerIn[l];
-        const __half* Hin = l == 0 ? b.X : b.H[l - 1];
-        // dW_l = H_in^T dY, db_l = column sums of dY
-        guide_gemm(st, Hin, 1, K, dY, ny, 1, gw + kGuideWOff[l], ny, K, ny, R, nullptr, 0, nullptr, true, split);
-        k_guide_colsum<<<296, 256, 0, st>>>(dY, rows, ny, gb + kGuideBOff[l]);
-        if (l == 0) break;
-        // dH_in = (dY W_l^T) masked by the ReLU of H_in
-        guide_gemm(st, dY, ny, 1, n.w16 + kGuideWOff[l], 1, ny, b.Hf, kGuideHidden, R, kGuideHidden, ny, nullptr, 0,
-                   nullptr, false, 1);
-        const size_t cnt = (size_t)rows * kGuideHidden;
-        k_guide_relu_mask<<<(unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 64), 256, 0, st>>>(b.H[l - 1], b.Hf,
-                                                                                                    b.dH, cnt);
-        dY = b.dH;
-        ny = kGuideHidden;
-    }
+    GuideTcArgs a{};
+    a.w16 = n.w16;
+    a.w32 = n.w32;
+    a.rows = rows;
+    a.weight_sum = scal + 1;
+    a.grad = n.grad;
+    a.loss_sum = scal;
+    a.err = reinterpret_cast<unsigned*>(scal + 2);
+    return a;
 }
 
 void guide_adam(cudaStream_t st, GuideNet& n, unsigned rows, float lr)
@@ -196,40 +164,42 @@ void guide_adam(cudaStream_t st, GuideNet& n, unsigned rows, float lr)
                                                             bc1, bc2, 1.f / (float)rows, n.w16, kGuideWeights);
 }
 
-// Loss and output gradients of the batch in b (weights normalised by the
-// batch mean).
-void guide_loss(cudaStream_t st, GuideBatch& b, unsigned rows)
-{
-    cudaMemsetAsync(b.scal, 0, 2 * sizeof(float), st);
-    k_guide_weight_sum<<<148, 256, 0, st>>>(b.T, rows, b.scal + 1);
-    k_guide_loss<<<(rows + 255) / 256, 256, 0, st>>>(b.O, b.T, rows, b.scal + 1, b.dO, b.scal);
-}
-
-// One training step on a batch drawn from the records.
-void guide_train_step(cudaStream_t st, GuideState& g, unsigned seed)
+// One training step on a batch drawn from the records: its weight sum,
+// then the fused forward / loss / backward kernel, then Adam.
+cudaError_t guide_train_step(cudaStream_t st, GuideState& g, unsigned seed)
 {
     GuideBatch& b = g.batch;
-    const float3 inv_ext = make_float3(1.f / g.ext.x, 1.f / g.ext.y, 1.f / g.ext.z);
-    k_guide_batch<<<(b.rows + kGuideRowsPerBlock - 1) / kGuideRowsPerBlock, kGuideRowsPerBlock, 0, st>>>(
-        g.recs, g.rec_count, g.rec_capacity, b.rows, seed, g.lo, inv_ext, g.med_g, g.medium_slot, b.X, b.T);
-    guide_forward(st, g.net, b, b.X, b.rows);
-    guide_loss(st, b, b.rows);
-    cudaMemsetAsync(g.net.grad, 0, kGuideParams * sizeof(float), st);
-    guide_backward(st, g.net, b, b.rows);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(b.scal, 0, 3 * sizeof(float), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(g.net.grad, 0, kGuideParams * sizeof(float), st)) != cudaSuccess) return e;
+    k_guide_record_weights<<<148, 256, 0, st>>>(g.recs, g.rec_count, g.rec_capacity, b.rows, seed, g.med_g,
+                                                g.medium_slot, b.scal + 1);
+    GuideTcArgs a = guide_tc_args(g.net, b.rows, b.scal);
+    a.recs = g.recs;
+    a.rec_count = g.rec_count;
+    a.rec_capacity = g.rec_capacity;
+    a.seed = seed;
+    a.lo = g.lo;
+    a.inv_ext = make_float3(1.f / g.ext.x, 1.f / g.ext.y, 1.f / g.ext.z);
+    a.med_g = g.med_g;
+    a.medium_slot = g.medium_slot;
+    if ((e = guide_tc_launch<kTcTrainRecords>(st, a)) != cudaSuccess) return e;
     guide_adam(st, g.net, b.rows, 1e-3f);
+    return cudaGetLastError();
 }
 
-// Bakes the network into the back table (cell centres x direction bins x
-// media slots), in chunks of the batch's rows.
-void guide_fill_table(cudaStream_t st, GuideState& g, float4* table)
+// Bakes the network into a table (cell centres x direction bins x media
+// slots) with the fused forward kernel.
+cudaError_t guide_fill_table(cudaStream_t st, GuideState& g, float4* table)
 {
-    GuideBatch& b = g.batch;
-    const float3 cell = make_float3(g.ext.x / g.cells, g.ext.y / g.cells, g.ext.z / g.cells);
-    const float3 inv_ext = make_float3(1.f / g.ext.x, 1.f / g.ext.y, 1.f / g.ext.z);
-    k_guide_table_inputs<<<(g.table_rows + kGuideRowsPerBlock - 1) / kGuideRowsPerBlock, kGuideRowsPerBlock, 0, st>>>(
-        g.cells, g.dir_res, g.slots, g.lo, cell, inv_ext, b.X);
-    guide_forward(st, g.net, b, b.X, g.table_rows);
-    k_guide_table_entries<<<(g.table_rows + 255) / 256, 256, 0, st>>>(b.O, g.table_rows, table);
+    GuideTcArgs a = guide_tc_args(g.net, g.table_rows, g.batch.scal);
+    a.cells = g.cells;
+    a.dir_res = g.dir_res;
+    a.lo = g.lo;
+    a.cell = make_float3(g.ext.x / g.cells, g.ext.y / g.cells, g.ext.z / g.cells);
+    a.inv_ext = make_float3(1.f / g.ext.x, 1.f / g.ext.y, 1.f / g.ext.z);
+    a.entries = table;
+    return guide_tc_launch<kTcBake>(st, a);
 }
 
 }  // namespace

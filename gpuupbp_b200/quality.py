@@ -57,3 +57,76 @@ def equal_time(plain_args: list[str], other_args: list[str], reference_iteration
             "other_iterations": n_other, "other_ms": t_other, "plain_iterations": n_plain, "plain_ms": t_plain,
             "relmse_other": e_other, "relmse_plain": e_plain,
             "relmse_ratio_plain_over_other": e_plain / e_other if e_other > 0 else None}
+
+
+def _batch_images(b) -> list:
+    return [r.accumulated() for r in b.renderers]
+
+
+def batch_equal_time(jobs: list, method_extra: list, reference_iterations: int, method_iterations: int,
+                     reference_start: int = 100000) -> dict:
+    """Equal-time comparison on many jobs (config 3 of the benchmark spec).
+
+    * reference: every job's converged plain render, reference_iterations
+      batch iterations on iteration indices from reference_start;
+    * method: the jobs with `method_extra` appended to their command lines
+      (e.g. the learned proposal), rendered together by upbp_run_batch with
+      the autotuner's choice, method_iterations iterations; its wall time T
+      (the autotuning iterations are part of the method's work and time);
+    * plain: the plain single-scene renderer taking the jobs one after
+      another (one worker, no launch cap), whole iterations of all jobs
+      until it has used the time T.
+    Returns per-job relMSEs, the mean relMSE of both, and their ratio."""
+    import time
+
+    import torch
+
+    from gpuupbp_b200 import batch as B
+
+    ref = B.Batch(jobs)
+    tune = B.autotune(ref, reference_start)
+    it = tune["next_iteration"]
+    while ref.renderers[0].iterations < reference_iterations:
+        ref.run_iteration(it)
+        it += 1
+    refs = _batch_images(ref)
+    ref.close()
+
+    m = B.Batch([j + method_extra for j in jobs])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tune_m = B.autotune(m, 0)
+    it = tune_m["next_iteration"]
+    while m.renderers[0].iterations < method_iterations:
+        m.run_iteration(it)
+        it += 1
+    torch.cuda.synchronize()
+    t_method = time.perf_counter() - t0
+    imgs_m = _batch_images(m)
+    n_method = m.renderers[0].iterations
+    m.close()
+
+    p = B.Batch(jobs)
+    p.set_grid_limit(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    it, t_plain = 0, 0.0
+    while t_plain < t_method:
+        p.run_iteration(it, workers=1)
+        it += 1
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+    imgs_p = _batch_images(p)
+    n_plain = it
+    p.close()
+
+    e_m = [relmse(x, r) for x, r in zip(imgs_m, refs)]
+    e_p = [relmse(x, r) for x, r in zip(imgs_p, refs)]
+    mean_m, mean_p = float(np.mean(e_m)), float(np.mean(e_p))
+    return {"jobs": len(jobs), "reference_iterations": reference_iterations,
+            "method_iterations": n_method, "method_s": t_method, "method_autotune": tune_m,
+            "plain_iterations": n_plain, "plain_s": t_plain,
+            "relmse_method_mean": mean_m, "relmse_plain_mean": mean_p,
+            "relmse_ratio_plain_over_method": mean_p / mean_m if mean_m > 0 else None,
+            "per_job_ratio_median": float(np.median(np.array(e_p) / np.maximum(np.array(e_m), 1e-30))),
+            "relmse_method": e_m, "relmse_plain": e_p}

@@ -63,6 +63,7 @@ class Stats(ctypes.Structure):
         ("work", (ctypes.c_uint64 * 8) * 9), ("ms_kernel_sum", ctypes.c_double * 9),
         ("segment_queries", ctypes.c_uint32), ("point_queries", ctypes.c_uint32),
         ("nee_samples", ctypes.c_uint32), ("bpt_pairs", ctypes.c_uint32),
+        ("ms_guide", ctypes.c_double), ("ms_guide_sum", ctypes.c_double),
     ]
 
 

@@ -233,6 +233,10 @@ typedef struct upbp_stats {
     double ms_kernel_sum[UPBP_KERNEL_KINDS];
     uint32_t segment_queries, point_queries;   /* query records of the last camera pass */
     uint32_t nee_samples, bpt_pairs;           /* deferred connections of the last camera pass */
+    /* Training of the learned proposal (its steps and the table bake) in
+     * the last iteration and summed like the pass times; zero without it.
+     * ms_light excludes it. */
+    double ms_guide, ms_guide_sum;
 } upbp_stats;
 
 /* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
