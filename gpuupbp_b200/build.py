@@ -26,7 +26,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompiler", "-f
 
 DEVICE_SOURCES = ["upbp_capi.cu"]
 HOST_SOURCES = ["host/upbp_cli.cpp", "host/upbp_scene.cpp", "host/upbp_predef.cpp", "host/upbp_exr.cpp",
-                "host/upbp_exr_read.cpp", "host/upbp_sah.cpp"]
+                "host/upbp_exr_read.cpp"]
 
 
 def _sources():

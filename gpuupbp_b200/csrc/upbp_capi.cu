@@ -15,11 +15,11 @@
 #include <thread>
 #include <vector>
 
-#include "host/upbp_sah.h"
 #include "host/upbp_scene.h"
 #include "upbp_build.cuh"
 #include "upbp_camera_pass.cuh"
 #include "upbp_light_pass.cuh"
+#include "upbp_scene_bvh.cuh"
 
 using namespace upbp;
 
@@ -282,6 +282,7 @@ struct upbp_ctx {
     uint2* d_hit_qb = nullptr;
     unsigned hit_capacity = 0;
     size_t hit_want = 0;  // list size the last growth asked for (the pool's best fit)
+    double ms_scene_bvh = 0;  // device time of the scene BVH builds in upbp_create
     size_t max_hits = 0;  // largest list: kMaxHits, or UPBP_MAX_HITS entries when that is smaller
     HitState* d_hit_state = nullptr;
     HitState h_hit_state = {};
@@ -485,6 +486,157 @@ int upload_env_map(upbp_ctx* c, const upbp_scene_desc* s)
     return UPBP_OK;
 }
 
+// Static scene: the binned-SAH tree of one class of triangles (original
+// order in `tri`: v0, e1, e2), built on the device once per context
+// (upbp_scene_bvh.cuh): g.nodes receives the n - 1 nodes, g.tri the
+// triangles in leaf order with the original index in v0.w.  The host runs
+// the levels of ranges above kSahSmall primitives (reading each level's
+// split counts back to lay out the next); one launch finishes the rest.
+cudaError_t build_scene_bvh(upbp_ctx* c, Geometry& g, const std::vector<float4>& tri)
+{
+    const unsigned n = g.count;
+    cudaStream_t st = c->st;
+    float4 *d_tri = nullptr, *blo = nullptr, *bhi = nullptr, *cen = nullptr;
+    unsigned *perm = nullptr, *perm2 = nullptr;
+    SahTask* d_tasks = nullptr;
+    SahWork* d_work = nullptr;
+    SahBins* d_bins = nullptr;
+    SahSplit* d_splits = nullptr;
+    unsigned *d_chunk_left = nullptr, *d_left_off = nullptr, *d_right_off = nullptr, *d_which = nullptr;
+    unsigned task_cap = 0, work_cap = 0;
+    auto run = [&]() -> cudaError_t {
+        cudaError_t e;
+#define SAH_CK(x)                               \
+    do {                                        \
+        if ((e = (x)) != cudaSuccess) return e; \
+    } while (0)
+        SAH_CK(dupload(&d_tri, tri.data(), tri.size(), st));
+        SAH_CK(dalloc(&blo, n));
+        SAH_CK(dalloc(&bhi, n));
+        SAH_CK(dalloc(&cen, n));
+        SAH_CK(dalloc(&perm, n));
+        SAH_CK(dalloc(&perm2, n));
+        k_sah_tri_boxes<<<(n + 255) / 256, 256, 0, st>>>(d_tri, n, blo, bhi, cen);
+        {
+            std::vector<unsigned> iota(n);
+            for (unsigned i = 0; i < n; i++) iota[i] = i;
+            SAH_CK(cudaMemcpyAsync(perm, iota.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+            SAH_CK(cudaStreamSynchronize(st));
+        }
+        std::vector<SahTask> level, small;
+        if (n >= 2) (n > kSahSmall ? level : small).push_back(SahTask{0, n, 0, 0});
+        while (!level.empty()) {
+            std::vector<SahWork> work;
+            for (unsigned t = 0; t < level.size(); t++)
+                for (unsigned a = level[t].a; a < level[t].e; a += kSahChunk)
+                    work.push_back(SahWork{t, a, std::min(a + kSahChunk, level[t].e)});
+            const unsigned nt = (unsigned)level.size(), nw = (unsigned)work.size();
+            if (nt > task_cap) {
+                cudaFree(d_tasks);
+                cudaFree(d_bins);
+                cudaFree(d_splits);
+                cudaFree(d_which);
+                d_tasks = nullptr;
+                d_bins = nullptr;
+                d_splits = nullptr;
+                d_which = nullptr;
+                task_cap = nt;
+                SAH_CK(dalloc(&d_tasks, task_cap));
+                SAH_CK(dalloc(&d_bins, task_cap));
+                SAH_CK(dalloc(&d_splits, task_cap));
+                SAH_CK(dalloc(&d_which, task_cap));
+            }
+            if (nw > work_cap) {
+                cudaFree(d_work);
+                cudaFree(d_chunk_left);
+                cudaFree(d_left_off);
+                cudaFree(d_right_off);
+                d_work = nullptr;
+                d_chunk_left = d_left_off = d_right_off = nullptr;
+                work_cap = nw;
+                SAH_CK(dalloc(&d_work, work_cap));
+                SAH_CK(dalloc(&d_chunk_left, work_cap));
+                SAH_CK(dalloc(&d_left_off, work_cap));
+                SAH_CK(dalloc(&d_right_off, work_cap));
+            }
+            SAH_CK(cudaMemcpyAsync(d_tasks, level.data(), nt * sizeof(SahTask), cudaMemcpyHostToDevice, st));
+            SAH_CK(cudaMemcpyAsync(d_work, work.data(), nw * sizeof(SahWork), cudaMemcpyHostToDevice, st));
+            k_sah_init_bins<<<nt, 128, 0, st>>>(d_bins, nt);
+            k_sah_centroid_bounds<<<nw, kSahThreads, 0, st>>>(d_work, perm, cen, d_bins);
+            k_sah_bins<<<nw, kSahThreads, 0, st>>>(d_work, perm, cen, blo, bhi, d_bins);
+            k_sah_choose<<<(nt + 127) / 128, 128, 0, st>>>(d_tasks, nt, d_bins, d_splits, g.nodes);
+            k_sah_count_left<<<nw, kSahThreads, 0, st>>>(d_work, d_tasks, d_splits, perm, cen, d_chunk_left);
+            SAH_CK(cudaGetLastError());
+            std::vector<SahSplit> splits(nt);
+            std::vector<unsigned> chunk_left(nw), left_off(nw), right_off(nw);
+            SAH_CK(cudaMemcpyAsync(splits.data(), d_splits, nt * sizeof(SahSplit), cudaMemcpyDeviceToHost, st));
+            SAH_CK(cudaMemcpyAsync(chunk_left.data(), d_chunk_left, nw * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+            SAH_CK(cudaStreamSynchronize(st));
+            {
+                unsigned task = ~0u, lsum = 0, rsum = 0;
+                for (unsigned w = 0; w < nw; w++) {
+                    if (work[w].task != task) {
+                        task = work[w].task;
+                        lsum = rsum = 0;
+                    }
+                    left_off[w] = lsum;
+                    right_off[w] = rsum;
+                    lsum += chunk_left[w];
+                    rsum += (work[w].e - work[w].a) - chunk_left[w];
+                }
+            }
+            SAH_CK(cudaMemcpyAsync(d_left_off, left_off.data(), nw * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+            SAH_CK(cudaMemcpyAsync(d_right_off, right_off.data(), nw * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+            SAH_CK(cudaMemcpyAsync(perm2, perm, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, st));
+            k_sah_scatter<<<nw, kSahThreads, 0, st>>>(d_work, d_tasks, d_splits, perm, cen, d_left_off, d_right_off,
+                                                      perm2);
+            std::swap(perm, perm2);
+            std::vector<unsigned> middle;
+            for (unsigned t = 0; t < nt; t++)
+                if (splits[t].axis < 0) middle.push_back(t);
+            if (!middle.empty()) {
+                SAH_CK(cudaMemcpyAsync(d_which, middle.data(), middle.size() * sizeof(unsigned),
+                                       cudaMemcpyHostToDevice, st));
+                k_sah_middle_nodes<<<(unsigned)middle.size(), kSahThreads, 0, st>>>(d_tasks, d_which, d_splits, perm,
+                                                                                   blo, bhi, g.nodes);
+            }
+            SAH_CK(cudaGetLastError());
+            std::vector<SahTask> next;
+            for (unsigned t = 0; t < nt; t++) {
+                const SahTask& tk = level[t];
+                const unsigned ml = splits[t].ml, mr = tk.e - tk.a - ml;
+                const SahTask kids[2] = {SahTask{tk.a, tk.a + ml, tk.slot + 1, tk.depth + 1},
+                                         SahTask{tk.a + ml, tk.e, tk.slot + ml, tk.depth + 1}};
+                const unsigned counts[2] = {ml, mr};
+                for (int k = 0; k < 2; k++)
+                    if (counts[k] >= 2) (counts[k] > kSahSmall ? next : small).push_back(kids[k]);
+            }
+            SAH_CK(cudaStreamSynchronize(st));  // the host vectors of this level are read by the copies above
+            level.swap(next);
+        }
+        if (!small.empty()) {
+            SahTask* d_small = nullptr;
+            SAH_CK(dupload(&d_small, small.data(), small.size(), st));
+            const unsigned ns = (unsigned)small.size();
+            k_sah_small<<<(ns + 127) / 128, 128, 0, st>>>(d_small, ns, perm, perm2, cen, blo, bhi, g.nodes);
+            SAH_CK(cudaGetLastError());
+            SAH_CK(cudaStreamSynchronize(st));
+            cudaFree(d_small);
+        }
+        k_sah_leaf_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri, perm, n, g.tri);
+        SAH_CK(cudaGetLastError());
+        return cudaStreamSynchronize(st);
+#undef SAH_CK
+    };
+    const cudaError_t e = run();
+    cudaStreamSynchronize(st);
+    void* bufs[] = {d_tri, blo, bhi, cen, perm, perm2, d_tasks, d_work, d_bins, d_splits, d_chunk_left,
+                    d_left_off, d_right_off, d_which};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    return e;
+}
+
 int upload_geometry(upbp_ctx* c, const upbp_scene_desc* s, bool real, Geometry& g)
 {
     std::vector<float4> tri, nrm;
@@ -525,47 +677,21 @@ int upload_geometry(upbp_ctx* c, const upbp_scene_desc* s, bool real, Geometry& 
     UPBP_CK(dupload(&g.normals, nrm.data(), nrm.size(), c->st));
     UPBP_CK(dupload(&g.record, rec.data(), rec.size(), c->st));
     UPBP_CK(dalloc(&g.nodes, g.count > 1 ? g.count - 1 : 1));
-    // Static scene: a binned-SAH tree built once on the host (the photon maps
-    // are rebuilt every iteration as GPU LBVHs).  Triangle boxes as the
-    // device intersects them: v0, v0 + e1, v0 + e2, slightly widened.
-    std::vector<float> boxes(6 * (size_t)g.count);
-    for (unsigned i = 0; i < g.count; i++) {
-        const float4 v0 = tri[3 * (size_t)i], e1 = tri[3 * (size_t)i + 1], e2 = tri[3 * (size_t)i + 2];
-        const float px[3] = {v0.x, v0.x + e1.x, v0.x + e2.x}, py[3] = {v0.y, v0.y + e1.y, v0.y + e2.y},
-                    pz[3] = {v0.z, v0.z + e1.z, v0.z + e2.z};
-        float lo[3] = {std::min({px[0], px[1], px[2]}), std::min({py[0], py[1], py[2]}), std::min({pz[0], pz[1], pz[2]})};
-        float hi[3] = {std::max({px[0], px[1], px[2]}), std::max({py[0], py[1], py[2]}), std::max({pz[0], pz[1], pz[2]})};
-        const float mag = 1e-7f * (std::fabs(lo[0]) + std::fabs(lo[1]) + std::fabs(lo[2]) + 1e-3f);
-        for (int k = 0; k < 3; k++) {
-            const float ext = (hi[k] - lo[k]) * 1e-6f + mag;
-            boxes[6 * (size_t)i + k] = lo[k] - ext;
-            boxes[6 * (size_t)i + 3 + k] = hi[k] + ext;
-        }
+    UPBP_CK(dalloc(&g.tri, 3 * (size_t)std::max(1u, g.count)));
+    if (g.count > 0) {
+        cudaEvent_t e0, e1;
+        UPBP_CK(cudaEventCreate(&e0));
+        UPBP_CK(cudaEventCreate(&e1));
+        UPBP_CK(cudaEventRecord(e0, c->st));
+        const cudaError_t be = build_scene_bvh(c, g, tri);
+        float ms = 0.f;
+        if (be == cudaSuccess && cudaEventRecord(e1, c->st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess)
+            cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        UPBP_CK(be);
+        c->ms_scene_bvh += ms;
     }
-    std::vector<float4> leaf_tri(3 * (size_t)std::max(1u, g.count));
-    if (g.count == 1) {
-        leaf_tri[0] = tri[0];
-        leaf_tri[1] = tri[1];
-        leaf_tri[2] = tri[2];
-    } else if (g.count > 1) {
-        std::vector<uint32_t> order(g.count);
-        std::vector<float> words(16 * (size_t)(g.count - 1));
-        const int threads = (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
-        upbp_host::sah_build(boxes.data(), g.count, words.data(), order.data(), threads);
-        for (unsigned k = 0; k < g.count; k++) {
-            const unsigned i = order[k];
-            float4 a = tri[3 * (size_t)i];
-            const int orig = (int)i;  // original triangle index (normals, records)
-            std::memcpy(&a.w, &orig, sizeof(orig));
-            leaf_tri[3 * (size_t)k] = a;
-            leaf_tri[3 * (size_t)k + 1] = tri[3 * (size_t)i + 1];
-            leaf_tri[3 * (size_t)k + 2] = tri[3 * (size_t)i + 2];
-        }
-        static_assert(sizeof(BvhNode) == 16 * sizeof(float), "node layout");
-        UPBP_CK(cudaMemcpy(g.nodes, words.data(), words.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
-    if (g.count == 1) leaf_tri[0].w = 0.f;  // original index 0
-    UPBP_CK(dupload(&g.tri, leaf_tri.data(), leaf_tri.size(), c->st));
     UPBP_CK(cudaStreamSynchronize(c->st));
     return UPBP_OK;
 }
@@ -1574,6 +1700,7 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
         o->h2d_bytes = (uint32_t)c->h2d_iter;
         o->d2h_bytes = (uint32_t)c->d2h_iter;
         o->kernel_launches = c->launches;
+        o->ms_scene_bvh = c->ms_scene_bvh;
         // per-pass times: the last iteration, and sums over the iterations run
         // since the previous stats call (up to the event ring size)
         for (unsigned k = 0; k < c->ev_pending; k++) {
@@ -1638,6 +1765,28 @@ extern "C" int upbp_debug_photons(upbp_ctx* c, int kind, float* out, uint32_t ca
                 std::memcpy(&o[7], &q3.z, 4);  // path index bits
             }
         }
+        return UPBP_OK;
+    });
+}
+
+// The static scene's BVH of one class of triangles (real 1, imaginary 0)
+// as built on the device: nodes (16 words each) and the triangles in leaf
+// order (12 floats each, v0.w the original index's bits).
+extern "C" int upbp_debug_scene_bvh(upbp_ctx* c, int real, float* nodes, uint64_t node_capacity, float* tris,
+                                    uint64_t tri_capacity, uint32_t* count)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !count) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        const Geometry& g = real ? c->real : c->imag;
+        *count = g.count;
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        const uint64_t nn = g.count > 1 ? (uint64_t)(g.count - 1) * 16 : 0, nt = (uint64_t)g.count * 12;
+        if (nodes && nn) UPBP_CK(cudaMemcpy(nodes, g.nodes, std::min(nn, node_capacity) * sizeof(float),
+                                            cudaMemcpyDeviceToHost));
+        if (tris && nt) UPBP_CK(cudaMemcpy(tris, g.tri, std::min(nt, tri_capacity) * sizeof(float),
+                                           cudaMemcpyDeviceToHost));
         return UPBP_OK;
     });
 }

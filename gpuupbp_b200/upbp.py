@@ -63,7 +63,7 @@ class Stats(ctypes.Structure):
         ("work", (ctypes.c_uint64 * 8) * 9), ("ms_kernel_sum", ctypes.c_double * 9),
         ("segment_queries", ctypes.c_uint32), ("point_queries", ctypes.c_uint32),
         ("nee_samples", ctypes.c_uint32), ("bpt_pairs", ctypes.c_uint32),
-        ("ms_guide", ctypes.c_double), ("ms_guide_sum", ctypes.c_double),
+        ("ms_guide", ctypes.c_double), ("ms_guide_sum", ctypes.c_double), ("ms_scene_bvh", ctypes.c_double),
     ]
 
 
@@ -120,7 +120,7 @@ EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_pr
            "upbp_write_image", "upbp_get_stream", "upbp_last_error",
            "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device",
            "upbp_debug_mis_records", "upbp_guide_info", "upbp_guide_gradients", "upbp_run_batch",
-           "upbp_set_grid_limit"]
+           "upbp_set_grid_limit", "upbp_debug_scene_bvh"]
 
 _libs = {}
 
@@ -162,6 +162,8 @@ def load_library(path: str = LIB_PATH):
     L.upbp_debug_photons.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, P(ctypes.c_uint32)]
     L.upbp_debug_query.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
     L.upbp_debug_query_static.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
+    L.upbp_debug_scene_bvh.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint64, VP, ctypes.c_uint64,
+                                       P(ctypes.c_uint32)]
     _libs[path] = L
     return L
 
@@ -285,6 +287,20 @@ class Renderer:
         out["work"] = {k: dict(zip(WORK_NAMES, list(st.work[i]))) for i, k in enumerate(KERNELS)}
         out["ms_kernel_sum"] = dict(zip(KERNELS, list(st.ms_kernel_sum)))
         return out
+
+    def scene_bvh(self, real: bool):
+        """The device-built scene BVH of one class of triangles
+        (upbp_debug_scene_bvh): (nodes n-1 x 16 float32, leaf-order
+        triangles n x 12 float32)."""
+        L = self._L
+        n = ctypes.c_uint32()
+        _check(L.upbp_debug_scene_bvh(self._ctx, int(real), None, 0, None, 0, ctypes.byref(n)), "scene_bvh")
+        nodes = np.zeros((max(n.value - 1, 0), 16), np.float32)
+        tris = np.zeros((n.value, 12), np.float32)
+        _check(L.upbp_debug_scene_bvh(self._ctx, int(real), nodes.ctypes.data if nodes.size else None, nodes.size,
+                                      tris.ctypes.data if tris.size else None, tris.size, ctypes.byref(n)),
+               "scene_bvh")
+        return nodes, tris
 
     def photons(self, kind: int) -> np.ndarray:
         """Photon map contents of the last iteration (see upbp_debug_photons)."""

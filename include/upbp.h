@@ -237,6 +237,9 @@ typedef struct upbp_stats {
      * the last iteration and summed like the pass times; zero without it.
      * ms_light excludes it. */
     double ms_guide, ms_guide_sum;
+    /* Device time of the scene BVH builds (both classes of triangles) in
+     * upbp_create, including the host's orchestration of their levels. */
+    double ms_scene_bvh;
 } upbp_stats;
 
 /* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
@@ -308,6 +311,16 @@ int upbp_write_image(const char* path, const float* rgb, uint32_t width, uint32_
  * near the segment), 4 BP2D (beams near x).  counts[i] = set size, ids =
  * up to ids_per_query vertex slots (0-2) or beam indices (3-4) per query. */
 int upbp_debug_photons(upbp_ctx* ctx, int kind, float* out, uint32_t capacity, uint32_t* count);
+/* upbp_debug_scene_bvh: the static scene's BVH of one class of triangles
+ * (real 1: surfaces, 0: imaginary medium boundaries), built on the device in
+ * upbp_create (a binned-SAH tree; the reference builds an OptiX GAS,
+ * renderer/renderer_init.cpp:134-289): up to node_capacity floats of nodes
+ * (16 words each: left box lo.xyz hi.xyz, right box, left and right links,
+ * left and right primitive counts; *count - 1 nodes) and up to tri_capacity
+ * floats of triangles in leaf order (12 each: v0 with the original index's
+ * bits in w, e1, e2); *count receives the triangle count. */
+int upbp_debug_scene_bvh(upbp_ctx* ctx, int real, float* nodes, uint64_t node_capacity, float* tris,
+                         uint64_t tri_capacity, uint32_t* count);
 int upbp_debug_query(upbp_ctx* ctx, int kind, const float* queries, uint32_t n, uint32_t* counts, uint32_t* ids,
                      uint32_t ids_per_query);
 

@@ -19,8 +19,13 @@ REFERENCE_ROOT = "/root/reference"
 _lib = None
 
 
+SAH_LIB_PATH = os.path.join(HERE, "_ref", "libsah_ref.so")
+
+
 def build(reference_root: str = REFERENCE_ROOT) -> bool:
-    """Compiles the oracle from the reference sources when they are present."""
+    """Compiles the scene-BVH checker, and the oracle from the reference
+    sources when they are present."""
+    subprocess.run(["make", "-C", HERE, "sah", "-s"], check=True)
     if not os.path.isdir(os.path.join(reference_root, "gpuupbp")):
         return os.path.exists(LIB_PATH)
     subprocess.run(["make", "-C", HERE, f"REF={reference_root}", "-s"], check=True)
@@ -153,3 +158,20 @@ class RefRenderer:
             self.close()
         except Exception:
             pass
+
+
+def sah_build(tri):
+    """The sequential statement of the device's scene BVH build
+    (oracle/sah_ref.cpp) on triangle records (n x 12 float32: v0, e1, e2 as
+    float4s): (nodes n-1 x 16 float32 words, leaf order, widened boxes)."""
+    import numpy as np
+    tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 12)
+    n = len(tri)
+    L = ctypes.CDLL(SAH_LIB_PATH)
+    L.upbp_sah_ref_build.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]
+    nodes = np.zeros((max(n - 1, 1), 16), np.float32)
+    order = np.zeros(n, np.uint32)
+    boxes = np.zeros((n, 6), np.float32)
+    L.upbp_sah_ref_build(tri.ctypes.data, n, nodes.ctypes.data, order.ctypes.data, boxes.ctypes.data)
+    return nodes[:max(n - 1, 0)], order, boxes

@@ -1,64 +1,42 @@
-"""Host binned-SAH build of the scene BVH (gpuupbp_b200/csrc/host/upbp_sah.cpp),
-compiled on its own with g++ and checked on random boxes: every primitive in
+"""The sequential statement of the device's scene BVH build
+(oracle/sah_ref.cpp, the checker the GPU build is compared with bit for bit
+in tests/test_scene_bvh_gpu.py), on random triangles: every primitive in
 exactly one leaf, every stored child box containing the boxes of its
 subtree, node slots as documented (a subtree of m primitives in m - 1
 consecutive slots), depth within the device walks' stack."""
 import os
-import shutil
 import subprocess
+import sys
 
 import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SRC = os.path.join(ROOT, "gpuupbp_b200", "csrc", "host", "upbp_sah.cpp")
-
-HARNESS = r"""
-#include <cstdio>
-#include <vector>
-#include "upbp_sah.h"
-int main(int argc, char** argv) {
-    FILE* f = fopen(argv[1], "rb");
-    unsigned n; if (fread(&n, 4, 1, f) != 1) return 2;
-    std::vector<float> boxes(6 * (size_t)n);
-    if (fread(boxes.data(), 4, boxes.size(), f) != boxes.size()) return 2;
-    fclose(f);
-    std::vector<float> nodes(16 * (size_t)(n - 1));
-    std::vector<unsigned> order(n);
-    upbp_host::sah_build(boxes.data(), n, nodes.data(), order.data(), 4);
-    FILE* o = fopen(argv[2], "wb");
-    fwrite(nodes.data(), 4, nodes.size(), o);
-    fwrite(order.data(), 4, order.size(), o);
-    fclose(o);
-    return 0;
-}
-"""
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 
 @pytest.fixture(scope="module")
-def harness(tmp_path_factory):
-    if shutil.which("g++") is None:
-        pytest.skip("g++ not available")
-    d = tmp_path_factory.mktemp("sah")
-    (d / "main.cpp").write_text(HARNESS)
-    exe = d / "sah"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-I", os.path.dirname(SRC), str(d / "main.cpp"), SRC,
-                    "-o", str(exe)], check=True)
-    return d, exe
+def sah():
+    import ref_cpu
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "sah", "-s"], check=True)
+    return ref_cpu.sah_build
 
 
-def run(harness, boxes):
-    d, exe = harness
-    n = len(boxes)
-    with open(d / "in.bin", "wb") as f:
-        f.write(np.uint32(n).tobytes())
-        f.write(boxes.astype(np.float32).tobytes())
-    subprocess.run([str(exe), str(d / "in.bin"), str(d / "out.bin")], check=True)
-    raw = np.fromfile(d / "out.bin", dtype=np.uint8)
-    nodes = raw[: 64 * (n - 1)].view(np.float32).reshape(n - 1, 16)
-    links = raw[: 64 * (n - 1)].view(np.int32).reshape(n - 1, 16)[:, 12:16]
-    order = raw[64 * (n - 1):].view(np.uint32)
-    return nodes, links, order
+def triangles(centres, size, rng):
+    """Triangle records (v0, e1, e2 as float4s) around the given centres."""
+    n = len(centres)
+    v = centres[:, None, :] + (rng.random((n, 3, 3)) - 0.5) * size
+    tri = np.zeros((n, 12), np.float32)
+    tri[:, 0:3] = v[:, 0]
+    tri[:, 4:7] = (v[:, 1].astype(np.float32) - v[:, 0].astype(np.float32))
+    tri[:, 8:11] = (v[:, 2].astype(np.float32) - v[:, 0].astype(np.float32))
+    return tri
+
+
+def run(sah, tri):
+    nodes, order, boxes = sah(tri)
+    links = nodes.view(np.int32)[:, 12:16] if len(nodes) else np.zeros((0, 4), np.int32)
+    return nodes, links, order, boxes
 
 
 def check_tree(boxes, nodes, links, order):
@@ -92,29 +70,28 @@ def check_tree(boxes, nodes, links, order):
 
 
 @pytest.mark.parametrize("n,seed", [(2, 0), (3, 1), (17, 2), (1000, 3), (20000, 4)])
-def test_sah_tree_is_valid(harness, n, seed):
+def test_sah_tree_is_valid(sah, n, seed):
     rng = np.random.default_rng(seed)
-    c = rng.random((n, 3)) * 10
-    ext = rng.random((n, 3)) * 0.2
-    boxes = np.concatenate([c - ext, c + ext], axis=1).astype(np.float32)
-    nodes, links, order = run(harness, boxes)
+    tri = triangles(rng.random((n, 3)) * 10, 0.4, rng)
+    nodes, links, order, boxes = run(sah, tri)
     check_tree(boxes, nodes, links, order)
 
 
-def test_sah_tolerates_nan_boxes(harness):
-    """A NaN box (a malformed vertex) still lands in exactly one leaf."""
+def test_sah_tolerates_nan_triangles(sah):
+    """A NaN vertex (a malformed triangle) still lands in exactly one leaf."""
     rng = np.random.default_rng(5)
     n = 200
-    c = rng.random((n, 3)) * 4
-    boxes = np.concatenate([c - 0.05, c + 0.05], axis=1).astype(np.float32)
-    boxes[[3, 77]] = np.nan
-    nodes, links, order = run(harness, boxes)
+    tri = triangles(rng.random((n, 3)) * 4, 0.1, rng)
+    tri[[3, 77], 0] = np.nan
+    nodes, links, order, boxes = run(sah, tri)
     assert sorted(order.tolist()) == list(range(n))
 
 
-def test_sah_coincident_centroids(harness):
+def test_sah_coincident_centroids(sah):
     """All centroids equal: the builder falls back to middle splits."""
     n = 300
-    boxes = np.tile(np.array([[0, 0, 0, 1, 1, 1]], np.float32), (n, 1))
-    nodes, links, order = run(harness, boxes)
+    tri = np.tile(np.array([[0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0]], np.float32), (n, 1))
+    nodes, links, order, boxes = run(sah, tri)
     assert check_tree(boxes, nodes, links, order) <= 10
+    # the middle split of a stable order keeps the input order
+    assert order.tolist() == list(range(n))
