@@ -64,6 +64,8 @@ void print_usage(const char* prog)
                 "                 the first n iterations\n");
     std::printf("    -mis_exact   (this build only) MIS weights of the full-path balance heuristic where the\n"
                 "                 reference's recursion departs from it (photon-beam distances, NEE through media)\n");
+    std::printf("    -checkpoint <file>  (this build only) write the render's state after the last iteration and\n"
+                "                 at every continuous output;  -resume <file>  continue a render from one\n");
 }
 
 }  // namespace
@@ -291,6 +293,13 @@ extern "C" int upbp_parse_command_line(int argc, const char** argv, upbp_config*
                 if (end == v || n < 0) return fail("invalid argument of -guide option");
                 c.guide_train_iterations = (int)n;
                 extra << "_guide" << n;
+            } else if (a == "-checkpoint" || a == "-resume") {
+                // not in the reference: checkpoint / resume of a render
+                const char* v = need(a.c_str());
+                if (!v) return fail("missing argument of " + a + " option");
+                if (std::strlen(v) >= sizeof(c.checkpoint_path)) return fail("path too long for " + a);
+                std::snprintf(a == "-checkpoint" ? c.checkpoint_path : c.resume_path, sizeof(c.checkpoint_path),
+                              "%s", v);
             } else if (a == "-mis_exact") {
                 // not in the reference: full-path balance-heuristic weights
                 // where the reference's recursion departs from them

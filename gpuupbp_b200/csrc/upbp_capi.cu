@@ -76,6 +76,7 @@ class DeviceGuard {
 // may exist, and up to kParamSlots of them run at once -- a further call
 // waits for a slot.
 constexpr int kMaxDevices = 64;
+constexpr int kAssertCounts = 7;  // -assert: failed assertions + the six UPBP_STATUS_* bits
 struct SlotTable {
     std::mutex mu;
     std::condition_variable freed;
@@ -283,6 +284,8 @@ struct upbp_ctx {
     unsigned hit_capacity = 0;
     size_t hit_want = 0;  // list size the last growth asked for (the pool's best fit)
     double ms_scene_bvh = 0;  // device time of the scene BVH builds in upbp_create
+    uint64_t render_hash = 0;  // configuration + scene fingerprint a checkpoint must match
+    unsigned* d_assert = nullptr;  // -assert: event counts (assertions, then one per status bit)
     size_t max_hits = 0;  // largest list: kMaxHits, or UPBP_MAX_HITS entries when that is smaller
     HitState* d_hit_state = nullptr;
     HitState h_hit_state = {};
@@ -484,6 +487,65 @@ int upload_env_map(upbp_ctx* c, const upbp_scene_desc* s)
     m.nv = nv;
     m.norm = .5f * 0.318309886183790671538f * 0.318309886183790671538f;
     return UPBP_OK;
+}
+
+// Fingerprint of everything that decides a render's images: the
+// configuration's render fields and the scene's records (FNV-1a over 8-byte
+// words).  A checkpoint loads only into a context with the same one.
+uint64_t hash_bytes(uint64_t h, const void* p, size_t bytes)
+{
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    size_t i = 0;
+    for (; i + 8 <= bytes; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, b + i, 8);
+        h = (h ^ w) * 0x100000001b3ull;
+    }
+    for (; i < bytes; i++) h = (h ^ b[i]) * 0x100000001b3ull;
+    return h;
+}
+
+template <class T>
+uint64_t hash_value(uint64_t h, const T& v)
+{
+    return hash_bytes(h, &v, sizeof(v));
+}
+
+uint64_t render_fingerprint(const upbp_scene_desc* s, const upbp_config* c)
+{
+    uint64_t h = 0xcbf29ce484222325ull;
+    const float radii[11] = {c->bb1d_radius_initial, c->bb1d_radius_alpha, c->bb1d_used_light_subpath_count,
+                             c->bp2d_radius_initial, c->bp2d_radius_alpha, c->pb2d_radius_initial,
+                             c->pb2d_radius_alpha,  c->pp3d_radius_initial, c->pp3d_radius_alpha,
+                             c->surf_radius_initial, c->surf_radius_alpha};
+    const int64_t ints[14] = {c->scene_id, c->algorithm_flags, c->res_x, c->res_y, c->max_path_length,
+                              c->min_path_length, c->query_beam_type, c->photon_beam_type,
+                              c->ignore_fully_spec_paths, (int64_t)c->iteration_offset, c->use_shading_normal,
+                              c->mis_exact, c->guide_train_iterations, 0};
+    h = hash_value(h, radii);
+    h = hash_value(h, ints);
+    h = hash_value(h, c->path_count_per_iter);
+    const size_t n = s->triangle_count;
+    h = hash_value(h, s->triangle_count);
+    h = hash_bytes(h, s->verts, 9 * n * sizeof(float));
+    h = hash_bytes(h, s->normals, 12 * n * sizeof(float));
+    h = hash_bytes(h, s->tri_material, n * sizeof(int32_t));
+    h = hash_bytes(h, s->tri_light, n * sizeof(int32_t));
+    h = hash_bytes(h, s->materials, s->material_count * sizeof(upbp_material));
+    h = hash_bytes(h, s->media, s->medium_count * sizeof(upbp_medium));
+    h = hash_bytes(h, s->lights, s->light_count * sizeof(upbp_light));
+    h = hash_value(h, s->camera);
+    h = hash_value(h, s->global_medium);
+    h = hash_value(h, s->background_light);
+    h = hash_value(h, s->sphere_count);
+    if (s->sphere_count) {
+        h = hash_bytes(h, s->spheres, 4 * (size_t)s->sphere_count * sizeof(float));
+        h = hash_bytes(h, s->sph_material, s->sphere_count * sizeof(int32_t));
+    }
+    h = hash_value(h, s->env_width);
+    h = hash_value(h, s->env_height);
+    if (s->env_rgb) h = hash_bytes(h, s->env_rgb, 3 * (size_t)s->env_width * s->env_height * sizeof(float));
+    return h;
 }
 
 // Static scene: the binned-SAH tree of one class of triangles (original
@@ -893,6 +955,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         upbp_ctx* c = new upbp_ctx();
         c->cfg = *cfg;
         c->dev = dev;
+        c->render_hash = render_fingerprint(s, cfg);
         {
             std::lock_guard<std::mutex> lk(g_hit_pool[dev].mu);
             g_hit_pool[dev].contexts++;
@@ -1068,6 +1131,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         UPBP_CK(dalloc(&c->d_fb, npx));
         UPBP_CK(dalloc(&c->d_acc, npx));
         UPBP_CK(dalloc(&c->d_status, 1));
+        if (cfg->gpu_assert) UPBP_CK(dalloc(&c->d_assert, kAssertCounts));
         UPBP_CK(dalloc(&c->d_work, (size_t)kKernRows * kCtrCount));
         UPBP_CK(dalloc(&c->d_qcount, 8));
         UPBP_CK(dalloc(&c->d_hit_state, 1));
@@ -1136,6 +1200,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         P.beams = c->d_beams;
         P.framebuffer = c->d_fb;
         P.status = c->d_status;
+        P.assert_counts = c->d_assert;
         P.seg_queue = c->d_seg_queue;
         P.seg_capacity = c->seg_capacity;
         P.pt_queue = c->d_pt_queue;
@@ -1230,6 +1295,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         UPBP_CK(cudaMemsetAsync(c->d_fb, 0, npx * sizeof(float), c->st));
         UPBP_CK(cudaMemsetAsync(c->d_work, 0, (size_t)kKernCount * kCtrCount * sizeof(unsigned long long), c->st));
         UPBP_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->st));  // this iteration's status bits
+        if (c->d_assert) UPBP_CK(cudaMemsetAsync(c->d_assert, 0, kAssertCounts * sizeof(unsigned), c->st));
         unsigned launches = 0;
         size_t h2d = 0, d2h = 0;  // host<->device bytes of this iteration
         P.work = c->d_work;
@@ -1624,6 +1690,20 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         c->iterations++;
         c->ev_pending = std::min(c->ev_pending + 1, (unsigned)kEventRing);
         c->status_seen |= *c->h_status;
+        if (c->d_assert) {
+            // -assert: the reference's exception program prints a line per
+            // event (kernel/exception.cu:27-52); here one per kind, counted
+            static const char* const what[kAssertCounts] = {
+                "assertion failed", "boundary_stack too small", "intersection_array too small",
+                "vol_segment_array or vol_lite_segment_array too small", "intersection_stack too small",
+                "beam buffer too small", "traversal stack too small"};
+            unsigned counts[kAssertCounts];
+            UPBP_CK(cudaMemcpy(counts, c->d_assert, sizeof(counts), cudaMemcpyDeviceToHost));
+            for (int k = 0; k < kAssertCounts; k++)
+                if (counts[k])
+                    std::fprintf(stderr, "[ 5][            USER]: %s (%u times in iteration %d)\n", what[k], counts[k],
+                                 iteration);
+        }
         if (guide_training) gs.front = gs.front_next;
         return (int)*c->h_status;
     });
@@ -1990,6 +2070,157 @@ extern "C" int upbp_guide_gradients(const float* params, uint32_t n_params, cons
     });
 }
 
+// ---------------------------------------------------------------- checkpoints
+//
+// File: "UPBPCKP1", u32 version 1, u64 render fingerprint, u32 iterations
+// rendered, u32 status bits seen, u32 width, u32 height, then width x height
+// x 3 doubles of the accumulation; then i32 1 if the learned proposal's
+// state follows: i32 Adam steps, i32 table in use (-1 none), f32 last loss,
+// u32 training records, kGuideParams floats each of the parameters and the
+// two Adam moments, the records (8 floats each).  Little-endian, as the
+// machines that write and read them.
+namespace {
+constexpr char kCkptMagic[8] = {'U', 'P', 'B', 'P', 'C', 'K', 'P', '1'};
+
+struct FileCloser {
+    FILE* f;
+    ~FileCloser()
+    {
+        if (f) std::fclose(f);
+    }
+};
+}  // namespace
+
+extern "C" int upbp_save_checkpoint(upbp_ctx* c, const char* path)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !path) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        const size_t n = (size_t)c->P.screen_pixel_count * 3;
+        std::vector<double> acc(n);
+        UPBP_CK(cudaMemcpy(acc.data(), c->d_acc, n * sizeof(double), cudaMemcpyDeviceToHost));
+        const GuideState& g = c->guide;
+        const int32_t has_guide = g.net.w32 ? 1 : 0;
+        std::vector<float> w, m, v;
+        std::vector<GuideRecord> recs;
+        unsigned nrec = 0;
+        if (has_guide) {
+            w.resize(kGuideParams);
+            m.resize(kGuideParams);
+            v.resize(kGuideParams);
+            UPBP_CK(cudaMemcpy(w.data(), g.net.w32, kGuideParams * sizeof(float), cudaMemcpyDeviceToHost));
+            UPBP_CK(cudaMemcpy(m.data(), g.net.m, kGuideParams * sizeof(float), cudaMemcpyDeviceToHost));
+            UPBP_CK(cudaMemcpy(v.data(), g.net.v, kGuideParams * sizeof(float), cudaMemcpyDeviceToHost));
+            UPBP_CK(cudaMemcpy(&nrec, g.rec_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+            nrec = std::min(nrec, g.rec_capacity);
+            recs.resize(nrec);
+            if (nrec)
+                UPBP_CK(cudaMemcpy(recs.data(), g.recs, nrec * sizeof(GuideRecord), cudaMemcpyDeviceToHost));
+        }
+        FileCloser fc{std::fopen(path, "wb")};
+        if (!fc.f) {
+            upbp_host::set_error(std::string("cannot write ") + path);
+            return UPBP_ERR_IO;
+        }
+        const uint32_t head[5] = {1u, c->iterations, c->status_seen, c->cfg.res_x, c->cfg.res_y};
+        bool ok = std::fwrite(kCkptMagic, 1, 8, fc.f) == 8 && std::fwrite(head, 4, 1, fc.f) == 1 &&
+                  std::fwrite(&c->render_hash, 8, 1, fc.f) == 1 && std::fwrite(head + 1, 4, 4, fc.f) == 4 &&
+                  std::fwrite(acc.data(), sizeof(double), n, fc.f) == n && std::fwrite(&has_guide, 4, 1, fc.f) == 1;
+        if (ok && has_guide) {
+            const int32_t gi[2] = {g.net.steps, g.front};
+            ok = std::fwrite(gi, 4, 2, fc.f) == 2 && std::fwrite(&g.last_loss, 4, 1, fc.f) == 1 &&
+                 std::fwrite(&nrec, 4, 1, fc.f) == 1 &&
+                 std::fwrite(w.data(), 4, kGuideParams, fc.f) == (size_t)kGuideParams &&
+                 std::fwrite(m.data(), 4, kGuideParams, fc.f) == (size_t)kGuideParams &&
+                 std::fwrite(v.data(), 4, kGuideParams, fc.f) == (size_t)kGuideParams &&
+                 std::fwrite(recs.data(), sizeof(GuideRecord), nrec, fc.f) == nrec;
+        }
+        if (!ok) {
+            upbp_host::set_error(std::string("short write to ") + path);
+            return UPBP_ERR_IO;
+        }
+        return UPBP_OK;
+    });
+}
+
+extern "C" int upbp_load_checkpoint(upbp_ctx* c, const char* path)
+{
+    return upbp_host::abi_guard([&]() -> int {
+        if (!c || !path) return UPBP_ERR_ARGS;
+        DeviceGuard dg(c->dev);
+        UPBP_CK(dg.error());
+        FileCloser fc{std::fopen(path, "rb")};
+        if (!fc.f) {
+            upbp_host::set_error(std::string("cannot read ") + path);
+            return UPBP_ERR_IO;
+        }
+        auto bad = [&](const std::string& why) {
+            upbp_host::set_error(std::string(path) + ": " + why);
+            return UPBP_ERR_ARGS;
+        };
+        char magic[8];
+        uint32_t version = 0, head[4];
+        uint64_t hash = 0;
+        if (std::fread(magic, 1, 8, fc.f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return bad("not a checkpoint");
+        if (std::fread(&version, 4, 1, fc.f) != 1 || version != 1) return bad("unknown checkpoint version");
+        if (std::fread(&hash, 8, 1, fc.f) != 1 || std::fread(head, 4, 4, fc.f) != 4) return bad("truncated header");
+        if (hash != c->render_hash)
+            return bad("written by a render of another scene or configuration (fingerprint differs)");
+        if (head[2] != c->cfg.res_x || head[3] != c->cfg.res_y) return bad("resolution differs");
+        const size_t n = (size_t)c->P.screen_pixel_count * 3;
+        std::vector<double> acc(n);
+        int32_t has_guide = 0;
+        if (std::fread(acc.data(), sizeof(double), n, fc.f) != n || std::fread(&has_guide, 4, 1, fc.f) != 1)
+            return bad("truncated accumulation");
+        GuideState& g = c->guide;
+        if ((has_guide != 0) != (g.net.w32 != nullptr)) return bad("learned-proposal state does not match");
+        std::vector<float> w, m, v;
+        std::vector<GuideRecord> recs;
+        int32_t gi[2] = {0, -1};
+        float last_loss = 0.f;
+        unsigned nrec = 0;
+        if (has_guide) {
+            w.resize(kGuideParams);
+            m.resize(kGuideParams);
+            v.resize(kGuideParams);
+            if (std::fread(gi, 4, 2, fc.f) != 2 || std::fread(&last_loss, 4, 1, fc.f) != 1 ||
+                std::fread(&nrec, 4, 1, fc.f) != 1 || nrec > g.rec_capacity ||
+                std::fread(w.data(), 4, kGuideParams, fc.f) != (size_t)kGuideParams ||
+                std::fread(m.data(), 4, kGuideParams, fc.f) != (size_t)kGuideParams ||
+                std::fread(v.data(), 4, kGuideParams, fc.f) != (size_t)kGuideParams)
+                return bad("truncated learned-proposal state");
+            recs.resize(nrec);
+            if (std::fread(recs.data(), sizeof(GuideRecord), nrec, fc.f) != nrec) return bad("truncated records");
+        }
+        UPBP_CK(cudaStreamSynchronize(c->st));
+        UPBP_CK(cudaMemcpy(c->d_acc, acc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+        if (has_guide) {
+            UPBP_CK(guide_set_params(g.net, w.data(), c->st));
+            UPBP_CK(cudaMemcpy(g.net.m, m.data(), kGuideParams * sizeof(float), cudaMemcpyHostToDevice));
+            UPBP_CK(cudaMemcpy(g.net.v, v.data(), kGuideParams * sizeof(float), cudaMemcpyHostToDevice));
+            g.net.steps = gi[0];
+            g.last_loss = last_loss;
+            UPBP_CK(cudaMemcpy(g.rec_count, &nrec, sizeof(unsigned), cudaMemcpyHostToDevice));
+            if (nrec) UPBP_CK(cudaMemcpy(g.recs, recs.data(), nrec * sizeof(GuideRecord), cudaMemcpyHostToDevice));
+            g.front = -1;
+            g.front_next = -1;
+            if (gi[1] >= 0) {
+                // the table in use is the bake of the network as saved
+                UPBP_CK(guide_fill_table(c->st, g, g.table[0]));
+                UPBP_CK(cudaStreamSynchronize(c->st));
+                g.front = 0;
+                g.front_next = 0;
+            }
+        }
+        c->iterations = head[0];
+        c->status_seen = head[1];
+        c->ev_pending = 0;
+        return UPBP_OK;
+    });
+}
+
 extern "C" int upbp_set_grid_limit(upbp_ctx* c, uint32_t max_blocks)
 {
     if (!c) return UPBP_ERR_ARGS;
@@ -2082,7 +2313,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     DeviceGuard dg(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->h_status) cudaFreeHost(c->h_status);
-    void* bufs[] = {c->mis.light, c->mis.camera, c->mis.events, c->mis.event_count, c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
+    void* bufs[] = {c->d_assert, c->mis.light, c->mis.camera, c->mis.events, c->mis.event_count, c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,
                     c->d_counters, c->d_idx_s, c->d_idx_m, c->d_beams, c->d_fb, c->d_acc, c->d_status,

@@ -372,6 +372,7 @@ struct DeviceParams {
     unsigned beam_capacity;
     float* framebuffer;               // W*H*3
     unsigned* status;
+    unsigned* assert_counts;  // -assert: failed assertions, then one count per status bit; null without it
     unsigned long long* work;         // kCtrCount counters of the running pass
 
     // photon maps built after the light pass

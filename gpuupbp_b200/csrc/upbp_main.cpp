@@ -85,14 +85,31 @@ int main(int argc, const char** argv)
         upbp_scene_free(scene);
         return 1;
     }
+    int start = 0;  // iterations rendered before this run (a resumed checkpoint's)
+    if (cfg.resume_path[0]) {
+        if (upbp_load_checkpoint(ctx, cfg.resume_path) != UPBP_OK) {
+            std::fprintf(stderr, "resume: %s\n", upbp_last_error());
+            upbp_destroy(ctx);
+            upbp_scene_free(scene);
+            return 1;
+        }
+        upbp_stats st;
+        if (upbp_get_stats(ctx, &st) == UPBP_OK) start = (int)st.iterations_done;
+        std::printf("Resumed:  %d iteration(s) from %s\n", start, cfg.resume_path);
+    }
+    auto checkpoint = [&]() {
+        if (cfg.checkpoint_path[0] && upbp_save_checkpoint(ctx, cfg.checkpoint_path) != UPBP_OK)
+            std::fprintf(stderr, "checkpoint: %s\n", upbp_last_error());
+    };
     const uint32_t w = cfg.res_x, h = cfg.res_y;
     const std::string out = cfg.output_name;
     const std::string stem = out.substr(0, out.size() - 4), ext = out.substr(out.size() - 3);
     CsvLog log(cfg.do_log != 0);
     auto t0 = std::chrono::steady_clock::now();
-    int iter = 0;
+    int iter = start;
     auto continuous = [&](int done) {
         if (cfg.continuous_output > 0 && done % cfg.continuous_output == 0) {
+            checkpoint();
             std::vector<float> img((size_t)w * h * 3, 0.f);
             upbp_accumulate_to_host(ctx, img.data(), 1.0 / done);
             char name[2048];
@@ -111,7 +128,7 @@ int main(int argc, const char** argv)
         }
     } else {
         int percent = -1;
-        for (iter = 0; iter < cfg.iteration_count; iter++) {
+        for (iter = start; iter < cfg.iteration_count; iter++) {
             if (upbp_run_iteration(ctx, iter) < 0) {  // > 0: status bits, the image is complete
                 std::fprintf(stderr, "iteration %d: %s\n", iter, upbp_last_error());
                 break;
@@ -125,6 +142,7 @@ int main(int argc, const char** argv)
             continuous(iter + 1);
         }
     }
+    checkpoint();
     std::vector<float> img((size_t)w * h * 3, 0.f);
     upbp_accumulate_to_host(ctx, img.data(), iter > 0 ? 1.0 / iter : 0.0);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -60,6 +60,7 @@ UPBP_D unsigned sample_scattering(bool& cont, const Bsdf& bsdf, float3 hitpoint,
         cont = false;
         return 0;
     }
+    check_assert(for_pdf > 0.f);  // functs_shared.cuh:56
     const bool specular = (ev & (kEvReflect | kEvRefract)) != 0;
     float rev_pdf = for_pdf;
     if (!specular) rev_pdf = bsdf_pdf(bsdf, s.dir, true);

@@ -99,7 +99,22 @@ UPBP_D int boundary_priority(int mat) { return mat >= 0 ? c_params.materials[mat
 
 UPBP_D bool is_real_material(int mat) { return mat >= 0 && c_params.materials[mat].real; }
 
-UPBP_D void flag_status(unsigned bits) { atomicOr(c_params.status, bits); }
+// Sets an iteration's status bits; with -assert also counts the event under
+// its lowest bit (the reference's exception program prints one line per
+// such event, kernel/exception.cu:27-52).
+UPBP_D void flag_status(unsigned bits)
+{
+    atomicOr(c_params.status, bits);
+    if (c_params.assert_counts && bits) atomicAdd(&c_params.assert_counts[__ffs(bits)], 1u);
+}
+
+// The reference's GPU_ASSERT (kernel/defs.cuh:90-96) with -assert: counts a
+// failed condition.  The reference's exception also ends the launch index;
+// here the path goes on, so the images with and without -assert agree.
+UPBP_D void check_assert(bool cond)
+{
+    if (!cond && c_params.assert_counts) atomicAdd(&c_params.assert_counts[0], 1u);
+}
 
 // A sphere normal component as the reference's closest-hit and any-hit
 // programs read it back from the hit attributes (intersector.cu:130-132): the

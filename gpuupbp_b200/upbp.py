@@ -46,6 +46,7 @@ class Config(ctypes.Structure):
         ("continuous_output", ctypes.c_int), ("ignore_fully_spec_paths", ctypes.c_int), ("gpu_assert", ctypes.c_int),
         ("iteration_offset", ctypes.c_uint64), ("do_log", ctypes.c_int), ("use_shading_normal", ctypes.c_int),
         ("mis_exact", ctypes.c_int), ("guide_train_iterations", ctypes.c_int),
+        ("checkpoint_path", ctypes.c_char * 1024), ("resume_path", ctypes.c_char * 1024),
     ]
 
 
@@ -120,7 +121,7 @@ EXPORTS = ["upbp_parse_command_line", "upbp_scene_load_obj", "upbp_scene_load_pr
            "upbp_write_image", "upbp_get_stream", "upbp_last_error",
            "upbp_debug_photons", "upbp_debug_query", "upbp_debug_query_static", "upbp_get_device",
            "upbp_debug_mis_records", "upbp_guide_info", "upbp_guide_gradients", "upbp_run_batch",
-           "upbp_set_grid_limit", "upbp_debug_scene_bvh"]
+           "upbp_set_grid_limit", "upbp_debug_scene_bvh", "upbp_save_checkpoint", "upbp_load_checkpoint"]
 
 _libs = {}
 
@@ -164,6 +165,8 @@ def load_library(path: str = LIB_PATH):
     L.upbp_debug_query_static.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint32, VP, VP, ctypes.c_uint32]
     L.upbp_debug_scene_bvh.argtypes = [VP, ctypes.c_int, VP, ctypes.c_uint64, VP, ctypes.c_uint64,
                                        P(ctypes.c_uint32)]
+    L.upbp_save_checkpoint.argtypes = [VP, ctypes.c_char_p]
+    L.upbp_load_checkpoint.argtypes = [VP, ctypes.c_char_p]
     _libs[path] = L
     return L
 
@@ -287,6 +290,18 @@ class Renderer:
         out["work"] = {k: dict(zip(WORK_NAMES, list(st.work[i]))) for i, k in enumerate(KERNELS)}
         out["ms_kernel_sum"] = dict(zip(KERNELS, list(st.ms_kernel_sum)))
         return out
+
+    def save_checkpoint(self, path: str):
+        """Writes the render's state (upbp_save_checkpoint)."""
+        _check(self._L.upbp_save_checkpoint(self._ctx, path.encode()), "save_checkpoint")
+
+    def load_checkpoint(self, path: str) -> int:
+        """Restores a render's state written by save_checkpoint for the same
+        scene and configuration; returns the iterations it had rendered (the
+        index to continue with)."""
+        _check(self._L.upbp_load_checkpoint(self._ctx, path.encode()), "load_checkpoint")
+        self.iterations = self.stats()["iterations_done"]
+        return self.iterations
 
     def scene_bvh(self, real: bool):
         """The device-built scene BVH of one class of triangles

@@ -111,6 +111,12 @@ typedef struct upbp_config {
      * from iteration 1 on; its pdf enters every camera-direction pdf of the
      * MIS recursion.  0 (the default): the plain method. */
     int guide_train_iterations;
+    /* Not in the reference (command line -checkpoint <file>, -resume <file>):
+     * the executable writes a checkpoint (upbp_save_checkpoint) after its
+     * last iteration and at every continuous output, and resumes from one
+     * (upbp_load_checkpoint) before its first; empty: none. */
+    char checkpoint_path[1024];
+    char resume_path[1024];
 } upbp_config;
 
 /* ------------------------------------------------------ scene records */
@@ -393,6 +399,20 @@ int upbp_guide_gradients(const float* params, uint32_t n_params, const float* x,
  * autotuner in gpuupbp_b200/batch.py picks workers and the cap by timing. */
 int upbp_run_batch(upbp_ctx* const* ctxs, uint32_t n, int iteration, int workers);
 int upbp_set_grid_limit(upbp_ctx* ctx, uint32_t max_blocks);
+
+/* Checkpoints (not in the reference, which has none): upbp_save_checkpoint
+ * writes the context's FP64 accumulation, the number of iterations it has
+ * rendered, the status bits seen and, with a learned proposal, its network,
+ * Adam state, training records and whether a table is in use, with a
+ * fingerprint of the configuration and scene; upbp_load_checkpoint restores
+ * them into a context created from the same scene and configuration
+ * (UPBP_ERR_ARGS with the reason otherwise, UPBP_ERR_IO if the file cannot
+ * be read or written).  Random numbers and radii depend only on the
+ * iteration index, so a caller that continues with iteration index =
+ * iterations rendered (upbp_stats.iterations_done) renders what the
+ * uninterrupted run would have, up to the order of float additions. */
+int upbp_save_checkpoint(upbp_ctx* ctx, const char* path);
+int upbp_load_checkpoint(upbp_ctx* ctx, const char* path);
 
 /* The CUDA stream (cudaStream_t) all of a context's work is issued on, so a
  * caller can order its own work or time the library with events. */

@@ -220,3 +220,14 @@ def test_hdr_writer_bytes(tmp_path):
 def test_image_writer_refuses_unknown_extension(tmp_path):
     with pytest.raises(upbp.UpbpError):
         upbp.write_image(str(tmp_path / "x.png"), np.zeros((2, 2, 3), np.float32))
+
+
+def test_checkpoint_flags_parse():
+    """-checkpoint / -resume (not in the reference) fill the configuration's
+    paths and leave the output name alone."""
+    from gpuupbp_b200 import upbp
+    c = upbp.parse_command_line(["-s", "2", "-checkpoint", "/tmp/a.ckpt", "-resume", "/tmp/b.ckpt"])
+    assert c.checkpoint_path == b"/tmp/a.ckpt" and c.resume_path == b"/tmp/b.ckpt"
+    assert b"ckpt" not in c.output_name
+    with pytest.raises(Exception):
+        upbp.parse_command_line(["-s", "2", "-resume"])
