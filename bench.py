@@ -530,6 +530,51 @@ def run_guided_workload(args) -> dict:
                                       "flop_per_iteration": flop}}}
 
 
+def run_dense_quality_workload(args) -> dict:
+    """Config 5's guided form: the dense-beam enclosure (one thick medium,
+    sigma_s 5, g 0.9, 0.5M triangles, path length 16, beam radius 0.004 x
+    scene radius, BB1D over the beams of the first 600 000 light paths) with
+    all 2 073 600 light paths of the 1920x1080 workload on a 480x270 camera
+    (a bounded sample: 1/16 of the camera paths, the photon, beam and query
+    densities of the full case), the learned proposal (-guide 8) against the
+    plain method at equal device time, by relMSE against a converged plain
+    render of --ref-iterations iterations.  Also the plain method's query
+    throughput (segment + point queries per second) and the BB1D kernels'
+    algorithmic GB/s."""
+    import torch
+
+    from gpuupbp_b200 import quality, scenes, upbp
+    path = scenes.write_workload("dense_beams", SCENE_DIR)
+    plain = workload_args(path, (480, 270), "dense_beams") + ["-pcpi", str(1920 * 1080)]
+    guided = plain + ["-guide", "8"]
+    res = quality.equal_time(plain, guided, args.ref_iterations, args.method_iterations)
+    r = upbp.Renderer(plain)
+    stream = torch.cuda.ExternalStream(r.stream_handle())
+    for it in range(2):
+        r.run_iteration(it)
+    r.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for it in range(2, 6):
+        r.run_iteration(it)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 4
+    st = r.stats()
+    r.close()
+    kernels = kernel_rooflines(st, 480 * 270)
+    queries = st["segment_queries"] + st["point_queries"]
+    return {"metric": "equal-time relMSE ratio, plain / guided UPBP (config 5 sample)",
+            "value": res["relmse_ratio_plain_over_other"], "unit": "x", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": "dense_quality: dense_beams enclosure, 480x270 camera with the 1920x1080 "
+                                   f"light paths, path length 16, -guide 8, {args.method_iterations} guided "
+                                   f"iterations; reference {args.ref_iterations} plain iterations"},
+            "equal_time": res, "plain_ms_per_iteration": ms,
+            "queries_per_s": queries / (ms * 1e-3),
+            "bb1d_query": kernels["bb1d_query"], "bp2d_query": kernels["bp2d_query"]}
+
+
 def run_batch_quality_workload(args) -> dict:
     """Config 3's quality target: the guided, batched renderer against the
     plain single-scene renderer at equal wall time, by relMSE per job
@@ -562,12 +607,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS) + ["batch", "batch_quality", "guided"])
+    ap.add_argument("--workload", default="media_field", choices=sorted(WORKLOADS) + ["batch", "batch_quality", "dense_quality", "guided"])
     ap.add_argument("--ref-iterations", type=int, default=None,
                     help="iterations of the converged plain render the guided (default 4096) and batch_quality "
                          "(default 192) workloads compare with")
     ap.add_argument("--jobs", type=int, default=16, help="batch_quality: jobs of the seeded 64")
-    ap.add_argument("--method-iterations", type=int, default=24, help="batch_quality: guided batch iterations")
+    ap.add_argument("--method-iterations", type=int, default=None,
+                    help="guided iterations of batch_quality (default 24) and dense_quality (default 16)")
     ap.add_argument("--res", default=None,
                     help="image size WxH (default: the workload's); smaller sizes are for profiling captures, "
                          "not bench lines")
@@ -579,8 +625,14 @@ def main():
         args.ref_iterations = args.ref_iterations or 4096
         print(json.dumps(run_guided_workload(args)))
         return
+    if args.workload == "dense_quality":
+        args.ref_iterations = args.ref_iterations or 64
+        args.method_iterations = args.method_iterations or 16
+        print(json.dumps(run_dense_quality_workload(args)))
+        return
     if args.workload == "batch_quality":
         args.ref_iterations = args.ref_iterations or 192
+        args.method_iterations = args.method_iterations or 24
         print(json.dumps(run_batch_quality_workload(args)))
         return
     args.res = (tuple(int(v) for v in args.res.lower().split("x")) if args.res

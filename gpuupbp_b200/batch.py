@@ -63,13 +63,17 @@ class Batch:
 
 
 def autotune(batch: Batch, first_iteration: int, workers=(4, 8, 16, 32), limits=(0, 148 * 2)) -> dict:
-    """Times one batch iteration for every (workers, grid limit) pair and
-    keeps the fastest; the jobs one after another (one worker, no cap) is
-    always among the candidates, so the choice is never slower than that.
+    """Times one batch iteration for every (workers, grid limit) pair, after
+    one untimed iteration, and keeps the fastest; the jobs one after another
+    (one worker, no cap) is always among the candidates, so the choice is
+    never slower than that.
     The iterations rendered while tuning are real ones (first_iteration
     onward), so the caller continues after them.  Returns the choice, its
     timings and the next iteration index."""
     it = first_iteration
+    # one untimed iteration first: a job's first iteration grows its buffers
+    batch.run_iteration(it, max(workers))
+    it += 1
     timings = {}
     pairs = [(1, 0)] + [(w, lim) for lim in limits for w in workers if (w, lim) != (1, 0)]
     for w, lim in pairs:

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CXX = "/usr/bin/g++"   # system toolchain (dynamic libstdc++)
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompiler", "-fPIC", "-diag-suppress", "549,550"]
 
-DEVICE_SOURCES = ["upbp_capi.cu"]
+DEVICE_SOURCES = ["upbp_capi.cu", "upbp_slot0.cu"]
 HOST_SOURCES = ["host/upbp_cli.cpp", "host/upbp_scene.cpp", "host/upbp_predef.cpp", "host/upbp_exr.cpp",
                 "host/upbp_exr_read.cpp"]
 

@@ -20,6 +20,7 @@
 #include "upbp_camera_pass.cuh"
 #include "upbp_light_pass.cuh"
 #include "upbp_scene_bvh.cuh"
+#include "upbp_kernel_table.h"
 
 using namespace upbp;
 
@@ -330,6 +331,32 @@ unsigned cap_grid(const upbp_ctx* c, unsigned blocks)
     return c->grid_limit ? std::max(1u, std::min(blocks, c->grid_limit)) : blocks;
 }
 
+// This compilation's parameter-reading kernels (the indexed slot bank).
+const upbp_kernels::ParamKernels& slotted_kernels()
+{
+    static const upbp_kernels::ParamKernels k = {
+        light_pass_kernel,
+        camera_pass_kernel,
+        nee_connect_kernel,
+        bpt_connect_kernel,
+        k_resolve_camera,
+        {k_query_keys<false>, k_query_keys<true>},
+        {range_search_kernel<kModePb2d>, range_search_kernel<kModeBb1d>, range_search_kernel<kModeBp2d>},
+        {{range_eval_kernel<kModePb2d, false>, range_eval_kernel<kModePb2d, true>},
+         {range_eval_kernel<kModeBb1d, false>, range_eval_kernel<kModeBb1d, true>},
+         {range_eval_kernel<kModeBp2d, false>, range_eval_kernel<kModeBp2d, true>}},
+        {{point_merge_kernel<false, false>, point_merge_kernel<false, true>},
+         {point_merge_kernel<true, false>, point_merge_kernel<true, true>}},
+    };
+    return k;
+}
+
+// The kernels a call of context c launches: the fixed-bank copy on slot 0.
+const upbp_kernels::ParamKernels& PK(const upbp_ctx* c)
+{
+    return c->slot == 0 ? upbp_kernels::slot0_kernels() : slotted_kernels();
+}
+
 HitLease::HitLease(upbp_ctx* c) : c_(c)
 {
     // the smallest idle list that holds what the context's last iteration
@@ -365,8 +392,10 @@ HitLease::~HitLease()
 // before the launches that read them).
 cudaError_t upload_params(upbp_ctx* c)
 {
-    return cudaMemcpyToSymbolAsync(c_slots, &c->P, sizeof(DeviceParams), sizeof(DeviceParams) * (size_t)c->slot,
+    const cudaError_t e = cudaMemcpyToSymbolAsync(c_slots, &c->P, sizeof(DeviceParams), sizeof(DeviceParams) * (size_t)c->slot,
                                    cudaMemcpyHostToDevice, c->st);
+    if (e != cudaSuccess || c->slot != 0) return e;
+    return upbp_kernels::slot0_upload_params(&c->P, sizeof(DeviceParams), c->st);
 }
 
 void init_medium(DMedium& m, const upbp_medium& in)
@@ -822,9 +851,9 @@ int sort_queries(upbp_ctx* c, int q, unsigned n, const unsigned** order)
     if (ensure_sort(c, q, n) != UPBP_OK) return UPBP_ERR_CUDA;
     unsigned** b = c->d_sort[q];
     if (q == 0)
-        k_query_keys<true><<<(n + 255) / 256, 256, 0, c->st>>>(c->slot, n, b[0], b[2]);
+        PK(c).query_keys[1]<<<(n + 255) / 256, 256, 0, c->st>>>(c->slot, n, b[0], b[2]);
     else
-        k_query_keys<false><<<(n + 255) / 256, 256, 0, c->st>>>(c->slot, n, b[0], b[2]);
+        PK(c).query_keys[0]<<<(n + 255) / 256, 256, 0, c->st>>>(c->slot, n, b[0], b[2]);
     UPBP_CK(cudaGetLastError());
     cub::DoubleBuffer<unsigned> kb(b[0], b[1]), vb(b[2], b[3]);
     size_t tb = c->sort_temp_bytes;
@@ -1306,6 +1335,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             UPBP_CK(cudaMemsetAsync(m.camera, 0, (size_t)m.camera_paths * m.max_verts * kMisVtxWords * sizeof(float4), c->st));
             UPBP_CK(cudaMemsetAsync(m.event_count, 0, sizeof(unsigned), c->st));
             UPBP_CK(cudaMemcpyToSymbolAsync(c_misdbg, &m, sizeof(m), 0, cudaMemcpyHostToDevice, c->st));
+            UPBP_CK(upbp_kernels::slot0_upload_misdbg(&m, sizeof(m), c->st));
         }
 #endif
         GuideState& gs = c->guide;
@@ -1369,7 +1399,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             h2d += sizeof(P);
             UPBP_CK(upload_params(c));
             if (L > 0) {
-                light_pass_kernel<<<cap_grid(c, std::min<unsigned>(c->light_grid, (L + 127) / 128)), 128, 0, c->st>>>(
+                PK(c).light_pass<<<cap_grid(c, std::min<unsigned>(c->light_grid, (L + 127) / 128)), 128, 0, c->st>>>(
                     c->slot);
                 launches++;
             }
@@ -1489,7 +1519,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 UPBP_CK(upload_params(c));
                     UPBP_CK(cudaMemsetAsync(c->d_work + (size_t)kKernCameraExtend * kCtrCount, 0,
                                         kCtrCount * sizeof(unsigned long long), c->st));
-                camera_pass_kernel<<<cap_grid(c, std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128)),
+                PK(c).camera_pass<<<cap_grid(c, std::min<unsigned>(c->camera_grid, (P.screen_pixel_count + 127) / 128)),
                                      128, 0, c->st>>>(c->slot);
                 launches++;
                 UPBP_CK(cudaGetLastError());
@@ -1537,16 +1567,16 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         if (P.trace_camera_paths)
             UPBP_CK(cudaMemsetAsync(c->d_path_err, 0xff, P.screen_pixel_count * sizeof(unsigned), c->st));
         if (nnee > 0) {
-            nee_connect_kernel<<<grid_for(nnee), 128, 0, c->st>>>(c->slot);
+            PK(c).nee_connect<<<grid_for(nnee), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[4], c->st));
         if (nbpt > 0) {
-            bpt_connect_kernel<<<grid_for(nbpt), 128, 0, c->st>>>(c->slot);
+            PK(c).bpt_connect<<<grid_for(nbpt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         if (P.trace_camera_paths) {
-            k_resolve_camera<<<std::max(1u, std::min((nnee + nbpt + P.screen_pixel_count + 255) / 256, 148u * 32u)), 256, 0,
+            PK(c).resolve_camera<<<std::max(1u, std::min((nnee + nbpt + P.screen_pixel_count + 255) / 256, 148u * 32u)), 256, 0,
                                c->st>>>(c->slot);
             launches++;
         }
@@ -1600,9 +1630,9 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 UPBP_CK(upload_params(c));
                 const int g = (int)cap_grid(c, (unsigned)c->search_grid[mode]);
                 switch (mode) {
-                case kModePb2d: range_search_kernel<kModePb2d><<<g, 128, 0, c->st>>>(c->slot); break;
-                case kModeBb1d: range_search_kernel<kModeBb1d><<<g, 128, 0, c->st>>>(c->slot); break;
-                default: range_search_kernel<kModeBp2d><<<g, 128, 0, c->st>>>(c->slot); break;
+                case kModePb2d: PK(c).range_search[kModePb2d]<<<g, 128, 0, c->st>>>(c->slot); break;
+                case kModeBb1d: PK(c).range_search[kModeBb1d]<<<g, 128, 0, c->st>>>(c->slot); break;
+                default: PK(c).range_search[kModeBp2d]<<<g, 128, 0, c->st>>>(c->slot); break;
                 }
                 launches++;
                 UPBP_CK(cudaGetLastError());
@@ -1630,16 +1660,16 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                     const bool gd = P.guide.entries != nullptr;
                     switch (mode) {
                     case kModePb2d:
-                        if (gd) range_eval_kernel<kModePb2d, true><<<g2, 128, 0, c->st>>>(c->slot);
-                        else range_eval_kernel<kModePb2d, false><<<g2, 128, 0, c->st>>>(c->slot);
+                        if (gd) PK(c).range_eval[kModePb2d][1]<<<g2, 128, 0, c->st>>>(c->slot);
+                        else PK(c).range_eval[kModePb2d][0]<<<g2, 128, 0, c->st>>>(c->slot);
                         break;
                     case kModeBb1d:
-                        if (gd) range_eval_kernel<kModeBb1d, true><<<g2, 128, 0, c->st>>>(c->slot);
-                        else range_eval_kernel<kModeBb1d, false><<<g2, 128, 0, c->st>>>(c->slot);
+                        if (gd) PK(c).range_eval[kModeBb1d][1]<<<g2, 128, 0, c->st>>>(c->slot);
+                        else PK(c).range_eval[kModeBb1d][0]<<<g2, 128, 0, c->st>>>(c->slot);
                         break;
                     default:
-                        if (gd) range_eval_kernel<kModeBp2d, true><<<g2, 128, 0, c->st>>>(c->slot);
-                        else range_eval_kernel<kModeBp2d, false><<<g2, 128, 0, c->st>>>(c->slot);
+                        if (gd) PK(c).range_eval[kModeBp2d][1]<<<g2, 128, 0, c->st>>>(c->slot);
+                        else PK(c).range_eval[kModeBp2d][0]<<<g2, 128, 0, c->st>>>(c->slot);
                         break;
                     }
                     launches++;
@@ -1657,14 +1687,14 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
         };
         UPBP_CK(cudaEventRecord(ev[6], c->st));
         if (run_surf) {
-            if (P.guide.entries) point_merge_kernel<false, true><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
-            else point_merge_kernel<false, false><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            if (P.guide.entries) PK(c).point_merge[0][1]<<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            else PK(c).point_merge[0][0]<<<grid_for(npt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[7], c->st));
         if (run_pp3d) {
-            if (P.guide.entries) point_merge_kernel<true, true><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
-            else point_merge_kernel<true, false><<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            if (P.guide.entries) PK(c).point_merge[1][1]<<<grid_for(npt), 128, 0, c->st>>>(c->slot);
+            else PK(c).point_merge[1][0]<<<grid_for(npt), 128, 0, c->st>>>(c->slot);
             launches++;
         }
         UPBP_CK(cudaEventRecord(ev[8], c->st));

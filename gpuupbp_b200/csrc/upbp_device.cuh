@@ -441,11 +441,23 @@ UPBP_HD unsigned event_key(unsigned bounce, unsigned step) { return bounce * 256
 // it in shared memory at entry; device code names the running kernel's
 // parameters c_params.  Contexts therefore run concurrently, each on its own
 // slot and stream.
+//
+// The hot kernels are also compiled a second time (upbp_slot0.cu, its own
+// namespace) against a bank of one fixed slot: reading c_slots[s_slot] is
+// a constant-bank load of its own at every access, reading a fixed bank an
+// operand of the instruction that uses it (3% of an iteration).  Slot 0 --
+// the slot of a context running alone -- launches that copy; its
+// parameters are uploaded to both banks.
 constexpr int kParamSlots = 48;
-__constant__ DeviceParams c_slots[kParamSlots];
 __shared__ int s_slot;
 __shared__ int s_kernel_kind;
+#ifdef UPBP_SLOT0_BANK
+__constant__ DeviceParams c_slot0;
+#define c_params (c_slot0)
+#else
+__constant__ DeviceParams c_slots[kParamSlots];
 #define c_params (c_slots[s_slot])
+#endif
 
 // Records the running kernel's parameter slot and kind (for its work
 // counters); every thread of the block calls it first, before any early

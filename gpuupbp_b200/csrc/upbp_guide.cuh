@@ -66,28 +66,39 @@ constexpr int kGuideEntryWords = kGuideLobes + 4;  // float4s
 
 // ---------------------------------------------------------------- encoding
 
-// Frequency encoding of a position normalised to the scene box: sin and
-// cos of 2^b pi x for b = 0..11 per axis, then the direction of travel, then
-// the medium's one-hot.
-UPBP_HD void guide_encode(float3 xn, float3 d, int medium, float* out)
+// Frequency encoding of a position normalised to the scene box, the
+// direction of travel and the medium's one-hot, in two halves of 48 inputs
+// (the fused kernels give each half to its own thread): half 0 holds sin and
+// cos of 2^b pi x and 2^b pi y for b = 0..11, half 1 those of z, then the
+// direction, the one-hot of the medium slot and a zero pad.  sincospif takes
+// the scaled coordinate exactly (a power-of-two multiple).
+constexpr int kGuideHalf = kGuideInPad / 2;
+
+UPBP_D void guide_bands(float x, float* out)
 {
-    const float c[3] = {xn.x, xn.y, xn.z};
-    int k = 0;
-    for (int a = 0; a < 3; a++) {
-        float f = 3.14159265358979f;
-        for (int b = 0; b < kGuideBands; b++) {
-            const float t = f * c[a];
-            out[k++] = sinf(t);
-            out[k++] = cosf(t);
-            f *= 2.f;
-        }
+#pragma unroll
+    for (int b = 0; b < kGuideBands; b++) {
+        sincospif(x, &out[2 * b], &out[2 * b + 1]);
+        x *= 2.f;
     }
-    out[k++] = d.x;
-    out[k++] = d.y;
-    out[k++] = d.z;
-    for (int m = 0; m < kGuideMedia; m++) out[k++] = (m == medium) ? 1.f : 0.f;
-    while (k < kGuideInPad) out[k++] = 0.f;
 }
+
+UPBP_D void guide_encode_half(float3 xn, float3 d, int medium, int half, float* out)
+{
+    if (half == 0) {
+        guide_bands(xn.x, out);
+        guide_bands(xn.y, out + 2 * kGuideBands);
+    } else {
+        guide_bands(xn.z, out);
+        out[2 * kGuideBands] = d.x;
+        out[2 * kGuideBands + 1] = d.y;
+        out[2 * kGuideBands + 2] = d.z;
+#pragma unroll
+        for (int m = 0; m < kGuideMedia; m++) out[2 * kGuideBands + 3 + m] = (m == medium) ? 1.f : 0.f;
+        out[kGuideHalf - 1] = 0.f;
+    }
+}
+static_assert(2 * kGuideBands + 3 + kGuideMedia + 1 == kGuideHalf, "second half of the input");
 
 // Octahedral map of a unit direction to [0,1)^2 and back.
 UPBP_HD float2 oct_encode(float3 d)
@@ -309,16 +320,17 @@ UPBP_D bool guide_train_sample(unsigned i, const GuideRecord* recs, const unsign
     return slot >= 0;
 }
 
-// Training row i: the network input (encoded position, w_i, medium slot) and the target.
+// Training row i: one half of the network input (encoded position, w_i,
+// medium slot) and the target.
 UPBP_D void guide_train_row(unsigned i, const GuideRecord* recs, const unsigned* rec_count, unsigned rec_capacity,
                             unsigned seed, float3 lo, float3 inv_ext, const float* med_g, const int* medium_slot,
-                            float* in, float4& target)
+                            int half, float* in, float4& target)
 {
     GuideRecord r;
     float3 wi;
     int slot;
     guide_train_sample(i, recs, rec_count, rec_capacity, seed, med_g, medium_slot, r, wi, slot, target);
-    guide_encode((xyz(r.a) - lo) * inv_ext, wi, slot, in);
+    guide_encode_half((xyz(r.a) - lo) * inv_ext, wi, slot, half, in);
 }
 
 UPBP_D float guide_train_weight(unsigned i, const GuideRecord* recs, const unsigned* rec_count, unsigned rec_capacity,
@@ -334,7 +346,8 @@ UPBP_D float guide_train_weight(unsigned i, const GuideRecord* recs, const unsig
 
 // Table row i: (slot, cell, direction bin) -> the cell centre, the bin's
 // centre direction, the slot's medium.
-UPBP_D void guide_table_row(unsigned i, int cells, int dir_res, float3 lo, float3 cell, float3 inv_ext, float* in)
+UPBP_D void guide_table_row(unsigned i, int cells, int dir_res, float3 lo, float3 cell, float3 inv_ext, int half,
+                            float* in)
 {
     const unsigned per_slot = (unsigned)cells * cells * cells * dir_res * dir_res;
     const unsigned slot = i / per_slot, r = i % per_slot;
@@ -342,7 +355,7 @@ UPBP_D void guide_table_row(unsigned i, int cells, int dir_res, float3 lo, float
     const unsigned ix = c % cells, iy = (c / cells) % cells, iz = c / (cells * cells);
     const float3 x = lo + make_float3((ix + .5f) * cell.x, (iy + .5f) * cell.y, (iz + .5f) * cell.z);
     const float3 d = oct_decode(make_float2(((b % dir_res) + .5f) / dir_res, ((b / dir_res) + .5f) / dir_res));
-    guide_encode((x - lo) * inv_ext, d, (int)slot, in);
+    guide_encode_half((x - lo) * inv_ext, d, (int)slot, half, in);
 }
 
 // Network output row -> table entry: lobe means and kappas, weights times

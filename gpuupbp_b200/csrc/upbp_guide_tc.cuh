@@ -11,8 +11,10 @@
 //                                cell centres x direction bins, written as
 //                                table entries
 //
-// A CTA of 128 threads owns one SM (its shared memory is above half of an
-// SM's) and walks 128-row tiles.  The four FP16 weight matrices stay in
+// A CTA of 256 threads owns one SM (its shared memory is above half of an
+// SM's) and walks 128-row tiles, two threads per row (warps w and w + 4 read
+// the same TMEM lanes): each takes half of the row's input encoding and of
+// every hidden layer's columns; the first computes the row's loss.  The four FP16 weight matrices stay in
 // shared memory for the whole kernel; a tile's inputs, hidden activations
 // and gradients live in shared memory too, and nothing but the inputs'
 // sources and the results touches global memory.  Each GEMM is a chain of
@@ -41,7 +43,7 @@
 namespace upbp {
 
 constexpr int kTcRows = 128;       // rows per tile = MMA M = TMEM lanes
-constexpr int kTcThreads = 128;    // one thread per tile row
+constexpr int kTcThreads = 256;    // two threads per tile row: half 0 and half 1 of its columns
 constexpr int kTcTmemCols = 512;   // forward / dH accumulator (64) + four weight-gradient accumulators (4 x 64)
 constexpr int kTcTrainRecords = 0, kTcTrainRows = 1, kTcBake = 2;
 
@@ -238,6 +240,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
     extern __shared__ __align__(128) unsigned char tc_smem_raw[];
     GuideTcSmem& s = *reinterpret_cast<GuideTcSmem*>(tc_smem_raw);
     const int t = threadIdx.x, warp = t >> 5;
+    const int r = t & (kTcRows - 1), half = t >> 7;  // tile row, half of its columns
     constexpr bool kTrain = MODE != kTcBake;
 
     // weights into their tiles (16-byte pieces of a row of W [in][out]), biases
@@ -264,7 +267,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s.tmem;
-    const uint32_t lane_tmem = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's quarter of the lanes
+    const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's quarter of the lanes
     const uint32_t acc_f = tmem;                                      // forward / dH accumulator, 64 columns
     auto acc_dw = [&](int l) { return tmem + 64u + 64u * (uint32_t)l; };
 
@@ -299,33 +302,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
 
     const unsigned ntiles = (a.rows + kTcRows - 1) / kTcRows;
     for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const unsigned row = tile * kTcRows + t;
+        const unsigned row = tile * kTcRows + r;
         const bool valid = row < a.rows;
         float4 target = make_float4(0.f, 0.f, 0.f, 0.f);
 
-        // ---- input row t
+        // ---- input row r: this thread's half of its 96 columns
         if (MODE == kTcTrainRows) {
             const uint4* src = reinterpret_cast<const uint4*>(a.X + (size_t)row * kGuideInPad);
-            for (int cg = 0; cg < kGuideInPad / 8; cg++)
-                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(s.x) + tiled_off(t, cg * 8, kGuideInPad)) =
+            for (int cg = half * 6; cg < half * 6 + 6; cg++)
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(s.x) + tiled_off(r, cg * 8, kGuideInPad)) =
                     valid ? __ldg(src + cg) : make_uint4(0, 0, 0, 0);
             if (valid) target = a.T[row];
         } else {
-            float in[kGuideInPad];
+            float in[kGuideHalf];
             if (!valid) {
-                for (int k = 0; k < kGuideInPad; k++) in[k] = 0.f;
+                for (int k = 0; k < kGuideHalf; k++) in[k] = 0.f;
             } else if (MODE == kTcTrainRecords) {
                 guide_train_row(row, a.recs, a.rec_count, a.rec_capacity, a.seed, a.lo, a.inv_ext, a.med_g,
-                                a.medium_slot, in, target);
+                                a.medium_slot, half, in, target);
             } else {
-                guide_table_row(row, a.cells, a.dir_res, a.lo, a.cell, a.inv_ext, in);
+                guide_table_row(row, a.cells, a.dir_res, a.lo, a.cell, a.inv_ext, half, in);
             }
-            for (int cg = 0; cg < kGuideInPad / 8; cg++) tile_store8(s.x, kGuideInPad, t, cg, in + cg * 8);
+            for (int cg = 0; cg < 6; cg++) tile_store8(s.x, kGuideInPad, r, half * 6 + cg, in + cg * 8);
         }
         to_tensor_cores();
 
         // ---- forward: H1..H3 (FP16, ReLU; masks of the positive ones), O
-        unsigned mask[3][2];
+        unsigned mask[3];  // positive units of this thread's 32 columns of H1..H3
         float o[kGuideOutPad];
 #pragma unroll
         for (int l = 0; l < kGuideLayers; l++) {
@@ -341,19 +344,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
             if (!(ok = wait_chain())) break;
             const float* b = s.bias + tc_b_off(l);
             if (l < kGuideLayers - 1) {
-                mask[l][0] = mask[l][1] = 0u;
-                for (int c0 = 0; c0 < N; c0 += 16) {
+                mask[l] = 0u;
+                for (int c0 = 32 * half; c0 < 32 * half + 32; c0 += 16) {
                     float v[16];
                     tmem_ld16(lane_tmem + acc_f + c0, v);
                     for (int i = 0; i < 16; i++) {
                         const float y = fmaxf(v[i] + b[c0 + i], 0.f);
                         v[i] = __half2float(__float2half(y));
-                        if (v[i] > 0.f) mask[l][(c0 + i) >> 5] |= 1u << ((c0 + i) & 31);
+                        if (v[i] > 0.f) mask[l] |= 1u << ((c0 + i) & 31);
                     }
-                    tile_store8(s.h[l], kGuideHidden, t, c0 / 8, v);
-                    tile_store8(s.h[l], kGuideHidden, t, c0 / 8 + 1, v + 8);
+                    tile_store8(s.h[l], kGuideHidden, r, c0 / 8, v);
+                    tile_store8(s.h[l], kGuideHidden, r, c0 / 8 + 1, v + 8);
                 }
-            } else {
+            } else if (half == 0) {
                 for (int c0 = 0; c0 < N; c0 += 16) {
                     tmem_ld16(lane_tmem + acc_f + c0, o + c0);
                     for (int i = 0; i < 16; i++) o[c0 + i] += b[c0 + i];
@@ -364,17 +367,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
         if (!ok) break;
 
         if (MODE == kTcBake) {
-            if (valid) guide_write_entry(o, a.entries + (size_t)row * kGuideEntryWords);
+            if (valid && half == 0) guide_write_entry(o, a.entries + (size_t)row * kGuideEntryWords);
             tiles_done++;
             continue;
         }
-        if (MODE == kTcTrainRows && a.O && valid) {
+        if (MODE == kTcTrainRows && a.O && valid && half == 0) {
             float4* dst = reinterpret_cast<float4*>(a.O + (size_t)row * kGuideOutPad);
             for (int k = 0; k < kGuideOutPad / 4; k++) dst[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
         }
 
         // ---- loss and output gradient (row weight over the batch mean), FP16 into d[0]
-        {
+        if (half == 0) {
             float g[kGuideOutPad], l = 0.f;
             if (valid) {
                 guide_row_grad(o, target, wscale, g, &l);
@@ -382,7 +385,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
                 for (int k = 0; k < kGuideOutPad; k++) g[k] = 0.f;
             }
             loss += l;
-            for (int cg = 0; cg < kGuideOutPad / 8; cg++) tile_store8(s.d[0], kGuideOutPad, t, cg, g + cg * 8);
+            for (int cg = 0; cg < kGuideOutPad / 8; cg++) tile_store8(s.d[0], kGuideOutPad, r, cg, g + cg * 8);
         }
         to_tensor_cores();
 
@@ -393,12 +396,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
             const int cur = (kGuideLayers - 1 - l) & 1;
             const __half* dy = s.d[cur];
             {  // bias gradient from the FP16 gradient rows of this tile
-                const int c = t & 63, r0 = (t >> 6) * 64;
+                const int c = t & 63, r0 = (t >> 6) * 32;
                 if (c < N) {
                     float sum = 0.f;
-                    for (int r = r0; r < r0 + 64; r++)
+                    for (int q = r0; q < r0 + 32; q++)
                         sum += __half2float(*reinterpret_cast<const __half*>(
-                            reinterpret_cast<const char*>(dy) + tiled_off(r, c, N)));
+                            reinterpret_cast<const char*>(dy) + tiled_off(q, c, N)));
                     bsum[l] += sum;
                 }
             }
@@ -415,13 +418,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
             if (!(ok = wait_chain())) break;
             if (l > 0) {
                 __half* nxt = s.d[cur ^ 1];
-                for (int c0 = 0; c0 < K; c0 += 16) {
+                for (int c0 = 32 * half; c0 < 32 * half + 32; c0 += 16) {
                     float v[16];
                     tmem_ld16(lane_tmem + acc_f + c0, v);
                     for (int i = 0; i < 16; i++)
-                        if (!((mask[l - 1][(c0 + i) >> 5] >> ((c0 + i) & 31)) & 1u)) v[i] = 0.f;
-                    tile_store8(nxt, kGuideHidden, t, c0 / 8, v);
-                    tile_store8(nxt, kGuideHidden, t, c0 / 8 + 1, v + 8);
+                        if (!((mask[l - 1] >> ((c0 + i) & 31)) & 1u)) v[i] = 0.f;
+                    tile_store8(nxt, kGuideHidden, r, c0 / 8, v);
+                    tile_store8(nxt, kGuideHidden, r, c0 / 8 + 1, v + 8);
                 }
                 to_tensor_cores();
             }
@@ -436,14 +439,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
         if (t == 0) atomicOr(a.err, 1u);
         mbar_wait_bounded(mbar, phase);
     } else if (kTrain && tiles_done > 0) {
-        // weight gradients: lane j of accumulator l holds row j of dW_l
+        // weight gradients: lane j of accumulator l holds row j of dW_l; the
+        // two threads of a lane take the lower and upper columns
         for (int l = 0; l < kGuideLayers; l++) {
             const int K = tc_layer_in(l), N = tc_layer_out(l);
-            float* gw = a.grad + tc_w_off(l) + (size_t)t * N;
-            for (int c0 = 0; c0 < N; c0 += 16) {
+            float* gw = a.grad + tc_w_off(l) + (size_t)r * N;
+            for (int c0 = 32 * half; c0 < min(N, 32 * half + 32); c0 += 16) {
                 float v[16];
                 tmem_ld16(lane_tmem + acc_dw(l) + c0, v);
-                if (t < K)
+                if (r < K)
                     for (int i = 0; i < 16; i++) atomicAdd(gw + c0 + i, v[i]);
             }
             const int c = t & 63;

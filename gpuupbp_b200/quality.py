@@ -6,10 +6,17 @@ equal-time comparison renders a converged reference with the plain method,
 then renders each method for the same device time and compares their
 relMSE: a method that reaches a k times lower relMSE in the same time is k
 times as efficient.
+
+The reference runs the same radius schedule from iteration 0 (the radii
+shrink with the iteration index, so later indices are noisier per
+iteration) on independent random streams: -ioff shifts only the random
+numbers' iteration index.
 """
 from __future__ import annotations
 
 import numpy as np
+
+REFERENCE_IOFF = ["-ioff", "1000000"]
 
 
 def relmse(x: np.ndarray, ref: np.ndarray) -> float:
@@ -42,14 +49,13 @@ def _timed_render(args: list[str], iterations: int | None, budget_ms: float | No
     return img, it, ms
 
 
-def equal_time(plain_args: list[str], other_args: list[str], reference_iterations: int, other_iterations: int,
-               reference_start: int = 100000) -> dict:
-    """The plain method's converged reference (reference_iterations, on
-    iteration indices from reference_start, so its random streams are
-    independent of the compared renders), the other method for
-    other_iterations, the plain method for the same device time, and both
-    relMSEs."""
-    ref, _, ref_ms = _timed_render(plain_args, reference_iterations, None, start=reference_start)
+def equal_time(plain_args: list[str], other_args: list[str], reference_iterations: int,
+               other_iterations: int) -> dict:
+    """The plain method's converged reference (reference_iterations on
+    random streams independent of the compared renders), the other method
+    for other_iterations, the plain method for the same device time, and
+    both relMSEs."""
+    ref, _, ref_ms = _timed_render(plain_args + REFERENCE_IOFF, reference_iterations, None)
     other, n_other, t_other = _timed_render(other_args, other_iterations, None)
     plain, n_plain, t_plain = _timed_render(plain_args, None, t_other)
     e_other, e_plain = relmse(other, ref), relmse(plain, ref)
@@ -63,12 +69,11 @@ def _batch_images(b) -> list:
     return [r.accumulated() for r in b.renderers]
 
 
-def batch_equal_time(jobs: list, method_extra: list, reference_iterations: int, method_iterations: int,
-                     reference_start: int = 100000) -> dict:
+def batch_equal_time(jobs: list, method_extra: list, reference_iterations: int, method_iterations: int) -> dict:
     """Equal-time comparison on many jobs (config 3 of the benchmark spec).
 
     * reference: every job's converged plain render, reference_iterations
-      batch iterations on iteration indices from reference_start;
+      batch iterations on independent random streams;
     * method: the jobs with `method_extra` appended to their command lines
       (e.g. the learned proposal), rendered together by upbp_run_batch with
       the autotuner's choice, method_iterations iterations; its wall time T
@@ -83,8 +88,8 @@ def batch_equal_time(jobs: list, method_extra: list, reference_iterations: int, 
 
     from gpuupbp_b200 import batch as B
 
-    ref = B.Batch(jobs)
-    tune = B.autotune(ref, reference_start)
+    ref = B.Batch([j + REFERENCE_IOFF for j in jobs])
+    tune = B.autotune(ref, 0)
     it = tune["next_iteration"]
     while ref.renderers[0].iterations < reference_iterations:
         ref.run_iteration(it)

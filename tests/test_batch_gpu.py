@@ -47,6 +47,6 @@ def test_autotuner_picks_a_measured_configuration(scene_dir):
     b = batch.Batch(jobs)
     choice = batch.autotune(b, 0, workers=(1, 4), limits=(0, 64))
     assert (choice["workers"], choice["grid_limit"]) in {(1, 0), (4, 0), (1, 64), (4, 64)}
-    assert choice["next_iteration"] == 4 and len(choice["timings_s"]) == 4
+    assert choice["next_iteration"] == 5 and len(choice["timings_s"]) == 4
     b.run_iteration(choice["next_iteration"])
     b.close()

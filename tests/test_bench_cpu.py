@@ -47,3 +47,17 @@ def test_clock_summary_counts_only_the_timed_window():
     s = c.summary(t, t + 0.4)
     assert s == {"sm_mhz": 1957.5, "sm_max_mhz": 1965.0, "reasons": [], "samples": 2}
     assert c.summary()["samples"] == 3 and c.summary()["reasons"] == ["sw_power_cap"]
+
+
+def test_relmse_and_reference_streams():
+    """relMSE as defined, and the equal-time references render the same
+    radius schedule on other random streams (-ioff shifts only those)."""
+    import numpy as np
+
+    from gpuupbp_b200 import quality
+    ref = np.array([[[1.0, 0.0, 2.0]]])
+    x = np.array([[[1.5, 0.1, 2.0]]])
+    want = np.mean(np.array([0.25 / 1.01, 0.01 / 0.01, 0.0]))
+    assert abs(quality.relmse(x, ref) - want) < 1e-12
+    assert quality.relmse(ref, ref) == 0.0
+    assert quality.REFERENCE_IOFF[0] == "-ioff" and int(quality.REFERENCE_IOFF[1]) > 100000
