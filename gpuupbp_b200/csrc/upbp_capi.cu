@@ -2063,7 +2063,8 @@ extern "C" int upbp_guide_gradients(const float* params, uint32_t n_params, cons
             std::vector<__half> xh((size_t)rows * kGuideInPad);
             for (size_t i = 0; i < xh.size(); i++) xh[i] = __float2half(x[i]);
             UPBP_CK(cudaMemcpyAsync(b.X, xh.data(), xh.size() * sizeof(__half), cudaMemcpyHostToDevice, st));
-            UPBP_CK(cudaMemcpyAsync(b.T, t, (size_t)rows * sizeof(float4), cudaMemcpyHostToDevice, st));
+            UPBP_CK(cudaMemcpyAsync(b.T, t, (size_t)rows * kGuideTargetWords * sizeof(float), cudaMemcpyHostToDevice,
+                                    st));
             UPBP_CK(cudaMemsetAsync(b.scal, 0, 3 * sizeof(float), st));
             UPBP_CK(cudaMemsetAsync(net.grad, 0, kGuideParams * sizeof(float), st));
             k_guide_weight_sum<<<148, 256, 0, st>>>(b.T, rows, b.scal + 1);

@@ -39,7 +39,11 @@ constexpr int kGuideIn = 3 * 2 * kGuideBands + 3 + kGuideMedia;  // 95
 constexpr int kGuideInPad = 96;
 constexpr int kGuideHidden = 64;
 constexpr int kGuideLobes = 8;
-constexpr int kGuideOut = kGuideLobes * 5;             // logits, mean xyz, log kappa
+constexpr int kGuideOut = kGuideLobes * 5 + 1;         // logits, mean xyz, log kappa, selection logit
+constexpr int kGuideAlphaCol = kGuideLobes * 5;
+// Largest probability of sampling the mixture rather than the phase
+// function: the phase function keeps at least a tenth (defensive sampling).
+constexpr float kGuideAlphaMax = 0.9f;
 constexpr int kGuideOutPad = 48;
 // layer shapes (in x out), row-major weights, FP16 copies of FP32 masters
 constexpr int kGuideLayers = 4;
@@ -63,6 +67,7 @@ constexpr float kGuideKappaMin = 1e-2f, kGuideKappaMax = 2e3f;
 // normalisation, and the cumulative lobe weights for sampling (GuideTable in
 // upbp_device.cuh).
 constexpr int kGuideEntryWords = kGuideLobes + 4;  // float4s
+constexpr int kGuideTargetWords = 5;               // a training target: direction xyz, weight, phase pdf
 
 // ---------------------------------------------------------------- encoding
 
@@ -160,6 +165,9 @@ UPBP_D int guide_cell(const GuideTable& g, float3 x, int medium)
     return ((slot * g.cells + iz) * g.cells + iy) * g.cells + ix;
 }
 
+// Selection probability of a table entry's mixture against the phase function.
+UPBP_D float guide_entry_alpha(const float4* e) { return __ldg(&e[kGuideLobes + 3]).w; }
+
 UPBP_D float vmf_mix_pdf(const float4* e, float3 w)
 {
     float p = 0.f;
@@ -218,6 +226,10 @@ UPBP_HD void vmf_from_output(const float* o, VmfLobes& v)
     }
 }
 
+// Probability of sampling the mixture rather than the phase function, from
+// the network's selection logit.
+UPBP_HD float guide_alpha(float logit) { return kGuideAlphaMax / (1.f + expf(-logit)); }
+
 UPBP_HD unsigned guide_hash(unsigned x)
 {
     x ^= x >> 16;
@@ -230,10 +242,14 @@ UPBP_HD unsigned guide_hash(unsigned x)
 
 UPBP_HD float guide_u01(unsigned h) { return (float)(h >> 8) * (1.f / 16777216.f); }
 
-// Loss rows: -w log q(target) with q the vMF mixture of the row's output;
-// writes dLoss/dOutput (FP16, per row, scaled so that the batch mean of the
-// weights is 1) and the row's weighted loss.
-UPBP_HD float guide_row_grad(const float* o, float4 t, float wscale, float* grad, float* loss)
+// Loss rows: -w log P(target), P = (1 - a) h + a q the blend the renderer
+// samples -- h the phase function's pdf of the target direction (given),
+// q the vMF mixture of the row's output, a the selection probability -- so
+// the network learns where the mixture helps (a grows) and where the phase
+// function alone fits the light's arrival directions (a shrinks).  Writes
+// dLoss/dOutput (scaled so that the batch mean of the weights is 1) and the
+// row's weighted loss.
+UPBP_HD float guide_row_grad(const float* o, float4 t, float h, float wscale, float* grad, float* loss)
 {
     VmfLobes v;
     vmf_from_output(o, v);
@@ -244,35 +260,43 @@ UPBP_HD float guide_row_grad(const float* o, float4 t, float wscale, float* grad
         q += v.pi[j] * val[j];
     }
     q = fmaxf(q, 1e-30f);
+    const float sig = 1.f / (1.f + expf(-o[kGuideAlphaCol])), a = kGuideAlphaMax * sig;
+    const float P = fmaxf((1.f - a) * h + a * q, 1e-30f);
     const float wt = t.w * wscale;
-    *loss = -wt * logf(q);
+    *loss = -wt * logf(P);
+    // d(-log P)/dq = -a / P: the mixture's gradients of -log q scaled by a q / P
+    const float sq = wt * a * q / P;
     for (int k = 0; k < kGuideOutPad; k++) grad[k] = 0.f;
     for (int j = 0; j < kGuideLobes; j++) {
         const float r = v.pi[j] * val[j] / q;  // responsibility of lobe j
         // d(-log q)/d logit_j = pi_j - r_j
-        grad[j] = wt * (v.pi[j] - r);
+        grad[j] = sq * (v.pi[j] - r);
         // d(-log q)/d mu_j = -r_j kappa_j w; through the normalisation mu = m/|m|
         const float3 gmu = w * (-r * v.kappa[j]);
         const float3 gm = (gmu - v.mu[j] * dot(gmu, v.mu[j])) * (1.f / v.m_len[j]);
-        grad[kGuideLobes + 3 * j] = wt * gm.x;
-        grad[kGuideLobes + 3 * j + 1] = wt * gm.y;
-        grad[kGuideLobes + 3 * j + 2] = wt * gm.z;
+        grad[kGuideLobes + 3 * j] = sq * gm.x;
+        grad[kGuideLobes + 3 * j + 1] = sq * gm.y;
+        grad[kGuideLobes + 3 * j + 2] = sq * gm.z;
         // d log val_j / d kappa = 1/kappa - 2 e^{-2k}/(1 - e^{-2k}) + (mu.w - 1); kappa = exp(o), clamped
         const float k = v.kappa[j];
         const float e2 = expf(-2.f * k);
         const float dlog = 1.f / k - 2.f * e2 / fmaxf(1.f - e2, 1e-30f) + (dot(v.mu[j], w) - 1.f);
         const float raw = expf(o[4 * kGuideLobes + j]);
         const float inside = (raw > kGuideKappaMin && raw < kGuideKappaMax) ? 1.f : 0.f;
-        grad[4 * kGuideLobes + j] = wt * (-r * dlog * k * inside);
+        grad[4 * kGuideLobes + j] = sq * (-r * dlog * k * inside);
     }
-    return q;
+    // d(-log P)/d logit_a = -(q - h) / P * da/dlogit
+    grad[kGuideAlphaCol] = -wt * (q - h) / P * kGuideAlphaMax * sig * (1.f - sig);
+    return P;
 }
 
-// Weighted-batch scale: 1 / mean weight.
-__global__ void k_guide_weight_sum(const float4* T, unsigned batch, float* sum)
+// Weighted-batch scale: 1 / mean weight (targets of 5 floats: direction,
+// weight, phase-function pdf).
+__global__ void k_guide_weight_sum(const float* T, unsigned batch, float* sum)
 {
     float s = 0.f;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) s += T[i].w;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x)
+        s += T[(size_t)kGuideTargetWords * i + 3];
     for (int off = 16; off; off >>= 1) s += __shfl_down_sync(~0u, s, off);
     if ((threadIdx.x & 31) == 0) atomicAdd(sum, s);
 }
@@ -301,7 +325,7 @@ __global__ void k_guide_adam(float* w, float* m, float* v, const float* g, int n
 // Returns false (weight 0) where the record's medium is not guided.
 UPBP_D bool guide_train_sample(unsigned i, const GuideRecord* recs, const unsigned* rec_count, unsigned rec_capacity,
                                unsigned seed, const float* med_g, const int* medium_slot, GuideRecord& r, float3& wi,
-                               int& slot, float4& target)
+                               int& slot, float4& target, float& phase_pdf)
 {
     const unsigned nrec = min(*rec_count, rec_capacity);
     const unsigned h0 = guide_hash(seed * 0x9e3779b9u + i);
@@ -317,6 +341,7 @@ UPBP_D bool guide_train_sample(unsigned i, const GuideRecord* recs, const unsign
     const float g2 = g * g, d = 1.f + g2 - 2.f * g * ct;
     const float phase = fabsf(g) < 1e-3f ? 0.0795774715f : 0.0795774715f * (1.f - g2) / (d * sqrtf(d));
     target = make_float4(tdir.x, tdir.y, tdir.z, slot >= 0 ? r.b.w * phase : 0.f);
+    phase_pdf = phase;
     return slot >= 0;
 }
 
@@ -324,12 +349,12 @@ UPBP_D bool guide_train_sample(unsigned i, const GuideRecord* recs, const unsign
 // medium slot) and the target.
 UPBP_D void guide_train_row(unsigned i, const GuideRecord* recs, const unsigned* rec_count, unsigned rec_capacity,
                             unsigned seed, float3 lo, float3 inv_ext, const float* med_g, const int* medium_slot,
-                            int half, float* in, float4& target)
+                            int half, float* in, float4& target, float& phase_pdf)
 {
     GuideRecord r;
     float3 wi;
     int slot;
-    guide_train_sample(i, recs, rec_count, rec_capacity, seed, med_g, medium_slot, r, wi, slot, target);
+    guide_train_sample(i, recs, rec_count, rec_capacity, seed, med_g, medium_slot, r, wi, slot, target, phase_pdf);
     guide_encode_half((xyz(r.a) - lo) * inv_ext, wi, slot, half, in);
 }
 
@@ -340,7 +365,8 @@ UPBP_D float guide_train_weight(unsigned i, const GuideRecord* recs, const unsig
     float3 wi;
     int slot;
     float4 target;
-    guide_train_sample(i, recs, rec_count, rec_capacity, seed, med_g, medium_slot, r, wi, slot, target);
+    float phase_pdf;
+    guide_train_sample(i, recs, rec_count, rec_capacity, seed, med_g, medium_slot, r, wi, slot, target, phase_pdf);
     return target.w;
 }
 
@@ -374,7 +400,8 @@ UPBP_D void guide_write_entry(const float* o, float4* e)
         c += v.pi[j];
         cdf[j] = c;
     }
-    cdf[kGuideLobes - 1] = 1.f;
+    // the last cumulative weight is 1 and never read: it holds the selection probability
+    cdf[kGuideLobes - 1] = guide_alpha(o[kGuideAlphaCol]);
     for (int k = 0; k < kGuideEntryWords; k++) e[k] = out[k];
 }
 

@@ -219,9 +219,10 @@ struct GuideTcArgs {
     float3 lo, inv_ext;
     const float* med_g;
     const int* medium_slot;
-    // kTcTrainRows: given rows and targets; O (optional) receives the outputs
+    // kTcTrainRows: given rows and targets (kGuideTargetWords floats each:
+    // direction, weight, phase-function pdf); O (optional) receives the outputs
     const __half* X;
-    const float4* T;
+    const float* T;
     float* O;
     // training: the batch's weight sum, gradient sums (kGuideParams) and summed loss, all accumulated atomically
     const float* weight_sum;
@@ -305,6 +306,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
         const unsigned row = tile * kTcRows + r;
         const bool valid = row < a.rows;
         float4 target = make_float4(0.f, 0.f, 0.f, 0.f);
+        float phase_pdf = 0.f;  // the phase function's pdf of the target direction
 
         // ---- input row r: this thread's half of its 96 columns
         if (MODE == kTcTrainRows) {
@@ -312,14 +314,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
             for (int cg = half * 6; cg < half * 6 + 6; cg++)
                 *reinterpret_cast<uint4*>(reinterpret_cast<char*>(s.x) + tiled_off(r, cg * 8, kGuideInPad)) =
                     valid ? __ldg(src + cg) : make_uint4(0, 0, 0, 0);
-            if (valid) target = a.T[row];
+            if (valid) {
+                const float* tr = a.T + (size_t)kGuideTargetWords * row;
+                target = make_float4(tr[0], tr[1], tr[2], tr[3]);
+                phase_pdf = tr[4];
+            }
         } else {
             float in[kGuideHalf];
             if (!valid) {
                 for (int k = 0; k < kGuideHalf; k++) in[k] = 0.f;
             } else if (MODE == kTcTrainRecords) {
                 guide_train_row(row, a.recs, a.rec_count, a.rec_capacity, a.seed, a.lo, a.inv_ext, a.med_g,
-                                a.medium_slot, half, in, target);
+                                a.medium_slot, half, in, target, phase_pdf);
             } else {
                 guide_table_row(row, a.cells, a.dir_res, a.lo, a.cell, a.inv_ext, half, in);
             }
@@ -380,7 +386,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_guide_tc(GuideTcArgs a)
         if (half == 0) {
             float g[kGuideOutPad], l = 0.f;
             if (valid) {
-                guide_row_grad(o, target, wscale, g, &l);
+                guide_row_grad(o, target, phase_pdf, wscale, g, &l);
             } else {
                 for (int k = 0; k < kGuideOutPad; k++) g[k] = 0.f;
             }

@@ -26,7 +26,7 @@ struct GuideNet {
 struct GuideBatch {
     unsigned rows = 0;
     __half* X = nullptr;      // rows x kGuideInPad, given rows only
-    float4* T = nullptr;      // rows: target direction, weight; given rows only
+    float* T = nullptr;       // rows x kGuideTargetWords: direction, weight, phase pdf; given rows only
     float* scal = nullptr;    // [0] weighted loss sum [1] weight sum [2] error bits (unsigned)
 };
 
@@ -58,7 +58,7 @@ cudaError_t guide_alloc_batch(GuideBatch& b, unsigned rows, bool given_rows)
     cudaError_t e;
     if (given_rows) {
         if ((e = dalloc(&b.X, (size_t)rows * kGuideInPad)) != cudaSuccess) return e;
-        if ((e = dalloc(&b.T, rows)) != cudaSuccess) return e;
+        if ((e = dalloc(&b.T, (size_t)kGuideTargetWords * rows)) != cudaSuccess) return e;
     }
     return dalloc(&b.scal, 3);
 }
@@ -91,6 +91,8 @@ void guide_init_params(std::vector<float>& w)
         for (int k = 0; k < 3; k++) b4[kGuideLobes + 3 * j + k] = dirs[j][k] * 0.577f;
         b4[4 * kGuideLobes + j] = std::log(2.f);  // kappa 2
     }
+    // selection probability 0.5 to begin with
+    b4[kGuideAlphaCol] = std::log(0.5f / kGuideAlphaMax / (1.f - 0.5f / kGuideAlphaMax));
 }
 
 cudaError_t guide_alloc_net(GuideNet& n, cudaStream_t st)

@@ -208,14 +208,17 @@ struct Bsdf {
 };
 
 // Pdf of a camera subpath scattering at a medium vertex from direction of
-// travel `travel` into `out`: the blend of the phase function (value hg) and
-// the learned mixture, or hg where the vertex is not guided.
+// travel `travel` into `out`: the blend (1 - a) hg + a mixture of the phase
+// function (value hg) and the learned mixture, a the table entry's
+// selection probability, or hg where the vertex is not guided.
 // Kept out of line: the unguided callers, the common case, pay only the
 // test of the cell.
 __device__ __noinline__ float guide_mix(int cell, float3 travel, float3 out, float hg)
 {
     const float4* e = guide_entry(c_params.guide, cell, travel);
-    return e ? .5f * hg + .5f * vmf_mix_pdf(e, out) : hg;
+    if (!e) return hg;
+    const float a = guide_entry_alpha(e);
+    return (1.f - a) * hg + a * vmf_mix_pdf(e, out);
 }
 
 UPBP_D float guide_pdf(const Bsdf& b, float3 travel, float3 out, float hg)
@@ -235,20 +238,22 @@ UPBP_D float guide_pdf_at(float3 x, int med, float3 travel, float3 out, float hg
     return c_params.guide.entries ? guide_mix_at(x, med, travel, out, hg) : hg;
 }
 
-// Samples the blend of the phase function and the learned mixture, one half
-// each: r2 picks the component (and, rescaled, the mixture's lobe).
+// Samples the blend of the phase function and the learned mixture: r2 picks
+// the mixture with the entry's selection probability a (and, rescaled, the
+// mixture's lobe), the phase function otherwise.
 __device__ __noinline__ float3 guide_sample(const Bsdf& b, float r0, float r1, float r2, float3& dir_gen, float& pdf,
                                             float& sin_theta)
 {
     const float4* e = guide_entry(c_params.guide, b.gcell, -b.world_dir_fix);
-    if (!e || r2 < .5f) {
+    const float a = e ? guide_entry_alpha(e) : 0.f;
+    if (!e || r2 >= a) {
         hg_sample(b.world_dir_fix, b.mean_cosine, r0, r1, b.frame, dir_gen, pdf, &sin_theta);
         if (!e) return b.scatter_coef * pdf;
     } else {
-        dir_gen = vmf_mix_sample(e, 2.f * r2 - 1.f, r0, r1);
+        dir_gen = vmf_mix_sample(e, r2 / a, r0, r1);
     }
     const float p = hg_pdf(b.world_dir_fix, dir_gen, b.mean_cosine, &sin_theta);
-    pdf = .5f * p + .5f * vmf_mix_pdf(e, dir_gen);
+    pdf = (1.f - a) * p + a * vmf_mix_pdf(e, dir_gen);
     return b.scatter_coef * p;
 }
 

@@ -418,6 +418,25 @@ def media_field_env(seed: int = 2, tiny: bool = False) -> SceneBuilder:
     return sb
 
 
+def media_row(seed: int = 7, tiny: bool = False) -> SceneBuilder:
+    """Overflow of the imaginary boundaries a ray may meet between two real
+    hits: 12 small fog spheres in a row along the camera's view axis, 24
+    crossings for a camera ray along the row, more than the 8 the reference
+    keeps (MAX_IMAGINARY_INTERSECTIONS), so those rays end with the
+    intersection-stack failure."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder()
+    _box_walls(sb, rng)
+    _quad_light(sb, "light", (0.0, 0.499, 0.0), 0.3)
+    v, f = icosphere(1 if tiny else 2)
+    sb.media.append(Medium("fog", absorption=(0.05, 0.05, 0.05), scattering=(0.2, 0.2, 0.2), g=0.2))
+    sb.materials.append(Material("fog_boundary", real=False, priority=1, medium="fog"))
+    for i in range(12):
+        sb.add("fog_boundary", v * 0.028 + np.array([0.0, 0.0, 0.33 - 0.068 * i]), f, v)
+    sb.camera = Camera(position=(0.0, 0.0, 0.45), target=(0.0, 0.0, -0.5), up=(0.0, 1.0, 0.0), hfov_deg=30.0)
+    return sb
+
+
 def batch_job(seed: int, tiny: bool = False) -> SceneBuilder:
     """One job of the batched workload, drawn from its seed: a closed box with
     a quad light and 1-3 randomly displaced icospheres bounding homogeneous
@@ -458,7 +477,7 @@ def batch_job_config(seed: int) -> dict:
 
 WORKLOADS = {"media_field_env": media_field_env, "box_medium": box_medium, "media_field": media_field, "dense_beams": dense_beams,
              "media_field_lights": media_field_lights, "glass_box": glass_box, "fog_box": fog_box,
-             "batch_job": batch_job}
+             "batch_job": batch_job, "media_row": media_row}
 
 
 # Version of the generators' output: a change to any generator that changes

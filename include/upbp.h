@@ -377,10 +377,13 @@ int upbp_debug_mis_records(upbp_ctx* ctx, int which, float* out, uint64_t capaci
  * (the layout of gpuupbp_b200/csrc/upbp_guide.cuh: four row-major [in][out]
  * weight matrices 96x64, 64x64, 64x64, 64x48, then their biases; n_params
  * must be their count, 17648, or UPBP_ERR_ARGS is returned), `rows`
- * inputs of 96 floats and targets of 4 floats (unit direction, weight); it
- * writes the gradient sums of the weighted negative log-likelihood (weights
- * normalised to a batch mean of 1) with respect to every parameter, the
- * rows x 48 outputs when `outputs` is not NULL, and the summed loss. */
+ * inputs of 96 floats and targets of 5 floats (unit direction, weight, the
+ * phase function's pdf of the direction); it writes the gradient sums of
+ * the weighted negative log-likelihood of the target under the sampled
+ * blend (1 - a) phase + a mixture (weights normalised to a batch mean of 1;
+ * outputs 0-39 the 8-lobe mixture, 40 the logit of a = 0.9 sigmoid) with
+ * respect to every parameter, the rows x 48 outputs when `outputs` is not
+ * NULL, and the summed loss. */
 int upbp_guide_info(upbp_ctx* ctx, float* out, uint32_t n);
 int upbp_guide_gradients(const float* params, uint32_t n_params, const float* x, const float* t, uint32_t rows,
                          float* grads, float* outputs, float* loss);

@@ -4,10 +4,13 @@ gpuupbp_b200/csrc/upbp_guide.cuh; nothing in the product imports it).
 
 Network: 96 inputs (12-band frequency encoding of the position normalised to
 the scene box, the direction of travel, a one-hot medium slot, one pad) ->
-3 hidden layers of 64 ReLU units -> 48 outputs, of which 40 are used: 8 lobe
+3 hidden layers of 64 ReLU units -> 48 outputs, of which 41 are used: 8 lobe
 logits, 8 mean vectors (normalised), 8 log-kappas (kappa clamped to
-[1e-2, 2e3]).  Loss of a row: -w log q(target), q the 8-lobe von
-Mises-Fisher mixture, w the row weight divided by the batch mean weight.
+[1e-2, 2e3]) and the logit of the selection probability a = 0.9
+sigmoid(o[40]).  Loss of a row: -w log P(target), P = (1 - a) h + a q the
+blend the renderer samples, h the phase function's pdf of the target
+direction (a target's fifth value), q the 8-lobe von Mises-Fisher
+mixture's, w the row weight divided by the batch mean weight.
 
 `fp16_like_gpu` rounds the operands where the GPU kernels hold FP16 (inputs,
 weights, the hidden activations after ReLU, the output gradients and the
@@ -68,8 +71,14 @@ def vmf_norm(k):
     return k / (2 * math.pi * (-np.expm1(-2 * k)))
 
 
+ALPHA_MAX = 0.9
+ALPHA_COL = 5 * LOBES
+
+
 def row_loss_grad(o: np.ndarray, t: np.ndarray, wscale: float):
-    """Loss and d loss / d output of one row (float64)."""
+    """Loss and d loss / d output of one row (float64): -w log P with P =
+    (1 - a) h + a q, h = t[4] the phase function's pdf of the target
+    direction t[0:3], q the vMF mixture's, a = ALPHA_MAX sigmoid(o[40])."""
     lg = o[:LOBES]
     pi = np.exp(lg - lg.max())
     pi /= pi.sum()
@@ -82,20 +91,26 @@ def row_loss_grad(o: np.ndarray, t: np.ndarray, wscale: float):
     cosv = mu @ w
     val = vmf_norm(kap) * np.exp(kap * (cosv - 1))
     q = max(float(pi @ val), 1e-30)
+    sig = 1.0 / (1.0 + math.exp(-o[ALPHA_COL]))
+    a = ALPHA_MAX * sig
+    h = float(t[4])
+    P = max((1 - a) * h + a * q, 1e-30)
     wt = t[3] * wscale
-    loss = -wt * math.log(q)
+    loss = -wt * math.log(P)
+    sq = wt * a * q / P
     g = np.zeros(OUT)
     r = pi * val / q
-    g[:LOBES] = wt * (pi - r)
+    g[:LOBES] = sq * (pi - r)
     for j in range(LOBES):
         gmu = w * (-r[j] * kap[j])
         gm = (gmu - mu[j] * (gmu @ mu[j])) / mlen[j]
-        g[LOBES + 3 * j:LOBES + 3 * j + 3] = wt * gm
+        g[LOBES + 3 * j:LOBES + 3 * j + 3] = sq * gm
         k = kap[j]
         e2 = math.exp(-2 * k)
         dlog = 1 / k - 2 * e2 / max(1 - e2, 1e-30) + (cosv[j] - 1)
         inside = 1.0 if KAPPA_MIN < raw[j] < KAPPA_MAX else 0.0
-        g[4 * LOBES + j] = wt * (-r[j] * dlog * k * inside)
+        g[4 * LOBES + j] = sq * (-r[j] * dlog * k * inside)
+    g[ALPHA_COL] = -wt * (q - h) / P * ALPHA_MAX * sig * (1 - sig)
     return loss, g
 
 

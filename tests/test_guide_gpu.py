@@ -26,7 +26,7 @@ def _batch(rows, seed):
                   for _ in range(rows)])
     d = rng.normal(size=(rows, 3))
     d /= np.linalg.norm(d, axis=1, keepdims=True)
-    T = np.concatenate([d, rng.uniform(0.1, 2.0, size=(rows, 1))], axis=1)
+    T = np.concatenate([d, rng.uniform(0.1, 2.0, size=(rows, 1)), rng.uniform(0.02, 1.0, size=(rows, 1))], axis=1)
     return X.astype(np.float32), T.astype(np.float32)
 
 
