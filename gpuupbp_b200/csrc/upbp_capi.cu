@@ -351,10 +351,12 @@ const upbp_kernels::ParamKernels& slotted_kernels()
     return k;
 }
 
-// The kernels a call of context c launches: the fixed-bank copy on slot 0.
+// The kernels a call of context c launches: the fixed-bank copy (built
+// without analytic spheres) on slot 0 for a scene without spheres.
 const upbp_kernels::ParamKernels& PK(const upbp_ctx* c)
 {
-    return c->slot == 0 ? upbp_kernels::slot0_kernels() : slotted_kernels();
+    const bool spheres = c->real.sph_count + c->imag.sph_count > 0;
+    return c->slot == 0 && !spheres ? upbp_kernels::slot0_kernels() : slotted_kernels();
 }
 
 HitLease::HitLease(upbp_ctx* c) : c_(c)

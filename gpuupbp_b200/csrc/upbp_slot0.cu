@@ -1,5 +1,7 @@
 // The hot kernels compiled a second time against a fixed parameter bank, for
-// the context on launch-parameter slot 0 (upbp_device.cuh explains why).
+// the context on launch-parameter slot 0 (upbp_device.cuh explains why), and
+// without analytic spheres (upbp_bvh.cuh): a context launches them when it
+// holds slot 0 and its scene has no spheres.
 // The preprocessor renames the device code's namespace, so these kernels,
 // their constant banks and device variables are symbols of their own.
 #include <cuda_runtime.h>
@@ -9,6 +11,7 @@
 #include "upbp_kernel_table.h"
 
 #define UPBP_SLOT0_BANK 1
+#define UPBP_NO_SPHERES 1  // used only for scenes without analytic spheres
 #define upbp upbp_slot0
 #include "upbp_camera_pass.cuh"
 #include "upbp_light_pass.cuh"

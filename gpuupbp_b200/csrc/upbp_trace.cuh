@@ -132,7 +132,7 @@ UPBP_D float sphere_attribute_component(float x)
 // a sphere's shading normal is its normal and it is no emitter).
 UPBP_D void fill_hit(const TriView& tv, const TriHit& h, float3 ray_dir, Isect& r)
 {
-    if (h.prim < 0) {
+    if (kSceneSpheres && h.prim < 0) {
         const int mat = __ldg(&tv.sph_mat[~h.prim]);
         const float3 nrm = make_float3(sphere_attribute_component(h.u), sphere_attribute_component(h.v),
                                        sphere_attribute_component(h.w));
