@@ -853,30 +853,32 @@ __global__ void __launch_bounds__(128) range_search_kernel(int slot)
         if (node != kWalkDone) {
             // one internal node: leaf children become pairs, internal ones are visited
             visits++;
-            const NodeBoxes nb = load_qnode(bvh.qnodes, node);
             bool hl, hr;
+            int cl, cr;
             if constexpr (M::seg) {
-                hl = slab(nb.llo, nb.lhi, inv, oinv, tmin, tmax);
-                hr = slab(nb.rlo, nb.rhi, inv, oinv, tmin, tmax);
+                qnode_slab(bvh.qnodes, node, inv, oinv, tmin, tmax, hl, hr, cl, cr);
             } else {
+                const NodeBoxes nb = load_qnode(bvh.qnodes, node);
                 hl = inside(nb.llo, nb.lhi, x);
                 hr = inside(nb.rlo, nb.rhi, x);
+                cl = nb.l;
+                cr = nb.r;
             }
             int next = -1, other = -1;
             if (hl) {
-                if (nb.l < 0) {
-                    leaf0 = leaf_first(nb.l);
+                if (cl < 0) {
+                    leaf0 = leaf_first(cl);
                 } else {
-                    next = nb.l;
+                    next = cl;
                 }
             }
             if (hr) {
-                if (nb.r < 0) {
-                    leaf1 = leaf_first(nb.r);
+                if (cr < 0) {
+                    leaf1 = leaf_first(cr);
                 } else if (next < 0) {
-                    next = nb.r;
+                    next = cr;
                 } else {
-                    other = nb.r;
+                    other = cr;
                 }
             }
             if (other >= 0) {
