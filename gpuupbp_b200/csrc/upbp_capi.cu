@@ -292,6 +292,7 @@ struct upbp_ctx {
     HitState h_hit_state = {};
     unsigned long long* d_work_saved = nullptr;
     int search_grid[kRangeModes] = {};  // per range-query mode (kModePb2d ...)
+    int eval_grid[kRangeModes] = {};    // resident blocks of each evaluation kernel
     int camera_grid = 0;   // resident blocks of the persistent camera pass
     int light_grid = 0;    // resident blocks of the persistent light pass
     unsigned grid_limit = 0;  // cap on any launch's blocks (0: none), so that concurrent contexts share the SMs
@@ -1183,6 +1184,13 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
                 UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search[m], 128, 0));
                 c->search_grid[m] = std::max(1, sms * std::max(1, per_sm));
             }
+            const void* eval[kRangeModes] = {(const void*)range_eval_kernel<kModePb2d, false>,
+                                             (const void*)range_eval_kernel<kModeBb1d, false>,
+                                             (const void*)range_eval_kernel<kModeBp2d, false>};
+            for (int m = 0; m < kRangeModes; m++) {
+                UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eval[m], 128, 0));
+                c->eval_grid[m] = std::max(1, sms * std::max(1, per_sm));
+            }
             UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, camera_pass_kernel, 128, 0));
             c->camera_grid = std::max(1, sms * std::max(1, per_sm));
             UPBP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light_pass_kernel, 128, 0));
@@ -1658,7 +1666,14 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                     continue;
                 }
                 if (total > 0) {
-                    const unsigned g2 = grid_for((unsigned)total);
+                    // no more blocks than are resident: the blocks then sweep
+                    // the list once, side by side, and the records of the
+                    // pairs in flight (neighbours in the list share queries
+                    // and nearby beams) stay in L2; with more blocks every
+                    // wave of resident blocks swept the whole list and read
+                    // the records again
+                    const unsigned g2 = cap_grid(
+                        c, std::max(1u, std::min<unsigned>((unsigned)((total + 127) / 128), (unsigned)c->eval_grid[mode])));
                     const bool gd = P.guide.entries != nullptr;
                     switch (mode) {
                     case kModePb2d:
