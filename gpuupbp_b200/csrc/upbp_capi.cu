@@ -18,6 +18,7 @@
 #include "host/upbp_scene.h"
 #include "upbp_build.cuh"
 #include "upbp_camera_pass.cuh"
+#include "upbp_ploc.cuh"
 #include "upbp_light_pass.cuh"
 #include "upbp_scene_bvh.cuh"
 #include "upbp_kernel_table.h"
@@ -259,6 +260,10 @@ struct upbp_ctx {
     unsigned *d_chunk_counts = nullptr, *d_chunk_offsets = nullptr;
     uint2* d_chunks = nullptr;
     unsigned chunk_capacity = 0;
+    PlocScratch ploc;  // the beam map's clustering (sized with the chunks)
+    unsigned beam_map_passes = 0;  // clustering passes of the last beam map (0: LBVH)
+    int ploc_budget = kPlocPasses;  // passes launched for the next beam map
+    bool ploc_off = false;  // UPBP_BEAM_MAP=lbvh: the beam map as a Morton-split LBVH
     void* d_scan_temp = nullptr;
     size_t scan_temp_bytes = 0;
     unsigned last_chunks = 0;
@@ -810,6 +815,34 @@ int alloc_scratch(BuildScratch& sc, unsigned cap)
     return UPBP_OK;
 }
 
+void free_ploc(PlocScratch& ps)
+{
+    void* b[] = {ps.cl[0], ps.cl[1], ps.nn,      ps.flag,    ps.tile_sum, ps.node_box,
+                 ps.node_child, ps.node_place, ps.written, ps.order, ps.count};
+    for (void* x : b)
+        if (x) cudaFree(x);
+    ps = PlocScratch{};
+}
+
+// Clustering scratch for cap leaves; on failure none (the beam map is then
+// built as an LBVH).
+void alloc_ploc(PlocScratch& ps, unsigned cap)
+{
+    free_ploc(ps);
+    bool ok = dalloc(&ps.cl[0], 2 * (size_t)cap) == cudaSuccess && dalloc(&ps.cl[1], 2 * (size_t)cap) == cudaSuccess &&
+              dalloc(&ps.nn, cap) == cudaSuccess && dalloc(&ps.flag, cap) == cudaSuccess &&
+              dalloc(&ps.tile_sum, cap / kPlocTile + 1) == cudaSuccess &&
+              dalloc(&ps.node_box, 2 * (size_t)cap) == cudaSuccess && dalloc(&ps.node_child, cap) == cudaSuccess &&
+              dalloc(&ps.node_place, cap) == cudaSuccess && dalloc(&ps.written, cap) == cudaSuccess &&
+              dalloc(&ps.order, cap) == cudaSuccess && dalloc(&ps.count, kPcWords) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        free_ploc(ps);
+        return;
+    }
+    ps.capacity = cap;
+}
+
 void free_scratch(BuildScratch& sc)
 {
     cudaFree(sc.keys);
@@ -1169,6 +1202,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         UPBP_CK(dalloc(&c->d_hit_state, 1));
         UPBP_CK(dalloc(&c->d_work_saved, kCtrCount));
         c->max_hits = kMaxHits;
+        if (const char* e = std::getenv("UPBP_BEAM_MAP")) c->ploc_off = std::strcmp(e, "lbvh") == 0;
         if (const char* e = std::getenv("UPBP_MAX_HITS")) {
             const long long v = std::atoll(e);
             if (v > 0) c->max_hits = std::min<size_t>((size_t)v, kMaxHits);
@@ -1501,7 +1535,30 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
             src.chunks = c->d_chunks;
             src.dilate = beam_dilate;
             const unsigned* order = nullptr;
-            UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
+            bool clustered = false;
+            if (!c->ploc_off && nchunks > c->ploc.capacity) {
+                UPBP_CK(cudaStreamSynchronize(c->st));
+                alloc_ploc(c->ploc, nchunks + nchunks / 4);
+            }
+            if (nchunks >= 2 && nchunks <= c->ploc.capacity) {
+                // the passes the last build needed and a margin: a build that
+                // runs out falls back to the LBVH and the next gets them all
+                const int budget = c->ploc_budget;
+                const cudaError_t pe = build_ploc(src, nchunks, c->d_beam_nodes, c->sc, c->ploc, c->st, &order,
+                                                  &launches, &c->beam_map_passes, budget);
+                if (pe == cudaSuccess) {
+                    clustered = true;
+                    c->ploc_budget = (int)c->beam_map_passes + 4;
+                } else if (pe == cudaErrorNotReady) {
+                    c->ploc_budget = kPlocPasses;
+                } else {
+                    UPBP_CK(pe);
+                }
+            }
+            if (!clustered) {
+                c->beam_map_passes = 0;
+                UPBP_CK(build_lbvh(src, nchunks, c->d_beam_nodes, c->sc, c->st, &order));
+            }
             k_gather_chunks<<<(nchunks + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, nchunks,
                                                                       P.bb1d_used_light_subpath_count, c->d_beam_seg);
             if (nchunks > 1)
@@ -1509,7 +1566,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                                                                          c->d_beam_qnodes);
             P.beam_map.bvh.count = nchunks;
             c->last_chunks = nchunks;
-            launches += 2 + (nchunks > 1 ? 5 : 2) + 1;
+            launches += 3 + (nchunks > 1 ? 1 : 0) + (clustered ? 0 : (nchunks > 1 ? 4 : 2));
         }
         UPBP_CK(cudaGetLastError());
         P.n_surface = found[1];
@@ -1828,6 +1885,7 @@ extern "C" int upbp_get_stats(upbp_ctx* c, upbp_stats* o)
         o->d2h_bytes = (uint32_t)c->d2h_iter;
         o->kernel_launches = c->launches;
         o->ms_scene_bvh = c->ms_scene_bvh;
+        o->beam_map_passes = c->beam_map_passes;
         // per-pass times: the last iteration, and sums over the iterations run
         // since the previous stats call (up to the event ring size)
         for (unsigned k = 0; k < c->ev_pending; k++) {
@@ -2374,6 +2432,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     for (void* b : bufs)
         if (b) cudaFree(b);
     free_scratch(c->sc);
+    free_ploc(c->ploc);
     {
         GuideState& g = c->guide;
         guide_free_net(g.net);

@@ -65,6 +65,7 @@ class Stats(ctypes.Structure):
         ("segment_queries", ctypes.c_uint32), ("point_queries", ctypes.c_uint32),
         ("nee_samples", ctypes.c_uint32), ("bpt_pairs", ctypes.c_uint32),
         ("ms_guide", ctypes.c_double), ("ms_guide_sum", ctypes.c_double), ("ms_scene_bvh", ctypes.c_double),
+        ("beam_map_passes", ctypes.c_uint32),
     ]
 
 

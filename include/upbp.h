@@ -246,6 +246,10 @@ typedef struct upbp_stats {
     /* Device time of the scene BVH builds (both classes of triangles) in
      * upbp_create, including the host's orchestration of their levels. */
     double ms_scene_bvh;
+    /* Clustering passes that built the last iteration's beam map (0: the
+     * Morton-split LBVH, as with UPBP_BEAM_MAP=lbvh or when the clustering
+     * falls back). */
+    uint32_t beam_map_passes;
 } upbp_stats;
 
 /* Replaces: parse_commandline (gpuupbp/misc/config.cpp:735-1370).  Same
