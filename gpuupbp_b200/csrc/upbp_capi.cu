@@ -817,8 +817,10 @@ int alloc_scratch(BuildScratch& sc, unsigned cap)
 
 void free_ploc(PlocScratch& ps)
 {
-    void* b[] = {ps.cl[0], ps.cl[1], ps.nn,      ps.flag,    ps.tile_sum, ps.node_box,
-                 ps.node_child, ps.node_place, ps.written, ps.order, ps.count};
+    if (ps.exec) cudaGraphExecDestroy(ps.exec);
+    if (ps.capture) cudaStreamDestroy(ps.capture);
+    void* b[] = {ps.cl[0], ps.cl[1], ps.leaf,       ps.nn,      ps.flag,    ps.tile_sum,
+                 ps.node_box, ps.node_child, ps.node_place, ps.written, ps.order, ps.count};
     for (void* x : b)
         if (x) cudaFree(x);
     ps = PlocScratch{};
@@ -830,11 +832,13 @@ void alloc_ploc(PlocScratch& ps, unsigned cap)
 {
     free_ploc(ps);
     bool ok = dalloc(&ps.cl[0], 2 * (size_t)cap) == cudaSuccess && dalloc(&ps.cl[1], 2 * (size_t)cap) == cudaSuccess &&
+              dalloc(&ps.leaf, 2 * (size_t)cap) == cudaSuccess &&
               dalloc(&ps.nn, cap) == cudaSuccess && dalloc(&ps.flag, cap) == cudaSuccess &&
               dalloc(&ps.tile_sum, cap / kPlocTile + 1) == cudaSuccess &&
               dalloc(&ps.node_box, 2 * (size_t)cap) == cudaSuccess && dalloc(&ps.node_child, cap) == cudaSuccess &&
               dalloc(&ps.node_place, cap) == cudaSuccess && dalloc(&ps.written, cap) == cudaSuccess &&
               dalloc(&ps.order, cap) == cudaSuccess && dalloc(&ps.count, kPcWords) == cudaSuccess;
+    if (ok && cudaStreamCreateWithFlags(&ps.capture, cudaStreamNonBlocking) != cudaSuccess) ps.capture = nullptr;
     if (!ok) {
         cudaGetLastError();
         free_ploc(ps);

@@ -45,6 +45,7 @@ enum : int {
     kPcCur0,         // cluster buffer of an even / odd pass
     kPcCur1,
     kPcPasses,       // passes that merged
+    kPcN,            // leaves
     kPcBounds = 16,  // nodes created before pass t (kPlocPasses + 1 words)
     kPcWords = kPcBounds + kPlocPasses + 1
 };
@@ -54,6 +55,7 @@ enum : int {
 struct PlocScratch {
     unsigned capacity = 0;
     float4* cl[2] = {nullptr, nullptr};
+    float4* leaf = nullptr;        // leaf boxes in Morton order: (lo, 0), (hi, 0)
     int* nn = nullptr;
     unsigned* flag = nullptr;
     unsigned* tile_sum = nullptr;  // per tile of kPlocTile flags, then its exclusive prefix
@@ -63,6 +65,14 @@ struct PlocScratch {
     unsigned* written = nullptr;   // writes per laid-out node index (the check)
     unsigned* order = nullptr;     // laid-out leaf order: chunk per leaf position
     unsigned* count = nullptr;     // kPcWords words
+    // the launches after the leaves are set up, captured once as a graph
+    // (they read everything that varies from device memory); re-captured
+    // when the pass budget or a buffer changes
+    cudaStream_t capture = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int exec_budget = -1;
+    const void* exec_nodes = nullptr;
+    const void* exec_vals = nullptr;
 };
 
 UPBP_D float ploc_area(float3 lo, float3 hi)
@@ -75,7 +85,7 @@ UPBP_D float3 min3f(float3 a, float3 b) { return make_float3(fminf(a.x, b.x), fm
 UPBP_D float3 max3f(float3 a, float3 b) { return make_float3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
 
 // Leaves in Morton order (vals: chunk per Morton position).
-__global__ void k_ploc_init(BoxSource src, const unsigned* vals, unsigned n, float4* cl)
+__global__ void k_ploc_init(BoxSource src, const unsigned* vals, unsigned n, float4* cl, float4* leaf)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -83,6 +93,8 @@ __global__ void k_ploc_init(BoxSource src, const unsigned* vals, unsigned n, flo
     source_box(src, vals[i], lo, hi);
     cl[2 * i] = make_float4(lo.x, lo.y, lo.z, __int_as_float(~(int)i));
     cl[2 * i + 1] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(1u));
+    leaf[2 * i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    leaf[2 * i + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
 }
 
 // Cluster count and buffer of pass t; 0 clusters once the tail's size is
@@ -276,7 +288,7 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_compact(float4* cl0, float4
 // Places the children of created node k: writes the laid-out node at its
 // index (children's boxes and links), the children's places, and the leaf
 // order at the leaves' positions.
-UPBP_D void ploc_place(unsigned k, unsigned n, const BoxSource& src, const unsigned* vals, const float4* node_box,
+UPBP_D void ploc_place(unsigned k, unsigned n, const float4* leaf, const unsigned* vals, const float4* node_box,
                        const int2* node_child, int2* node_place, unsigned* written, unsigned* order, BvhNode* nodes,
                        unsigned* count)
 {
@@ -291,7 +303,8 @@ UPBP_D void ploc_place(unsigned k, unsigned n, const BoxSource& src, const unsig
     unsigned cnt[2];
     for (int s = 0; s < 2; s++) {
         if (c[s] < 0) {
-            source_box(src, vals[~c[s]], lo[s], hi[s]);
+            lo[s] = xyz(leaf[2 * ~c[s]]);
+            hi[s] = xyz(leaf[2 * ~c[s] + 1]);
             cnt[s] = 1u;
         } else {
             const float4 b0 = node_box[2 * c[s]], b1 = node_box[2 * c[s] + 1];
@@ -326,8 +339,8 @@ UPBP_D void ploc_place(unsigned k, unsigned n, const BoxSource& src, const unsig
 // root at leaf position 0 and index 0).  count[3] receives its iterations,
 // count[1] the clusters left (1 when it completed).
 __global__ void __launch_bounds__(kPlocTailThreads) k_ploc_tail(const float4* cl0, const float4* cl1, int passes,
-                                                                 unsigned n,
-                                                                 BoxSource src, const unsigned* vals, unsigned* count,
+                                                                 const float4* leaf, const unsigned* vals,
+                                                                 unsigned* count,
                                                                  float4* node_box, int2* node_child,
                                                                  int2* node_place, unsigned* written,
                                                                  unsigned* order, BvhNode* nodes)
@@ -341,6 +354,7 @@ __global__ void __launch_bounds__(kPlocTailThreads) k_ploc_tail(const float4* cl
     __shared__ unsigned s_nodes, s_m, s_warp[kPlocTailThreads / 32];
     const unsigned tid = threadIdx.x;
     const unsigned node_base = count[kPcNodes];
+    const unsigned n = count[kPcN];
     // the state after the last pass of the many-cluster phase
     const unsigned m = count[kPcM0 + (passes & 1)];
     const float4* cl = count[kPcCur0 + (passes & 1)] ? cl1 : cl0;
@@ -461,28 +475,31 @@ __global__ void __launch_bounds__(kPlocTailThreads) k_ploc_tail(const float4* cl
     __syncthreads();
     for (int t = it - 1; t >= 0; t--) {
         for (unsigned k = s_bounds[t] + tid; k < s_bounds[t + 1]; k += blockDim.x)
-            ploc_place(node_base + k, n, src, vals, node_box, node_child, node_place, written, order, nodes, count);
+            ploc_place(node_base + k, n, leaf, vals, node_box, node_child, node_place, written, order, nodes, count);
         __syncthreads();
     }
 }
 
 // Places of the nodes created in pass t of the many-cluster phase.
-__global__ void k_ploc_place(const unsigned* count_ro, int t, unsigned n, BoxSource src, const unsigned* vals,
-                             const float4* node_box, const int2* node_child, int2* node_place, unsigned* written,
-                             unsigned* order, BvhNode* nodes, unsigned* count)
+__global__ void k_ploc_place(int t, const float4* leaf, const unsigned* vals, const float4* node_box,
+                             const int2* node_child, int2* node_place, unsigned* written, unsigned* order,
+                             BvhNode* nodes, unsigned* count)
 {
-    const unsigned k0 = count_ro[kPcBounds + t], k1 = count_ro[kPcBounds + t + 1];
+    const unsigned k0 = count[kPcBounds + t], k1 = count[kPcBounds + t + 1], n = count[kPcN];
     for (unsigned k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < k1; k += gridDim.x * blockDim.x)
-        ploc_place(k, n, src, vals, node_box, node_child, node_place, written, order, nodes, count);
+        ploc_place(k, n, leaf, vals, node_box, node_child, node_place, written, order, nodes, count);
 }
 
 // The check: every internal index of the laid-out tree written exactly once
 // (then each node's children cover disjoint, smaller leaf ranges, and every
 // walk ends).
-__global__ void k_ploc_check(const unsigned* written, unsigned n_internal, unsigned* count)
+__global__ void k_ploc_check(const unsigned* written, unsigned* count)
 {
-    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n_internal && written[i] != 1u) atomicAdd(&count[kPcFail], 1u);
+    const unsigned n_internal = count[kPcN] - 1u;
+    unsigned bad = 0;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n_internal; i += gridDim.x * blockDim.x)
+        bad += written[i] != 1u;
+    if (bad) atomicAdd(&count[kPcFail], bad);
 }
 
 inline size_t ploc_tail_smem() { return (size_t)kPlocTail * 2 * sizeof(float4) + (size_t)kPlocTail * 8 + (kPlocTailIters + 1) * 4; }
@@ -518,31 +535,58 @@ inline cudaError_t build_ploc(const BoxSource& src, unsigned n, BvhNode* nodes, 
     static thread_local unsigned h_init[kPcWords];
     for (int i = 0; i < kPcWords; i++) h_init[i] = 0u;
     h_init[kPcM0] = n;
+    h_init[kPcN] = n;
     e = cudaMemcpyAsync(ps.count, h_init, sizeof(h_init), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(ps.written, 0, (size_t)(n - 1) * sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
-    k_ploc_init<<<grid, bs, 0, st>>>(src, vals, n, ps.cl[0]);
-    const unsigned g = std::min<unsigned>(kPlocGrid, (n + kPlocBlock - 1) / kPlocBlock);
-    for (int t = 0; t < budget; t++) {
-        k_ploc_nn<<<g, kPlocBlock, 0, st>>>(ps.cl[0], ps.cl[1], ps.count, t, ps.nn);
-        k_ploc_merge<<<g, kPlocBlock, 0, st>>>(ps.cl[0], ps.cl[1], ps.count, t, ps.nn, ps.node_box, ps.node_child,
-                                               ps.flag, ps.tile_sum);
-        k_ploc_tile_scan<<<1, 1024, 0, st>>>(ps.count, t, ps.tile_sum);
-        k_ploc_compact<<<g, kPlocBlock, 0, st>>>(ps.cl[0], ps.cl[1], ps.count, t, ps.flag, ps.tile_sum);
-    }
+    k_ploc_init<<<grid, bs, 0, st>>>(src, vals, n, ps.cl[0], ps.leaf);
     const size_t smem = ploc_tail_smem();
     e = cudaFuncSetAttribute(k_ploc_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_ploc_tail<<<1, kPlocTailThreads, smem, st>>>(ps.cl[0], ps.cl[1], budget, n, src, vals, ps.count,
-                                                   ps.node_box, ps.node_child, ps.node_place, ps.written, ps.order,
-                                                   nodes);
-    // places of the many-cluster phase's nodes, last pass first (a pass
-    // that merged nothing has an empty range)
-    for (int t = budget - 1; t >= 0; t--)
-        k_ploc_place<<<g, bs, 0, st>>>(ps.count, t, n, src, vals, ps.node_box, ps.node_child, ps.node_place,
-                                       ps.written, ps.order, nodes, ps.count);
-    k_ploc_check<<<(n - 1 + bs - 1) / bs, bs, 0, st>>>(ps.written, n - 1, ps.count);
+    // the passes, the tail, the places and the check: the same launches for
+    // every build with this budget and these buffers
+    auto sequence = [&](cudaStream_t s) {
+        const unsigned g = kPlocGrid;
+        for (int t = 0; t < budget; t++) {
+            k_ploc_nn<<<g, kPlocBlock, 0, s>>>(ps.cl[0], ps.cl[1], ps.count, t, ps.nn);
+            k_ploc_merge<<<g, kPlocBlock, 0, s>>>(ps.cl[0], ps.cl[1], ps.count, t, ps.nn, ps.node_box,
+                                                  ps.node_child, ps.flag, ps.tile_sum);
+            k_ploc_tile_scan<<<1, 1024, 0, s>>>(ps.count, t, ps.tile_sum);
+            k_ploc_compact<<<g, kPlocBlock, 0, s>>>(ps.cl[0], ps.cl[1], ps.count, t, ps.flag, ps.tile_sum);
+        }
+        k_ploc_tail<<<1, kPlocTailThreads, smem, s>>>(ps.cl[0], ps.cl[1], budget, ps.leaf, vals, ps.count,
+                                                      ps.node_box, ps.node_child, ps.node_place, ps.written,
+                                                      ps.order, nodes);
+        // places of the many-cluster phase's nodes, last pass first (a pass
+        // that merged nothing has an empty range)
+        for (int t = budget - 1; t >= 0; t--)
+            k_ploc_place<<<g, bs, 0, s>>>(t, ps.leaf, vals, ps.node_box, ps.node_child, ps.node_place, ps.written,
+                                          ps.order, nodes, ps.count);
+        k_ploc_check<<<g, bs, 0, s>>>(ps.written, ps.count);
+    };
+    if (!ps.exec || ps.exec_budget != budget || ps.exec_nodes != nodes || ps.exec_vals != vals) {
+        if (ps.exec) cudaGraphExecDestroy(ps.exec);
+        ps.exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        if (ps.capture && cudaStreamBeginCapture(ps.capture, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            sequence(ps.capture);
+            if (cudaStreamEndCapture(ps.capture, &graph) == cudaSuccess && graph) {
+                if (cudaGraphInstantiate(&ps.exec, graph, 0) != cudaSuccess) ps.exec = nullptr;
+                cudaGraphDestroy(graph);
+            }
+        }
+        cudaGetLastError();
+        ps.exec_budget = budget;
+        ps.exec_nodes = nodes;
+        ps.exec_vals = vals;
+    }
+    if (ps.exec) {
+        e = cudaGraphLaunch(ps.exec, st);
+        if (e != cudaSuccess) return e;
+    } else {
+        sequence(st);  // without a graph (capture unavailable)
+    }
     *launches += 7 + 5 * budget;
     unsigned res[kPcPasses + 1];
     e = cudaMemcpyAsync(res, ps.count, sizeof(res), cudaMemcpyDeviceToHost, st);
