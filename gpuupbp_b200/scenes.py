@@ -24,6 +24,7 @@ structure.
 from __future__ import annotations
 
 import math
+import contextlib
 import os
 from dataclasses import dataclass, field
 
@@ -122,6 +123,16 @@ class Camera:
 
 
 @dataclass
+@contextlib.contextmanager
+def _atomic_open(path: str):
+    """A text file opened under a temporary name of this process and
+    renamed to `path` when the block ends without an error."""
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        yield f
+    os.replace(tmp, path)
+
+
 class SceneBuilder:
     groups: list = field(default_factory=list)  # (material name, verts, faces, normals|None)
     materials: list = field(default_factory=list)
@@ -139,10 +150,14 @@ class SceneBuilder:
         return int(sum(len(g[2]) for g in self.groups))
 
     def write(self, obj_path: str):
+        """Writes the .mtl, .obj and .aux files.  Each file is written under a
+        name of this process and then renamed into place, so that processes
+        writing the same scene at once (the ranks of a multi-process run)
+        never read a partly written file."""
         base = os.path.basename(obj_path)
         mtl_name = base + ".mtl"
         d = os.path.dirname(obj_path) or "."
-        with open(os.path.join(d, mtl_name), "w") as fm:
+        with _atomic_open(os.path.join(d, mtl_name)) as fm:
             for m in self.materials:
                 fm.write(f"newmtl {m.name}\n")
                 fm.write("Kd %.6f %.6f %.6f\n" % m.kd)
@@ -150,7 +165,7 @@ class SceneBuilder:
                 fm.write("Ns %.6f\n" % m.ns)
                 if m.ke is not None:
                     fm.write("Ke %.6f %.6f %.6f\n" % m.ke)
-        with open(obj_path, "w") as fo:
+        with _atomic_open(obj_path) as fo:
             fo.write(f"mtllib {mtl_name}\n")
             voff, noff = 1, 1
             for mat, v, f, n in self.groups:
@@ -167,7 +182,7 @@ class SceneBuilder:
                 else:
                     np.savetxt(fo, fv, fmt="f %d %d %d")
                 voff += len(v)
-        with open(obj_path + ".aux", "w") as fa:
+        with _atomic_open(obj_path + ".aux") as fa:
             c = self.camera
             pos = np.array(c.position, np.float64)
             fwd = np.array(c.target, np.float64) - pos

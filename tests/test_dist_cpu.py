@@ -69,6 +69,8 @@ def test_two_rank_render_equals_single_rank(oracle_available):
     import sys
     world = 2
     with tempfile.TemporaryDirectory() as scene_dir:
+        from cases import prepare
+        prepare(CASE, scene_dir)  # the scene files exist before the ranks start
         mgr = mp.get_context("spawn").Manager()
         out = mgr.dict()
         mp.start_processes(_worker, args=(world, _free_port(), scene_dir, out, list(sys.path)), nprocs=world,
