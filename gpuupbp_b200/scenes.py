@@ -122,7 +122,6 @@ class Camera:
     hfov_deg: float
 
 
-@dataclass
 @contextlib.contextmanager
 def _atomic_open(path: str):
     """A text file opened under a temporary name of this process and
@@ -133,6 +132,7 @@ def _atomic_open(path: str):
     os.replace(tmp, path)
 
 
+@dataclass
 class SceneBuilder:
     groups: list = field(default_factory=list)  # (material name, verts, faces, normals|None)
     materials: list = field(default_factory=list)
