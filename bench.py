@@ -78,9 +78,10 @@ def measured_peaks() -> dict:
 
 class ClockSampler:
     """nvidia-smi clock / throttle-reason samples, started before the warm-up
-    (nvidia-smi's start-up stalls the host's CUDA calls for a while on a
-    freshly booted machine) and summarised over the samples taken inside the
-    timed region."""
+    once its first sample is in (nvidia-smi's start-up stalls the host's CUDA
+    calls for a while: started at the warm-up alone, it stalled the first
+    timed window by about a third of a second) and summarised over the
+    samples taken inside the timed region."""
 
     QUERY = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -92,7 +93,11 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Starts nvidia-smi and waits (up to 10 s) for its first sample:
+        its start-up (NVML initialisation) stalls the host's CUDA calls, so
+        it must be over before anything is timed."""
         import atexit
+        import threading
         atexit.register(self.stop)
         try:
             self.proc = subprocess.Popen(
@@ -100,6 +105,19 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        first = threading.Event()
+
+        def pump(stream):
+            for ln in stream:
+                if ln.strip():
+                    self.lines.append(ln.rstrip("\n"))
+                    first.set()
+            first.set()
+
+        self._reader = threading.Thread(target=pump, args=(self.proc.stdout,), daemon=True)
+        self._reader.start()
+        first.wait(timeout=10.0)
         return self
 
     def stop(self):
@@ -107,11 +125,11 @@ class ClockSampler:
             time.sleep(0.25)
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+                self.proc.wait()
+            self._reader.join(timeout=5)
             self.proc = None
 
     def summary(self, t0: float | None = None, t1: float | None = None) -> dict:

@@ -262,7 +262,12 @@ struct upbp_ctx {
     unsigned chunk_capacity = 0;
     PlocScratch ploc;  // the beam map's clustering (sized with the chunks)
     unsigned beam_map_passes = 0;  // clustering passes of the last beam map (0: LBVH)
+    unsigned* h_ploc = nullptr;    // page-locked outcome of the last clustering (kPcWords)
+    bool ploc_pending = false;     // its outcome is not read yet
+    BoxSource ploc_src{};          // the build's source and size, to replace the tree
+    unsigned ploc_n = 0;
     int ploc_budget = kPlocPasses;  // passes launched for the next beam map
+    int ploc_cap = kPlocPasses;     // UPBP_PLOC_PASSES: at most this many
     bool ploc_off = false;  // UPBP_BEAM_MAP=lbvh: the beam map as a Morton-split LBVH
     void* d_scan_temp = nullptr;
     size_t scan_temp_bytes = 0;
@@ -1033,6 +1038,7 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         UPBP_CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         UPBP_CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_status), sizeof(unsigned)));
         *c->h_status = 0;
+        UPBP_CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_ploc), kPcWords * sizeof(unsigned)));
         {
             // Set-up of the no-allocation query (upbp_debug_query_static):
             // the static array's device address on this device.  Its host-side
@@ -1207,6 +1213,11 @@ extern "C" int upbp_create(const upbp_scene_desc* s, const upbp_config* cfg, upb
         UPBP_CK(dalloc(&c->d_work_saved, kCtrCount));
         c->max_hits = kMaxHits;
         if (const char* e = std::getenv("UPBP_BEAM_MAP")) c->ploc_off = std::strcmp(e, "lbvh") == 0;
+        if (const char* e = std::getenv("UPBP_PLOC_PASSES")) {
+            const int v = std::atoi(e);
+            if (v > 0) c->ploc_cap = std::min(v, kPlocPasses);
+        }
+        c->ploc_budget = c->ploc_cap;
         if (const char* e = std::getenv("UPBP_MAX_HITS")) {
             const long long v = std::atoll(e);
             if (v > 0) c->max_hits = std::min<size_t>((size_t)v, kMaxHits);
@@ -1548,16 +1559,12 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 // the passes the last build needed and a margin: a build that
                 // runs out falls back to the LBVH and the next gets them all
                 const int budget = c->ploc_budget;
-                const cudaError_t pe = build_ploc(src, nchunks, c->d_beam_nodes, c->sc, c->ploc, c->st, &order,
-                                                  &launches, &c->beam_map_passes, budget);
-                if (pe == cudaSuccess) {
-                    clustered = true;
-                    c->ploc_budget = (int)c->beam_map_passes + 4;
-                } else if (pe == cudaErrorNotReady) {
-                    c->ploc_budget = kPlocPasses;
-                } else {
-                    UPBP_CK(pe);
-                }
+                UPBP_CK(build_ploc(src, nchunks, c->d_beam_nodes, c->sc, c->ploc, c->st, &order, &launches,
+                                   c->h_ploc, budget));
+                clustered = true;
+                c->ploc_pending = true;  // checked after the camera pass's synchronisation
+                c->ploc_src = src;
+                c->ploc_n = nchunks;
             }
             if (!clustered) {
                 c->beam_map_passes = 0;
@@ -1627,6 +1634,27 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 P.nee_color = c->d_nee_color;
                 P.bpt_color = c->d_bpt_color;
                 UPBP_CK(cudaMemsetAsync(c->d_cam_fb, 0, npx * sizeof(float), c->st));
+            }
+        }
+        if (c->ploc_pending) {
+            // the clustered beam map's outcome (copied before the camera pass,
+            // which the host has waited for); an incomplete tree is replaced
+            // by the LBVH before any search walks it
+            c->ploc_pending = false;
+            UPBP_CK(cudaStreamSynchronize(c->st));
+            const unsigned n = c->ploc_n;
+            if (ploc_complete(c->h_ploc, n)) {
+                c->beam_map_passes = c->h_ploc[kPcPasses] + c->h_ploc[kPcTailIters];
+                c->ploc_budget = std::min((int)c->h_ploc[kPcPasses] + 4, c->ploc_cap);
+            } else {
+                c->beam_map_passes = 0;
+                c->ploc_budget = c->ploc_cap;
+                const unsigned* order = nullptr;
+                UPBP_CK(build_lbvh(c->ploc_src, n, c->d_beam_nodes, c->sc, c->st, &order));
+                k_gather_chunks<<<(n + 255) / 256, 256, 0, c->st>>>(c->d_chunks, c->d_beams, order, n,
+                                                                    P.bb1d_used_light_subpath_count, c->d_beam_seg);
+                k_quantize<<<(n - 1 + 255) / 256, 256, 0, c->st>>>(c->d_beam_nodes, (int)n - 1, c->d_beam_qnodes);
+                launches += 7;
             }
         }
         UPBP_CK(cudaEventRecord(ev[3], c->st));
@@ -2423,6 +2451,7 @@ extern "C" void upbp_destroy(upbp_ctx* c)
     DeviceGuard dg(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_ploc) cudaFreeHost(c->h_ploc);
     void* bufs[] = {c->d_assert, c->mis.light, c->mis.camera, c->mis.events, c->mis.event_count, c->d_mat, c->d_med, c->d_lights, c->real.nodes, c->real.tri, c->real.normals, c->real.record,
                     c->d_env_img, c->d_env_dist, c->d_env_row_int, c->real.spheres, c->real.sph_mat, c->imag.spheres, c->imag.sph_mat,
                     c->imag.nodes, c->imag.tri, c->imag.normals, c->imag.record, c->d_vertices, c->d_path_count,

@@ -507,13 +507,14 @@ inline size_t ploc_tail_smem() { return (size_t)kPlocTail * 2 * sizeof(float4) +
 // Builds the n-leaf tree (n >= 2) over the boxes of `src` into `nodes`
 // (n - 1 nodes) and its leaf order (*sorted_vals): a fixed sequence of
 // launches (`budget` passes, at most kPlocPasses; a pass that finds the
-// tail's size reached does nothing), then one synchronisation for the
-// outcome.  Returns
-// cudaErrorNotReady, with nothing of the tree to use, if the passes ran out
-// (boxes so alike that few merge per pass) or the layout check failed.
-// *passes receives the passes that merged.
+// tail's size reached does nothing), and a copy of the outcome into the
+// page-locked words `outcome` (kPcWords).  Nothing waits for it: the caller
+// reads the outcome with ploc_complete after its next synchronisation with
+// the stream, and until then uses the tree for nothing; a tree that is not
+// complete (the passes ran out -- boxes so alike that few merge per pass --
+// or the layout check failed) is replaced.
 inline cudaError_t build_ploc(const BoxSource& src, unsigned n, BvhNode* nodes, BuildScratch& sc, PlocScratch& ps,
-                              cudaStream_t st, const unsigned** sorted_vals, unsigned* launches, unsigned* passes,
+                              cudaStream_t st, const unsigned** sorted_vals, unsigned* launches, unsigned* outcome,
                               int budget)
 {
     budget = std::max(1, std::min(budget, kPlocPasses));
@@ -588,15 +589,17 @@ inline cudaError_t build_ploc(const BoxSource& src, unsigned n, BvhNode* nodes, 
         sequence(st);  // without a graph (capture unavailable)
     }
     *launches += 7 + 5 * budget;
-    unsigned res[kPcPasses + 1];
-    e = cudaMemcpyAsync(res, ps.count, sizeof(res), cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(outcome, ps.count, kPcWords * sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return e;
-    *passes = res[kPcPasses];
-    if (res[kPcLeft] != 1u || res[kPcNodes] != n - 1 || res[kPcFail] != 0u) return cudaErrorNotReady;
     *sorted_vals = ps.order;
     return cudaGetLastError();
+}
+
+// Whether the build whose outcome words these are (n leaves) produced a
+// complete, checked tree.
+inline bool ploc_complete(const unsigned* outcome, unsigned n)
+{
+    return outcome[kPcLeft] == 1u && outcome[kPcNodes] == n - 1 && outcome[kPcFail] == 0u;
 }
 
 }  // namespace upbp

@@ -246,9 +246,11 @@ typedef struct upbp_stats {
     /* Device time of the scene BVH builds (both classes of triangles) in
      * upbp_create, including the host's orchestration of their levels. */
     double ms_scene_bvh;
-    /* Clustering passes that built the last iteration's beam map (0: the
-     * Morton-split LBVH, as with UPBP_BEAM_MAP=lbvh or when the clustering
-     * falls back). */
+    /* Clustering passes (many-cluster passes and the final block's
+     * iterations) that built the last iteration's beam map; 0: the
+     * Morton-split LBVH (UPBP_BEAM_MAP=lbvh, or the clustering fell back:
+     * its passes ran out -- UPBP_PLOC_PASSES caps them -- or its layout
+     * check failed). */
     uint32_t beam_map_passes;
 } upbp_stats;
 
