@@ -268,6 +268,7 @@ struct upbp_ctx {
     unsigned ploc_n = 0;
     int ploc_budget = kPlocPasses;  // passes launched for the next beam map
     int ploc_cap = kPlocPasses;     // UPBP_PLOC_PASSES: at most this many
+    int ploc_failures = 0;          // builds that ran out with every pass allowed
     bool ploc_off = false;  // UPBP_BEAM_MAP=lbvh: the beam map as a Morton-split LBVH
     void* d_scan_temp = nullptr;
     size_t scan_temp_bytes = 0;
@@ -1555,7 +1556,7 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 UPBP_CK(cudaStreamSynchronize(c->st));
                 alloc_ploc(c->ploc, nchunks + nchunks / 4);
             }
-            if (nchunks >= 2 && nchunks <= c->ploc.capacity) {
+            if (!c->ploc_off && nchunks >= 2 && nchunks <= c->ploc.capacity) {
                 // the passes the last build needed and a margin: a build that
                 // runs out falls back to the LBVH and the next gets them all
                 const int budget = c->ploc_budget;
@@ -1647,7 +1648,11 @@ extern "C" int upbp_run_iteration(upbp_ctx* c, int iteration)
                 c->beam_map_passes = c->h_ploc[kPcPasses] + c->h_ploc[kPcTailIters];
                 c->ploc_budget = std::min((int)c->h_ploc[kPcPasses] + 4, c->ploc_cap);
             } else {
+                // replaced by the LBVH; a context whose builds run out of
+                // passes even with all of them (boxes too alike to merge
+                // fast) builds the LBVH from then on
                 c->beam_map_passes = 0;
+                if (c->ploc_budget >= c->ploc_cap && ++c->ploc_failures >= 2) c->ploc_off = true;
                 c->ploc_budget = c->ploc_cap;
                 const unsigned* order = nullptr;
                 UPBP_CK(build_lbvh(c->ploc_src, n, c->d_beam_nodes, c->sc, c->st, &order));

@@ -29,7 +29,7 @@ constexpr int kPlocBlock = 256;
 constexpr int kPlocTile = 1024;    // flags per tile of the compaction's prefix sum
 constexpr int kPlocGrid = 148 * 8; // blocks of the many-cluster passes (grid-stride)
 constexpr int kPlocTailIters = 4 * kPlocTail;  // at least one merge per iteration
-constexpr int kPlocPasses = 48;    // most passes of the many-cluster phase
+constexpr int kPlocPasses = 96;    // most passes of the many-cluster phase
 
 // Device-side state of a build (unsigned words): the many-cluster passes
 // read their cluster count and buffer from the slots of their parity and
