@@ -606,7 +606,7 @@ UPBP_D const BvhView& range_map_bvh()
 
 constexpr int kSearchWarps = 4;
 constexpr unsigned kNoQuery = 0xffffffffu;  // no more queries in this round
-constexpr unsigned kCandRing = 64;  // > 31 waiting + 32 new pairs per round
+constexpr unsigned kCandRing = 128;  // > 31 waiting + 64 new pairs per step
 
 // The top kSmemStack entries of each lane's traversal stack live in shared
 // memory (column per lane, so lanes never share a bank); deeper entries go
@@ -898,18 +898,18 @@ __global__ void __launch_bounds__(128) range_search_kernel(int slot)
                 node = kWalkDone;
             }
         }
-        // each reached leaf becomes a waiting pair, in two rounds (a lane adds
-        // up to two); 32 waiting pairs are tested at once.  The walk tests
-        // compressed boxes, which contain the exact ones: the leaf test
-        // re-checks a chunk's own box where it matters.
+        // each reached leaf becomes a waiting pair (a lane adds up to two,
+        // next to each other); 32 waiting pairs are tested at once.  The
+        // walk tests compressed boxes, which contain the exact ones: the leaf
+        // test re-checks a chunk's own box where it matters.
+        {
+            const unsigned m0 = __ballot_sync(~0u, leaf0 >= 0), m1 = __ballot_sync(~0u, leaf1 >= 0);
+            unsigned at = tail + __popc(m0 & below) + __popc(m1 & below);
+            if (leaf0 >= 0) w.cand[at++ % kCandRing] = make_uint2(qk, (unsigned)leaf0 | (lane << kLeafShift));
+            if (leaf1 >= 0) w.cand[at % kCandRing] = make_uint2(qk, (unsigned)leaf1 | (lane << kLeafShift));
+            tail += __popc(m0) + __popc(m1);
 #pragma unroll 1
-        for (int side = 0; side < 2; side++) {
-            const int lv = side ? leaf1 : leaf0;
-            const unsigned m = __ballot_sync(~0u, lv >= 0);
-            if (lv >= 0)
-                w.cand[(tail + __popc(m & below)) % kCandRing] = make_uint2(qk, (unsigned)lv | (lane << kLeafShift));
-            tail += __popc(m);
-            if (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);
+            while (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);
         }
         if (__all_sync(~0u, exhausted && node == kWalkDone)) break;
     }
