@@ -792,15 +792,17 @@ __global__ void __launch_bounds__(128) range_search_kernel(int slot)
     float3 inv = v3(0.f), oinv = v3(0.f), x = v3(0.f);
     float tmin = 0.f, tmax = 0.f;
     unsigned qk = 0;
-    bool exhausted = false, overflow = false;
+    bool exhausted = false;  // no queries left for this warp (the same in every lane)
+    bool overflow = false;
     unsigned head = 0, tail = 0, hfill = 0;  // same values in every lane
     unsigned visits = 0, cand = 0, hits = 0;
     for (;;) {
         // primitives of the leaf children reached this step (a compressed
         // node's leaves hold one primitive each), -1 for none
         int leaf0 = -1, leaf1 = -1;
-        const bool idle = node == kWalkDone;
-        const unsigned want = __ballot_sync(~0u, idle && !exhausted);
+        const unsigned idle = __ballot_sync(~0u, node == kWalkDone);
+        if (exhausted && idle == ~0u) break;
+        const unsigned want = exhausted ? 0u : idle;
         if (want) {
             // a lane that takes a new query overwrites its geometry: test the
             // pairs still waiting first
@@ -814,11 +816,12 @@ __global__ void __launch_bounds__(128) range_search_kernel(int slot)
             if ((int)lane == leader && seen < p.hit_soft_limit)
                 base = atomicAdd(&p.hit_state->fetched, (unsigned)__popc(want));
             base = __shfl_sync(~0u, base, leader);
-            if (idle && !exhausted) {
+            // the queue is used up once a lane's index falls past its end
+            if (base == kNoQuery || base + (unsigned)__popc(want) > n) exhausted = true;
+            if ((want >> lane) & 1u) {
                 const unsigned r = base + __popc(want & below);
                 bool take = base != kNoQuery && r < n;
                 const unsigned j = p.query_begin + r;
-                exhausted = !take;
                 if (take) {
                     if constexpr (M::seg) {
                         qk = p.seg_order ? __ldg(&p.seg_order[j]) : j;
@@ -911,7 +914,6 @@ __global__ void __launch_bounds__(128) range_search_kernel(int slot)
 #pragma unroll 1
             while (tail - head >= 32) search_test_pairs<kMode>(w, head, 32, hfill, lane, cand, hits, seen);
         }
-        if (__all_sync(~0u, exhausted && node == kWalkDone)) break;
     }
     if (tail != head) search_test_pairs<kMode>(w, head, tail - head, hfill, lane, cand, hits, seen);
     __syncwarp();
