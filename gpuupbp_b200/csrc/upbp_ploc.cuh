@@ -14,8 +14,8 @@
 // a right child (the root at 0), so that its children are g and g + 1.  Every
 // internal node gets a distinct index that way, and the compressed nodes and
 // all walks read the result exactly as an LBVH.  The layout is checked on
-// the device (each index written once); the caller falls back to the LBVH
-// when the check fails or the clustering stalls.
+// the device (each index written once); the caller replaces the tree by the
+// LBVH when the check fails or the passes run out.
 #pragma once
 
 #include "upbp_build.cuh"
@@ -334,10 +334,11 @@ UPBP_D void ploc_place(unsigned k, unsigned n, const float4* leaf, const unsigne
         node_place[c[1]] = make_int2(g + 1, g + 1);
 }
 
-// The last m <= kPlocTail clusters, merged to one by a single block in
-// shared memory, then the places of the nodes it created (last first; the
-// root at leaf position 0 and index 0).  count[3] receives its iterations,
-// count[1] the clusters left (1 when it completed).
+// The last m <= kPlocTail clusters (the state after `passes` passes),
+// merged to one by a single block in shared memory, then the places of the
+// nodes it created (last first; the root at leaf position 0 and index 0).
+// count[kPcTailIters] receives its iterations, count[kPcLeft] the clusters
+// left (1 when it completed; the passes' count when they ran out).
 __global__ void __launch_bounds__(kPlocTailThreads) k_ploc_tail(const float4* cl0, const float4* cl1, int passes,
                                                                  const float4* leaf, const unsigned* vals,
                                                                  unsigned* count,
